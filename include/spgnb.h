@@ -1,0 +1,260 @@
+/*
+ * spgnb -- B200 short-range nonbonded engine for SPONGE (C ABI).
+ *
+ * The Lennard-Jones + PME direct-space pair force/energy/virial over a Verlet
+ * neighbour list, and the cell-list neighbour-list rebuild that feeds it.  The
+ * entry points mirror SPONGE's module API one call for one call:
+ *
+ *   NEIGHBOR_LIST               SPONGE/neighbor_list/neighbor_list.h:7-128
+ *   LENNARD_JONES_INFORMATION   SPONGE/Lennard_Jones_force/Lennard_Jones_force.h:86-173
+ *   SOLVENT_LENNARD_JONES       SPONGE/Lennard_Jones_force/solvent_LJ.h:9-43
+ *
+ * Conventions (same as the reference):
+ *   - coordinates, charges, forces, energies and virials are DEVICE pointers
+ *     owned by the caller; tables passed at creation are host pointers;
+ *   - frc, atom_energy and atom_virial are accumulated into (+=); the module's
+ *     own per-atom LJ energy and atom_direct_pme_energy are zeroed by the
+ *     callee when energy is requested (Lennard_Jones_force.cpp:376-382);
+ *   - charges are pre-scaled by 18.2223, LJ tables are the internal A = 12*A_file,
+ *     B = 6*B_file in triangular order max*(max+1)/2 + min;
+ *   - the cell is SPONGE's lower-triangular LTMatrix3 (row vectors), rcell its
+ *     inverse; any triclinic cell SPONGE accepts is accepted.
+ * Unlike the reference, every call returns a status instead of aborting the
+ * process; spgnb_last_error() holds the message of the last failure.
+ *
+ * All work is issued on the stream set with spgnb_set_stream (default: the
+ * legacy stream, as the reference) and no call synchronises the device except
+ * those documented as reading results back.
+ */
+#ifndef SPGNB_H
+#define SPGNB_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Layout-compatible with VECTOR (SPONGE/utils/vector.hpp:30-34). */
+typedef struct
+{
+    float x, y, z;
+} spgnb_vector;
+
+/* Layout-compatible with LTMatrix3 (SPONGE/utils/vector.hpp:256-258). */
+typedef struct
+{
+    float a11, a21, a22, a31, a32, a33;
+} spgnb_ltmatrix3;
+
+/* Layout-compatible with ATOM_GROUP (SPONGE/common.h:175-180): one half
+ * neighbour list per local atom, atom_serial pointing into one slab. */
+typedef struct
+{
+    int atom_numbers;
+    int ghost_numbers;
+    int* atom_serial;
+} spgnb_atom_group;
+
+enum
+{
+    SPGNB_OK = 0,
+    SPGNB_E_ARG = 1,         /* invalid argument (maps to spongeErrorValueErrorCommand) */
+    SPGNB_E_OOM = 2,         /* device allocation failed (spongeErrorMallocFailed) */
+    SPGNB_E_CUDA = 3,        /* CUDA runtime error */
+    SPGNB_E_OVERFLOW = 4,    /* a fixed-capacity buffer overflowed (spongeErrorOverflow) */
+    SPGNB_E_NONFINITE = 5,   /* non-finite force or energy (spongeErrorSimulationBreakDown) */
+    SPGNB_E_STATE = 6,       /* call out of order (e.g. force before the first list build) */
+    SPGNB_E_TIMEOUT = 7,     /* a bounded device-side wait gave up */
+    SPGNB_E_UNSUPPORTED = 8  /* configuration outside what this build implements */
+};
+
+const char* spgnb_version(void);
+const char* spgnb_status_string(int status);
+/* Message of the last failing call on this host thread. */
+const char* spgnb_last_error(void);
+/* Stream for all later launches issued by this host thread (a cudaStream_t). */
+int spgnb_set_stream(void* cuda_stream);
+/* Ewald beta from the direct-space tolerance: erfc(beta*rc)/rc == tol.
+ * Replaces Get_Beta, SPONGE/PM_force/PM_force.cpp:244-272. */
+float spgnb_get_beta(float cutoff, float tolerance);
+
+/* ----------------------------------------------------------- NEIGHBOR_LIST */
+typedef struct spgnb_nl spgnb_nl;
+
+/* The [neighbor_list] control keys of NEIGHBOR_LIST::Initial
+ * (neighbor_list.cpp:747-799, :134-160). */
+typedef struct
+{
+    int max_neighbor_numbers;      /* neighbor_list_max_neighbor_numbers, 1200 */
+    int max_atom_in_grid_numbers;  /* neighbor_list_max_atom_in_grid_numbers, 150 */
+    int max_ghost_in_grid_numbers; /* neighbor_list_max_ghost_in_grid_numbers, 150 */
+    int refresh_interval;          /* neighbor_list_refresh_interval, 0 = skin trigger */
+    float skin_permit;             /* neighbor_list_skin_permit, 0.5 */
+    int check_overflow_interval;   /* neighbor_list_check_overflow_interval, 150 */
+    int throw_error_when_overflow; /* neighbor_list_throw_error_when_overflow, 0 */
+    int export_atom_groups;        /* keep the ATOM_GROUP list (d_nl/d_temp) current, 1 */
+    int max_entries_per_cluster;   /* capacity of the internal cluster-pair list per
+                                      8-atom cluster; 0 = sized from the density */
+} spgnb_nl_options;
+
+void spgnb_nl_default_options(spgnb_nl_options* opt);
+
+/* NEIGHBOR_LIST::Initial (neighbor_list.h:17-18, neighbor_list.cpp:729-832).
+ * Grid cells of (cutoff+skin)/2, at least 3 per box dimension. */
+int spgnb_nl_create(int atom_numbers, float cutoff, float skin, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
+                    const spgnb_nl_options* opt, spgnb_nl** out);
+
+enum
+{
+    SPGNB_CONDITIONAL_UPDATE = 0,
+    SPGNB_FORCED_UPDATE = 1
+};
+
+/* NEIGHBOR_LIST::Update (neighbor_list.h:19-23, neighbor_list.cpp:834-885).
+ * Rebuilds when update == FORCED, or refresh_interval > 0 and
+ * (step+1) % refresh_interval == 0, or refresh_interval <= 0 and some atom
+ * moved more than skin*skin_permit since the last build (decided on the
+ * device, no host synchronisation).  The list holds every pair with
+ * atom_local[j] > atom_local[i] whose FP32 minimum-image distance^2 is below
+ * (cutoff+skin)^2, excluded pairs removed -- the reference's set, pair for
+ * pair.  One rank: ghost_numbers must be 0. */
+int spgnb_nl_update(spgnb_nl* nl, const int* d_atom_local, int local_atom_numbers, int ghost_numbers,
+                    const spgnb_vector* d_crd, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, int step, int update,
+                    const int* d_excluded_list_start, const int* d_excluded_list,
+                    const int* d_excluded_numbers);
+
+/* NEIGHBOR_LIST::Check_Overflow (neighbor_list.h:24-25, neighbor_list.cpp:887-965).
+ * On steps where (steps+1) % check_overflow_interval == 0 reads the overflow
+ * flags (synchronises); on overflow grows the buffers by 1.1x and sets
+ * *reinitialized (or returns SPGNB_E_OVERFLOW when throw_error_when_overflow). */
+int spgnb_nl_check_overflow(spgnb_nl* nl, int steps, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
+                            int* reinitialized);
+
+/* The reference-layout list (NEIGHBOR_LIST::d_nl / d_temp, neighbor_list.cpp:764-773)
+ * for other consumers: d_nl[i].atom_serial points at d_temp + i*max_neighbor_numbers.
+ * Kept current on each rebuild when export_atom_groups is set. */
+int spgnb_nl_atom_groups(spgnb_nl* nl, spgnb_atom_group** d_nl, int** d_temp);
+
+/* Host copy of the reference-layout list (the reference keeps h_nl for the
+ * same purpose): counts[local_atom_numbers] always, each atom's entries
+ * back to back in lists[] when capacity (in ints) suffices.  Returns the
+ * number of entries through *total.  Synchronises. */
+int spgnb_nl_copy_atom_groups(spgnb_nl* nl, int* h_counts, int* h_lists, long long capacity, long long* total);
+
+typedef struct
+{
+    int atom_numbers;
+    int grid_numbers;
+    int grid_dims[3];
+    int clusters;           /* 8-atom clusters of the last build */
+    long long entries;      /* cluster pairs with at least one listed pair */
+    int work_items;
+    long long builds;       /* rebuilds performed so far */
+    int overflow;           /* bit 0 list, 1 grid, 2 cluster-pair list */
+} spgnb_nl_stats;
+
+/* Reads counters back (synchronises the stream). */
+int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out);
+
+/* NEIGHBOR_LIST::Clear (neighbor_list.h:26, neighbor_list.cpp:967-981). */
+int spgnb_nl_destroy(spgnb_nl* nl);
+
+/* ----------------------------------------------- LENNARD_JONES_INFORMATION */
+typedef struct spgnb_lj spgnb_lj;
+
+/* LENNARD_JONES_INFORMATION::Initial (Lennard_Jones_force.h:117-118,
+ * Lennard_Jones_force.cpp:186-283): per-atom types and the internal pair
+ * tables (host pointers).  Also evaluates the long-range factor
+ * -2/3 pi sum_ij B_ij / rc^3 / 6 (Total_C6_Get, :146-184, :267-268) through a
+ * type histogram instead of the O(N^2) double loop, same value. */
+int spgnb_lj_create(int atom_numbers, int atom_type_numbers, const int* h_atom_type, const float* h_pair_A,
+                    const float* h_pair_B, float cutoff, spgnb_lj** out);
+
+/* LENNARD_JONES_INFORMATION::Get_Local (Lennard_Jones_force.h:134-135). */
+int spgnb_lj_get_local(spgnb_lj* lj, const int* d_atom_local, int local_atom_numbers, int ghost_numbers);
+
+/* LENNARD_JONES_INFORMATION::LJ_PME_Direct_Force_With_Atom_Energy_And_Virial
+ * (Lennard_Jones_force.h:138-144, Lennard_Jones_force.cpp:359-417) over the
+ * spgnb neighbour list.  Per pair inside the cutoff:
+ *   F/r = (B - A r^-6) r^-8 - q_i q_j r^-3 (erfc(beta r) + 2 beta r/sqrt(pi) e^-(beta r)^2),
+ *   frc_i += F/r dr, frc_j -= F/r dr, dr = r_j - r_i.
+ * Forces accumulate in int64 fixed point (2^-32 kcal/mol/A), so the result
+ * does not depend on summation order.  The pair energy and virial go to the
+ * pair's owner (the lower atom_local index, or for water sites when
+ * solvent_numbers > 0 the residue's first atom, as solvent_LJ.cpp:124-143
+ * does); totals are also reduced exactly and read with spgnb_lj_totals.
+ * All pairs are evaluated in this call, water included: the solvent module's
+ * call becomes a no-op (spgnb_solvent_pme_direct_force). */
+int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_numbers, int solvent_numbers,
+                              int ghost_numbers, const spgnb_vector* d_crd, const float* d_charge,
+                              spgnb_vector* d_frc, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
+                              const spgnb_nl* nl, float pme_beta, int need_atom_energy, float* d_atom_energy,
+                              int need_virial, spgnb_ltmatrix3* d_atom_virial, float* d_atom_direct_pme_energy);
+
+/* The same call over a reference-layout list produced by anyone (the exact
+ * signature of the reference method): atoms [0, local_atom_numbers -
+ * solvent_numbers) own their lists, the water tail is left to the solvent
+ * module, exactly as the reference splits the work. */
+int spgnb_lj_pme_direct_force_atom_groups(spgnb_lj* lj, int atom_numbers, int local_atom_numbers,
+                                          int solvent_numbers, int ghost_numbers, const spgnb_vector* d_crd,
+                                          const float* d_charge, spgnb_vector* d_frc, spgnb_ltmatrix3 cell,
+                                          spgnb_ltmatrix3 rcell, const spgnb_atom_group* d_nl, float pme_beta,
+                                          int need_atom_energy, float* d_atom_energy, int need_virial,
+                                          spgnb_ltmatrix3* d_atom_virial, float* d_atom_direct_pme_energy);
+
+/* LENNARD_JONES_INFORMATION::Long_Range_Correction (Lennard_Jones_force.h:168-170,
+ * Lennard_Jones_force.cpp:320-341): adds 2*factor/V to the virial diagonal and
+ * factor/V to the potential, element 0 only. */
+int spgnb_lj_long_range_correction(spgnb_lj* lj, int need_pressure, spgnb_ltmatrix3* d_virial,
+                                   int need_potential, float* d_potential, float volume);
+
+/* Step_Print (Lennard_Jones_force.cpp:419-433): LJ_short, LJ_long, LJ of the
+ * last energy step, plus the direct-space Coulomb energy.  Synchronises. */
+int spgnb_lj_energies(spgnb_lj* lj, double* lj_short, double* lj_long, double* lj_total, double* direct_coulomb);
+
+/* FP64 totals of the last force call: {E_lj, E_coulomb_direct, virial a11,
+ * a21, a22, a31, a32, a33} (symmetrised off-diagonals, as the per-atom
+ * virial).  Energy totals need need_atom_energy, the virial need_virial.
+ * Synchronises. */
+int spgnb_lj_totals(spgnb_lj* lj, double out[8]);
+
+/* Long-range factor computed at creation (host value). */
+double spgnb_lj_long_range_factor(const spgnb_lj* lj);
+
+int spgnb_lj_destroy(spgnb_lj* lj);
+
+/* --------------------------------------------------- SOLVENT_LENNARD_JONES */
+typedef struct spgnb_solvent spgnb_solvent;
+
+/* SOLVENT_LENNARD_JONES::Initial (solvent_LJ.h:23-25, solvent_LJ.cpp:148-247)
+ * for a trailing run of water_points-site residues (3 or 4). */
+int spgnb_solvent_create(spgnb_lj* lj, int water_points, spgnb_solvent** out);
+
+/* SOLVENT_LENNARD_JONES::Get_Local (solvent_LJ.h:41-42, solvent_LJ.cpp:433-482):
+ * counts the trailing water residues from residue lengths and masses (device
+ * pointers) and returns the solvent atom count (synchronises, as the reference). */
+int spgnb_solvent_get_local(spgnb_solvent* s, int local_res_numbers, const int* d_res_len, int atom_numbers,
+                            const float* d_mass, int* local_solvent_numbers);
+
+/* SOLVENT_LENNARD_JONES::LJ_PME_Direct_Force_With_Atom_Energy_And_Virial
+ * (solvent_LJ.h:26-32, solvent_LJ.cpp:255-431) over a reference-layout list:
+ * water residues from d_res_start[solvent_start_local..residue_numbers), all
+ * sites against the first site's list.  Over an spgnb list (nl != NULL) the
+ * water pairs were already evaluated by spgnb_lj_pme_direct_force and this
+ * call returns immediately. */
+int spgnb_solvent_pme_direct_force(spgnb_solvent* s, int atom_numbers, int residue_numbers,
+                                   const int* d_res_start, const spgnb_vector* d_crd, const float* d_charge,
+                                   spgnb_vector* d_frc, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
+                                   const spgnb_nl* nl, const spgnb_atom_group* d_nl, float pme_beta,
+                                   int need_atom_energy, float* d_atom_energy, int need_virial,
+                                   spgnb_ltmatrix3* d_atom_virial, float* d_atom_direct_pme_energy);
+
+int spgnb_solvent_destroy(spgnb_solvent* s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SPGNB_H */

@@ -1,0 +1,214 @@
+"""Python access to the oracle (TEST INFRASTRUCTURE ONLY).
+
+``Oracle`` wraps ``libspgnb_oracle.so`` (the C restatement in
+``spgnb_oracle.c``); ``Reference`` wraps ``_ref/libspgref_cpu.so`` or
+``_ref/libspgref_cuda.so`` (the reference's own code, built from its sources
+by ``oracle/Makefile``).  Only the tests, the smoke check and the benchmark's
+CPU-baseline leg import this module, as the checker.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def _load(name):
+    path = os.path.join(HERE, name)
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is not built (make -C oracle)")
+    return C.CDLL(path)
+
+
+def _c32(a):
+    return np.ascontiguousarray(a, np.float32)
+
+
+def _ci32(a):
+    return np.ascontiguousarray(a, np.int32)
+
+
+class Oracle:
+    def __init__(self):
+        lib = _load("libspgnb_oracle.so")
+        lib.orc_beta.restype = C.c_float
+        lib.orc_beta.argtypes = [C.c_float, C.c_float]
+        lib.orc_nl_build.restype = C.c_longlong
+        lib.orc_nl_build.argtypes = [C.c_int, _f32p, _f32p, _f32p, C.c_float, C.c_float, _i32p, _i32p, _i32p,
+                                     C.c_int, _i32p, C.c_void_p, C.c_longlong]
+        lib.orc_pair_force_fp64.restype = C.c_longlong
+        lib.orc_pair_force_fp64.argtypes = [C.c_int, _f32p, _f32p, _i32p, _f32p, _f32p, _f32p, C.c_float,
+                                            C.c_float, _i32p, _i32p, _f64p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, _f64p]
+        lib.orc_direct_sum_fp64.restype = C.c_longlong
+        lib.orc_direct_sum_fp64.argtypes = [C.c_int, _f32p, _f32p, _i32p, _f32p, _f32p, _f32p, C.c_float,
+                                            C.c_float, _i32p, _i32p, _i32p, _f64p, C.c_void_p, C.c_void_p,
+                                            C.c_void_p, _f64p]
+        lib.orc_long_range_factor.restype = C.c_double
+        lib.orc_long_range_factor.argtypes = [C.c_int, _i32p, C.c_int, _f32p, C.c_float]
+        lib.orc_pair_dr2.restype = C.c_float
+        lib.orc_pair_dr2.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int]
+        self.lib = lib
+
+    def beta(self, cutoff, tol=1e-5):
+        return float(self.lib.orc_beta(cutoff, tol))
+
+    def nl_build(self, s, crd=None, mode=1):
+        """Reference half list as (counts[n], lists) with each list sorted."""
+        crd = _c32(s.crd if crd is None else crd)
+        n = s.n
+        counts = np.zeros(n, np.int32)
+        args = (n, crd, _c32(s.cell), _c32(s.rcell), s.cutoff, s.skin, _ci32(s.excl_start),
+                _ci32(s.excl_numbers), _ci32(s.excl_list if len(s.excl_list) else np.zeros(1, np.int32)), mode)
+        total = self.lib.orc_nl_build(*args, counts, None, 0)
+        if total < 0:
+            raise RuntimeError(f"oracle neighbour build failed ({total})")
+        lists = np.zeros(max(int(total), 1), np.int32)
+        total2 = self.lib.orc_nl_build(*args, counts, lists.ctypes.data_as(C.c_void_p), int(total))
+        assert total2 == total
+        return counts, lists[:total]
+
+    def pair_force(self, s, counts, lists, crd=None, per_atom=True):
+        crd = _c32(s.crd if crd is None else crd)
+        n = s.n
+        frc = np.zeros(3 * n, np.float64)
+        elj = np.zeros(n, np.float64) if per_atom else None
+        ec = np.zeros(n, np.float64) if per_atom else None
+        vir = np.zeros(6 * n, np.float64) if per_atom else None
+        tot = np.zeros(8, np.float64)
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        npairs = self.lib.orc_pair_force_fp64(n, crd, _c32(s.charge), _ci32(s.atom_type), _c32(s.pair_A),
+                                              _c32(s.pair_B), _c32(s.cell), s.cutoff, s.beta, _ci32(counts),
+                                              _ci32(lists if len(lists) else np.zeros(1, np.int32)), frc,
+                                              ptr(elj), ptr(ec), ptr(vir), tot)
+        return _result(frc, elj, ec, vir, tot, npairs)
+
+    def direct_sum(self, s, crd=None, per_atom=False):
+        crd = _c32(s.crd if crd is None else crd)
+        n = s.n
+        frc = np.zeros(3 * n, np.float64)
+        elj = np.zeros(n, np.float64) if per_atom else None
+        ec = np.zeros(n, np.float64) if per_atom else None
+        vir = np.zeros(6 * n, np.float64) if per_atom else None
+        tot = np.zeros(8, np.float64)
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        npairs = self.lib.orc_direct_sum_fp64(n, crd, _c32(s.charge), _ci32(s.atom_type), _c32(s.pair_A),
+                                              _c32(s.pair_B), _c32(s.cell), s.cutoff, s.beta,
+                                              _ci32(s.excl_start), _ci32(s.excl_numbers),
+                                              _ci32(s.excl_list if len(s.excl_list) else np.zeros(1, np.int32)),
+                                              frc, ptr(elj), ptr(ec), ptr(vir), tot)
+        return _result(frc, elj, ec, vir, tot, npairs)
+
+    def long_range_factor(self, s):
+        return float(self.lib.orc_long_range_factor(s.n, _ci32(s.atom_type), s.n_types, _c32(s.pair_B),
+                                                    s.cutoff))
+
+
+def _result(frc, elj, ec, vir, tot, npairs):
+    return {
+        "frc": frc.reshape(-1, 3),
+        "e_lj_atom": elj,
+        "e_coul_atom": ec,
+        "virial_atom": None if vir is None else vir.reshape(-1, 6),
+        "e_lj": float(tot[0]),
+        "e_coul": float(tot[1]),
+        "virial": tot[2:8].copy(),
+        "pairs_in_cutoff": int(npairs),
+    }
+
+
+class Reference:
+    """The reference's own implementation of the path (CPU or CUDA build)."""
+
+    def __init__(self, gpu=False):
+        lib = _load(os.path.join("_ref", "libspgref_cuda.so" if gpu else "libspgref_cpu.so"))
+        lib.ref_init.argtypes = [C.c_int, C.c_int, _i32p, _f32p, _f32p, C.c_float, C.c_float, _f32p, _f32p,
+                                 C.c_int, C.c_int, _i32p, _i32p, _i32p, C.c_int]
+        lib.ref_nl_update.argtypes = [_f32p, C.c_int, C.c_int]
+        lib.ref_nl_get.restype = C.c_longlong
+        lib.ref_nl_get.argtypes = [_i32p, C.c_void_p, C.c_longlong, C.c_void_p]
+        lib.ref_force.argtypes = [_f32p, _f32p, C.c_float, C.c_int, C.c_int, _f32p, C.c_void_p, C.c_void_p,
+                                  C.c_void_p, C.c_void_p]
+        lib.ref_time_steps.restype = C.c_double
+        lib.ref_time_steps.argtypes = [_f32p, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int]
+        lib.ref_time_rebuild.restype = C.c_double
+        lib.ref_time_rebuild.argtypes = [_f32p, C.c_int]
+        lib.ref_long_range_factor.restype = C.c_double
+        lib.ref_enable_solvent.argtypes = [C.c_int, _i32p, C.c_int, C.c_int]
+        lib.ref_set_threads.argtypes = [C.c_int]
+        self.lib = lib
+        self.gpu = bool(lib.ref_is_gpu())
+        self.s = None
+
+    def set_threads(self, t):
+        self.lib.ref_set_threads(int(t))
+
+    def init(self, s, max_neighbor=1200, refresh_interval=0, solvent=False):
+        self.s = s
+        ex = _ci32(s.excl_list if len(s.excl_list) else np.zeros(1, np.int32))
+        self.lib.ref_init(s.n, s.n_types, _ci32(s.atom_type), _c32(s.pair_A), _c32(s.pair_B), s.cutoff, s.skin,
+                          _c32(s.cell), _c32(s.rcell), max_neighbor, refresh_interval, _ci32(s.excl_start),
+                          _ci32(s.excl_numbers), ex, len(s.excl_list))
+        if solvent:
+            first_res = len(s.res_start) - s.n_waters
+            rc = self.lib.ref_enable_solvent(len(s.res_start), _ci32(s.res_start), first_res, 3 * s.n_waters)
+            if rc != 0:
+                raise RuntimeError("the solvent module exists only in the reference's GPU build")
+
+    def nl_update(self, crd=None, step=0, forced=True):
+        self.lib.ref_nl_update(_c32(self.s.crd if crd is None else crd), step, 1 if forced else 0)
+
+    def nl_get(self, sort=True):
+        n = self.s.n
+        counts = np.zeros(n, np.int32)
+        total = self.lib.ref_nl_get(counts, None, 0, None)
+        lists = np.zeros(max(int(total), 1), np.int32)
+        flags = np.zeros(2, np.int32)
+        self.lib.ref_nl_get(counts, lists.ctypes.data_as(C.c_void_p), int(total), flags.ctypes.data_as(C.c_void_p))
+        lists = lists[:total]
+        if sort:
+            off = 0
+            for i in range(n):
+                c = int(counts[i])
+                lists[off:off + c].sort()
+                off += c
+        return counts, lists, flags
+
+    def force(self, crd=None, need_energy=True, need_virial=True):
+        s = self.s
+        n = s.n
+        frc = np.zeros(3 * n, np.float32)
+        e = np.zeros(n, np.float32)
+        v = np.zeros(6 * n, np.float32)
+        d = np.zeros(n, np.float32)
+        lj = np.zeros(n, np.float32)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)
+        self.lib.ref_force(_c32(s.crd if crd is None else crd), _c32(s.charge), s.beta, int(need_energy),
+                           int(need_virial), frc, p(e), p(v), p(d), p(lj))
+        return {"frc": frc.reshape(-1, 3), "atom_energy": e, "atom_virial": v.reshape(-1, 6),
+                "atom_direct": d, "atom_lj": lj}
+
+    def time_steps(self, steps, first_step=0, need_energy=False, need_virial=False, crd=None):
+        s = self.s
+        return float(self.lib.ref_time_steps(_c32(s.crd if crd is None else crd), _c32(s.charge), s.beta,
+                                             first_step, steps, int(need_energy), int(need_virial)))
+
+    def time_rebuild(self, reps=1, crd=None):
+        return float(self.lib.ref_time_rebuild(_c32(self.s.crd if crd is None else crd), reps))
+
+    def long_range_factor(self):
+        return float(self.lib.ref_long_range_factor())
+
+    def clear(self):
+        self.lib.ref_clear()

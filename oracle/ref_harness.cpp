@@ -1,0 +1,351 @@
+// Reference harness -- TEST INFRASTRUCTURE ONLY.
+//
+// Plain C entry points over the reference's own module classes
+// (NEIGHBOR_LIST, LENNARD_JONES_INFORMATION, SOLVENT_LENNARD_JONES), compiled
+// from the reference sources where they lie (oracle/Makefile).  The CPU build
+// generates golden fixtures and is the timed CPU baseline; the CUDA build runs
+// the reference's own kernels on a B200 for the reference-kernel parity check
+// and the speed comparison.  The product never loads this library.
+//
+// The call sequence mirrors SPONGE/main.cpp: Main_Refresh_Local_State
+// (FORCED_UPDATE, :571; lj.Get_Local, :581) and Main_Calculate_Force
+// (CONDITIONAL_UPDATE, :307-311; LJ, :371-377; solvent LJ, :387-392).
+#include <fcntl.h>
+#include <unistd.h>
+
+#include <chrono>
+
+#include "Lennard_Jones_force/Lennard_Jones_force.h"
+#include "Lennard_Jones_force/solvent_LJ.h"
+#include "common.h"
+#include "control.h"
+#include "neighbor_list/neighbor_list.h"
+#include "xponge/xponge.h"
+
+CONTROLLER controller;
+namespace Xponge
+{
+System system;
+}
+
+namespace
+{
+struct Quiet
+{
+    int saved = -1;
+    Quiet()
+    {
+        fflush(stdout);
+        saved = dup(1);
+        int devnull = open("/dev/null", O_WRONLY);
+        if (devnull >= 0)
+        {
+            dup2(devnull, 1);
+            close(devnull);
+        }
+    }
+    ~Quiet()
+    {
+        fflush(stdout);
+        if (saved >= 0)
+        {
+            dup2(saved, 1);
+            close(saved);
+        }
+    }
+};
+
+struct State
+{
+    int n = 0;
+    int max_neighbor = 1200;
+    float cutoff = 10.0f, skin = 2.0f;
+    LTMatrix3 cell, rcell;
+    NEIGHBOR_LIST* nl = nullptr;
+    LENNARD_JONES_INFORMATION* lj = nullptr;
+    SOLVENT_LENNARD_JONES* slj = nullptr;
+    LJ_SOFT_CORE* lj_soft = nullptr;
+    int* d_atom_local = nullptr;
+    VECTOR* d_crd = nullptr;
+    float* d_charge = nullptr;
+    VECTOR* d_frc = nullptr;
+    float* d_energy = nullptr;
+    LTMatrix3* d_virial = nullptr;
+    float* d_direct = nullptr;
+    int *d_excl_start = nullptr, *d_excl_list = nullptr, *d_excl_num = nullptr;
+    int* d_res_start = nullptr;
+    int res_numbers = 0;
+    int solvent_atoms = 0;
+} S;
+
+template <typename T>
+T* dev_alloc(size_t count)
+{
+    void* p = nullptr;
+    Device_Malloc_Safely(&p, sizeof(T) * (count > 0 ? count : 1));
+    return (T*)p;
+}
+
+template <typename T>
+void to_dev(T* dst, const T* src, size_t count)
+{
+    if (count) deviceMemcpy(dst, src, sizeof(T) * count, deviceMemcpyHostToDevice);
+}
+
+template <typename T>
+void to_host(T* dst, const T* src, size_t count)
+{
+    if (count) deviceMemcpy(dst, src, sizeof(T) * count, deviceMemcpyDeviceToHost);
+}
+
+LTMatrix3 ltm(const float* m) { return LTMatrix3(m[0], m[1], m[2], m[3], m[4], m[5]); }
+
+void sync_device()
+{
+#ifdef USE_GPU
+    cudaDeviceSynchronize();
+#endif
+}
+}  // namespace
+
+extern "C" {
+
+int ref_is_gpu()
+{
+#ifdef USE_GPU
+    return 1;
+#else
+    return 0;
+#endif
+}
+
+void ref_set_threads(int threads)
+{
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+}
+
+// NEIGHBOR_LIST::Initial + LENNARD_JONES_INFORMATION::Initial + Get_Local
+// (identity atom_local, one rank, no ghosts).  refresh_interval <= 0 selects
+// the skin-triggered rebuild.
+int ref_init(int n, int n_types, const int* types, const float* pair_A, const float* pair_B, float cutoff,
+             float skin, const float* cell, const float* rcell, int max_neighbor, int refresh_interval,
+             const int* excl_start, const int* excl_numbers, const int* excl_list, int n_excl)
+{
+    Quiet q;
+    S.n = n;
+    S.cutoff = cutoff;
+    S.skin = skin;
+    S.cell = ltm(cell);
+    S.rcell = ltm(rcell);
+    S.max_neighbor = max_neighbor;
+    controller.commands["neighbor_list_max_neighbor_numbers"] = std::to_string(max_neighbor);
+    if (refresh_interval > 0)
+        controller.commands["neighbor_list_refresh_interval"] = std::to_string(refresh_interval);
+    else
+        controller.commands.erase("neighbor_list_refresh_interval");
+
+    auto& lj = Xponge::system.classical_force_field.lj;
+    int p = n_types * (n_types + 1) / 2;
+    lj.atom_type.assign(types, types + n);
+    lj.pair_A.assign(pair_A, pair_A + p);
+    lj.pair_B.assign(pair_B, pair_B + p);
+    lj.atom_type_numbers = n_types;
+
+    S.nl = new NEIGHBOR_LIST();
+    S.nl->Initial(&controller, n, cutoff, skin, S.cell, S.rcell);
+    S.lj = new LENNARD_JONES_INFORMATION();
+    S.lj->Initial(&controller, cutoff, NULL);
+
+    std::vector<int> ident(n);
+    for (int i = 0; i < n; i++) ident[i] = i;
+    S.d_atom_local = dev_alloc<int>(n);
+    to_dev(S.d_atom_local, ident.data(), n);
+    S.d_crd = dev_alloc<VECTOR>(n);
+    S.d_charge = dev_alloc<float>(n);
+    S.d_frc = dev_alloc<VECTOR>(n);
+    S.d_energy = dev_alloc<float>(n);
+    S.d_virial = dev_alloc<LTMatrix3>(n);
+    S.d_direct = dev_alloc<float>(n);
+    S.d_excl_start = dev_alloc<int>(n);
+    S.d_excl_num = dev_alloc<int>(n);
+    S.d_excl_list = dev_alloc<int>(n_excl);
+    to_dev(S.d_excl_start, excl_start, n);
+    to_dev(S.d_excl_num, excl_numbers, n);
+    to_dev(S.d_excl_list, excl_list, n_excl);
+    S.lj->Get_Local(S.d_atom_local, n, 0);
+    sync_device();
+    return 0;
+}
+
+double ref_long_range_factor() { return S.lj ? (double)S.lj->long_range_factor : 0.0; }
+
+// NEIGHBOR_LIST::Update with the step counter and the forced flag.
+int ref_nl_update(const float* crd, int step, int forced)
+{
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    S.nl->Update(S.d_atom_local, S.n, 0, S.d_crd, S.cell, S.rcell, step,
+                 forced ? NEIGHBOR_LIST::FORCED_UPDATE : NEIGHBOR_LIST::CONDITIONAL_UPDATE, S.d_excl_start,
+                 S.d_excl_list, S.d_excl_num);
+    sync_device();
+    return 0;
+}
+
+// Copies the half list out: counts[n] always, lists when capacity suffices.
+// Returns the total number of entries.
+long long ref_nl_get(int* counts, int* lists, long long capacity, int* overflow_flags)
+{
+    std::vector<ATOM_GROUP> h(S.n);
+    to_host(h.data(), S.nl->d_nl, S.n);
+    long long total = 0;
+    for (int i = 0; i < S.n; i++)
+    {
+        counts[i] = h[i].atom_numbers;
+        total += h[i].atom_numbers;
+    }
+    if (lists && capacity >= total)
+    {
+        long long off = 0;
+        for (int i = 0; i < S.n; i++)
+        {
+            int c = h[i].atom_numbers < S.max_neighbor ? h[i].atom_numbers : S.max_neighbor;
+            to_host(lists + off, h[i].atom_serial, c);
+            off += h[i].atom_numbers;
+        }
+    }
+    if (overflow_flags)
+    {
+        to_host(&overflow_flags[0], S.nl->d_neighbor_list_overflow, 1);
+        to_host(&overflow_flags[1], S.nl->d_neighbor_grid_overflow, 1);
+    }
+    return total;
+}
+
+// The water-residue module, configured the way SOLVENT_LENNARD_JONES::Initial
+// and Get_Local leave it for a trailing run of 3-site waters
+// (solvent_LJ.cpp:186-228, :469-482).  GPU build only: the reference disables
+// the module on CPU builds (solvent_LJ.cpp:183-185).
+int ref_enable_solvent(int res_numbers, const int* res_start, int first_water_residue, int solvent_atoms)
+{
+#ifdef USE_GPU
+    S.lj_soft = new LJ_SOFT_CORE();
+    S.slj = new SOLVENT_LENNARD_JONES();
+    S.slj->lj_info = S.lj;
+    S.slj->lj_soft_info = S.lj_soft;
+    S.slj->water_points = 3;
+    S.slj->solvent_numbers = solvent_atoms;
+    S.slj->solvent_start = first_water_residue;
+    S.slj->solvent_start_local = first_water_residue;
+    S.slj->local_solvent_numbers = solvent_atoms;
+    S.slj->is_initialized = 1;
+    S.res_numbers = res_numbers;
+    S.d_res_start = dev_alloc<int>(res_numbers);
+    to_dev(S.d_res_start, res_start, res_numbers);
+    S.solvent_atoms = solvent_atoms;
+    return 0;
+#else
+    (void)res_numbers;
+    (void)res_start;
+    (void)first_water_residue;
+    (void)solvent_atoms;
+    return -1;
+#endif
+}
+
+// One force evaluation.  Outputs are overwritten: the harness zeroes the
+// accumulated arrays the way MD_core / DD do before the call.
+int ref_force(const float* crd, const float* charge, float beta, int need_energy, int need_virial, float* frc,
+              float* atom_energy, float* atom_virial, float* atom_direct, float* atom_lj)
+{
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    to_dev(S.d_charge, charge, S.n);
+    deviceMemset(S.d_frc, 0, sizeof(VECTOR) * S.n);
+    deviceMemset(S.d_energy, 0, sizeof(float) * S.n);
+    deviceMemset(S.d_virial, 0, sizeof(LTMatrix3) * S.n);
+    deviceMemset(S.d_direct, 0, sizeof(float) * S.n);
+    int solvent = S.slj ? S.slj->local_solvent_numbers : 0;
+    S.lj->LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(S.n, S.n, solvent, 0, S.d_crd, S.d_charge, S.d_frc,
+                                                           S.cell, S.rcell, S.nl->d_nl, beta, need_energy,
+                                                           S.d_energy, need_virial, S.d_virial, S.d_direct);
+    if (S.slj)
+        S.slj->LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(S.n, S.res_numbers, S.d_res_start, S.d_crd,
+                                                                S.d_charge, S.d_frc, S.cell, S.rcell, S.nl->d_nl,
+                                                                beta, need_energy, S.d_energy, need_virial,
+                                                                S.d_virial, S.d_direct);
+    sync_device();
+    to_host((VECTOR*)frc, S.d_frc, S.n);
+    if (atom_energy) to_host(atom_energy, S.d_energy, S.n);
+    if (atom_virial) to_host((LTMatrix3*)atom_virial, S.d_virial, S.n);
+    if (atom_direct) to_host(atom_direct, S.d_direct, S.n);
+    if (atom_lj) to_host(atom_lj, S.lj->d_LJ_energy_atom, S.n);
+    return 0;
+}
+
+// Timed loop of the path the way Main_Calculate_Force runs it: per step a
+// conditional neighbour-list update then the LJ + PME-direct force (and the
+// solvent module when enabled).  Coordinates and charges are uploaded once;
+// the returned seconds cover only the loop.
+double ref_time_steps(const float* crd, const float* charge, float beta, int first_step, int steps,
+                      int need_energy, int need_virial)
+{
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    to_dev(S.d_charge, charge, S.n);
+    int solvent = S.slj ? S.slj->local_solvent_numbers : 0;
+    sync_device();
+    auto t0 = std::chrono::steady_clock::now();
+    {
+        Quiet q;
+        for (int s = first_step; s < first_step + steps; s++)
+        {
+            S.nl->Update(S.d_atom_local, S.n, 0, S.d_crd, S.cell, S.rcell, s, NEIGHBOR_LIST::CONDITIONAL_UPDATE,
+                         S.d_excl_start, S.d_excl_list, S.d_excl_num);
+            S.lj->LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(
+                S.n, S.n, solvent, 0, S.d_crd, S.d_charge, S.d_frc, S.cell, S.rcell, S.nl->d_nl, beta,
+                need_energy, S.d_energy, need_virial, S.d_virial, S.d_direct);
+            if (S.slj)
+                S.slj->LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(
+                    S.n, S.res_numbers, S.d_res_start, S.d_crd, S.d_charge, S.d_frc, S.cell, S.rcell, S.nl->d_nl,
+                    beta, need_energy, S.d_energy, need_virial, S.d_virial, S.d_direct);
+        }
+        sync_device();
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Times the two parts separately: a forced rebuild and a force-only step.
+double ref_time_rebuild(const float* crd, int reps)
+{
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    sync_device();
+    auto t0 = std::chrono::steady_clock::now();
+    {
+        Quiet q;
+        for (int r = 0; r < reps; r++)
+            S.nl->Update(S.d_atom_local, S.n, 0, S.d_crd, S.cell, S.rcell, 0, NEIGHBOR_LIST::FORCED_UPDATE,
+                         S.d_excl_start, S.d_excl_list, S.d_excl_num);
+        sync_device();
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count() / (reps > 0 ? reps : 1);
+}
+
+void ref_clear()
+{
+    Quiet q;
+    if (S.nl)
+    {
+        S.nl->Clear();
+        delete S.nl;
+        S.nl = nullptr;
+    }
+    delete S.lj;
+    S.lj = nullptr;
+    delete S.slj;
+    S.slj = nullptr;
+    delete S.lj_soft;
+    S.lj_soft = nullptr;
+}
+
+}  // extern "C"

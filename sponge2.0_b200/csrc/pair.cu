@@ -1,0 +1,1042 @@
+// LJ + PME direct-space pair force, energy and virial:
+// LENNARD_JONES_INFORMATION and SOLVENT_LENNARD_JONES of
+// SPONGE/Lennard_Jones_force/{Lennard_Jones_force,solvent_LJ}.cpp.
+//
+// Pair function (Lennard_Jones_force.h:44-73), evaluated in FP32:
+//   F/r = (B - A r^-6) r^-8 - q_i q_j [r^-3 - beta^3 K(beta^2 r^2)]
+//   E_lj = (A/12 r^-6 - B/6) r^-6,  E_c = q_i q_j [r^-1 - beta M(beta^2 r^2)]
+// where K, M are the smooth parts of the screened Coulomb kernels
+// (ewald_fit.h).  The force on atoms accumulates in int64 fixed point, the
+// energy/virial totals too, so neither depends on summation order.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+
+namespace spgnb
+{
+namespace
+{
+
+constexpr int kPairWarps = 4;  // warps per block of the cluster-pair kernel
+constexpr float kTwoPow32 = 4294967296.0f;
+
+struct PairConst
+{
+    float rc2;
+    float beta;
+    float beta3;
+    float w_scale;  // beta^2 / W_MAX
+    int n_types;
+    int use_fit;    // beta*rc inside the fitted range
+};
+
+__device__ __forceinline__ float poly5(float x, const float* c)
+{
+    float p = c[5];
+    p = __fmaf_rn(p, x, c[4]);
+    p = __fmaf_rn(p, x, c[3]);
+    p = __fmaf_rn(p, x, c[2]);
+    p = __fmaf_rn(p, x, c[1]);
+    return __fmaf_rn(p, x, c[0]);
+}
+
+// Scalar pair force F/r (and energies when requested) for r2 > 0.
+template <bool ENERGY>
+__device__ __forceinline__ float pair_scalar(float r2, float qq, float A, float B, const PairConst& pc,
+                                             float& e_lj, float& e_c)
+{
+    float rinv = rsqrtf(r2);
+    rinv = rinv * __fmaf_rn(-0.5f * r2 * rinv, rinv, 1.5f);  // one Newton step
+    const float r2inv = rinv * rinv;
+    const float r6inv = r2inv * r2inv * r2inv;
+    const float flj = __fmaf_rn(-A, r6inv, B) * r6inv * r2inv;
+    float fc;
+    if (pc.use_fit)
+    {
+        const float x = r2 * pc.w_scale;
+        const float K = __fdividef(poly5(x, kEwaldKP), poly5(x, kEwaldKQ));
+        fc = qq * __fmaf_rn(-pc.beta3, K, rinv * r2inv);
+        if (ENERGY)
+        {
+            const float M = __fdividef(poly5(x, kEwaldMP), poly5(x, kEwaldMQ));
+            e_c = qq * __fmaf_rn(-pc.beta, M, rinv);
+        }
+    }
+    else
+    {
+        const float r = r2 * rinv;
+        const float br = pc.beta * r;
+        const float erfcv = erfcf(br);
+        fc = qq * rinv * r2inv * __fmaf_rn(br * 1.1283791670955126f, __expf(-br * br), erfcv);
+        if (ENERGY) e_c = qq * erfcv * rinv;
+    }
+    if (ENERGY) e_lj = __fmaf_rn(A * (1.0f / 12.0f), r6inv, -B * (1.0f / 6.0f)) * r6inv;
+    return flj - fc;
+}
+
+__device__ __forceinline__ void red_fixed(long long* acc, float v)
+{
+    long long q = __float2ll_rn(v * kTwoPow32);
+    if (q != 0) atomicAdd((unsigned long long*)acc, (unsigned long long)q);
+}
+
+__device__ __forceinline__ float3 frac_delta(uint4 ui, uint4 uj)
+{
+    const float s = 2.3283064365386963e-10f;  // 2^-32
+    return make_float3((float)(int)(uj.x - ui.x) * s, (float)(int)(uj.y - ui.y) * s, (float)(int)(uj.z - ui.z) * s);
+}
+
+struct OwnerMap
+{
+    const int* atom_local;   // global index of each local atom
+    int solvent_start;       // first local atom of the water tail (n when none)
+    int water_points;
+    __device__ __forceinline__ int remap(int a) const
+    {
+        return a >= solvent_start ? solvent_start + ((a - solvent_start) / water_points) * water_points : a;
+    }
+};
+
+struct PerAtomOut
+{
+    float* energy;       // caller's atom_energy (+=)
+    float* lj_energy;    // module's per-atom LJ energy
+    float* direct;       // atom_direct_pme_energy
+    float* virial;       // caller's LTMatrix3 array (+=), 6 floats per atom
+};
+
+// per-step slot pack: offsets from the build-time cluster centre moved by the
+// displacement since the build (minimum image, so a caller that wraps
+// coordinates between builds is fine), with the charge.
+__global__ void k_pack_slots(int slots_cap, const int* __restrict__ counters, const int* __restrict__ slot_atom,
+                             const float4* __restrict__ x0, const float4* __restrict__ d0,
+                             const float3* __restrict__ crd, const float* __restrict__ charge,
+                             const int* __restrict__ local_type, Cell cell, Cell rcell, float4* __restrict__ pos,
+                             int* __restrict__ ptype)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= slots_cap || s >= counters[kCntClusters] * kClusterSize) return;
+    int a = slot_atom[s];
+    float4 d = d0[s];
+    if (a < 0)
+    {
+        pos[s] = make_float4(d.x, d.y, d.z, 0.0f);
+        ptype[s] = 0;
+        return;
+    }
+    float3 c = crd[a];
+    float4 o = x0[s];
+    float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+    float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
+    float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
+    float sz = rintf(dz * rcell.a33);
+    dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
+    dy -= sy * cell.a22 + sz * cell.a32;
+    dz -= sz * cell.a33;
+    pos[s] = make_float4(d.x + dx, d.y + dy, d.z + dz, charge[a]);
+    ptype[s] = local_type[a];
+}
+
+// MODE 0: forces.  MODE 1: + energy/virial totals.  MODE 2: + per-atom
+// energy and virial arrays.
+template <int MODE>
+__global__ void __launch_bounds__(kPairWarps * 32)
+    k_pair_clusters(PairConst pc, Cell cell, Cell rcell, const int* __restrict__ counters,
+                    const int4* __restrict__ items, const int4* __restrict__ ents, const uint4* __restrict__ cl_u,
+                    const int* __restrict__ slot_atom, const float4* __restrict__ pos,
+                    const int* __restrict__ ptype, const float2* __restrict__ gtable, long long* __restrict__ acc,
+                    long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, int items_cap)
+{
+    extern __shared__ float2 table[];
+    const int TT = pc.n_types * pc.n_types;
+    for (int k = threadIdx.x; k < TT; k += blockDim.x) table[k] = gtable[k];
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31;
+    const int jl = lane & 7;
+    const int row = lane >> 3;
+    const int nitems = min(counters[kCntItems], items_cap);
+    const int total_warps = gridDim.x * kPairWarps;
+    constexpr bool EN = MODE >= 1;
+    constexpr bool PA = MODE >= 2;
+
+    for (int it = blockIdx.x * kPairWarps + (threadIdx.x >> 5); it < nitems; it += total_warps)
+    {
+        const int4 item = items[it];
+        const int ci = item.x;
+        const float4 pi0 = pos[ci * kClusterSize + row];
+        const float4 pi1 = pos[ci * kClusterSize + row + 4];
+        const int ti0 = ptype[ci * kClusterSize + row] * pc.n_types;
+        const int ti1 = ptype[ci * kClusterSize + row + 4] * pc.n_types;
+        const uint4 ui = cl_u[ci];
+        int ai0 = 0, ai1 = 0, gi0 = 0, gi1 = 0;
+        if (PA)
+        {
+            ai0 = slot_atom[ci * kClusterSize + row];
+            ai1 = slot_atom[ci * kClusterSize + row + 4];
+            gi0 = ai0 >= 0 ? om.atom_local[ai0] : 0;
+            gi1 = ai1 >= 0 ? om.atom_local[ai1] : 0;
+        }
+        float fi0x = 0, fi0y = 0, fi0z = 0, fi1x = 0, fi1y = 0, fi1z = 0;
+        float tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        float pai[2][8];
+        if (PA)
+            for (int h = 0; h < 2; h++)
+                for (int q = 0; q < 8; q++) pai[h][q] = 0.0f;
+
+        for (int e = item.y; e < item.y + item.z; e++)
+        {
+            const int4 en = ents[e];
+            const int cj = en.x;
+            const float4 pj = pos[cj * kClusterSize + jl];
+            const int tj = ptype[cj * kClusterSize + jl];
+            const uint4 uj = cl_u[cj];
+            const float3 f = frac_delta(ui, uj);
+            const float px = f.x * cell.a11 + f.y * cell.a21 + f.z * cell.a31 + pj.x;
+            const float py = f.y * cell.a22 + f.z * cell.a32 + pj.y;
+            const float pz = f.z * cell.a33 + pj.z;
+            int aj = 0, gj = 0;
+            if (PA)
+            {
+                aj = slot_atom[cj * kClusterSize + jl];
+                gj = aj >= 0 ? om.atom_local[aj] : 0;
+            }
+            float fjx = 0, fjy = 0, fjz = 0;
+            float paj[8];
+            if (PA)
+                for (int q = 0; q < 8; q++) paj[q] = 0.0f;
+#pragma unroll
+            for (int h = 0; h < 2; h++)
+            {
+                const unsigned m = (unsigned)(h ? en.w : en.z);
+                if (m == 0) continue;
+                const float4 pi = h ? pi1 : pi0;
+                float dx = px - pi.x, dy = py - pi.y, dz = pz - pi.z;
+                if (en.y & kEntPairImage)
+                {
+                    const float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
+                    const float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
+                    const float sz = rintf(dz * rcell.a33);
+                    dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
+                    dy -= sy * cell.a22 + sz * cell.a32;
+                    dz -= sz * cell.a33;
+                }
+                const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
+                const bool in = ((m >> lane) & 1u) && r2 < pc.rc2;
+                const float2 AB = table[(h ? ti1 : ti0) + tj];
+                float elj = 0.0f, ec = 0.0f;
+                float fs = pair_scalar<EN>(r2, pi.w * pj.w, AB.x, AB.y, pc, elj, ec);
+                fs = in ? fs : 0.0f;
+                const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
+                if (h)
+                {
+                    fi1x += fx;
+                    fi1y += fy;
+                    fi1z += fz;
+                }
+                else
+                {
+                    fi0x += fx;
+                    fi0y += fy;
+                    fi0z += fz;
+                }
+                fjx -= fx;
+                fjy -= fy;
+                fjz -= fz;
+                if (EN)
+                {
+                    elj = in ? elj : 0.0f;
+                    ec = in ? ec : 0.0f;
+                    float v[6] = {-fx * dx, -(fx * dy + fy * dx), -fy * dy, -(fx * dz + fz * dx),
+                                  -(fy * dz + fz * dy), -fz * dz};
+                    tot[0] += elj;
+                    tot[1] += ec;
+                    for (int q = 0; q < 6; q++) tot[2 + q] += v[q];
+                    if (PA)
+                    {
+                        const bool i_owns = (h ? gi1 : gi0) < gj;
+                        float* dst = i_owns ? pai[h] : paj;
+                        dst[0] += elj;
+                        dst[1] += ec;
+                        for (int q = 0; q < 6; q++) dst[2 + q] += v[q];
+                    }
+                }
+            }
+            // j forces: sum over the four rows, one fixed-point add per atom
+            fjx += __shfl_xor_sync(0xffffffffu, fjx, 8);
+            fjy += __shfl_xor_sync(0xffffffffu, fjy, 8);
+            fjz += __shfl_xor_sync(0xffffffffu, fjz, 8);
+            fjx += __shfl_xor_sync(0xffffffffu, fjx, 16);
+            fjy += __shfl_xor_sync(0xffffffffu, fjy, 16);
+            fjz += __shfl_xor_sync(0xffffffffu, fjz, 16);
+            if (PA)
+            {
+                for (int q = 0; q < 8; q++)
+                {
+                    paj[q] += __shfl_xor_sync(0xffffffffu, paj[q], 8);
+                    paj[q] += __shfl_xor_sync(0xffffffffu, paj[q], 16);
+                }
+            }
+            if (row == 0)
+            {
+                const int a = PA ? aj : slot_atom[cj * kClusterSize + jl];
+                if (a >= 0)
+                {
+                    red_fixed(acc + 4 * (size_t)a + 0, fjx);
+                    red_fixed(acc + 4 * (size_t)a + 1, fjy);
+                    red_fixed(acc + 4 * (size_t)a + 2, fjz);
+                    if (PA)
+                    {
+                        const int o = om.remap(a);
+                        if (pa.energy) atomicAdd(pa.energy + o, paj[0] + paj[1]);
+                        if (pa.lj_energy) atomicAdd(pa.lj_energy + o, paj[0]);
+                        if (pa.direct) atomicAdd(pa.direct + o, paj[1]);
+                        if (pa.virial)
+                            for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)o + q, paj[2 + q]);
+                    }
+                }
+            }
+        }
+        // i forces: sum over the eight j lanes
+#pragma unroll
+        for (int o = 1; o < 8; o <<= 1)
+        {
+            fi0x += __shfl_xor_sync(0xffffffffu, fi0x, o);
+            fi0y += __shfl_xor_sync(0xffffffffu, fi0y, o);
+            fi0z += __shfl_xor_sync(0xffffffffu, fi0z, o);
+            fi1x += __shfl_xor_sync(0xffffffffu, fi1x, o);
+            fi1y += __shfl_xor_sync(0xffffffffu, fi1y, o);
+            fi1z += __shfl_xor_sync(0xffffffffu, fi1z, o);
+            if (PA)
+                for (int h = 0; h < 2; h++)
+                    for (int q = 0; q < 8; q++) pai[h][q] += __shfl_xor_sync(0xffffffffu, pai[h][q], o);
+        }
+        if (jl == 0)
+        {
+            const int a0 = PA ? ai0 : slot_atom[ci * kClusterSize + row];
+            const int a1 = PA ? ai1 : slot_atom[ci * kClusterSize + row + 4];
+            if (a0 >= 0)
+            {
+                red_fixed(acc + 4 * (size_t)a0 + 0, fi0x);
+                red_fixed(acc + 4 * (size_t)a0 + 1, fi0y);
+                red_fixed(acc + 4 * (size_t)a0 + 2, fi0z);
+            }
+            if (a1 >= 0)
+            {
+                red_fixed(acc + 4 * (size_t)a1 + 0, fi1x);
+                red_fixed(acc + 4 * (size_t)a1 + 1, fi1y);
+                red_fixed(acc + 4 * (size_t)a1 + 2, fi1z);
+            }
+            if (PA)
+            {
+                for (int h = 0; h < 2; h++)
+                {
+                    const int a = h ? a1 : a0;
+                    if (a < 0) continue;
+                    const int o = om.remap(a);
+                    if (pa.energy) atomicAdd(pa.energy + o, pai[h][0] + pai[h][1]);
+                    if (pa.lj_energy) atomicAdd(pa.lj_energy + o, pai[h][0]);
+                    if (pa.direct) atomicAdd(pa.direct + o, pai[h][1]);
+                    if (pa.virial)
+                        for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)o + q, pai[h][2 + q]);
+                }
+            }
+        }
+        if (EN)
+        {
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+                for (int o = 16; o > 0; o >>= 1) tot[q] += __shfl_xor_sync(0xffffffffu, tot[q], o);
+            if (lane == 0)
+                for (int q = 0; q < 8; q++)
+                {
+                    long long v = __double2ll_rn((double)tot[q] * kEnergyScale);
+                    if (v) atomicAdd((unsigned long long*)&totals[q], (unsigned long long)v);
+                }
+        }
+    }
+}
+
+// Fixed point -> caller's float force (+=), accumulators cleared for the
+// next call.
+__global__ void k_finalize(int n, long long* __restrict__ acc, float3* __restrict__ frc)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    long long* a = acc + 4 * (size_t)i;
+    long long x = a[0], y = a[1], z = a[2];
+    if (x | y | z)
+    {
+        float3 f = frc[i];
+        f.x += (float)((double)x * kForceUnscale);
+        f.y += (float)((double)y * kForceUnscale);
+        f.z += (float)((double)z * kForceUnscale);
+        frc[i] = f;
+        a[0] = 0;
+        a[1] = 0;
+        a[2] = 0;
+    }
+}
+
+__global__ void k_local_types(int n, const int* __restrict__ atom_local, const int* __restrict__ atom_type,
+                              int* __restrict__ local_type)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) local_type[i] = atom_type[atom_local[i]];
+}
+
+// ------------------------------------------------ reference-layout lists
+__global__ void k_pack_atoms(int n, const float3* __restrict__ crd, const float* __restrict__ charge,
+                             const int* __restrict__ local_type, float4* __restrict__ pos, int* __restrict__ ptype)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 c = crd[i];
+    pos[i] = make_float4(c.x, c.y, c.z, charge[i]);
+    ptype[i] = local_type[i];
+}
+
+// Reference minimum image (vector.hpp:322-327), dr = b - a.
+__device__ __forceinline__ void ref_image(float& dx, float& dy, float& dz, const Cell& c, const Cell& r)
+{
+    float sx = floorf(dx * r.a11 + dy * r.a21 + dz * r.a31 + 0.5f);
+    float sy = floorf(dy * r.a22 + dz * r.a32 + 0.5f);
+    float sz = floorf(dz * r.a33 + 0.5f);
+    dx -= sx * c.a11 + sy * c.a21 + sz * c.a31;
+    dy -= sy * c.a22 + sz * c.a32;
+    dz -= sz * c.a33;
+}
+
+// Warp per owner atom over its reference-layout half list
+// (Lennard_Jones_force.cpp:43-136 semantics, int64 accumulation).
+template <int MODE>
+__global__ void k_pair_atom_groups(PairConst pc, Cell cell, Cell rcell, int n_owner, int local_atoms,
+                                   const spgnb_atom_group* __restrict__ nl, const float4* __restrict__ pos,
+                                   const int* __restrict__ ptype, const float2* __restrict__ table,
+                                   long long* __restrict__ acc, long long* __restrict__ totals, PerAtomOut pa)
+{
+    constexpr bool EN = MODE >= 1;
+    const int lane = threadIdx.x & 31;
+    const int total_warps = gridDim.x * (blockDim.x >> 5);
+    for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n_owner; i += total_warps)
+    {
+        const spgnb_atom_group g = nl[i];
+        const float4 pi = pos[i];
+        const int ti = ptype[i] * pc.n_types;
+        float fx = 0, fy = 0, fz = 0;
+        float acc8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = lane; k < g.atom_numbers; k += 32)
+        {
+            const int j = g.atom_serial[k];
+            const float4 pj = pos[j];
+            float dx = pj.x - pi.x, dy = pj.y - pi.y, dz = pj.z - pi.z;
+            ref_image(dx, dy, dz, cell, rcell);
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            if (!(r2 < pc.rc2)) continue;
+            const float2 AB = table[ti + ptype[j]];
+            float elj = 0, ec = 0;
+            const float fs = pair_scalar<EN>(r2, pi.w * pj.w, AB.x, AB.y, pc, elj, ec);
+            const float ij = j < local_atoms ? 1.0f : 0.5f;
+            const float gx = fs * dx, gy = fs * dy, gz = fs * dz;
+            fx += gx;
+            fy += gy;
+            fz += gz;
+            if (j < local_atoms)
+            {
+                red_fixed(acc + 4 * (size_t)j + 0, -gx);
+                red_fixed(acc + 4 * (size_t)j + 1, -gy);
+                red_fixed(acc + 4 * (size_t)j + 2, -gz);
+            }
+            if (EN)
+            {
+                acc8[0] += ij * elj;
+                acc8[1] += ij * ec;
+                acc8[2] -= ij * gx * dx;
+                acc8[3] -= ij * (gx * dy + gy * dx);
+                acc8[4] -= ij * gy * dy;
+                acc8[5] -= ij * (gx * dz + gz * dx);
+                acc8[6] -= ij * (gy * dz + gz * dy);
+                acc8[7] -= ij * gz * dz;
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            fx += __shfl_xor_sync(0xffffffffu, fx, o);
+            fy += __shfl_xor_sync(0xffffffffu, fy, o);
+            fz += __shfl_xor_sync(0xffffffffu, fz, o);
+            if (EN)
+                for (int q = 0; q < 8; q++) acc8[q] += __shfl_xor_sync(0xffffffffu, acc8[q], o);
+        }
+        if (lane == 0)
+        {
+            red_fixed(acc + 4 * (size_t)i + 0, fx);
+            red_fixed(acc + 4 * (size_t)i + 1, fy);
+            red_fixed(acc + 4 * (size_t)i + 2, fz);
+            if (EN)
+            {
+                for (int q = 0; q < 8; q++)
+                {
+                    long long v = __double2ll_rn((double)acc8[q] * kEnergyScale);
+                    if (v) atomicAdd((unsigned long long*)&totals[q], (unsigned long long)v);
+                }
+                if (MODE >= 2)
+                {
+                    if (pa.energy) atomicAdd(pa.energy + i, acc8[0] + acc8[1]);
+                    if (pa.lj_energy) atomicAdd(pa.lj_energy + i, acc8[0]);
+                    if (pa.direct) atomicAdd(pa.direct + i, acc8[1]);
+                    if (pa.virial)
+                        for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)i + q, acc8[2 + q]);
+                }
+            }
+        }
+    }
+}
+
+// Water residues over the first site's reference-layout list
+// (solvent_LJ.cpp:25-145 semantics): every site of residue r against each j
+// of the first site's list; energy and virial to the first site.
+template <int MODE, int WP>
+__global__ void k_pair_solvent(PairConst pc, Cell cell, Cell rcell, int res_begin, int res_end, int local_atoms,
+                               const int* __restrict__ res_start, const spgnb_atom_group* __restrict__ nl,
+                               const float4* __restrict__ pos, const int* __restrict__ ptype,
+                               const float2* __restrict__ table, long long* __restrict__ acc,
+                               long long* __restrict__ totals, PerAtomOut pa)
+{
+    constexpr bool EN = MODE >= 1;
+    const int lane = threadIdx.x & 31;
+    const int total_warps = gridDim.x * (blockDim.x >> 5);
+    for (int r = res_begin + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); r < res_end; r += total_warps)
+    {
+        const int a0 = res_start[r];
+        float4 si[WP];
+        int ti[WP];
+        float fs_[WP][3];
+        for (int s = 0; s < WP; s++)
+        {
+            si[s] = pos[a0 + s];
+            ti[s] = ptype[a0 + s] * pc.n_types;
+            fs_[s][0] = fs_[s][1] = fs_[s][2] = 0.0f;
+        }
+        float acc8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        const spgnb_atom_group g = nl[a0];
+        for (int k = lane; k < g.atom_numbers; k += 32)
+        {
+            const int j = g.atom_serial[k];
+            const float4 pj = pos[j];
+            const int tj = ptype[j];
+            const float ij = j < local_atoms ? 1.0f : 0.5f;
+            float gjx = 0, gjy = 0, gjz = 0;
+            for (int s = 0; s < WP; s++)
+            {
+                float dx = pj.x - si[s].x, dy = pj.y - si[s].y, dz = pj.z - si[s].z;
+                ref_image(dx, dy, dz, cell, rcell);
+                const float r2 = dx * dx + dy * dy + dz * dz;
+                if (!(r2 < pc.rc2)) continue;
+                const float2 AB = table[ti[s] + tj];
+                float elj = 0, ec = 0;
+                const float f = pair_scalar<EN>(r2, si[s].w * pj.w, AB.x, AB.y, pc, elj, ec);
+                const float gx = f * dx, gy = f * dy, gz = f * dz;
+                fs_[s][0] += gx;
+                fs_[s][1] += gy;
+                fs_[s][2] += gz;
+                gjx -= gx;
+                gjy -= gy;
+                gjz -= gz;
+                if (EN)
+                {
+                    acc8[0] += ij * elj;
+                    acc8[1] += ij * ec;
+                    acc8[2] -= ij * gx * dx;
+                    acc8[3] -= ij * (gx * dy + gy * dx);
+                    acc8[4] -= ij * gy * dy;
+                    acc8[5] -= ij * (gx * dz + gz * dx);
+                    acc8[6] -= ij * (gy * dz + gz * dy);
+                    acc8[7] -= ij * gz * dz;
+                }
+            }
+            if (j < local_atoms)
+            {
+                red_fixed(acc + 4 * (size_t)j + 0, gjx);
+                red_fixed(acc + 4 * (size_t)j + 1, gjy);
+                red_fixed(acc + 4 * (size_t)j + 2, gjz);
+            }
+        }
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            for (int s = 0; s < WP; s++)
+                for (int d = 0; d < 3; d++) fs_[s][d] += __shfl_xor_sync(0xffffffffu, fs_[s][d], o);
+            if (EN)
+                for (int q = 0; q < 8; q++) acc8[q] += __shfl_xor_sync(0xffffffffu, acc8[q], o);
+        }
+        if (lane == 0)
+        {
+            for (int s = 0; s < WP; s++)
+                for (int d = 0; d < 3; d++) red_fixed(acc + 4 * (size_t)(a0 + s) + d, fs_[s][d]);
+            if (EN)
+            {
+                for (int q = 0; q < 8; q++)
+                {
+                    long long v = __double2ll_rn((double)acc8[q] * kEnergyScale);
+                    if (v) atomicAdd((unsigned long long*)&totals[q], (unsigned long long)v);
+                }
+                if (MODE >= 2)
+                {
+                    if (pa.energy) atomicAdd(pa.energy + a0, acc8[0] + acc8[1]);
+                    if (pa.lj_energy) atomicAdd(pa.lj_energy + a0, acc8[0]);
+                    if (pa.direct) atomicAdd(pa.direct + a0, acc8[1]);
+                    if (pa.virial)
+                        for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)a0 + q, acc8[2 + q]);
+                }
+            }
+        }
+    }
+}
+
+__global__ void k_long_range(int need_pressure, float* virial, int need_potential, float* potential, float vfac,
+                             float efac)
+{
+    if (need_pressure)
+    {
+        virial[0] += vfac;
+        virial[2] += vfac;
+        virial[5] += vfac;
+    }
+    if (need_potential) potential[0] += efac;
+}
+
+__global__ void k_solvent_count(int local_res_numbers, const int* __restrict__ res_len, int water_points,
+                                int atom_numbers, const float* __restrict__ mass, int* out)
+{
+    // SOLVENT_LENNARD_JONES get_local_device (solvent_LJ.cpp:433-467)
+    int start = local_res_numbers, cnt = 0;
+    for (int i = local_res_numbers - 1; i >= 0; i--)
+    {
+        int rs = atom_numbers - water_points * (cnt + 1);
+        if (rs < 0) break;
+        float mo = mass[rs], m1 = mass[rs + 1], m2 = mass[rs + 2];
+        if (res_len[i] == water_points && mo > 15.8f && mo < 16.2f && m1 > 1.007f && m1 < 1.009f && m2 > 1.007f &&
+            m2 < 1.009f)
+        {
+            start--;
+            cnt++;
+        }
+        else
+            break;
+    }
+    out[0] = start;
+    out[1] = cnt * water_points;
+}
+
+PairConst make_pair_const(const spgnb_lj* lj, float beta)
+{
+    PairConst pc;
+    pc.rc2 = lj->cutoff * lj->cutoff;
+    pc.beta = beta;
+    pc.beta3 = beta * beta * beta;
+    pc.w_scale = beta * beta * SPGNB_EWALD_INV_W_MAX;
+    pc.n_types = lj->n_types;
+    float z = beta * lj->cutoff;
+    pc.use_fit = (z * z <= SPGNB_EWALD_W_MAX * 0.999f) ? 1 : 0;
+    return pc;
+}
+
+int ensure_pos(spgnb_lj* lj, int count)
+{
+    if (count <= lj->pos_cap) return SPGNB_OK;
+    dfree(lj->d_pos);
+    dfree(lj->d_pos_type);
+    int st;
+    if ((st = dalloc(&lj->d_pos, count))) return st;
+    if ((st = dalloc(&lj->d_pos_type, count))) return st;
+    lj->pos_cap = count;
+    return SPGNB_OK;
+}
+
+int check_common(spgnb_lj* lj, int local_atom_numbers, int ghost_numbers, const spgnb_vector* d_crd,
+                 const float* d_charge, spgnb_vector* d_frc)
+{
+    if (!lj) return fail(SPGNB_E_ARG, "LJ handle is NULL");
+    if (ghost_numbers != 0)
+        return fail(SPGNB_E_UNSUPPORTED, "ghost atoms (multi-rank domain decomposition) are not supported");
+    if (local_atom_numbers > lj->atom_numbers)
+        return fail(SPGNB_E_ARG, "%d local atoms exceed the %d the module was created for", local_atom_numbers,
+                    lj->atom_numbers);
+    if (!lj->d_local_type) return fail(SPGNB_E_STATE, "LJ: Get_Local has not been called");
+    if (local_atom_numbers > lj->local_atoms)
+        return fail(SPGNB_E_STATE, "LJ: %d local atoms but Get_Local saw %d", local_atom_numbers, lj->local_atoms);
+    if (!d_crd || !d_charge || !d_frc) return fail(SPGNB_E_ARG, "LJ: NULL device pointer");
+    return SPGNB_OK;
+}
+
+}  // namespace
+}  // namespace spgnb
+
+using namespace spgnb;
+
+extern "C" {
+
+int spgnb_lj_create(int atom_numbers, int atom_type_numbers, const int* h_atom_type, const float* h_pair_A,
+                    const float* h_pair_B, float cutoff, spgnb_lj** out)
+{
+    if (!out) return fail(SPGNB_E_ARG, "spgnb_lj_create: out is NULL");
+    *out = nullptr;
+    if (atom_numbers <= 0 || atom_type_numbers <= 0 || !h_atom_type || !h_pair_A || !h_pair_B || !(cutoff > 0))
+        return fail(SPGNB_E_ARG, "spgnb_lj_create: bad arguments");
+    const int T = atom_type_numbers;
+    if (T * T * (int)sizeof(float2) > 96 * 1024)
+        return fail(SPGNB_E_UNSUPPORTED, "spgnb_lj_create: %d LJ types exceed the shared-memory pair table", T);
+    std::vector<double> hist(T, 0.0);
+    for (int i = 0; i < atom_numbers; i++)
+    {
+        int t = h_atom_type[i];
+        if (t < 0 || t >= T) return fail(SPGNB_E_ARG, "spgnb_lj_create: atom %d has type %d outside [0,%d)", i, t, T);
+        hist[t] += 1.0;
+    }
+    std::vector<float2> table((size_t)T * T);
+    double c6 = 0.0;
+    for (int a = 0; a < T; a++)
+        for (int b = 0; b < T; b++)
+        {
+            int hi = a > b ? a : b, lo = a > b ? b : a;
+            int p = hi * (hi + 1) / 2 + lo;
+            table[(size_t)a * T + b] = make_float2(h_pair_A[p], h_pair_B[p]);
+            c6 += hist[a] * hist[b] * (double)h_pair_B[p];
+        }
+    spgnb_lj* lj = new spgnb_lj();
+    lj->atom_numbers = atom_numbers;
+    lj->n_types = T;
+    lj->cutoff = cutoff;
+    // Lennard_Jones_force.cpp:263-268 in float arithmetic
+    float f = (float)c6;
+    f *= -2.0f / 3.0f * 3.1415926535897932f / cutoff / cutoff / cutoff / 6.0f;
+    lj->long_range_factor = f;
+    int st;
+    if ((st = dalloc(&lj->d_atom_type, atom_numbers)) || (st = dalloc(&lj->d_table, table.size())) ||
+        (st = dalloc(&lj->d_lj_energy_atom, atom_numbers)) || (st = dalloc(&lj->d_frc_acc, 4 * (size_t)atom_numbers)) ||
+        (st = dalloc(&lj->d_totals, 8)))
+    {
+        spgnb_lj_destroy(lj);
+        return st;
+    }
+    const int smem = (int)(sizeof(float2) * T * T);
+    if (smem > 48 * 1024)
+    {
+        cudaFuncSetAttribute(k_pair_clusters<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_pair_clusters<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(k_pair_clusters<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    }
+    cudaMemcpy(lj->d_atom_type, h_atom_type, sizeof(int) * atom_numbers, cudaMemcpyHostToDevice);
+    cudaMemcpy(lj->d_table, table.data(), sizeof(float2) * table.size(), cudaMemcpyHostToDevice);
+    cudaMemset(lj->d_frc_acc, 0, sizeof(long long) * 4 * (size_t)atom_numbers);
+    cudaMemset(lj->d_totals, 0, sizeof(long long) * 8);
+    cudaMemset(lj->d_lj_energy_atom, 0, sizeof(float) * atom_numbers);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess)
+    {
+        spgnb_lj_destroy(lj);
+        return cuda_fail(e, "spgnb_lj_create");
+    }
+    *out = lj;
+    return SPGNB_OK;
+}
+
+int spgnb_lj_get_local(spgnb_lj* lj, const int* d_atom_local, int local_atom_numbers, int ghost_numbers)
+{
+    if (!lj || !d_atom_local) return fail(SPGNB_E_ARG, "spgnb_lj_get_local: NULL argument");
+    const int n = local_atom_numbers + ghost_numbers;
+    if (n > lj->atom_numbers) return fail(SPGNB_E_ARG, "spgnb_lj_get_local: too many local atoms");
+    if (!lj->d_local_type)
+    {
+        int st = dalloc(&lj->d_local_type, lj->atom_numbers);
+        if (st) return st;
+    }
+    k_local_types<<<(n + 255) / 256, 256, 0, stream()>>>(n, d_atom_local, lj->d_atom_type, lj->d_local_type);
+    SPGNB_CHECK_LAUNCH("k_local_types");
+    lj->local_atoms = local_atom_numbers;
+    lj->d_atom_local = d_atom_local;
+    return SPGNB_OK;
+}
+
+int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_numbers, int solvent_numbers,
+                              int ghost_numbers, const spgnb_vector* d_crd, const float* d_charge,
+                              spgnb_vector* d_frc, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, const spgnb_nl* nl,
+                              float pme_beta, int need_atom_energy, float* d_atom_energy, int need_virial,
+                              spgnb_ltmatrix3* d_atom_virial, float* d_atom_direct_pme_energy)
+{
+    (void)atom_numbers;
+    int st = check_common(lj, local_atom_numbers, ghost_numbers, d_crd, d_charge, d_frc);
+    if (st) return st;
+    if (!nl) return fail(SPGNB_E_ARG, "spgnb_lj_pme_direct_force: nl is NULL");
+    if (!nl->built) return fail(SPGNB_E_STATE, "spgnb_lj_pme_direct_force: the neighbour list was never built");
+    if (local_atom_numbers != nl->local_atoms)
+        return fail(SPGNB_E_STATE, "spgnb_lj_pme_direct_force: list built for %d atoms, called with %d",
+                    nl->local_atoms, local_atom_numbers);
+    if (local_atom_numbers == 0) return SPGNB_OK;
+    cudaStream_t s = stream();
+    const int slots = nl->clusters_cap * kClusterSize;
+    if ((st = ensure_pos(lj, slots))) return st;
+    const Cell c = make_cell(cell), rc = make_cell(rcell);
+    SPGNB_CUDA(cudaMemsetAsync(lj->d_totals, 0, sizeof(long long) * 8, s));
+    if (need_atom_energy)
+    {
+        SPGNB_CUDA(cudaMemsetAsync(lj->d_lj_energy_atom, 0, sizeof(float) * lj->atom_numbers, s));
+        if (d_atom_direct_pme_energy)
+            SPGNB_CUDA(cudaMemsetAsync(d_atom_direct_pme_energy, 0, sizeof(float) * lj->atom_numbers, s));
+    }
+    k_pack_slots<<<(slots + 255) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_slot_x0,
+                                                     nl->d_slot_d0, (const float3*)d_crd, d_charge,
+                                                     lj->d_local_type, c, rc, lj->d_pos, lj->d_pos_type);
+    SPGNB_CHECK_LAUNCH("k_pack_slots");
+    PairConst pc = make_pair_const(lj, pme_beta);
+    OwnerMap om{nullptr, local_atom_numbers, 3};
+    PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
+    int mode = 0;
+    if (need_atom_energy || need_virial) mode = 1;
+    if ((need_atom_energy && (d_atom_energy || d_atom_direct_pme_energy)) || (need_virial && d_atom_virial))
+        mode = 2;
+    if (mode == 2)
+    {
+        om.solvent_start = local_atom_numbers - (solvent_numbers > 0 ? solvent_numbers : 0);
+        om.water_points = 3;
+        pa.energy = need_atom_energy ? d_atom_energy : nullptr;
+        pa.lj_energy = need_atom_energy ? lj->d_lj_energy_atom : nullptr;
+        pa.direct = need_atom_energy ? d_atom_direct_pme_energy : nullptr;
+        pa.virial = need_virial ? (float*)d_atom_virial : nullptr;
+    }
+    const size_t smem = sizeof(float2) * lj->n_types * lj->n_types;
+    const int blocks = num_sms() * 4;
+    if (mode == 0)
+        k_pair_clusters<0><<<blocks, kPairWarps * 32, smem, s>>>(pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents,
+                                                                 nl->d_cl_u, nl->d_slot_atom, lj->d_pos,
+                                                                 lj->d_pos_type, lj->d_table, lj->d_frc_acc,
+                                                                 lj->d_totals, om, pa, nl->items_cap);
+    else if (mode == 1)
+        k_pair_clusters<1><<<blocks, kPairWarps * 32, smem, s>>>(pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents,
+                                                                 nl->d_cl_u, nl->d_slot_atom, lj->d_pos,
+                                                                 lj->d_pos_type, lj->d_table, lj->d_frc_acc,
+                                                                 lj->d_totals, om, pa, nl->items_cap);
+    else
+    {
+        om.atom_local = lj->d_atom_local;
+        k_pair_clusters<2><<<blocks, kPairWarps * 32, smem, s>>>(pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents,
+                                                                 nl->d_cl_u, nl->d_slot_atom, lj->d_pos,
+                                                                 lj->d_pos_type, lj->d_table, lj->d_frc_acc,
+                                                                 lj->d_totals, om, pa, nl->items_cap);
+    }
+    SPGNB_CHECK_LAUNCH("k_pair_clusters");
+    k_finalize<<<(local_atom_numbers + 255) / 256, 256, 0, s>>>(local_atom_numbers, lj->d_frc_acc, (float3*)d_frc);
+    SPGNB_CHECK_LAUNCH("k_finalize");
+    lj->have_energy = need_atom_energy != 0;
+    lj->have_virial = need_virial != 0;
+    return SPGNB_OK;
+}
+
+int spgnb_lj_pme_direct_force_atom_groups(spgnb_lj* lj, int atom_numbers, int local_atom_numbers,
+                                          int solvent_numbers, int ghost_numbers, const spgnb_vector* d_crd,
+                                          const float* d_charge, spgnb_vector* d_frc, spgnb_ltmatrix3 cell,
+                                          spgnb_ltmatrix3 rcell, const spgnb_atom_group* d_nl, float pme_beta,
+                                          int need_atom_energy, float* d_atom_energy, int need_virial,
+                                          spgnb_ltmatrix3* d_atom_virial, float* d_atom_direct_pme_energy)
+{
+    (void)atom_numbers;
+    int st = check_common(lj, local_atom_numbers, ghost_numbers, d_crd, d_charge, d_frc);
+    if (st) return st;
+    if (!d_nl) return fail(SPGNB_E_ARG, "spgnb_lj_pme_direct_force_atom_groups: d_nl is NULL");
+    cudaStream_t s = stream();
+    if ((st = ensure_pos(lj, lj->atom_numbers))) return st;
+    const Cell c = make_cell(cell), rc = make_cell(rcell);
+    SPGNB_CUDA(cudaMemsetAsync(lj->d_totals, 0, sizeof(long long) * 8, s));
+    if (need_atom_energy)
+    {
+        SPGNB_CUDA(cudaMemsetAsync(lj->d_lj_energy_atom, 0, sizeof(float) * lj->atom_numbers, s));
+        if (d_atom_direct_pme_energy)
+            SPGNB_CUDA(cudaMemsetAsync(d_atom_direct_pme_energy, 0, sizeof(float) * lj->atom_numbers, s));
+    }
+    const int n = local_atom_numbers;
+    if (n == 0) return SPGNB_OK;
+    k_pack_atoms<<<(n + 255) / 256, 256, 0, s>>>(n, (const float3*)d_crd, d_charge, lj->d_local_type, lj->d_pos,
+                                                 lj->d_pos_type);
+    SPGNB_CHECK_LAUNCH("k_pack_atoms");
+    PairConst pc = make_pair_const(lj, pme_beta);
+    PerAtomOut pa{need_atom_energy ? d_atom_energy : nullptr, need_atom_energy ? lj->d_lj_energy_atom : nullptr,
+                  need_atom_energy ? d_atom_direct_pme_energy : nullptr, need_virial ? (float*)d_atom_virial : nullptr};
+    const int owners = n - (solvent_numbers > 0 ? solvent_numbers : 0);
+    const int blocks = std::max(1, std::min((owners + 3) / 4, num_sms() * 8));
+    const int mode = (need_atom_energy || need_virial) ? 2 : 0;
+    if (owners > 0)
+    {
+        if (mode == 0)
+            k_pair_atom_groups<0><<<blocks, 128, 0, s>>>(pc, c, rc, owners, n, d_nl, lj->d_pos, lj->d_pos_type,
+                                                         lj->d_table, lj->d_frc_acc, lj->d_totals, pa);
+        else
+            k_pair_atom_groups<2><<<blocks, 128, 0, s>>>(pc, c, rc, owners, n, d_nl, lj->d_pos, lj->d_pos_type,
+                                                         lj->d_table, lj->d_frc_acc, lj->d_totals, pa);
+        SPGNB_CHECK_LAUNCH("k_pair_atom_groups");
+    }
+    k_finalize<<<(n + 255) / 256, 256, 0, s>>>(n, lj->d_frc_acc, (float3*)d_frc);
+    SPGNB_CHECK_LAUNCH("k_finalize");
+    lj->have_energy = need_atom_energy != 0;
+    lj->have_virial = need_virial != 0;
+    return SPGNB_OK;
+}
+
+int spgnb_lj_long_range_correction(spgnb_lj* lj, int need_pressure, spgnb_ltmatrix3* d_virial,
+                                   int need_potential, float* d_potential, float volume)
+{
+    if (!lj) return fail(SPGNB_E_ARG, "spgnb_lj_long_range_correction: NULL handle");
+    if ((need_pressure && !d_virial) || (need_potential && !d_potential))
+        return fail(SPGNB_E_ARG, "spgnb_lj_long_range_correction: NULL output");
+    if (!(volume > 0)) return fail(SPGNB_E_ARG, "spgnb_lj_long_range_correction: volume must be positive");
+    float f = (float)lj->long_range_factor;
+    float vfac = 2 * f / volume;
+    float efac = f / volume;
+    lj->last_volume = volume;
+    if (need_potential) lj->h_last_long_energy = efac;
+    k_long_range<<<1, 1, 0, stream()>>>(need_pressure, (float*)d_virial, need_potential, d_potential, vfac, efac);
+    SPGNB_CHECK_LAUNCH("k_long_range");
+    return SPGNB_OK;
+}
+
+int spgnb_lj_totals(spgnb_lj* lj, double out[8])
+{
+    if (!lj || !out) return fail(SPGNB_E_ARG, "spgnb_lj_totals: NULL argument");
+    long long h[8];
+    SPGNB_CUDA(cudaMemcpyAsync(h, lj->d_totals, sizeof(h), cudaMemcpyDeviceToHost, stream()));
+    SPGNB_CUDA(cudaStreamSynchronize(stream()));
+    for (int q = 0; q < 8; q++) out[q] = (double)h[q] / kEnergyScale;
+    for (int q = 0; q < 8; q++) lj->totals[q] = out[q];
+    return SPGNB_OK;
+}
+
+int spgnb_lj_energies(spgnb_lj* lj, double* lj_short, double* lj_long, double* lj_total, double* direct_coulomb)
+{
+    double t[8];
+    int st = spgnb_lj_totals(lj, t);
+    if (st) return st;
+    if (lj_short) *lj_short = t[0];
+    if (lj_long) *lj_long = lj->h_last_long_energy;
+    if (lj_total) *lj_total = t[0] + lj->h_last_long_energy;
+    if (direct_coulomb) *direct_coulomb = t[1];
+    return SPGNB_OK;
+}
+
+double spgnb_lj_long_range_factor(const spgnb_lj* lj) { return lj ? lj->long_range_factor : 0.0; }
+
+int spgnb_lj_destroy(spgnb_lj* lj)
+{
+    if (!lj) return SPGNB_OK;
+    dfree(lj->d_atom_type);
+    dfree(lj->d_local_type);
+    dfree(lj->d_table);
+    dfree(lj->d_lj_energy_atom);
+    dfree(lj->d_frc_acc);
+    dfree(lj->d_totals);
+    dfree(lj->d_pos);
+    dfree(lj->d_pos_type);
+    delete lj;
+    return SPGNB_OK;
+}
+
+// ----------------------------------------------------- SOLVENT_LENNARD_JONES
+int spgnb_solvent_create(spgnb_lj* lj, int water_points, spgnb_solvent** out)
+{
+    if (!out || !lj) return fail(SPGNB_E_ARG, "spgnb_solvent_create: NULL argument");
+    *out = nullptr;
+    if (water_points != 3 && water_points != 4)
+        return fail(SPGNB_E_ARG, "spgnb_solvent_create: water_points must be 3 or 4");
+    spgnb_solvent* s = new spgnb_solvent();
+    s->lj = lj;
+    s->water_points = water_points;
+    int st = dalloc(&s->d_scratch, 2);
+    if (st)
+    {
+        delete s;
+        return st;
+    }
+    *out = s;
+    return SPGNB_OK;
+}
+
+int spgnb_solvent_get_local(spgnb_solvent* s, int local_res_numbers, const int* d_res_len, int atom_numbers,
+                            const float* d_mass, int* local_solvent_numbers)
+{
+    if (!s || !d_res_len || !d_mass) return fail(SPGNB_E_ARG, "spgnb_solvent_get_local: NULL argument");
+    k_solvent_count<<<1, 1, 0, stream()>>>(local_res_numbers, d_res_len, s->water_points, atom_numbers, d_mass,
+                                           s->d_scratch);
+    SPGNB_CHECK_LAUNCH("k_solvent_count");
+    int h[2];
+    SPGNB_CUDA(cudaMemcpyAsync(h, s->d_scratch, sizeof(h), cudaMemcpyDeviceToHost, stream()));
+    SPGNB_CUDA(cudaStreamSynchronize(stream()));
+    s->solvent_start_local = h[0];
+    s->local_solvent_numbers = h[1];
+    if (local_solvent_numbers) *local_solvent_numbers = h[1];
+    return SPGNB_OK;
+}
+
+int spgnb_solvent_pme_direct_force(spgnb_solvent* sv, int atom_numbers, int residue_numbers,
+                                   const int* d_res_start, const spgnb_vector* d_crd, const float* d_charge,
+                                   spgnb_vector* d_frc, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
+                                   const spgnb_nl* nl, const spgnb_atom_group* d_nl, float pme_beta,
+                                   int need_atom_energy, float* d_atom_energy, int need_virial,
+                                   spgnb_ltmatrix3* d_atom_virial, float* d_atom_direct_pme_energy)
+{
+    (void)d_charge;
+    if (!sv) return fail(SPGNB_E_ARG, "spgnb_solvent_pme_direct_force: NULL handle");
+    if (nl) return SPGNB_OK;  // evaluated by spgnb_lj_pme_direct_force over the spgnb list
+    if (!d_nl || !d_res_start || !d_crd || !d_frc)
+        return fail(SPGNB_E_ARG, "spgnb_solvent_pme_direct_force: NULL device pointer");
+    spgnb_lj* lj = sv->lj;
+    if (residue_numbers <= sv->solvent_start_local || sv->local_solvent_numbers == 0) return SPGNB_OK;
+    // positions were packed per atom by spgnb_lj_pme_direct_force_atom_groups of this step
+    if (lj->pos_cap < atom_numbers)
+        return fail(SPGNB_E_STATE, "solvent module: call the LJ module's force first (it packs the coordinates)");
+    cudaStream_t s = stream();
+    // the LJ call already converted and cleared its accumulators; reuse them
+    PairConst pc = make_pair_const(lj, pme_beta);
+    PerAtomOut pa{need_atom_energy ? d_atom_energy : nullptr, need_atom_energy ? lj->d_lj_energy_atom : nullptr,
+                  need_atom_energy ? d_atom_direct_pme_energy : nullptr, need_virial ? (float*)d_atom_virial : nullptr};
+    const Cell c = make_cell(cell), rc = make_cell(rcell);
+    const int nres = residue_numbers - sv->solvent_start_local;
+    const int blocks = std::max(1, std::min((nres + 3) / 4, num_sms() * 8));
+    const bool en = need_atom_energy || need_virial;
+    if (sv->water_points == 3)
+    {
+        if (en)
+            k_pair_solvent<2, 3><<<blocks, 128, 0, s>>>(pc, c, rc, sv->solvent_start_local, residue_numbers,
+                                                        atom_numbers, d_res_start, d_nl, lj->d_pos, lj->d_pos_type,
+                                                        lj->d_table, lj->d_frc_acc, lj->d_totals, pa);
+        else
+            k_pair_solvent<0, 3><<<blocks, 128, 0, s>>>(pc, c, rc, sv->solvent_start_local, residue_numbers,
+                                                        atom_numbers, d_res_start, d_nl, lj->d_pos, lj->d_pos_type,
+                                                        lj->d_table, lj->d_frc_acc, lj->d_totals, pa);
+    }
+    else
+    {
+        if (en)
+            k_pair_solvent<2, 4><<<blocks, 128, 0, s>>>(pc, c, rc, sv->solvent_start_local, residue_numbers,
+                                                        atom_numbers, d_res_start, d_nl, lj->d_pos, lj->d_pos_type,
+                                                        lj->d_table, lj->d_frc_acc, lj->d_totals, pa);
+        else
+            k_pair_solvent<0, 4><<<blocks, 128, 0, s>>>(pc, c, rc, sv->solvent_start_local, residue_numbers,
+                                                        atom_numbers, d_res_start, d_nl, lj->d_pos, lj->d_pos_type,
+                                                        lj->d_table, lj->d_frc_acc, lj->d_totals, pa);
+    }
+    SPGNB_CHECK_LAUNCH("k_pair_solvent");
+    k_finalize<<<(atom_numbers + 255) / 256, 256, 0, s>>>(atom_numbers, lj->d_frc_acc, (float3*)d_frc);
+    SPGNB_CHECK_LAUNCH("k_finalize");
+    return SPGNB_OK;
+}
+
+int spgnb_solvent_destroy(spgnb_solvent* s)
+{
+    if (!s) return SPGNB_OK;
+    dfree(s->d_scratch);
+    delete s;
+    return SPGNB_OK;
+}
+
+}  // extern "C"

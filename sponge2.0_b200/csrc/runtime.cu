@@ -1,0 +1,116 @@
+// Error reporting, stream selection and small host utilities of the C ABI.
+#include <math.h>
+#include <stdarg.h>
+#include <stdio.h>
+
+#include "common.cuh"
+
+namespace spgnb
+{
+namespace
+{
+thread_local char g_last_error[1024] = "";
+thread_local cudaStream_t g_stream = nullptr;
+}  // namespace
+
+int fail(int status, const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+    return status;
+}
+
+int cuda_fail(cudaError_t e, const char* what)
+{
+    return fail(SPGNB_E_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+cudaStream_t stream() { return g_stream; }
+
+int num_sms()
+{
+    static int cached = 0;
+    if (cached == 0)
+    {
+        int dev = 0, v = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0) v = 148;
+        cached = v;
+    }
+    return cached;
+}
+
+}  // namespace spgnb
+
+extern "C" {
+
+const char* spgnb_version(void) { return "spgnb 0.1 (sm_100a)"; }
+
+const char* spgnb_status_string(int status)
+{
+    switch (status)
+    {
+        case SPGNB_OK:
+            return "ok";
+        case SPGNB_E_ARG:
+            return "invalid argument";
+        case SPGNB_E_OOM:
+            return "device allocation failed";
+        case SPGNB_E_CUDA:
+            return "CUDA error";
+        case SPGNB_E_OVERFLOW:
+            return "buffer overflow";
+        case SPGNB_E_NONFINITE:
+            return "non-finite result";
+        case SPGNB_E_STATE:
+            return "call out of order";
+        case SPGNB_E_TIMEOUT:
+            return "device wait timed out";
+        case SPGNB_E_UNSUPPORTED:
+            return "unsupported configuration";
+        default:
+            return "unknown status";
+    }
+}
+
+const char* spgnb_last_error(void) { return spgnb::g_last_error; }
+
+int spgnb_set_stream(void* cuda_stream)
+{
+    spgnb::g_stream = (cudaStream_t)cuda_stream;
+    return SPGNB_OK;
+}
+
+// Bisection on erfc(beta*rc)/rc = tol, the search PM_force.cpp:244-272 runs,
+// in the same float arithmetic.
+float spgnb_get_beta(float cutoff, float tolerance)
+{
+    float beta = 0.0f, low, high, tempf;
+    int ilow, ihigh;
+    if (!(cutoff > 0.0f) || !(tolerance > 0.0f)) return 0.0f;
+    high = 1.0f;
+    ihigh = 1;
+    for (;;)
+    {
+        tempf = erfcf(high * cutoff) / cutoff;
+        if (tempf <= tolerance) break;
+        high *= 2;
+        ihigh++;
+    }
+    ihigh += 50;
+    low = 0.0f;
+    for (ilow = 1; ilow < ihigh; ilow++)
+    {
+        beta = (low + high) / 2;
+        tempf = erfcf(beta * cutoff) / cutoff;
+        if (tempf >= tolerance)
+            low = beta;
+        else
+            high = beta;
+    }
+    return beta;
+}
+
+}  // extern "C"

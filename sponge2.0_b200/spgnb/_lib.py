@@ -1,0 +1,114 @@
+"""ctypes binding of libspgnb.so (the C ABI declared in include/spgnb.h).
+
+The shared library is built in-tree (``sponge2.0_b200/libspgnb.so``).  There
+is no fallback: if it is missing or cannot be loaded, every entry point
+raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+PKG_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_DIR, "libspgnb.so")
+
+SPGNB_OK = 0
+STATUS_NAMES = {0: "SPGNB_OK", 1: "SPGNB_E_ARG", 2: "SPGNB_E_OOM", 3: "SPGNB_E_CUDA", 4: "SPGNB_E_OVERFLOW",
+                5: "SPGNB_E_NONFINITE", 6: "SPGNB_E_STATE", 7: "SPGNB_E_TIMEOUT", 8: "SPGNB_E_UNSUPPORTED"}
+
+# every symbol include/spgnb.h declares
+EXPORTED = [
+    "spgnb_version", "spgnb_status_string", "spgnb_last_error", "spgnb_set_stream", "spgnb_get_beta",
+    "spgnb_nl_default_options", "spgnb_nl_create", "spgnb_nl_update", "spgnb_nl_check_overflow",
+    "spgnb_nl_atom_groups", "spgnb_nl_copy_atom_groups", "spgnb_nl_get_stats", "spgnb_nl_destroy",
+    "spgnb_lj_create", "spgnb_lj_get_local", "spgnb_lj_pme_direct_force", "spgnb_lj_pme_direct_force_atom_groups",
+    "spgnb_lj_long_range_correction", "spgnb_lj_energies", "spgnb_lj_totals", "spgnb_lj_long_range_factor",
+    "spgnb_lj_destroy",
+    "spgnb_solvent_create", "spgnb_solvent_get_local", "spgnb_solvent_pme_direct_force", "spgnb_solvent_destroy",
+]
+
+
+class SpgnbError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class LTMatrix3(C.Structure):
+    _fields_ = [("a11", C.c_float), ("a21", C.c_float), ("a22", C.c_float), ("a31", C.c_float),
+                ("a32", C.c_float), ("a33", C.c_float)]
+
+    @classmethod
+    def of(cls, m):
+        m = [float(v) for v in m]
+        return cls(*m)
+
+
+class NLOptions(C.Structure):
+    _fields_ = [("max_neighbor_numbers", C.c_int), ("max_atom_in_grid_numbers", C.c_int),
+                ("max_ghost_in_grid_numbers", C.c_int), ("refresh_interval", C.c_int),
+                ("skin_permit", C.c_float), ("check_overflow_interval", C.c_int),
+                ("throw_error_when_overflow", C.c_int), ("export_atom_groups", C.c_int),
+                ("max_entries_per_cluster", C.c_int)]
+
+
+class NLStats(C.Structure):
+    _fields_ = [("atom_numbers", C.c_int), ("grid_numbers", C.c_int), ("grid_dims", C.c_int * 3),
+                ("clusters", C.c_int), ("entries", C.c_longlong), ("work_items", C.c_int),
+                ("builds", C.c_longlong), ("overflow", C.c_int)]
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise SpgnbError(8, f"{LIB_PATH} is not built; run __graft_entry__.build() or make -C sponge2.0_b200/csrc")
+    L = C.CDLL(LIB_PATH)
+    vp, i, f, d = C.c_void_p, C.c_int, C.c_float, C.c_double
+    M = LTMatrix3
+    L.spgnb_version.restype = C.c_char_p
+    L.spgnb_status_string.restype = C.c_char_p
+    L.spgnb_status_string.argtypes = [i]
+    L.spgnb_last_error.restype = C.c_char_p
+    L.spgnb_set_stream.argtypes = [vp]
+    L.spgnb_get_beta.restype = f
+    L.spgnb_get_beta.argtypes = [f, f]
+    L.spgnb_nl_default_options.argtypes = [C.POINTER(NLOptions)]
+    L.spgnb_nl_default_options.restype = None
+    L.spgnb_nl_create.argtypes = [i, f, f, M, M, C.POINTER(NLOptions), C.POINTER(vp)]
+    L.spgnb_nl_update.argtypes = [vp, vp, i, i, vp, M, M, i, i, vp, vp, vp]
+    L.spgnb_nl_check_overflow.argtypes = [vp, i, M, M, C.POINTER(i)]
+    L.spgnb_nl_atom_groups.argtypes = [vp, C.POINTER(vp), C.POINTER(vp)]
+    L.spgnb_nl_copy_atom_groups.argtypes = [vp, vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]
+    L.spgnb_nl_get_stats.argtypes = [vp, C.POINTER(NLStats)]
+    L.spgnb_nl_destroy.argtypes = [vp]
+    L.spgnb_lj_create.argtypes = [i, i, vp, vp, vp, f, C.POINTER(vp)]
+    L.spgnb_lj_get_local.argtypes = [vp, vp, i, i]
+    L.spgnb_lj_pme_direct_force.argtypes = [vp, i, i, i, i, vp, vp, vp, M, M, vp, f, i, vp, i, vp, vp]
+    L.spgnb_lj_pme_direct_force_atom_groups.argtypes = [vp, i, i, i, i, vp, vp, vp, M, M, vp, f, i, vp, i, vp, vp]
+    L.spgnb_lj_long_range_correction.argtypes = [vp, i, vp, i, vp, f]
+    L.spgnb_lj_energies.argtypes = [vp, C.POINTER(d), C.POINTER(d), C.POINTER(d), C.POINTER(d)]
+    L.spgnb_lj_totals.argtypes = [vp, C.POINTER(d)]
+    L.spgnb_lj_long_range_factor.restype = d
+    L.spgnb_lj_long_range_factor.argtypes = [vp]
+    L.spgnb_lj_destroy.argtypes = [vp]
+    L.spgnb_solvent_create.argtypes = [vp, i, C.POINTER(vp)]
+    L.spgnb_solvent_get_local.argtypes = [vp, i, vp, i, vp, C.POINTER(i)]
+    L.spgnb_solvent_pme_direct_force.argtypes = [vp, i, i, vp, vp, vp, vp, M, M, vp, vp, f, i, vp, i, vp, vp]
+    L.spgnb_solvent_destroy.argtypes = [vp]
+    _lib = L
+    return L
+
+
+def check(status):
+    if status != SPGNB_OK:
+        raise SpgnbError(status, lib().spgnb_last_error().decode())
+    return status
+
+
+def version():
+    return lib().spgnb_version().decode()

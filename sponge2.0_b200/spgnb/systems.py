@@ -1,0 +1,417 @@
+"""Seeded synthetic periodic systems for the short-range nonbonded path.
+
+The reference measures on no public dataset; these generators build the
+water / water+solute boxes its workloads describe, in the units and encodings
+SPONGE's modules receive:
+
+* coordinates in Angstrom as float32 ``VECTOR`` triples, unwrapped;
+* charges pre-multiplied by SPONGE's internal charge scale 18.2223
+  (``SPONGE/common.h`` ``CONSTANT_SPONGE_CHARGE_SCALE``), so q_i*q_j/r is in
+  kcal/mol;
+* LJ pair tables in SPONGE's internal convention: ``A = 12*4*eps*sigma^12``,
+  ``B = 6*4*eps*sigma^6`` (the native loader multiplies the file's A by 12 and
+  B by 6, ``SPONGE/xponge/load/native/lj.hpp:47,57``), stored in the
+  triangular order ``idx(a,b) = max*(max+1)/2 + min``
+  (``SPONGE/Lennard_Jones_force/Lennard_Jones_force.h:18-27``);
+* exclusions as the upper-triangular CSR triple (``excluded_list_start``,
+  ``excluded_numbers``, ``excluded_list``) that ``MD_core/nb.hpp:30-70``
+  builds;
+* the lower-triangular cell ``(a11, a21, a22, a31, a32, a33)`` and its inverse
+  built like ``SPONGE/MD_core/pbc.hpp:66-101``.
+
+Waters go last, one residue per molecule with masses 16.00/1.008/1.008, so a
+solvent module recognises them the way ``solvent_LJ.cpp:193-211`` does.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+CHARGE_SCALE = np.float32(18.2223)
+KB = 0.00198716  # kcal/mol/K, SPONGE/common.h CONSTANT_kB
+OH_BOND = 0.9572
+HOH_ANGLE_DEG = 104.52
+Q_O = -0.834
+Q_H = 0.417
+SIGMA_O = 3.1507
+EPS_O = 0.1521
+MASS_O = 16.00
+MASS_H = 1.008
+MASS_SOLUTE = 12.011
+
+
+def cell_from_box(a, b, c, alpha=90.0, beta=90.0, gamma=90.0):
+    """Lower-triangular cell and inverse, float32, as pbc.hpp:66-101 builds them."""
+    f = np.float32
+    deg = f(0.0174532925)
+    al, be, ga = f(alpha) * deg, f(beta) * deg, f(gamma) * deg
+    a, b, c = f(a), f(b), f(c)
+    ca, cb, cg = np.cos(al), np.cos(be), np.cos(ga)
+    sg = np.sin(ga)
+    za = np.sqrt(f(1) - ca * ca - cb * cb - cg * cg + f(2) * ca * cb * cg)
+    cell = np.array([a, b * cg, b * sg, c * cb, c / sg * (ca - cb * cg), c / sg * za], dtype=np.float32)
+    rcell = np.zeros(6, np.float32)
+    rcell[0] = f(1) / cell[0]
+    rcell[2] = f(1) / cell[2]
+    rcell[5] = f(1) / cell[5]
+    rcell[1] = -rcell[0] / np.tan(ga)
+    rcell[3] = (ca / np.tan(ga) - cb / sg) / za / a
+    rcell[4] = (cb / np.tan(ga) - ca / sg) / za / b
+    for k in (1, 3, 4):
+        if abs(cell[k]) < 1e-3:
+            cell[k] = 0
+        if abs(rcell[k]) < 1e-3:
+            rcell[k] = 0
+    return cell, rcell
+
+
+def frac_to_cart(s, cell):
+    """Row-vector convention r = s * cell (VECTOR * LTMatrix3, vector.hpp:316-321)."""
+    a11, a21, a22, a31, a32, a33 = [float(v) for v in cell]
+    x = s[:, 0] * a11 + s[:, 1] * a21 + s[:, 2] * a31
+    y = s[:, 1] * a22 + s[:, 2] * a32
+    z = s[:, 2] * a33
+    return np.stack([x, y, z], axis=1)
+
+
+def get_beta(cutoff, tolerance=1e-5):
+    """Ewald screening parameter: erfc(beta*rc)/rc == tol by bisection.
+
+    Restates ``Get_Beta`` (``SPONGE/PM_force/PM_force.cpp:244-272``) in float32.
+    """
+    f = np.float32
+    cutoff = f(cutoff)
+    tol = f(tolerance)
+    high = f(1.0)
+    ihigh = 1
+    while True:
+        tempf = f(math.erfc(float(high * cutoff))) / cutoff
+        if tempf <= tol:
+            break
+        high = high * f(2)
+        ihigh += 1
+    ihigh += 50
+    low = f(0.0)
+    beta = f(0.0)
+    for _ in range(1, ihigh):
+        beta = (low + high) / f(2)
+        tempf = f(math.erfc(float(beta * cutoff))) / cutoff
+        if tempf >= tol:
+            low = beta
+        else:
+            high = beta
+    return float(beta)
+
+
+def lj_pair_tables(sigma, eps):
+    """Lorentz-Berthelot pair tables in SPONGE's internal triangular form."""
+    sigma = np.asarray(sigma, np.float64)
+    eps = np.asarray(eps, np.float64)
+    t = len(sigma)
+    p = t * (t + 1) // 2
+    A = np.zeros(p, np.float32)
+    B = np.zeros(p, np.float32)
+    for a in range(t):
+        for b in range(a + 1):
+            s = 0.5 * (sigma[a] + sigma[b])
+            e = math.sqrt(eps[a] * eps[b])
+            idx = a * (a + 1) // 2 + b
+            A[idx] = np.float32(4.0 * e * s ** 12) * np.float32(12.0)
+            B[idx] = np.float32(4.0 * e * s ** 6) * np.float32(6.0)
+    return A, B
+
+
+def lj_type_index(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    hi = np.maximum(a, b)
+    lo = np.minimum(a, b)
+    return hi * (hi + 1) // 2 + lo
+
+
+@dataclass
+class System:
+    crd: np.ndarray            # (N,3) float32
+    charge: np.ndarray         # (N,) float32, scaled
+    atom_type: np.ndarray      # (N,) int32
+    pair_A: np.ndarray         # (P,) float32 internal
+    pair_B: np.ndarray         # (P,) float32 internal
+    n_types: int
+    excl_start: np.ndarray     # (N,) int32
+    excl_numbers: np.ndarray   # (N,) int32
+    excl_list: np.ndarray      # (E,) int32
+    mass: np.ndarray           # (N,) float32
+    res_start: np.ndarray      # (R,) int32
+    res_len: np.ndarray        # (R,) int32
+    cell: np.ndarray           # (6,) float32
+    rcell: np.ndarray          # (6,) float32
+    cutoff: float
+    skin: float
+    beta: float
+    vel: np.ndarray = field(default=None)
+    n_solute: int = 0
+    name: str = ""
+
+    @property
+    def n(self):
+        return int(self.crd.shape[0])
+
+    @property
+    def n_waters(self):
+        return (self.n - self.n_solute) // 3
+
+    @property
+    def volume(self):
+        return float(self.cell[0]) * float(self.cell[2]) * float(self.cell[5])
+
+    @property
+    def solvent_atoms(self):
+        """Atoms in the trailing run of 3-site water residues."""
+        return 3 * self.n_waters
+
+
+def _random_rotations(rng, n):
+    q = rng.normal(size=(n, 4))
+    q /= np.linalg.norm(q, axis=1, keepdims=True)
+    w, x, y, z = q.T
+    R = np.empty((n, 3, 3))
+    R[:, 0, 0] = 1 - 2 * (y * y + z * z)
+    R[:, 0, 1] = 2 * (x * y - z * w)
+    R[:, 0, 2] = 2 * (x * z + y * w)
+    R[:, 1, 0] = 2 * (x * y + z * w)
+    R[:, 1, 1] = 1 - 2 * (x * x + z * z)
+    R[:, 1, 2] = 2 * (y * z - x * w)
+    R[:, 2, 0] = 2 * (x * z - y * w)
+    R[:, 2, 1] = 2 * (y * z + x * w)
+    R[:, 2, 2] = 1 - 2 * (x * x + y * y)
+    return R
+
+
+def _solute_types(rng, n_types=20):
+    sig = rng.uniform(2.5, 4.0, n_types)
+    eps = np.exp(rng.uniform(math.log(0.02), math.log(0.3), n_types))
+    return sig, eps
+
+
+def water_system(n_waters, box, seed, n_solute=0, cutoff=10.0, skin=2.0,
+                 tolerance=1e-5, jitter=0.3, angles=(90.0, 90.0, 90.0),
+                 temperature=300.0, n_solute_types=20, name=""):
+    """Water (+ optional LJ solute) box on a jittered lattice.
+
+    Lattice sites fill the box; waters sit on jittered sites with uniformly
+    random orientations, solutes (if any) take other sites unjittered, and
+    waters crowding a solute are re-jittered until every solute keeps
+    0.7*sigma_ij from other solutes and oxygens.
+    """
+    rng = np.random.default_rng(seed)
+    if np.isscalar(box):
+        box = (box, box, box)
+    cell, rcell = cell_from_box(box[0], box[1], box[2], *angles)
+    n_sites_needed = n_waters + n_solute
+    m = int(math.ceil(n_sites_needed ** (1.0 / 3.0) - 1e-9))
+    while m ** 3 < n_sites_needed:
+        m += 1
+    sites = rng.choice(m ** 3, size=n_sites_needed, replace=False)
+    ijk = np.stack(np.unravel_index(sites, (m, m, m)), axis=1).astype(np.float64)
+    frac = (ijk + 0.5) / m
+    lattice = frac_to_cart(frac, cell)
+    centers = lattice + rng.uniform(-jitter, jitter, size=lattice.shape)
+    centers[:n_solute] = lattice[:n_solute]
+
+    sol_sig = sol_eps = None
+    if n_solute:
+        sol_sig, sol_eps = _solute_types(rng, n_solute_types)
+    sigma_all = np.concatenate([[SIGMA_O, 0.0], sol_sig if n_solute else []])
+    eps_all = np.concatenate([[EPS_O, 0.0], sol_eps if n_solute else []])
+    n_types = len(sigma_all)
+    pair_A, pair_B = lj_pair_tables(sigma_all, eps_all)
+
+    sol_center = centers[:n_solute]
+    wat_center = centers[n_solute:]
+    sol_type = rng.integers(2, n_types, size=n_solute) if n_solute else np.zeros(0, int)
+    if n_solute:
+        _resolve_solute_overlaps(rng, sol_center, sol_type, wat_center, sigma_all, cell, box, jitter,
+                                 sites_wat=lattice[n_solute:])
+
+    # water geometry in its body frame, O at the origin
+    half = math.radians(HOH_ANGLE_DEG) / 2
+    body = np.array([[0.0, 0.0, 0.0],
+                     [OH_BOND * math.sin(half), 0.0, OH_BOND * math.cos(half)],
+                     [-OH_BOND * math.sin(half), 0.0, OH_BOND * math.cos(half)]])
+    R = _random_rotations(rng, n_waters)
+    wat = wat_center[:, None, :] + np.einsum("nij,kj->nki", R, body)
+
+    n = n_solute + 3 * n_waters
+    crd = np.empty((n, 3), np.float64)
+    crd[:n_solute] = sol_center
+    crd[n_solute:] = wat.reshape(-1, 3)
+    crd = crd.astype(np.float32)
+
+    charge = np.empty(n, np.float64)
+    if n_solute:
+        q = rng.normal(0.0, 0.4, n_solute)
+        q -= q.mean()
+        charge[:n_solute] = q
+    charge[n_solute:] = np.tile([Q_O, Q_H, Q_H], n_waters)
+    charge = (charge.astype(np.float32) * CHARGE_SCALE).astype(np.float32)
+
+    atom_type = np.empty(n, np.int32)
+    atom_type[:n_solute] = sol_type
+    atom_type[n_solute:] = np.tile([0, 1, 1], n_waters)
+
+    mass = np.empty(n, np.float32)
+    mass[:n_solute] = MASS_SOLUTE
+    mass[n_solute:] = np.tile([MASS_O, MASS_H, MASS_H], n_waters)
+
+    # exclusions: intra-water O-H1, O-H2, H1-H2 (upper triangular)
+    excl_numbers = np.zeros(n, np.int32)
+    o = n_solute + 3 * np.arange(n_waters)
+    excl_numbers[o] = 2
+    excl_numbers[o + 1] = 1
+    excl_start = np.zeros(n, np.int32)
+    excl_start[1:] = np.cumsum(excl_numbers)[:-1]
+    excl_list = np.empty(int(excl_numbers.sum()), np.int32)
+    s = excl_start[o]
+    excl_list[s] = o + 1
+    excl_list[s + 1] = o + 2
+    excl_list[excl_start[o + 1]] = o + 2
+
+    res_len = np.concatenate([np.ones(n_solute, np.int32), np.full(n_waters, 3, np.int32)])
+    res_start = np.zeros(len(res_len), np.int32)
+    res_start[1:] = np.cumsum(res_len)[:-1]
+
+    vel = (rng.normal(size=(n, 3)) * np.sqrt(KB * temperature / mass)[:, None]).astype(np.float32)
+    return System(crd=crd, charge=charge, atom_type=atom_type, pair_A=pair_A, pair_B=pair_B,
+                  n_types=n_types, excl_start=excl_start, excl_numbers=excl_numbers,
+                  excl_list=excl_list, mass=mass, res_start=res_start, res_len=res_len,
+                  cell=cell, rcell=rcell, cutoff=float(cutoff), skin=float(skin),
+                  beta=get_beta(cutoff, tolerance), vel=vel, n_solute=n_solute, name=name)
+
+
+def _resolve_solute_overlaps(rng, sol_center, sol_type, wat_center, sigma, cell, box, jitter,
+                             sites_sol=None, sites_wat=None, tries=200):
+    """Keep every solute at least 0.7*sigma_ij from other solutes and oxygens.
+
+    Solutes sit on their lattice sites without jitter; waters that crowd a
+    solute get their jitter redrawn (halved on each retry).  At this site
+    density (2.9 A spacing) a 0.7*sigma_ij clearance is the tightest one a
+    lattice can always satisfy for sigma up to 4 A.
+    """
+    from scipy.spatial import cKDTree
+    orth = all(abs(float(cell[k])) < 1e-6 for k in (1, 3, 4))
+    L = np.array([float(cell[0]), float(cell[2]), float(cell[5])])
+    ns = len(sol_center)
+    amp = np.full(len(wat_center), jitter)
+    for _ in range(tries):
+        pts = np.concatenate([sol_center, wat_center])
+        typ = np.concatenate([sol_type, np.zeros(len(wat_center), int)])
+        if orth:
+            tree = cKDTree(np.mod(pts, L), boxsize=L)
+        else:
+            tree = cKDTree(pts)
+        pairs = tree.query_pairs(0.7 * 4.0, output_type="ndarray")
+        if len(pairs) == 0:
+            return
+        pairs = pairs[(pairs[:, 0] < ns) | (pairs[:, 1] < ns)]
+        d = pts[pairs[:, 0]] - pts[pairs[:, 1]]
+        if orth:
+            d -= np.round(d / L) * L
+        r = np.linalg.norm(d, axis=1)
+        sij = 0.5 * (sigma[typ[pairs[:, 0]]] + sigma[typ[pairs[:, 1]]])
+        bad = pairs[r < 0.7 * sij]
+        if len(bad) == 0:
+            return
+        w = np.unique(bad.ravel())
+        w = w[w >= ns] - ns
+        if len(w) == 0:
+            raise RuntimeError("solute-solute clearance impossible at this density")
+        amp[w] *= 0.5
+        wat_center[w] = sites_wat[w] + rng.uniform(-1, 1, size=(len(w), 3)) * amp[w, None]
+    raise RuntimeError("could not place solutes without overlaps")
+
+
+# ---------------------------------------------------------------------------
+# Named workloads.  Sizes follow the workload descriptions: a 40 A box of
+# 2,160 waters; a 96,000-atom mixed box; a ~1.0M-atom water box; 256 uneven
+# systems; a Poisson stream of MD segments.
+# ---------------------------------------------------------------------------
+
+def water_box_6480(seed=1):
+    return water_system(2160, 40.0, seed, cutoff=10.0, skin=2.0, name="water-6480")
+
+
+def mixed_box_96k(seed=2):
+    # 30,000 waters + 6,000 solute atoms in a 99 A cubic box (0.0989 atoms/A^3)
+    return water_system(30000, 99.0, seed, n_solute=6000, cutoff=10.0, skin=2.0, name="mixed-96k")
+
+
+def water_box_1m(seed=3):
+    n_w = 333333
+    L = (n_w / 0.0334) ** (1.0 / 3.0)
+    return water_system(n_w, L, seed, cutoff=12.0, skin=2.0, name="water-1m")
+
+
+def batch_systems(n_systems=256, seed=4, n_min=1500, n_max=24000, skin=2.0):
+    """Independent systems with log-uniform atom counts and uneven cutoffs.
+
+    The cutoff is drawn uniformly from {8, 10, 12} among the values that keep
+    rc + skin <= L/2, so each pair has a single minimum image.
+    """
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n_systems):
+        n_atoms = int(math.exp(rng.uniform(math.log(n_min), math.log(n_max))))
+        frac_sol = rng.uniform(0.0, 0.15)
+        n_sol = int(round(frac_sol * n_atoms))
+        n_w = max(1, (n_atoms - n_sol) // 3)
+        L = ((n_w + n_sol) / 0.0334) ** (1.0 / 3.0)
+        allowed = [rc for rc in (8.0, 10.0, 12.0) if rc + skin <= L / 2]
+        if not allowed:
+            allowed = [max(4.0, L / 2 - skin)]
+        rc = float(rng.choice(allowed))
+        out.append(water_system(n_w, L, int(rng.integers(1 << 31)), n_solute=n_sol, cutoff=rc,
+                                skin=skin, name=f"batch-{k}"))
+    return out
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival_s: float
+    n_atoms: int
+    steps: int
+    seed: int
+
+
+def request_stream(duration_s=600.0, rate_per_s=40.0, seed=5, n_min=1000, n_max=50000,
+                   steps_min=500, steps_max=5000):
+    """Poisson arrivals of MD segments with log-uniform sizes."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    rid = 0
+    while True:
+        t += rng.exponential(1.0 / rate_per_s)
+        if t > duration_s:
+            break
+        n_atoms = int(math.exp(rng.uniform(math.log(n_min), math.log(n_max))))
+        steps = int(rng.integers(steps_min, steps_max + 1))
+        out.append(Request(rid, t, n_atoms, steps, int(rng.integers(1 << 31))))
+        rid += 1
+    return out
+
+
+def request_system(req: Request, skin=2.0):
+    rng = np.random.default_rng(req.seed)
+    frac_sol = rng.uniform(0.0, 0.15)
+    n_sol = int(round(frac_sol * req.n_atoms))
+    n_w = max(1, (req.n_atoms - n_sol) // 3)
+    L = ((n_w + n_sol) / 0.0334) ** (1.0 / 3.0)
+    allowed = [rc for rc in (8.0, 10.0, 12.0) if rc + skin <= L / 2]
+    if not allowed:
+        allowed = [max(4.0, L / 2 - skin)]
+    rc = float(rng.choice(allowed))
+    return water_system(n_w, L, int(rng.integers(1 << 31)), n_solute=n_sol, cutoff=rc, skin=skin,
+                        name=f"req-{req.rid}")

@@ -1,0 +1,241 @@
+"""Parity of the CUDA path with the oracle (and the reference's own kernels).
+
+Bar: the exported neighbour list equals the oracle's reference-rule list pair
+for pair; forces within 1e-5 relative RMS of the FP64 direct pair sum;
+energies and virial within 1e-5 relative of FP64; runs bitwise reproducible.
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, rel_rms
+
+pytestmark = pytest.mark.gpu
+
+FORCE_REL_RMS_TOL = 1e-5      # force error vs FP64, relative RMS
+ENERGY_REL_TOL = 1e-5         # total energy / virial vs FP64, relative
+
+
+def _systems():
+    from spgnb import systems as S
+    return {
+        "water-6480": lambda: S.water_box_6480(),
+        "mixed-small": lambda: S.water_system(2600, 31.0, 11, n_solute=400, cutoff=8.0, skin=2.0, name="mixed"),
+        "triclinic": lambda: S.water_system(1800, (30.0, 31.0, 33.0), 12, n_solute=100, cutoff=8.0, skin=2.0,
+                                            angles=(75.0, 80.0, 70.0), name="tri"),
+        "small-box": lambda: S.water_system(500, 24.6, 13, cutoff=8.0, skin=2.0, name="small"),
+    }
+
+
+SYSTEMS = _systems()
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch
+
+
+def _path(system, **kw):
+    from spgnb.engine import PlainPath
+    return PlainPath(system, **kw)
+
+
+@pytest.mark.parametrize("name", list(SYSTEMS))
+def test_neighbor_set_identical_to_oracle(torch_cuda, oracle, name):
+    s = SYSTEMS[name]()
+    p = _path(s, export_atom_groups=True)
+    counts, lists = p.nl.host_atom_groups()
+    oc, ol = oracle.nl_build(s, mode=1)
+    assert counts.sum() == oc.sum(), f"{name}: {counts.sum()} pairs vs oracle {oc.sum()}"
+    assert np.array_equal(counts, oc)
+    assert np.array_equal(lists, ol)
+    st = p.nl.stats()
+    assert st["overflow"] == 0
+
+
+@pytest.mark.parametrize("name", list(SYSTEMS))
+def test_forces_vs_fp64_direct_sum(torch_cuda, oracle, name):
+    s = SYSTEMS[name]()
+    p = _path(s)
+    frc = p.force(need_energy=True, need_virial=True).cpu().numpy()
+    ref = oracle.direct_sum(s)
+    err = rel_rms(frc, ref["frc"])
+    assert err <= FORCE_REL_RMS_TOL, f"{name}: force rel RMS {err:.3e}"
+    tot = p.lj.totals()
+    e_lj, e_c = tot[0], tot[1]
+    assert abs(e_lj - ref["e_lj"]) <= ENERGY_REL_TOL * abs(ref["e_lj"]) + 1e-3
+    assert abs(e_c - ref["e_coul"]) <= ENERGY_REL_TOL * (abs(ref["e_lj"]) + abs(ref["e_coul"])) + 1e-3
+    vir_scale = np.abs(ref["virial"]).max()
+    assert np.abs(tot[2:] - ref["virial"]).max() <= ENERGY_REL_TOL * vir_scale + 1e-3
+
+
+def test_per_atom_energy_and_virial_owner(torch_cuda, oracle):
+    """Per-atom energy/virial go to the pair's owner (the lower index), as the
+    generic reference kernel attributes them."""
+    from spgnb.engine import PlainPath
+    s = SYSTEMS["mixed-small"]()
+    p = PlainPath(s, solvent=False)
+    p.force(need_energy=True, need_virial=True)
+    e = p.atom_energy.cpu().numpy().astype(np.float64)
+    v = p.atom_virial.cpu().numpy().astype(np.float64)
+    counts, lists = oracle.nl_build(s, mode=1)
+    ref = oracle.pair_force(s, counts, lists)
+    e_ref = ref["e_lj_atom"] + ref["e_coul_atom"]
+    scale = np.abs(e_ref).max()
+    assert np.abs(e - e_ref).max() <= 1e-4 * scale
+    assert np.abs(v - ref["virial_atom"]).max() <= 1e-4 * np.abs(ref["virial_atom"]).max()
+    lj_atom = p.lj.handle  # module-owned LJ energy is summed through Step_Print
+    sp = p.lj.Step_Print()
+    assert abs(sp["LJ_short"] - ref["e_lj"]) <= 1e-5 * abs(ref["e_lj"]) + 1e-3
+    del lj_atom
+
+
+def test_bitwise_reproducible(torch_cuda):
+    s = SYSTEMS["water-6480"]()
+    p = _path(s)
+    a = p.force().clone()
+    b = p.force().clone()
+    assert torch_cuda.equal(a, b)
+    p.update(0, forced=True)
+    c = p.force().clone()
+    assert torch_cuda.equal(a, c)
+
+
+def test_atom_group_path_matches(torch_cuda, oracle):
+    """The reference-layout entry point over the exported list gives the same
+    forces (generic kernel for solutes, solvent module for waters)."""
+    s = SYSTEMS["mixed-small"]()
+    p = _path(s, export_atom_groups=True)
+    f_fast = p.force(need_energy=True, need_virial=True).clone()
+    tot_fast = p.lj.totals()
+    torch = torch_cuda
+    frc = torch.zeros_like(p.frc)
+    p.lj.LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(p.n, p.n, p.solvent_numbers, 0, p.crd, p.charge, frc,
+                                                         s.cell, s.rcell, p.nl.d_nl, s.beta, 1, p.atom_energy, 1,
+                                                         p.atom_virial, p.atom_direct)
+    p.solvent.LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(p.n, len(s.res_len), p.res_start, p.crd, p.charge,
+                                                              frc, s.cell, s.rcell, p.nl.d_nl, s.beta, 1,
+                                                              p.atom_energy, 1, p.atom_virial, p.atom_direct)
+    tot_groups = p.lj.totals()
+    ref = oracle.direct_sum(s)
+    assert rel_rms(frc.cpu().numpy(), ref["frc"]) <= FORCE_REL_RMS_TOL
+    assert rel_rms(frc.cpu().numpy(), f_fast.cpu().numpy()) <= FORCE_REL_RMS_TOL
+    assert np.allclose(tot_groups, tot_fast, rtol=1e-5, atol=1e-2)
+
+
+def test_long_range_correction(torch_cuda, oracle):
+    s = SYSTEMS["mixed-small"]()
+    p = _path(s)
+    f = oracle.long_range_factor(s)
+    assert abs(p.lj.long_range_factor - f) <= 1e-6 * abs(f)
+    torch = torch_cuda
+    vir = torch.zeros((1, 6), dtype=torch.float32, device="cuda")
+    pot = torch.zeros(1, dtype=torch.float32, device="cuda")
+    p.lj.Long_Range_Correction(1, vir, 1, pot, s.volume)
+    v = vir.cpu().numpy()[0]
+    assert abs(pot.item() - f / s.volume) <= 1e-5 * abs(f / s.volume)
+    assert abs(v[0] - 2 * f / s.volume) <= 1e-5 * abs(2 * f / s.volume)
+    assert v[1] == 0 and v[3] == 0 and v[4] == 0
+
+
+def test_stale_list_after_motion(torch_cuda, oracle):
+    """Between rebuilds the pairs of the build-time list are evaluated at the
+    current coordinates, exactly as the reference does."""
+    torch = torch_cuda
+    s = SYSTEMS["water-6480"]()
+    p = _path(s, refresh_interval=1000)
+    rng = np.random.default_rng(5)
+    moved = (s.crd + rng.uniform(-0.3, 0.3, size=s.crd.shape)).astype(np.float32)
+    mc = torch.from_numpy(moved).cuda()
+    p.update(1, crd=mc)  # not a rebuild step
+    frc = p.force(crd=mc).cpu().numpy()
+    counts, lists = oracle.nl_build(s, mode=1)  # build-time list
+    ref = oracle.pair_force(s, counts, lists, crd=moved)
+    assert rel_rms(frc, ref["frc"]) <= FORCE_REL_RMS_TOL
+
+
+def test_skin_triggered_rebuild(torch_cuda):
+    torch = torch_cuda
+    s = SYSTEMS["water-6480"]()
+    p = _path(s, refresh_interval=0)
+    b0 = p.nl.stats()["builds"]
+    small = torch.from_numpy(s.crd + np.float32(0.1)).cuda()
+    p.update(1, crd=small)
+    assert p.nl.stats()["builds"] == b0  # 0.1 A < skin*permit = 1 A
+    big = s.crd.copy()
+    big[17] += np.float32(1.5)
+    p.update(2, crd=torch.from_numpy(big).cuda())
+    assert p.nl.stats()["builds"] == b0 + 1
+
+
+def test_wrapped_coordinates_between_builds(torch_cuda):
+    """A caller that wraps coordinates into the box between rebuilds gets the
+    same forces (the pack step takes the minimum image of the displacement)."""
+    torch = torch_cuda
+    s = SYSTEMS["water-6480"]()
+    p = _path(s, refresh_interval=1000)
+    a = p.force().cpu().numpy()
+    L = float(s.cell[0])
+    shifted = s.crd.copy()
+    shifted[::7, 0] += np.float32(L)
+    p.update(1, crd=torch.from_numpy(shifted).cuda())
+    b = p.force(crd=torch.from_numpy(shifted).cuda()).cpu().numpy()
+    assert rel_rms(b, a) <= 1e-6
+
+
+def test_overflow_detected_and_regrown(torch_cuda, oracle):
+    from spgnb.modules import NEIGHBOR_LIST
+    torch = torch_cuda
+    s = SYSTEMS["water-6480"]()
+    from spgnb.engine import PlainPath
+    p = PlainPath.__new__(PlainPath)
+    # a list with room for only a few cluster pairs per cluster overflows
+    nl = NEIGHBOR_LIST()
+    nl.Initial({"neighbor_list_max_entries_per_cluster": 8, "neighbor_list_check_overflow_interval": 1},
+               s.n, s.cutoff, s.skin, s.cell, s.rcell, export_atom_groups=True)
+    dev = "cuda"
+    crd = torch.from_numpy(s.crd).to(dev)
+    al = torch.arange(s.n, dtype=torch.int32, device=dev)
+    es = torch.from_numpy(s.excl_start).to(dev)
+    el = torch.from_numpy(s.excl_list).to(dev)
+    en = torch.from_numpy(s.excl_numbers).to(dev)
+    nl.Update(al, s.n, 0, crd, s.cell, s.rcell, 0, 1, es, el, en)
+    assert nl.stats()["overflow"] & 4
+    grown = False
+    for k in range(60):
+        if not nl.Check_Overflow({}, 0, s.cell, s.rcell):
+            break
+        grown = True
+        nl.Update(al, s.n, 0, crd, s.cell, s.rcell, 0, 1, es, el, en)
+    assert grown and nl.stats()["overflow"] == 0
+    counts, lists = nl.host_atom_groups()
+    oc, ol = oracle.nl_build(s, mode=1)
+    assert np.array_equal(counts, oc) and np.array_equal(lists, ol)
+    del p
+
+
+REF_CUDA = os.path.join(ROOT, "oracle", "_ref", "libspgref_cuda.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CUDA), reason="reference CUDA harness not built")
+@pytest.mark.parametrize("name", ["water-6480", "mixed-small", "triclinic"])
+def test_matches_reference_gpu_kernels(torch_cuda, oracle, name):
+    """Same inputs through the reference's own CUDA kernels (built from its
+    sources for sm_100a): identical neighbour set, forces within 1e-5."""
+    import oracle as O
+    s = SYSTEMS[name]()
+    ref = O.Reference(gpu=True)
+    ref.init(s, refresh_interval=20, solvent=True)
+    ref.nl_update(forced=True)
+    rc, rl, flags = ref.nl_get()
+    p = _path(s, export_atom_groups=True)
+    counts, lists = p.nl.host_atom_groups()
+    assert np.array_equal(counts, rc) and np.array_equal(lists, rl)
+    r = ref.force()
+    ours = p.force(need_energy=True, need_virial=True).cpu().numpy()
+    assert rel_rms(ours, r["frc"]) <= FORCE_REL_RMS_TOL
+    ref.clear()
