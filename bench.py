@@ -1,0 +1,315 @@
+#!/usr/bin/env python
+"""Benchmark of the short-range nonbonded path on the 96,000-atom mixed box.
+
+One step is what SPONGE's Main_Calculate_Force runs on this path
+(SPONGE/main.cpp:307-397): a conditional neighbour-list update (a full
+rebuild every 20 steps), the LJ + PME direct-space force with energy and
+virial, and the long-range correction.  Workload: 30,000 rigid-geometry
+waters + 6,000 LJ solute atoms of 20 types in a 99 A box, cutoff 10 A,
+skin 2 A, beta from tolerance 1e-5, seeded synthetic coordinates (static
+between steps; the rebuild cadence is the reference's refresh_interval).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl spgnb|reference]
+
+Metric: atom-steps/s (whole job, all ranks) and ns/day at dt = 2 fs.  Each
+timed step is bracketed by CUDA events on the launching stream, with L2
+flushed (a 512 MiB write) between steps outside the events; the job time is
+the max over ranks.  N > 1 runs independent replicas, one per GPU
+(one-rank-per-system sharding, no collective in the data path).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "sponge2.0_b200"))
+
+DT_PS = 0.002
+REFRESH_INTERVAL = 20
+WORKLOAD = "mixed-box-96k: 30000 waters + 6000 LJ solutes (20 types), 99 A cubic, rc 10 A, skin 2 A"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=400)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", choices=["spgnb", "reference"], default="spgnb")
+    p.add_argument("--terms", choices=["fev", "f"], default="fev",
+                   help="fev: force + energy + virial every step; f: force only")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    return p.parse_args()
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.lines = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.index)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if f[5 + k].lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_reference_rate(system, terms, budget_s, threads=None):
+    """The reference's own CPU implementation of the path (oracle/_ref, built
+    from its sources) timed on this host: forced build, then conditional
+    update + force per step, refresh_interval 20."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ref = O.Reference(gpu=False)
+    threads = threads or os.cpu_count() or 1
+    ref.set_threads(threads)
+    ref.init(system, refresh_interval=REFRESH_INTERVAL)
+    ref.nl_update(forced=True)
+    fe = terms == "fev"
+    probe = ref.time_steps(2, first_step=0, need_energy=fe, need_virial=fe)
+    per = probe / 2
+    steps = max(REFRESH_INTERVAL, min(200, int(budget_s / max(per, 1e-6))))
+    steps = (steps // REFRESH_INTERVAL) * REFRESH_INTERVAL
+    t = ref.time_steps(steps, first_step=2, need_energy=fe, need_virial=fe)
+    ref.clear()
+    return system.n * steps / t, threads, steps, t
+
+
+def run_reference_arm(args, world, rank):
+    from spgnb import systems as S
+    if rank != 0:
+        return
+    s = S.mixed_box_96k()
+    budget = max(20.0, min(150.0, 0.5 * (args.steps + args.warmup)))
+    rate, threads, steps, t = cpu_reference_rate(s, args.terms, budget)
+    line = {"metric": "atom-steps/s", "value": rate, "unit": "atom-steps/s", "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": 2, "ms_per_step": 1e3 * t / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "ns_per_day": steps * 86.4 * DT_PS / t,
+            "config": {"workload": WORKLOAD, "terms": args.terms, "refresh_interval": REFRESH_INTERVAL,
+                       "atoms": s.n, "parallelism": "replicas"},
+            "cpu_baseline": {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+                             "sample": f"{steps} steps of the 96k box (incl. {steps // REFRESH_INTERVAL} rebuilds)"},
+            "e2e": {"value": rate, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    world, rank, local = dist_setup()
+    import torch
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    if args.impl == "reference":
+        run_reference_arm(args, world, rank)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    from spgnb import systems as S
+    from spgnb._lib import lib
+    from spgnb.engine import PlainPath
+    import ctypes as C
+
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    s = S.mixed_box_96k()
+    fe = args.terms == "fev"
+    L = lib()
+    path = PlainPath(s, refresh_interval=REFRESH_INTERVAL, export_atom_groups=False, device=dev)
+    stream = torch.cuda.current_stream()
+
+    def step(k):
+        path.update(k)
+        path.force(need_energy=fe, need_virial=fe, per_atom=False)
+        if fe:
+            path.lj.Long_Range_Correction(1, path.atom_virial, 1, path.atom_energy, s.volume)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+
+    # algorithmic work of one pair-kernel launch (convention: 20 FLOP per
+    # listed pair, 45 per pair inside rc, +22 with energy and virial)
+    listed, inside = C.c_longlong(), C.c_longlong()
+    L.spgnb_nl_count_pairs(path.nl.handle, C.c_void_p(path.crd.data_ptr()), _ltm(s.cell), _ltm(s.rcell),
+                           s.cutoff, C.byref(listed), C.byref(inside))
+    flop_per_launch = 20.0 * listed.value + (45.0 + (22.0 if fe else 0.0)) * inside.value
+    peak = C.c_double()
+    L.spgnb_probe_fp32_fma_tflops(5, C.byref(peak))
+
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    K = args.steps
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    for a, b in ev + pev:
+        a.record()
+        b.record()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    launches0 = L.spgnb_launch_count()
+    for k in range(K):
+        flush.fill_(k & 0xff)
+        ev[k][0].record(stream)
+        L.spgnb_debug_set_pair_events(C.c_void_p(pev[k][0].cuda_event), C.c_void_p(pev[k][1].cuda_event))
+        step(args.warmup + k)
+        ev[k][1].record(stream)
+    L.spgnb_debug_set_pair_events(None, None)
+    torch.cuda.synchronize()
+    launches = L.spgnb_launch_count() - launches0
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    pair_ms = [a.elapsed_time(b) for a, b in pev]
+    total_ms = sum(step_ms)
+
+    # end to end through the module API with host buffers: pinned H2D of the
+    # coordinates, the step, D2H of forces and the FP64 totals, every step
+    crd_host = torch.from_numpy(s.crd.copy()).pin_memory()
+    frc_host = torch.empty((s.n, 3), dtype=torch.float32).pin_memory()
+    e2e_ms = []
+    for k in range(K):
+        flush.fill_(k & 0xff)
+        a, b = ev[k]
+        a.record(stream)
+        path.crd.copy_(crd_host, non_blocking=True)
+        step(args.warmup + K + k)
+        frc_host.copy_(path.frc, non_blocking=True)
+        if fe:
+            path.lj.totals()
+        b.record(stream)
+        b.synchronize()
+        e2e_ms.append(a.elapsed_time(b))
+    e2e_total = sum(e2e_ms)
+
+    if dist is not None:
+        t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_total = float(t[0]), float(t[1])
+
+    if rank == 0:
+        atoms_steps = world * s.n * K
+        value = atoms_steps / (total_ms * 1e-3)
+        pair_avg_ms = sum(pair_ms) / len(pair_ms)
+        achieved = flop_per_launch / (pair_avg_ms * 1e-3) / 1e12
+        prof = _profile_traffic()
+        line = {
+            "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": K,
+            "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "ns_per_day": K * 86.4 * DT_PS / (total_ms * 1e-3),
+            "config": {"workload": WORKLOAD, "atoms_per_gpu": s.n, "terms": args.terms,
+                       "refresh_interval": REFRESH_INTERVAL, "l2": "flushed between steps (512 MiB write)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single system"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
+                         "frac": achieved / peak.value if peak.value else None,
+                         "traffic": prof.get("bytes_per_launch"),
+                         "kernel": "k_pair_clusters", "kernel_ms": pair_avg_ms,
+                         "flop_per_launch": flop_per_launch, "listed_pairs": listed.value,
+                         "pairs_in_cutoff": inside.value,
+                         "peak_source": "measured FP32 FFMA throughput on this device (spgnb_probe_fp32_fma_tflops)",
+                         "traffic_source": prof.get("source")},
+            "clocks": clocks,
+            "gpu_launches": int(launches),
+            "e2e": {"value": world * s.n * K / (e2e_total * 1e-3), "unit": "atom-steps/s",
+                    "h2d_bytes_per_step": s.n * 12, "d2h_bytes_per_step": s.n * 12 + (64 if fe else 0)},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                rate, threads, steps, t = cpu_reference_rate(s, args.terms, args.cpu_seconds)
+                line["cpu_baseline"] = {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
+                                        "sample": f"{steps} steps of the same box on the host "
+                                                  f"({steps // REFRESH_INTERVAL} rebuilds), {t:.1f} s"}
+            except Exception as exc:  # the baseline is reported, not required
+                line["cpu_baseline"] = {"value": None, "unit": "atom-steps/s", "cores": 0, "kind": "reference",
+                                        "sample": f"unavailable: {exc}"}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _ltm(m):
+    from spgnb._lib import LTMatrix3
+    return LTMatrix3.of(m)
+
+
+def _profile_traffic():
+    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "k_pair_clusters_mixed96k.json")
+    if not os.path.exists(p):
+        return {}
+    try:
+        d = json.load(open(p))
+        return {"bytes_per_launch": d.get("dram_bytes_per_launch"), "source": d.get("source")}
+    except Exception:
+        return {}
+
+
+if __name__ == "__main__":
+    main()

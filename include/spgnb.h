@@ -253,6 +253,20 @@ int spgnb_solvent_pme_direct_force(spgnb_solvent* s, int atom_numbers, int resid
 
 int spgnb_solvent_destroy(spgnb_solvent* s);
 
+/* ------------------------------------------------------------ diagnostics */
+/* Kernel launches issued by the library so far (all threads). */
+unsigned long long spgnb_launch_count(void);
+/* CUDA events (cudaEvent_t, or NULL to stop) recorded around every later
+ * cluster-pair force kernel launched from this host thread. */
+int spgnb_debug_set_pair_events(void* start_event, void* stop_event);
+/* Listed pairs of the last build and those inside `cutoff` at d_crd
+ * (synchronises; the inputs of the algorithmic work count). */
+int spgnb_nl_count_pairs(spgnb_nl* nl, const spgnb_vector* d_crd, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
+                         float cutoff, long long* listed, long long* in_cutoff);
+/* FP32 fused-multiply-add throughput of this device in TFLOP/s (best of
+ * `repeats` timed launches of independent FMA chains). */
+int spgnb_probe_fp32_fma_tflops(int repeats, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

@@ -26,12 +26,18 @@ int num_sms();
         if (e__ != cudaSuccess) return ::spgnb::cuda_fail(e__, #call); \
     } while (0)
 
+void count_launch();
+
 #define SPGNB_CHECK_LAUNCH(name)                                        \
     do                                                                  \
     {                                                                   \
+        ::spgnb::count_launch();                                        \
         cudaError_t e__ = cudaGetLastError();                           \
         if (e__ != cudaSuccess) return ::spgnb::cuda_fail(e__, name);   \
     } while (0)
+
+// events recorded around the pair kernel when set (benchmark instrumentation)
+void pair_events(cudaEvent_t* start, cudaEvent_t* stop);
 
 template <typename T>
 int dalloc(T** p, size_t count)

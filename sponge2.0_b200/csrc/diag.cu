@@ -1,0 +1,173 @@
+// Diagnostics used by the benchmark: pair counts of a built list and an
+// FP32 fused-multiply-add throughput probe (the denominator of the FP32
+// roofline, measured on the device the benchmark runs on).
+#include <algorithm>
+
+#include "common.cuh"
+
+namespace spgnb
+{
+namespace
+{
+
+// Counts listed pairs (mask bits) and those inside the cutoff at the given
+// coordinates, reading the slots the last force call packed.
+__global__ void k_count_pairs(const int* __restrict__ counters, int items_cap, const int4* __restrict__ items,
+                              const int4* __restrict__ ents, const uint4* __restrict__ cl_u,
+                              const int* __restrict__ slot_atom, const float4* __restrict__ x0,
+                              const float4* __restrict__ d0, const float3* __restrict__ crd, Cell cell, Cell rcell,
+                              float rc2, unsigned long long* out)
+{
+    const int lane = threadIdx.x & 31, jl = lane & 7, row = lane >> 3;
+    const int nitems = min(counters[kCntItems], items_cap);
+    const int total_warps = gridDim.x * (blockDim.x >> 5);
+    unsigned long long listed = 0, inside = 0;
+    auto pos = [&](int s) {
+        int a = slot_atom[s];
+        float4 d = d0[s];
+        if (a < 0) return make_float3(d.x, d.y, d.z);
+        float3 c = crd[a];
+        float4 o = x0[s];
+        float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+        float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
+        float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
+        float sz = rintf(dz * rcell.a33);
+        dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
+        dy -= sy * cell.a22 + sz * cell.a32;
+        dz -= sz * cell.a33;
+        return make_float3(d.x + dx, d.y + dy, d.z + dz);
+    };
+    for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += total_warps)
+    {
+        int4 item = items[it];
+        uint4 ui = cl_u[item.x];
+        for (int e = item.y; e < item.y + item.z; e++)
+        {
+            int4 en = ents[e];
+            uint4 uj = cl_u[en.x];
+            const float s32 = 2.3283064365386963e-10f;
+            float fx = (float)(int)(uj.x - ui.x) * s32, fy = (float)(int)(uj.y - ui.y) * s32,
+                  fz = (float)(int)(uj.z - ui.z) * s32;
+            float3 pj = pos(en.x * kClusterSize + jl);
+            for (int h = 0; h < 2; h++)
+            {
+                unsigned m = (unsigned)(h ? en.w : en.z);
+                if (!((m >> lane) & 1u)) continue;
+                float3 pi = pos(item.x * kClusterSize + row + 4 * h);
+                float dx = fx * cell.a11 + fy * cell.a21 + fz * cell.a31 + pj.x - pi.x;
+                float dy = fy * cell.a22 + fz * cell.a32 + pj.y - pi.y;
+                float dz = fz * cell.a33 + pj.z - pi.z;
+                float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
+                float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
+                float sz = rintf(dz * rcell.a33);
+                dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
+                dy -= sy * cell.a22 + sz * cell.a32;
+                dz -= sz * cell.a33;
+                listed++;
+                if (dx * dx + dy * dy + dz * dz < rc2) inside++;
+            }
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        listed += __shfl_xor_sync(0xffffffffu, listed, o);
+        inside += __shfl_xor_sync(0xffffffffu, inside, o);
+    }
+    if (lane == 0)
+    {
+        atomicAdd(&out[0], listed);
+        atomicAdd(&out[1], inside);
+    }
+}
+
+// Independent FMA chains, eight per thread, so the pipe never waits on a
+// dependency; the result is stored to keep the work alive.
+__global__ void k_fma_probe(int iters, float* out)
+{
+    float a0 = threadIdx.x * 1e-7f, a1 = a0 + 1e-7f, a2 = a0 + 2e-7f, a3 = a0 + 3e-7f;
+    float a4 = a0 + 4e-7f, a5 = a0 + 5e-7f, a6 = a0 + 6e-7f, a7 = a0 + 7e-7f;
+    const float m = 0.999999f, c = 1e-7f;
+    for (int i = 0; i < iters; i++)
+    {
+#pragma unroll
+        for (int k = 0; k < 16; k++)
+        {
+            a0 = __fmaf_rn(a0, m, c);
+            a1 = __fmaf_rn(a1, m, c);
+            a2 = __fmaf_rn(a2, m, c);
+            a3 = __fmaf_rn(a3, m, c);
+            a4 = __fmaf_rn(a4, m, c);
+            a5 = __fmaf_rn(a5, m, c);
+            a6 = __fmaf_rn(a6, m, c);
+            a7 = __fmaf_rn(a7, m, c);
+        }
+    }
+    float s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+    if (s == 12345.0f) out[blockIdx.x] = s;
+}
+
+}  // namespace
+}  // namespace spgnb
+
+using namespace spgnb;
+
+extern "C" {
+
+int spgnb_nl_count_pairs(spgnb_nl* nl, const spgnb_vector* d_crd, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
+                         float cutoff, long long* listed, long long* in_cutoff)
+{
+    if (!nl || !d_crd) return fail(SPGNB_E_ARG, "spgnb_nl_count_pairs: NULL argument");
+    if (!nl->built) return fail(SPGNB_E_STATE, "spgnb_nl_count_pairs: list never built");
+    unsigned long long* d = nullptr;
+    int st = dalloc(&d, 2);
+    if (st) return st;
+    cudaStream_t s = stream();
+    cudaMemsetAsync(d, 0, 16, s);
+    k_count_pairs<<<num_sms() * 8, 128, 0, s>>>(nl->d_counters, nl->items_cap, nl->d_items, nl->d_ents, nl->d_cl_u,
+                                                nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_d0, (const float3*)d_crd,
+                                                make_cell(cell), make_cell(rcell), cutoff * cutoff, d);
+    cudaError_t e = cudaGetLastError();
+    unsigned long long h[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, 16, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaFree(d);
+    if (e != cudaSuccess) return cuda_fail(e, "spgnb_nl_count_pairs");
+    if (listed) *listed = (long long)h[0];
+    if (in_cutoff) *in_cutoff = (long long)h[1];
+    return SPGNB_OK;
+}
+
+int spgnb_probe_fp32_fma_tflops(int repeats, double* tflops)
+{
+    if (!tflops) return fail(SPGNB_E_ARG, "spgnb_probe_fp32_fma_tflops: NULL output");
+    const int blocks = num_sms() * 8, threads = 256, iters = 4096;
+    float* out = nullptr;
+    int st = dalloc(&out, blocks);
+    if (st) return st;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    cudaStream_t s = stream();
+    k_fma_probe<<<blocks, threads, 0, s>>>(iters, out);  // warm-up
+    float best = 1e30f;
+    for (int r = 0; r < std::max(1, repeats); r++)
+    {
+        cudaEventRecord(a, s);
+        k_fma_probe<<<blocks, threads, 0, s>>>(iters, out);
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        best = std::min(best, ms);
+    }
+    cudaError_t e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(out);
+    if (e != cudaSuccess) return cuda_fail(e, "spgnb_probe_fp32_fma_tflops");
+    double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return SPGNB_OK;
+}
+
+}  // extern "C"

@@ -809,6 +809,9 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     }
     const size_t smem = sizeof(float2) * lj->n_types * lj->n_types;
     const int blocks = num_sms() * 4;
+    cudaEvent_t ev0, ev1;
+    pair_events(&ev0, &ev1);
+    if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
     if (mode == 0)
         k_pair_clusters<0><<<blocks, kPairWarps * 32, smem, s>>>(pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents,
                                                                  nl->d_cl_u, nl->d_slot_atom, lj->d_pos,
@@ -828,6 +831,7 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
                                                                  lj->d_totals, om, pa, nl->items_cap);
     }
     SPGNB_CHECK_LAUNCH("k_pair_clusters");
+    if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
     k_finalize<<<(local_atom_numbers + 255) / 256, 256, 0, s>>>(local_atom_numbers, lj->d_frc_acc, (float3*)d_frc);
     SPGNB_CHECK_LAUNCH("k_finalize");
     lj->have_energy = need_atom_energy != 0;

@@ -11,7 +11,24 @@ namespace
 {
 thread_local char g_last_error[1024] = "";
 thread_local cudaStream_t g_stream = nullptr;
+thread_local cudaEvent_t g_pair_start = nullptr, g_pair_stop = nullptr;
+unsigned long long g_launches = 0;
 }  // namespace
+
+void count_launch() { __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAXED); }
+
+void pair_events(cudaEvent_t* start, cudaEvent_t* stop)
+{
+    *start = g_pair_start;
+    *stop = g_pair_stop;
+}
+
+unsigned long long launches() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
+void set_pair_events(cudaEvent_t a, cudaEvent_t b)
+{
+    g_pair_start = a;
+    g_pair_stop = b;
+}
 
 int fail(int status, const char* fmt, ...)
 {
@@ -76,6 +93,14 @@ const char* spgnb_status_string(int status)
 }
 
 const char* spgnb_last_error(void) { return spgnb::g_last_error; }
+
+unsigned long long spgnb_launch_count(void) { return spgnb::launches(); }
+
+int spgnb_debug_set_pair_events(void* start_event, void* stop_event)
+{
+    spgnb::set_pair_events((cudaEvent_t)start_event, (cudaEvent_t)stop_event);
+    return SPGNB_OK;
+}
 
 int spgnb_set_stream(void* cuda_stream)
 {

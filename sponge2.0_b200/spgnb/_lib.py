@@ -25,6 +25,7 @@ EXPORTED = [
     "spgnb_lj_long_range_correction", "spgnb_lj_energies", "spgnb_lj_totals", "spgnb_lj_long_range_factor",
     "spgnb_lj_destroy",
     "spgnb_solvent_create", "spgnb_solvent_get_local", "spgnb_solvent_pme_direct_force", "spgnb_solvent_destroy",
+    "spgnb_launch_count", "spgnb_debug_set_pair_events", "spgnb_nl_count_pairs", "spgnb_probe_fp32_fma_tflops",
 ]
 
 
@@ -100,6 +101,10 @@ def lib():
     L.spgnb_solvent_get_local.argtypes = [vp, i, vp, i, vp, C.POINTER(i)]
     L.spgnb_solvent_pme_direct_force.argtypes = [vp, i, i, vp, vp, vp, vp, M, M, vp, vp, f, i, vp, i, vp, vp]
     L.spgnb_solvent_destroy.argtypes = [vp]
+    L.spgnb_launch_count.restype = C.c_ulonglong
+    L.spgnb_debug_set_pair_events.argtypes = [vp, vp]
+    L.spgnb_nl_count_pairs.argtypes = [vp, vp, M, M, f, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    L.spgnb_probe_fp32_fma_tflops.argtypes = [i, C.POINTER(d)]
     _lib = L
     return L
 
