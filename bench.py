@@ -44,6 +44,8 @@ def parse():
                    help="fev: force + energy + virial every step; f: force only")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
+    p.add_argument("--profile", action="store_true",
+                   help="profiling run for ncu: warm-up and --steps plain steps, no L2 flush, no e2e, no baseline")
     return p.parse_args()
 
 
@@ -151,6 +153,10 @@ def run_reference_arm(args, world, rank):
 def main():
     args = parse()
     world, rank, local = dist_setup()
+    if args.impl == "reference":
+        # the reference arm is the reference's CPU path: rank 0 alone, no GPU work
+        run_reference_arm(args, world, rank)
+        return
     import torch
     dist = None
     if world > 1:
@@ -159,12 +165,6 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    if args.impl == "reference":
-        run_reference_arm(args, world, rank)
-        if dist is not None:
-            dist.destroy_process_group()
-        return
-
     from spgnb import systems as S
     from spgnb._lib import lib
     from spgnb.engine import PlainPath
@@ -187,6 +187,15 @@ def main():
     for k in range(args.warmup):
         step(k)
     torch.cuda.synchronize()
+    if args.profile:
+        for k in range(args.steps):
+            step(args.warmup + k)
+        torch.cuda.synchronize()
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "steps": args.steps, "warmup": args.warmup, "atoms": s.n}))
+        if dist is not None:
+            dist.destroy_process_group()
+        return
 
     # algorithmic work of one pair-kernel launch (convention: 20 FLOP per
     # listed pair, 45 per pair inside rc, +22 with energy and virial)
