@@ -223,6 +223,16 @@ int spgnb_lj_totals(spgnb_lj* lj, double out[8]);
 /* Long-range factor computed at creation (host value). */
 double spgnb_lj_long_range_factor(const spgnb_lj* lj);
 
+/* The module's per-atom LJ energy array (LENNARD_JONES_INFORMATION::
+ * d_LJ_energy_atom, Lennard_Jones_force.h:111), filled on energy steps. */
+int spgnb_lj_atom_lj_energy(spgnb_lj* lj, float** d_atom_lj_energy);
+
+/* Writes n packed {x, y, z, LJ type, charge} records, the VECTOR_LJ layout of
+ * Lennard_Jones_force.h:13-17 that other modules read as
+ * crd_with_LJ_parameters_local (Copy_Crd_And_Charge_To_New_Crd, :17-27). */
+int spgnb_lj_export_vector_lj(spgnb_lj* lj, const spgnb_vector* d_crd, const float* d_charge, void* d_vector_lj,
+                              int n);
+
 int spgnb_lj_destroy(spgnb_lj* lj);
 
 /* --------------------------------------------------- SOLVENT_LENNARD_JONES */

@@ -131,8 +131,9 @@ def _result(frc, elj, ec, vir, tot, npairs):
 class Reference:
     """The reference's own implementation of the path (CPU or CUDA build)."""
 
-    def __init__(self, gpu=False):
-        lib = _load(os.path.join("_ref", "libspgref_cuda.so" if gpu else "libspgref_cpu.so"))
+    def __init__(self, gpu=False, shim=False):
+        name = "libspgref_shim.so" if shim else ("libspgref_cuda.so" if gpu else "libspgref_cpu.so")
+        lib = _load(os.path.join("_ref", name))
         lib.ref_init.argtypes = [C.c_int, C.c_int, _i32p, _f32p, _f32p, C.c_float, C.c_float, _f32p, _f32p,
                                  C.c_int, C.c_int, _i32p, _i32p, _i32p, C.c_int]
         lib.ref_nl_update.argtypes = [_f32p, C.c_int, C.c_int]
@@ -149,6 +150,7 @@ class Reference:
         lib.ref_set_threads.argtypes = [C.c_int]
         self.lib = lib
         self.gpu = bool(lib.ref_is_gpu())
+        self.shim = shim
         self.s = None
 
     def set_threads(self, t):
@@ -163,7 +165,7 @@ class Reference:
         if solvent:
             first_res = len(s.res_start) - s.n_waters
             rc = self.lib.ref_enable_solvent(len(s.res_start), _ci32(s.res_start), first_res, 3 * s.n_waters)
-            if rc != 0:
+            if rc != 0 and not self.shim:
                 raise RuntimeError("the solvent module exists only in the reference's GPU build")
 
     def nl_update(self, crd=None, step=0, forced=True):

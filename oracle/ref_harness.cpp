@@ -216,8 +216,9 @@ long long ref_nl_get(int* counts, int* lists, long long capacity, int* overflow_
     }
     if (overflow_flags)
     {
-        to_host(&overflow_flags[0], S.nl->d_neighbor_list_overflow, 1);
-        to_host(&overflow_flags[1], S.nl->d_neighbor_grid_overflow, 1);
+        overflow_flags[0] = overflow_flags[1] = 0;
+        if (S.nl->d_neighbor_list_overflow) to_host(&overflow_flags[0], S.nl->d_neighbor_list_overflow, 1);
+        if (S.nl->d_neighbor_grid_overflow) to_host(&overflow_flags[1], S.nl->d_neighbor_grid_overflow, 1);
     }
     return total;
 }
@@ -228,7 +229,7 @@ long long ref_nl_get(int* counts, int* lists, long long capacity, int* overflow_
 // the module on CPU builds (solvent_LJ.cpp:183-185).
 int ref_enable_solvent(int res_numbers, const int* res_start, int first_water_residue, int solvent_atoms)
 {
-#ifdef USE_GPU
+#if defined(USE_GPU) && !defined(REF_HARNESS_SHIM)
     S.lj_soft = new LJ_SOFT_CORE();
     S.slj = new SOLVENT_LENNARD_JONES();
     S.slj->lj_info = S.lj;

@@ -382,6 +382,21 @@ __global__ void k_finalize(int n, long long* __restrict__ acc, float3* __restric
     }
 }
 
+// 20-byte {float3 crd; int type; float charge} records
+__global__ void k_vector_lj(int n, const float3* __restrict__ crd, const float* __restrict__ charge,
+                            const int* __restrict__ local_type, float* __restrict__ out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 c = crd[i];
+    float* o = out + 5 * (size_t)i;
+    o[0] = c.x;
+    o[1] = c.y;
+    o[2] = c.z;
+    o[3] = __int_as_float(local_type[i]);
+    o[4] = charge[i];
+}
+
 __global__ void k_local_types(int n, const int* __restrict__ atom_local, const int* __restrict__ atom_type,
                               int* __restrict__ local_type)
 {
@@ -929,6 +944,26 @@ int spgnb_lj_energies(spgnb_lj* lj, double* lj_short, double* lj_long, double* l
 }
 
 double spgnb_lj_long_range_factor(const spgnb_lj* lj) { return lj ? lj->long_range_factor : 0.0; }
+
+int spgnb_lj_atom_lj_energy(spgnb_lj* lj, float** d_atom_lj_energy)
+{
+    if (!lj || !d_atom_lj_energy) return fail(SPGNB_E_ARG, "spgnb_lj_atom_lj_energy: NULL argument");
+    *d_atom_lj_energy = lj->d_lj_energy_atom;
+    return SPGNB_OK;
+}
+
+int spgnb_lj_export_vector_lj(spgnb_lj* lj, const spgnb_vector* d_crd, const float* d_charge, void* d_vector_lj,
+                              int n)
+{
+    if (!lj || !d_crd || !d_charge || !d_vector_lj) return fail(SPGNB_E_ARG, "spgnb_lj_export_vector_lj: NULL argument");
+    if (!lj->d_local_type) return fail(SPGNB_E_STATE, "spgnb_lj_export_vector_lj: Get_Local has not been called");
+    if (n <= 0) return SPGNB_OK;
+    if (n > lj->atom_numbers) return fail(SPGNB_E_ARG, "spgnb_lj_export_vector_lj: n exceeds the module's atoms");
+    k_vector_lj<<<(n + 255) / 256, 256, 0, stream()>>>(n, (const float3*)d_crd, d_charge, lj->d_local_type,
+                                                       (float*)d_vector_lj);
+    SPGNB_CHECK_LAUNCH("k_vector_lj");
+    return SPGNB_OK;
+}
 
 int spgnb_lj_destroy(spgnb_lj* lj)
 {
