@@ -147,8 +147,10 @@ struct spgnb_nl
     int* d_cl_cell = nullptr;
     uint4* d_cl_u = nullptr;      // fractional centre (2^32 per box vector), w = radius bits
     float4* d_cl_c = nullptr;     // Cartesian centre (wrapped frame), w = radius
+    int* d_atom_slot = nullptr;   // slot of each atom in the last build
     // cluster-pair list
-    int4* d_ents = nullptr;
+    int4* d_ents = nullptr;       // {j-cluster, flags, mask bits 0-31, mask bits 32-63}
+    float4* d_ents_d = nullptr;   // centre difference c_j - c_i (minimum image), Cartesian
     int4* d_items = nullptr;
     int* d_counters = nullptr;
     // reference-layout export
@@ -170,7 +172,9 @@ struct spgnb_lj
     const int* d_atom_local = nullptr;  // caller's local -> global map (Get_Local)
     float2* d_table = nullptr;       // T*T square table {A, B}
     float* d_lj_energy_atom = nullptr;
-    long long* d_frc_acc = nullptr;  // 4 x int64 per local atom
+    long long* d_frc_acc = nullptr;  // 4 x int64 per local atom (reference-layout path)
+    long long* d_slot_acc = nullptr; // 3 x slots_cap int64, SoA by slot (cluster path)
+    int slot_acc_cap = 0;
     long long* d_totals = nullptr;   // 8 x int64 fixed point
     float4* d_pos = nullptr;         // per slot (spgnb list) or per atom (atom-group path)
     int* d_pos_type = nullptr;

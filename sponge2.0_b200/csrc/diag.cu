@@ -13,7 +13,7 @@ namespace
 // Counts listed pairs (mask bits) and those inside the cutoff at the given
 // coordinates, reading the slots the last force call packed.
 __global__ void k_count_pairs(const int* __restrict__ counters, int items_cap, const int4* __restrict__ items,
-                              const int4* __restrict__ ents, const uint4* __restrict__ cl_u,
+                              const int4* __restrict__ ents, const float4* __restrict__ ents_d,
                               const int* __restrict__ slot_atom, const float4* __restrict__ x0,
                               const float4* __restrict__ d0, const float3* __restrict__ crd, Cell cell, Cell rcell,
                               float rc2, unsigned long long* out)
@@ -40,23 +40,19 @@ __global__ void k_count_pairs(const int* __restrict__ counters, int items_cap, c
     for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += total_warps)
     {
         int4 item = items[it];
-        uint4 ui = cl_u[item.x];
         for (int e = item.y; e < item.y + item.z; e++)
         {
             int4 en = ents[e];
-            uint4 uj = cl_u[en.x];
-            const float s32 = 2.3283064365386963e-10f;
-            float fx = (float)(int)(uj.x - ui.x) * s32, fy = (float)(int)(uj.y - ui.y) * s32,
-                  fz = (float)(int)(uj.z - ui.z) * s32;
+            float4 D = ents_d[e];
             float3 pj = pos(en.x * kClusterSize + jl);
             for (int h = 0; h < 2; h++)
             {
                 unsigned m = (unsigned)(h ? en.w : en.z);
                 if (!((m >> lane) & 1u)) continue;
                 float3 pi = pos(item.x * kClusterSize + row + 4 * h);
-                float dx = fx * cell.a11 + fy * cell.a21 + fz * cell.a31 + pj.x - pi.x;
-                float dy = fy * cell.a22 + fz * cell.a32 + pj.y - pi.y;
-                float dz = fz * cell.a33 + pj.z - pi.z;
+                float dx = D.x + pj.x - pi.x;
+                float dy = D.y + pj.y - pi.y;
+                float dz = D.z + pj.z - pi.z;
                 float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
                 float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
                 float sz = rintf(dz * rcell.a33);
@@ -123,7 +119,7 @@ int spgnb_nl_count_pairs(spgnb_nl* nl, const spgnb_vector* d_crd, spgnb_ltmatrix
     if (st) return st;
     cudaStream_t s = stream();
     cudaMemsetAsync(d, 0, 16, s);
-    k_count_pairs<<<num_sms() * 8, 128, 0, s>>>(nl->d_counters, nl->items_cap, nl->d_items, nl->d_ents, nl->d_cl_u,
+    k_count_pairs<<<num_sms() * 8, 128, 0, s>>>(nl->d_counters, nl->items_cap, nl->d_items, nl->d_ents, nl->d_ents_d,
                                                 nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_d0, (const float3*)d_crd,
                                                 make_cell(cell), make_cell(rcell), cutoff * cutoff, d);
     cudaError_t e = cudaGetLastError();

@@ -217,8 +217,8 @@ __device__ __forceinline__ unsigned spread3(unsigned v)
 // index, so clusters are spatially compact and the build reproducible.
 __global__ void k_sort_cells(Grid g, const int* __restrict__ cell_count, const int* __restrict__ cell_cl_start,
                              const int* __restrict__ tmp_atoms, const float4* __restrict__ wrapped,
-                             int* __restrict__ slot_atom, int* __restrict__ cl_cell, int slots_cap,
-                             const int* __restrict__ counters)
+                             int* __restrict__ slot_atom, int* __restrict__ cl_cell, int* __restrict__ atom_slot,
+                             int slots_cap, const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
     extern __shared__ unsigned long long keys[];
@@ -249,7 +249,9 @@ __global__ void k_sort_cells(Grid g, const int* __restrict__ cell_count, const i
                 unsigned long long k = keys[e];
                 int r = 0;
                 for (int f = 0; f < n; f++) r += keys[f] < k;
-                slot_atom[base + r] = (int)(k & 0xffffffffu);
+                const int a = (int)(k & 0xffffffffu);
+                slot_atom[base + r] = a;
+                atom_slot[a] = base + r;
             }
             else
             {
@@ -265,9 +267,9 @@ __global__ void k_sort_cells(Grid g, const int* __restrict__ cell_count, const i
 // radius, fractional fixed-point centre, per-slot offsets and build
 // coordinates.  Eight lanes per cluster.
 __global__ void k_cluster_props(const float3* __restrict__ crd, const int* __restrict__ slot_atom,
-                                const int* __restrict__ atom_shift, Cell cell, int* counters, uint4* __restrict__ cl_u,
-                                float4* __restrict__ cl_c, float4* __restrict__ slot_x0, float4* __restrict__ slot_d0,
-                                int clusters_cap)
+                                const int* __restrict__ atom_shift, const int* __restrict__ atom_local, Cell cell,
+                                int* counters, uint4* __restrict__ cl_u, float4* __restrict__ cl_c,
+                                float4* __restrict__ slot_x0, float4* __restrict__ slot_d0, int clusters_cap)
 {
     if (counters[kCntNeed] == 0) return;
     int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -326,13 +328,14 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, const int* __res
         double d0 = w[0] - cq[0], d1 = w[1] - cq[1], d2 = w[2] - cq[2];
         r2 = d0 * d0 + d1 * d1 + d2 * d2;
         slot_d0[s] = make_float4((float)d0, (float)d1, (float)d2, 0.0f);
-        slot_x0[s] = make_float4(x.x, x.y, x.z, 0.0f);
+        // raw build coordinates, w = the atom's global index (-1: padding)
+        slot_x0[s] = make_float4(x.x, x.y, x.z, __int_as_float(atom_local[a]));
     }
     else if (live)
     {
         float p = kPadCoordinate + (float)s;
         slot_d0[s] = make_float4(p, p, p, 0.0f);
-        slot_x0[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        slot_x0[s] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
     }
     for (int o = 1; o < 8; o <<= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
     if (live && l8 == 0)
@@ -387,12 +390,12 @@ constexpr int kSearchWarps = 4;
 __global__ void __launch_bounds__(kSearchWarps * 32)
     k_search(SearchParams p, const int* __restrict__ cand_start, const int* __restrict__ cand,
              const int* __restrict__ cell_cl_start, const int* __restrict__ cl_cell, const uint4* __restrict__ cl_u,
-             const int* __restrict__ slot_atom, const float3* __restrict__ crd, const int* __restrict__ atom_local,
-             const int* __restrict__ ex_start, const int* __restrict__ ex_list, const int* __restrict__ ex_num,
-             int4* __restrict__ ents, int4* __restrict__ items, int* counters)
+             const float4* __restrict__ slot_x0, const int* __restrict__ ex_start, const int* __restrict__ ex_list, const int* __restrict__ ex_num,
+             int4* __restrict__ ents, float4* __restrict__ ents_d, int4* __restrict__ items, int* counters)
 {
     if (counters[kCntNeed] == 0) return;
     __shared__ int4 stage[kSearchWarps][kChunk];
+    __shared__ float4 stage_d[kSearchWarps][kChunk];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int nc = counters[kCntClusters];
@@ -405,14 +408,14 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
         const uint4 ui = cl_u[ci];
         const float ri = __uint_as_float(ui.w);
         // the two i-atoms this lane tests (rounds h = 0, 1)
-        int ia[2], ga[2];
+        int ga[2];
         float3 xa[2];
         for (int h = 0; h < 2; h++)
         {
-            int a = h * 4 + (lane >> 3);
-            ia[h] = slot_atom[ci * kClusterSize + a];
-            ga[h] = ia[h] >= 0 ? atom_local[ia[h]] : 0;
-            xa[h] = ia[h] >= 0 ? crd[ia[h]] : make_float3(0, 0, 0);
+            const int a = h * 4 + (lane >> 3);
+            const float4 x = slot_x0[ci * kClusterSize + a];
+            ga[h] = __float_as_int(x.w);
+            xa[h] = make_float3(x.x, x.y, x.z);
         }
         int staged = 0;
         auto flush = [&](int count) {
@@ -427,7 +430,11 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
             e0 = __shfl_sync(0xffffffffu, e0, 0);
             it = __shfl_sync(0xffffffffu, it, 0);
             const bool ok = (e0 + count <= p.entries_cap) && (it < p.items_cap);
-            if (ok && lane < count) ents[e0 + lane] = stage[wib][lane];
+            if (ok && lane < count)
+            {
+                ents[e0 + lane] = stage[wib][lane];
+                ents_d[e0 + lane] = stage_d[wib][lane];
+            }
             // an item slot that exists is always written, empty when its
             // entries did not fit, so readers never see a stale range
             if (lane == 0 && it < p.items_cap) items[it] = make_int4(ci, ok ? (int)e0 : 0, ok ? count : 0, 0);
@@ -476,14 +483,14 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
                     surv &= surv - 1;
                     const int cjs = b0 + src;
                     const int b = lane & 7;
-                    const int jb = slot_atom[cjs * kClusterSize + b];
-                    const int gb = jb >= 0 ? atom_local[jb] : 0;
-                    const float3 xb = jb >= 0 ? crd[jb] : make_float3(0, 0, 0);
+                    const float4 xj = slot_x0[cjs * kClusterSize + b];
+                    const int gb = __float_as_int(xj.w);
+                    const float3 xb = make_float3(xj.x, xj.y, xj.z);
                     unsigned bits[2];
                     for (int h = 0; h < 2; h++)
                     {
                         const int a = h * 4 + (lane >> 3);
-                        bool in = ia[h] >= 0 && jb >= 0 && (cjs != ci || b > a);
+                        bool in = ga[h] >= 0 && gb >= 0 && (cjs != ci || b > a);
                         if (in)
                         {
                             const bool a_lo = ga[h] < gb;
@@ -511,8 +518,18 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
                                     fabsf(f.y) + rr * p.frac_norm[1] < 0.49f &&
                                     fabsf(f.z) + rr * p.frac_norm[2] < 0.49f;
                         if (lane == 0)
+                        {
                             stage[wib][staged] =
                                 make_int4(cjs, safe ? 0 : kEntPairImage, (int)bits[0], (int)bits[1]);
+                            // centre difference from the quantised centres, in double
+                            const double q = 2.3283064365386963e-10;
+                            const double fx = (double)(int)(uj.x - ui.x) * q, fy = (double)(int)(uj.y - ui.y) * q,
+                                         fz = (double)(int)(uj.z - ui.z) * q;
+                            const Cell& c = p.g.cell;
+                            stage_d[wib][staged] = make_float4(
+                                (float)(fx * (double)c.a11 + fy * (double)c.a21 + fz * (double)c.a31),
+                                (float)(fy * (double)c.a22 + fz * (double)c.a32), (float)(fz * (double)c.a33), 0.0f);
+                        }
                         staged++;
                         __syncwarp();
                         if (staged == kChunk)
@@ -709,8 +726,10 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_cl_u);
     dfree(nl->d_cl_c);
     dfree(nl->d_ents);
+    dfree(nl->d_ents_d);
     dfree(nl->d_items);
     dfree(nl->d_counters);
+    dfree(nl->d_atom_slot);
     dfree(nl->d_nl);
     dfree(nl->d_temp);
     dfree(nl->d_wrapped);
@@ -720,10 +739,12 @@ int alloc_pair_list(spgnb_nl* nl)
 {
     int st;
     dfree(nl->d_ents);
+    dfree(nl->d_ents_d);
     dfree(nl->d_items);
     nl->entries_cap = (long long)nl->clusters_cap * nl->entries_per_cluster;
     nl->items_cap = (int)std::min<long long>(nl->entries_cap / kChunk + nl->clusters_cap + 1024, 0x7fffffffLL);
     if ((st = dalloc(&nl->d_ents, (size_t)nl->entries_cap))) return st;
+    if ((st = dalloc(&nl->d_ents_d, (size_t)nl->entries_cap))) return st;
     if ((st = dalloc(&nl->d_items, (size_t)nl->items_cap))) return st;
     return SPGNB_OK;
 }
@@ -749,6 +770,8 @@ int alloc_nl(spgnb_nl* nl)
     if ((st = dalloc(&nl->d_atom_cell, n))) return st;
     if ((st = dalloc(&nl->d_atom_shift, n))) return st;
     if ((st = dalloc(&nl->d_wrapped, n))) return st;
+    if ((st = dalloc(&nl->d_atom_slot, n))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_atom_slot, 0xff, sizeof(int) * n));
     if ((st = dalloc(&nl->d_tmp_atoms, slots))) return st;
     if ((st = dalloc(&nl->d_slot_atom, slots))) return st;
     if ((st = dalloc(&nl->d_slot_x0, slots))) return st;
@@ -911,10 +934,11 @@ int spgnb_nl_update(spgnb_nl* nl, const int* d_atom_local, int local_atom_number
     int sort_blocks = std::min(nl->G, num_sms() * 16);
     k_sort_cells<<<sort_blocks, 128, 2048 * sizeof(unsigned long long), s>>>(
         g, nl->d_cell_count, nl->d_cell_cl_start, nl->d_tmp_atoms, nl->d_wrapped, nl->d_slot_atom,
-        nl->d_cl_cell, slots_cap, nl->d_counters);
+        nl->d_cl_cell, nl->d_atom_slot, slots_cap, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_sort_cells");
     k_cluster_props<<<(slots_cap + 255) / 256, 256, 0, s>>>((const float3*)d_crd, nl->d_slot_atom,
-                                                             nl->d_atom_shift, c, nl->d_counters, nl->d_cl_u,
+                                                             nl->d_atom_shift, d_atom_local, c, nl->d_counters,
+                                                             nl->d_cl_u,
                                                              nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0,
                                                              nl->clusters_cap);
     SPGNB_CHECK_LAUNCH("k_cluster_props");
@@ -930,9 +954,9 @@ int spgnb_nl_update(spgnb_nl* nl, const int* d_atom_local, int local_atom_number
     sp.clusters_cap = nl->clusters_cap;
     int search_blocks = std::min((nl->clusters_cap + kSearchWarps - 1) / kSearchWarps, num_sms() * 8);
     k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
-        sp, nl->d_cand_start, nl->d_cand, nl->d_cell_cl_start, nl->d_cl_cell, nl->d_cl_u, nl->d_slot_atom,
-        (const float3*)d_crd, d_atom_local, d_excluded_list_start, d_excluded_list, d_excluded_numbers,
-        nl->d_ents, nl->d_items, nl->d_counters);
+        sp, nl->d_cand_start, nl->d_cand, nl->d_cell_cl_start, nl->d_cl_cell, nl->d_cl_u, nl->d_slot_x0,
+        d_excluded_list_start, d_excluded_list, d_excluded_numbers,
+        nl->d_ents, nl->d_ents_d, nl->d_items, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_search");
     if (nl->opt.export_atom_groups)
     {

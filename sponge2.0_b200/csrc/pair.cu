@@ -84,12 +84,6 @@ __device__ __forceinline__ void red_fixed(long long* acc, float v)
     if (q != 0) atomicAdd((unsigned long long*)acc, (unsigned long long)q);
 }
 
-__device__ __forceinline__ float3 frac_delta(uint4 ui, uint4 uj)
-{
-    const float s = 2.3283064365386963e-10f;  // 2^-32
-    return make_float3((float)(int)(uj.x - ui.x) * s, (float)(int)(uj.y - ui.y) * s, (float)(int)(uj.z - ui.z) * s);
-}
-
 struct OwnerMap
 {
     const int* atom_local;   // global index of each local atom
@@ -141,14 +135,44 @@ __global__ void k_pack_slots(int slots_cap, const int* __restrict__ counters, co
     ptype[s] = local_type[a];
 }
 
-// MODE 0: forces.  MODE 1: + energy/virial totals.  MODE 2: + per-atom
-// energy and virial arrays.
+// Symmetrised virial increment -(f (x) d) in the LTMatrix3 order a11, a21,
+// a22, a31, a32, a33 (Get_Virial_From_Force_Dis, vector.hpp:336-347).
+__device__ __forceinline__ void add_outer(float* v, float fx, float fy, float fz, float dx, float dy, float dz,
+                                          float sign)
+{
+    v[0] = __fmaf_rn(sign * fx, dx, v[0]);
+    v[1] = __fmaf_rn(sign * fx, dy, __fmaf_rn(sign * fy, dx, v[1]));
+    v[2] = __fmaf_rn(sign * fy, dy, v[2]);
+    v[3] = __fmaf_rn(sign * fx, dz, __fmaf_rn(sign * fz, dx, v[3]));
+    v[4] = __fmaf_rn(sign * fy, dz, __fmaf_rn(sign * fz, dy, v[4]));
+    v[5] = __fmaf_rn(sign * fz, dz, v[5]);
+}
+
+struct SlotAcc
+{
+    long long* x;
+    long long* y;
+    long long* z;
+};
+
+// Cluster-pair force kernel.  A warp takes one work item (an i-cluster and
+// up to kChunk j-clusters); lane (row = lane/8, j = lane%8) evaluates pairs
+// (i = row and row + 4, j) of each 8 x 8 entry.  j forces are summed over the
+// four rows by shuffles and added once per atom and entry (int64 fixed
+// point, slot-ordered, so eight lanes write two sectors); i forces stay in
+// registers for the whole item.
+//
+// MODE 0: forces.  MODE 1: + energy and virial totals; the virial is taken
+// as sum_entries D (x) F_j + sum_atoms delta (x) F (the second part in the
+// finalize kernel), D the entry's centre difference, which needs no per-pair
+// outer product.  MODE 2: + per-atom energy/virial arrays owned by the
+// pair's lower-index atom, per pair.
 template <int MODE>
 __global__ void __launch_bounds__(kPairWarps * 32)
     k_pair_clusters(PairConst pc, Cell cell, Cell rcell, const int* __restrict__ counters,
-                    const int4* __restrict__ items, const int4* __restrict__ ents, const uint4* __restrict__ cl_u,
+                    const int4* __restrict__ items, const int4* __restrict__ ents, const float4* __restrict__ ents_d,
                     const int* __restrict__ slot_atom, const float4* __restrict__ pos,
-                    const int* __restrict__ ptype, const float2* __restrict__ gtable, long long* __restrict__ acc,
+                    const int* __restrict__ ptype, const float2* __restrict__ gtable, SlotAcc acc,
                     long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, int items_cap)
 {
     extern __shared__ float2 table[];
@@ -172,7 +196,6 @@ __global__ void __launch_bounds__(kPairWarps * 32)
         const float4 pi1 = pos[ci * kClusterSize + row + 4];
         const int ti0 = ptype[ci * kClusterSize + row] * pc.n_types;
         const int ti1 = ptype[ci * kClusterSize + row + 4] * pc.n_types;
-        const uint4 ui = cl_u[ci];
         int ai0 = 0, ai1 = 0, gi0 = 0, gi1 = 0;
         if (PA)
         {
@@ -188,23 +211,39 @@ __global__ void __launch_bounds__(kPairWarps * 32)
             for (int h = 0; h < 2; h++)
                 for (int q = 0; q < 8; q++) pai[h][q] = 0.0f;
 
-        for (int e = item.y; e < item.y + item.z; e++)
+        const int e_end = item.y + item.z;
+        int4 en_n = make_int4(0, 0, 0, 0);
+        float4 ed_n = make_float4(0, 0, 0, 0), pj_n = make_float4(0, 0, 0, 0);
+        int tj_n = 0;
+        if (item.z > 0)
         {
-            const int4 en = ents[e];
+            en_n = ents[item.y];
+            ed_n = ents_d[item.y];
+            pj_n = pos[en_n.x * kClusterSize + jl];
+            tj_n = ptype[en_n.x * kClusterSize + jl];
+        }
+        for (int e = item.y; e < e_end; e++)
+        {
+            const int4 en = en_n;
+            const float4 ed = ed_n;
+            const float4 pj = pj_n;
+            const int tj = tj_n;
+            if (e + 1 < e_end)
+            {
+                en_n = ents[e + 1];
+                ed_n = ents_d[e + 1];
+                pj_n = pos[en_n.x * kClusterSize + jl];
+                tj_n = ptype[en_n.x * kClusterSize + jl];
+            }
             const int cj = en.x;
-            const float4 pj = pos[cj * kClusterSize + jl];
-            const int tj = ptype[cj * kClusterSize + jl];
-            const uint4 uj = cl_u[cj];
-            const float3 f = frac_delta(ui, uj);
-            const float px = f.x * cell.a11 + f.y * cell.a21 + f.z * cell.a31 + pj.x;
-            const float py = f.y * cell.a22 + f.z * cell.a32 + pj.y;
-            const float pz = f.z * cell.a33 + pj.z;
+            const float px = ed.x + pj.x, py = ed.y + pj.y, pz = ed.z + pj.z;
             int aj = 0, gj = 0;
             if (PA)
             {
                 aj = slot_atom[cj * kClusterSize + jl];
                 gj = aj >= 0 ? om.atom_local[aj] : 0;
             }
+            const bool pair_image = (en.y & kEntPairImage) != 0;
             float fjx = 0, fjy = 0, fjz = 0;
             float paj[8];
             if (PA)
@@ -216,14 +255,18 @@ __global__ void __launch_bounds__(kPairWarps * 32)
                 if (m == 0) continue;
                 const float4 pi = h ? pi1 : pi0;
                 float dx = px - pi.x, dy = py - pi.y, dz = pz - pi.z;
-                if (en.y & kEntPairImage)
+                float tx = 0, ty = 0, tz = 0;
+                if (pair_image)
                 {
                     const float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
                     const float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
                     const float sz = rintf(dz * rcell.a33);
-                    dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
-                    dy -= sy * cell.a22 + sz * cell.a32;
-                    dz -= sz * cell.a33;
+                    tx = -(sx * cell.a11 + sy * cell.a21 + sz * cell.a31);
+                    ty = -(sy * cell.a22 + sz * cell.a32);
+                    tz = -(sz * cell.a33);
+                    dx += tx;
+                    dy += ty;
+                    dz += tz;
                 }
                 const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
                 const bool in = ((m >> lane) & 1u) && r2 < pc.rc2;
@@ -249,22 +292,30 @@ __global__ void __launch_bounds__(kPairWarps * 32)
                 fjz -= fz;
                 if (EN)
                 {
-                    elj = in ? elj : 0.0f;
-                    ec = in ? ec : 0.0f;
-                    float v[6] = {-fx * dx, -(fx * dy + fy * dx), -fy * dy, -(fx * dz + fz * dx),
-                                  -(fy * dz + fz * dy), -fz * dz};
-                    tot[0] += elj;
-                    tot[1] += ec;
-                    for (int q = 0; q < 6; q++) tot[2 + q] += v[q];
+                    tot[0] += in ? elj : 0.0f;
+                    tot[1] += in ? ec : 0.0f;
                     if (PA)
                     {
+                        float v[6] = {0, 0, 0, 0, 0, 0};
+                        add_outer(v, fx, fy, fz, dx, dy, dz, -1.0f);
+                        for (int q = 0; q < 6; q++) tot[2 + q] += v[q];
                         const bool i_owns = (h ? gi1 : gi0) < gj;
                         float* dst = i_owns ? pai[h] : paj;
-                        dst[0] += elj;
-                        dst[1] += ec;
+                        dst[0] += in ? elj : 0.0f;
+                        dst[1] += in ? ec : 0.0f;
                         for (int q = 0; q < 6; q++) dst[2 + q] += v[q];
                     }
+                    else if (pair_image)
+                    {
+                        // the lattice shift this pair took beyond the entry's image
+                        add_outer(tot + 2, fx, fy, fz, tx, ty, tz, -1.0f);
+                    }
                 }
+            }
+            if (EN && !PA)
+            {
+                // -(f (x) D) summed over this lane's pairs: f_j accumulated -f
+                add_outer(tot + 2, fjx, fjy, fjz, ed.x, ed.y, ed.z, 1.0f);
             }
             // j forces: sum over the four rows, one fixed-point add per atom
             fjx += __shfl_xor_sync(0xffffffffu, fjx, 8);
@@ -283,21 +334,18 @@ __global__ void __launch_bounds__(kPairWarps * 32)
             }
             if (row == 0)
             {
-                const int a = PA ? aj : slot_atom[cj * kClusterSize + jl];
-                if (a >= 0)
+                const int sj = cj * kClusterSize + jl;
+                red_fixed(acc.x + sj, fjx);
+                red_fixed(acc.y + sj, fjy);
+                red_fixed(acc.z + sj, fjz);
+                if (PA && aj >= 0)
                 {
-                    red_fixed(acc + 4 * (size_t)a + 0, fjx);
-                    red_fixed(acc + 4 * (size_t)a + 1, fjy);
-                    red_fixed(acc + 4 * (size_t)a + 2, fjz);
-                    if (PA)
-                    {
-                        const int o = om.remap(a);
-                        if (pa.energy) atomicAdd(pa.energy + o, paj[0] + paj[1]);
-                        if (pa.lj_energy) atomicAdd(pa.lj_energy + o, paj[0]);
-                        if (pa.direct) atomicAdd(pa.direct + o, paj[1]);
-                        if (pa.virial)
-                            for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)o + q, paj[2 + q]);
-                    }
+                    const int o = om.remap(aj);
+                    if (pa.energy) atomicAdd(pa.energy + o, paj[0] + paj[1]);
+                    if (pa.lj_energy) atomicAdd(pa.lj_energy + o, paj[0]);
+                    if (pa.direct) atomicAdd(pa.direct + o, paj[1]);
+                    if (pa.virial)
+                        for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)o + q, paj[2 + q]);
                 }
             }
         }
@@ -317,25 +365,18 @@ __global__ void __launch_bounds__(kPairWarps * 32)
         }
         if (jl == 0)
         {
-            const int a0 = PA ? ai0 : slot_atom[ci * kClusterSize + row];
-            const int a1 = PA ? ai1 : slot_atom[ci * kClusterSize + row + 4];
-            if (a0 >= 0)
-            {
-                red_fixed(acc + 4 * (size_t)a0 + 0, fi0x);
-                red_fixed(acc + 4 * (size_t)a0 + 1, fi0y);
-                red_fixed(acc + 4 * (size_t)a0 + 2, fi0z);
-            }
-            if (a1 >= 0)
-            {
-                red_fixed(acc + 4 * (size_t)a1 + 0, fi1x);
-                red_fixed(acc + 4 * (size_t)a1 + 1, fi1y);
-                red_fixed(acc + 4 * (size_t)a1 + 2, fi1z);
-            }
+            const int s0 = ci * kClusterSize + row, s1 = s0 + 4;
+            red_fixed(acc.x + s0, fi0x);
+            red_fixed(acc.y + s0, fi0y);
+            red_fixed(acc.z + s0, fi0z);
+            red_fixed(acc.x + s1, fi1x);
+            red_fixed(acc.y + s1, fi1y);
+            red_fixed(acc.z + s1, fi1z);
             if (PA)
             {
                 for (int h = 0; h < 2; h++)
                 {
-                    const int a = h ? a1 : a0;
+                    const int a = h ? ai1 : ai0;
                     if (a < 0) continue;
                     const int o = om.remap(a);
                     if (pa.energy) atomicAdd(pa.energy + o, pai[h][0] + pai[h][1]);
@@ -361,8 +402,76 @@ __global__ void __launch_bounds__(kPairWarps * 32)
     }
 }
 
-// Fixed point -> caller's float force (+=), accumulators cleared for the
-// next call.
+// Fixed point -> caller's float force (+=) for the cluster path, slot-indexed
+// accumulators cleared for the next call.  With virial totals it adds
+// sum_atoms F (x) delta, the per-atom half of the decomposition above.
+template <bool VIRIAL>
+__global__ void k_finalize_slots(int n, const int* __restrict__ atom_slot, int slots_cap, SlotAcc acc,
+                                 const float4* __restrict__ pos, float3* __restrict__ frc,
+                                 long long* __restrict__ totals)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    double v[6] = {0, 0, 0, 0, 0, 0};
+    if (i < n)
+    {
+        const int s = atom_slot[i];
+        if (s >= 0 && s < slots_cap)
+        {
+            const long long x = acc.x[s], y = acc.y[s], z = acc.z[s];
+            const double fx = (double)x * kForceUnscale, fy = (double)y * kForceUnscale,
+                         fz = (double)z * kForceUnscale;
+            if (x | y | z)
+            {
+                float3 f = frc[i];
+                f.x += (float)fx;
+                f.y += (float)fy;
+                f.z += (float)fz;
+                frc[i] = f;
+                acc.x[s] = 0;
+                acc.y[s] = 0;
+                acc.z[s] = 0;
+            }
+            if (VIRIAL)
+            {
+                const float4 d = pos[s];
+                v[0] = fx * d.x;
+                v[1] = fx * d.y + fy * d.x;
+                v[2] = fy * d.y;
+                v[3] = fx * d.z + fz * d.x;
+                v[4] = fy * d.z + fz * d.y;
+                v[5] = fz * d.z;
+            }
+        }
+    }
+    if (VIRIAL)
+    {
+        __shared__ double red[6][32];
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        for (int q = 0; q < 6; q++)
+        {
+            for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+            if (lane == 0) red[q][w] = v[q];
+        }
+        __syncthreads();
+        if (w == 0)
+        {
+            const int nw = blockDim.x >> 5;
+            for (int q = 0; q < 6; q++)
+            {
+                double t = lane < nw ? red[q][lane] : 0.0;
+                for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+                if (lane == 0)
+                {
+                    long long b = __double2ll_rn(t * kEnergyScale);
+                    if (b) atomicAdd((unsigned long long*)&totals[2 + q], (unsigned long long)b);
+                }
+            }
+        }
+    }
+}
+
+// Fixed point -> caller's float force (+=) for the reference-layout path,
+// accumulators cleared for the next call.
 __global__ void k_finalize(int n, long long* __restrict__ acc, float3* __restrict__ frc)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -671,6 +780,31 @@ int ensure_pos(spgnb_lj* lj, int count)
     return SPGNB_OK;
 }
 
+int ensure_slot_acc(spgnb_lj* lj, int slots)
+{
+    if (slots <= lj->slot_acc_cap) return SPGNB_OK;
+    dfree(lj->d_slot_acc);
+    int st = dalloc(&lj->d_slot_acc, 3 * (size_t)slots);
+    if (st) return st;
+    SPGNB_CUDA(cudaMemset(lj->d_slot_acc, 0, sizeof(long long) * 3 * (size_t)slots));
+    lj->slot_acc_cap = slots;
+    return SPGNB_OK;
+}
+
+// A persistent grid: as many blocks as can be resident on every SM.
+template <typename K>
+int pair_blocks(K kernel, size_t smem)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPairWarps * 32, smem) != cudaSuccess ||
+        per_sm <= 0)
+    {
+        cudaGetLastError();
+        per_sm = 4;
+    }
+    return per_sm * num_sms();
+}
+
 int check_common(spgnb_lj* lj, int local_atom_numbers, int ghost_numbers, const spgnb_vector* d_crd,
                  const float* d_charge, spgnb_vector* d_frc)
 {
@@ -822,33 +956,37 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
         pa.direct = need_atom_energy ? d_atom_direct_pme_energy : nullptr;
         pa.virial = need_virial ? (float*)d_atom_virial : nullptr;
     }
+    if ((st = ensure_slot_acc(lj, slots))) return st;
+    SlotAcc acc{lj->d_slot_acc, lj->d_slot_acc + lj->slot_acc_cap, lj->d_slot_acc + 2 * (size_t)lj->slot_acc_cap};
     const size_t smem = sizeof(float2) * lj->n_types * lj->n_types;
-    const int blocks = num_sms() * 4;
     cudaEvent_t ev0, ev1;
     pair_events(&ev0, &ev1);
     if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
     if (mode == 0)
-        k_pair_clusters<0><<<blocks, kPairWarps * 32, smem, s>>>(pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents,
-                                                                 nl->d_cl_u, nl->d_slot_atom, lj->d_pos,
-                                                                 lj->d_pos_type, lj->d_table, lj->d_frc_acc,
-                                                                 lj->d_totals, om, pa, nl->items_cap);
+        k_pair_clusters<0><<<pair_blocks(k_pair_clusters<0>, smem), kPairWarps * 32, smem, s>>>(
+            pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents, nl->d_ents_d, nl->d_slot_atom, lj->d_pos,
+            lj->d_pos_type, lj->d_table, acc, lj->d_totals, om, pa, nl->items_cap);
     else if (mode == 1)
-        k_pair_clusters<1><<<blocks, kPairWarps * 32, smem, s>>>(pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents,
-                                                                 nl->d_cl_u, nl->d_slot_atom, lj->d_pos,
-                                                                 lj->d_pos_type, lj->d_table, lj->d_frc_acc,
-                                                                 lj->d_totals, om, pa, nl->items_cap);
+        k_pair_clusters<1><<<pair_blocks(k_pair_clusters<1>, smem), kPairWarps * 32, smem, s>>>(
+            pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents, nl->d_ents_d, nl->d_slot_atom, lj->d_pos,
+            lj->d_pos_type, lj->d_table, acc, lj->d_totals, om, pa, nl->items_cap);
     else
     {
         om.atom_local = lj->d_atom_local;
-        k_pair_clusters<2><<<blocks, kPairWarps * 32, smem, s>>>(pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents,
-                                                                 nl->d_cl_u, nl->d_slot_atom, lj->d_pos,
-                                                                 lj->d_pos_type, lj->d_table, lj->d_frc_acc,
-                                                                 lj->d_totals, om, pa, nl->items_cap);
+        k_pair_clusters<2><<<pair_blocks(k_pair_clusters<2>, smem), kPairWarps * 32, smem, s>>>(
+            pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents, nl->d_ents_d, nl->d_slot_atom, lj->d_pos,
+            lj->d_pos_type, lj->d_table, acc, lj->d_totals, om, pa, nl->items_cap);
     }
     SPGNB_CHECK_LAUNCH("k_pair_clusters");
     if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
-    k_finalize<<<(local_atom_numbers + 255) / 256, 256, 0, s>>>(local_atom_numbers, lj->d_frc_acc, (float3*)d_frc);
-    SPGNB_CHECK_LAUNCH("k_finalize");
+    const int fb = (local_atom_numbers + 255) / 256;
+    if (mode == 1 && need_virial)
+        k_finalize_slots<true><<<fb, 256, 0, s>>>(local_atom_numbers, nl->d_atom_slot, slots, acc, lj->d_pos,
+                                                  (float3*)d_frc, lj->d_totals);
+    else
+        k_finalize_slots<false><<<fb, 256, 0, s>>>(local_atom_numbers, nl->d_atom_slot, slots, acc, lj->d_pos,
+                                                   (float3*)d_frc, lj->d_totals);
+    SPGNB_CHECK_LAUNCH("k_finalize_slots");
     lj->have_energy = need_atom_energy != 0;
     lj->have_virial = need_virial != 0;
     return SPGNB_OK;
@@ -973,6 +1111,7 @@ int spgnb_lj_destroy(spgnb_lj* lj)
     dfree(lj->d_table);
     dfree(lj->d_lj_energy_atom);
     dfree(lj->d_frc_acc);
+    dfree(lj->d_slot_acc);
     dfree(lj->d_totals);
     dfree(lj->d_pos);
     dfree(lj->d_pos_type);

@@ -269,3 +269,30 @@ def _record(group, key, values):
     data = json.load(open(path)) if os.path.exists(path) else {}
     data.setdefault(group, {})[key] = values
     json.dump(data, open(path, "w"), indent=1, sort_keys=True)
+
+
+REF_SHIM = os.path.join(ROOT, "oracle", "_ref", "libspgref_shim.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SHIM), reason="shim harness not built")
+@pytest.mark.parametrize("name", ["water-6480", "mixed-small"])
+def test_dropin_through_sponge_module_api(torch_cuda, oracle, name):
+    """SPONGE's own NEIGHBOR_LIST / LENNARD_JONES_INFORMATION calls (the
+    reference harness, unchanged) linked against the spgnb shim instead of the
+    reference's module sources: same neighbour set, forces, energies."""
+    import oracle as O
+    s = SYSTEMS[name]()
+    ref = O.Reference(shim=True)
+    ref.init(s, refresh_interval=20, solvent=True)
+    ref.nl_update(forced=True)
+    rc, rl, flags = ref.nl_get()
+    oc, ol = oracle.nl_build(s, mode=1)
+    assert np.array_equal(rc, oc) and np.array_equal(rl, ol)
+    r = ref.force(need_energy=True, need_virial=True)
+    fp64 = oracle.pair_force(s, oc, ol)
+    assert rel_rms(r["frc"], fp64["frc"]) <= FORCE_REL_RMS_TOL
+    assert abs(r["atom_lj"].astype(np.float64).sum() - fp64["e_lj"]) <= 1e-4 * abs(fp64["e_lj"])
+    vir = r["atom_virial"].astype(np.float64).sum(0)
+    assert np.abs(vir - fp64["virial"]).max() <= 1e-4 * np.abs(fp64["virial"]).max()
+    assert abs(ref.long_range_factor() - oracle.long_range_factor(s)) <= 1e-6 * abs(oracle.long_range_factor(s))
+    ref.clear()
