@@ -263,6 +263,31 @@ int spgnb_solvent_pme_direct_force(spgnb_solvent* s, int atom_numbers, int resid
 
 int spgnb_solvent_destroy(spgnb_solvent* s);
 
+/* ------------------------------------------------ no-allocation force call */
+/* No counterpart in the reference.  The force of
+ * spgnb_lj_pme_direct_force_atom_groups (forces only, accumulated into d_frc)
+ * for callers that cannot allocate device memory where they need the force:
+ * a plugin hook inside the MD step (cudaMalloc would synchronise the device
+ * and stall the work already queued) or a process whose device memory is
+ * fixed in advance by an admission budget.  It creates nothing and allocates
+ * nothing: its scratch is a fixed array inside the library (about 2.6 MB,
+ * held by every GPU that loads the library until the process exits).
+ * Limits: at most 65,536 local atoms and 64 LJ types (larger inputs return
+ * SPGNB_E_ARG).  Inputs: per-local-atom LJ types (values in
+ * [0, atom_type_numbers)), the triangular pair tables A = 12*A_file and
+ * B = 6*B_file on the device, coordinates, charges, the reference-layout
+ * list; owners are atoms [0, local_atom_numbers - solvent_numbers) as in the
+ * reference's LJ call.  All calls share the one scratch array and each call
+ * clears what must start at zero; calls whose kernels overlap on the GPU race
+ * on it, so serialise them.  The first call on a device looks up the array's
+ * device address with that device current; make it before capturing any
+ * stream on that device. */
+int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_numbers, int atom_type_numbers,
+                                      const int* d_atom_type, const float* d_pair_A, const float* d_pair_B,
+                                      const spgnb_vector* d_crd, const float* d_charge, spgnb_vector* d_frc,
+                                      spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, const spgnb_atom_group* d_nl,
+                                      float cutoff, float pme_beta);
+
 /* ------------------------------------------------------------ diagnostics */
 /* Kernel launches issued by the library so far (all threads). */
 unsigned long long spgnb_launch_count(void);

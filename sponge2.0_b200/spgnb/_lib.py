@@ -26,6 +26,7 @@ EXPORTED = [
     "spgnb_lj_destroy", "spgnb_lj_atom_lj_energy", "spgnb_lj_export_vector_lj",
     "spgnb_solvent_create", "spgnb_solvent_get_local", "spgnb_solvent_pme_direct_force", "spgnb_solvent_destroy",
     "spgnb_launch_count", "spgnb_debug_set_pair_events", "spgnb_nl_count_pairs", "spgnb_probe_fp32_fma_tflops",
+    "spgnb_lj_pme_direct_force_noalloc",
 ]
 
 
@@ -107,6 +108,7 @@ def lib():
     L.spgnb_debug_set_pair_events.argtypes = [vp, vp]
     L.spgnb_nl_count_pairs.argtypes = [vp, vp, M, M, f, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     L.spgnb_probe_fp32_fma_tflops.argtypes = [i, C.POINTER(d)]
+    L.spgnb_lj_pme_direct_force_noalloc.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, M, M, vp, f, f]
     _lib = L
     return L
 
