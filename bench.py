@@ -261,6 +261,10 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms, e2e_total = float(t[0]), float(t[1])
 
+    from spgnb._lib import NLStats
+    st = NLStats()
+    L.spgnb_nl_get_stats(path.nl.handle, C.byref(st))
+
     if rank == 0:
         atoms_steps = world * s.n * K
         value = atoms_steps / (total_ms * 1e-3)
@@ -278,9 +282,11 @@ def main():
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None,
                          "traffic": prof.get("bytes_per_launch"),
-                         "kernel": "k_pair_clusters", "kernel_ms": pair_avg_ms,
+                         "kernel": "k_pair_full", "kernel_ms": pair_avg_ms,
                          "flop_per_launch": flop_per_launch, "listed_pairs": listed.value,
                          "pairs_in_cutoff": inside.value,
+                         "full_list_words": st.full_list_words, "pruned_list_words": st.pruned_list_words,
+                         "prunings": st.prunes, "rebuilds": st.builds,
                          "peak_source": "measured FP32 FFMA throughput on this device (spgnb_probe_fp32_fma_tflops)",
                          "traffic_source": prof.get("source")},
             "clocks": clocks,
@@ -310,7 +316,7 @@ def _ltm(m):
 
 def _profile_traffic():
     """DRAM bytes per pair-kernel launch from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_pair_clusters_mixed96k.json")
+    p = os.path.join(ROOT, "profiles", "k_pair_full_mixed96k.json")
     if not os.path.exists(p):
         return {}
     try:

@@ -97,6 +97,13 @@ typedef struct
     int export_atom_groups;        /* keep the ATOM_GROUP list (d_nl/d_temp) current, 1 */
     int max_entries_per_cluster;   /* capacity of the internal cluster-pair list per
                                       8-atom cluster; 0 = sized from the density */
+    float prune_buffer;            /* the force call evaluates a pruned copy of the list
+                                      holding the pairs within cutoff + prune_buffer (A),
+                                      re-pruned on the device whenever an atom has moved
+                                      more than prune_buffer/2 since the last pruning, so
+                                      no pair within the cutoff is ever left out; 0 = off,
+                                      1.0 by default (no reference counterpart: the
+                                      reference evaluates the whole list each step) */
 } spgnb_nl_options;
 
 void spgnb_nl_default_options(spgnb_nl_options* opt);
@@ -153,6 +160,9 @@ typedef struct
     int work_items;
     long long builds;       /* rebuilds performed so far */
     int overflow;           /* bit 0 list, 1 grid, 2 cluster-pair list */
+    long long full_list_words;  /* listed partners summed over atoms (each pair twice) */
+    long long prunes;       /* prunings performed so far */
+    long long pruned_list_words; /* partners in the pruned lists of the last pruning */
 } spgnb_nl_stats;
 
 /* Reads counters back (synchronises the stream). */

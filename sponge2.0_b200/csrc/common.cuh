@@ -81,7 +81,14 @@ enum Counter
     kCntNeed = 5,       // rebuild requested for the current update
     kCntBuilds = 6,
     kCntMaxCell = 7,
-    kCntSize = 8
+    kCntWords = 8,      // 64-bit: full-list words of the last build (slots 8,9)
+    kCntNbr = 10,       // neighbour-table entries of the last build
+    kCntPrune = 11,     // pruned lists must be rebuilt before the next force
+    kCntPruneDone = 12, // blocks of the running prune kernel that finished
+    kCntPrunes = 13,    // prunings performed
+    kCntPWords = 14,    // 64-bit: words of the running pruning (slots 14,15)
+    kCntPWordsLast = 16,  // 64-bit: words of the last completed pruning (slots 16,17)
+    kCntSize = 24
 };
 
 enum OverflowBits
@@ -90,7 +97,9 @@ enum OverflowBits
     kOvfGrid = 2,      // cell above max_atom_in_grid_numbers
     kOvfPairs = 4,     // cluster-pair list capacity
     kOvfCellHard = 8,  // cell above the in-cell sort capacity
-    kOvfStencil = 16
+    kOvfStencil = 16,
+    kOvfTable = 32,    // neighbour table of a cluster above its capacity
+    kOvfWords = 64     // full-list words capacity
 };
 
 // entry flags
@@ -109,15 +118,55 @@ __host__ __device__ inline Cell make_cell(const spgnb_ltmatrix3& m)
     return Cell{m.a11, m.a21, m.a22, m.a31, m.a32, m.a33};
 }
 
+// One periodic system of a list: geometry of its reference grid and the
+// ranges it owns in the concatenated atom and cell arrays.
+struct SysDesc
+{
+    Cell cell, rcell;
+    float gl, cs2, list_radius;
+    float frac_norm[3];
+    int Nx, Ny, Nz, cell_begin;
+    int atom_begin, atom_count, triclinic;
+    float permit2;  // squared displacement that triggers a rebuild (skin * skin_permit)^2
+    Cell qcell;     // cell / 2^22: Cartesian length of one step of the 22-bit cluster centres
+};
+
+// Pair-function parameters of one system.
+struct ForceParams
+{
+    float rc2, beta, beta3, w_scale;
+    int use_fit, n_types, table_begin, pad;
+};
+
+constexpr int kMaxTable = 8192;      // neighbour-table entries per cluster (13-bit index)
+constexpr int kMaxSlots = 1 << 23;   // slot index field of a pruned-list word
+constexpr int kMaxTypes = 256;       // LJ type field of a pruned-list word
+constexpr int kSortCap = 1024;       // entries a warp sorts in shared memory
+
 }  // namespace spgnb
 
 // ----------------------------------------------------------- host handles
+struct SysHost
+{
+    int atom_begin = 0, atom_count = 0;
+    spgnb_ltmatrix3 cell{}, rcell{};
+    float cutoff = 0, skin = 0, gl = 0, cs2 = 0;
+    int dims[3] = {0, 0, 0};
+    int cell_begin = 0;
+    bool triclinic = false;
+};
+
+// A neighbour list over one or more independent periodic systems whose atoms
+// are concatenated.  The C ABI's NEIGHBOR_LIST is the one-system case; the
+// batched engine uses many.
 struct spgnb_nl
 {
-    int n_cap = 0;
-    float cutoff = 0, skin = 0, grid_length = 0, cs2 = 0;
+    int S = 1;
+    std::vector<SysHost> sys;
+    int n_cap = 0;         // atoms, all systems
+    int G = 0;             // cells, all systems
+    float cutoff = 0, skin = 0, grid_length = 0, cs2 = 0;   // system 0 (one-system API)
     int dims[3] = {0, 0, 0};
-    int G = 0;
     spgnb_ltmatrix3 cell{}, rcell{};
     bool triclinic = false;
     spgnb_nl_options opt{};
@@ -125,9 +174,16 @@ struct spgnb_nl
     long long entries_cap = 0;
     int items_cap = 0;
     int entries_per_cluster = 0;
+    long long nbr_cap = 0;
+    long long words_cap = 0;
+    double words_per_atom = 0;
     bool built = false;
     int local_atoms = 0;
 
+    std::vector<spgnb::SysDesc> h_desc;  // host copy of d_sys
+    spgnb::SysDesc* d_sys = nullptr;
+    int* d_atom_sys = nullptr;    // system of each atom
+    int* d_cell_sys = nullptr;    // system of each cell
     // grid
     int* d_cand_start = nullptr;  // G+1
     int* d_cand = nullptr;        // cell | flags
@@ -139,24 +195,41 @@ struct spgnb_nl
     int* d_atom_shift = nullptr;  // packed lattice shift used by the wrap
     int* d_tmp_atoms = nullptr;   // slots_cap
     float4* d_wrapped = nullptr;  // brick-wrapped coordinates of the last binning
+    int* d_atom_slot = nullptr;   // slot of each atom in the last build
     // per slot
     int* d_slot_atom = nullptr;
-    float4* d_slot_x0 = nullptr;  // raw coordinates at the build
+    float4* d_slot_x0 = nullptr;  // raw coordinates at the build, w = global index
     float4* d_slot_d0 = nullptr;  // offset from the cluster centre at the build
+    int* d_slot_count = nullptr;  // full-list length of each slot
+    long long* d_slot_start = nullptr;  // first word of each slot
     // per cluster
     int* d_cl_cell = nullptr;
+    int* d_cl_sys = nullptr;
     uint4* d_cl_u = nullptr;      // fractional centre (2^32 per box vector), w = radius bits
+    int4* d_cl_q = nullptr;       // the same centre as 22-bit integers (2^22 per box vector)
     float4* d_cl_c = nullptr;     // Cartesian centre (wrapped frame), w = radius
-    int* d_atom_slot = nullptr;   // slot of each atom in the last build
-    // cluster-pair list
+    int* d_nbr_count = nullptr;   // neighbour-table length of each cluster
+    int* d_nbr_start = nullptr;   // clusters_cap + 1
+    int* d_nbr_fill = nullptr;
+    long long* d_cl_words = nullptr;       // full-list words of each cluster
+    long long* d_cl_word_start = nullptr;  // clusters_cap + 1
+    // cluster-pair list (half, exact masks)
     int4* d_ents = nullptr;       // {j-cluster, flags, mask bits 0-31, mask bits 32-63}
     float4* d_ents_d = nullptr;   // centre difference c_j - c_i (minimum image), Cartesian
     int4* d_items = nullptr;
+    // per-cluster neighbour tables and per-slot full lists
+    int2* d_nbr = nullptr;        // {entry, neighbour cluster | side << 30}
+    float4* d_tab = nullptr;      // {D, neighbour slot base | flags}
+    unsigned short* d_words = nullptr;  // (table index << 3) | j-slot in the neighbour cluster
+    // pruned copies of the full lists (same starts, shorter counts), one
+    // 32-bit word per pair: partner slot | LJ type << 23 | image flag << 31
+    unsigned* d_pwords = nullptr;
+    int* d_pcount = nullptr;
+    float4* d_pref = nullptr;     // slot offsets at the last pruning
     int* d_counters = nullptr;
     // reference-layout export
     spgnb_atom_group* d_nl = nullptr;
     int* d_temp = nullptr;
-    // last excluded-list pointers (for exports without a rebuild)
     long long host_builds = 0;
 };
 
@@ -173,8 +246,6 @@ struct spgnb_lj
     float2* d_table = nullptr;       // T*T square table {A, B}
     float* d_lj_energy_atom = nullptr;
     long long* d_frc_acc = nullptr;  // 4 x int64 per local atom (reference-layout path)
-    long long* d_slot_acc = nullptr; // 3 x slots_cap int64, SoA by slot (cluster path)
-    int slot_acc_cap = 0;
     long long* d_totals = nullptr;   // 8 x int64 fixed point
     float4* d_pos = nullptr;         // per slot (spgnb list) or per atom (atom-group path)
     int* d_pos_type = nullptr;
@@ -193,3 +264,19 @@ struct spgnb_solvent
     int local_solvent_numbers = 0;
     int* d_scratch = nullptr;
 };
+
+namespace spgnb
+{
+// Neighbour-list internals shared with the force and batch code.
+int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,
+                    const spgnb_ltmatrix3* rcells, const float* cutoffs, const float* skins,
+                    const spgnb_nl_options* opt, spgnb_nl** out);
+int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
+                   const int* ex_list, const int* ex_num, bool host_rebuild, cudaStream_t s);
+int nl_regrow(spgnb_nl* nl, int flags);
+
+__device__ __forceinline__ long long word_total(const int* counters)
+{
+    return ((long long)counters[kCntWords + 1] << 32) | (unsigned)counters[kCntWords];
+}
+}  // namespace spgnb

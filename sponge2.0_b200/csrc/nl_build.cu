@@ -1,6 +1,6 @@
 // Neighbour-list rebuild: NEIGHBOR_LIST::Initial / Update / Check_Overflow /
-// Clear of SPONGE/neighbor_list/neighbor_list.cpp, rebuilt around 8-atom
-// clusters.
+// Clear of SPONGE/neighbor_list/neighbor_list.cpp, over one or many
+// independent periodic systems, built around 8-atom clusters.
 //
 // The listed set is the reference's, pair for pair: atoms are binned into the
 // reference grid (cells of (rc+skin)/2, same wrap and clamp, :206-275), pairs
@@ -8,9 +8,16 @@
 // with atom_local[i] < atom_local[j] is listed when the FP32 expression
 // Get_Periodic_Displacement(crd_i, crd_j)^2 (vector.hpp:322-327) is below
 // 4*grid_length^2 (:367-372, :705) and j is not in i's exclusion list
-// (:594-665).  Instead of per-atom arrays the result is stored as
-// (i-cluster, j-cluster, 64-bit pair mask) entries that the pair kernel
-// consumes; spgnb_nl_atom_groups exports the reference layout.
+// (:594-665).
+//
+// Stages of one rebuild (every kernel returns at once when no rebuild is due,
+// so a step never synchronises with the host):
+//   bin -> scan -> scatter -> in-cell sort -> cluster centres   (clusters)
+//   search            -> half cluster-pair list, exact 64-bit pair masks
+//   neighbour tables  -> per cluster, every neighbour cluster, sorted
+//   full lists        -> per atom, every listed partner as a 16-bit word
+// The force kernel reads the full lists; the reference-layout export reads the
+// half list.
 #include <math.h>
 #include <string.h>
 
@@ -23,13 +30,6 @@ namespace spgnb
 {
 namespace
 {
-
-struct Grid
-{
-    int Nx, Ny, Nz, G;
-    float gl, cs2;
-    Cell cell, rcell;
-};
 
 __device__ __forceinline__ int pack_shift(int k1, int k2, int k3)
 {
@@ -48,7 +48,7 @@ __device__ __forceinline__ void unpack_shift(int p, int& k1, int& k2, int& k3)
 
 // FP32 squared distance of the reference's candidate test, crd_a - crd_b,
 // with the rounding sequence a CUDA build of vector.hpp:322-327 followed by
-// the dot product produces (see orc_pair_dr2, mode 1, in the oracle).
+// the dot product produces (orc_pair_dr2, mode 1, in the oracle).
 __device__ __forceinline__ float ref_pair_dr2(float3 a, float3 b, const Cell& c, const Cell& r)
 {
     float dx = __fsub_rn(a.x, b.x), dy = __fsub_rn(a.y, b.y), dz = __fsub_rn(a.z, b.z);
@@ -65,32 +65,54 @@ __device__ __forceinline__ float ref_pair_dr2(float3 a, float3 b, const Cell& c,
     return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
 }
 
+// A cluster-pair mask has bit a*8 + b set when i-slot a and j-slot b are
+// listed.  Row a: the j-slots paired with i-slot a.  Column b: the i-slots
+// paired with j-slot b, gathered into a byte (the multiply moves bit 8k to
+// bit 56 + k with no carries between the eight terms).
+__device__ __forceinline__ unsigned mask_row(unsigned long long m, int a) { return (unsigned)(m >> (8 * a)) & 0xffu; }
+
+__device__ __forceinline__ unsigned mask_column(unsigned long long m, int b)
+{
+    const unsigned long long x = (m >> b) & 0x0101010101010101ull;
+    return (unsigned)((x * 0x0102040810204080ull) >> 56);
+}
+
+// Partners of own slot a in a neighbour-table element of the given side
+// (0: own cluster is the entry's i-cluster, 1: its j-cluster, 2: both).
+__device__ __forceinline__ unsigned partners(unsigned long long m, int side, int a)
+{
+    unsigned p = side == 0 ? mask_row(m, a) : mask_column(m, a);
+    if (side == 2) p |= mask_row(m, a);
+    return p;
+}
+
 // ---------------------------------------------------------------- kernels
 
 // Check_Refresh (neighbor_list.cpp:166-180): any atom moved more than
 // skin*skin_permit since the last build.
-__global__ void k_check_refresh(int n_slots, const int* __restrict__ slot_atom,
-                                const float3* __restrict__ crd, const float4* __restrict__ x0, Cell cell,
-                                Cell rcell, float permit2, int* counters)
+__global__ void k_check_refresh(int n_slots, const int* __restrict__ slot_atom, const int* __restrict__ cl_sys,
+                                const SysDesc* __restrict__ sys, const float3* __restrict__ crd,
+                                const float4* __restrict__ x0, int* counters)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    int total = counters[kCntClusters] * kClusterSize;
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int total = counters[kCntClusters] * kClusterSize;
     bool move = false;
     if (s < n_slots && s < total)
     {
-        int a = slot_atom[s];
+        const int a = slot_atom[s];
         if (a >= 0)
         {
-            float3 c = crd[a];
-            float4 o = x0[s];
+            const SysDesc& D = sys[cl_sys[s >> 3]];
+            const float3 c = crd[a];
+            const float4 o = x0[s];
             float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
-            float sx = floorf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31 + 0.5f);
-            float sy = floorf(dy * rcell.a22 + dz * rcell.a32 + 0.5f);
-            float sz = floorf(dz * rcell.a33 + 0.5f);
-            dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
-            dy -= sy * cell.a22 + sz * cell.a32;
-            dz -= sz * cell.a33;
-            move = dx * dx + dy * dy + dz * dz > permit2;
+            const float sx = floorf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31 + 0.5f);
+            const float sy = floorf(dy * D.rcell.a22 + dz * D.rcell.a32 + 0.5f);
+            const float sz = floorf(dz * D.rcell.a33 + 0.5f);
+            dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
+            dy -= sy * D.cell.a22 + sz * D.cell.a32;
+            dz -= sz * D.cell.a33;
+            move = dx * dx + dy * dy + dz * dz > D.permit2;
         }
     }
     if (__any_sync(0xffffffffu, move) && (threadIdx.x & 31) == 0) atomicExch(&counters[kCntNeed], 1);
@@ -98,22 +120,23 @@ __global__ void k_check_refresh(int n_slots, const int* __restrict__ slot_atom,
 
 // Put_Atom_In_Grids (neighbor_list.cpp:206-275): brick wrap, cell index
 // nx*Ny*Nz + ny*Nz + nz with clamping, per-cell count.
-__global__ void k_bin(int n, const float3* __restrict__ crd, Grid g, int* __restrict__ atom_cell,
-                      int* __restrict__ atom_shift, float4* __restrict__ wrapped, int* __restrict__ cell_count,
-                      const int* __restrict__ counters)
+__global__ void k_bin(int n, const float3* __restrict__ crd, const int* __restrict__ atom_sys,
+                      const SysDesc* __restrict__ sys, int* __restrict__ atom_cell, int* __restrict__ atom_shift,
+                      float4* __restrict__ wrapped, int* __restrict__ cell_count, const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    float3 c = crd[i];
+    const SysDesc& g = sys[atom_sys[i]];
+    const float3 c = crd[i];
     float x = c.x, y = c.y, z = c.z;
-    float k3 = floorf(__fdiv_rn(z, g.cell.a33));
+    const float k3 = floorf(__fdiv_rn(z, g.cell.a33));
     z = __fsub_rn(z, __fmul_rn(k3, g.cell.a33));
     y = __fsub_rn(y, __fmul_rn(k3, g.cell.a32));
-    float k2 = floorf(__fdiv_rn(y, g.cell.a22));
+    const float k2 = floorf(__fdiv_rn(y, g.cell.a22));
     y = __fsub_rn(y, __fmul_rn(k2, g.cell.a22));
     x = __fsub_rn(x, __fadd_rn(__fmul_rn(k3, g.cell.a31), __fmul_rn(k2, g.cell.a21)));
-    float k1 = floorf(__fdiv_rn(x, g.cell.a11));
+    const float k1 = floorf(__fdiv_rn(x, g.cell.a11));
     x = __fsub_rn(x, __fmul_rn(k1, g.cell.a11));
     int nx = (int)__fdiv_rn(x, g.gl);
     int ny = (int)__fdiv_rn(y, g.gl);
@@ -121,75 +144,83 @@ __global__ void k_bin(int n, const float3* __restrict__ crd, Grid g, int* __rest
     nx = nx < 0 ? 0 : (nx < g.Nx ? nx : g.Nx - 1);
     ny = ny < 0 ? 0 : (ny < g.Ny ? ny : g.Ny - 1);
     nz = nz < 0 ? 0 : (nz < g.Nz ? nz : g.Nz - 1);
-    int cid = nx * g.Ny * g.Nz + ny * g.Nz + nz;
+    const int cid = g.cell_begin + nx * g.Ny * g.Nz + ny * g.Nz + nz;
     atom_cell[i] = cid;
     atom_shift[i] = pack_shift((int)k1, (int)k2, (int)k3);
     wrapped[i] = make_float4(x, y, z, 0.0f);
     atomicAdd(&cell_count[cid], 1);
 }
 
-// Cluster counts per cell (ceil(count/8)) and their exclusive scan; one block.
+// Exclusive scan of value(0..n-1) into out[0..n-1] by one block (a multiple
+// of 32 threads, each taking a contiguous chunk); the total is returned to
+// every thread.
+template <typename T, typename F>
+__device__ T block_scan(int n, F value, T* out)
+{
+    __shared__ T warp_sums[32];
+    const int threads = blockDim.x;
+    const int per = (n + threads - 1) / threads;
+    const int lo = min(n, threadIdx.x * per);
+    const int hi = min(n, lo + per);
+    T sum = 0;
+    for (int c = lo; c < hi; c++) sum += value(c);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T v = sum;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const T t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_sums[warp] = v;
+    __syncthreads();
+    const int nw = threads >> 5;
+    if (warp == 0)
+    {
+        T w = lane < nw ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const T t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < nw) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    T excl = v - sum + (warp > 0 ? warp_sums[warp - 1] : 0);
+    for (int c = lo; c < hi; c++)
+    {
+        out[c] = excl;
+        excl += value(c);
+    }
+    const T total = warp_sums[nw - 1];
+    __syncthreads();
+    return total;
+}
+
+// Cluster counts per cell (ceil(count/8)), their exclusive scan, overflow
+// checks of the cells; one block.
 __global__ void k_scan_cells(int G, const int* __restrict__ cell_count, int* __restrict__ cell_cl_start,
                              int max_atom_in_grid, int clusters_cap, int* counters)
 {
     if (counters[kCntNeed] == 0) return;
-    __shared__ int warp_sums[32];
-    __shared__ int warp_max[32];
-    const int T = blockDim.x;
-    const int per = (G + T - 1) / T;
-    const int lo = threadIdx.x * per;
-    const int hi = min(G, lo + per);
-    int sum = 0, mx = 0;
-    for (int c = lo; c < hi; c++)
-    {
-        int cnt = cell_count[c];
-        sum += (cnt + kClusterSize - 1) / kClusterSize;
-        mx = max(mx, cnt);
-    }
-    // block exclusive scan of sum
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int v = sum;
-    for (int o = 1; o < 32; o <<= 1)
-    {
-        int t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += t;
-    }
-    int m = mx;
-    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 31) warp_sums[warp] = v;
-    if (lane == 0) warp_max[warp] = m;
+    __shared__ int max_cell;
+    if (threadIdx.x == 0) max_cell = 0;
     __syncthreads();
-    if (warp == 0)
+    int local_max = 0;
+    for (int c = threadIdx.x; c < G; c += blockDim.x) local_max = max(local_max, cell_count[c]);
+    atomicMax(&max_cell, local_max);
+    const int total = block_scan<int>(
+        G, [&](int c) { return (min(cell_count[c], kMaxCellAtoms) + kClusterSize - 1) / kClusterSize; },
+        cell_cl_start);
+    if (threadIdx.x == 0)
     {
-        int nw = T >> 5;
-        int w = lane < nw ? warp_sums[lane] : 0;
-        int wm = lane < nw ? warp_max[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1)
-        {
-            int t = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += t;
-        }
-        for (int o = 16; o > 0; o >>= 1) wm = max(wm, __shfl_xor_sync(0xffffffffu, wm, o));
-        if (lane < nw) warp_sums[lane] = w;
-        if (lane == 0) warp_max[0] = wm;
-    }
-    __syncthreads();
-    int excl = v - sum + (warp > 0 ? warp_sums[warp - 1] : 0);
-    for (int c = lo; c < hi; c++)
-    {
-        cell_cl_start[c] = excl;
-        excl += (cell_count[c] + kClusterSize - 1) / kClusterSize;
-    }
-    if (threadIdx.x == T - 1)
-    {
-        int total = warp_sums[(T >> 5) - 1];
         cell_cl_start[G] = total;
-        counters[kCntClusters] = min(total, clusters_cap);
-        counters[kCntMaxCell] = warp_max[0];
+        // (cannot exceed the capacity n/8 + cells; if it did, build nothing)
+        counters[kCntClusters] = total <= clusters_cap ? total : 0;
+        counters[kCntMaxCell] = max_cell;
         int flags = 0;
-        if (warp_max[0] > max_atom_in_grid) flags |= kOvfGrid;
+        if (max_cell > max_atom_in_grid) flags |= kOvfGrid;
         if (total > clusters_cap) flags |= kOvfPairs;
-        if (warp_max[0] > 2048) flags |= kOvfCellHard;
+        if (max_cell > kMaxCellAtoms) flags |= kOvfCellHard;
         if (flags) atomicOr(&counters[kCntOverflow], flags);
     }
 }
@@ -199,12 +230,12 @@ __global__ void k_scatter(int n, const int* __restrict__ atom_cell, const int* _
                           const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    int c = atom_cell[i];
-    int pos = atomicAdd(&cell_cursor[c], 1);
-    int s = cell_cl_start[c] * kClusterSize + pos;
-    if (s < slots_cap) tmp_atoms[s] = i;
+    const int c = atom_cell[i];
+    const int pos = atomicAdd(&cell_cursor[c], 1);
+    const int s = cell_cl_start[c] * kClusterSize + pos;
+    if (pos < kMaxCellAtoms && s < slots_cap) tmp_atoms[s] = i;
 }
 
 __device__ __forceinline__ unsigned spread3(unsigned v)
@@ -215,30 +246,34 @@ __device__ __forceinline__ unsigned spread3(unsigned v)
 
 // Deterministic in-cell order: by a 4x4x4 Morton sub-cell key, then by atom
 // index, so clusters are spatially compact and the build reproducible.
-__global__ void k_sort_cells(Grid g, const int* __restrict__ cell_count, const int* __restrict__ cell_cl_start,
+__global__ void k_sort_cells(int G, const int* __restrict__ cell_sys, const SysDesc* __restrict__ sys,
+                             const int* __restrict__ cell_count, const int* __restrict__ cell_cl_start,
                              const int* __restrict__ tmp_atoms, const float4* __restrict__ wrapped,
-                             int* __restrict__ slot_atom, int* __restrict__ cl_cell, int* __restrict__ atom_slot,
-                             int slots_cap, const int* __restrict__ counters)
+                             int* __restrict__ slot_atom, int* __restrict__ cl_cell, int* __restrict__ cl_sys,
+                             int* __restrict__ atom_slot, int slots_cap, const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
     extern __shared__ unsigned long long keys[];
-    for (int c = blockIdx.x; c < g.G; c += gridDim.x)
+    for (int c = blockIdx.x; c < G; c += gridDim.x)
     {
-        int n = min(cell_count[c], 2048);
-        int cl0 = cell_cl_start[c], cl1 = cell_cl_start[c + 1];
-        int base = cl0 * kClusterSize;
-        int nslots = (cl1 - cl0) * kClusterSize;
+        const int sy = cell_sys[c];
+        const SysDesc& g = sys[sy];
+        const int n = min(cell_count[c], kMaxCellAtoms);
+        const int cl0 = cell_cl_start[c], cl1 = cell_cl_start[c + 1];
+        const int base = cl0 * kClusterSize;
+        const int nslots = (cl1 - cl0) * kClusterSize;
         if (base + nslots > slots_cap) continue;
-        int nz = c % g.Nz, ny = (c / g.Nz) % g.Ny, nx = c / (g.Ny * g.Nz);
-        float inv = 4.0f / g.gl;
+        const int local = c - g.cell_begin;
+        const int nz = local % g.Nz, ny = (local / g.Nz) % g.Ny, nx = local / (g.Ny * g.Nz);
+        const float inv = 4.0f / g.gl;
         for (int e = threadIdx.x; e < n; e += blockDim.x)
         {
-            int a = tmp_atoms[base + e];
-            float4 w = wrapped[a];
-            int sx = min(3, max(0, (int)((w.x - nx * g.gl) * inv)));
-            int sy = min(3, max(0, (int)((w.y - ny * g.gl) * inv)));
-            int sz = min(3, max(0, (int)((w.z - nz * g.gl) * inv)));
-            unsigned key = (spread3(sx) << 2) | (spread3(sy) << 1) | spread3(sz);
+            const int a = tmp_atoms[base + e];
+            const float4 w = wrapped[a];
+            const int sx = min(3, max(0, (int)((w.x - nx * g.gl) * inv)));
+            const int syy = min(3, max(0, (int)((w.y - ny * g.gl) * inv)));
+            const int sz = min(3, max(0, (int)((w.z - nz * g.gl) * inv)));
+            const unsigned key = (spread3(sx) << 2) | (spread3(syy) << 1) | spread3(sz);
             keys[e] = ((unsigned long long)key << 32) | (unsigned)a;
         }
         __syncthreads();
@@ -246,7 +281,7 @@ __global__ void k_sort_cells(Grid g, const int* __restrict__ cell_count, const i
         {
             if (e < n)
             {
-                unsigned long long k = keys[e];
+                const unsigned long long k = keys[e];
                 int r = 0;
                 for (int f = 0; f < n; f++) r += keys[f] < k;
                 const int a = (int)(k & 0xffffffffu);
@@ -258,27 +293,35 @@ __global__ void k_sort_cells(Grid g, const int* __restrict__ cell_count, const i
                 slot_atom[base + e] = -1;
             }
         }
-        for (int k = cl0 + threadIdx.x; k < cl1; k += blockDim.x) cl_cell[k] = c;
+        for (int k = cl0 + threadIdx.x; k < cl1; k += blockDim.x)
+        {
+            cl_cell[k] = c;
+            cl_sys[k] = sy;
+        }
         __syncthreads();
     }
 }
 
 // Per cluster: centre (double, bounding-box middle of the wrapped positions),
 // radius, fractional fixed-point centre, per-slot offsets and build
-// coordinates.  Eight lanes per cluster.
+// coordinates (w = the atom's global index, -1 for padding).  Eight lanes per
+// cluster.
 __global__ void k_cluster_props(const float3* __restrict__ crd, const int* __restrict__ slot_atom,
-                                const int* __restrict__ atom_shift, const int* __restrict__ atom_local, Cell cell,
-                                int* counters, uint4* __restrict__ cl_u, float4* __restrict__ cl_c,
+                                const int* __restrict__ atom_shift, const int* __restrict__ atom_local,
+                                const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys, int* counters,
+                                uint4* __restrict__ cl_u, int4* __restrict__ cl_q, float4* __restrict__ cl_c,
                                 float4* __restrict__ slot_x0, float4* __restrict__ slot_d0, int clusters_cap)
 {
     if (counters[kCntNeed] == 0) return;
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    int k = t >> 3;
-    int l8 = t & 7;
-    int nc = counters[kCntClusters];
-    bool live = k < nc && k < clusters_cap;
-    int s = k * kClusterSize + l8;
-    int a = live ? slot_atom[s] : -1;
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int k = t >> 3;
+    const int l8 = t & 7;
+    const int nc = counters[kCntClusters];
+    const bool live = k < nc && k < clusters_cap;
+    const int s = k * kClusterSize + l8;
+    const int a = live ? slot_atom[s] : -1;
+    Cell cell{1, 0, 1, 0, 0, 1};
+    if (live) cell = sys[cl_sys[k]].cell;
     double w[3] = {0, 0, 0};
     float3 x = make_float3(0, 0, 0);
     if (a >= 0)
@@ -302,60 +345,54 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, const int* __res
         }
     }
     double cen[3];
-    for (int d = 0; d < 3; d++) cen[d] = 0.5 * (lo[d] + hi[d]);
-    // fractional centre; the double inverse of the float cell
-    double c11 = cell.a11, c21 = cell.a21, c22 = cell.a22, c31 = cell.a31, c32 = cell.a32, c33 = cell.a33;
-    double r33 = 1.0 / c33, r22 = 1.0 / c22, r11 = 1.0 / c11;
-    double r32 = -c32 * r33 / c22;
-    double r31 = (c32 * c21 * r33 - c31 * c22) / (c11 * c22 * c33);
-    double r21 = -c21 * r22 / c11;
-    double sfr[3] = {cen[0] * r11 + cen[1] * r21 + cen[2] * r31, cen[1] * r22 + cen[2] * r32, cen[2] * r33};
-    unsigned u[3];
+    for (int d = 0; d < 3; d++) cen[d] = (lo[d] <= hi[d]) ? 0.5 * (lo[d] + hi[d]) : 0.0;
+    // fractional centre on the double inverse of the float cell
+    const double c11 = cell.a11, c21 = cell.a21, c22 = cell.a22, c31 = cell.a31, c32 = cell.a32, c33 = cell.a33;
+    const double r33 = 1.0 / c33, r22 = 1.0 / c22, r11 = 1.0 / c11;
+    const double r32 = -c32 * r33 / c22;
+    const double r31 = (c32 * c21 * r33 - c31 * c22) / (c11 * c22 * c33);
+    const double r21 = -c21 * r22 / c11;
+    const double sfr[3] = {cen[0] * r11 + cen[1] * r21 + cen[2] * r31, cen[1] * r22 + cen[2] * r32, cen[2] * r33};
+    // the centre is rounded to 2^-22 of each box vector, so centre
+    // differences are exact 22-bit integers (the force kernel converts them
+    // without a table); the 32-bit form is the same value shifted by 10
+    unsigned u[3], u22[3];
     double q[3];
     for (int d = 0; d < 3; d++)
     {
-        double f = floor(sfr[d]);
-        double frac = sfr[d] - f;
-        double scaled = floor(frac * 4294967296.0);
-        if (scaled >= 4294967296.0) scaled = 4294967295.0;
-        u[d] = (unsigned)scaled;
-        q[d] = scaled / 4294967296.0 + f;  // the quantised centre, unwrapped
+        const double f = floor(sfr[d]);
+        const double frac = sfr[d] - f;
+        double scaled = floor(frac * 4194304.0);
+        if (scaled >= 4194304.0) scaled = 4194303.0;
+        if (!(scaled >= 0.0)) scaled = 0.0;
+        u22[d] = (unsigned)scaled;
+        u[d] = u22[d] << 10;
+        q[d] = scaled / 4194304.0 + f;  // the quantised centre, unwrapped
     }
-    double cq[3] = {q[0] * c11 + q[1] * c21 + q[2] * c31, q[1] * c22 + q[2] * c32, q[2] * c33};
+    const double cq[3] = {q[0] * c11 + q[1] * c21 + q[2] * c31, q[1] * c22 + q[2] * c32, q[2] * c33};
     double r2 = 0;
     if (a >= 0)
     {
-        double d0 = w[0] - cq[0], d1 = w[1] - cq[1], d2 = w[2] - cq[2];
+        const double d0 = w[0] - cq[0], d1 = w[1] - cq[1], d2 = w[2] - cq[2];
         r2 = d0 * d0 + d1 * d1 + d2 * d2;
         slot_d0[s] = make_float4((float)d0, (float)d1, (float)d2, 0.0f);
-        // raw build coordinates, w = the atom's global index (-1: padding)
         slot_x0[s] = make_float4(x.x, x.y, x.z, __int_as_float(atom_local[a]));
     }
     else if (live)
     {
-        float p = kPadCoordinate + (float)s;
+        const float p = kPadCoordinate + (float)s;
         slot_d0[s] = make_float4(p, p, p, 0.0f);
         slot_x0[s] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
     }
     for (int o = 1; o < 8; o <<= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
     if (live && l8 == 0)
     {
-        float rad = (float)(sqrt(r2) * (1.0 + 1e-6) + 1e-5);
+        const float rad = (float)(sqrt(r2) * (1.0 + 1e-6) + 1e-5);
         cl_u[k] = make_uint4(u[0], u[1], u[2], __float_as_uint(rad));
+        cl_q[k] = make_int4((int)u22[0], (int)u22[1], (int)u22[2], 0);
         cl_c[k] = make_float4((float)cq[0], (float)cq[1], (float)cq[2], rad);
     }
 }
-
-struct SearchParams
-{
-    Grid g;
-    float list_radius;    // sqrt(cs2) with a margin, for the sphere prefilter
-    float frac_norm[3];   // norms of the columns of rcell
-    int triclinic;
-    long long entries_cap;
-    int items_cap;
-    int clusters_cap;
-};
 
 __device__ __forceinline__ float3 frac_delta(uint4 ui, uint4 uj)
 {
@@ -371,7 +408,7 @@ __device__ __forceinline__ float3 frac_to_cart(float3 f, const Cell& c)
 __device__ __forceinline__ bool excluded_pair(int glo, int ghi, const int* __restrict__ ex_start,
                                               const int* __restrict__ ex_list, const int* __restrict__ ex_num)
 {
-    int k = ex_num[glo];
+    const int k = ex_num[glo];
     if (k <= 0) return false;
     const int* l = ex_list + ex_start[glo];
     if (ghi < l[0] || ghi > l[k - 1]) return false;
@@ -388,10 +425,12 @@ __device__ __forceinline__ bool excluded_pair(int glo, int ghi, const int* __res
 constexpr int kSearchWarps = 4;
 
 __global__ void __launch_bounds__(kSearchWarps * 32)
-    k_search(SearchParams p, const int* __restrict__ cand_start, const int* __restrict__ cand,
-             const int* __restrict__ cell_cl_start, const int* __restrict__ cl_cell, const uint4* __restrict__ cl_u,
-             const float4* __restrict__ slot_x0, const int* __restrict__ ex_start, const int* __restrict__ ex_list, const int* __restrict__ ex_num,
-             int4* __restrict__ ents, float4* __restrict__ ents_d, int4* __restrict__ items, int* counters)
+    k_search(const SysDesc* __restrict__ sys, long long entries_cap, int items_cap,
+             const int* __restrict__ cand_start, const int* __restrict__ cand, const int* __restrict__ cell_cl_start,
+             const int* __restrict__ cl_cell, const int* __restrict__ cl_sys, const uint4* __restrict__ cl_u,
+             const float4* __restrict__ slot_x0, const int* __restrict__ ex_start, const int* __restrict__ ex_list,
+             const int* __restrict__ ex_num, int4* __restrict__ ents, float4* __restrict__ ents_d,
+             int4* __restrict__ items, int* counters)
 {
     if (counters[kCntNeed] == 0) return;
     __shared__ int4 stage[kSearchWarps][kChunk];
@@ -404,6 +443,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
 
     for (int ci = blockIdx.x * kSearchWarps + wib; ci < nc; ci += total_warps)
     {
+        const SysDesc& p = sys[cl_sys[ci]];
         const int cellA = cl_cell[ci];
         const uint4 ui = cl_u[ci];
         const float ri = __uint_as_float(ui.w);
@@ -419,7 +459,6 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
         }
         int staged = 0;
         auto flush = [&](int count) {
-            // reserve space for `count` entries and one work item
             long long e0 = 0;
             int it = 0;
             if (lane == 0)
@@ -429,7 +468,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
             }
             e0 = __shfl_sync(0xffffffffu, e0, 0);
             it = __shfl_sync(0xffffffffu, it, 0);
-            const bool ok = (e0 + count <= p.entries_cap) && (it < p.items_cap);
+            const bool ok = (e0 + count <= entries_cap) && (it < items_cap);
             if (ok && lane < count)
             {
                 ents[e0 + lane] = stage[wib][lane];
@@ -437,7 +476,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
             }
             // an item slot that exists is always written, empty when its
             // entries did not fit, so readers never see a stale range
-            if (lane == 0 && it < p.items_cap) items[it] = make_int4(ci, ok ? (int)e0 : 0, ok ? count : 0, 0);
+            if (lane == 0 && it < items_cap) items[it] = make_int4(ci, ok ? (int)e0 : 0, ok ? count : 0, 0);
             if (lane == 0 && !ok) atomicOr(&counters[kCntOverflow], kOvfPairs);
             __syncwarp();
         };
@@ -453,25 +492,25 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
             const int b1 = min(cell_cl_start[cellB + 1], nc);
             for (; b0 < b1; b0 += 32)
             {
-                int cj = b0 + lane;
+                const int cj = b0 + lane;
                 bool ok = false;
                 if (cj < b1)
                 {
-                    uint4 uj = cl_u[cj];
-                    float rsum = ri + __uint_as_float(uj.w) + p.list_radius;
-                    float3 f = frac_delta(ui, uj);
+                    const uint4 uj = cl_u[cj];
+                    const float rsum = ri + __uint_as_float(uj.w) + p.list_radius;
+                    const float3 f = frac_delta(ui, uj);
                     if (!p.triclinic)
                     {
-                        float3 d = frac_to_cart(f, p.g.cell);
+                        const float3 d = frac_to_cart(f, p.cell);
                         ok = d.x * d.x + d.y * d.y + d.z * d.z < rsum * rsum;
                     }
                     else
                     {
                         for (int im = 0; im < 27 && !ok; im++)
                         {
-                            float3 fi = make_float3(f.x + (float)(im / 9 - 1), f.y + (float)((im / 3) % 3 - 1),
-                                                    f.z + (float)(im % 3 - 1));
-                            float3 d = frac_to_cart(fi, p.g.cell);
+                            const float3 fi = make_float3(f.x + (float)(im / 9 - 1), f.y + (float)((im / 3) % 3 - 1),
+                                                          f.z + (float)(im % 3 - 1));
+                            const float3 d = frac_to_cart(fi, p.cell);
                             ok = d.x * d.x + d.y * d.y + d.z * d.z < rsum * rsum;
                         }
                     }
@@ -497,9 +536,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
                             in = a_lo ? fwd : rev;
                             if (in)
                             {
-                                float d2 = a_lo ? ref_pair_dr2(xa[h], xb, p.g.cell, p.g.rcell)
-                                                : ref_pair_dr2(xb, xa[h], p.g.cell, p.g.rcell);
-                                in = d2 < p.g.cs2;
+                                const float d2 = a_lo ? ref_pair_dr2(xa[h], xb, p.cell, p.rcell)
+                                                      : ref_pair_dr2(xb, xa[h], p.cell, p.rcell);
+                                in = d2 < p.cs2;
                                 if (in)
                                     in = !(a_lo ? excluded_pair(ga[h], gb, ex_start, ex_list, ex_num)
                                                 : excluded_pair(gb, ga[h], ex_start, ex_list, ex_num));
@@ -514,9 +553,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
                         const uint4 uj = cl_u[cjs];
                         const float3 f = frac_delta(ui, uj);
                         const float rr = ri + __uint_as_float(uj.w);
-                        bool safe = fabsf(f.x) + rr * p.frac_norm[0] < 0.49f &&
-                                    fabsf(f.y) + rr * p.frac_norm[1] < 0.49f &&
-                                    fabsf(f.z) + rr * p.frac_norm[2] < 0.49f;
+                        const bool safe = fabsf(f.x) + rr * p.frac_norm[0] < 0.49f &&
+                                          fabsf(f.y) + rr * p.frac_norm[1] < 0.49f &&
+                                          fabsf(f.z) + rr * p.frac_norm[2] < 0.49f;
                         if (lane == 0)
                         {
                             stage[wib][staged] =
@@ -525,7 +564,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
                             const double q = 2.3283064365386963e-10;
                             const double fx = (double)(int)(uj.x - ui.x) * q, fy = (double)(int)(uj.y - ui.y) * q,
                                          fz = (double)(int)(uj.z - ui.z) * q;
-                            const Cell& c = p.g.cell;
+                            const Cell& c = p.cell;
                             stage_d[wib][staged] = make_float4(
                                 (float)(fx * (double)c.a11 + fy * (double)c.a21 + fz * (double)c.a31),
                                 (float)(fy * (double)c.a22 + fz * (double)c.a32), (float)(fz * (double)c.a33), 0.0f);
@@ -545,12 +584,308 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
     }
 }
 
+// --------------------------------------------- neighbour tables, full lists
+
+__global__ void k_zero_tables(int n, int* __restrict__ a, int* __restrict__ b, const int* __restrict__ counters)
+{
+    if (counters[kCntNeed] == 0) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        a[i] = 0;
+        b[i] = 0;
+    }
+}
+
+// Table length per cluster: each cluster pair counts on both sides, a
+// cluster paired with itself once.
+__global__ void k_nbr_count(const int4* __restrict__ items, const int4* __restrict__ ents, int items_cap,
+                            int* __restrict__ nbr_count, const int* __restrict__ counters)
+{
+    if (counters[kCntNeed] == 0) return;
+    const int nitems = min(counters[kCntItems], items_cap);
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += warps)
+    {
+        const int4 item = items[it];
+        if (lane < item.z)
+        {
+            const int cj = ents[item.y + lane].x;
+            atomicAdd(&nbr_count[item.x], 1);
+            if (cj != item.x) atomicAdd(&nbr_count[cj], 1);
+        }
+    }
+}
+
+__global__ void k_scan_nbr(int nc_cap, const int* __restrict__ nbr_count, int* __restrict__ nbr_start,
+                           long long nbr_cap, int* counters)
+{
+    if (counters[kCntNeed] == 0) return;
+    const int nc = min(counters[kCntClusters], nc_cap);
+    const int total = block_scan<int>(nc, [&](int c) { return nbr_count[c]; }, nbr_start);
+    if (threadIdx.x == 0)
+    {
+        nbr_start[nc] = total;
+        counters[kCntNbr] = total;
+        if (total > nbr_cap) atomicOr(&counters[kCntOverflow], kOvfTable);
+    }
+}
+
+// Table elements {entry, neighbour cluster | side << 29} in arrival order;
+// the table kernel sorts them.
+__global__ void k_nbr_fill(const int4* __restrict__ items, const int4* __restrict__ ents, int items_cap,
+                           const int* __restrict__ nbr_start, int* __restrict__ nbr_fill, int2* __restrict__ nbr,
+                           long long nbr_cap, const int* __restrict__ counters)
+{
+    if (counters[kCntNeed] == 0) return;
+    if (counters[kCntNbr] > nbr_cap) return;
+    const int nitems = min(counters[kCntItems], items_cap);
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += warps)
+    {
+        const int4 item = items[it];
+        if (lane < item.z)
+        {
+            const int e = item.y + lane;
+            const int ci = item.x, cj = ents[e].x;
+            if (cj == ci)
+            {
+                const int p = atomicAdd(&nbr_fill[ci], 1);
+                nbr[nbr_start[ci] + p] = make_int2(e, ci | (2 << 29));
+            }
+            else
+            {
+                const int p = atomicAdd(&nbr_fill[ci], 1);
+                nbr[nbr_start[ci] + p] = make_int2(e, cj);
+                const int q = atomicAdd(&nbr_fill[cj], 1);
+                nbr[nbr_start[cj] + q] = make_int2(e, ci | (1 << 29));
+            }
+        }
+    }
+}
+
+constexpr int kTabWarps = 4;
+
+// Per cluster (one warp): sort the table by neighbour cluster so the build is
+// reproducible, write {D, neighbour slot base | flags} (D = neighbour centre
+// minus own centre, minimum image), count each slot's partners.  Tables
+// longer than kSortCap, or all of them when the table array overflowed, get
+// no partners (flagged).
+__global__ void __launch_bounds__(kTabWarps * 32)
+    k_nbr_table(int nc_cap, const int* __restrict__ nbr_start, int2* __restrict__ nbr, long long nbr_cap,
+                const int4* __restrict__ ents, const float4* __restrict__ ents_d, float4* __restrict__ tab,
+                int* __restrict__ slot_count, long long* __restrict__ cl_words, int* counters)
+{
+    if (counters[kCntNeed] == 0) return;
+    __shared__ unsigned long long keys[kTabWarps][kSortCap];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int nc = min(counters[kCntClusters], nc_cap);
+    const bool tables_ok = counters[kCntNbr] <= nbr_cap;
+    const int warps = gridDim.x * kTabWarps;
+    unsigned long long* k = keys[wib];
+    for (int c = blockIdx.x * kTabWarps + wib; c < nc; c += warps)
+    {
+        const int base = tables_ok ? nbr_start[c] : 0;
+        const int T = tables_ok ? nbr_start[c + 1] - base : 0;
+        if (T > kSortCap)
+        {
+            if (lane == 0) atomicOr(&counters[kCntOverflow], kOvfTable);
+        }
+        if (T == 0 || T > kSortCap)
+        {
+            if (lane < 8) slot_count[c * kClusterSize + lane] = 0;
+            if (lane == 0) cl_words[c] = 0;
+            continue;
+        }
+        int npad = 32;
+        while (npad < T) npad <<= 1;
+        for (int t = lane; t < npad; t += 32)
+        {
+            if (t < T)
+            {
+                const int2 v = nbr[base + t];
+                k[t] = ((unsigned long long)(unsigned)(v.y & 0x1fffffff) << 32) |
+                       ((unsigned long long)((v.y >> 29) & 3) << 30) | (unsigned)t;
+            }
+            else
+                k[t] = ~0ull;
+        }
+        __syncwarp();
+        // bitonic sort in shared memory
+        for (int size = 2; size <= npad; size <<= 1)
+            for (int stride = size >> 1; stride > 0; stride >>= 1)
+            {
+                for (int t = lane; t < npad / 2; t += 32)
+                {
+                    const int lo = 2 * t - (t & (stride - 1));
+                    const int hi = lo + stride;
+                    const bool up = (lo & size) == 0;
+                    const unsigned long long x = k[lo], y = k[hi];
+                    if ((x > y) == up)
+                    {
+                        k[lo] = y;
+                        k[hi] = x;
+                    }
+                }
+                __syncwarp();
+            }
+        // gather the elements in sorted order into the key array (each
+        // lane reads and writes only its own positions), then write back
+        for (int t = lane; t < T; t += 32)
+        {
+            const int2 v = nbr[base + (int)(k[t] & 0x3fffffffu)];
+            k[t] = ((unsigned long long)(unsigned)v.y << 32) | (unsigned)v.x;
+        }
+        __syncwarp();
+        unsigned cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int t = lane; t < T; t += 32)
+        {
+            const unsigned long long kv = k[t];
+            const int e = (int)(kv & 0xffffffffu);
+            const int y = (int)(kv >> 32);
+            nbr[base + t] = make_int2(e, y);
+            const int side = (y >> 29) & 3;
+            const int other = y & 0x1fffffff;
+            const int4 en = ents[e];
+            const float4 d = ents_d[e];
+            float dx = 0.0f, dy = 0.0f, dz = 0.0f;
+            if (side == 0)
+            {
+                dx = d.x;
+                dy = d.y;
+                dz = d.z;
+            }
+            else if (side == 1)
+            {
+                dx = -d.x;
+                dy = -d.y;
+                dz = -d.z;
+            }
+            const int flags = (en.y & kEntPairImage) ? (1 << 30) : 0;
+            tab[base + t] = make_float4(dx, dy, dz, __int_as_float((other * kClusterSize) | flags));
+            const unsigned long long m = ((unsigned long long)(unsigned)en.w << 32) | (unsigned)en.z;
+#pragma unroll
+            for (int a = 0; a < 8; a++) cnt[a] += __popc(partners(m, side, a));
+        }
+        __syncwarp();
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+            for (int o = 16; o > 0; o >>= 1) cnt[a] += __shfl_xor_sync(0xffffffffu, cnt[a], o);
+        unsigned mine = 0;
+        long long tot = 0;
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+        {
+            mine = lane == a ? cnt[a] : mine;
+            tot += cnt[a];
+        }
+        if (lane < 8) slot_count[c * kClusterSize + lane] = (int)mine;
+        if (lane == 0) cl_words[c] = tot;
+    }
+}
+
+__global__ void k_scan_words(int nc_cap, const long long* __restrict__ cl_words, long long* __restrict__ cl_word_start,
+                             long long words_cap, int* counters)
+{
+    if (counters[kCntNeed] == 0) return;
+    const int nc = min(counters[kCntClusters], nc_cap);
+    const long long total = block_scan<long long>(nc, [&](int c) { return cl_words[c]; }, cl_word_start);
+    if (threadIdx.x == 0)
+    {
+        cl_word_start[nc] = total;
+        counters[kCntWords] = (int)(total & 0xffffffffll);
+        counters[kCntWords + 1] = (int)(total >> 32);
+        if (total > words_cap) atomicOr(&counters[kCntOverflow], kOvfWords);
+    }
+}
+
+// Per cluster (one warp): each slot's partners as 16-bit words
+// (table index << 3 | partner slot in the neighbour cluster), in table order
+// then partner order.  When the words do not fit every slot gets none
+// (flagged), so the force kernel never reads past the array.
+__global__ void k_slot_lists(int nc_cap, const int* __restrict__ nbr_start, const int2* __restrict__ nbr,
+                             const int4* __restrict__ ents, const long long* __restrict__ cl_word_start,
+                             int* __restrict__ slot_count, long long* __restrict__ slot_start,
+                             unsigned short* __restrict__ words, long long words_cap, const int* counters)
+{
+    if (counters[kCntNeed] == 0) return;
+    const bool fits = word_total(counters) <= words_cap;
+    const int lane = threadIdx.x & 31;
+    const int nc = min(counters[kCntClusters], nc_cap);
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nc; c += warps)
+    {
+        if (!fits)
+        {
+            if (lane < 8)
+            {
+                slot_count[c * kClusterSize + lane] = 0;
+                slot_start[c * kClusterSize + lane] = 0;
+            }
+            continue;
+        }
+        long long off[8];
+        long long run = cl_word_start[c];
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+        {
+            off[a] = run;
+            run += slot_count[c * kClusterSize + a];
+        }
+        if (lane < 8)
+        {
+            long long v = 0;
+#pragma unroll
+            for (int a = 0; a < 8; a++) v = (lane == a) ? off[a] : v;
+            slot_start[c * kClusterSize + lane] = v;
+        }
+        if (run == cl_word_start[c]) continue;  // no partners (also: table skipped)
+        const int base = nbr_start[c];
+        const int T = nbr_start[c + 1] - base;
+        for (int t0 = 0; t0 < T; t0 += 32)
+        {
+            const int t = t0 + lane;
+            unsigned long long m = 0;
+            int side = 0;
+            if (t < T)
+            {
+                const int2 v = nbr[base + t];
+                side = (v.y >> 29) & 3;
+                const int4 en = ents[v.x];
+                m = ((unsigned long long)(unsigned)en.w << 32) | (unsigned)en.z;
+            }
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+            {
+                unsigned m8 = t < T ? partners(m, side, a) : 0u;
+                const int n8 = __popc(m8);
+                int incl = n8;
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                long long w = off[a] + incl - n8;
+                while (m8)
+                {
+                    const int b = __ffs(m8) - 1;
+                    m8 &= m8 - 1;
+                    words[w++] = (unsigned short)((t << 3) | b);
+                }
+                off[a] += __shfl_sync(0xffffffffu, incl, 31);
+            }
+        }
+    }
+}
+
 // Reference-layout export: zero the counts, then scatter every listed pair
 // to its owner (the lower atom_local index) as the reference stores it.
 __global__ void k_export_zero(int n, spgnb_atom_group* __restrict__ nl, const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
     {
         nl[i].atom_numbers = 0;
@@ -569,21 +904,21 @@ __global__ void k_export(const int4* __restrict__ items, const int4* __restrict_
     const int total_warps = gridDim.x * (blockDim.x >> 5);
     for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += total_warps)
     {
-        int4 item = items[it];
+        const int4 item = items[it];
         const int ci = item.x;
         for (int e = item.y; e < item.y + item.z; e++)
         {
-            int4 en = ents[e];
+            const int4 en = ents[e];
             for (int h = 0; h < 2; h++)
             {
-                unsigned m = (unsigned)(h ? en.w : en.z);
+                const unsigned m = (unsigned)(h ? en.w : en.z);
                 if (!((m >> lane) & 1u)) continue;
-                int a = h * 4 + (lane >> 3), b = lane & 7;
-                int ia = slot_atom[ci * kClusterSize + a];
-                int jb = slot_atom[en.x * kClusterSize + b];
-                int owner = atom_local[ia] < atom_local[jb] ? ia : jb;
-                int other = owner == ia ? jb : ia;
-                int slot = atomicAdd(&nl[owner].atom_numbers, 1);
+                const int a = h * 4 + (lane >> 3), b = lane & 7;
+                const int ia = slot_atom[ci * kClusterSize + a];
+                const int jb = slot_atom[en.x * kClusterSize + b];
+                const int owner = atom_local[ia] < atom_local[jb] ? ia : jb;
+                const int other = owner == ia ? jb : ia;
+                const int slot = atomicAdd(&nl[owner].atom_numbers, 1);
                 if (slot < max_nb)
                     temp[(size_t)owner * max_nb + slot] = other;
                 else
@@ -596,13 +931,17 @@ __global__ void k_export(const int4* __restrict__ items, const int4* __restrict_
 __global__ void k_finish(int G, int* __restrict__ cell_count, int* __restrict__ cell_cursor, int* counters)
 {
     if (counters[kCntNeed] == 0) return;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c < G)
     {
         cell_count[c] = 0;
         cell_cursor[c] = 0;
     }
-    if (c == 0) counters[kCntBuilds] += 1;
+    if (c == 0)
+    {
+        counters[kCntBuilds] += 1;
+        counters[kCntPrune] = 1;  // the pruned lists belong to the old build
+    }
 }
 
 __global__ void k_set_need(int* counters) { counters[kCntNeed] = 1; }
@@ -617,7 +956,7 @@ __global__ void k_reset_list_counters(int* counters)
 
 __global__ void k_init_atom_groups(int n, spgnb_atom_group* nl, int* temp, int max_nb)
 {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n)
     {
         nl[i].atom_numbers = 0;
@@ -628,45 +967,44 @@ __global__ void k_init_atom_groups(int n, spgnb_atom_group* nl, int* temp, int m
 
 // --------------------------------------------------------------- host side
 
-int grid_dims(const spgnb_ltmatrix3& cell, float cutoff, float skin, int dims[3], float* gl)
+void grid_dims(const spgnb_ltmatrix3& cell, float cutoff, float skin, int dims[3], float* gl)
 {
-    float g = 0.5f * (cutoff + skin);
+    const float g = 0.5f * (cutoff + skin);
     dims[0] = (int)floorf(cell.a11 / g);
     dims[1] = (int)floorf(cell.a22 / g);
     dims[2] = (int)floorf(cell.a33 / g);
     *gl = g;
-    return SPGNB_OK;
 }
 
 // The reference's stencil rule (Find_Neighor_Grids_Device), evaluated per
 // cell by enumerating the offsets instead of the O(G^2) scan; forward and
 // reverse stencils merged with flags (bit 28: B in stencil(A), bit 29: A in
-// stencil(B)).
-int build_candidates(spgnb_nl* nl, std::vector<int>& start, std::vector<int>& cand)
+// stencil(B)).  Cell ids are global (the system's first cell added).
+int build_candidates(const SysHost& sh, std::vector<int>& start, std::vector<int>& cand)
 {
-    const int Nx = nl->dims[0], Ny = nl->dims[1], Nz = nl->dims[2];
-    const int G = nl->G;
-    const float gl = nl->grid_length;
-    const spgnb_ltmatrix3& c = nl->cell;
-    int dxy = (int)(c.a21 / gl), dxz = (int)(c.a31 / gl), dyz = (int)(c.a32 / gl);
+    const int Nx = sh.dims[0], Ny = sh.dims[1], Nz = sh.dims[2];
+    const int G = Nx * Ny * Nz;
+    const float gl = sh.gl;
+    const spgnb_ltmatrix3& c = sh.cell;
+    const int dxy = (int)(c.a21 / gl), dxz = (int)(c.a31 / gl), dyz = (int)(c.a32 / gl);
     std::vector<std::vector<int>> fwd(G);
     std::vector<int> mark(G, -1);
     for (int g = 0; g < G; g++)
     {
-        int gx = g / (Ny * Nz), gy = (g / Nz) % Ny, gz = g % Nz;
+        const int gx = g / (Ny * Nz), gy = (g / Nz) % Ny, gz = g % Nz;
         for (int k = 0; k < 27; k++)
         {
-            int dx = k / 9 - 1, dy = (k % 9) / 3 - 1, dz = k % 3 - 1;
-            int cx = (dy * c.a21 + dz * c.a31 == 0) ? -2 : -3;
-            int cy = (dz * c.a32 == 0) ? -2 : -3;
-            int sx = gx + dx * Nx + dy * dxy + dz * dxz, sy = gy + dy * Ny + dz * dyz, sz = gz + dz * Nz;
+            const int dx = k / 9 - 1, dy = (k % 9) / 3 - 1, dz = k % 3 - 1;
+            const int cx = (dy * c.a21 + dz * c.a31 == 0) ? -2 : -3;
+            const int cy = (dz * c.a32 == 0) ? -2 : -3;
+            const int sx = gx + dx * Nx + dy * dxy + dz * dxz, sy = gy + dy * Ny + dz * dyz, sz = gz + dz * Nz;
             for (int tx = cx; tx <= 2; tx++)
                 for (int ty = cy; ty <= 2; ty++)
                     for (int tz = -2; tz <= 2; tz++)
                     {
-                        int jx = sx - tx, jy = sy - ty, jz = sz - tz;
+                        const int jx = sx - tx, jy = sy - ty, jz = sz - tz;
                         if (jx < 0 || jx >= Nx || jy < 0 || jy >= Ny || jz < 0 || jz >= Nz) continue;
-                        int j = (jx * Ny + jy) * Nz + jz;
+                        const int j = (jx * Ny + jy) * Nz + jz;
                         if (mark[j] != g)
                         {
                             mark[j] = g;
@@ -681,8 +1019,6 @@ int build_candidates(spgnb_nl* nl, std::vector<int>& start, std::vector<int>& ca
     std::vector<std::vector<int>> rev(G);
     for (int g = 0; g < G; g++)
         for (int j : fwd[g]) rev[j].push_back(g);
-    start.assign(G + 1, 0);
-    cand.clear();
     std::vector<int> flag(G, 0);
     std::vector<int> touched;
     for (int g = 0; g < G; g++)
@@ -701,16 +1037,19 @@ int build_candidates(spgnb_nl* nl, std::vector<int>& start, std::vector<int>& ca
         std::sort(touched.begin(), touched.end());
         for (int j : touched)
         {
-            cand.push_back(j | ((flag[j] & 1) << 28) | ((flag[j] & 2) << 28));
+            cand.push_back((sh.cell_begin + j) | ((flag[j] & 1) << 28) | ((flag[j] & 2) << 28));
             flag[j] = 0;
         }
-        start[g + 1] = (int)cand.size();
+        start.push_back((int)cand.size());
     }
     return SPGNB_OK;
 }
 
 void free_nl(spgnb_nl* nl)
 {
+    dfree(nl->d_sys);
+    dfree(nl->d_atom_sys);
+    dfree(nl->d_cell_sys);
     dfree(nl->d_cand_start);
     dfree(nl->d_cand);
     dfree(nl->d_cell_count);
@@ -719,20 +1058,35 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_atom_cell);
     dfree(nl->d_atom_shift);
     dfree(nl->d_tmp_atoms);
+    dfree(nl->d_wrapped);
+    dfree(nl->d_atom_slot);
     dfree(nl->d_slot_atom);
     dfree(nl->d_slot_x0);
     dfree(nl->d_slot_d0);
+    dfree(nl->d_slot_count);
+    dfree(nl->d_slot_start);
     dfree(nl->d_cl_cell);
+    dfree(nl->d_cl_sys);
     dfree(nl->d_cl_u);
+    dfree(nl->d_cl_q);
     dfree(nl->d_cl_c);
+    dfree(nl->d_nbr_count);
+    dfree(nl->d_nbr_start);
+    dfree(nl->d_nbr_fill);
+    dfree(nl->d_cl_words);
+    dfree(nl->d_cl_word_start);
     dfree(nl->d_ents);
     dfree(nl->d_ents_d);
     dfree(nl->d_items);
+    dfree(nl->d_nbr);
+    dfree(nl->d_tab);
+    dfree(nl->d_words);
+    dfree(nl->d_pwords);
+    dfree(nl->d_pcount);
+    dfree(nl->d_pref);
     dfree(nl->d_counters);
-    dfree(nl->d_atom_slot);
     dfree(nl->d_nl);
     dfree(nl->d_temp);
-    dfree(nl->d_wrapped);
 }
 
 int alloc_pair_list(spgnb_nl* nl)
@@ -741,23 +1095,88 @@ int alloc_pair_list(spgnb_nl* nl)
     dfree(nl->d_ents);
     dfree(nl->d_ents_d);
     dfree(nl->d_items);
+    dfree(nl->d_nbr);
+    dfree(nl->d_tab);
     nl->entries_cap = (long long)nl->clusters_cap * nl->entries_per_cluster;
     nl->items_cap = (int)std::min<long long>(nl->entries_cap / kChunk + nl->clusters_cap + 1024, 0x7fffffffLL);
+    nl->nbr_cap = std::min<long long>(2 * nl->entries_cap, (1LL << 30) - 1);
     if ((st = dalloc(&nl->d_ents, (size_t)nl->entries_cap))) return st;
     if ((st = dalloc(&nl->d_ents_d, (size_t)nl->entries_cap))) return st;
     if ((st = dalloc(&nl->d_items, (size_t)nl->items_cap))) return st;
+    if ((st = dalloc(&nl->d_nbr, (size_t)nl->nbr_cap))) return st;
+    if ((st = dalloc(&nl->d_tab, (size_t)nl->nbr_cap))) return st;
     return SPGNB_OK;
+}
+
+int alloc_words(spgnb_nl* nl)
+{
+    dfree(nl->d_words);
+    dfree(nl->d_pwords);
+    nl->words_cap = (long long)(nl->words_per_atom * nl->n_cap) + 4096;
+    int st = dalloc(&nl->d_words, (size_t)nl->words_cap);
+    if (!st) st = dalloc(&nl->d_pwords, (size_t)nl->words_cap);
+    return st;
+}
+
+SysDesc make_desc(const SysHost& sh, float skin_permit)
+{
+    SysDesc d;
+    d.cell = make_cell(sh.cell);
+    d.rcell = make_cell(sh.rcell);
+    d.gl = sh.gl;
+    d.cs2 = sh.cs2;
+    d.list_radius = sqrtf(sh.cs2) * 1.0001f + 1e-3f;
+    d.frac_norm[0] = sqrtf(d.rcell.a11 * d.rcell.a11 + d.rcell.a21 * d.rcell.a21 + d.rcell.a31 * d.rcell.a31);
+    d.frac_norm[1] = sqrtf(d.rcell.a22 * d.rcell.a22 + d.rcell.a32 * d.rcell.a32);
+    d.frac_norm[2] = fabsf(d.rcell.a33);
+    d.Nx = sh.dims[0];
+    d.Ny = sh.dims[1];
+    d.Nz = sh.dims[2];
+    d.cell_begin = sh.cell_begin;
+    d.atom_begin = sh.atom_begin;
+    d.atom_count = sh.atom_count;
+    d.triclinic = sh.triclinic ? 1 : 0;
+    const float permit = sh.skin * skin_permit;
+    d.permit2 = permit * permit;
+    const float q = 2.384185791015625e-07f;  // 2^-22, exact scaling
+    d.qcell = Cell{d.cell.a11 * q, d.cell.a21 * q, d.cell.a22 * q, d.cell.a31 * q, d.cell.a32 * q, d.cell.a33 * q};
+    return d;
 }
 
 int alloc_nl(spgnb_nl* nl)
 {
     int st;
     const int n = nl->n_cap;
-    const int G = nl->G;
-    nl->clusters_cap = n / kClusterSize + G + 1;
+    int G = 0;
+    for (auto& sh : nl->sys)
+    {
+        sh.cell_begin = G;
+        G += sh.dims[0] * sh.dims[1] * sh.dims[2];
+    }
+    nl->G = G;
+    nl->clusters_cap = n / kClusterSize + G + nl->S + 1;
+    if ((long long)nl->clusters_cap * kClusterSize > kMaxSlots)
+        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d atoms in %d cells exceed the %d-slot limit of the lists",
+                    n, G, kMaxSlots);
     const size_t slots = (size_t)nl->clusters_cap * kClusterSize;
-    std::vector<int> start, cand;
-    if ((st = build_candidates(nl, start, cand))) return st;
+    std::vector<int> start(1, 0), cand;
+    for (auto& sh : nl->sys)
+        if ((st = build_candidates(sh, start, cand))) return st;
+    nl->h_desc.resize(nl->S);
+    std::vector<int> atom_sys(n, 0), cell_sys(G, 0);
+    for (int s = 0; s < nl->S; s++)
+    {
+        const SysHost& sh = nl->sys[s];
+        nl->h_desc[s] = make_desc(sh, nl->opt.skin_permit);
+        for (int i = sh.atom_begin; i < sh.atom_begin + sh.atom_count && i < n; i++) atom_sys[i] = s;
+        for (int c = 0; c < sh.dims[0] * sh.dims[1] * sh.dims[2]; c++) cell_sys[sh.cell_begin + c] = s;
+    }
+    if ((st = dalloc(&nl->d_sys, nl->S))) return st;
+    if ((st = dalloc(&nl->d_atom_sys, n))) return st;
+    if ((st = dalloc(&nl->d_cell_sys, G))) return st;
+    SPGNB_CUDA(cudaMemcpy(nl->d_sys, nl->h_desc.data(), sizeof(SysDesc) * nl->S, cudaMemcpyHostToDevice));
+    SPGNB_CUDA(cudaMemcpy(nl->d_atom_sys, atom_sys.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    SPGNB_CUDA(cudaMemcpy(nl->d_cell_sys, cell_sys.data(), sizeof(int) * G, cudaMemcpyHostToDevice));
     if ((st = dalloc(&nl->d_cand_start, G + 1))) return st;
     if ((st = dalloc(&nl->d_cand, cand.size()))) return st;
     SPGNB_CUDA(cudaMemcpy(nl->d_cand_start, start.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice));
@@ -774,14 +1193,31 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemset(nl->d_atom_slot, 0xff, sizeof(int) * n));
     if ((st = dalloc(&nl->d_tmp_atoms, slots))) return st;
     if ((st = dalloc(&nl->d_slot_atom, slots))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_slot_atom, 0xff, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_slot_x0, slots))) return st;
     if ((st = dalloc(&nl->d_slot_d0, slots))) return st;
+    if ((st = dalloc(&nl->d_slot_count, slots))) return st;
+    if ((st = dalloc(&nl->d_slot_start, slots))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_slot_count, 0, sizeof(int) * slots));
+    SPGNB_CUDA(cudaMemset(nl->d_slot_start, 0, sizeof(long long) * slots));
+    if ((st = dalloc(&nl->d_pcount, slots))) return st;
+    if ((st = dalloc(&nl->d_pref, slots))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_pcount, 0, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_cl_cell, nl->clusters_cap))) return st;
+    if ((st = dalloc(&nl->d_cl_sys, nl->clusters_cap))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_cl_sys, 0, sizeof(int) * nl->clusters_cap));
     if ((st = dalloc(&nl->d_cl_u, nl->clusters_cap))) return st;
+    if ((st = dalloc(&nl->d_cl_q, nl->clusters_cap))) return st;
     if ((st = dalloc(&nl->d_cl_c, nl->clusters_cap))) return st;
+    if ((st = dalloc(&nl->d_nbr_count, nl->clusters_cap))) return st;
+    if ((st = dalloc(&nl->d_nbr_fill, nl->clusters_cap))) return st;
+    if ((st = dalloc(&nl->d_nbr_start, nl->clusters_cap + 1))) return st;
+    if ((st = dalloc(&nl->d_cl_words, nl->clusters_cap + 1))) return st;
+    if ((st = dalloc(&nl->d_cl_word_start, nl->clusters_cap + 1))) return st;
     if ((st = dalloc(&nl->d_counters, kCntSize))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_counters, 0, sizeof(int) * kCntSize));
     if ((st = alloc_pair_list(nl))) return st;
+    if ((st = alloc_words(nl))) return st;
     if (nl->opt.export_atom_groups)
     {
         if ((st = dalloc(&nl->d_nl, n))) return st;
@@ -793,18 +1229,212 @@ int alloc_nl(spgnb_nl* nl)
     return SPGNB_OK;
 }
 
-int estimate_entries_per_cluster(const spgnb_nl* nl)
+// Capacities from the densest system: cluster pairs within rc + skin + 6 A
+// per 8-atom cluster (half list, 2x margin), and listed partners per atom
+// within rc + skin (full list, 1.5x margin).
+void estimate_capacities(spgnb_nl* nl)
 {
-    if (nl->opt.max_entries_per_cluster > 0) return nl->opt.max_entries_per_cluster;
-    double vol = (double)nl->cell.a11 * nl->cell.a22 * nl->cell.a33;
-    double rho = nl->n_cap / vol;
-    double R = nl->cutoff + nl->skin + 6.0;
-    double per = 4.18879 * R * R * R * rho / kClusterSize;  // clusters within R
-    int e = (int)(per * 0.5 * 2.0) + 64;                     // half list, 2x margin
-    return std::max(e, 96);
+    double per_cluster = 0, per_atom = 0;
+    for (const auto& sh : nl->sys)
+    {
+        const double vol = (double)sh.cell.a11 * sh.cell.a22 * sh.cell.a33;
+        const double rho = sh.atom_count / vol;
+        const double R = sh.cutoff + sh.skin + 6.0;
+        per_cluster = std::max(per_cluster, 4.18879 * R * R * R * rho / kClusterSize);
+        const double Rl = sh.cutoff + sh.skin;
+        per_atom = std::max(per_atom, std::min(4.18879 * Rl * Rl * Rl * rho, (double)sh.atom_count));
+    }
+    nl->entries_per_cluster = nl->opt.max_entries_per_cluster > 0 ? nl->opt.max_entries_per_cluster
+                                                                  : std::max((int)per_cluster + 64, 96);
+    nl->words_per_atom = per_atom * 1.5 + 64;
 }
 
 }  // namespace
+
+int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,
+                    const spgnb_ltmatrix3* rcells, const float* cutoffs, const float* skins,
+                    const spgnb_nl_options* opt, spgnb_nl** out)
+{
+    *out = nullptr;
+    if (n_systems <= 0) return fail(SPGNB_E_ARG, "neighbour list: no systems");
+    spgnb_nl* nl = new spgnb_nl();
+    if (opt)
+        nl->opt = *opt;
+    else
+        spgnb_nl_default_options(&nl->opt);
+    if (nl->opt.max_neighbor_numbers <= 0) nl->opt.max_neighbor_numbers = 1200;
+    if (!(nl->opt.prune_buffer >= 0.0f)) nl->opt.prune_buffer = 0.0f;
+    nl->S = n_systems;
+    nl->sys.resize(n_systems);
+    long long begin = 0;
+    for (int s = 0; s < n_systems; s++)
+    {
+        SysHost& sh = nl->sys[s];
+        if (atom_counts[s] <= 0 || !(cutoffs[s] > 0.0f) || !(skins[s] >= 0.0f) ||
+            !(cells[s].a11 > 0.0f && cells[s].a22 > 0.0f && cells[s].a33 > 0.0f))
+        {
+            delete nl;
+            return fail(SPGNB_E_ARG, "neighbour list: system %d has bad atoms/cutoff/skin/cell", s);
+        }
+        sh.atom_begin = (int)begin;
+        sh.atom_count = atom_counts[s];
+        begin += atom_counts[s];
+        sh.cell = cells[s];
+        sh.rcell = rcells[s];
+        sh.cutoff = cutoffs[s];
+        sh.skin = skins[s];
+        sh.triclinic = cells[s].a21 != 0.0f || cells[s].a31 != 0.0f || cells[s].a32 != 0.0f;
+        grid_dims(cells[s], cutoffs[s], skins[s], sh.dims, &sh.gl);
+        sh.cs2 = sh.gl * sh.gl * 4.0f;
+        if (sh.dims[0] <= 2 || sh.dims[1] <= 2 || sh.dims[2] <= 2)
+        {
+            const int d0 = sh.dims[0], d1 = sh.dims[1], d2 = sh.dims[2];
+            delete nl;
+            return fail(SPGNB_E_ARG,
+                        "NEIGHBOR_LIST: the box is too small (system %d: grid %dx%dx%d, need >= 3 per dimension)", s,
+                        d0, d1, d2);
+        }
+    }
+    if (begin > (1LL << 28))
+    {
+        delete nl;
+        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %lld atoms exceed the 2^28 limit", begin);
+    }
+    nl->n_cap = (int)begin;
+    nl->cutoff = nl->sys[0].cutoff;
+    nl->skin = nl->sys[0].skin;
+    nl->grid_length = nl->sys[0].gl;
+    nl->cs2 = nl->sys[0].cs2;
+    nl->cell = nl->sys[0].cell;
+    nl->rcell = nl->sys[0].rcell;
+    nl->triclinic = nl->sys[0].triclinic;
+    memcpy(nl->dims, nl->sys[0].dims, sizeof(nl->dims));
+    estimate_capacities(nl);
+    const int st = alloc_nl(nl);
+    if (st)
+    {
+        free_nl(nl);
+        delete nl;
+        return st;
+    }
+    *out = nl;
+    return SPGNB_OK;
+}
+
+// Queues one rebuild, or the device-side decision about one, on stream s.
+// host_rebuild: rebuild unconditionally; otherwise the skin check decides.
+int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
+                   const int* ex_list, const int* ex_num, bool host_rebuild, cudaStream_t s)
+{
+    const int sms = num_sms();
+    const int slots_cap = nl->clusters_cap * kClusterSize;
+    const int ccap = nl->clusters_cap;
+    if (host_rebuild)
+    {
+        k_set_need<<<1, 1, 0, s>>>(nl->d_counters);
+        SPGNB_CHECK_LAUNCH("k_set_need");
+    }
+    else
+    {
+        SPGNB_CUDA(cudaMemsetAsync(nl->d_counters + kCntNeed, 0, sizeof(int), s));
+        k_check_refresh<<<(slots_cap + 255) / 256, 256, 0, s>>>(slots_cap, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
+                                                                  d_crd, nl->d_slot_x0, nl->d_counters);
+        SPGNB_CHECK_LAUNCH("k_check_refresh");
+    }
+    k_reset_list_counters<<<1, 1, 0, s>>>(nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_reset_list_counters");
+    k_bin<<<(n + 255) / 256, 256, 0, s>>>(n, d_crd, nl->d_atom_sys, nl->d_sys, nl->d_atom_cell, nl->d_atom_shift,
+                                            nl->d_wrapped, nl->d_cell_count, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_bin");
+    k_scan_cells<<<1, 1024, 0, s>>>(nl->G, nl->d_cell_count, nl->d_cell_cl_start, nl->opt.max_atom_in_grid_numbers,
+                                     nl->clusters_cap, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_scan_cells");
+    k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_atom_cell, nl->d_cell_cl_start, nl->d_cell_cursor,
+                                                nl->d_tmp_atoms, slots_cap, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_scatter");
+    k_sort_cells<<<std::min(nl->G, sms * 16), 128, kMaxCellAtoms * sizeof(unsigned long long), s>>>(
+        nl->G, nl->d_cell_sys, nl->d_sys, nl->d_cell_count, nl->d_cell_cl_start, nl->d_tmp_atoms, nl->d_wrapped,
+        nl->d_slot_atom, nl->d_cl_cell, nl->d_cl_sys, nl->d_atom_slot, slots_cap, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_sort_cells");
+    k_cluster_props<<<(slots_cap + 255) / 256, 256, 0, s>>>(d_crd, nl->d_slot_atom, nl->d_atom_shift, d_atom_local,
+                                                             nl->d_cl_sys, nl->d_sys, nl->d_counters, nl->d_cl_u,
+                                                             nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0,
+                                                             ccap);
+    SPGNB_CHECK_LAUNCH("k_cluster_props");
+    const int search_blocks = std::min((ccap + kSearchWarps - 1) / kSearchWarps, sms * 8);
+    k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
+        nl->d_sys, nl->entries_cap, nl->items_cap, nl->d_cand_start, nl->d_cand, nl->d_cell_cl_start, nl->d_cl_cell,
+        nl->d_cl_sys, nl->d_cl_u, nl->d_slot_x0, ex_start, ex_list, ex_num, nl->d_ents, nl->d_ents_d, nl->d_items,
+        nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_search");
+    k_zero_tables<<<(ccap + 255) / 256, 256, 0, s>>>(ccap, nl->d_nbr_count, nl->d_nbr_fill, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_zero_tables");
+    k_nbr_count<<<sms * 8, 128, 0, s>>>(nl->d_items, nl->d_ents, nl->items_cap, nl->d_nbr_count, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_nbr_count");
+    k_scan_nbr<<<1, 1024, 0, s>>>(ccap, nl->d_nbr_count, nl->d_nbr_start, nl->nbr_cap, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_scan_nbr");
+    k_nbr_fill<<<sms * 8, 128, 0, s>>>(nl->d_items, nl->d_ents, nl->items_cap, nl->d_nbr_start, nl->d_nbr_fill,
+                                        nl->d_nbr, nl->nbr_cap, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_nbr_fill");
+    const int table_blocks = std::max(1, std::min((ccap + kTabWarps - 1) / kTabWarps, sms * 8));
+    k_nbr_table<<<table_blocks, kTabWarps * 32, 0, s>>>(ccap, nl->d_nbr_start, nl->d_nbr, nl->nbr_cap, nl->d_ents,
+                                                         nl->d_ents_d, nl->d_tab, nl->d_slot_count, nl->d_cl_words,
+                                                         nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_nbr_table");
+    k_scan_words<<<1, 1024, 0, s>>>(ccap, nl->d_cl_words, nl->d_cl_word_start, nl->words_cap, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_scan_words");
+    k_slot_lists<<<std::max(1, std::min((ccap + 3) / 4, sms * 8)), 128, 0, s>>>(
+        ccap, nl->d_nbr_start, nl->d_nbr, nl->d_ents, nl->d_cl_word_start, nl->d_slot_count, nl->d_slot_start,
+        nl->d_words, nl->words_cap, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_slot_lists");
+    if (nl->opt.export_atom_groups)
+    {
+        k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
+        SPGNB_CHECK_LAUNCH("k_export_zero");
+        k_export<<<sms * 8, 128, 0, s>>>(nl->d_items, nl->d_ents, nl->d_slot_atom, d_atom_local, nl->d_nl,
+                                          nl->d_temp, nl->opt.max_neighbor_numbers, nl->d_counters, nl->items_cap);
+        SPGNB_CHECK_LAUNCH("k_export");
+    }
+    k_finish<<<(nl->G + 255) / 256, 256, 0, s>>>(nl->G, nl->d_cell_count, nl->d_cell_cursor, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_finish");
+    nl->built = true;
+    nl->local_atoms = n;
+    nl->host_builds++;
+    return SPGNB_OK;
+}
+
+// Regrows what overflowed (1.1x, as neighbor_list.cpp:896-941 does) and
+// clears the flags; the caller forces the next build.
+int nl_regrow(spgnb_nl* nl, int flags)
+{
+    int st;
+    if (flags & kOvfGrid) nl->opt.max_atom_in_grid_numbers = (int)(nl->opt.max_atom_in_grid_numbers * 1.1) + 1;
+    if (flags & kOvfList)
+    {
+        nl->opt.max_neighbor_numbers = (int)(nl->opt.max_neighbor_numbers * 1.1) + 1;
+        dfree(nl->d_nl);
+        dfree(nl->d_temp);
+        if ((st = dalloc(&nl->d_nl, nl->n_cap))) return st;
+        if ((st = dalloc(&nl->d_temp, (size_t)nl->n_cap * nl->opt.max_neighbor_numbers))) return st;
+        k_init_atom_groups<<<(nl->n_cap + 255) / 256, 256, 0, stream()>>>(nl->n_cap, nl->d_nl, nl->d_temp,
+                                                                         nl->opt.max_neighbor_numbers);
+        SPGNB_CHECK_LAUNCH("k_init_atom_groups");
+    }
+    if (flags & kOvfPairs)
+    {
+        nl->entries_per_cluster = (int)(nl->entries_per_cluster * 1.1) + 8;
+        if ((st = alloc_pair_list(nl))) return st;
+    }
+    if (flags & kOvfWords)
+    {
+        nl->words_per_atom = nl->words_per_atom * 1.1 + 8;
+        if ((st = alloc_words(nl))) return st;
+    }
+    SPGNB_CUDA(cudaMemsetAsync(nl->d_counters + kCntOverflow, 0, sizeof(int), stream()));
+    nl->built = false;
+    return SPGNB_OK;
+}
+
 }  // namespace spgnb
 
 using namespace spgnb;
@@ -823,6 +1453,7 @@ void spgnb_nl_default_options(spgnb_nl_options* o)
     o->throw_error_when_overflow = 0;
     o->export_atom_groups = 1;
     o->max_entries_per_cluster = 0;
+    o->prune_buffer = 1.0f;
 }
 
 int spgnb_nl_create(int atom_numbers, float cutoff, float skin, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
@@ -834,38 +1465,7 @@ int spgnb_nl_create(int atom_numbers, float cutoff, float skin, spgnb_ltmatrix3 
     if (!(cutoff > 0.0f) || !(skin >= 0.0f)) return fail(SPGNB_E_ARG, "spgnb_nl_create: bad cutoff/skin");
     if (!(cell.a11 > 0.0f && cell.a22 > 0.0f && cell.a33 > 0.0f))
         return fail(SPGNB_E_ARG, "spgnb_nl_create: cell diagonal must be positive");
-    spgnb_nl* nl = new spgnb_nl();
-    if (opt)
-        nl->opt = *opt;
-    else
-        spgnb_nl_default_options(&nl->opt);
-    if (nl->opt.max_neighbor_numbers <= 0) nl->opt.max_neighbor_numbers = 1200;
-    nl->n_cap = atom_numbers;
-    nl->cutoff = cutoff;
-    nl->skin = skin;
-    nl->cell = cell;
-    nl->rcell = rcell;
-    nl->triclinic = cell.a21 != 0.0f || cell.a31 != 0.0f || cell.a32 != 0.0f;
-    grid_dims(cell, cutoff, skin, nl->dims, &nl->grid_length);
-    nl->cs2 = nl->grid_length * nl->grid_length * 4.0f;
-    if (nl->dims[0] <= 2 || nl->dims[1] <= 2 || nl->dims[2] <= 2)
-    {
-        delete nl;
-        return fail(SPGNB_E_ARG, "NEIGHBOR_LIST: the box is too small (grid %dx%dx%d, need >= 3 per dimension)",
-                    (int)floorf(cell.a11 / (0.5f * (cutoff + skin))), (int)floorf(cell.a22 / (0.5f * (cutoff + skin))),
-                    (int)floorf(cell.a33 / (0.5f * (cutoff + skin))));
-    }
-    nl->G = nl->dims[0] * nl->dims[1] * nl->dims[2];
-    nl->entries_per_cluster = estimate_entries_per_cluster(nl);
-    int st = alloc_nl(nl);
-    if (st)
-    {
-        free_nl(nl);
-        delete nl;
-        return st;
-    }
-    *out = nl;
-    return SPGNB_OK;
+    return nl_create_multi(1, &atom_numbers, &cell, &rcell, &cutoff, &skin, opt, out);
 }
 
 int spgnb_nl_update(spgnb_nl* nl, const int* d_atom_local, int local_atom_numbers, int ghost_numbers,
@@ -874,6 +1474,7 @@ int spgnb_nl_update(spgnb_nl* nl, const int* d_atom_local, int local_atom_number
 {
     if (!nl) return fail(SPGNB_E_ARG, "spgnb_nl_update: nl is NULL");
     if (local_atom_numbers <= 0 && ghost_numbers <= 0) return SPGNB_OK;
+    if (nl->S != 1) return fail(SPGNB_E_STATE, "spgnb_nl_update: the list holds several systems");
     if (ghost_numbers != 0)
         return fail(SPGNB_E_UNSUPPORTED, "spgnb_nl_update: ghost atoms (multi-rank domain decomposition) are not "
                                          "supported; run one rank per system");
@@ -882,97 +1483,43 @@ int spgnb_nl_update(spgnb_nl* nl, const int* d_atom_local, int local_atom_number
                     local_atom_numbers, nl->n_cap);
     if (!d_atom_local || !d_crd || !d_excluded_list_start || !d_excluded_list || !d_excluded_numbers)
         return fail(SPGNB_E_ARG, "spgnb_nl_update: NULL device pointer");
+    cudaStream_t s = stream();
+    bool box_changed = false;
     if (memcmp(&cell, &nl->cell, sizeof(cell)) != 0)
     {
         // The reference re-initialises on a large box change (main.cpp:864-939);
-        // here the grid follows the new box when its shape allows.
+        // here the grid follows the new box when its shape allows, and the
+        // list is rebuilt (the stored centre differences belong to the old box).
         int dims[3];
         float gl;
         grid_dims(cell, nl->cutoff, nl->skin, dims, &gl);
         if (dims[0] != nl->dims[0] || dims[1] != nl->dims[1] || dims[2] != nl->dims[2])
             return fail(SPGNB_E_STATE, "spgnb_nl_update: the box changed the grid; recreate the list");
+        SysHost& sh = nl->sys[0];
+        sh.cell = cell;
+        sh.rcell = rcell;
+        sh.gl = gl;
+        sh.cs2 = gl * gl * 4.0f;
+        sh.triclinic = cell.a21 != 0.0f || cell.a31 != 0.0f || cell.a32 != 0.0f;
         nl->cell = cell;
         nl->rcell = rcell;
         nl->grid_length = gl;
-        nl->cs2 = gl * gl * 4.0f;
+        nl->cs2 = sh.cs2;
+        nl->triclinic = sh.triclinic;
+        nl->h_desc[0] = make_desc(sh, nl->opt.skin_permit);
+        SPGNB_CUDA(cudaMemcpyAsync(nl->d_sys, nl->h_desc.data(), sizeof(SysDesc), cudaMemcpyHostToDevice, s));
+        box_changed = true;
     }
-    cudaStream_t s = stream();
-    const Cell c = make_cell(cell), rc = make_cell(rcell);
     const bool host_knows = update == SPGNB_FORCED_UPDATE || !nl->built || nl->opt.refresh_interval > 0 ||
-                            local_atom_numbers != nl->local_atoms;
+                            local_atom_numbers != nl->local_atoms || box_changed;
     if (host_knows)
     {
-        bool rebuild = update == SPGNB_FORCED_UPDATE || !nl->built || local_atom_numbers != nl->local_atoms ||
-                       ((step + 1) % nl->opt.refresh_interval == 0);
+        const bool rebuild = update == SPGNB_FORCED_UPDATE || !nl->built || local_atom_numbers != nl->local_atoms ||
+                             box_changed || ((step + 1) % nl->opt.refresh_interval == 0);
         if (!rebuild) return SPGNB_OK;
-        k_set_need<<<1, 1, 0, s>>>(nl->d_counters);
-        SPGNB_CHECK_LAUNCH("k_set_need");
     }
-    else
-    {
-        SPGNB_CUDA(cudaMemsetAsync(nl->d_counters + kCntNeed, 0, sizeof(int), s));
-        float permit = nl->skin * nl->opt.skin_permit;
-        int slots = nl->clusters_cap * kClusterSize;
-        k_check_refresh<<<(slots + 255) / 256, 256, 0, s>>>(slots, nl->d_slot_atom, (const float3*)d_crd,
-                                                              nl->d_slot_x0, c, rc, permit * permit,
-                                                              nl->d_counters);
-        SPGNB_CHECK_LAUNCH("k_check_refresh");
-    }
-    const int n = local_atom_numbers;
-    Grid g{nl->dims[0], nl->dims[1], nl->dims[2], nl->G, nl->grid_length, nl->cs2, c, rc};
-    k_reset_list_counters<<<1, 1, 0, s>>>(nl->d_counters);
-    k_bin<<<(n + 255) / 256, 256, 0, s>>>(n, (const float3*)d_crd, g, nl->d_atom_cell, nl->d_atom_shift,
-                                            nl->d_wrapped, nl->d_cell_count, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_bin");
-    k_scan_cells<<<1, 1024, 0, s>>>(nl->G, nl->d_cell_count, nl->d_cell_cl_start,
-                                     nl->opt.max_atom_in_grid_numbers, nl->clusters_cap, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_scan_cells");
-    const int slots_cap = nl->clusters_cap * kClusterSize;
-    k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_atom_cell, nl->d_cell_cl_start, nl->d_cell_cursor,
-                                                nl->d_tmp_atoms, slots_cap, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_scatter");
-    int sort_blocks = std::min(nl->G, num_sms() * 16);
-    k_sort_cells<<<sort_blocks, 128, 2048 * sizeof(unsigned long long), s>>>(
-        g, nl->d_cell_count, nl->d_cell_cl_start, nl->d_tmp_atoms, nl->d_wrapped, nl->d_slot_atom,
-        nl->d_cl_cell, nl->d_atom_slot, slots_cap, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_sort_cells");
-    k_cluster_props<<<(slots_cap + 255) / 256, 256, 0, s>>>((const float3*)d_crd, nl->d_slot_atom,
-                                                             nl->d_atom_shift, d_atom_local, c, nl->d_counters,
-                                                             nl->d_cl_u,
-                                                             nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0,
-                                                             nl->clusters_cap);
-    SPGNB_CHECK_LAUNCH("k_cluster_props");
-    SearchParams sp;
-    sp.g = g;
-    sp.list_radius = sqrtf(nl->cs2) * 1.0001f + 1e-3f;
-    sp.frac_norm[0] = sqrtf(rc.a11 * rc.a11 + rc.a21 * rc.a21 + rc.a31 * rc.a31);
-    sp.frac_norm[1] = sqrtf(rc.a22 * rc.a22 + rc.a32 * rc.a32);
-    sp.frac_norm[2] = fabsf(rc.a33);
-    sp.triclinic = nl->triclinic ? 1 : 0;
-    sp.entries_cap = nl->entries_cap;
-    sp.items_cap = nl->items_cap;
-    sp.clusters_cap = nl->clusters_cap;
-    int search_blocks = std::min((nl->clusters_cap + kSearchWarps - 1) / kSearchWarps, num_sms() * 8);
-    k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
-        sp, nl->d_cand_start, nl->d_cand, nl->d_cell_cl_start, nl->d_cl_cell, nl->d_cl_u, nl->d_slot_x0,
-        d_excluded_list_start, d_excluded_list, d_excluded_numbers,
-        nl->d_ents, nl->d_ents_d, nl->d_items, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_search");
-    if (nl->opt.export_atom_groups)
-    {
-        k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
-        SPGNB_CHECK_LAUNCH("k_export_zero");
-        k_export<<<num_sms() * 8, 128, 0, s>>>(nl->d_items, nl->d_ents, nl->d_slot_atom, d_atom_local, nl->d_nl,
-                                                nl->d_temp, nl->opt.max_neighbor_numbers, nl->d_counters,
-                                                nl->items_cap);
-        SPGNB_CHECK_LAUNCH("k_export");
-    }
-    k_finish<<<(nl->G + 255) / 256, 256, 0, s>>>(nl->G, nl->d_cell_count, nl->d_cell_cursor, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_finish");
-    nl->built = true;
-    nl->local_atoms = local_atom_numbers;
-    nl->host_builds++;
-    return SPGNB_OK;
+    return nl_queue_build(nl, local_atom_numbers, (const float3*)d_crd, d_atom_local, d_excluded_list_start,
+                          d_excluded_list, d_excluded_numbers, host_knows, s);
 }
 
 int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out)
@@ -993,12 +1540,17 @@ int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out)
     out->work_items = h[kCntItems];
     out->builds = h[kCntBuilds];
     out->overflow = h[kCntOverflow];
+    out->full_list_words = ((long long)h[kCntWords + 1] << 32) | (unsigned)h[kCntWords];
+    out->prunes = h[kCntPrunes];
+    memcpy(&out->pruned_list_words, &h[kCntPWordsLast], sizeof(long long));
     return SPGNB_OK;
 }
 
 int spgnb_nl_check_overflow(spgnb_nl* nl, int steps, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell,
                             int* reinitialized)
 {
+    (void)cell;
+    (void)rcell;
     if (!nl) return fail(SPGNB_E_ARG, "spgnb_nl_check_overflow: nl is NULL");
     if (reinitialized) *reinitialized = 0;
     if (nl->opt.check_overflow_interval > 0 && (steps + 1) % nl->opt.check_overflow_interval != 0)
@@ -1012,34 +1564,15 @@ int spgnb_nl_check_overflow(spgnb_nl* nl, int steps, spgnb_ltmatrix3 cell, spgnb
         return fail(SPGNB_E_OVERFLOW, "NEIGHBOR_LIST::Check_Overflow: overflow occurred in neighbor searching "
                                       "(flags 0x%x)",
                     flags);
-    // Regrow by 1.1x as the reference does (neighbor_list.cpp:896-941) and
-    // force a rebuild on the next update.
-    if (flags & kOvfGrid) nl->opt.max_atom_in_grid_numbers = (int)(nl->opt.max_atom_in_grid_numbers * 1.1);
-    if (flags & kOvfList)
-    {
-        nl->opt.max_neighbor_numbers = (int)(nl->opt.max_neighbor_numbers * 1.1);
-        dfree(nl->d_nl);
-        dfree(nl->d_temp);
-        int st;
-        if ((st = dalloc(&nl->d_nl, nl->n_cap))) return st;
-        if ((st = dalloc(&nl->d_temp, (size_t)nl->n_cap * nl->opt.max_neighbor_numbers))) return st;
-        k_init_atom_groups<<<(nl->n_cap + 255) / 256, 256, 0, stream()>>>(nl->n_cap, nl->d_nl, nl->d_temp,
-                                                                         nl->opt.max_neighbor_numbers);
-        SPGNB_CHECK_LAUNCH("k_init_atom_groups");
-    }
-    if (flags & kOvfPairs)
-    {
-        nl->entries_per_cluster = (int)(nl->entries_per_cluster * 1.1) + 8;
-        int st = alloc_pair_list(nl);
-        if (st) return st;
-    }
-    if (memcmp(&cell, &nl->cell, sizeof(cell)) != 0)
-    {
-        nl->cell = cell;
-        nl->rcell = rcell;
-    }
-    SPGNB_CUDA(cudaMemsetAsync(nl->d_counters + kCntOverflow, 0, sizeof(int), stream()));
-    nl->built = false;
+    if (flags & kOvfCellHard)
+        return fail(SPGNB_E_UNSUPPORTED, "NEIGHBOR_LIST: a grid cell holds more than %d atoms", kMaxCellAtoms);
+    if (flags & kOvfTable)
+        return fail(SPGNB_E_UNSUPPORTED,
+                    "NEIGHBOR_LIST: a cluster has more than %d neighbour clusters (cutoff too large for the "
+                    "cluster tables)",
+                    kSortCap);
+    int st = nl_regrow(nl, flags);
+    if (st) return st;
     if (reinitialized) *reinitialized = 1;
     return SPGNB_OK;
 }
@@ -1078,7 +1611,7 @@ int spgnb_nl_copy_atom_groups(spgnb_nl* nl, int* h_counts, int* h_lists, long lo
         long long off = 0;
         for (int i = 0; i < n; i++)
         {
-            int c = std::min(h[i].atom_numbers, m);
+            const int c = std::min(h[i].atom_numbers, m);
             memcpy(h_lists + off, slab.data() + (size_t)i * m, sizeof(int) * c);
             off += h[i].atom_numbers;
         }

@@ -6,8 +6,10 @@
 //   F/r = (B - A r^-6) r^-8 - q_i q_j [r^-3 - beta^3 K(beta^2 r^2)]
 //   E_lj = (A/12 r^-6 - B/6) r^-6,  E_c = q_i q_j [r^-1 - beta M(beta^2 r^2)]
 // where K, M are the smooth parts of the screened Coulomb kernels
-// (ewald_fit.h).  The force on atoms accumulates in int64 fixed point, the
-// energy/virial totals too, so neither depends on summation order.
+// (ewald_fit.h).  Over an spgnb list every atom is one warp walking its full
+// partner list, so its force is complete in registers and written once, with
+// no atomics; energy/virial totals accumulate in int64 fixed point.  Over a
+// reference-layout (half) list the force accumulates in int64 fixed point.
 #include <math.h>
 #include <string.h>
 
@@ -21,18 +23,10 @@ namespace spgnb
 namespace
 {
 
-constexpr int kPairWarps = 4;  // warps per block of the cluster-pair kernel
+constexpr int kForceWarps = 8;  // warps per block of the full-list kernel: one cluster per block pass
 constexpr float kTwoPow32 = 4294967296.0f;
 
-struct PairConst
-{
-    float rc2;
-    float beta;
-    float beta3;
-    float w_scale;  // beta^2 / W_MAX
-    int n_types;
-    int use_fit;    // beta*rc inside the fitted range
-};
+using PairConst = ForceParams;
 
 __device__ __forceinline__ float poly5(float x, const float* c)
 {
@@ -45,7 +39,9 @@ __device__ __forceinline__ float poly5(float x, const float* c)
 }
 
 // Scalar pair force F/r (and energies when requested) for r2 > 0.
-template <bool ENERGY>
+// FIT: 1 the rational fits (beta*rc inside their range), 0 erfcf/expf,
+// 2 chosen at run time from pc.use_fit.
+template <bool ENERGY, int FIT = 2>
 __device__ __forceinline__ float pair_scalar(float r2, float qq, float A, float B, const PairConst& pc,
                                              float& e_lj, float& e_c)
 {
@@ -55,7 +51,7 @@ __device__ __forceinline__ float pair_scalar(float r2, float qq, float A, float 
     const float r6inv = r2inv * r2inv * r2inv;
     const float flj = __fmaf_rn(-A, r6inv, B) * r6inv * r2inv;
     float fc;
-    if (pc.use_fit)
+    if (FIT == 1 || (FIT == 2 && pc.use_fit))
     {
         const float x = r2 * pc.w_scale;
         const float K = __fdividef(poly5(x, kEwaldKP), poly5(x, kEwaldKQ));
@@ -103,369 +99,447 @@ struct PerAtomOut
     float* virial;       // caller's LTMatrix3 array (+=), 6 floats per atom
 };
 
-// per-step slot pack: offsets from the build-time cluster centre moved by the
-// displacement since the build (minimum image, so a caller that wraps
-// coordinates between builds is fine), with the charge.
-__global__ void k_pack_slots(int slots_cap, const int* __restrict__ counters, const int* __restrict__ slot_atom,
+// Per-step slot pack: offsets from the build-time cluster centre moved by the
+// displacement since the build (minimum image in the system's box, so a
+// caller that wraps coordinates between builds is fine), with the charge.
+// With pruning on (pref set) it also flags a re-pruning when some atom moved
+// more than half the prune buffer since the last one.
+__global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict__ slot_atom,
+                             const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
                              const float4* __restrict__ x0, const float4* __restrict__ d0,
                              const float3* __restrict__ crd, const float* __restrict__ charge,
-                             const int* __restrict__ local_type, Cell cell, Cell rcell, float4* __restrict__ pos,
-                             int* __restrict__ ptype)
+                             const int* __restrict__ local_type, float4* __restrict__ pos, int* __restrict__ ptype,
+                             const float4* __restrict__ pref, float half_buffer2)
 {
-    int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= slots_cap || s >= counters[kCntClusters] * kClusterSize) return;
-    int a = slot_atom[s];
-    float4 d = d0[s];
-    if (a < 0)
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    bool moved = false;
+    if (s < slots_cap && s < counters[kCntClusters] * kClusterSize)
     {
-        pos[s] = make_float4(d.x, d.y, d.z, 0.0f);
-        ptype[s] = 0;
-        return;
+        const int a = slot_atom[s];
+        const float4 d = d0[s];
+        if (a < 0)
+        {
+            pos[s] = make_float4(d.x, d.y, d.z, 0.0f);
+            ptype[s] = 0;
+        }
+        else
+        {
+            const SysDesc& D = sys[cl_sys[s >> 3]];
+            const float3 c = crd[a];
+            const float4 o = x0[s];
+            float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+            const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
+            const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
+            const float sz = rintf(dz * D.rcell.a33);
+            dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
+            dy -= sy * D.cell.a22 + sz * D.cell.a32;
+            dz -= sz * D.cell.a33;
+            const float4 p = make_float4(d.x + dx, d.y + dy, d.z + dz, charge[a]);
+            pos[s] = p;
+            ptype[s] = local_type[a];
+            if (pref)
+            {
+                const float4 r = pref[s];
+                const float ex = p.x - r.x, ey = p.y - r.y, ez = p.z - r.z;
+                moved = ex * ex + ey * ey + ez * ez > half_buffer2;
+            }
+        }
     }
-    float3 c = crd[a];
-    float4 o = x0[s];
-    float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
-    float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
-    float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
-    float sz = rintf(dz * rcell.a33);
-    dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
-    dy -= sy * cell.a22 + sz * cell.a32;
-    dz -= sz * cell.a33;
-    pos[s] = make_float4(d.x + dx, d.y + dy, d.z + dz, charge[a]);
-    ptype[s] = local_type[a];
+    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicExch(&counters[kCntPrune], 1);
 }
 
-// Symmetrised virial increment -(f (x) d) in the LTMatrix3 order a11, a21,
-// a22, a31, a32, a33 (Get_Virial_From_Force_Dis, vector.hpp:336-347).
-__device__ __forceinline__ void add_outer(float* v, float fx, float fy, float fz, float dx, float dy, float dz,
-                                          float sign)
-{
-    v[0] = __fmaf_rn(sign * fx, dx, v[0]);
-    v[1] = __fmaf_rn(sign * fx, dy, __fmaf_rn(sign * fy, dx, v[1]));
-    v[2] = __fmaf_rn(sign * fy, dy, v[2]);
-    v[3] = __fmaf_rn(sign * fx, dz, __fmaf_rn(sign * fz, dx, v[3]));
-    v[4] = __fmaf_rn(sign * fy, dz, __fmaf_rn(sign * fz, dy, v[4]));
-    v[5] = __fmaf_rn(sign * fz, dz, v[5]);
-}
+// Pruning (no reference counterpart; results unchanged).  Run after every
+// rebuild and whenever some atom moved more than buffer/2 since the last run
+// (the pack kernel checks): copies each atom's full-list partners whose
+// distance is below cutoff + buffer now, in list order, as 32-bit words
+// {partner slot | LJ type << 23 | per-pair image flag << 31}, and records the
+// slot offsets it saw.  Any pair within the cutoff before the next pruning
+// was within cutoff + buffer at this one, so the copy misses none.  buffer <= 0
+// keeps every listed pair (format conversion only).  The last block to finish
+// clears the flag.
+constexpr int kPruneWarps = 8;
 
-struct SlotAcc
+__global__ void __launch_bounds__(kPruneWarps * 32)
+    k_prune(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, long long words_cap,
+            int clusters_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
+            const int* __restrict__ nbr_start, const float4* __restrict__ tab,
+            const long long* __restrict__ slot_start, const int* __restrict__ slot_count,
+            const unsigned short* __restrict__ words, const float4* __restrict__ pos, const int* __restrict__ ptype,
+            float4* __restrict__ pref, int* __restrict__ pcount, unsigned* __restrict__ pwords)
 {
-    long long* x;
-    long long* y;
-    long long* z;
-};
-
-// Cluster-pair force kernel.  A warp takes one work item (an i-cluster and
-// up to kChunk j-clusters); lane (row = lane/8, j = lane%8) evaluates pairs
-// (i = row and row + 4, j) of each 8 x 8 entry.  j forces are summed over the
-// four rows by shuffles and added once per atom and entry (int64 fixed
-// point, slot-ordered, so eight lanes write two sectors); i forces stay in
-// registers for the whole item.
-//
-// MODE 0: forces.  MODE 1: + energy and virial totals; the virial is taken
-// as sum_entries D (x) F_j + sum_atoms delta (x) F (the second part in the
-// finalize kernel), D the entry's centre difference, which needs no per-pair
-// outer product.  MODE 2: + per-atom energy/virial arrays owned by the
-// pair's lower-index atom, per pair.
-template <int MODE>
-__global__ void __launch_bounds__(kPairWarps * 32)
-    k_pair_clusters(PairConst pc, Cell cell, Cell rcell, const int* __restrict__ counters,
-                    const int4* __restrict__ items, const int4* __restrict__ ents, const float4* __restrict__ ents_d,
-                    const int* __restrict__ slot_atom, const float4* __restrict__ pos,
-                    const int* __restrict__ ptype, const float2* __restrict__ gtable, SlotAcc acc,
-                    long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, int items_cap)
-{
-    extern __shared__ float2 table[];
-    const int TT = pc.n_types * pc.n_types;
-    for (int k = threadIdx.x; k < TT; k += blockDim.x) table[k] = gtable[k];
-    __syncthreads();
-
+    if (counters[kCntPrune] == 0) return;
     const int lane = threadIdx.x & 31;
-    const int jl = lane & 7;
-    const int row = lane >> 3;
-    const int nitems = min(counters[kCntItems], items_cap);
-    const int total_warps = gridDim.x * kPairWarps;
+    const int a = threadIdx.x >> 5;
+    const int nc = min(counters[kCntClusters], clusters_cap);
+    const bool lists_ok = word_total(counters) <= words_cap;
+    __shared__ unsigned long long kept_total;
+    if (threadIdx.x == 0) kept_total = 0;
+    __syncthreads();
+    for (int c = blockIdx.x; c < nc; c += gridDim.x)
+    {
+        const int s = c * kClusterSize + a;
+        const float4 pi = pos[s];
+        if (lane == 0) pref[s] = pi;
+        const int n = lists_ok ? slot_count[s] : 0;
+        int kept = 0;
+        if (n > 0)
+        {
+            const ForceParams P = fps ? fps[cl_sys[c]] : p0;
+            const float rp = sqrtf(P.rc2) + buffer + 1e-3f;
+            const float rp2 = buffer > 0.0f ? rp * rp : 3.0e38f;
+            const long long base = slot_start[s];
+            const unsigned short* __restrict__ wl = words + base;
+            const float4* __restrict__ tb = tab + nbr_start[c];
+            unsigned w = lane < n ? wl[lane] : 0u;
+            for (int k0 = 0; k0 < n; k0 += 32)
+            {
+                const int k = k0 + lane;
+                const unsigned cw = w;
+                w = k + 32 < n ? wl[k + 32] : 0u;
+                bool keep = false;
+                unsigned out = 0;
+                if (k < n)
+                {
+                    const float4 e = tb[cw >> 3];
+                    const int eb = __float_as_int(e.w);
+                    const int js = (eb & 0x3fffffff) + (int)(cw & 7u);
+                    const float4 pj = pos[js];
+                    const int tj = ptype[js];
+                    float dx = (e.x - pi.x) + pj.x;
+                    float dy = (e.y - pi.y) + pj.y;
+                    float dz = (e.z - pi.z) + pj.z;
+                    if (eb & (1 << 30))
+                    {
+                        const SysDesc& D = sys[cl_sys[c]];
+                        const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
+                        const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
+                        const float sz = rintf(dz * D.rcell.a33);
+                        dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
+                        dy -= sy * D.cell.a22 + sz * D.cell.a32;
+                        dz -= sz * D.cell.a33;
+                    }
+                    keep = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx)) < rp2;
+                    out = (unsigned)js | ((unsigned)tj << 23) | ((eb & (1 << 30)) ? 0x80000000u : 0u);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep) pwords[base + kept + __popc(m & ((1u << lane) - 1u))] = out;
+                kept += __popc(m);
+            }
+        }
+        if (lane == 0)
+        {
+            pcount[s] = kept;
+            atomicAdd(&kept_total, (unsigned long long)kept);
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        atomicAdd((unsigned long long*)&counters[kCntPWords], kept_total);
+        __threadfence();
+        const int done = atomicAdd(&counters[kCntPruneDone], 1);
+        if (done == gridDim.x - 1)
+        {
+            unsigned long long* w = (unsigned long long*)&counters[kCntPWords];
+            *(unsigned long long*)&counters[kCntPWordsLast] = atomicExch(w, 0ull);
+            counters[kCntPruneDone] = 0;
+            counters[kCntPrune] = 0;
+            counters[kCntPrunes] += 1;
+        }
+    }
+}
+
+// ------------------------------------------------ packed FP32x2 pair math
+__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
+
+__device__ __forceinline__ float2 poly5x2(float2 x, const float* c)
+{
+    float2 p = f2(c[5]);
+    p = __ffma2_rn(p, x, f2(c[4]));
+    p = __ffma2_rn(p, x, f2(c[3]));
+    p = __ffma2_rn(p, x, f2(c[2]));
+    p = __ffma2_rn(p, x, f2(c[1]));
+    return __ffma2_rn(p, x, f2(c[0]));
+}
+
+// pair_scalar for two pairs at once; nA = -A.
+template <bool ENERGY, int FIT>
+__device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, float2 B, const ForceParams& pc,
+                                               float2& e_lj, float2& e_c)
+{
+    float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+    const float2 h = __fmul2_rn(__fmul2_rn(r2, f2(-0.5f)), rinv);
+    rinv = __fmul2_rn(rinv, __ffma2_rn(h, rinv, f2(1.5f)));  // one Newton step
+    const float2 r2inv = __fmul2_rn(rinv, rinv);
+    const float2 r6inv = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
+    const float2 flj = __fmul2_rn(__fmul2_rn(__ffma2_rn(nA, r6inv, B), r6inv), r2inv);
+    float2 fc;
+    if (FIT == 1)
+    {
+        const float2 x = __fmul2_rn(r2, f2(pc.w_scale));
+        const float2 kp = poly5x2(x, kEwaldKP), kq = poly5x2(x, kEwaldKQ);
+        const float2 K = make_float2(__fdividef(kp.x, kq.x), __fdividef(kp.y, kq.y));
+        fc = __fmul2_rn(qq, __ffma2_rn(f2(-pc.beta3), K, __fmul2_rn(rinv, r2inv)));
+        if (ENERGY)
+        {
+            const float2 mp = poly5x2(x, kEwaldMP), mq = poly5x2(x, kEwaldMQ);
+            const float2 M = make_float2(__fdividef(mp.x, mq.x), __fdividef(mp.y, mq.y));
+            e_c = __fmul2_rn(qq, __ffma2_rn(f2(-pc.beta), M, rinv));
+        }
+    }
+    else
+    {
+        float c[2], e[2];
+        const float rr[2] = {r2.x, r2.y}, ri[2] = {rinv.x, rinv.y}, q[2] = {qq.x, qq.y};
+        for (int h2 = 0; h2 < 2; h2++)
+        {
+            const float r = rr[h2] * ri[h2];
+            const float br = pc.beta * r;
+            const float erfcv = erfcf(br);
+            c[h2] = q[h2] * ri[h2] * ri[h2] * ri[h2] * __fmaf_rn(br * 1.1283791670955126f, __expf(-br * br), erfcv);
+            e[h2] = q[h2] * erfcv * ri[h2];
+        }
+        fc = make_float2(c[0], c[1]);
+        if (ENERGY) e_c = make_float2(e[0], e[1]);
+    }
+    if (ENERGY) e_lj = __fmul2_rn(__ffma2_rn(nA, __fmul2_rn(r6inv, f2(-1.0f / 12.0f)), __fmul2_rn(B, f2(-1.0f / 6.0f))), r6inv);
+    return __ffma2_rn(fc, f2(-1.0f), flj);
+}
+
+// A difference of two 22-bit cluster-centre coordinates, wrapped to
+// [-2^21, 2^21) (minimum image of the centres) and converted exactly: the
+// wrapped value plus 2^23 + 2^21 is an integer below 2^23 + 2^22, whose float
+// bit pattern is 0x4B000000 | value.
+__device__ __forceinline__ float centre_step(int qj, int qi)
+{
+    return __int_as_float(((qj - qi + 0x200000) & 0x3fffff) | 0x4b000000) - 10485760.0f;
+}
+
+// Pruned-list force kernel.  A block takes one cluster per pass and each of
+// its eight warps one slot (atom); each lane evaluates two partner words per
+// iteration (k and k + 32 of a 64-word window) with packed FP32x2 arithmetic,
+// and prefetches the next window's words.  A word names the partner slot, so
+// its offset {delta + displacement, q} and its cluster's 22-bit centre load
+// side by side; dr = (c_j - c_i) * cell / 2^22 + p_j - p_i.  Each lane's
+// partial force is converted to int64 fixed point (2^-32 kcal/mol/A) and
+// reduced over the lanes, so the atom's force does not depend on the
+// reduction order; one lane adds it to the caller's array: no atomics,
+// bitwise reproducible.
+//
+// MODE 0: forces.  MODE 1: + energy and virial totals (each pair is seen
+// from both atoms, so the sums are halved).  MODE 2: + per-atom energy and
+// virial of the pairs the atom owns (the lower global index; water sites
+// hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES does).
+template <int MODE, int FIT, bool TRI>
+__global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 3 : 2)
+    k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
+                const int* __restrict__ counters, long long words_cap, int clusters_cap,
+                const int* __restrict__ cl_sys, const int4* __restrict__ cl_q,
+                const long long* __restrict__ slot_start, const int* __restrict__ pcount,
+                const unsigned* __restrict__ pwords, const int* __restrict__ slot_atom,
+                const float4* __restrict__ slot_x0, const float4* __restrict__ pos, const int* __restrict__ ptype,
+                const float2* __restrict__ gtable, int table_size, float3* __restrict__ frc,
+                long long* __restrict__ totals, OwnerMap om, PerAtomOut pa)
+{
+    extern __shared__ float2 table[];           // {-A, B}
+    __shared__ long long red[kForceWarps][8];  // per-warp fixed-point totals
+    for (int k = threadIdx.x; k < table_size; k += blockDim.x)
+    {
+        const float2 g = gtable[k];
+        table[k] = make_float2(-g.x, g.y);
+    }
+    if (threadIdx.x < kForceWarps * 8) red[threadIdx.x >> 3][threadIdx.x & 7] = 0;
+    __syncthreads();
     constexpr bool EN = MODE >= 1;
     constexpr bool PA = MODE >= 2;
+    const int lane = threadIdx.x & 31;
+    const int a = threadIdx.x >> 5;
+    const int nc = min(counters[kCntClusters], clusters_cap);
+    const bool lists_ok = word_total(counters) <= words_cap;
 
-    for (int it = blockIdx.x * kPairWarps + (threadIdx.x >> 5); it < nitems; it += total_warps)
+    for (int c = blockIdx.x; lists_ok && c < nc; c += gridDim.x)
     {
-        const int4 item = items[it];
-        const int ci = item.x;
-        const float4 pi0 = pos[ci * kClusterSize + row];
-        const float4 pi1 = pos[ci * kClusterSize + row + 4];
-        const int ti0 = ptype[ci * kClusterSize + row] * pc.n_types;
-        const int ti1 = ptype[ci * kClusterSize + row + 4] * pc.n_types;
-        int ai0 = 0, ai1 = 0, gi0 = 0, gi1 = 0;
-        if (PA)
-        {
-            ai0 = slot_atom[ci * kClusterSize + row];
-            ai1 = slot_atom[ci * kClusterSize + row + 4];
-            gi0 = ai0 >= 0 ? om.atom_local[ai0] : 0;
-            gi1 = ai1 >= 0 ? om.atom_local[ai1] : 0;
-        }
-        float fi0x = 0, fi0y = 0, fi0z = 0, fi1x = 0, fi1y = 0, fi1z = 0;
-        float tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        float pai[2][8];
-        if (PA)
-            for (int h = 0; h < 2; h++)
-                for (int q = 0; q < 8; q++) pai[h][q] = 0.0f;
-
-        const int e_end = item.y + item.z;
-        int4 en_n = make_int4(0, 0, 0, 0);
-        float4 ed_n = make_float4(0, 0, 0, 0), pj_n = make_float4(0, 0, 0, 0);
-        int tj_n = 0;
-        if (item.z > 0)
-        {
-            en_n = ents[item.y];
-            ed_n = ents_d[item.y];
-            pj_n = pos[en_n.x * kClusterSize + jl];
-            tj_n = ptype[en_n.x * kClusterSize + jl];
-        }
-        for (int e = item.y; e < e_end; e++)
-        {
-            const int4 en = en_n;
-            const float4 ed = ed_n;
-            const float4 pj = pj_n;
-            const int tj = tj_n;
-            if (e + 1 < e_end)
-            {
-                en_n = ents[e + 1];
-                ed_n = ents_d[e + 1];
-                pj_n = pos[en_n.x * kClusterSize + jl];
-                tj_n = ptype[en_n.x * kClusterSize + jl];
-            }
-            const int cj = en.x;
-            const float px = ed.x + pj.x, py = ed.y + pj.y, pz = ed.z + pj.z;
-            int aj = 0, gj = 0;
-            if (PA)
-            {
-                aj = slot_atom[cj * kClusterSize + jl];
-                gj = aj >= 0 ? om.atom_local[aj] : 0;
-            }
-            const bool pair_image = (en.y & kEntPairImage) != 0;
-            float fjx = 0, fjy = 0, fjz = 0;
-            float paj[8];
-            if (PA)
-                for (int q = 0; q < 8; q++) paj[q] = 0.0f;
+        const int s = c * kClusterSize + a;
+        const int n = pcount[s];
+        if (n == 0) continue;
+        const int sy = cl_sys[c];
+        const ForceParams P = fps ? fps[sy] : p0;
+        const Cell qc = sys[sy].qcell;
+        const float4 pi = pos[s];
+        const int4 qi = cl_q[c];
+        const int ti = ptype[s] * P.n_types + P.table_begin;
+        const unsigned* __restrict__ wl = pwords + slot_start[s];
+        int gi = 0;
+        if (PA) gi = __float_as_int(slot_x0[s].w);
+        const float2 npx = f2(-pi.x), npy = f2(-pi.y), npz = f2(-pi.z);
+        float2 fx = f2(0.0f), fy = f2(0.0f), fz = f2(0.0f);
+        float2 acc[8], own[8];
 #pragma unroll
-            for (int h = 0; h < 2; h++)
-            {
-                const unsigned m = (unsigned)(h ? en.w : en.z);
-                if (m == 0) continue;
-                const float4 pi = h ? pi1 : pi0;
-                float dx = px - pi.x, dy = py - pi.y, dz = pz - pi.z;
-                float tx = 0, ty = 0, tz = 0;
-                if (pair_image)
-                {
-                    const float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
-                    const float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
-                    const float sz = rintf(dz * rcell.a33);
-                    tx = -(sx * cell.a11 + sy * cell.a21 + sz * cell.a31);
-                    ty = -(sy * cell.a22 + sz * cell.a32);
-                    tz = -(sz * cell.a33);
-                    dx += tx;
-                    dy += ty;
-                    dz += tz;
-                }
-                const float r2 = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx));
-                const bool in = ((m >> lane) & 1u) && r2 < pc.rc2;
-                const float2 AB = table[(h ? ti1 : ti0) + tj];
-                float elj = 0.0f, ec = 0.0f;
-                float fs = pair_scalar<EN>(r2, pi.w * pj.w, AB.x, AB.y, pc, elj, ec);
-                fs = in ? fs : 0.0f;
-                const float fx = fs * dx, fy = fs * dy, fz = fs * dz;
-                if (h)
-                {
-                    fi1x += fx;
-                    fi1y += fy;
-                    fi1z += fz;
-                }
-                else
-                {
-                    fi0x += fx;
-                    fi0y += fy;
-                    fi0z += fz;
-                }
-                fjx -= fx;
-                fjy -= fy;
-                fjz -= fz;
-                if (EN)
-                {
-                    tot[0] += in ? elj : 0.0f;
-                    tot[1] += in ? ec : 0.0f;
-                    if (PA)
-                    {
-                        float v[6] = {0, 0, 0, 0, 0, 0};
-                        add_outer(v, fx, fy, fz, dx, dy, dz, -1.0f);
-                        for (int q = 0; q < 6; q++) tot[2 + q] += v[q];
-                        const bool i_owns = (h ? gi1 : gi0) < gj;
-                        float* dst = i_owns ? pai[h] : paj;
-                        dst[0] += in ? elj : 0.0f;
-                        dst[1] += in ? ec : 0.0f;
-                        for (int q = 0; q < 6; q++) dst[2 + q] += v[q];
-                    }
-                    else if (pair_image)
-                    {
-                        // the lattice shift this pair took beyond the entry's image
-                        add_outer(tot + 2, fx, fy, fz, tx, ty, tz, -1.0f);
-                    }
-                }
-            }
-            if (EN && !PA)
-            {
-                // -(f (x) D) summed over this lane's pairs: f_j accumulated -f
-                add_outer(tot + 2, fjx, fjy, fjz, ed.x, ed.y, ed.z, 1.0f);
-            }
-            // j forces: sum over the four rows, one fixed-point add per atom
-            fjx += __shfl_xor_sync(0xffffffffu, fjx, 8);
-            fjy += __shfl_xor_sync(0xffffffffu, fjy, 8);
-            fjz += __shfl_xor_sync(0xffffffffu, fjz, 8);
-            fjx += __shfl_xor_sync(0xffffffffu, fjx, 16);
-            fjy += __shfl_xor_sync(0xffffffffu, fjy, 16);
-            fjz += __shfl_xor_sync(0xffffffffu, fjz, 16);
-            if (PA)
-            {
-                for (int q = 0; q < 8; q++)
-                {
-                    paj[q] += __shfl_xor_sync(0xffffffffu, paj[q], 8);
-                    paj[q] += __shfl_xor_sync(0xffffffffu, paj[q], 16);
-                }
-            }
-            if (row == 0)
-            {
-                const int sj = cj * kClusterSize + jl;
-                red_fixed(acc.x + sj, fjx);
-                red_fixed(acc.y + sj, fjy);
-                red_fixed(acc.z + sj, fjz);
-                if (PA && aj >= 0)
-                {
-                    const int o = om.remap(aj);
-                    if (pa.energy) atomicAdd(pa.energy + o, paj[0] + paj[1]);
-                    if (pa.lj_energy) atomicAdd(pa.lj_energy + o, paj[0]);
-                    if (pa.direct) atomicAdd(pa.direct + o, paj[1]);
-                    if (pa.virial)
-                        for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)o + q, paj[2 + q]);
-                }
-            }
-        }
-        // i forces: sum over the eight j lanes
-#pragma unroll
-        for (int o = 1; o < 8; o <<= 1)
+        for (int q = 0; q < 8; q++)
         {
-            fi0x += __shfl_xor_sync(0xffffffffu, fi0x, o);
-            fi0y += __shfl_xor_sync(0xffffffffu, fi0y, o);
-            fi0z += __shfl_xor_sync(0xffffffffu, fi0z, o);
-            fi1x += __shfl_xor_sync(0xffffffffu, fi1x, o);
-            fi1y += __shfl_xor_sync(0xffffffffu, fi1y, o);
-            fi1z += __shfl_xor_sync(0xffffffffu, fi1z, o);
-            if (PA)
-                for (int h = 0; h < 2; h++)
-                    for (int q = 0; q < 8; q++) pai[h][q] += __shfl_xor_sync(0xffffffffu, pai[h][q], o);
+            acc[q] = f2(0.0f);
+            own[q] = f2(0.0f);
         }
-        if (jl == 0)
+        unsigned wA = lane < n ? wl[lane] : 0u;
+        unsigned wB = lane + 32 < n ? wl[lane + 32] : 0u;
+#pragma unroll 1
+        for (int k0 = 0; k0 < n; k0 += 64)
         {
-            const int s0 = ci * kClusterSize + row, s1 = s0 + 4;
-            red_fixed(acc.x + s0, fi0x);
-            red_fixed(acc.y + s0, fi0y);
-            red_fixed(acc.z + s0, fi0z);
-            red_fixed(acc.x + s1, fi1x);
-            red_fixed(acc.y + s1, fi1y);
-            red_fixed(acc.z + s1, fi1z);
-            if (PA)
+            const unsigned cA = wA, cB = wB;
+            const bool vA = k0 + lane < n, vB = k0 + lane + 32 < n;
             {
+                const int k = k0 + 64 + lane;
+                wA = k < n ? wl[k] : 0u;
+                wB = k + 32 < n ? wl[k + 32] : 0u;
+            }
+            const int jA = (int)(cA & 0x7fffffu), jB = (int)(cB & 0x7fffffu);
+            const float4 pA = pos[jA], pB = pos[jB];
+            const int4 qA = cl_q[jA >> 3], qB = cl_q[jB >> 3];
+            const float2 abA = table[ti + (int)((cA >> 23) & 0xffu)];
+            const float2 abB = table[ti + (int)((cB >> 23) & 0xffu)];
+            const float2 ux = make_float2(centre_step(qA.x, qi.x), centre_step(qB.x, qi.x));
+            const float2 uy = make_float2(centre_step(qA.y, qi.y), centre_step(qB.y, qi.y));
+            const float2 uz = make_float2(centre_step(qA.z, qi.z), centre_step(qB.z, qi.z));
+            float2 dx = __fadd2_rn(make_float2(pA.x, pB.x), npx);
+            float2 dy = __fadd2_rn(make_float2(pA.y, pB.y), npy);
+            float2 dz = __fadd2_rn(make_float2(pA.z, pB.z), npz);
+            dx = __ffma2_rn(ux, f2(qc.a11), dx);
+            dy = __ffma2_rn(uy, f2(qc.a22), dy);
+            dz = __ffma2_rn(uz, f2(qc.a33), dz);
+            if (TRI)
+            {
+                dx = __ffma2_rn(uy, f2(qc.a21), dx);
+                dx = __ffma2_rn(uz, f2(qc.a31), dx);
+                dy = __ffma2_rn(uz, f2(qc.a32), dy);
+            }
+            if ((cA | cB) & 0x80000000u)
+            {
+                // small box: these partners need a per-pair image
+                const SysDesc& D = sys[sy];
+                float ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
+                const unsigned cw[2] = {cA, cB};
                 for (int h = 0; h < 2; h++)
                 {
-                    const int a = h ? ai1 : ai0;
-                    if (a < 0) continue;
-                    const int o = om.remap(a);
-                    if (pa.energy) atomicAdd(pa.energy + o, pai[h][0] + pai[h][1]);
-                    if (pa.lj_energy) atomicAdd(pa.lj_energy + o, pai[h][0]);
-                    if (pa.direct) atomicAdd(pa.direct + o, pai[h][1]);
-                    if (pa.virial)
-                        for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)o + q, pai[h][2 + q]);
+                    if (!(cw[h] & 0x80000000u)) continue;
+                    const float sx = rintf(ddx[h] * D.rcell.a11 + ddy[h] * D.rcell.a21 + ddz[h] * D.rcell.a31);
+                    const float sy2 = rintf(ddy[h] * D.rcell.a22 + ddz[h] * D.rcell.a32);
+                    const float sz = rintf(ddz[h] * D.rcell.a33);
+                    ddx[h] -= sx * D.cell.a11 + sy2 * D.cell.a21 + sz * D.cell.a31;
+                    ddy[h] -= sy2 * D.cell.a22 + sz * D.cell.a32;
+                    ddz[h] -= sz * D.cell.a33;
+                }
+                dx = make_float2(ddx[0], ddx[1]);
+                dy = make_float2(ddy[0], ddy[1]);
+                dz = make_float2(ddz[0], ddz[1]);
+            }
+            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+            const bool inA = vA && r2.x < P.rc2, inB = vB && r2.y < P.rc2;
+            float2 elj, ec;
+            float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(make_float2(pA.w, pB.w), f2(pi.w)),
+                                             make_float2(abA.x, abB.x), make_float2(abA.y, abB.y), P, elj, ec);
+            f = make_float2(inA ? f.x : 0.0f, inB ? f.y : 0.0f);
+            const float2 gx = __fmul2_rn(f, dx), gy = __fmul2_rn(f, dy), gz = __fmul2_rn(f, dz);
+            fx = __fadd2_rn(fx, gx);
+            fy = __fadd2_rn(fy, gy);
+            fz = __fadd2_rn(fz, gz);
+            if (EN)
+            {
+                elj = make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f);
+                ec = make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f);
+                acc[0] = __fadd2_rn(acc[0], elj);
+                acc[1] = __fadd2_rn(acc[1], ec);
+                acc[2] = __ffma2_rn(gx, dx, acc[2]);
+                acc[3] = __ffma2_rn(gx, dy, acc[3]);
+                acc[4] = __ffma2_rn(gy, dy, acc[4]);
+                acc[5] = __ffma2_rn(gx, dz, acc[5]);
+                acc[6] = __ffma2_rn(gy, dz, acc[6]);
+                acc[7] = __ffma2_rn(gz, dz, acc[7]);
+                if (PA)
+                {
+                    const int gjA = __float_as_int(slot_x0[jA].w), gjB = __float_as_int(slot_x0[jB].w);
+                    const float2 m = make_float2(gi < gjA ? 1.0f : 0.0f, gi < gjB ? 1.0f : 0.0f);
+                    own[0] = __ffma2_rn(m, elj, own[0]);
+                    own[1] = __ffma2_rn(m, ec, own[1]);
+                    const float2 mgx = __fmul2_rn(m, gx), mgy = __fmul2_rn(m, gy), mgz = __fmul2_rn(m, gz);
+                    own[2] = __ffma2_rn(mgx, dx, own[2]);
+                    own[3] = __ffma2_rn(mgx, dy, own[3]);
+                    own[4] = __ffma2_rn(mgy, dy, own[4]);
+                    own[5] = __ffma2_rn(mgx, dz, own[5]);
+                    own[6] = __ffma2_rn(mgy, dz, own[6]);
+                    own[7] = __ffma2_rn(mgz, dz, own[7]);
                 }
             }
         }
-        if (EN)
-        {
+        long long qx = __float2ll_rn((fx.x + fx.y) * kTwoPow32), qy = __float2ll_rn((fy.x + fy.y) * kTwoPow32),
+                  qz = __float2ll_rn((fz.x + fz.y) * kTwoPow32);
+        float accs[8], owns[8];
 #pragma unroll
-            for (int q = 0; q < 8; q++)
-                for (int o = 16; o > 0; o >>= 1) tot[q] += __shfl_xor_sync(0xffffffffu, tot[q], o);
-            if (lane == 0)
+        for (int q = 0; q < 8; q++)
+        {
+            // the virial terms were accumulated as +g (x) d: the virial is -g (x) d
+            const float sg = q >= 2 ? -1.0f : 1.0f;
+            accs[q] = sg * (acc[q].x + acc[q].y);
+            owns[q] = sg * (own[q].x + own[q].y);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+            qx += __shfl_xor_sync(0xffffffffu, qx, o);
+            qy += __shfl_xor_sync(0xffffffffu, qy, o);
+            qz += __shfl_xor_sync(0xffffffffu, qz, o);
+            if (EN)
+#pragma unroll
+                for (int q = 0; q < 8; q++) accs[q] += __shfl_xor_sync(0xffffffffu, accs[q], o);
+            if (PA)
+#pragma unroll
+                for (int q = 0; q < 8; q++) owns[q] += __shfl_xor_sync(0xffffffffu, owns[q], o);
+        }
+        if (lane == 0)
+        {
+            const int ai = slot_atom[s];
+            float3 F = frc[ai];
+            F.x += (float)((double)qx * kForceUnscale);
+            F.y += (float)((double)qy * kForceUnscale);
+            F.z += (float)((double)qz * kForceUnscale);
+            frc[ai] = F;
+            if (EN)
+            {
+                // halve the double-counted sums; the symmetric off-diagonal
+                // terms (xy + yx etc.) are twice the one accumulated
+#pragma unroll
                 for (int q = 0; q < 8; q++)
                 {
-                    long long v = __double2ll_rn((double)tot[q] * kEnergyScale);
-                    if (v) atomicAdd((unsigned long long*)&totals[q], (unsigned long long)v);
+                    const double sc = (q == 3 || q == 5 || q == 6) ? 1.0 : 0.5;
+                    red[a][q] += __double2ll_rn((double)accs[q] * sc * kEnergyScale);
                 }
-        }
-    }
-}
-
-// Fixed point -> caller's float force (+=) for the cluster path, slot-indexed
-// accumulators cleared for the next call.  With virial totals it adds
-// sum_atoms F (x) delta, the per-atom half of the decomposition above.
-template <bool VIRIAL>
-__global__ void k_finalize_slots(int n, const int* __restrict__ atom_slot, int slots_cap, SlotAcc acc,
-                                 const float4* __restrict__ pos, float3* __restrict__ frc,
-                                 long long* __restrict__ totals)
-{
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    double v[6] = {0, 0, 0, 0, 0, 0};
-    if (i < n)
-    {
-        const int s = atom_slot[i];
-        if (s >= 0 && s < slots_cap)
-        {
-            const long long x = acc.x[s], y = acc.y[s], z = acc.z[s];
-            const double fx = (double)x * kForceUnscale, fy = (double)y * kForceUnscale,
-                         fz = (double)z * kForceUnscale;
-            if (x | y | z)
-            {
-                float3 f = frc[i];
-                f.x += (float)fx;
-                f.y += (float)fy;
-                f.z += (float)fz;
-                frc[i] = f;
-                acc.x[s] = 0;
-                acc.y[s] = 0;
-                acc.z[s] = 0;
             }
-            if (VIRIAL)
+            if (PA)
             {
-                const float4 d = pos[s];
-                v[0] = fx * d.x;
-                v[1] = fx * d.y + fy * d.x;
-                v[2] = fy * d.y;
-                v[3] = fx * d.z + fz * d.x;
-                v[4] = fy * d.z + fz * d.y;
-                v[5] = fz * d.z;
+                const int o = om.remap(ai);
+                if (pa.energy) atomicAdd(pa.energy + o, owns[0] + owns[1]);
+                if (pa.lj_energy) atomicAdd(pa.lj_energy + o, owns[0]);
+                if (pa.direct) atomicAdd(pa.direct + o, owns[1]);
+                if (pa.virial)
+                {
+                    float* v = pa.virial + 6 * (size_t)o;
+                    atomicAdd(v + 0, owns[2]);
+                    atomicAdd(v + 1, 2.0f * owns[3]);
+                    atomicAdd(v + 2, owns[4]);
+                    atomicAdd(v + 3, 2.0f * owns[5]);
+                    atomicAdd(v + 4, 2.0f * owns[6]);
+                    atomicAdd(v + 5, owns[7]);
+                }
             }
         }
     }
-    if (VIRIAL)
+    if (EN)
     {
-        __shared__ double red[6][32];
-        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-        for (int q = 0; q < 6; q++)
-        {
-            for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
-            if (lane == 0) red[q][w] = v[q];
-        }
         __syncthreads();
-        if (w == 0)
+        if (threadIdx.x < 8)
         {
-            const int nw = blockDim.x >> 5;
-            for (int q = 0; q < 6; q++)
-            {
-                double t = lane < nw ? red[q][lane] : 0.0;
-                for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-                if (lane == 0)
-                {
-                    long long b = __double2ll_rn(t * kEnergyScale);
-                    if (b) atomicAdd((unsigned long long*)&totals[2 + q], (unsigned long long)b);
-                }
-            }
+            long long t = 0;
+            for (int w = 0; w < kForceWarps; w++) t += red[w][threadIdx.x];
+            if (t) atomicAdd((unsigned long long*)&totals[threadIdx.x], (unsigned long long)t);
         }
     }
 }
@@ -765,6 +839,8 @@ PairConst make_pair_const(const spgnb_lj* lj, float beta)
     pc.n_types = lj->n_types;
     float z = beta * lj->cutoff;
     pc.use_fit = (z * z <= SPGNB_EWALD_W_MAX * 0.999f) ? 1 : 0;
+    pc.table_begin = 0;
+    pc.pad = 0;
     return pc;
 }
 
@@ -780,29 +856,76 @@ int ensure_pos(spgnb_lj* lj, int count)
     return SPGNB_OK;
 }
 
-int ensure_slot_acc(spgnb_lj* lj, int slots)
-{
-    if (slots <= lj->slot_acc_cap) return SPGNB_OK;
-    dfree(lj->d_slot_acc);
-    int st = dalloc(&lj->d_slot_acc, 3 * (size_t)slots);
-    if (st) return st;
-    SPGNB_CUDA(cudaMemset(lj->d_slot_acc, 0, sizeof(long long) * 3 * (size_t)slots));
-    lj->slot_acc_cap = slots;
-    return SPGNB_OK;
-}
-
 // A persistent grid: as many blocks as can be resident on every SM.
 template <typename K>
-int pair_blocks(K kernel, size_t smem)
+int pair_blocks(K kernel, int threads, size_t smem)
 {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kPairWarps * 32, smem) != cudaSuccess ||
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
         per_sm <= 0)
     {
         cudaGetLastError();
         per_sm = 4;
     }
     return per_sm * num_sms();
+}
+
+template <int M>
+void set_fast_smem(size_t smem)
+{
+    cudaFuncSetAttribute(k_pair_fast<M, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_pair_fast<M, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_pair_fast<M, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_pair_fast<M, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+// Launches the pruned-list force kernel for the given mode / pair-function /
+// box-shape variant.
+struct FastArgs
+{
+    ForceParams p0;
+    const ForceParams* fps;
+    const spgnb_nl* nl;
+    const float4* pos;
+    const int* ptype;
+    const float2* table;
+    int table_size;
+    float3* frc;
+    long long* totals;
+    OwnerMap om;
+    PerAtomOut pa;
+};
+
+template <int M, int F, bool T>
+int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
+{
+    const spgnb_nl* nl = x.nl;
+    const int grid = std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T>, kForceWarps * 32, smem), nl->clusters_cap));
+    k_pair_fast<M, F, T><<<grid, kForceWarps * 32, smem, s>>>(
+        x.p0, x.fps, nl->d_sys, nl->d_counters, nl->words_cap, nl->clusters_cap, nl->d_cl_sys, nl->d_cl_q,
+        nl->d_slot_start, nl->d_pcount, nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, x.pos, x.ptype, x.table,
+        x.table_size, x.frc, x.totals, x.om, x.pa);
+    SPGNB_CHECK_LAUNCH("k_pair_fast");
+    return SPGNB_OK;
+}
+
+template <int M, int F>
+int launch_fast_t(const FastArgs& x, bool tri, size_t smem, cudaStream_t s)
+{
+    return tri ? launch_fast<M, F, true>(x, smem, s) : launch_fast<M, F, false>(x, smem, s);
+}
+
+template <int M>
+int launch_fast_ft(const FastArgs& x, bool fit, bool tri, size_t smem, cudaStream_t s)
+{
+    return fit ? launch_fast_t<M, 1>(x, tri, smem, s) : launch_fast_t<M, 0>(x, tri, smem, s);
+}
+
+int launch_fast_any(const FastArgs& x, int mode, bool fit, bool tri, size_t smem, cudaStream_t s)
+{
+    if (mode == 0) return launch_fast_ft<0>(x, fit, tri, smem, s);
+    if (mode == 1) return launch_fast_ft<1>(x, fit, tri, smem, s);
+    return launch_fast_ft<2>(x, fit, tri, smem, s);
 }
 
 int check_common(spgnb_lj* lj, int local_atom_numbers, int ghost_numbers, const spgnb_vector* d_crd,
@@ -836,7 +959,7 @@ int spgnb_lj_create(int atom_numbers, int atom_type_numbers, const int* h_atom_t
     if (atom_numbers <= 0 || atom_type_numbers <= 0 || !h_atom_type || !h_pair_A || !h_pair_B || !(cutoff > 0))
         return fail(SPGNB_E_ARG, "spgnb_lj_create: bad arguments");
     const int T = atom_type_numbers;
-    if (T * T * (int)sizeof(float2) > 96 * 1024)
+    if (T * T * (int)sizeof(float2) > 96 * 1024 || T > kMaxTypes)
         return fail(SPGNB_E_UNSUPPORTED, "spgnb_lj_create: %d LJ types exceed the shared-memory pair table", T);
     std::vector<double> hist(T, 0.0);
     for (int i = 0; i < atom_numbers; i++)
@@ -874,9 +997,9 @@ int spgnb_lj_create(int atom_numbers, int atom_type_numbers, const int* h_atom_t
     const int smem = (int)(sizeof(float2) * T * T);
     if (smem > 48 * 1024)
     {
-        cudaFuncSetAttribute(k_pair_clusters<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(k_pair_clusters<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        cudaFuncSetAttribute(k_pair_clusters<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        set_fast_smem<0>(smem);
+        set_fast_smem<1>(smem);
+        set_fast_smem<2>(smem);
     }
     cudaMemcpy(lj->d_atom_type, h_atom_type, sizeof(int) * atom_numbers, cudaMemcpyHostToDevice);
     cudaMemcpy(lj->d_table, table.data(), sizeof(float2) * table.size(), cudaMemcpyHostToDevice);
@@ -925,10 +1048,13 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
         return fail(SPGNB_E_STATE, "spgnb_lj_pme_direct_force: list built for %d atoms, called with %d",
                     nl->local_atoms, local_atom_numbers);
     if (local_atom_numbers == 0) return SPGNB_OK;
+    if (nl->S != 1) return fail(SPGNB_E_STATE, "spgnb_lj_pme_direct_force: the list holds several systems");
+    if (memcmp(&cell, &nl->cell, sizeof(cell)) != 0)
+        return fail(SPGNB_E_STATE, "spgnb_lj_pme_direct_force: the box differs from the one of the last list "
+                                   "update; update the list after a box change");
     cudaStream_t s = stream();
     const int slots = nl->clusters_cap * kClusterSize;
     if ((st = ensure_pos(lj, slots))) return st;
-    const Cell c = make_cell(cell), rc = make_cell(rcell);
     SPGNB_CUDA(cudaMemsetAsync(lj->d_totals, 0, sizeof(long long) * 8, s));
     if (need_atom_energy)
     {
@@ -936,11 +1062,20 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
         if (d_atom_direct_pme_energy)
             SPGNB_CUDA(cudaMemsetAsync(d_atom_direct_pme_energy, 0, sizeof(float) * lj->atom_numbers, s));
     }
-    k_pack_slots<<<(slots + 255) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_slot_x0,
-                                                     nl->d_slot_d0, (const float3*)d_crd, d_charge,
-                                                     lj->d_local_type, c, rc, lj->d_pos, lj->d_pos_type);
+    const bool track = nl->opt.prune_buffer > 0.0f;
+    const float half = 0.5f * nl->opt.prune_buffer;
+    k_pack_slots<<<(slots + 255) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_cl_sys,
+                                                     nl->d_sys, nl->d_slot_x0, nl->d_slot_d0, (const float3*)d_crd,
+                                                     d_charge, lj->d_local_type, lj->d_pos, lj->d_pos_type,
+                                                     track ? nl->d_pref : nullptr, half * half);
     SPGNB_CHECK_LAUNCH("k_pack_slots");
-    PairConst pc = make_pair_const(lj, pme_beta);
+    const ForceParams fp = make_pair_const(lj, pme_beta);
+    const int grid = std::max(1, std::min(num_sms() * 4, nl->clusters_cap));
+    k_prune<<<grid, kPruneWarps * 32, 0, s>>>(fp, nullptr, nl->opt.prune_buffer, nl->d_counters, nl->words_cap,
+                                              nl->clusters_cap, nl->d_cl_sys, nl->d_sys, nl->d_nbr_start, nl->d_tab,
+                                              nl->d_slot_start, nl->d_slot_count, nl->d_words, lj->d_pos,
+                                              lj->d_pos_type, nl->d_pref, nl->d_pcount, nl->d_pwords);
+    SPGNB_CHECK_LAUNCH("k_prune");
     OwnerMap om{nullptr, local_atom_numbers, 3};
     PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
     int mode = 0;
@@ -949,6 +1084,7 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
         mode = 2;
     if (mode == 2)
     {
+        om.atom_local = lj->d_atom_local;
         om.solvent_start = local_atom_numbers - (solvent_numbers > 0 ? solvent_numbers : 0);
         om.water_points = 3;
         pa.energy = need_atom_energy ? d_atom_energy : nullptr;
@@ -956,37 +1092,15 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
         pa.direct = need_atom_energy ? d_atom_direct_pme_energy : nullptr;
         pa.virial = need_virial ? (float*)d_atom_virial : nullptr;
     }
-    if ((st = ensure_slot_acc(lj, slots))) return st;
-    SlotAcc acc{lj->d_slot_acc, lj->d_slot_acc + lj->slot_acc_cap, lj->d_slot_acc + 2 * (size_t)lj->slot_acc_cap};
-    const size_t smem = sizeof(float2) * lj->n_types * lj->n_types;
+    const int table_size = lj->n_types * lj->n_types;
+    const size_t smem = sizeof(float2) * table_size;
     cudaEvent_t ev0, ev1;
     pair_events(&ev0, &ev1);
     if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
-    if (mode == 0)
-        k_pair_clusters<0><<<pair_blocks(k_pair_clusters<0>, smem), kPairWarps * 32, smem, s>>>(
-            pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents, nl->d_ents_d, nl->d_slot_atom, lj->d_pos,
-            lj->d_pos_type, lj->d_table, acc, lj->d_totals, om, pa, nl->items_cap);
-    else if (mode == 1)
-        k_pair_clusters<1><<<pair_blocks(k_pair_clusters<1>, smem), kPairWarps * 32, smem, s>>>(
-            pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents, nl->d_ents_d, nl->d_slot_atom, lj->d_pos,
-            lj->d_pos_type, lj->d_table, acc, lj->d_totals, om, pa, nl->items_cap);
-    else
-    {
-        om.atom_local = lj->d_atom_local;
-        k_pair_clusters<2><<<pair_blocks(k_pair_clusters<2>, smem), kPairWarps * 32, smem, s>>>(
-            pc, c, rc, nl->d_counters, nl->d_items, nl->d_ents, nl->d_ents_d, nl->d_slot_atom, lj->d_pos,
-            lj->d_pos_type, lj->d_table, acc, lj->d_totals, om, pa, nl->items_cap);
-    }
-    SPGNB_CHECK_LAUNCH("k_pair_clusters");
+    const FastArgs fa{fp, nullptr, nl, lj->d_pos, lj->d_pos_type, lj->d_table, table_size, (float3*)d_frc,
+                      lj->d_totals, om, pa};
+    if ((st = launch_fast_any(fa, mode, fp.use_fit != 0, nl->triclinic, smem, s))) return st;
     if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
-    const int fb = (local_atom_numbers + 255) / 256;
-    if (mode == 1 && need_virial)
-        k_finalize_slots<true><<<fb, 256, 0, s>>>(local_atom_numbers, nl->d_atom_slot, slots, acc, lj->d_pos,
-                                                  (float3*)d_frc, lj->d_totals);
-    else
-        k_finalize_slots<false><<<fb, 256, 0, s>>>(local_atom_numbers, nl->d_atom_slot, slots, acc, lj->d_pos,
-                                                   (float3*)d_frc, lj->d_totals);
-    SPGNB_CHECK_LAUNCH("k_finalize_slots");
     lj->have_energy = need_atom_energy != 0;
     lj->have_virial = need_virial != 0;
     return SPGNB_OK;
@@ -1111,7 +1225,6 @@ int spgnb_lj_destroy(spgnb_lj* lj)
     dfree(lj->d_table);
     dfree(lj->d_lj_energy_atom);
     dfree(lj->d_frc_acc);
-    dfree(lj->d_slot_acc);
     dfree(lj->d_totals);
     dfree(lj->d_pos);
     dfree(lj->d_pos_type);

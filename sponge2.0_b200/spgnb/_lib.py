@@ -51,13 +51,14 @@ class NLOptions(C.Structure):
                 ("max_ghost_in_grid_numbers", C.c_int), ("refresh_interval", C.c_int),
                 ("skin_permit", C.c_float), ("check_overflow_interval", C.c_int),
                 ("throw_error_when_overflow", C.c_int), ("export_atom_groups", C.c_int),
-                ("max_entries_per_cluster", C.c_int)]
+                ("max_entries_per_cluster", C.c_int), ("prune_buffer", C.c_float)]
 
 
 class NLStats(C.Structure):
     _fields_ = [("atom_numbers", C.c_int), ("grid_numbers", C.c_int), ("grid_dims", C.c_int * 3),
                 ("clusters", C.c_int), ("entries", C.c_longlong), ("work_items", C.c_int),
-                ("builds", C.c_longlong), ("overflow", C.c_int)]
+                ("builds", C.c_longlong), ("overflow", C.c_int), ("full_list_words", C.c_longlong),
+                ("prunes", C.c_longlong), ("pruned_list_words", C.c_longlong)]
 
 
 _lib = None
