@@ -250,6 +250,9 @@ struct spgnb_lj
     float4* d_pos = nullptr;         // per slot (spgnb list) or per atom (atom-group path)
     int* d_pos_type = nullptr;
     int pos_cap = 0;
+    float4* d_sdata = nullptr;       // spgnb list: per-step slot offsets and charges (+ the null slot)
+    int* d_slot_type = nullptr;
+    int sdata_cap = 0;
     int local_atoms = 0;
     bool have_energy = false, have_virial = false;
     double totals[8] = {0};

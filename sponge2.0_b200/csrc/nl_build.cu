@@ -1114,7 +1114,8 @@ int alloc_words(spgnb_nl* nl)
     dfree(nl->d_pwords);
     nl->words_cap = (long long)(nl->words_per_atom * nl->n_cap) + 4096;
     int st = dalloc(&nl->d_words, (size_t)nl->words_cap);
-    if (!st) st = dalloc(&nl->d_pwords, (size_t)nl->words_cap);
+    // the pruned copies: same starts rounded to even words, 64 spare words per slot
+    if (!st) st = dalloc(&nl->d_pwords, (size_t)(nl->words_cap + 64LL * (nl->clusters_cap + 1) * kClusterSize + 2));
     return st;
 }
 
@@ -1155,7 +1156,7 @@ int alloc_nl(spgnb_nl* nl)
     }
     nl->G = G;
     nl->clusters_cap = n / kClusterSize + G + nl->S + 1;
-    if ((long long)nl->clusters_cap * kClusterSize > kMaxSlots)
+    if ((long long)(nl->clusters_cap + 1) * kClusterSize > kMaxSlots)
         return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d atoms in %d cells exceed the %d-slot limit of the lists",
                     n, G, kMaxSlots);
     const size_t slots = (size_t)nl->clusters_cap * kClusterSize;
@@ -1207,7 +1208,9 @@ int alloc_nl(spgnb_nl* nl)
     if ((st = dalloc(&nl->d_cl_sys, nl->clusters_cap))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_cl_sys, 0, sizeof(int) * nl->clusters_cap));
     if ((st = dalloc(&nl->d_cl_u, nl->clusters_cap))) return st;
-    if ((st = dalloc(&nl->d_cl_q, nl->clusters_cap))) return st;
+    // one more: the null cluster of the padding slot (centre 0)
+    if ((st = dalloc(&nl->d_cl_q, nl->clusters_cap + 1))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_cl_q, 0, sizeof(int4) * (nl->clusters_cap + 1)));
     if ((st = dalloc(&nl->d_cl_c, nl->clusters_cap))) return st;
     if ((st = dalloc(&nl->d_nbr_count, nl->clusters_cap))) return st;
     if ((st = dalloc(&nl->d_nbr_fill, nl->clusters_cap))) return st;

@@ -99,11 +99,13 @@ struct PerAtomOut
     float* virial;       // caller's LTMatrix3 array (+=), 6 floats per atom
 };
 
-// Per-step slot pack: offsets from the build-time cluster centre moved by the
-// displacement since the build (minimum image in the system's box, so a
-// caller that wraps coordinates between builds is fine), with the charge.
-// With pruning on (pref set) it also flags a re-pruning when some atom moved
-// more than half the prune buffer since the last one.
+// Per-step slot pack: each slot's offset from the build-time cluster centre
+// moved by the displacement since the build (minimum image in the system's
+// box, so a caller that wraps coordinates between builds is fine), with the
+// charge, and its LJ type.  Slot slots_cap is the null partner that pads the
+// pruned lists: 10^4 A away from everything, charge 0.  With pruning on
+// (pref set) the kernel also flags a re-pruning when some atom moved more
+// than half the prune buffer since the last one.
 __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict__ slot_atom,
                              const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
                              const float4* __restrict__ x0, const float4* __restrict__ d0,
@@ -113,16 +115,18 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     bool moved = false;
-    if (s < slots_cap && s < counters[kCntClusters] * kClusterSize)
+    if (s == slots_cap)
+    {
+        pos[s] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
+        ptype[s] = 0;
+    }
+    else if (s < slots_cap && s < counters[kCntClusters] * kClusterSize)
     {
         const int a = slot_atom[s];
         const float4 d = d0[s];
-        if (a < 0)
-        {
-            pos[s] = make_float4(d.x, d.y, d.z, 0.0f);
-            ptype[s] = 0;
-        }
-        else
+        float4 p = make_float4(d.x, d.y, d.z, 0.0f);
+        int t = 0;
+        if (a >= 0)
         {
             const SysDesc& D = sys[cl_sys[s >> 3]];
             const float3 c = crd[a];
@@ -134,9 +138,8 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
             dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
             dy -= sy * D.cell.a22 + sz * D.cell.a32;
             dz -= sz * D.cell.a33;
-            const float4 p = make_float4(d.x + dx, d.y + dy, d.z + dz, charge[a]);
-            pos[s] = p;
-            ptype[s] = local_type[a];
+            p = make_float4(d.x + dx, d.y + dy, d.z + dz, charge[a]);
+            t = local_type[a];
             if (pref)
             {
                 const float4 r = pref[s];
@@ -144,18 +147,29 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
                 moved = ex * ex + ey * ey + ez * ez > half_buffer2;
             }
         }
+        pos[s] = p;
+        ptype[s] = t;
     }
     if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicExch(&counters[kCntPrune], 1);
+}
+
+// First word of a slot's pruned list: the full list's start rounded up to
+// an even word (8-byte aligned pairs of words) plus 64 spare words per slot
+// for the padding.
+__device__ __forceinline__ long long pruned_start(long long full_start, int s)
+{
+    return ((full_start + 1) & ~1LL) + 64LL * s;
 }
 
 // Pruning (no reference counterpart; results unchanged).  Run after every
 // rebuild and whenever some atom moved more than buffer/2 since the last run
 // (the pack kernel checks): copies each atom's full-list partners whose
 // distance is below cutoff + buffer now, in list order, as 32-bit words
-// {partner slot | LJ type << 23 | per-pair image flag << 31}, and records the
-// slot offsets it saw.  Any pair within the cutoff before the next pruning
-// was within cutoff + buffer at this one, so the copy misses none.  buffer <= 0
-// keeps every listed pair (format conversion only).  The last block to finish
+// {partner slot | LJ type << 23 | per-pair image flag << 31}, pads the copy
+// to a multiple of 64 words with the null slot, and records the slot offsets
+// it saw.  Any pair within the cutoff before the next pruning was within
+// cutoff + buffer at this one, so the copy misses none.  buffer <= 0 keeps
+// every listed pair (format conversion only).  The last block to finish
 // clears the flag.
 constexpr int kPruneWarps = 8;
 
@@ -172,6 +186,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
     const int a = threadIdx.x >> 5;
     const int nc = min(counters[kCntClusters], clusters_cap);
     const bool lists_ok = word_total(counters) <= words_cap;
+    const unsigned null_word = (unsigned)(clusters_cap * kClusterSize);
     __shared__ unsigned long long kept_total;
     if (threadIdx.x == 0) kept_total = 0;
     __syncthreads();
@@ -182,12 +197,13 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
         if (lane == 0) pref[s] = pi;
         const int n = lists_ok ? slot_count[s] : 0;
         int kept = 0;
+        const long long base = slot_start[s];
+        unsigned* __restrict__ out_words = pwords + pruned_start(base, s);
         if (n > 0)
         {
             const ForceParams P = fps ? fps[cl_sys[c]] : p0;
             const float rp = sqrtf(P.rc2) + buffer + 1e-3f;
             const float rp2 = buffer > 0.0f ? rp * rp : 3.0e38f;
-            const long long base = slot_start[s];
             const unsigned short* __restrict__ wl = words + base;
             const float4* __restrict__ tb = tab + nbr_start[c];
             unsigned w = lane < n ? wl[lane] : 0u;
@@ -222,13 +238,16 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
                     out = (unsigned)js | ((unsigned)tj << 23) | ((eb & (1 << 30)) ? 0x80000000u : 0u);
                 }
                 const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (keep) pwords[base + kept + __popc(m & ((1u << lane) - 1u))] = out;
+                if (keep) out_words[kept + __popc(m & ((1u << lane) - 1u))] = out;
                 kept += __popc(m);
             }
         }
+        // pad to a multiple of 64 words with the null partner
+        const int padded = (kept + 63) & ~63;
+        for (int k = kept + lane; k < padded; k += 32) out_words[k] = null_word;
         if (lane == 0)
         {
-            pcount[s] = kept;
+            pcount[s] = padded;
             atomicAdd(&kept_total, (unsigned long long)kept);
         }
     }
@@ -262,7 +281,17 @@ __device__ __forceinline__ float2 poly5x2(float2 x, const float* c)
     return __ffma2_rn(p, x, f2(c[0]));
 }
 
-// pair_scalar for two pairs at once; nA = -A.
+__device__ __forceinline__ float ex2_approx(float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// pair_scalar for two pairs at once; nA = -A.  Without energies the screened
+// Coulomb force uses the K fit; with energies it uses the M fit and
+// exp(-w): beta^3 K(w) = beta (M(w) - 2/sqrt(pi) exp(-w)) / r^2, so
+//   F_c/qq = (t + beta 2/sqrt(pi) exp(-w)) / r^2,  E_c/qq = t,  t = 1/r - beta M(w).
 template <bool ENERGY, int FIT>
 __device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, float2 B, const ForceParams& pc,
                                                float2& e_lj, float2& e_c)
@@ -277,14 +306,22 @@ __device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, 
     if (FIT == 1)
     {
         const float2 x = __fmul2_rn(r2, f2(pc.w_scale));
-        const float2 kp = poly5x2(x, kEwaldKP), kq = poly5x2(x, kEwaldKQ);
-        const float2 K = make_float2(__fdividef(kp.x, kq.x), __fdividef(kp.y, kq.y));
-        fc = __fmul2_rn(qq, __ffma2_rn(f2(-pc.beta3), K, __fmul2_rn(rinv, r2inv)));
-        if (ENERGY)
+        if (!ENERGY)
+        {
+            const float2 kp = poly5x2(x, kEwaldKP), kq = poly5x2(x, kEwaldKQ);
+            const float2 K = make_float2(__fdividef(kp.x, kq.x), __fdividef(kp.y, kq.y));
+            fc = __fmul2_rn(qq, __ffma2_rn(f2(-pc.beta3), K, __fmul2_rn(rinv, r2inv)));
+        }
+        else
         {
             const float2 mp = poly5x2(x, kEwaldMP), mq = poly5x2(x, kEwaldMQ);
             const float2 M = make_float2(__fdividef(mp.x, mq.x), __fdividef(mp.y, mq.y));
-            e_c = __fmul2_rn(qq, __ffma2_rn(f2(-pc.beta), M, rinv));
+            // -w log2(e) = -beta^2 r^2 log2(e)
+            const float2 wl = __fmul2_rn(r2, f2(-pc.beta * pc.beta * 1.4426950408889634f));
+            const float2 E = make_float2(ex2_approx(wl.x), ex2_approx(wl.y));
+            const float2 t = __ffma2_rn(f2(-pc.beta), M, rinv);
+            e_c = __fmul2_rn(qq, t);
+            fc = __fmul2_rn(__fmul2_rn(qq, r2inv), __ffma2_rn(f2(pc.beta * 1.1283791670955126f), E, t));
         }
     }
     else
@@ -316,28 +353,29 @@ __device__ __forceinline__ float centre_step(int qj, int qi)
 }
 
 // Pruned-list force kernel.  A block takes one cluster per pass and each of
-// its eight warps one slot (atom); each lane evaluates two partner words per
-// iteration (k and k + 32 of a 64-word window) with packed FP32x2 arithmetic,
-// and prefetches the next window's words.  A word names the partner slot, so
-// its offset {delta + displacement, q} and its cluster's 22-bit centre load
-// side by side; dr = (c_j - c_i) * cell / 2^22 + p_j - p_i.  Each lane's
-// partial force is converted to int64 fixed point (2^-32 kcal/mol/A) and
-// reduced over the lanes, so the atom's force does not depend on the
-// reduction order; one lane adds it to the caller's array: no atomics,
-// bitwise reproducible.
+// its eight warps one slot (atom); per iteration a lane takes two adjacent
+// words of a 64-word window (one 8-byte load; the lists are padded to whole
+// windows with the null partner, so no bounds checks) and evaluates both
+// pairs with packed FP32x2 arithmetic, with the next window's words already
+// in flight.  A word names the partner slot, so its offset
+// {delta + displacement, q} and its cluster's 22-bit centre load side by
+// side; dr = (c_j - c_i) * cell / 2^22 + p_j - p_i.  Each lane's partial force is
+// converted to int64 fixed point (2^-32 kcal/mol/A) and reduced over the
+// lanes, so the atom's force does not depend on the reduction order; one
+// lane adds it to the caller's array: no atomics, bitwise reproducible.
 //
 // MODE 0: forces.  MODE 1: + energy and virial totals (each pair is seen
 // from both atoms, so the sums are halved).  MODE 2: + per-atom energy and
 // virial of the pairs the atom owns (the lower global index; water sites
 // hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES does).
 template <int MODE, int FIT, bool TRI>
-__global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 3 : 2)
+__global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ? 3 : 2))
     k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
                 const int* __restrict__ counters, long long words_cap, int clusters_cap,
-                const int* __restrict__ cl_sys, const int4* __restrict__ cl_q,
-                const long long* __restrict__ slot_start, const int* __restrict__ pcount,
-                const unsigned* __restrict__ pwords, const int* __restrict__ slot_atom,
-                const float4* __restrict__ slot_x0, const float4* __restrict__ pos, const int* __restrict__ ptype,
+                const int* __restrict__ cl_sys, const long long* __restrict__ slot_start,
+                const int* __restrict__ pcount, const unsigned* __restrict__ pwords,
+                const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0, const int4* __restrict__ cl_q,
+                const float4* __restrict__ pos, const int* __restrict__ ptype,
                 const float2* __restrict__ gtable, int table_size, float3* __restrict__ frc,
                 long long* __restrict__ totals, OwnerMap om, PerAtomOut pa)
 {
@@ -360,18 +398,19 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 3 : 2)
     for (int c = blockIdx.x; lists_ok && c < nc; c += gridDim.x)
     {
         const int s = c * kClusterSize + a;
-        const int n = pcount[s];
+        const int n = pcount[s];  // a multiple of 64
         if (n == 0) continue;
         const int sy = cl_sys[c];
         const ForceParams P = fps ? fps[sy] : p0;
         const Cell qc = sys[sy].qcell;
         const float4 pi = pos[s];
-        const int4 qi = cl_q[c];
-        const int ti = ptype[s] * P.n_types + P.table_begin;
-        const unsigned* __restrict__ wl = pwords + slot_start[s];
+        const int4 ci = cl_q[c];
+        const int qix = ci.x, qiy = ci.y, qiz = ci.z;
         int gi = 0;
         if (PA) gi = __float_as_int(slot_x0[s].w);
-        const float2 npx = f2(-pi.x), npy = f2(-pi.y), npz = f2(-pi.z);
+        const int ti = ptype[s] * P.n_types + P.table_begin;
+        const uint2* __restrict__ wl = reinterpret_cast<const uint2*>(pwords + pruned_start(slot_start[s], s));
+        const float2 npx = f2(-pi.x), npy = f2(-pi.y), npz = f2(-pi.z), qi2 = f2(pi.w);
         float2 fx = f2(0.0f), fy = f2(0.0f), fz = f2(0.0f);
         float2 acc[8], own[8];
 #pragma unroll
@@ -380,47 +419,38 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 3 : 2)
             acc[q] = f2(0.0f);
             own[q] = f2(0.0f);
         }
-        unsigned wA = lane < n ? wl[lane] : 0u;
-        unsigned wB = lane + 32 < n ? wl[lane + 32] : 0u;
+        uint2 w = wl[lane];
 #pragma unroll 1
         for (int k0 = 0; k0 < n; k0 += 64)
         {
-            const unsigned cA = wA, cB = wB;
-            const bool vA = k0 + lane < n, vB = k0 + lane + 32 < n;
-            {
-                const int k = k0 + 64 + lane;
-                wA = k < n ? wl[k] : 0u;
-                wB = k + 32 < n ? wl[k + 32] : 0u;
-            }
-            const int jA = (int)(cA & 0x7fffffu), jB = (int)(cB & 0x7fffffu);
+            const uint2 cw = w;
+            if (k0 + 64 < n) w = wl[(k0 + 64) / 2 + lane];
+            const int jA = (int)(cw.x & 0x7fffffu), jB = (int)(cw.y & 0x7fffffu);
             const float4 pA = pos[jA], pB = pos[jB];
-            const int4 qA = cl_q[jA >> 3], qB = cl_q[jB >> 3];
-            const float2 abA = table[ti + (int)((cA >> 23) & 0xffu)];
-            const float2 abB = table[ti + (int)((cB >> 23) & 0xffu)];
-            const float2 ux = make_float2(centre_step(qA.x, qi.x), centre_step(qB.x, qi.x));
-            const float2 uy = make_float2(centre_step(qA.y, qi.y), centre_step(qB.y, qi.y));
-            const float2 uz = make_float2(centre_step(qA.z, qi.z), centre_step(qB.z, qi.z));
-            float2 dx = __fadd2_rn(make_float2(pA.x, pB.x), npx);
-            float2 dy = __fadd2_rn(make_float2(pA.y, pB.y), npy);
-            float2 dz = __fadd2_rn(make_float2(pA.z, pB.z), npz);
-            dx = __ffma2_rn(ux, f2(qc.a11), dx);
-            dy = __ffma2_rn(uy, f2(qc.a22), dy);
-            dz = __ffma2_rn(uz, f2(qc.a33), dz);
+            const int4 cA = cl_q[jA >> 3], cB = cl_q[jB >> 3];
+            const float2 abA = table[ti + (int)((cw.x >> 23) & 0xffu)];
+            const float2 abB = table[ti + (int)((cw.y >> 23) & 0xffu)];
+            const float2 ux = make_float2(centre_step(cA.x, qix), centre_step(cB.x, qix));
+            const float2 uy = make_float2(centre_step(cA.y, qiy), centre_step(cB.y, qiy));
+            const float2 uz = make_float2(centre_step(cA.z, qiz), centre_step(cB.z, qiz));
+            float2 dx = __ffma2_rn(ux, f2(qc.a11), __fadd2_rn(make_float2(pA.x, pB.x), npx));
+            float2 dy = __ffma2_rn(uy, f2(qc.a22), __fadd2_rn(make_float2(pA.y, pB.y), npy));
+            float2 dz = __ffma2_rn(uz, f2(qc.a33), __fadd2_rn(make_float2(pA.z, pB.z), npz));
             if (TRI)
             {
                 dx = __ffma2_rn(uy, f2(qc.a21), dx);
                 dx = __ffma2_rn(uz, f2(qc.a31), dx);
                 dy = __ffma2_rn(uz, f2(qc.a32), dy);
             }
-            if ((cA | cB) & 0x80000000u)
+            if ((cw.x | cw.y) & 0x80000000u)
             {
                 // small box: these partners need a per-pair image
                 const SysDesc& D = sys[sy];
                 float ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
-                const unsigned cw[2] = {cA, cB};
+                const unsigned wv[2] = {cw.x, cw.y};
                 for (int h = 0; h < 2; h++)
                 {
-                    if (!(cw[h] & 0x80000000u)) continue;
+                    if (!(wv[h] & 0x80000000u)) continue;
                     const float sx = rintf(ddx[h] * D.rcell.a11 + ddy[h] * D.rcell.a21 + ddz[h] * D.rcell.a31);
                     const float sy2 = rintf(ddy[h] * D.rcell.a22 + ddz[h] * D.rcell.a32);
                     const float sz = rintf(ddz[h] * D.rcell.a33);
@@ -433,10 +463,10 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 3 : 2)
                 dz = make_float2(ddz[0], ddz[1]);
             }
             const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-            const bool inA = vA && r2.x < P.rc2, inB = vB && r2.y < P.rc2;
+            const bool inA = r2.x < P.rc2, inB = r2.y < P.rc2;
             float2 elj, ec;
-            float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(make_float2(pA.w, pB.w), f2(pi.w)),
-                                             make_float2(abA.x, abB.x), make_float2(abA.y, abB.y), P, elj, ec);
+            float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(make_float2(pA.w, pB.w), qi2), make_float2(abA.x, abB.x),
+                                             make_float2(abA.y, abB.y), P, elj, ec);
             f = make_float2(inA ? f.x : 0.0f, inB ? f.y : 0.0f);
             const float2 gx = __fmul2_rn(f, dx), gy = __fmul2_rn(f, dy), gz = __fmul2_rn(f, dz);
             fx = __fadd2_rn(fx, gx);
@@ -844,6 +874,19 @@ PairConst make_pair_const(const spgnb_lj* lj, float beta)
     return pc;
 }
 
+// Slot offsets and types plus the null slot.
+int ensure_slots(spgnb_lj* lj, int slots)
+{
+    if (slots + 1 <= lj->sdata_cap) return SPGNB_OK;
+    dfree(lj->d_sdata);
+    dfree(lj->d_slot_type);
+    int st;
+    if ((st = dalloc(&lj->d_sdata, (size_t)(slots + 1)))) return st;
+    if ((st = dalloc(&lj->d_slot_type, (size_t)(slots + 1)))) return st;
+    lj->sdata_cap = slots + 1;
+    return SPGNB_OK;
+}
+
 int ensure_pos(spgnb_lj* lj, int count)
 {
     if (count <= lj->pos_cap) return SPGNB_OK;
@@ -902,8 +945,8 @@ int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
     const spgnb_nl* nl = x.nl;
     const int grid = std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T>, kForceWarps * 32, smem), nl->clusters_cap));
     k_pair_fast<M, F, T><<<grid, kForceWarps * 32, smem, s>>>(
-        x.p0, x.fps, nl->d_sys, nl->d_counters, nl->words_cap, nl->clusters_cap, nl->d_cl_sys, nl->d_cl_q,
-        nl->d_slot_start, nl->d_pcount, nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, x.pos, x.ptype, x.table,
+        x.p0, x.fps, nl->d_sys, nl->d_counters, nl->words_cap, nl->clusters_cap, nl->d_cl_sys, nl->d_slot_start,
+        nl->d_pcount, nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table,
         x.table_size, x.frc, x.totals, x.om, x.pa);
     SPGNB_CHECK_LAUNCH("k_pair_fast");
     return SPGNB_OK;
@@ -1054,7 +1097,7 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
                                    "update; update the list after a box change");
     cudaStream_t s = stream();
     const int slots = nl->clusters_cap * kClusterSize;
-    if ((st = ensure_pos(lj, slots))) return st;
+    if ((st = ensure_slots(lj, slots))) return st;
     SPGNB_CUDA(cudaMemsetAsync(lj->d_totals, 0, sizeof(long long) * 8, s));
     if (need_atom_energy)
     {
@@ -1064,17 +1107,17 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     }
     const bool track = nl->opt.prune_buffer > 0.0f;
     const float half = 0.5f * nl->opt.prune_buffer;
-    k_pack_slots<<<(slots + 255) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_cl_sys,
+    k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_cl_sys,
                                                      nl->d_sys, nl->d_slot_x0, nl->d_slot_d0, (const float3*)d_crd,
-                                                     d_charge, lj->d_local_type, lj->d_pos, lj->d_pos_type,
+                                                     d_charge, lj->d_local_type, lj->d_sdata, lj->d_slot_type,
                                                      track ? nl->d_pref : nullptr, half * half);
     SPGNB_CHECK_LAUNCH("k_pack_slots");
     const ForceParams fp = make_pair_const(lj, pme_beta);
     const int grid = std::max(1, std::min(num_sms() * 4, nl->clusters_cap));
     k_prune<<<grid, kPruneWarps * 32, 0, s>>>(fp, nullptr, nl->opt.prune_buffer, nl->d_counters, nl->words_cap,
                                               nl->clusters_cap, nl->d_cl_sys, nl->d_sys, nl->d_nbr_start, nl->d_tab,
-                                              nl->d_slot_start, nl->d_slot_count, nl->d_words, lj->d_pos,
-                                              lj->d_pos_type, nl->d_pref, nl->d_pcount, nl->d_pwords);
+                                              nl->d_slot_start, nl->d_slot_count, nl->d_words, lj->d_sdata,
+                                              lj->d_slot_type, nl->d_pref, nl->d_pcount, nl->d_pwords);
     SPGNB_CHECK_LAUNCH("k_prune");
     OwnerMap om{nullptr, local_atom_numbers, 3};
     PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
@@ -1097,7 +1140,7 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     cudaEvent_t ev0, ev1;
     pair_events(&ev0, &ev1);
     if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
-    const FastArgs fa{fp, nullptr, nl, lj->d_pos, lj->d_pos_type, lj->d_table, table_size, (float3*)d_frc,
+    const FastArgs fa{fp, nullptr, nl, lj->d_sdata, lj->d_slot_type, lj->d_table, table_size, (float3*)d_frc,
                       lj->d_totals, om, pa};
     if ((st = launch_fast_any(fa, mode, fp.use_fit != 0, nl->triclinic, smem, s))) return st;
     if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
@@ -1228,6 +1271,8 @@ int spgnb_lj_destroy(spgnb_lj* lj)
     dfree(lj->d_totals);
     dfree(lj->d_pos);
     dfree(lj->d_pos_type);
+    dfree(lj->d_sdata);
+    dfree(lj->d_slot_type);
     delete lj;
     return SPGNB_OK;
 }
