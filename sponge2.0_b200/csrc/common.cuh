@@ -63,7 +63,7 @@ void dfree(T*& p)
 
 // ---------------------------------------------------------------- constants
 constexpr int kClusterSize = 8;       // atoms per cluster
-constexpr int kChunk = 32;            // cluster-pair entries per work item
+constexpr int kChunk = 32;            // table elements a search warp stages before writing
 constexpr int kMaxStencil = 192;      // MAX_GRID_NEIGHBORS of neighbor_list.cpp:3
 constexpr int kMaxCellAtoms = 2048;   // hard per-cell capacity of the in-cell sort
 constexpr double kForceScale = 4294967296.0;   // 2^32 per kcal/mol/A
@@ -76,13 +76,13 @@ enum Counter
 {
     kCntClusters = 0,
     kCntItems = 1,
-    kCntEntries = 2,    // 64-bit counter occupies slots 2,3
+    kCntEntries = 2,    // 64-bit: neighbour-table elements of the last build (slots 2,3)
     kCntOverflow = 4,   // bit flags
     kCntNeed = 5,       // rebuild requested for the current update
     kCntBuilds = 6,
     kCntMaxCell = 7,
     kCntWords = 8,      // 64-bit: full-list words of the last build (slots 8,9)
-    kCntNbr = 10,       // neighbour-table entries of the last build
+    kCntNbr = 10,       // (unused)
     kCntPrune = 11,     // pruned lists must be rebuilt before the next force
     kCntPruneDone = 12, // blocks of the running prune kernel that finished
     kCntPrunes = 13,    // prunings performed
@@ -95,10 +95,10 @@ enum OverflowBits
 {
     kOvfList = 1,      // neighbour count above max_neighbor_numbers (export)
     kOvfGrid = 2,      // cell above max_atom_in_grid_numbers
-    kOvfPairs = 4,     // cluster-pair list capacity
+    kOvfPairs = 4,     // a neighbour table above its capacity
     kOvfCellHard = 8,  // cell above the in-cell sort capacity
     kOvfStencil = 16,
-    kOvfTable = 32,    // neighbour table of a cluster above its capacity
+    kOvfTable = 32,    // (unused)
     kOvfWords = 64     // full-list words capacity
 };
 
@@ -138,10 +138,8 @@ struct ForceParams
     int use_fit, n_types, table_begin, pad;
 };
 
-constexpr int kMaxTable = 8192;      // neighbour-table entries per cluster (13-bit index)
 constexpr int kMaxSlots = 1 << 23;   // slot index field of a pruned-list word
 constexpr int kMaxTypes = 256;       // LJ type field of a pruned-list word
-constexpr int kSortCap = 1024;       // entries a warp sorts in shared memory
 
 }  // namespace spgnb
 
@@ -171,10 +169,7 @@ struct spgnb_nl
     bool triclinic = false;
     spgnb_nl_options opt{};
     int clusters_cap = 0;
-    long long entries_cap = 0;
-    int items_cap = 0;
-    int entries_per_cluster = 0;
-    long long nbr_cap = 0;
+    int table_cap = 0;     // neighbour-table elements per cluster
     long long words_cap = 0;
     double words_per_atom = 0;
     bool built = false;
@@ -185,8 +180,8 @@ struct spgnb_nl
     int* d_atom_sys = nullptr;    // system of each atom
     int* d_cell_sys = nullptr;    // system of each cell
     // grid
-    int* d_cand_start = nullptr;  // G+1
-    int* d_cand = nullptr;        // cell | flags
+    int* d_run_start = nullptr;   // G+1: candidate runs of each cell
+    int2* d_runs = nullptr;       // {first cell | stencil flags << 28, last cell + 1}
     int* d_cell_count = nullptr;  // G
     int* d_cell_cursor = nullptr; // G
     int* d_cell_cl_start = nullptr;  // G+1 (cluster index)
@@ -200,29 +195,24 @@ struct spgnb_nl
     int* d_slot_atom = nullptr;
     float4* d_slot_x0 = nullptr;  // raw coordinates at the build, w = global index
     float4* d_slot_d0 = nullptr;  // offset from the cluster centre at the build
+    int2* d_slot_ex = nullptr;    // first and last entry of the atom's exclusion list
     int* d_slot_count = nullptr;  // full-list length of each slot
-    long long* d_slot_start = nullptr;  // first word of each slot
+    long long* d_slot_start = nullptr;  // prefix of the full-list lengths
     // per cluster
     int* d_cl_cell = nullptr;
     int* d_cl_sys = nullptr;
     uint4* d_cl_u = nullptr;      // fractional centre (2^32 per box vector), w = radius bits
     int4* d_cl_q = nullptr;       // the same centre as 22-bit integers (2^22 per box vector)
     float4* d_cl_c = nullptr;     // Cartesian centre (wrapped frame), w = radius
-    int* d_nbr_count = nullptr;   // neighbour-table length of each cluster
-    int* d_nbr_start = nullptr;   // clusters_cap + 1
-    int* d_nbr_fill = nullptr;
     long long* d_cl_words = nullptr;       // full-list words of each cluster
     long long* d_cl_word_start = nullptr;  // clusters_cap + 1
-    // cluster-pair list (half, exact masks)
-    int4* d_ents = nullptr;       // {j-cluster, flags, mask bits 0-31, mask bits 32-63}
-    float4* d_ents_d = nullptr;   // centre difference c_j - c_i (minimum image), Cartesian
-    int4* d_items = nullptr;
-    // per-cluster neighbour tables and per-slot full lists
-    int2* d_nbr = nullptr;        // {entry, neighbour cluster | side << 30}
-    float4* d_tab = nullptr;      // {D, neighbour slot base | flags}
-    unsigned short* d_words = nullptr;  // (table index << 3) | j-slot in the neighbour cluster
-    // pruned copies of the full lists (same starts, shorter counts), one
-    // 32-bit word per pair: partner slot | LJ type << 23 | image flag << 31
+    // neighbour tables: every cluster sharing a listed pair with this one, in
+    // search order, table_cap elements reserved per cluster
+    int* d_tcount = nullptr;      // elements of each cluster's table
+    float4* d_tab = nullptr;      // {D = centre difference (minimum image), neighbour slot base | image flag << 30}
+    uint2* d_tmask = nullptr;     // 64-bit pair mask: bit a*8 + b = own slot a with neighbour slot b
+    // pruned per-atom lists, one 32-bit word per pair: partner slot | LJ type
+    // << 23 | image flag << 31, padded to 64-word windows
     unsigned* d_pwords = nullptr;
     int* d_pcount = nullptr;
     float4* d_pref = nullptr;     // slot offsets at the last pruning

@@ -10,52 +10,54 @@ namespace spgnb
 namespace
 {
 
-// Counts listed pairs (mask bits) and those inside the cutoff at the given
-// coordinates, reading the slots the last force call packed.
-__global__ void k_count_pairs(const int* __restrict__ counters, int items_cap, const int4* __restrict__ items,
-                              const int4* __restrict__ ents, const float4* __restrict__ ents_d,
-                              const int* __restrict__ slot_atom, const float4* __restrict__ x0,
-                              const float4* __restrict__ d0, const float3* __restrict__ crd, Cell cell, Cell rcell,
-                              float rc2, unsigned long long* out)
+// Counts listed pairs (each once: from the side of its lower-index atom) and
+// those inside the cutoff at the given coordinates, from the neighbour tables.
+__global__ void k_count_pairs(const int* __restrict__ counters, int clusters_cap, int table_cap,
+                              const int* __restrict__ tcount, const float4* __restrict__ tab,
+                              const uint2* __restrict__ tmask, const int* __restrict__ slot_atom,
+                              const float4* __restrict__ x0, const float4* __restrict__ d0,
+                              const float3* __restrict__ crd, Cell cell, Cell rcell, float rc2,
+                              unsigned long long* out)
 {
-    const int lane = threadIdx.x & 31, jl = lane & 7, row = lane >> 3;
-    const int nitems = min(counters[kCntItems], items_cap);
-    const int total_warps = gridDim.x * (blockDim.x >> 5);
+    const int lane = threadIdx.x & 31;
+    const int nc = min(counters[kCntClusters], clusters_cap);
+    const int warps = gridDim.x * (blockDim.x >> 5);
     unsigned long long listed = 0, inside = 0;
     auto pos = [&](int s) {
-        int a = slot_atom[s];
-        float4 d = d0[s];
+        const int a = slot_atom[s];
+        const float4 d = d0[s];
         if (a < 0) return make_float3(d.x, d.y, d.z);
-        float3 c = crd[a];
-        float4 o = x0[s];
+        const float3 c = crd[a];
+        const float4 o = x0[s];
         float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
-        float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
-        float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
-        float sz = rintf(dz * rcell.a33);
+        const float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
+        const float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
+        const float sz = rintf(dz * rcell.a33);
         dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
         dy -= sy * cell.a22 + sz * cell.a32;
         dz -= sz * cell.a33;
         return make_float3(d.x + dx, d.y + dy, d.z + dz);
     };
-    for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += total_warps)
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nc; c += warps)
     {
-        int4 item = items[it];
-        for (int e = item.y; e < item.y + item.z; e++)
+        const int T = tcount[c];
+        for (int t = lane; t < T; t += 32)
         {
-            int4 en = ents[e];
-            float4 D = ents_d[e];
-            float3 pj = pos(en.x * kClusterSize + jl);
-            for (int h = 0; h < 2; h++)
+            const float4 e = tab[(size_t)c * table_cap + t];
+            const uint2 mm = tmask[(size_t)c * table_cap + t];
+            unsigned long long m = ((unsigned long long)mm.y << 32) | mm.x;
+            const int base = __float_as_int(e.w) & 0x3fffffff;
+            while (m)
             {
-                unsigned m = (unsigned)(h ? en.w : en.z);
-                if (!((m >> lane) & 1u)) continue;
-                float3 pi = pos(item.x * kClusterSize + row + 4 * h);
-                float dx = D.x + pj.x - pi.x;
-                float dy = D.y + pj.y - pi.y;
-                float dz = D.z + pj.z - pi.z;
-                float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
-                float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
-                float sz = rintf(dz * rcell.a33);
+                const int k = __ffsll((long long)m) - 1;
+                m &= m - 1;
+                const int si = c * kClusterSize + (k >> 3), sj = base + (k & 7);
+                if (!(__float_as_int(x0[si].w) < __float_as_int(x0[sj].w))) continue;
+                const float3 pi = pos(si), pj = pos(sj);
+                float dx = e.x + pj.x - pi.x, dy = e.y + pj.y - pi.y, dz = e.z + pj.z - pi.z;
+                const float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
+                const float sy = rintf(dy * rcell.a22 + dz * rcell.a32);
+                const float sz = rintf(dz * rcell.a33);
                 dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
                 dy -= sy * cell.a22 + sz * cell.a32;
                 dz -= sz * cell.a33;
@@ -119,9 +121,10 @@ int spgnb_nl_count_pairs(spgnb_nl* nl, const spgnb_vector* d_crd, spgnb_ltmatrix
     if (st) return st;
     cudaStream_t s = stream();
     cudaMemsetAsync(d, 0, 16, s);
-    k_count_pairs<<<num_sms() * 8, 128, 0, s>>>(nl->d_counters, nl->items_cap, nl->d_items, nl->d_ents, nl->d_ents_d,
-                                                nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_d0, (const float3*)d_crd,
-                                                make_cell(cell), make_cell(rcell), cutoff * cutoff, d);
+    k_count_pairs<<<num_sms() * 8, 128, 0, s>>>(nl->d_counters, nl->clusters_cap, nl->table_cap, nl->d_tcount,
+                                                nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_d0,
+                                                (const float3*)d_crd, make_cell(cell), make_cell(rcell),
+                                                cutoff * cutoff, d);
     cudaError_t e = cudaGetLastError();
     unsigned long long h[2] = {0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, 16, cudaMemcpyDeviceToHost, s);

@@ -13,11 +13,10 @@
 // Stages of one rebuild (every kernel returns at once when no rebuild is due,
 // so a step never synchronises with the host):
 //   bin -> scan -> scatter -> in-cell sort -> cluster centres   (clusters)
-//   search            -> half cluster-pair list, exact 64-bit pair masks
-//   neighbour tables  -> per cluster, every neighbour cluster, sorted
-//   full lists        -> per atom, every listed partner as a 16-bit word
-// The force kernel reads the full lists; the reference-layout export reads the
-// half list.
+//   search  -> per cluster, its neighbour clusters with exact 64-bit masks
+//   starts  -> per-atom list lengths and offsets
+// The force call prunes the tables into per-atom lists (pair.cu); the
+// reference-layout export reads the tables.
 #include <math.h>
 #include <string.h>
 
@@ -63,27 +62,6 @@ __device__ __forceinline__ float ref_pair_dr2(float3 a, float3 b, const Cell& c,
     dy = __fsub_rn(dy, ty);
     dz = __fmaf_rn(-sz, c.a33, dz);
     return __fmaf_rn(dz, dz, __fmaf_rn(dx, dx, __fmul_rn(dy, dy)));
-}
-
-// A cluster-pair mask has bit a*8 + b set when i-slot a and j-slot b are
-// listed.  Row a: the j-slots paired with i-slot a.  Column b: the i-slots
-// paired with j-slot b, gathered into a byte (the multiply moves bit 8k to
-// bit 56 + k with no carries between the eight terms).
-__device__ __forceinline__ unsigned mask_row(unsigned long long m, int a) { return (unsigned)(m >> (8 * a)) & 0xffu; }
-
-__device__ __forceinline__ unsigned mask_column(unsigned long long m, int b)
-{
-    const unsigned long long x = (m >> b) & 0x0101010101010101ull;
-    return (unsigned)((x * 0x0102040810204080ull) >> 56);
-}
-
-// Partners of own slot a in a neighbour-table element of the given side
-// (0: own cluster is the entry's i-cluster, 1: its j-cluster, 2: both).
-__device__ __forceinline__ unsigned partners(unsigned long long m, int side, int a)
-{
-    unsigned p = side == 0 ? mask_row(m, a) : mask_column(m, a);
-    if (side == 2) p |= mask_row(m, a);
-    return p;
 }
 
 // ---------------------------------------------------------------- kernels
@@ -310,7 +288,9 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, const int* __res
                                 const int* __restrict__ atom_shift, const int* __restrict__ atom_local,
                                 const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys, int* counters,
                                 uint4* __restrict__ cl_u, int4* __restrict__ cl_q, float4* __restrict__ cl_c,
-                                float4* __restrict__ slot_x0, float4* __restrict__ slot_d0, int clusters_cap)
+                                float4* __restrict__ slot_x0, float4* __restrict__ slot_d0,
+                                int2* __restrict__ slot_ex, const int* __restrict__ ex_start,
+                                const int* __restrict__ ex_list, const int* __restrict__ ex_num, int clusters_cap)
 {
     if (counters[kCntNeed] == 0) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -376,13 +356,18 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, const int* __res
         const double d0 = w[0] - cq[0], d1 = w[1] - cq[1], d2 = w[2] - cq[2];
         r2 = d0 * d0 + d1 * d1 + d2 * d2;
         slot_d0[s] = make_float4((float)d0, (float)d1, (float)d2, 0.0f);
-        slot_x0[s] = make_float4(x.x, x.y, x.z, __int_as_float(atom_local[a]));
+        const int g = atom_local[a];
+        slot_x0[s] = make_float4(x.x, x.y, x.z, __int_as_float(g));
+        // [first, last] of the atom's (sorted) exclusion list, empty when none
+        const int k = ex_num[g];
+        slot_ex[s] = k > 0 ? make_int2(ex_list[ex_start[g]], ex_list[ex_start[g] + k - 1]) : make_int2(0x7fffffff, -1);
     }
     else if (live)
     {
         const float p = kPadCoordinate + (float)s;
         slot_d0[s] = make_float4(p, p, p, 0.0f);
         slot_x0[s] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+        slot_ex[s] = make_int2(0x7fffffff, -1);
     }
     for (int o = 1; o < 8; o <<= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
     if (live && l8 == 0)
@@ -405,91 +390,98 @@ __device__ __forceinline__ float3 frac_to_cart(float3 f, const Cell& c)
     return make_float3(f.x * c.a11 + f.y * c.a21 + f.z * c.a31, f.y * c.a22 + f.z * c.a32, f.z * c.a33);
 }
 
-__device__ __forceinline__ bool excluded_pair(int glo, int ghi, const int* __restrict__ ex_start,
-                                              const int* __restrict__ ex_list, const int* __restrict__ ex_num)
+// Neighbour search, one warp per cluster, symmetric: every cluster finds all
+// of its neighbour clusters (lower and higher), so its table comes out
+// complete and in a deterministic order (candidate runs, then cluster index)
+// with no sorting or atomics.  For each candidate cluster that passes a
+// conservative sphere test, the 64 atom pairs are decided as the reference
+// decides them: a pair needs the higher-index atom's cell in the stencil of
+// the lower-index atom's cell, squared distance below 4*grid_length^2 in the
+// reference's FP32 expression, and no exclusion.  The distance is first
+// evaluated from the cluster-relative offsets; only pairs within 1e-4*cs2 of
+// the threshold (or of clusters whose spheres reach half a box) are
+// re-evaluated with the reference's exact expression, so every decision is the
+// reference's.  Exclusion lists are scanned only when the partner lies within
+// the list's [first, last] range (the reference's pre-check).  A cluster pair
+// with any listed pair becomes a table element {centre difference, neighbour
+// slot base | image flag} plus its 64-bit mask (bit a*8 + b: own slot a with
+// neighbour slot b); the per-slot partner counts come out with it.
+constexpr int kSearchWarps = 4;
+constexpr float kBorderBand = 1.0e-4f;
+
+__device__ bool excluded_scan(int glo, int ghi, const int* __restrict__ ex_start, const int* __restrict__ ex_list,
+                              const int* __restrict__ ex_num)
 {
     const int k = ex_num[glo];
-    if (k <= 0) return false;
     const int* l = ex_list + ex_start[glo];
-    if (ghi < l[0] || ghi > l[k - 1]) return false;
     for (int t = 0; t < k; t++)
         if (l[t] == ghi) return true;
     return false;
 }
 
-// Cluster-pair search, one warp per i-cluster.  For every stencil cell of the
-// i-cluster's cell, every j-cluster (j >= i in cluster order) that survives a
-// conservative sphere test gets its 64 pairs tested with the reference's
-// expression; a non-zero mask becomes an entry.  Entries of one i-cluster are
-// written in chunks of kChunk behind a work item.
-constexpr int kSearchWarps = 4;
-
 __global__ void __launch_bounds__(kSearchWarps * 32)
-    k_search(const SysDesc* __restrict__ sys, long long entries_cap, int items_cap,
-             const int* __restrict__ cand_start, const int* __restrict__ cand, const int* __restrict__ cell_cl_start,
-             const int* __restrict__ cl_cell, const int* __restrict__ cl_sys, const uint4* __restrict__ cl_u,
-             const float4* __restrict__ slot_x0, const int* __restrict__ ex_start, const int* __restrict__ ex_list,
-             const int* __restrict__ ex_num, int4* __restrict__ ents, float4* __restrict__ ents_d,
-             int4* __restrict__ items, int* counters)
+    k_search(const SysDesc* __restrict__ sys, int table_cap, const int* __restrict__ run_start,
+             const int2* __restrict__ runs, const int* __restrict__ cell_cl_start, const int* __restrict__ cl_cell,
+             const int* __restrict__ cl_sys, const uint4* __restrict__ cl_u, const int4* __restrict__ cl_q,
+             const float4* __restrict__ slot_x0, const float4* __restrict__ slot_d0, const int2* __restrict__ slot_ex,
+             const int* __restrict__ ex_start, const int* __restrict__ ex_list, const int* __restrict__ ex_num,
+             int* __restrict__ tcount, float4* __restrict__ tab, uint2* __restrict__ tmask,
+             int* __restrict__ slot_count, long long* __restrict__ cl_words, int* counters)
 {
     if (counters[kCntNeed] == 0) return;
-    __shared__ int4 stage[kSearchWarps][kChunk];
-    __shared__ float4 stage_d[kSearchWarps][kChunk];
+    __shared__ float4 stage_t[kSearchWarps][kChunk];
+    __shared__ uint2 stage_m[kSearchWarps][kChunk];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int nc = counters[kCntClusters];
     const int total_warps = gridDim.x * kSearchWarps;
-    unsigned long long* ent_counter = (unsigned long long*)&counters[kCntEntries];
+    unsigned long long elements = 0;
 
-    for (int ci = blockIdx.x * kSearchWarps + wib; ci < nc; ci += total_warps)
+    for (int c = blockIdx.x * kSearchWarps + wib; c < nc; c += total_warps)
     {
-        const SysDesc& p = sys[cl_sys[ci]];
-        const int cellA = cl_cell[ci];
-        const uint4 ui = cl_u[ci];
+        const SysDesc& p = sys[cl_sys[c]];
+        const int cellA = cl_cell[c];
+        const uint4 ui = cl_u[c];
+        const int4 qc = cl_q[c];
         const float ri = __uint_as_float(ui.w);
-        // the two i-atoms this lane tests (rounds h = 0, 1)
+        const float band = kBorderBand * p.cs2;
+        // the two own atoms this lane tests (rounds h = 0, 1)
         int ga[2];
-        float3 xa[2];
+        float3 xa[2], da[2];
+        int2 ea[2];
         for (int h = 0; h < 2; h++)
         {
             const int a = h * 4 + (lane >> 3);
-            const float4 x = slot_x0[ci * kClusterSize + a];
+            const float4 x = slot_x0[c * kClusterSize + a];
+            const float4 d = slot_d0[c * kClusterSize + a];
             ga[h] = __float_as_int(x.w);
             xa[h] = make_float3(x.x, x.y, x.z);
+            da[h] = make_float3(d.x, d.y, d.z);
+            ea[h] = slot_ex[c * kClusterSize + a];
         }
-        int staged = 0;
+        unsigned row_count = 0;  // lanes 0-7: partners of own slot `lane`
+        int written = 0, staged = 0;
+        float4* __restrict__ my_tab = tab + (size_t)c * table_cap;
+        uint2* __restrict__ my_mask = tmask + (size_t)c * table_cap;
         auto flush = [&](int count) {
-            long long e0 = 0;
-            int it = 0;
-            if (lane == 0)
+            const int k = written + lane;
+            if (lane < count && k < table_cap)
             {
-                e0 = (long long)atomicAdd(ent_counter, (unsigned long long)count);
-                it = atomicAdd(&counters[kCntItems], 1);
+                my_tab[k] = stage_t[wib][lane];
+                my_mask[k] = stage_m[wib][lane];
             }
-            e0 = __shfl_sync(0xffffffffu, e0, 0);
-            it = __shfl_sync(0xffffffffu, it, 0);
-            const bool ok = (e0 + count <= entries_cap) && (it < items_cap);
-            if (ok && lane < count)
-            {
-                ents[e0 + lane] = stage[wib][lane];
-                ents_d[e0 + lane] = stage_d[wib][lane];
-            }
-            // an item slot that exists is always written, empty when its
-            // entries did not fit, so readers never see a stale range
-            if (lane == 0 && it < items_cap) items[it] = make_int4(ci, ok ? (int)e0 : 0, ok ? count : 0, 0);
-            if (lane == 0 && !ok) atomicOr(&counters[kCntOverflow], kOvfPairs);
+            if (lane == 0 && written + count > table_cap) atomicOr(&counters[kCntOverflow], kOvfPairs);
+            written = min(written + count, table_cap);
             __syncwarp();
         };
 
-        const int k0 = cand_start[cellA], k1 = cand_start[cellA + 1];
-        for (int k = k0; k < k1; k++)
+        for (int r = run_start[cellA]; r < run_start[cellA + 1]; r++)
         {
-            const int cv = cand[k];
-            const int cellB = cv & 0x0fffffff;
-            const bool fwd = (cv >> 28) & 1;  // cellB in stencil(cellA)
-            const bool rev = (cv >> 29) & 1;  // cellA in stencil(cellB)
-            int b0 = max(cell_cl_start[cellB], ci);
-            const int b1 = min(cell_cl_start[cellB + 1], nc);
+            const int2 run = runs[r];
+            const bool fwd = (run.x >> 28) & 1;  // the run's cells are in stencil(cellA)
+            const bool rev = (run.x >> 29) & 1;  // cellA is in their stencils
+            int b0 = cell_cl_start[run.x & 0x0fffffff];
+            const int b1 = min(cell_cl_start[run.y], nc);
             for (; b0 < b1; b0 += 32)
             {
                 const int cj = b0 + lane;
@@ -518,56 +510,65 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
                 unsigned surv = __ballot_sync(0xffffffffu, ok);
                 while (surv)
                 {
-                    const int src = __ffs(surv) - 1;
+                    const int cjs = b0 + __ffs(surv) - 1;
                     surv &= surv - 1;
-                    const int cjs = b0 + src;
                     const int b = lane & 7;
                     const float4 xj = slot_x0[cjs * kClusterSize + b];
+                    const float4 dj = slot_d0[cjs * kClusterSize + b];
+                    const int2 ej = slot_ex[cjs * kClusterSize + b];
                     const int gb = __float_as_int(xj.w);
                     const float3 xb = make_float3(xj.x, xj.y, xj.z);
+                    // centre difference: minimum image of the 22-bit centres
+                    const uint4 uj = cl_u[cjs];
+                    const int4 qj = cl_q[cjs];
+                    const float ux = (float)(((qj.x - qc.x + 0x200000) & 0x3fffff) - 0x200000);
+                    const float uy = (float)(((qj.y - qc.y + 0x200000) & 0x3fffff) - 0x200000);
+                    const float uz = (float)(((qj.z - qc.z + 0x200000) & 0x3fffff) - 0x200000);
+                    const float Dx = ux * p.qcell.a11 + uy * p.qcell.a21 + uz * p.qcell.a31;
+                    const float Dy = uy * p.qcell.a22 + uz * p.qcell.a32;
+                    const float Dz = uz * p.qcell.a33;
+                    // one image per cluster pair is enough when every pair of the
+                    // two spheres stays inside half a box in fractional terms
+                    const float3 fd = frac_delta(ui, uj);
+                    const float rr = ri + __uint_as_float(uj.w);
+                    const bool safe = fabsf(fd.x) + rr * p.frac_norm[0] < 0.49f &&
+                                      fabsf(fd.y) + rr * p.frac_norm[1] < 0.49f &&
+                                      fabsf(fd.z) + rr * p.frac_norm[2] < 0.49f;
                     unsigned bits[2];
                     for (int h = 0; h < 2; h++)
                     {
                         const int a = h * 4 + (lane >> 3);
-                        bool in = ga[h] >= 0 && gb >= 0 && (cjs != ci || b > a);
+                        const bool a_lo = ga[h] < gb;
+                        const bool rule = ga[h] >= 0 && gb >= 0 && (cjs != c || b != a) && (a_lo ? fwd : rev);
+                        const float dx = Dx + (dj.x - da[h].x), dy = Dy + (dj.y - da[h].y), dz = Dz + (dj.z - da[h].z);
+                        const float d2 = dx * dx + dy * dy + dz * dz;
+                        const bool border = rule && (!safe || fabsf(d2 - p.cs2) < band);
+                        bool in = d2 < p.cs2;
+                        if (__any_sync(0xffffffffu, border) && border)
+                        {
+                            const float e2 = a_lo ? ref_pair_dr2(xa[h], xb, p.cell, p.rcell)
+                                                  : ref_pair_dr2(xb, xa[h], p.cell, p.rcell);
+                            in = e2 < p.cs2;
+                        }
+                        in = in && rule;
                         if (in)
                         {
-                            const bool a_lo = ga[h] < gb;
-                            in = a_lo ? fwd : rev;
-                            if (in)
-                            {
-                                const float d2 = a_lo ? ref_pair_dr2(xa[h], xb, p.cell, p.rcell)
-                                                      : ref_pair_dr2(xb, xa[h], p.cell, p.rcell);
-                                in = d2 < p.cs2;
-                                if (in)
-                                    in = !(a_lo ? excluded_pair(ga[h], gb, ex_start, ex_list, ex_num)
-                                                : excluded_pair(gb, ga[h], ex_start, ex_list, ex_num));
-                            }
+                            // the lower index's exclusion list, scanned only within its range
+                            const int2 e = a_lo ? ea[h] : ej;
+                            const int glo = a_lo ? ga[h] : gb, ghi = a_lo ? gb : ga[h];
+                            if (ghi >= e.x && ghi <= e.y) in = !excluded_scan(glo, ghi, ex_start, ex_list, ex_num);
                         }
                         bits[h] = __ballot_sync(0xffffffffu, in);
                     }
                     if (bits[0] | bits[1])
                     {
-                        // one image per entry is enough when every pair of the two
-                        // spheres stays inside half a box in fractional terms
-                        const uint4 uj = cl_u[cjs];
-                        const float3 f = frac_delta(ui, uj);
-                        const float rr = ri + __uint_as_float(uj.w);
-                        const bool safe = fabsf(f.x) + rr * p.frac_norm[0] < 0.49f &&
-                                          fabsf(f.y) + rr * p.frac_norm[1] < 0.49f &&
-                                          fabsf(f.z) + rr * p.frac_norm[2] < 0.49f;
+                        const unsigned long long m = ((unsigned long long)bits[1] << 32) | bits[0];
+                        if (written + staged < table_cap && lane < 8) row_count += __popc((unsigned)(m >> (8 * lane)) & 0xffu);
                         if (lane == 0)
                         {
-                            stage[wib][staged] =
-                                make_int4(cjs, safe ? 0 : kEntPairImage, (int)bits[0], (int)bits[1]);
-                            // centre difference from the quantised centres, in double
-                            const double q = 2.3283064365386963e-10;
-                            const double fx = (double)(int)(uj.x - ui.x) * q, fy = (double)(int)(uj.y - ui.y) * q,
-                                         fz = (double)(int)(uj.z - ui.z) * q;
-                            const Cell& c = p.cell;
-                            stage_d[wib][staged] = make_float4(
-                                (float)(fx * (double)c.a11 + fy * (double)c.a21 + fz * (double)c.a31),
-                                (float)(fy * (double)c.a22 + fz * (double)c.a32), (float)(fz * (double)c.a33), 0.0f);
+                            stage_t[wib][staged] = make_float4(Dx, Dy, Dz,
+                                                               __int_as_float((cjs * kClusterSize) | (safe ? 0 : (1 << 30))));
+                            stage_m[wib][staged] = make_uint2(bits[0], bits[1]);
                         }
                         staged++;
                         __syncwarp();
@@ -581,209 +582,17 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
             }
         }
         if (staged > 0) flush(staged);
-    }
-}
-
-// --------------------------------------------- neighbour tables, full lists
-
-__global__ void k_zero_tables(int n, int* __restrict__ a, int* __restrict__ b, const int* __restrict__ counters)
-{
-    if (counters[kCntNeed] == 0) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n)
-    {
-        a[i] = 0;
-        b[i] = 0;
-    }
-}
-
-// Table length per cluster: each cluster pair counts on both sides, a
-// cluster paired with itself once.
-__global__ void k_nbr_count(const int4* __restrict__ items, const int4* __restrict__ ents, int items_cap,
-                            int* __restrict__ nbr_count, const int* __restrict__ counters)
-{
-    if (counters[kCntNeed] == 0) return;
-    const int nitems = min(counters[kCntItems], items_cap);
-    const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += warps)
-    {
-        const int4 item = items[it];
-        if (lane < item.z)
+        if (lane < 8) slot_count[c * kClusterSize + lane] = (int)row_count;
+        unsigned long long words = lane < 8 ? row_count : 0u;
+        for (int o = 16; o > 0; o >>= 1) words += __shfl_xor_sync(0xffffffffu, words, o);
+        if (lane == 0)
         {
-            const int cj = ents[item.y + lane].x;
-            atomicAdd(&nbr_count[item.x], 1);
-            if (cj != item.x) atomicAdd(&nbr_count[cj], 1);
+            tcount[c] = written;
+            cl_words[c] = (long long)words;
+            elements += (unsigned long long)written;
         }
     }
-}
-
-__global__ void k_scan_nbr(int nc_cap, const int* __restrict__ nbr_count, int* __restrict__ nbr_start,
-                           long long nbr_cap, int* counters)
-{
-    if (counters[kCntNeed] == 0) return;
-    const int nc = min(counters[kCntClusters], nc_cap);
-    const int total = block_scan<int>(nc, [&](int c) { return nbr_count[c]; }, nbr_start);
-    if (threadIdx.x == 0)
-    {
-        nbr_start[nc] = total;
-        counters[kCntNbr] = total;
-        if (total > nbr_cap) atomicOr(&counters[kCntOverflow], kOvfTable);
-    }
-}
-
-// Table elements {entry, neighbour cluster | side << 29} in arrival order;
-// the table kernel sorts them.
-__global__ void k_nbr_fill(const int4* __restrict__ items, const int4* __restrict__ ents, int items_cap,
-                           const int* __restrict__ nbr_start, int* __restrict__ nbr_fill, int2* __restrict__ nbr,
-                           long long nbr_cap, const int* __restrict__ counters)
-{
-    if (counters[kCntNeed] == 0) return;
-    if (counters[kCntNbr] > nbr_cap) return;
-    const int nitems = min(counters[kCntItems], items_cap);
-    const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += warps)
-    {
-        const int4 item = items[it];
-        if (lane < item.z)
-        {
-            const int e = item.y + lane;
-            const int ci = item.x, cj = ents[e].x;
-            if (cj == ci)
-            {
-                const int p = atomicAdd(&nbr_fill[ci], 1);
-                nbr[nbr_start[ci] + p] = make_int2(e, ci | (2 << 29));
-            }
-            else
-            {
-                const int p = atomicAdd(&nbr_fill[ci], 1);
-                nbr[nbr_start[ci] + p] = make_int2(e, cj);
-                const int q = atomicAdd(&nbr_fill[cj], 1);
-                nbr[nbr_start[cj] + q] = make_int2(e, ci | (1 << 29));
-            }
-        }
-    }
-}
-
-constexpr int kTabWarps = 4;
-
-// Per cluster (one warp): sort the table by neighbour cluster so the build is
-// reproducible, write {D, neighbour slot base | flags} (D = neighbour centre
-// minus own centre, minimum image), count each slot's partners.  Tables
-// longer than kSortCap, or all of them when the table array overflowed, get
-// no partners (flagged).
-__global__ void __launch_bounds__(kTabWarps * 32)
-    k_nbr_table(int nc_cap, const int* __restrict__ nbr_start, int2* __restrict__ nbr, long long nbr_cap,
-                const int4* __restrict__ ents, const float4* __restrict__ ents_d, float4* __restrict__ tab,
-                int* __restrict__ slot_count, long long* __restrict__ cl_words, int* counters)
-{
-    if (counters[kCntNeed] == 0) return;
-    __shared__ unsigned long long keys[kTabWarps][kSortCap];
-    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
-    const int nc = min(counters[kCntClusters], nc_cap);
-    const bool tables_ok = counters[kCntNbr] <= nbr_cap;
-    const int warps = gridDim.x * kTabWarps;
-    unsigned long long* k = keys[wib];
-    for (int c = blockIdx.x * kTabWarps + wib; c < nc; c += warps)
-    {
-        const int base = tables_ok ? nbr_start[c] : 0;
-        const int T = tables_ok ? nbr_start[c + 1] - base : 0;
-        if (T > kSortCap)
-        {
-            if (lane == 0) atomicOr(&counters[kCntOverflow], kOvfTable);
-        }
-        if (T == 0 || T > kSortCap)
-        {
-            if (lane < 8) slot_count[c * kClusterSize + lane] = 0;
-            if (lane == 0) cl_words[c] = 0;
-            continue;
-        }
-        int npad = 32;
-        while (npad < T) npad <<= 1;
-        for (int t = lane; t < npad; t += 32)
-        {
-            if (t < T)
-            {
-                const int2 v = nbr[base + t];
-                k[t] = ((unsigned long long)(unsigned)(v.y & 0x1fffffff) << 32) |
-                       ((unsigned long long)((v.y >> 29) & 3) << 30) | (unsigned)t;
-            }
-            else
-                k[t] = ~0ull;
-        }
-        __syncwarp();
-        // bitonic sort in shared memory
-        for (int size = 2; size <= npad; size <<= 1)
-            for (int stride = size >> 1; stride > 0; stride >>= 1)
-            {
-                for (int t = lane; t < npad / 2; t += 32)
-                {
-                    const int lo = 2 * t - (t & (stride - 1));
-                    const int hi = lo + stride;
-                    const bool up = (lo & size) == 0;
-                    const unsigned long long x = k[lo], y = k[hi];
-                    if ((x > y) == up)
-                    {
-                        k[lo] = y;
-                        k[hi] = x;
-                    }
-                }
-                __syncwarp();
-            }
-        // gather the elements in sorted order into the key array (each
-        // lane reads and writes only its own positions), then write back
-        for (int t = lane; t < T; t += 32)
-        {
-            const int2 v = nbr[base + (int)(k[t] & 0x3fffffffu)];
-            k[t] = ((unsigned long long)(unsigned)v.y << 32) | (unsigned)v.x;
-        }
-        __syncwarp();
-        unsigned cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int t = lane; t < T; t += 32)
-        {
-            const unsigned long long kv = k[t];
-            const int e = (int)(kv & 0xffffffffu);
-            const int y = (int)(kv >> 32);
-            nbr[base + t] = make_int2(e, y);
-            const int side = (y >> 29) & 3;
-            const int other = y & 0x1fffffff;
-            const int4 en = ents[e];
-            const float4 d = ents_d[e];
-            float dx = 0.0f, dy = 0.0f, dz = 0.0f;
-            if (side == 0)
-            {
-                dx = d.x;
-                dy = d.y;
-                dz = d.z;
-            }
-            else if (side == 1)
-            {
-                dx = -d.x;
-                dy = -d.y;
-                dz = -d.z;
-            }
-            const int flags = (en.y & kEntPairImage) ? (1 << 30) : 0;
-            tab[base + t] = make_float4(dx, dy, dz, __int_as_float((other * kClusterSize) | flags));
-            const unsigned long long m = ((unsigned long long)(unsigned)en.w << 32) | (unsigned)en.z;
-#pragma unroll
-            for (int a = 0; a < 8; a++) cnt[a] += __popc(partners(m, side, a));
-        }
-        __syncwarp();
-#pragma unroll
-        for (int a = 0; a < 8; a++)
-            for (int o = 16; o > 0; o >>= 1) cnt[a] += __shfl_xor_sync(0xffffffffu, cnt[a], o);
-        unsigned mine = 0;
-        long long tot = 0;
-#pragma unroll
-        for (int a = 0; a < 8; a++)
-        {
-            mine = lane == a ? cnt[a] : mine;
-            tot += cnt[a];
-        }
-        if (lane < 8) slot_count[c * kClusterSize + lane] = (int)mine;
-        if (lane == 0) cl_words[c] = tot;
-    }
+    if (lane == 0 && elements) atomicAdd((unsigned long long*)&counters[kCntEntries], elements);
 }
 
 __global__ void k_scan_words(int nc_cap, const long long* __restrict__ cl_words, long long* __restrict__ cl_word_start,
@@ -801,87 +610,27 @@ __global__ void k_scan_words(int nc_cap, const long long* __restrict__ cl_words,
     }
 }
 
-// Per cluster (one warp): each slot's partners as 16-bit words
-// (table index << 3 | partner slot in the neighbour cluster), in table order
-// then partner order.  When the words do not fit every slot gets none
-// (flagged), so the force kernel never reads past the array.
-__global__ void k_slot_lists(int nc_cap, const int* __restrict__ nbr_start, const int2* __restrict__ nbr,
-                             const int4* __restrict__ ents, const long long* __restrict__ cl_word_start,
-                             int* __restrict__ slot_count, long long* __restrict__ slot_start,
-                             unsigned short* __restrict__ words, long long words_cap, const int* counters)
+// Per-slot starts of the full lists (prefix of the partner counts).
+__global__ void k_slot_starts(int nc_cap, const long long* __restrict__ cl_word_start,
+                              const int* __restrict__ slot_count, long long* __restrict__ slot_start,
+                              const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
-    const bool fits = word_total(counters) <= words_cap;
-    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
     const int nc = min(counters[kCntClusters], nc_cap);
-    const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nc; c += warps)
+    if (c >= nc) return;
+    long long st = cl_word_start[c];
+    for (int a = 0; a < kClusterSize; a++)
     {
-        if (!fits)
-        {
-            if (lane < 8)
-            {
-                slot_count[c * kClusterSize + lane] = 0;
-                slot_start[c * kClusterSize + lane] = 0;
-            }
-            continue;
-        }
-        long long off[8];
-        long long run = cl_word_start[c];
-#pragma unroll
-        for (int a = 0; a < 8; a++)
-        {
-            off[a] = run;
-            run += slot_count[c * kClusterSize + a];
-        }
-        if (lane < 8)
-        {
-            long long v = 0;
-#pragma unroll
-            for (int a = 0; a < 8; a++) v = (lane == a) ? off[a] : v;
-            slot_start[c * kClusterSize + lane] = v;
-        }
-        if (run == cl_word_start[c]) continue;  // no partners (also: table skipped)
-        const int base = nbr_start[c];
-        const int T = nbr_start[c + 1] - base;
-        for (int t0 = 0; t0 < T; t0 += 32)
-        {
-            const int t = t0 + lane;
-            unsigned long long m = 0;
-            int side = 0;
-            if (t < T)
-            {
-                const int2 v = nbr[base + t];
-                side = (v.y >> 29) & 3;
-                const int4 en = ents[v.x];
-                m = ((unsigned long long)(unsigned)en.w << 32) | (unsigned)en.z;
-            }
-#pragma unroll
-            for (int a = 0; a < 8; a++)
-            {
-                unsigned m8 = t < T ? partners(m, side, a) : 0u;
-                const int n8 = __popc(m8);
-                int incl = n8;
-                for (int o = 1; o < 32; o <<= 1)
-                {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                long long w = off[a] + incl - n8;
-                while (m8)
-                {
-                    const int b = __ffs(m8) - 1;
-                    m8 &= m8 - 1;
-                    words[w++] = (unsigned short)((t << 3) | b);
-                }
-                off[a] += __shfl_sync(0xffffffffu, incl, 31);
-            }
-        }
+        slot_start[c * kClusterSize + a] = st;
+        st += slot_count[c * kClusterSize + a];
     }
 }
 
-// Reference-layout export: zero the counts, then scatter every listed pair
-// to its owner (the lower atom_local index) as the reference stores it.
+// Reference-layout export: zero the counts, then every listed pair goes to
+// its owner (the lower atom_local index) as the reference stores it.  Each
+// pair sits in both clusters' tables; the side whose own atom is the lower
+// index emits it.
 __global__ void k_export_zero(int n, spgnb_atom_group* __restrict__ nl, const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
@@ -893,36 +642,52 @@ __global__ void k_export_zero(int n, spgnb_atom_group* __restrict__ nl, const in
     }
 }
 
-__global__ void k_export(const int4* __restrict__ items, const int4* __restrict__ ents,
-                         const int* __restrict__ slot_atom, const int* __restrict__ atom_local,
-                         spgnb_atom_group* __restrict__ nl, int* __restrict__ temp, int max_nb, int* counters,
-                         int items_cap)
+__global__ void k_export(int nc_cap, int table_cap, const int* __restrict__ tcount, const float4* __restrict__ tab,
+                         const uint2* __restrict__ tmask, const int* __restrict__ slot_atom,
+                         const float4* __restrict__ slot_x0, spgnb_atom_group* __restrict__ nl,
+                         int* __restrict__ temp, int max_nb, int* counters)
 {
     if (counters[kCntNeed] == 0) return;
     const int lane = threadIdx.x & 31;
-    const int nitems = min(counters[kCntItems], items_cap);
-    const int total_warps = gridDim.x * (blockDim.x >> 5);
-    for (int it = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); it < nitems; it += total_warps)
+    const int nc = min(counters[kCntClusters], nc_cap);
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nc; c += warps)
     {
-        const int4 item = items[it];
-        const int ci = item.x;
-        for (int e = item.y; e < item.y + item.z; e++)
+        // own atoms and global indices, lane a holds slot a
+        const int own_atom = lane < 8 ? slot_atom[c * kClusterSize + lane] : -1;
+        const int own_g = lane < 8 ? __float_as_int(slot_x0[c * kClusterSize + lane].w) : -1;
+        const int T = tcount[c];
+        for (int t0 = 0; t0 < T; t0 += 32)
         {
-            const int4 en = ents[e];
-            for (int h = 0; h < 2; h++)
+            const int t = t0 + lane;
+            unsigned long long m = 0;
+            int base = 0;
+            if (t < T)
             {
-                const unsigned m = (unsigned)(h ? en.w : en.z);
-                if (!((m >> lane) & 1u)) continue;
-                const int a = h * 4 + (lane >> 3), b = lane & 7;
-                const int ia = slot_atom[ci * kClusterSize + a];
-                const int jb = slot_atom[en.x * kClusterSize + b];
-                const int owner = atom_local[ia] < atom_local[jb] ? ia : jb;
-                const int other = owner == ia ? jb : ia;
-                const int slot = atomicAdd(&nl[owner].atom_numbers, 1);
-                if (slot < max_nb)
-                    temp[(size_t)owner * max_nb + slot] = other;
-                else
-                    atomicOr(&counters[kCntOverflow], kOvfList);
+                const uint2 mm = tmask[(size_t)c * table_cap + t];
+                m = ((unsigned long long)mm.y << 32) | mm.x;
+                base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
+            }
+            for (int a = 0; a < kClusterSize; a++)
+            {
+                const int ia = __shfl_sync(0xffffffffu, own_atom, a);
+                const int gia = __shfl_sync(0xffffffffu, own_g, a);
+                unsigned row = (unsigned)(m >> (8 * a)) & 0xffu;
+                while (row)
+                {
+                    const int b = __ffs(row) - 1;
+                    row &= row - 1;
+                    const float4 xb = slot_x0[base + b];
+                    if (gia < __float_as_int(xb.w))
+                    {
+                        const int jb = slot_atom[base + b];
+                        const int k = atomicAdd(&nl[ia].atom_numbers, 1);
+                        if (k < max_nb)
+                            temp[(size_t)ia * max_nb + k] = jb;
+                        else
+                            atomicOr(&counters[kCntOverflow], kOvfList);
+                    }
+                }
             }
         }
     }
@@ -977,10 +742,12 @@ void grid_dims(const spgnb_ltmatrix3& cell, float cutoff, float skin, int dims[3
 }
 
 // The reference's stencil rule (Find_Neighor_Grids_Device), evaluated per
-// cell by enumerating the offsets instead of the O(G^2) scan; forward and
-// reverse stencils merged with flags (bit 28: B in stencil(A), bit 29: A in
-// stencil(B)).  Cell ids are global (the system's first cell added).
-int build_candidates(const SysHost& sh, std::vector<int>& start, std::vector<int>& cand)
+// cell by enumerating the offsets instead of the O(G^2) scan.  A cell's
+// candidates are the cells B with B in stencil(A) (flag 1) or A in
+// stencil(B) (flag 2), grouped into runs of consecutive cell ids with equal
+// flags: {first | flags << 28, last + 1}.  Cell ids are global (the system's
+// first cell added).
+int build_runs(const SysHost& sh, std::vector<int>& start, std::vector<int2>& runs)
 {
     const int Nx = sh.dims[0], Ny = sh.dims[1], Nz = sh.dims[2];
     const int G = Nx * Ny * Nz;
@@ -1035,12 +802,16 @@ int build_candidates(const SysHost& sh, std::vector<int>& start, std::vector<int
             flag[j] |= 2;
         }
         std::sort(touched.begin(), touched.end());
-        for (int j : touched)
+        for (size_t i = 0; i < touched.size();)
         {
-            cand.push_back((sh.cell_begin + j) | ((flag[j] & 1) << 28) | ((flag[j] & 2) << 28));
-            flag[j] = 0;
+            size_t e = i + 1;
+            while (e < touched.size() && touched[e] == touched[e - 1] + 1 && flag[touched[e]] == flag[touched[i]]) e++;
+            runs.push_back(make_int2((sh.cell_begin + touched[i]) | (flag[touched[i]] << 28),
+                                     sh.cell_begin + touched[e - 1] + 1));
+            i = e;
         }
-        start.push_back((int)cand.size());
+        for (int j : touched) flag[j] = 0;
+        start.push_back((int)runs.size());
     }
     return SPGNB_OK;
 }
@@ -1050,8 +821,8 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_sys);
     dfree(nl->d_atom_sys);
     dfree(nl->d_cell_sys);
-    dfree(nl->d_cand_start);
-    dfree(nl->d_cand);
+    dfree(nl->d_run_start);
+    dfree(nl->d_runs);
     dfree(nl->d_cell_count);
     dfree(nl->d_cell_cursor);
     dfree(nl->d_cell_cl_start);
@@ -1063,6 +834,7 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_slot_atom);
     dfree(nl->d_slot_x0);
     dfree(nl->d_slot_d0);
+    dfree(nl->d_slot_ex);
     dfree(nl->d_slot_count);
     dfree(nl->d_slot_start);
     dfree(nl->d_cl_cell);
@@ -1070,17 +842,11 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_cl_u);
     dfree(nl->d_cl_q);
     dfree(nl->d_cl_c);
-    dfree(nl->d_nbr_count);
-    dfree(nl->d_nbr_start);
-    dfree(nl->d_nbr_fill);
     dfree(nl->d_cl_words);
     dfree(nl->d_cl_word_start);
-    dfree(nl->d_ents);
-    dfree(nl->d_ents_d);
-    dfree(nl->d_items);
-    dfree(nl->d_nbr);
+    dfree(nl->d_tcount);
     dfree(nl->d_tab);
-    dfree(nl->d_words);
+    dfree(nl->d_tmask);
     dfree(nl->d_pwords);
     dfree(nl->d_pcount);
     dfree(nl->d_pref);
@@ -1089,34 +855,24 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_temp);
 }
 
-int alloc_pair_list(spgnb_nl* nl)
+int alloc_tables(spgnb_nl* nl)
 {
     int st;
-    dfree(nl->d_ents);
-    dfree(nl->d_ents_d);
-    dfree(nl->d_items);
-    dfree(nl->d_nbr);
     dfree(nl->d_tab);
-    nl->entries_cap = (long long)nl->clusters_cap * nl->entries_per_cluster;
-    nl->items_cap = (int)std::min<long long>(nl->entries_cap / kChunk + nl->clusters_cap + 1024, 0x7fffffffLL);
-    nl->nbr_cap = std::min<long long>(2 * nl->entries_cap, (1LL << 30) - 1);
-    if ((st = dalloc(&nl->d_ents, (size_t)nl->entries_cap))) return st;
-    if ((st = dalloc(&nl->d_ents_d, (size_t)nl->entries_cap))) return st;
-    if ((st = dalloc(&nl->d_items, (size_t)nl->items_cap))) return st;
-    if ((st = dalloc(&nl->d_nbr, (size_t)nl->nbr_cap))) return st;
-    if ((st = dalloc(&nl->d_tab, (size_t)nl->nbr_cap))) return st;
+    dfree(nl->d_tmask);
+    const size_t n = (size_t)nl->clusters_cap * nl->table_cap;
+    if ((st = dalloc(&nl->d_tab, n))) return st;
+    if ((st = dalloc(&nl->d_tmask, n))) return st;
     return SPGNB_OK;
 }
 
+// The pruned lists: the full lists' starts rounded to even words plus 64
+// spare words per slot for the padding.
 int alloc_words(spgnb_nl* nl)
 {
-    dfree(nl->d_words);
     dfree(nl->d_pwords);
     nl->words_cap = (long long)(nl->words_per_atom * nl->n_cap) + 4096;
-    int st = dalloc(&nl->d_words, (size_t)nl->words_cap);
-    // the pruned copies: same starts rounded to even words, 64 spare words per slot
-    if (!st) st = dalloc(&nl->d_pwords, (size_t)(nl->words_cap + 64LL * (nl->clusters_cap + 1) * kClusterSize + 2));
-    return st;
+    return dalloc(&nl->d_pwords, (size_t)(nl->words_cap + 64LL * (nl->clusters_cap + 1) * kClusterSize + 2));
 }
 
 SysDesc make_desc(const SysHost& sh, float skin_permit)
@@ -1160,9 +916,10 @@ int alloc_nl(spgnb_nl* nl)
         return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d atoms in %d cells exceed the %d-slot limit of the lists",
                     n, G, kMaxSlots);
     const size_t slots = (size_t)nl->clusters_cap * kClusterSize;
-    std::vector<int> start(1, 0), cand;
+    std::vector<int> start(1, 0);
+    std::vector<int2> runs;
     for (auto& sh : nl->sys)
-        if ((st = build_candidates(sh, start, cand))) return st;
+        if ((st = build_runs(sh, start, runs))) return st;
     nl->h_desc.resize(nl->S);
     std::vector<int> atom_sys(n, 0), cell_sys(G, 0);
     for (int s = 0; s < nl->S; s++)
@@ -1178,10 +935,10 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemcpy(nl->d_sys, nl->h_desc.data(), sizeof(SysDesc) * nl->S, cudaMemcpyHostToDevice));
     SPGNB_CUDA(cudaMemcpy(nl->d_atom_sys, atom_sys.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
     SPGNB_CUDA(cudaMemcpy(nl->d_cell_sys, cell_sys.data(), sizeof(int) * G, cudaMemcpyHostToDevice));
-    if ((st = dalloc(&nl->d_cand_start, G + 1))) return st;
-    if ((st = dalloc(&nl->d_cand, cand.size()))) return st;
-    SPGNB_CUDA(cudaMemcpy(nl->d_cand_start, start.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice));
-    SPGNB_CUDA(cudaMemcpy(nl->d_cand, cand.data(), sizeof(int) * cand.size(), cudaMemcpyHostToDevice));
+    if ((st = dalloc(&nl->d_run_start, G + 1))) return st;
+    if ((st = dalloc(&nl->d_runs, runs.size()))) return st;
+    SPGNB_CUDA(cudaMemcpy(nl->d_run_start, start.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice));
+    SPGNB_CUDA(cudaMemcpy(nl->d_runs, runs.data(), sizeof(int2) * runs.size(), cudaMemcpyHostToDevice));
     if ((st = dalloc(&nl->d_cell_count, G))) return st;
     if ((st = dalloc(&nl->d_cell_cursor, G))) return st;
     if ((st = dalloc(&nl->d_cell_cl_start, G + 1))) return st;
@@ -1197,6 +954,7 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemset(nl->d_slot_atom, 0xff, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_slot_x0, slots))) return st;
     if ((st = dalloc(&nl->d_slot_d0, slots))) return st;
+    if ((st = dalloc(&nl->d_slot_ex, slots))) return st;
     if ((st = dalloc(&nl->d_slot_count, slots))) return st;
     if ((st = dalloc(&nl->d_slot_start, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_slot_count, 0, sizeof(int) * slots));
@@ -1212,14 +970,13 @@ int alloc_nl(spgnb_nl* nl)
     if ((st = dalloc(&nl->d_cl_q, nl->clusters_cap + 1))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_cl_q, 0, sizeof(int4) * (nl->clusters_cap + 1)));
     if ((st = dalloc(&nl->d_cl_c, nl->clusters_cap))) return st;
-    if ((st = dalloc(&nl->d_nbr_count, nl->clusters_cap))) return st;
-    if ((st = dalloc(&nl->d_nbr_fill, nl->clusters_cap))) return st;
-    if ((st = dalloc(&nl->d_nbr_start, nl->clusters_cap + 1))) return st;
     if ((st = dalloc(&nl->d_cl_words, nl->clusters_cap + 1))) return st;
     if ((st = dalloc(&nl->d_cl_word_start, nl->clusters_cap + 1))) return st;
+    if ((st = dalloc(&nl->d_tcount, nl->clusters_cap))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_tcount, 0, sizeof(int) * nl->clusters_cap));
     if ((st = dalloc(&nl->d_counters, kCntSize))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_counters, 0, sizeof(int) * kCntSize));
-    if ((st = alloc_pair_list(nl))) return st;
+    if ((st = alloc_tables(nl))) return st;
     if ((st = alloc_words(nl))) return st;
     if (nl->opt.export_atom_groups)
     {
@@ -1232,9 +989,9 @@ int alloc_nl(spgnb_nl* nl)
     return SPGNB_OK;
 }
 
-// Capacities from the densest system: cluster pairs within rc + skin + 6 A
-// per 8-atom cluster (half list, 2x margin), and listed partners per atom
-// within rc + skin (full list, 1.5x margin).
+// Capacities from the densest system: neighbour clusters within
+// rc + skin + 6 A of an 8-atom cluster (the table, 1.3x margin), and listed
+// partners per atom within rc + skin (the lists, 1.5x margin).
 void estimate_capacities(spgnb_nl* nl)
 {
     double per_cluster = 0, per_atom = 0;
@@ -1243,12 +1000,12 @@ void estimate_capacities(spgnb_nl* nl)
         const double vol = (double)sh.cell.a11 * sh.cell.a22 * sh.cell.a33;
         const double rho = sh.atom_count / vol;
         const double R = sh.cutoff + sh.skin + 6.0;
-        per_cluster = std::max(per_cluster, 4.18879 * R * R * R * rho / kClusterSize);
+        per_cluster = std::max(per_cluster, std::min(4.18879 * R * R * R * rho, (double)sh.atom_count) / kClusterSize);
         const double Rl = sh.cutoff + sh.skin;
         per_atom = std::max(per_atom, std::min(4.18879 * Rl * Rl * Rl * rho, (double)sh.atom_count));
     }
-    nl->entries_per_cluster = nl->opt.max_entries_per_cluster > 0 ? nl->opt.max_entries_per_cluster
-                                                                  : std::max((int)per_cluster + 64, 96);
+    nl->table_cap = nl->opt.max_entries_per_cluster > 0 ? nl->opt.max_entries_per_cluster
+                                                        : std::max((int)(per_cluster * 1.3) + 64, 128);
     nl->words_per_atom = per_atom * 1.5 + 64;
 }
 
@@ -1362,40 +1119,26 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     k_cluster_props<<<(slots_cap + 255) / 256, 256, 0, s>>>(d_crd, nl->d_slot_atom, nl->d_atom_shift, d_atom_local,
                                                              nl->d_cl_sys, nl->d_sys, nl->d_counters, nl->d_cl_u,
                                                              nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0,
-                                                             ccap);
+                                                             nl->d_slot_ex, ex_start, ex_list, ex_num, ccap);
     SPGNB_CHECK_LAUNCH("k_cluster_props");
-    const int search_blocks = std::min((ccap + kSearchWarps - 1) / kSearchWarps, sms * 8);
+    const int search_blocks = std::max(1, std::min((ccap + kSearchWarps - 1) / kSearchWarps, sms * 8));
     k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
-        nl->d_sys, nl->entries_cap, nl->items_cap, nl->d_cand_start, nl->d_cand, nl->d_cell_cl_start, nl->d_cl_cell,
-        nl->d_cl_sys, nl->d_cl_u, nl->d_slot_x0, ex_start, ex_list, ex_num, nl->d_ents, nl->d_ents_d, nl->d_items,
-        nl->d_counters);
+        nl->d_sys, nl->table_cap, nl->d_run_start, nl->d_runs, nl->d_cell_cl_start, nl->d_cl_cell, nl->d_cl_sys,
+        nl->d_cl_u, nl->d_cl_q, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex, ex_start, ex_list, ex_num, nl->d_tcount,
+        nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_cl_words, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_search");
-    k_zero_tables<<<(ccap + 255) / 256, 256, 0, s>>>(ccap, nl->d_nbr_count, nl->d_nbr_fill, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_zero_tables");
-    k_nbr_count<<<sms * 8, 128, 0, s>>>(nl->d_items, nl->d_ents, nl->items_cap, nl->d_nbr_count, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_nbr_count");
-    k_scan_nbr<<<1, 1024, 0, s>>>(ccap, nl->d_nbr_count, nl->d_nbr_start, nl->nbr_cap, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_scan_nbr");
-    k_nbr_fill<<<sms * 8, 128, 0, s>>>(nl->d_items, nl->d_ents, nl->items_cap, nl->d_nbr_start, nl->d_nbr_fill,
-                                        nl->d_nbr, nl->nbr_cap, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_nbr_fill");
-    const int table_blocks = std::max(1, std::min((ccap + kTabWarps - 1) / kTabWarps, sms * 8));
-    k_nbr_table<<<table_blocks, kTabWarps * 32, 0, s>>>(ccap, nl->d_nbr_start, nl->d_nbr, nl->nbr_cap, nl->d_ents,
-                                                         nl->d_ents_d, nl->d_tab, nl->d_slot_count, nl->d_cl_words,
-                                                         nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_nbr_table");
     k_scan_words<<<1, 1024, 0, s>>>(ccap, nl->d_cl_words, nl->d_cl_word_start, nl->words_cap, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_scan_words");
-    k_slot_lists<<<std::max(1, std::min((ccap + 3) / 4, sms * 8)), 128, 0, s>>>(
-        ccap, nl->d_nbr_start, nl->d_nbr, nl->d_ents, nl->d_cl_word_start, nl->d_slot_count, nl->d_slot_start,
-        nl->d_words, nl->words_cap, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_slot_lists");
+    k_slot_starts<<<(ccap + 255) / 256, 256, 0, s>>>(ccap, nl->d_cl_word_start, nl->d_slot_count, nl->d_slot_start,
+                                                      nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_slot_starts");
     if (nl->opt.export_atom_groups)
     {
         k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_export_zero");
-        k_export<<<sms * 8, 128, 0, s>>>(nl->d_items, nl->d_ents, nl->d_slot_atom, d_atom_local, nl->d_nl,
-                                          nl->d_temp, nl->opt.max_neighbor_numbers, nl->d_counters, nl->items_cap);
+        k_export<<<std::max(1, std::min((ccap + 3) / 4, sms * 8)), 128, 0, s>>>(
+            ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_nl,
+            nl->d_temp, nl->opt.max_neighbor_numbers, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_export");
     }
     k_finish<<<(nl->G + 255) / 256, 256, 0, s>>>(nl->G, nl->d_cell_count, nl->d_cell_cursor, nl->d_counters);
@@ -1406,8 +1149,8 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     return SPGNB_OK;
 }
 
-// Regrows what overflowed (1.1x, as neighbor_list.cpp:896-941 does) and
-// clears the flags; the caller forces the next build.
+// Regrows what overflowed (1.1x, as neighbor_list.cpp:896-941 does; the
+// cluster tables 1.3x) and clears the flags; the caller forces the next build.
 int nl_regrow(spgnb_nl* nl, int flags)
 {
     int st;
@@ -1425,8 +1168,8 @@ int nl_regrow(spgnb_nl* nl, int flags)
     }
     if (flags & kOvfPairs)
     {
-        nl->entries_per_cluster = (int)(nl->entries_per_cluster * 1.1) + 8;
-        if ((st = alloc_pair_list(nl))) return st;
+        nl->table_cap = (int)(nl->table_cap * 1.3) + 8;
+        if ((st = alloc_tables(nl))) return st;
     }
     if (flags & kOvfWords)
     {
@@ -1540,7 +1283,7 @@ int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out)
     long long e;
     memcpy(&e, &h[kCntEntries], sizeof(e));
     out->entries = e;
-    out->work_items = h[kCntItems];
+    out->work_items = h[kCntClusters];
     out->builds = h[kCntBuilds];
     out->overflow = h[kCntOverflow];
     out->full_list_words = ((long long)h[kCntWords + 1] << 32) | (unsigned)h[kCntWords];
@@ -1569,11 +1312,6 @@ int spgnb_nl_check_overflow(spgnb_nl* nl, int steps, spgnb_ltmatrix3 cell, spgnb
                     flags);
     if (flags & kOvfCellHard)
         return fail(SPGNB_E_UNSUPPORTED, "NEIGHBOR_LIST: a grid cell holds more than %d atoms", kMaxCellAtoms);
-    if (flags & kOvfTable)
-        return fail(SPGNB_E_UNSUPPORTED,
-                    "NEIGHBOR_LIST: a cluster has more than %d neighbour clusters (cutoff too large for the "
-                    "cluster tables)",
-                    kSortCap);
     int st = nl_regrow(nl, flags);
     if (st) return st;
     if (reinitialized) *reinitialized = 1;

@@ -163,33 +163,36 @@ __device__ __forceinline__ long long pruned_start(long long full_start, int s)
 
 // Pruning (no reference counterpart; results unchanged).  Run after every
 // rebuild and whenever some atom moved more than buffer/2 since the last run
-// (the pack kernel checks): copies each atom's full-list partners whose
-// distance is below cutoff + buffer now, in list order, as 32-bit words
-// {partner slot | LJ type << 23 | per-pair image flag << 31}, pads the copy
-// to a multiple of 64 words with the null slot, and records the slot offsets
-// it saw.  Any pair within the cutoff before the next pruning was within
-// cutoff + buffer at this one, so the copy misses none.  buffer <= 0 keeps
-// every listed pair (format conversion only).  The last block to finish
-// clears the flag.
+// (the pack kernel checks).  For each atom (one warp) it walks its cluster's
+// neighbour table, expands the atom's partners (mask row) of 32 elements at a
+// time into shared memory, keeps those whose distance is below
+// cutoff + buffer now, in table order, as 32-bit words {partner slot | LJ type
+// << 23 | per-pair image flag << 31}, pads the list to a multiple of 64 words
+// with the null slot, and records the slot offsets it saw.  Any pair within
+// the cutoff before the next pruning was within cutoff + buffer at this one,
+// so the copy misses none.  buffer <= 0 keeps every listed pair.  The last
+// block to finish clears the flag.
 constexpr int kPruneWarps = 8;
 
 __global__ void __launch_bounds__(kPruneWarps * 32)
     k_prune(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, long long words_cap,
-            int clusters_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
-            const int* __restrict__ nbr_start, const float4* __restrict__ tab,
+            int clusters_cap, int table_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
+            const int* __restrict__ tcount, const float4* __restrict__ tab, const uint2* __restrict__ tmask,
             const long long* __restrict__ slot_start, const int* __restrict__ slot_count,
-            const unsigned short* __restrict__ words, const float4* __restrict__ pos, const int* __restrict__ ptype,
-            float4* __restrict__ pref, int* __restrict__ pcount, unsigned* __restrict__ pwords)
+            const float4* __restrict__ pos, const int* __restrict__ ptype, float4* __restrict__ pref,
+            int* __restrict__ pcount, unsigned* __restrict__ pwords)
 {
     if (counters[kCntPrune] == 0) return;
+    __shared__ float4 buf[kPruneWarps][kChunk * kClusterSize];
+    __shared__ unsigned long long kept_total;
     const int lane = threadIdx.x & 31;
     const int a = threadIdx.x >> 5;
     const int nc = min(counters[kCntClusters], clusters_cap);
     const bool lists_ok = word_total(counters) <= words_cap;
     const unsigned null_word = (unsigned)(clusters_cap * kClusterSize);
-    __shared__ unsigned long long kept_total;
     if (threadIdx.x == 0) kept_total = 0;
     __syncthreads();
+    float4* __restrict__ mybuf = buf[a];
     for (int c = blockIdx.x; c < nc; c += gridDim.x)
     {
         const int s = c * kClusterSize + a;
@@ -197,49 +200,77 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
         if (lane == 0) pref[s] = pi;
         const int n = lists_ok ? slot_count[s] : 0;
         int kept = 0;
-        const long long base = slot_start[s];
-        unsigned* __restrict__ out_words = pwords + pruned_start(base, s);
+        unsigned* __restrict__ out_words = pwords + pruned_start(slot_start[s], s);
         if (n > 0)
         {
             const ForceParams P = fps ? fps[cl_sys[c]] : p0;
             const float rp = sqrtf(P.rc2) + buffer + 1e-3f;
             const float rp2 = buffer > 0.0f ? rp * rp : 3.0e38f;
-            const unsigned short* __restrict__ wl = words + base;
-            const float4* __restrict__ tb = tab + nbr_start[c];
-            unsigned w = lane < n ? wl[lane] : 0u;
-            for (int k0 = 0; k0 < n; k0 += 32)
+            const int T = tcount[c];
+            const float4* __restrict__ tb = tab + (size_t)c * table_cap;
+            const uint2* __restrict__ tm = tmask + (size_t)c * table_cap;
+            for (int t0 = 0; t0 < T; t0 += 32)
             {
-                const int k = k0 + lane;
-                const unsigned cw = w;
-                w = k + 32 < n ? wl[k + 32] : 0u;
-                bool keep = false;
-                unsigned out = 0;
-                if (k < n)
+                const int t = t0 + lane;
+                unsigned row = 0;
+                float4 e = make_float4(0, 0, 0, 0);
+                if (t < T)
                 {
-                    const float4 e = tb[cw >> 3];
-                    const int eb = __float_as_int(e.w);
-                    const int js = (eb & 0x3fffffff) + (int)(cw & 7u);
-                    const float4 pj = pos[js];
-                    const int tj = ptype[js];
-                    float dx = (e.x - pi.x) + pj.x;
-                    float dy = (e.y - pi.y) + pj.y;
-                    float dz = (e.z - pi.z) + pj.z;
-                    if (eb & (1 << 30))
-                    {
-                        const SysDesc& D = sys[cl_sys[c]];
-                        const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
-                        const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
-                        const float sz = rintf(dz * D.rcell.a33);
-                        dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
-                        dy -= sy * D.cell.a22 + sz * D.cell.a32;
-                        dz -= sz * D.cell.a33;
-                    }
-                    keep = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx)) < rp2;
-                    out = (unsigned)js | ((unsigned)tj << 23) | ((eb & (1 << 30)) ? 0x80000000u : 0u);
+                    e = tb[t];
+                    const uint2 mm = tm[t];
+                    row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (keep) out_words[kept + __popc(m & ((1u << lane) - 1u))] = out;
-                kept += __popc(m);
+                const int cnt = __popc(row);
+                int incl = cnt;
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                const int eb = __float_as_int(e.w);
+                const int flag = (eb & (1 << 30)) ? (int)0x80000000 : 0;
+                int k = incl - cnt;
+                while (row)
+                {
+                    const int b = __ffs(row) - 1;
+                    row &= row - 1;
+                    mybuf[k++] = make_float4(e.x, e.y, e.z, __int_as_float(((eb & 0x3fffffff) + b) | flag));
+                }
+                __syncwarp();
+                for (int q0 = 0; q0 < total; q0 += 32)
+                {
+                    const int q = q0 + lane;
+                    bool keep = false;
+                    unsigned out = 0;
+                    if (q < total)
+                    {
+                        const float4 w = mybuf[q];
+                        const int wi = __float_as_int(w.w);
+                        const int js = wi & 0x7fffffff;
+                        const float4 pj = pos[js];
+                        const int tj = ptype[js];
+                        float dx = (w.x - pi.x) + pj.x;
+                        float dy = (w.y - pi.y) + pj.y;
+                        float dz = (w.z - pi.z) + pj.z;
+                        if (wi < 0)
+                        {
+                            const SysDesc& D = sys[cl_sys[c]];
+                            const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
+                            const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
+                            const float sz = rintf(dz * D.rcell.a33);
+                            dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
+                            dy -= sy * D.cell.a22 + sz * D.cell.a32;
+                            dz -= sz * D.cell.a33;
+                        }
+                        keep = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx)) < rp2;
+                        out = (unsigned)js | ((unsigned)tj << 23) | (wi < 0 ? 0x80000000u : 0u);
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, keep);
+                    if (keep) out_words[kept + __popc(m & ((1u << lane) - 1u))] = out;
+                    kept += __popc(m);
+                }
+                __syncwarp();
             }
         }
         // pad to a multiple of 64 words with the null partner
@@ -1115,9 +1146,9 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     const ForceParams fp = make_pair_const(lj, pme_beta);
     const int grid = std::max(1, std::min(num_sms() * 4, nl->clusters_cap));
     k_prune<<<grid, kPruneWarps * 32, 0, s>>>(fp, nullptr, nl->opt.prune_buffer, nl->d_counters, nl->words_cap,
-                                              nl->clusters_cap, nl->d_cl_sys, nl->d_sys, nl->d_nbr_start, nl->d_tab,
-                                              nl->d_slot_start, nl->d_slot_count, nl->d_words, lj->d_sdata,
-                                              lj->d_slot_type, nl->d_pref, nl->d_pcount, nl->d_pwords);
+                                              nl->clusters_cap, nl->table_cap, nl->d_cl_sys, nl->d_sys, nl->d_tcount,
+                                              nl->d_tab, nl->d_tmask, nl->d_slot_start, nl->d_slot_count,
+                                              lj->d_sdata, lj->d_slot_type, nl->d_pref, nl->d_pcount, nl->d_pwords);
     SPGNB_CHECK_LAUNCH("k_prune");
     OwnerMap om{nullptr, local_atom_numbers, 3};
     PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
