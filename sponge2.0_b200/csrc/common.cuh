@@ -81,7 +81,7 @@ enum Counter
     kCntNeed = 5,       // rebuild requested for the current update
     kCntBuilds = 6,
     kCntMaxCell = 7,
-    kCntWords = 8,      // 64-bit: full-list words of the last build (slots 8,9)
+    kCntWords = 8,      // 64-bit: listed partners summed over atoms, last build (slots 8,9)
     kCntNbr = 10,       // (unused)
     kCntPrune = 11,     // pruned lists must be rebuilt before the next force
     kCntPruneDone = 12, // blocks of the running prune kernel that finished
@@ -99,7 +99,7 @@ enum OverflowBits
     kOvfCellHard = 8,  // cell above the in-cell sort capacity
     kOvfStencil = 16,
     kOvfTable = 32,    // (unused)
-    kOvfWords = 64     // full-list words capacity
+    kOvfWords = 64     // a pruned per-atom list above its capacity
 };
 
 // entry flags
@@ -127,6 +127,8 @@ struct SysDesc
     float frac_norm[3];
     int Nx, Ny, Nz, cell_begin;
     int atom_begin, atom_count, triclinic;
+    int all_safe;   // every cluster pair the search can meet is inside half a box: one image per pair
+    float prune_r2; // squared radius of the pruned lists, (cutoff + buffer)^2; huge when pruning is off
     float permit2;  // squared displacement that triggers a rebuild (skin * skin_permit)^2
     Cell qcell;     // cell / 2^22: Cartesian length of one step of the 22-bit cluster centres
 };
@@ -170,8 +172,8 @@ struct spgnb_nl
     spgnb_nl_options opt{};
     int clusters_cap = 0;
     int table_cap = 0;     // neighbour-table elements per cluster
-    long long words_cap = 0;
-    double words_per_atom = 0;
+    int slot_cap = 0;      // words reserved per atom for its pruned list (a multiple of 64)
+    float prune_rc = 0;    // cutoff the pruned lists are made for
     bool built = false;
     int local_atoms = 0;
 
@@ -197,22 +199,19 @@ struct spgnb_nl
     float4* d_slot_d0 = nullptr;  // offset from the cluster centre at the build
     int2* d_slot_ex = nullptr;    // first and last entry of the atom's exclusion list
     int* d_slot_count = nullptr;  // full-list length of each slot
-    long long* d_slot_start = nullptr;  // prefix of the full-list lengths
     // per cluster
     int* d_cl_cell = nullptr;
     int* d_cl_sys = nullptr;
     uint4* d_cl_u = nullptr;      // fractional centre (2^32 per box vector), w = radius bits
     int4* d_cl_q = nullptr;       // the same centre as 22-bit integers (2^22 per box vector)
-    float4* d_cl_c = nullptr;     // Cartesian centre (wrapped frame), w = radius
-    long long* d_cl_words = nullptr;       // full-list words of each cluster
-    long long* d_cl_word_start = nullptr;  // clusters_cap + 1
+    float4* d_cl_c = nullptr;     // half extents of the cluster's bounding box about its centre, w = radius
     // neighbour tables: every cluster sharing a listed pair with this one, in
     // search order, table_cap elements reserved per cluster
     int* d_tcount = nullptr;      // elements of each cluster's table
     float4* d_tab = nullptr;      // {D = centre difference (minimum image), neighbour slot base | image flag << 30}
     uint2* d_tmask = nullptr;     // 64-bit pair mask: bit a*8 + b = own slot a with neighbour slot b
-    // pruned per-atom lists, one 32-bit word per pair: partner slot | LJ type
-    // << 23 | image flag << 31, padded to 64-word windows
+    // pruned per-atom lists, slot_cap words reserved per slot, one 32-bit word
+    // per pair: partner slot | image flag << 31, padded to 64-word windows
     unsigned* d_pwords = nullptr;
     int* d_pcount = nullptr;
     float4* d_pref = nullptr;     // slot offsets at the last pruning
@@ -267,9 +266,6 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
 int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
                    const int* ex_list, const int* ex_num, bool host_rebuild, cudaStream_t s);
 int nl_regrow(spgnb_nl* nl, int flags);
+int nl_set_prune_rc(spgnb_nl* nl, float rc, cudaStream_t s);
 
-__device__ __forceinline__ long long word_total(const int* counters)
-{
-    return ((long long)counters[kCntWords + 1] << 32) | (unsigned)counters[kCntWords];
-}
 }  // namespace spgnb

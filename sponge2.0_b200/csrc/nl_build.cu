@@ -14,7 +14,6 @@
 // so a step never synchronises with the host):
 //   bin -> scan -> scatter -> in-cell sort -> cluster centres   (clusters)
 //   search  -> per cluster, its neighbour clusters with exact 64-bit masks
-//   starts  -> per-atom list lengths and offsets
 // The force call prunes the tables into per-atom lists (pair.cu); the
 // reference-layout export reads the tables.
 #include <math.h>
@@ -375,7 +374,12 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, const int* __res
         const float rad = (float)(sqrt(r2) * (1.0 + 1e-6) + 1e-5);
         cl_u[k] = make_uint4(u[0], u[1], u[2], __float_as_uint(rad));
         cl_q[k] = make_int4((int)u22[0], (int)u22[1], (int)u22[2], 0);
-        cl_c[k] = make_float4((float)cq[0], (float)cq[1], (float)cq[2], rad);
+        // bounding box about the quantised centre (its offset from the box
+        // middle included), with a little slack
+        float h[3];
+        for (int d = 0; d < 3; d++)
+            h[d] = lo[d] <= hi[d] ? (float)(0.5 * (hi[d] - lo[d]) + fabs(cq[d] - cen[d]) + 1e-4) : 0.0f;
+        cl_c[k] = make_float4(h[0], h[1], h[2], rad);
     }
 }
 
@@ -419,14 +423,15 @@ __device__ bool excluded_scan(int glo, int ghi, const int* __restrict__ ex_start
     return false;
 }
 
-__global__ void __launch_bounds__(kSearchWarps * 32)
+__global__ void __launch_bounds__(kSearchWarps * 32, 5)
     k_search(const SysDesc* __restrict__ sys, int table_cap, const int* __restrict__ run_start,
              const int2* __restrict__ runs, const int* __restrict__ cell_cl_start, const int* __restrict__ cl_cell,
              const int* __restrict__ cl_sys, const uint4* __restrict__ cl_u, const int4* __restrict__ cl_q,
-             const float4* __restrict__ slot_x0, const float4* __restrict__ slot_d0, const int2* __restrict__ slot_ex,
+             const float4* __restrict__ cl_c, const float4* __restrict__ slot_x0, const float4* __restrict__ slot_d0,
+             const int2* __restrict__ slot_ex,
              const int* __restrict__ ex_start, const int* __restrict__ ex_list, const int* __restrict__ ex_num,
              int* __restrict__ tcount, float4* __restrict__ tab, uint2* __restrict__ tmask,
-             int* __restrict__ slot_count, long long* __restrict__ cl_words, int* counters)
+             int* __restrict__ slot_count, int* counters)
 {
     if (counters[kCntNeed] == 0) return;
     __shared__ float4 stage_t[kSearchWarps][kChunk];
@@ -435,7 +440,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
     const int wib = threadIdx.x >> 5;
     const int nc = counters[kCntClusters];
     const int total_warps = gridDim.x * kSearchWarps;
-    unsigned long long elements = 0;
+    unsigned long long elements = 0, listed = 0;
 
     for (int c = blockIdx.x * kSearchWarps + wib; c < nc; c += total_warps)
     {
@@ -444,6 +449,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
         const uint4 ui = cl_u[c];
         const int4 qc = cl_q[c];
         const float ri = __uint_as_float(ui.w);
+        const float4 hc = cl_c[c];
         const float band = kBorderBand * p.cs2;
         // the two own atoms this lane tests (rounds h = 0, 1)
         int ga[2];
@@ -489,15 +495,20 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
                 if (cj < b1)
                 {
                     const uint4 uj = cl_u[cj];
-                    const float rsum = ri + __uint_as_float(uj.w) + p.list_radius;
                     const float3 f = frac_delta(ui, uj);
                     if (!p.triclinic)
                     {
+                        // bounding boxes within the list radius
                         const float3 d = frac_to_cart(f, p.cell);
-                        ok = d.x * d.x + d.y * d.y + d.z * d.z < rsum * rsum;
+                        const float4 hj = cl_c[cj];
+                        const float gx = fmaxf(fabsf(d.x) - (hc.x + hj.x), 0.0f);
+                        const float gy = fmaxf(fabsf(d.y) - (hc.y + hj.y), 0.0f);
+                        const float gz = fmaxf(fabsf(d.z) - (hc.z + hj.z), 0.0f);
+                        ok = gx * gx + gy * gy + gz * gz < p.list_radius * p.list_radius;
                     }
                     else
                     {
+                        const float rsum = ri + __uint_as_float(uj.w) + p.list_radius;
                         for (int im = 0; im < 27 && !ok; im++)
                         {
                             const float3 fi = make_float3(f.x + (float)(im / 9 - 1), f.y + (float)((im / 3) % 3 - 1),
@@ -529,11 +540,14 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
                     const float Dz = uz * p.qcell.a33;
                     // one image per cluster pair is enough when every pair of the
                     // two spheres stays inside half a box in fractional terms
-                    const float3 fd = frac_delta(ui, uj);
-                    const float rr = ri + __uint_as_float(uj.w);
-                    const bool safe = fabsf(fd.x) + rr * p.frac_norm[0] < 0.49f &&
-                                      fabsf(fd.y) + rr * p.frac_norm[1] < 0.49f &&
-                                      fabsf(fd.z) + rr * p.frac_norm[2] < 0.49f;
+                    bool safe = true;
+                    if (!p.all_safe)
+                    {
+                        const float3 fd = frac_delta(ui, uj);
+                        const float rr = ri + __uint_as_float(uj.w);
+                        safe = fabsf(fd.x) + rr * p.frac_norm[0] < 0.49f && fabsf(fd.y) + rr * p.frac_norm[1] < 0.49f &&
+                               fabsf(fd.z) + rr * p.frac_norm[2] < 0.49f;
+                    }
                     unsigned bits[2];
                     for (int h = 0; h < 2; h++)
                     {
@@ -588,42 +602,14 @@ __global__ void __launch_bounds__(kSearchWarps * 32)
         if (lane == 0)
         {
             tcount[c] = written;
-            cl_words[c] = (long long)words;
             elements += (unsigned long long)written;
+            listed += words;
         }
     }
-    if (lane == 0 && elements) atomicAdd((unsigned long long*)&counters[kCntEntries], elements);
-}
-
-__global__ void k_scan_words(int nc_cap, const long long* __restrict__ cl_words, long long* __restrict__ cl_word_start,
-                             long long words_cap, int* counters)
-{
-    if (counters[kCntNeed] == 0) return;
-    const int nc = min(counters[kCntClusters], nc_cap);
-    const long long total = block_scan<long long>(nc, [&](int c) { return cl_words[c]; }, cl_word_start);
-    if (threadIdx.x == 0)
+    if (lane == 0)
     {
-        cl_word_start[nc] = total;
-        counters[kCntWords] = (int)(total & 0xffffffffll);
-        counters[kCntWords + 1] = (int)(total >> 32);
-        if (total > words_cap) atomicOr(&counters[kCntOverflow], kOvfWords);
-    }
-}
-
-// Per-slot starts of the full lists (prefix of the partner counts).
-__global__ void k_slot_starts(int nc_cap, const long long* __restrict__ cl_word_start,
-                              const int* __restrict__ slot_count, long long* __restrict__ slot_start,
-                              const int* __restrict__ counters)
-{
-    if (counters[kCntNeed] == 0) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nc = min(counters[kCntClusters], nc_cap);
-    if (c >= nc) return;
-    long long st = cl_word_start[c];
-    for (int a = 0; a < kClusterSize; a++)
-    {
-        slot_start[c * kClusterSize + a] = st;
-        st += slot_count[c * kClusterSize + a];
+        if (elements) atomicAdd((unsigned long long*)&counters[kCntEntries], elements);
+        if (listed) atomicAdd((unsigned long long*)&counters[kCntWords], listed);
     }
 }
 
@@ -717,6 +703,10 @@ __global__ void k_reset_list_counters(int* counters)
     counters[kCntItems] = 0;
     counters[kCntEntries] = 0;
     counters[kCntEntries + 1] = 0;
+    counters[kCntWords] = 0;
+    counters[kCntWords + 1] = 0;
+    counters[kCntPWordsLast] = 0;
+    counters[kCntPWordsLast + 1] = 0;
 }
 
 __global__ void k_init_atom_groups(int n, spgnb_atom_group* nl, int* temp, int max_nb)
@@ -836,14 +826,11 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_slot_d0);
     dfree(nl->d_slot_ex);
     dfree(nl->d_slot_count);
-    dfree(nl->d_slot_start);
     dfree(nl->d_cl_cell);
     dfree(nl->d_cl_sys);
     dfree(nl->d_cl_u);
     dfree(nl->d_cl_q);
     dfree(nl->d_cl_c);
-    dfree(nl->d_cl_words);
-    dfree(nl->d_cl_word_start);
     dfree(nl->d_tcount);
     dfree(nl->d_tab);
     dfree(nl->d_tmask);
@@ -866,13 +853,19 @@ int alloc_tables(spgnb_nl* nl)
     return SPGNB_OK;
 }
 
-// The pruned lists: the full lists' starts rounded to even words plus 64
-// spare words per slot for the padding.
+// The pruned lists: slot_cap words per slot.
 int alloc_words(spgnb_nl* nl)
 {
     dfree(nl->d_pwords);
-    nl->words_cap = (long long)(nl->words_per_atom * nl->n_cap) + 4096;
-    return dalloc(&nl->d_pwords, (size_t)(nl->words_cap + 64LL * (nl->clusters_cap + 1) * kClusterSize + 2));
+    return dalloc(&nl->d_pwords, (size_t)nl->clusters_cap * kClusterSize * nl->slot_cap);
+}
+
+// Squared radius of the pruned lists for the pruning cutoff rc.
+float prune_r2_of(float rc, float buffer)
+{
+    if (!(buffer > 0.0f)) return 3.0e38f;
+    const float r = rc + buffer + 1e-3f;
+    return r * r;
 }
 
 SysDesc make_desc(const SysHost& sh, float skin_permit)
@@ -895,6 +888,17 @@ SysDesc make_desc(const SysHost& sh, float skin_permit)
     d.triclinic = sh.triclinic ? 1 : 0;
     const float permit = sh.skin * skin_permit;
     d.permit2 = permit * permit;
+    // a cluster lies inside one grid cell (the last cell of a row is the
+    // widest, up to the box edge), so its centre is within half a cell
+    // diagonal of its atoms; every pair the search meets then has fractional
+    // separation below (list radius + 4 half diagonals) * |rcell row|
+    const float wx = fmaxf(sh.gl, sh.cell.a11 - (sh.dims[0] - 1) * sh.gl);
+    const float wy = fmaxf(sh.gl, sh.cell.a22 - (sh.dims[1] - 1) * sh.gl);
+    const float wz = fmaxf(sh.gl, sh.cell.a33 - (sh.dims[2] - 1) * sh.gl);
+    const float hd = 0.5f * sqrtf(wx * wx + wy * wy + wz * wz) + 1e-3f;
+    const float fmax_norm = fmaxf(d.frac_norm[0], fmaxf(d.frac_norm[1], d.frac_norm[2]));
+    d.all_safe = (!sh.triclinic && (d.list_radius + 4.0f * hd) * fmax_norm < 0.45f) ? 1 : 0;
+    d.prune_r2 = 3.0e38f;  // set by the caller
     const float q = 2.384185791015625e-07f;  // 2^-22, exact scaling
     d.qcell = Cell{d.cell.a11 * q, d.cell.a21 * q, d.cell.a22 * q, d.cell.a31 * q, d.cell.a32 * q, d.cell.a33 * q};
     return d;
@@ -926,6 +930,7 @@ int alloc_nl(spgnb_nl* nl)
     {
         const SysHost& sh = nl->sys[s];
         nl->h_desc[s] = make_desc(sh, nl->opt.skin_permit);
+        nl->h_desc[s].prune_r2 = prune_r2_of(nl->prune_rc, nl->opt.prune_buffer);
         for (int i = sh.atom_begin; i < sh.atom_begin + sh.atom_count && i < n; i++) atom_sys[i] = s;
         for (int c = 0; c < sh.dims[0] * sh.dims[1] * sh.dims[2]; c++) cell_sys[sh.cell_begin + c] = s;
     }
@@ -956,9 +961,7 @@ int alloc_nl(spgnb_nl* nl)
     if ((st = dalloc(&nl->d_slot_d0, slots))) return st;
     if ((st = dalloc(&nl->d_slot_ex, slots))) return st;
     if ((st = dalloc(&nl->d_slot_count, slots))) return st;
-    if ((st = dalloc(&nl->d_slot_start, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_slot_count, 0, sizeof(int) * slots));
-    SPGNB_CUDA(cudaMemset(nl->d_slot_start, 0, sizeof(long long) * slots));
     if ((st = dalloc(&nl->d_pcount, slots))) return st;
     if ((st = dalloc(&nl->d_pref, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_pcount, 0, sizeof(int) * slots));
@@ -970,8 +973,6 @@ int alloc_nl(spgnb_nl* nl)
     if ((st = dalloc(&nl->d_cl_q, nl->clusters_cap + 1))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_cl_q, 0, sizeof(int4) * (nl->clusters_cap + 1)));
     if ((st = dalloc(&nl->d_cl_c, nl->clusters_cap))) return st;
-    if ((st = dalloc(&nl->d_cl_words, nl->clusters_cap + 1))) return st;
-    if ((st = dalloc(&nl->d_cl_word_start, nl->clusters_cap + 1))) return st;
     if ((st = dalloc(&nl->d_tcount, nl->clusters_cap))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_tcount, 0, sizeof(int) * nl->clusters_cap));
     if ((st = dalloc(&nl->d_counters, kCntSize))) return st;
@@ -990,8 +991,9 @@ int alloc_nl(spgnb_nl* nl)
 }
 
 // Capacities from the densest system: neighbour clusters within
-// rc + skin + 6 A of an 8-atom cluster (the table, 1.3x margin), and listed
-// partners per atom within rc + skin (the lists, 1.5x margin).
+// rc + skin + 6 A of an 8-atom cluster (the table, 1.3x margin), and pruned
+// partners per atom within rc + buffer + 1 A (the lists, 1.3x margin, whole
+// 64-word windows plus one window for the padding).
 void estimate_capacities(spgnb_nl* nl)
 {
     double per_cluster = 0, per_atom = 0;
@@ -1001,13 +1003,15 @@ void estimate_capacities(spgnb_nl* nl)
         const double rho = sh.atom_count / vol;
         const double R = sh.cutoff + sh.skin + 6.0;
         per_cluster = std::max(per_cluster, std::min(4.18879 * R * R * R * rho, (double)sh.atom_count) / kClusterSize);
-        const double Rl = sh.cutoff + sh.skin;
+        const double buf = nl->opt.prune_buffer > 0.0f ? nl->opt.prune_buffer + 1.0 : sh.skin;
+        const double Rl = sh.cutoff + buf;
         per_atom = std::max(per_atom, std::min(4.18879 * Rl * Rl * Rl * rho, (double)sh.atom_count));
     }
     nl->table_cap = nl->opt.max_entries_per_cluster > 0 ? nl->opt.max_entries_per_cluster
                                                         : std::max((int)(per_cluster * 1.3) + 64, 128);
-    nl->words_per_atom = per_atom * 1.5 + 64;
+    nl->slot_cap = (((int)(per_atom * 1.3) + 63) & ~63) + 128;
 }
+
 
 }  // namespace
 
@@ -1069,6 +1073,8 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
     nl->rcell = nl->sys[0].rcell;
     nl->triclinic = nl->sys[0].triclinic;
     memcpy(nl->dims, nl->sys[0].dims, sizeof(nl->dims));
+    nl->prune_rc = 0.0f;
+    for (const auto& sh : nl->sys) nl->prune_rc = std::max(nl->prune_rc, sh.cutoff);
     estimate_capacities(nl);
     const int st = alloc_nl(nl);
     if (st)
@@ -1124,14 +1130,10 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     const int search_blocks = std::max(1, std::min((ccap + kSearchWarps - 1) / kSearchWarps, sms * 8));
     k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
         nl->d_sys, nl->table_cap, nl->d_run_start, nl->d_runs, nl->d_cell_cl_start, nl->d_cl_cell, nl->d_cl_sys,
-        nl->d_cl_u, nl->d_cl_q, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex, ex_start, ex_list, ex_num, nl->d_tcount,
-        nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_cl_words, nl->d_counters);
+        nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex, ex_start, ex_list, ex_num,
+        nl->d_tcount,
+        nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_search");
-    k_scan_words<<<1, 1024, 0, s>>>(ccap, nl->d_cl_words, nl->d_cl_word_start, nl->words_cap, nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_scan_words");
-    k_slot_starts<<<(ccap + 255) / 256, 256, 0, s>>>(ccap, nl->d_cl_word_start, nl->d_slot_count, nl->d_slot_start,
-                                                      nl->d_counters);
-    SPGNB_CHECK_LAUNCH("k_slot_starts");
     if (nl->opt.export_atom_groups)
     {
         k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
@@ -1146,6 +1148,21 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     nl->built = true;
     nl->local_atoms = n;
     nl->host_builds++;
+    return SPGNB_OK;
+}
+
+// Makes the pruned lists cover pairs within rc (a force module whose cutoff
+// exceeds the list's): the radius grows and a pruning is queued.
+int nl_set_prune_rc(spgnb_nl* nl, float rc, cudaStream_t s)
+{
+    if (!(rc > nl->prune_rc)) return SPGNB_OK;
+    nl->prune_rc = rc;
+    for (auto& d : nl->h_desc) d.prune_r2 = prune_r2_of(rc, nl->opt.prune_buffer);
+    SPGNB_CUDA(cudaMemcpyAsync(nl->d_sys, nl->h_desc.data(), sizeof(SysDesc) * nl->S, cudaMemcpyHostToDevice, s));
+    SPGNB_CUDA(cudaStreamSynchronize(s));
+    const int one = 1;
+    SPGNB_CUDA(cudaMemcpyAsync(nl->d_counters + kCntPrune, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    SPGNB_CUDA(cudaStreamSynchronize(s));
     return SPGNB_OK;
 }
 
@@ -1173,7 +1190,7 @@ int nl_regrow(spgnb_nl* nl, int flags)
     }
     if (flags & kOvfWords)
     {
-        nl->words_per_atom = nl->words_per_atom * 1.1 + 8;
+        nl->slot_cap = (((int)(nl->slot_cap * 1.3)) + 63) & ~63;
         if ((st = alloc_words(nl))) return st;
     }
     SPGNB_CUDA(cudaMemsetAsync(nl->d_counters + kCntOverflow, 0, sizeof(int), stream()));
@@ -1253,6 +1270,7 @@ int spgnb_nl_update(spgnb_nl* nl, const int* d_atom_local, int local_atom_number
         nl->cs2 = sh.cs2;
         nl->triclinic = sh.triclinic;
         nl->h_desc[0] = make_desc(sh, nl->opt.skin_permit);
+        nl->h_desc[0].prune_r2 = prune_r2_of(nl->prune_rc, nl->opt.prune_buffer);
         SPGNB_CUDA(cudaMemcpyAsync(nl->d_sys, nl->h_desc.data(), sizeof(SysDesc), cudaMemcpyHostToDevice, s));
         box_changed = true;
     }
@@ -1286,7 +1304,7 @@ int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out)
     out->work_items = h[kCntClusters];
     out->builds = h[kCntBuilds];
     out->overflow = h[kCntOverflow];
-    out->full_list_words = ((long long)h[kCntWords + 1] << 32) | (unsigned)h[kCntWords];
+    memcpy(&out->full_list_words, &h[kCntWords], sizeof(long long));
     out->prunes = h[kCntPrunes];
     memcpy(&out->pruned_list_words, &h[kCntPWordsLast], sizeof(long long));
     return SPGNB_OK;

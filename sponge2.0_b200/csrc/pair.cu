@@ -153,55 +153,44 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
     if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicExch(&counters[kCntPrune], 1);
 }
 
-// First word of a slot's pruned list: the full list's start rounded up to
-// an even word (8-byte aligned pairs of words) plus 64 spare words per slot
-// for the padding.
-__device__ __forceinline__ long long pruned_start(long long full_start, int s)
-{
-    return ((full_start + 1) & ~1LL) + 64LL * s;
-}
-
-// Pruning (no reference counterpart; results unchanged).  Run after every
+// Pruning (no reference counterpart; results unchanged).  Runs after every
 // rebuild and whenever some atom moved more than buffer/2 since the last run
-// (the pack kernel checks).  For each atom (one warp) it walks its cluster's
-// neighbour table, expands the atom's partners (mask row) of 32 elements at a
-// time into shared memory, keeps those whose distance is below
-// cutoff + buffer now, in table order, as 32-bit words {partner slot | LJ type
-// << 23 | per-pair image flag << 31}, pads the list to a multiple of 64 words
-// with the null slot, and records the slot offsets it saw.  Any pair within
-// the cutoff before the next pruning was within cutoff + buffer at this one,
-// so the copy misses none.  buffer <= 0 keeps every listed pair.  The last
-// block to finish clears the flag.
+// (the pack kernel checks).  For each atom (one warp) it walks its cluster's neighbour table,
+// expands the atom's partners (mask row) of 32 elements at a time into shared
+// memory, keeps those whose distance is below cutoff + buffer now, in table
+// order, as 32-bit words {partner slot | LJ type << 23 | per-pair image flag
+// << 31}, pads the
+// list to a multiple of 64 words with the null slot, and records the slot
+// offsets it saw.  Any pair within the cutoff before the next pruning was
+// within cutoff + buffer at this one, so the copy misses none.  buffer <= 0
+// keeps every listed pair.  The last block to finish clears the flag.
 constexpr int kPruneWarps = 8;
 
 __global__ void __launch_bounds__(kPruneWarps * 32)
-    k_prune(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, long long words_cap,
-            int clusters_cap, int table_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
+    k_prune(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, int clusters_cap,
+            int table_cap, int slot_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
             const int* __restrict__ tcount, const float4* __restrict__ tab, const uint2* __restrict__ tmask,
-            const long long* __restrict__ slot_start, const int* __restrict__ slot_count,
             const float4* __restrict__ pos, const int* __restrict__ ptype, float4* __restrict__ pref,
             int* __restrict__ pcount, unsigned* __restrict__ pwords)
 {
     if (counters[kCntPrune] == 0) return;
-    __shared__ float4 buf[kPruneWarps][kChunk * kClusterSize];
+    __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];  // {partner slot | image flag, element}
     __shared__ unsigned long long kept_total;
     const int lane = threadIdx.x & 31;
     const int a = threadIdx.x >> 5;
     const int nc = min(counters[kCntClusters], clusters_cap);
-    const bool lists_ok = word_total(counters) <= words_cap;
     const unsigned null_word = (unsigned)(clusters_cap * kClusterSize);
+    const int usable = slot_cap - 64;
     if (threadIdx.x == 0) kept_total = 0;
     __syncthreads();
-    float4* __restrict__ mybuf = buf[a];
+    uint2* __restrict__ mybuf = buf[a];
     for (int c = blockIdx.x; c < nc; c += gridDim.x)
     {
         const int s = c * kClusterSize + a;
         const float4 pi = pos[s];
         if (lane == 0) pref[s] = pi;
-        const int n = lists_ok ? slot_count[s] : 0;
         int kept = 0;
-        unsigned* __restrict__ out_words = pwords + pruned_start(slot_start[s], s);
-        if (n > 0)
+        unsigned* __restrict__ out_words = pwords + (size_t)s * slot_cap;
         {
             const ForceParams P = fps ? fps[cl_sys[c]] : p0;
             const float rp = sqrtf(P.rc2) + buffer + 1e-3f;
@@ -229,31 +218,32 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
                 }
                 const int total = __shfl_sync(0xffffffffu, incl, 31);
                 const int eb = __float_as_int(e.w);
-                const int flag = (eb & (1 << 30)) ? (int)0x80000000 : 0;
+                const unsigned flag = (eb & (1 << 30)) ? 0x80000000u : 0u;
+                const unsigned base = (unsigned)(eb & 0x3fffffff) | flag;
                 int k = incl - cnt;
-                while (row)
-                {
-                    const int b = __ffs(row) - 1;
-                    row &= row - 1;
-                    mybuf[k++] = make_float4(e.x, e.y, e.z, __int_as_float(((eb & 0x3fffffff) + b) | flag));
-                }
+#pragma unroll
+                for (int b = 0; b < kClusterSize; b++)
+                    if ((row >> b) & 1u) mybuf[k++] = make_uint2(base + b, (unsigned)lane);
                 __syncwarp();
                 for (int q0 = 0; q0 < total; q0 += 32)
                 {
                     const int q = q0 + lane;
+                    const uint2 w = mybuf[q < total ? q : 0];
+                    // the element's centre difference from the lane that read it
+                    const float ex = __shfl_sync(0xffffffffu, e.x, (int)w.y);
+                    const float ey = __shfl_sync(0xffffffffu, e.y, (int)w.y);
+                    const float ez = __shfl_sync(0xffffffffu, e.z, (int)w.y);
                     bool keep = false;
                     unsigned out = 0;
                     if (q < total)
                     {
-                        const float4 w = mybuf[q];
-                        const int wi = __float_as_int(w.w);
-                        const int js = wi & 0x7fffffff;
+                        const int js = (int)(w.x & 0x7fffffffu);
                         const float4 pj = pos[js];
                         const int tj = ptype[js];
-                        float dx = (w.x - pi.x) + pj.x;
-                        float dy = (w.y - pi.y) + pj.y;
-                        float dz = (w.z - pi.z) + pj.z;
-                        if (wi < 0)
+                        float dx = (ex - pi.x) + pj.x;
+                        float dy = (ey - pi.y) + pj.y;
+                        float dz = (ez - pi.z) + pj.z;
+                        if (w.x & 0x80000000u)
                         {
                             const SysDesc& D = sys[cl_sys[c]];
                             const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
@@ -264,16 +254,24 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
                             dz -= sz * D.cell.a33;
                         }
                         keep = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx)) < rp2;
-                        out = (unsigned)js | ((unsigned)tj << 23) | (wi < 0 ? 0x80000000u : 0u);
+                        out = (unsigned)js | ((unsigned)tj << 23) | (w.x & 0x80000000u);
                     }
                     const unsigned m = __ballot_sync(0xffffffffu, keep);
-                    if (keep) out_words[kept + __popc(m & ((1u << lane) - 1u))] = out;
+                    if (keep)
+                    {
+                        const int k = kept + __popc(m & ((1u << lane) - 1u));
+                        if (k < usable)
+                            out_words[k] = out;
+                        else
+                            atomicOr(&counters[kCntOverflow], kOvfWords);
+                    }
                     kept += __popc(m);
                 }
                 __syncwarp();
             }
         }
         // pad to a multiple of 64 words with the null partner
+        kept = min(kept, usable);
         const int padded = (kept + 63) & ~63;
         for (int k = kept + lane; k < padded; k += 32) out_words[k] = null_word;
         if (lane == 0)
@@ -402,9 +400,8 @@ __device__ __forceinline__ float centre_step(int qj, int qi)
 template <int MODE, int FIT, bool TRI>
 __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ? 3 : 2))
     k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
-                const int* __restrict__ counters, long long words_cap, int clusters_cap,
-                const int* __restrict__ cl_sys, const long long* __restrict__ slot_start,
-                const int* __restrict__ pcount, const unsigned* __restrict__ pwords,
+                const int* __restrict__ counters, int clusters_cap, int slot_cap,
+                const int* __restrict__ cl_sys, const int* __restrict__ pcount, const unsigned* __restrict__ pwords,
                 const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0, const int4* __restrict__ cl_q,
                 const float4* __restrict__ pos, const int* __restrict__ ptype,
                 const float2* __restrict__ gtable, int table_size, float3* __restrict__ frc,
@@ -424,9 +421,8 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
     const int lane = threadIdx.x & 31;
     const int a = threadIdx.x >> 5;
     const int nc = min(counters[kCntClusters], clusters_cap);
-    const bool lists_ok = word_total(counters) <= words_cap;
 
-    for (int c = blockIdx.x; lists_ok && c < nc; c += gridDim.x)
+    for (int c = blockIdx.x; c < nc; c += gridDim.x)
     {
         const int s = c * kClusterSize + a;
         const int n = pcount[s];  // a multiple of 64
@@ -440,7 +436,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
         int gi = 0;
         if (PA) gi = __float_as_int(slot_x0[s].w);
         const int ti = ptype[s] * P.n_types + P.table_begin;
-        const uint2* __restrict__ wl = reinterpret_cast<const uint2*>(pwords + pruned_start(slot_start[s], s));
+        const uint2* __restrict__ wl = reinterpret_cast<const uint2*>(pwords + (size_t)s * slot_cap);
         const float2 npx = f2(-pi.x), npy = f2(-pi.y), npz = f2(-pi.z), qi2 = f2(pi.w);
         float2 fx = f2(0.0f), fy = f2(0.0f), fz = f2(0.0f);
         float2 acc[8], own[8];
@@ -976,8 +972,8 @@ int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
     const spgnb_nl* nl = x.nl;
     const int grid = std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T>, kForceWarps * 32, smem), nl->clusters_cap));
     k_pair_fast<M, F, T><<<grid, kForceWarps * 32, smem, s>>>(
-        x.p0, x.fps, nl->d_sys, nl->d_counters, nl->words_cap, nl->clusters_cap, nl->d_cl_sys, nl->d_slot_start,
-        nl->d_pcount, nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table,
+        x.p0, x.fps, nl->d_sys, nl->d_counters, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount,
+        nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table,
         x.table_size, x.frc, x.totals, x.om, x.pa);
     SPGNB_CHECK_LAUNCH("k_pair_fast");
     return SPGNB_OK;
@@ -1136,6 +1132,7 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
         if (d_atom_direct_pme_energy)
             SPGNB_CUDA(cudaMemsetAsync(d_atom_direct_pme_energy, 0, sizeof(float) * lj->atom_numbers, s));
     }
+    if ((st = nl_set_prune_rc(const_cast<spgnb_nl*>(nl), lj->cutoff, s))) return st;
     const bool track = nl->opt.prune_buffer > 0.0f;
     const float half = 0.5f * nl->opt.prune_buffer;
     k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_cl_sys,
@@ -1145,10 +1142,10 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     SPGNB_CHECK_LAUNCH("k_pack_slots");
     const ForceParams fp = make_pair_const(lj, pme_beta);
     const int grid = std::max(1, std::min(num_sms() * 4, nl->clusters_cap));
-    k_prune<<<grid, kPruneWarps * 32, 0, s>>>(fp, nullptr, nl->opt.prune_buffer, nl->d_counters, nl->words_cap,
-                                              nl->clusters_cap, nl->table_cap, nl->d_cl_sys, nl->d_sys, nl->d_tcount,
-                                              nl->d_tab, nl->d_tmask, nl->d_slot_start, nl->d_slot_count,
-                                              lj->d_sdata, lj->d_slot_type, nl->d_pref, nl->d_pcount, nl->d_pwords);
+    k_prune<<<grid, kPruneWarps * 32, 0, s>>>(fp, nullptr, nl->opt.prune_buffer, nl->d_counters, nl->clusters_cap,
+                                              nl->table_cap, nl->slot_cap, nl->d_cl_sys, nl->d_sys, nl->d_tcount,
+                                              nl->d_tab, nl->d_tmask, lj->d_sdata, lj->d_slot_type, nl->d_pref,
+                                              nl->d_pcount, nl->d_pwords);
     SPGNB_CHECK_LAUNCH("k_prune");
     OwnerMap om{nullptr, local_atom_numbers, 3};
     PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
