@@ -298,6 +298,74 @@ int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_number
                                       spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, const spgnb_atom_group* d_nl,
                                       float cutoff, float pme_beta);
 
+/* ----------------------------------------------------------------- BATCH */
+/* Many independent periodic systems stepped together (no reference
+ * counterpart: the reference runs one system per process).  Every system
+ * keeps its own box, cutoff, skin, Ewald beta, exclusions and rigid waters;
+ * they share one LJ type table.  One step = leap-frog velocity Verlet (kick
+ * with F(t), drift, SETTLE for the rigid waters) + the neighbour-list
+ * update (per system, by the skin trigger of NEIGHBOR_LIST::Update) + LJ and
+ * PME direct-space forces over all systems in one kernel launch.  Steps are
+ * replayed from captured CUDA graphs.  A system's results do not depend on the
+ * other systems in the batch. */
+typedef struct spgnb_batch spgnb_batch;
+
+typedef struct
+{
+    int atom_numbers;
+    float cutoff;                  /* LJ/PME direct-space cutoff (A) */
+    float skin;                    /* neighbour-list skin (A) */
+    float pme_beta;                /* Ewald beta (1/A) */
+    spgnb_ltmatrix3 cell, rcell;   /* orthorhombic or triclinic box */
+    const float* h_crd;            /* 3N, A */
+    const float* h_vel;            /* 3N, A/ps, or NULL for zero */
+    const float* h_charge;         /* N, scaled by the reference's charge factor */
+    const float* h_mass;           /* N, g/mol (0 = fixed atom) */
+    const int* h_atom_type;        /* N, index into the batch's type table */
+    const int* h_excluded_start;   /* N, this system's exclusion CSR (local indices, j > i) */
+    const int* h_excluded_numbers; /* N */
+    const int* h_excluded_list;    /* excluded_total entries */
+    int excluded_total;
+    int water_begin;               /* rigid 3-site waters O,H,H from this local atom */
+    int water_numbers;             /* how many */
+} spgnb_batch_system;
+
+typedef struct
+{
+    float dt;                      /* ps, 0.002 by default */
+    float water_doh, water_dhh;    /* rigid water geometry (A): 0.9572, 1.5139 */
+    float skin_permit;             /* rebuild at skin * skin_permit displacement, 0.5 */
+    float prune_buffer;            /* as spgnb_nl_options.prune_buffer, 1.0 */
+    int steps_per_graph;           /* steps per captured graph, 10 */
+    int use_graphs;                /* 1 = replay captured graphs, 0 = launch each step */
+} spgnb_batch_options;
+
+void spgnb_batch_default_options(spgnb_batch_options* opt);
+
+/* Copies the systems to the device and builds their lists.  The type table
+ * (atom_type_numbers types) is shared: pair_A / pair_B in the reference's
+ * triangular layout (already x12 / x6). */
+int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int atom_type_numbers,
+                       const float* h_pair_A, const float* h_pair_B, const spgnb_batch_options* opt,
+                       spgnb_batch** out);
+/* Advances every system by `steps` steps; when energy_interval > 0, energies
+ * and virials are evaluated on steps whose count is a multiple of it (the
+ * last ones are kept).  Returns without synchronising. */
+int spgnb_batch_run(spgnb_batch* b, int steps, int energy_interval);
+/* Per system, 9 doubles: LJ short-range, LJ long-range correction, PME
+ * direct-space Coulomb (kcal/mol), virial a11 a21 a22 a31 a32 a33 of the
+ * last energy evaluation.  Synchronises. */
+int spgnb_batch_energies(spgnb_batch* b, double* out);
+/* Coordinates, velocities and forces of system `sys` (3N floats each, NULL
+ * to skip).  Synchronises. */
+int spgnb_batch_download(spgnb_batch* b, int sys, float* h_crd, float* h_vel, float* h_frc);
+/* Steps done, list rebuilds (all systems), prunings, overflow flags. */
+int spgnb_batch_stats(spgnb_batch* b, long long* steps, long long* rebuilds, long long* prunings, int* overflow);
+/* Picks the prune buffer with the fastest step for this batch by timing a
+ * few steps of each candidate (the systems advance meanwhile). */
+int spgnb_batch_autotune(spgnb_batch* b, int steps_per_candidate, float* chosen_buffer);
+int spgnb_batch_destroy(spgnb_batch* b);
+
 /* ------------------------------------------------------------ diagnostics */
 /* Kernel launches issued by the library so far (all threads). */
 unsigned long long spgnb_launch_count(void);

@@ -27,12 +27,14 @@ int num_sms();
     } while (0)
 
 void count_launch();
+bool sync_check();
 
 #define SPGNB_CHECK_LAUNCH(name)                                        \
     do                                                                  \
     {                                                                   \
         ::spgnb::count_launch();                                        \
         cudaError_t e__ = cudaGetLastError();                           \
+        if (e__ == cudaSuccess && ::spgnb::sync_check()) e__ = cudaDeviceSynchronize(); \
         if (e__ != cudaSuccess) return ::spgnb::cuda_fail(e__, name);   \
     } while (0)
 
@@ -74,16 +76,16 @@ constexpr float kPadCoordinate = 1.0e4f;
 // device counters (int slots of NL::d_counters)
 enum Counter
 {
-    kCntClusters = 0,
+    kCntClusters = 0,   // (unused)
     kCntItems = 1,
     kCntEntries = 2,    // 64-bit: neighbour-table elements of the last build (slots 2,3)
     kCntOverflow = 4,   // bit flags
-    kCntNeed = 5,       // rebuild requested for the current update
+    kCntNeed = 5,       // some system rebuilds in the current update
     kCntBuilds = 6,
     kCntMaxCell = 7,
     kCntWords = 8,      // 64-bit: listed partners summed over atoms, last build (slots 8,9)
     kCntNbr = 10,       // (unused)
-    kCntPrune = 11,     // pruned lists must be rebuilt before the next force
+    kCntPrune = 11,     // some system's pruned lists must be redone before the next force
     kCntPruneDone = 12, // blocks of the running prune kernel that finished
     kCntPrunes = 13,    // prunings performed
     kCntPWords = 14,    // 64-bit: words of the running pruning (slots 14,15)
@@ -126,6 +128,7 @@ struct SysDesc
     float gl, cs2, list_radius;
     float frac_norm[3];
     int Nx, Ny, Nz, cell_begin;
+    int cl_begin, cl_cap;   // the system's fixed range of clusters
     int atom_begin, atom_count, triclinic;
     int all_safe;   // every cluster pair the search can meet is inside half a box: one image per pair
     float prune_r2; // squared radius of the pruned lists, (cutoff + buffer)^2; huge when pruning is off
@@ -153,6 +156,7 @@ struct SysHost
     float cutoff = 0, skin = 0, gl = 0, cs2 = 0;
     int dims[3] = {0, 0, 0};
     int cell_begin = 0;
+    int cl_begin = 0, cl_cap = 0;
     bool triclinic = false;
 };
 
@@ -186,7 +190,11 @@ struct spgnb_nl
     int2* d_runs = nullptr;       // {first cell | stencil flags << 28, last cell + 1}
     int* d_cell_count = nullptr;  // G
     int* d_cell_cursor = nullptr; // G
-    int* d_cell_cl_start = nullptr;  // G+1 (cluster index)
+    int2* d_cell_cl = nullptr;    // G: the cell's clusters [x, y)
+    // per system: rebuild and prune requests, clusters of the last build
+    int* d_need = nullptr;
+    int* d_prune = nullptr;
+    int* d_ncl = nullptr;
     // per atom
     int* d_atom_cell = nullptr;
     int* d_atom_shift = nullptr;  // packed lattice shift used by the wrap
@@ -259,6 +267,101 @@ struct spgnb_solvent
 
 namespace spgnb
 {
+// Exclusive scan of value(0..n-1), handed to store(c, prefix), by one block (a multiple
+// of 32 threads, each taking a contiguous chunk); the total is returned to
+// every thread.
+template <typename T, typename F, typename S>
+__device__ __forceinline__ T block_scan_to(int n, F value, S store)
+{
+    __shared__ T warp_sums[32];
+    const int threads = blockDim.x;
+    const int per = (n + threads - 1) / threads;
+    const int lo = min(n, threadIdx.x * per);
+    const int hi = min(n, lo + per);
+    T sum = 0;
+    for (int c = lo; c < hi; c++) sum += value(c);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T v = sum;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        const T t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) warp_sums[warp] = v;
+    __syncthreads();
+    const int nw = threads >> 5;
+    if (warp == 0)
+    {
+        T w = lane < nw ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1)
+        {
+            const T t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < nw) warp_sums[lane] = w;
+    }
+    __syncthreads();
+    T excl = v - sum + (warp > 0 ? warp_sums[warp - 1] : 0);
+    for (int c = lo; c < hi; c++)
+    {
+        store(c, excl);
+        excl += value(c);
+    }
+    const T total = warp_sums[nw - 1];
+    __syncthreads();
+    return total;
+}
+
+template <typename T, typename F>
+__device__ __forceinline__ T block_scan(int n, F value, T* out)
+{
+    return block_scan_to<T>(n, value, [&](int c, T v) { out[c] = v; });
+}
+
+
+struct OwnerMap
+{
+    const int* atom_local;   // global index of each local atom
+    int solvent_start;       // first local atom of the water tail (n when none)
+    int water_points;
+    __device__ __forceinline__ int remap(int a) const
+    {
+        return a >= solvent_start ? solvent_start + ((a - solvent_start) / water_points) * water_points : a;
+    }
+};
+
+struct PerAtomOut
+{
+    float* energy;       // caller's atom_energy (+=)
+    float* lj_energy;    // module's per-atom LJ energy
+    float* direct;       // atom_direct_pme_energy
+    float* virial;       // caller's LTMatrix3 array (+=), 6 floats per atom
+};
+
+// One force evaluation over an spgnb list: slot pack (with the per-system
+// prune trigger), pruning when due, and the pruned-list force kernel.
+struct ForceInputs
+{
+    spgnb_nl* nl = nullptr;
+    const float3* crd = nullptr;       // per atom, the list's atom order
+    const float* charge = nullptr;
+    const int* atom_type = nullptr;    // into the LJ table
+    float4* slot_pos = nullptr;        // scratch, slots + 1
+    int* slot_type = nullptr;          // scratch, slots + 1
+    ForceParams p0{};                  // the one system's parameters (d_fps null)
+    const ForceParams* d_fps = nullptr;  // per system (several systems)
+    bool fit = true;                   // every system inside the rational fits' range
+    const float2* table = nullptr;     // T x T {A, B}
+    int table_size = 0;
+    float3* frc = nullptr;             // += forces
+    long long* totals = nullptr;       // 8 fixed-point sums per system (mode >= 1)
+    int mode = 0;                      // 0 forces, 1 + totals, 2 + per-atom outputs
+    OwnerMap om{nullptr, 0, 3};
+    PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
+};
+int force_pipeline(const ForceInputs& in, cudaStream_t s);
+int force_kernels_init(int table_size);
+
 // Neighbour-list internals shared with the force and batch code.
 int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,
                     const spgnb_ltmatrix3* rcells, const float* cutoffs, const float* skins,

@@ -20,7 +20,8 @@ __global__ void k_count_pairs(const int* __restrict__ counters, int clusters_cap
                               unsigned long long* out)
 {
     const int lane = threadIdx.x & 31;
-    const int nc = min(counters[kCntClusters], clusters_cap);
+    const int nc = clusters_cap;
+    (void)counters;
     const int warps = gridDim.x * (blockDim.x >> 5);
     unsigned long long listed = 0, inside = 0;
     auto pos = [&](int s) {

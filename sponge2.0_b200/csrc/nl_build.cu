@@ -65,45 +65,47 @@ __device__ __forceinline__ float ref_pair_dr2(float3 a, float3 b, const Cell& c,
 
 // ---------------------------------------------------------------- kernels
 
-// Check_Refresh (neighbor_list.cpp:166-180): any atom moved more than
-// skin*skin_permit since the last build.
+// Check_Refresh (neighbor_list.cpp:166-180), per system: a system rebuilds
+// when one of its atoms moved more than skin*skin_permit since its last build.
 __global__ void k_check_refresh(int n_slots, const int* __restrict__ slot_atom, const int* __restrict__ cl_sys,
                                 const SysDesc* __restrict__ sys, const float3* __restrict__ crd,
-                                const float4* __restrict__ x0, int* counters)
+                                const float4* __restrict__ x0, int* __restrict__ need, int* counters)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    const int total = counters[kCntClusters] * kClusterSize;
     bool move = false;
-    if (s < n_slots && s < total)
+    if (s < n_slots)
     {
         const int a = slot_atom[s];
         if (a >= 0)
         {
-            const SysDesc& D = sys[cl_sys[s >> 3]];
+            const int sy = cl_sys[s >> 3];
+            const SysDesc& D = sys[sy];
             const float3 c = crd[a];
             const float4 o = x0[s];
             float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
             const float sx = floorf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31 + 0.5f);
-            const float sy = floorf(dy * D.rcell.a22 + dz * D.rcell.a32 + 0.5f);
+            const float sy2 = floorf(dy * D.rcell.a22 + dz * D.rcell.a32 + 0.5f);
             const float sz = floorf(dz * D.rcell.a33 + 0.5f);
-            dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
-            dy -= sy * D.cell.a22 + sz * D.cell.a32;
+            dx -= sx * D.cell.a11 + sy2 * D.cell.a21 + sz * D.cell.a31;
+            dy -= sy2 * D.cell.a22 + sz * D.cell.a32;
             dz -= sz * D.cell.a33;
             move = dx * dx + dy * dy + dz * dz > D.permit2;
+            if (move) need[sy] = 1;
         }
     }
-    if (__any_sync(0xffffffffu, move) && (threadIdx.x & 31) == 0) atomicExch(&counters[kCntNeed], 1);
+    if (__any_sync(0xffffffffu, move) && (threadIdx.x & 31) == 0) counters[kCntNeed] = 1;
 }
 
 // Put_Atom_In_Grids (neighbor_list.cpp:206-275): brick wrap, cell index
 // nx*Ny*Nz + ny*Nz + nz with clamping, per-cell count.
 __global__ void k_bin(int n, const float3* __restrict__ crd, const int* __restrict__ atom_sys,
                       const SysDesc* __restrict__ sys, int* __restrict__ atom_cell, int* __restrict__ atom_shift,
-                      float4* __restrict__ wrapped, int* __restrict__ cell_count, const int* __restrict__ counters)
+                      float4* __restrict__ wrapped, int* __restrict__ cell_count, const int* __restrict__ need,
+                      const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || !need[atom_sys[i]]) return;
     const SysDesc& g = sys[atom_sys[i]];
     const float3 c = crd[i];
     float x = c.x, y = c.y, z = c.z;
@@ -128,91 +130,56 @@ __global__ void k_bin(int n, const float3* __restrict__ crd, const int* __restri
     atomicAdd(&cell_count[cid], 1);
 }
 
-// Exclusive scan of value(0..n-1) into out[0..n-1] by one block (a multiple
-// of 32 threads, each taking a contiguous chunk); the total is returned to
-// every thread.
-template <typename T, typename F>
-__device__ T block_scan(int n, F value, T* out)
+// Cluster counts per cell (ceil(count/8)), their exclusive scan from the
+// system's first cluster, overflow checks of the cells; one block per system.
+__global__ void k_scan_cells(const SysDesc* __restrict__ sys, const int* __restrict__ cell_count,
+                             int2* __restrict__ cell_cl, int max_atom_in_grid, const int* __restrict__ need,
+                             int* __restrict__ ncl, int* counters)
 {
-    __shared__ T warp_sums[32];
-    const int threads = blockDim.x;
-    const int per = (n + threads - 1) / threads;
-    const int lo = min(n, threadIdx.x * per);
-    const int hi = min(n, lo + per);
-    T sum = 0;
-    for (int c = lo; c < hi; c++) sum += value(c);
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    T v = sum;
-    for (int o = 1; o < 32; o <<= 1)
-    {
-        const T t = __shfl_up_sync(0xffffffffu, v, o);
-        if (lane >= o) v += t;
-    }
-    if (lane == 31) warp_sums[warp] = v;
-    __syncthreads();
-    const int nw = threads >> 5;
-    if (warp == 0)
-    {
-        T w = lane < nw ? warp_sums[lane] : 0;
-        for (int o = 1; o < 32; o <<= 1)
-        {
-            const T t = __shfl_up_sync(0xffffffffu, w, o);
-            if (lane >= o) w += t;
-        }
-        if (lane < nw) warp_sums[lane] = w;
-    }
-    __syncthreads();
-    T excl = v - sum + (warp > 0 ? warp_sums[warp - 1] : 0);
-    for (int c = lo; c < hi; c++)
-    {
-        out[c] = excl;
-        excl += value(c);
-    }
-    const T total = warp_sums[nw - 1];
-    __syncthreads();
-    return total;
-}
-
-// Cluster counts per cell (ceil(count/8)), their exclusive scan, overflow
-// checks of the cells; one block.
-__global__ void k_scan_cells(int G, const int* __restrict__ cell_count, int* __restrict__ cell_cl_start,
-                             int max_atom_in_grid, int clusters_cap, int* counters)
-{
-    if (counters[kCntNeed] == 0) return;
+    const int sy = blockIdx.x;
+    if (counters[kCntNeed] == 0 || !need[sy]) return;
+    const SysDesc& g = sys[sy];
+    const int G = g.Nx * g.Ny * g.Nz;
+    const int* cc = cell_count + g.cell_begin;
     __shared__ int max_cell;
     if (threadIdx.x == 0) max_cell = 0;
     __syncthreads();
     int local_max = 0;
-    for (int c = threadIdx.x; c < G; c += blockDim.x) local_max = max(local_max, cell_count[c]);
+    for (int c = threadIdx.x; c < G; c += blockDim.x) local_max = max(local_max, cc[c]);
     atomicMax(&max_cell, local_max);
-    const int total = block_scan<int>(
-        G, [&](int c) { return (min(cell_count[c], kMaxCellAtoms) + kClusterSize - 1) / kClusterSize; },
-        cell_cl_start);
+    int2* out = cell_cl + g.cell_begin;
+    const int base = g.cl_begin;
+    auto clusters = [&](int c) { return (min(cc[c], kMaxCellAtoms) + kClusterSize - 1) / kClusterSize; };
+    const int total = block_scan_to<int>(G, clusters, [&](int c, int excl) {
+        out[c] = make_int2(base + excl, base + excl + clusters(c));
+    });
     if (threadIdx.x == 0)
     {
-        cell_cl_start[G] = total;
-        // (cannot exceed the capacity n/8 + cells; if it did, build nothing)
-        counters[kCntClusters] = total <= clusters_cap ? total : 0;
-        counters[kCntMaxCell] = max_cell;
+        // (cannot exceed the system's capacity atoms/8 + cells; if it did, build nothing)
+        ncl[sy] = total <= g.cl_cap ? total : 0;
+        atomicMax(&counters[kCntMaxCell], max_cell);
         int flags = 0;
         if (max_cell > max_atom_in_grid) flags |= kOvfGrid;
-        if (total > clusters_cap) flags |= kOvfPairs;
+        if (total > g.cl_cap) flags |= kOvfPairs;
         if (max_cell > kMaxCellAtoms) flags |= kOvfCellHard;
         if (flags) atomicOr(&counters[kCntOverflow], flags);
     }
 }
 
-__global__ void k_scatter(int n, const int* __restrict__ atom_cell, const int* __restrict__ cell_cl_start,
-                          int* __restrict__ cell_cursor, int* __restrict__ tmp_atoms, int slots_cap,
-                          const int* __restrict__ counters)
+__global__ void k_scatter(int n, const int* __restrict__ atom_sys, const int* __restrict__ atom_cell,
+                          const int2* __restrict__ cell_cl, const int* __restrict__ ncl,
+                          const SysDesc* __restrict__ sys, int* __restrict__ cell_cursor, int* __restrict__ tmp_atoms,
+                          const int* __restrict__ need, const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const int sy = atom_sys[i];
+    if (!need[sy] || ncl[sy] == 0) return;
     const int c = atom_cell[i];
     const int pos = atomicAdd(&cell_cursor[c], 1);
-    const int s = cell_cl_start[c] * kClusterSize + pos;
-    if (pos < kMaxCellAtoms && s < slots_cap) tmp_atoms[s] = i;
+    const int2 r = cell_cl[c];
+    if (pos < kMaxCellAtoms && r.y <= sys[sy].cl_begin + ncl[sy]) tmp_atoms[r.x * kClusterSize + pos] = i;
 }
 
 __device__ __forceinline__ unsigned spread3(unsigned v)
@@ -224,22 +191,23 @@ __device__ __forceinline__ unsigned spread3(unsigned v)
 // Deterministic in-cell order: by a 4x4x4 Morton sub-cell key, then by atom
 // index, so clusters are spatially compact and the build reproducible.
 __global__ void k_sort_cells(int G, const int* __restrict__ cell_sys, const SysDesc* __restrict__ sys,
-                             const int* __restrict__ cell_count, const int* __restrict__ cell_cl_start,
-                             const int* __restrict__ tmp_atoms, const float4* __restrict__ wrapped,
-                             int* __restrict__ slot_atom, int* __restrict__ cl_cell, int* __restrict__ cl_sys,
-                             int* __restrict__ atom_slot, int slots_cap, const int* __restrict__ counters)
+                             const int* __restrict__ cell_count, const int2* __restrict__ cell_cl,
+                             const int* __restrict__ ncl, const int* __restrict__ tmp_atoms,
+                             const float4* __restrict__ wrapped, int* __restrict__ slot_atom, int* __restrict__ cl_cell,
+                             int* __restrict__ atom_slot, const int* __restrict__ need, const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
     extern __shared__ unsigned long long keys[];
     for (int c = blockIdx.x; c < G; c += gridDim.x)
     {
         const int sy = cell_sys[c];
+        if (!need[sy]) continue;
         const SysDesc& g = sys[sy];
         const int n = min(cell_count[c], kMaxCellAtoms);
-        const int cl0 = cell_cl_start[c], cl1 = cell_cl_start[c + 1];
-        const int base = cl0 * kClusterSize;
-        const int nslots = (cl1 - cl0) * kClusterSize;
-        if (base + nslots > slots_cap) continue;
+        const int2 r = cell_cl[c];
+        if (ncl[sy] == 0 || r.y > g.cl_begin + ncl[sy]) continue;
+        const int base = r.x * kClusterSize;
+        const int nslots = (r.y - r.x) * kClusterSize;
         const int local = c - g.cell_begin;
         const int nz = local % g.Nz, ny = (local / g.Nz) % g.Ny, nx = local / (g.Ny * g.Nz);
         const float inv = 4.0f / g.gl;
@@ -259,22 +227,18 @@ __global__ void k_sort_cells(int G, const int* __restrict__ cell_sys, const SysD
             if (e < n)
             {
                 const unsigned long long k = keys[e];
-                int r = 0;
-                for (int f = 0; f < n; f++) r += keys[f] < k;
+                int rank = 0;
+                for (int f = 0; f < n; f++) rank += keys[f] < k;
                 const int a = (int)(k & 0xffffffffu);
-                slot_atom[base + r] = a;
-                atom_slot[a] = base + r;
+                slot_atom[base + rank] = a;
+                atom_slot[a] = base + rank;
             }
             else
             {
                 slot_atom[base + e] = -1;
             }
         }
-        for (int k = cl0 + threadIdx.x; k < cl1; k += blockDim.x)
-        {
-            cl_cell[k] = c;
-            cl_sys[k] = sy;
-        }
+        for (int k = r.x + threadIdx.x; k < r.y; k += blockDim.x) cl_cell[k] = c;
         __syncthreads();
     }
 }
@@ -283,24 +247,37 @@ __global__ void k_sort_cells(int G, const int* __restrict__ cell_sys, const SysD
 // radius, fractional fixed-point centre, per-slot offsets and build
 // coordinates (w = the atom's global index, -1 for padding).  Eight lanes per
 // cluster.
-__global__ void k_cluster_props(const float3* __restrict__ crd, const int* __restrict__ slot_atom,
+__global__ void k_cluster_props(const float3* __restrict__ crd, int* __restrict__ slot_atom,
                                 const int* __restrict__ atom_shift, const int* __restrict__ atom_local,
                                 const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys, int* counters,
                                 uint4* __restrict__ cl_u, int4* __restrict__ cl_q, float4* __restrict__ cl_c,
                                 float4* __restrict__ slot_x0, float4* __restrict__ slot_d0,
                                 int2* __restrict__ slot_ex, const int* __restrict__ ex_start,
-                                const int* __restrict__ ex_list, const int* __restrict__ ex_num, int clusters_cap)
+                                const int* __restrict__ ex_list, const int* __restrict__ ex_num, int clusters_cap,
+                                const int* __restrict__ need, const int* __restrict__ ncl, int* __restrict__ tcount,
+                                int* __restrict__ slot_count, int* __restrict__ pcount)
 {
     if (counters[kCntNeed] == 0) return;
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int k = t >> 3;
     const int l8 = t & 7;
-    const int nc = counters[kCntClusters];
-    const bool live = k < nc && k < clusters_cap;
+    const int sy = k < clusters_cap ? cl_sys[k] : 0;
+    // every lane takes part in the shuffles below; only clusters of systems
+    // being rebuilt write anything
+    const bool active = k < clusters_cap && need[sy];
+    const bool live = active && k - sys[sy].cl_begin < ncl[sy];
     const int s = k * kClusterSize + l8;
+    if (active && !live)
+    {
+        // a cluster of the system's range that this build does not use
+        slot_atom[s] = -1;
+        slot_count[s] = 0;
+        pcount[s] = 0;
+        if (l8 == 0) tcount[k] = 0;
+    }
     const int a = live ? slot_atom[s] : -1;
     Cell cell{1, 0, 1, 0, 0, 1};
-    if (live) cell = sys[cl_sys[k]].cell;
+    if (live) cell = sys[sy].cell;
     double w[3] = {0, 0, 0};
     float3 x = make_float3(0, 0, 0);
     if (a >= 0)
@@ -361,7 +338,7 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, const int* __res
         const int k = ex_num[g];
         slot_ex[s] = k > 0 ? make_int2(ex_list[ex_start[g]], ex_list[ex_start[g] + k - 1]) : make_int2(0x7fffffff, -1);
     }
-    else if (live)
+    else if (active)
     {
         const float p = kPadCoordinate + (float)s;
         slot_d0[s] = make_float4(p, p, p, 0.0f);
@@ -424,8 +401,9 @@ __device__ bool excluded_scan(int glo, int ghi, const int* __restrict__ ex_start
 }
 
 __global__ void __launch_bounds__(kSearchWarps * 32, 5)
-    k_search(const SysDesc* __restrict__ sys, int table_cap, const int* __restrict__ run_start,
-             const int2* __restrict__ runs, const int* __restrict__ cell_cl_start, const int* __restrict__ cl_cell,
+    k_search(const SysDesc* __restrict__ sys, int clusters_cap, int table_cap, const int* __restrict__ need,
+             const int* __restrict__ ncl, const int* __restrict__ run_start, const int2* __restrict__ runs,
+             const int2* __restrict__ cell_cl, const int* __restrict__ cl_cell,
              const int* __restrict__ cl_sys, const uint4* __restrict__ cl_u, const int4* __restrict__ cl_q,
              const float4* __restrict__ cl_c, const float4* __restrict__ slot_x0, const float4* __restrict__ slot_d0,
              const int2* __restrict__ slot_ex,
@@ -438,13 +416,14 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
     __shared__ uint2 stage_m[kSearchWarps][kChunk];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int nc = counters[kCntClusters];
     const int total_warps = gridDim.x * kSearchWarps;
     unsigned long long elements = 0, listed = 0;
 
-    for (int c = blockIdx.x * kSearchWarps + wib; c < nc; c += total_warps)
+    for (int c = blockIdx.x * kSearchWarps + wib; c < clusters_cap; c += total_warps)
     {
-        const SysDesc& p = sys[cl_sys[c]];
+        const int sy = cl_sys[c];
+        if (!need[sy] || c - sys[sy].cl_begin >= ncl[sy]) continue;
+        const SysDesc& p = sys[sy];
         const int cellA = cl_cell[c];
         const uint4 ui = cl_u[c];
         const int4 qc = cl_q[c];
@@ -486,8 +465,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
             const int2 run = runs[r];
             const bool fwd = (run.x >> 28) & 1;  // the run's cells are in stencil(cellA)
             const bool rev = (run.x >> 29) & 1;  // cellA is in their stencils
-            int b0 = cell_cl_start[run.x & 0x0fffffff];
-            const int b1 = min(cell_cl_start[run.y], nc);
+            int b0 = cell_cl[run.x & 0x0fffffff].x;
+            const int b1 = cell_cl[run.y - 1].y;
             for (; b0 < b1; b0 += 32)
             {
                 const int cj = b0 + lane;
@@ -628,16 +607,15 @@ __global__ void k_export_zero(int n, spgnb_atom_group* __restrict__ nl, const in
     }
 }
 
-__global__ void k_export(int nc_cap, int table_cap, const int* __restrict__ tcount, const float4* __restrict__ tab,
+__global__ void k_export(int clusters_cap, int table_cap, const int* __restrict__ tcount, const float4* __restrict__ tab,
                          const uint2* __restrict__ tmask, const int* __restrict__ slot_atom,
                          const float4* __restrict__ slot_x0, spgnb_atom_group* __restrict__ nl,
                          int* __restrict__ temp, int max_nb, int* counters)
 {
     if (counters[kCntNeed] == 0) return;
     const int lane = threadIdx.x & 31;
-    const int nc = min(counters[kCntClusters], nc_cap);
     const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < nc; c += warps)
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < clusters_cap; c += warps)
     {
         // own atoms and global indices, lane a holds slot a
         const int own_atom = lane < 8 ? slot_atom[c * kClusterSize + lane] : -1;
@@ -679,23 +657,31 @@ __global__ void k_export(int nc_cap, int table_cap, const int* __restrict__ tcou
     }
 }
 
-__global__ void k_finish(int G, int* __restrict__ cell_count, int* __restrict__ cell_cursor, int* counters)
+__global__ void k_finish(int G, int S, const int* __restrict__ cell_sys, const int* __restrict__ need,
+                         int* __restrict__ prune, int* __restrict__ cell_count, int* __restrict__ cell_cursor,
+                         int* counters)
 {
     if (counters[kCntNeed] == 0) return;
     const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c < G)
+    if (c < G && need[cell_sys[c]])
     {
         cell_count[c] = 0;
         cell_cursor[c] = 0;
     }
-    if (c == 0)
+    if (c < S && need[c])
     {
-        counters[kCntBuilds] += 1;
-        counters[kCntPrune] = 1;  // the pruned lists belong to the old build
+        prune[c] = 1;  // its pruned lists belong to the old build
+        atomicAdd(&counters[kCntBuilds], 1);
+        counters[kCntPrune] = 1;
     }
 }
 
-__global__ void k_set_need(int* counters) { counters[kCntNeed] = 1; }
+__global__ void k_set_need(int S, int* __restrict__ need, int* counters)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s < S) need[s] = 1;
+    if (s == 0) counters[kCntNeed] = 1;
+}
 
 __global__ void k_reset_list_counters(int* counters)
 {
@@ -815,7 +801,10 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_runs);
     dfree(nl->d_cell_count);
     dfree(nl->d_cell_cursor);
-    dfree(nl->d_cell_cl_start);
+    dfree(nl->d_cell_cl);
+    dfree(nl->d_need);
+    dfree(nl->d_prune);
+    dfree(nl->d_ncl);
     dfree(nl->d_atom_cell);
     dfree(nl->d_atom_shift);
     dfree(nl->d_tmp_atoms);
@@ -870,7 +859,7 @@ float prune_r2_of(float rc, float buffer)
 
 SysDesc make_desc(const SysHost& sh, float skin_permit)
 {
-    SysDesc d;
+    SysDesc d{};
     d.cell = make_cell(sh.cell);
     d.rcell = make_cell(sh.rcell);
     d.gl = sh.gl;
@@ -883,6 +872,8 @@ SysDesc make_desc(const SysHost& sh, float skin_permit)
     d.Ny = sh.dims[1];
     d.Nz = sh.dims[2];
     d.cell_begin = sh.cell_begin;
+    d.cl_begin = sh.cl_begin;
+    d.cl_cap = sh.cl_cap;
     d.atom_begin = sh.atom_begin;
     d.atom_count = sh.atom_count;
     d.triclinic = sh.triclinic ? 1 : 0;
@@ -915,8 +906,16 @@ int alloc_nl(spgnb_nl* nl)
         G += sh.dims[0] * sh.dims[1] * sh.dims[2];
     }
     nl->G = G;
-    nl->clusters_cap = n / kClusterSize + G + nl->S + 1;
-    if ((long long)(nl->clusters_cap + 1) * kClusterSize > kMaxSlots)
+    // each system owns a fixed cluster range: its atoms/8 + its cells + 1
+    long long ccap = 0;
+    for (auto& sh : nl->sys)
+    {
+        sh.cl_begin = (int)std::min<long long>(ccap, 0x7fffffff);
+        sh.cl_cap = sh.atom_count / kClusterSize + sh.dims[0] * sh.dims[1] * sh.dims[2] + 1;
+        ccap += sh.cl_cap;
+    }
+    nl->clusters_cap = (int)std::min<long long>(ccap, 0x7fffffff);
+    if ((ccap + 1) * kClusterSize > kMaxSlots)
         return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d atoms in %d cells exceed the %d-slot limit of the lists",
                     n, G, kMaxSlots);
     const size_t slots = (size_t)nl->clusters_cap * kClusterSize;
@@ -925,7 +924,7 @@ int alloc_nl(spgnb_nl* nl)
     for (auto& sh : nl->sys)
         if ((st = build_runs(sh, start, runs))) return st;
     nl->h_desc.resize(nl->S);
-    std::vector<int> atom_sys(n, 0), cell_sys(G, 0);
+    std::vector<int> atom_sys(n, 0), cell_sys(G, 0), cl_sys(nl->clusters_cap, 0);
     for (int s = 0; s < nl->S; s++)
     {
         const SysHost& sh = nl->sys[s];
@@ -933,6 +932,7 @@ int alloc_nl(spgnb_nl* nl)
         nl->h_desc[s].prune_r2 = prune_r2_of(nl->prune_rc, nl->opt.prune_buffer);
         for (int i = sh.atom_begin; i < sh.atom_begin + sh.atom_count && i < n; i++) atom_sys[i] = s;
         for (int c = 0; c < sh.dims[0] * sh.dims[1] * sh.dims[2]; c++) cell_sys[sh.cell_begin + c] = s;
+        for (int k = 0; k < sh.cl_cap; k++) cl_sys[sh.cl_begin + k] = s;
     }
     if ((st = dalloc(&nl->d_sys, nl->S))) return st;
     if ((st = dalloc(&nl->d_atom_sys, n))) return st;
@@ -946,7 +946,14 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemcpy(nl->d_runs, runs.data(), sizeof(int2) * runs.size(), cudaMemcpyHostToDevice));
     if ((st = dalloc(&nl->d_cell_count, G))) return st;
     if ((st = dalloc(&nl->d_cell_cursor, G))) return st;
-    if ((st = dalloc(&nl->d_cell_cl_start, G + 1))) return st;
+    if ((st = dalloc(&nl->d_cell_cl, G))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_cell_cl, 0, sizeof(int2) * G));
+    if ((st = dalloc(&nl->d_need, nl->S))) return st;
+    if ((st = dalloc(&nl->d_prune, nl->S))) return st;
+    if ((st = dalloc(&nl->d_ncl, nl->S))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_need, 0, sizeof(int) * nl->S));
+    SPGNB_CUDA(cudaMemset(nl->d_prune, 0, sizeof(int) * nl->S));
+    SPGNB_CUDA(cudaMemset(nl->d_ncl, 0, sizeof(int) * nl->S));
     SPGNB_CUDA(cudaMemset(nl->d_cell_count, 0, sizeof(int) * G));
     SPGNB_CUDA(cudaMemset(nl->d_cell_cursor, 0, sizeof(int) * G));
     if ((st = dalloc(&nl->d_atom_cell, n))) return st;
@@ -967,7 +974,7 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemset(nl->d_pcount, 0, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_cl_cell, nl->clusters_cap))) return st;
     if ((st = dalloc(&nl->d_cl_sys, nl->clusters_cap))) return st;
-    SPGNB_CUDA(cudaMemset(nl->d_cl_sys, 0, sizeof(int) * nl->clusters_cap));
+    SPGNB_CUDA(cudaMemcpy(nl->d_cl_sys, cl_sys.data(), sizeof(int) * nl->clusters_cap, cudaMemcpyHostToDevice));
     if ((st = dalloc(&nl->d_cl_u, nl->clusters_cap))) return st;
     // one more: the null cluster of the padding slot (centre 0)
     if ((st = dalloc(&nl->d_cl_q, nl->clusters_cap + 1))) return st;
@@ -1071,7 +1078,8 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
     nl->cs2 = nl->sys[0].cs2;
     nl->cell = nl->sys[0].cell;
     nl->rcell = nl->sys[0].rcell;
-    nl->triclinic = nl->sys[0].triclinic;
+    nl->triclinic = false;  // any system: the force kernel's box-shape variant
+    for (const auto& sh : nl->sys) nl->triclinic = nl->triclinic || sh.triclinic;
     memcpy(nl->dims, nl->sys[0].dims, sizeof(nl->dims));
     nl->prune_rc = 0.0f;
     for (const auto& sh : nl->sys) nl->prune_rc = std::max(nl->prune_rc, sh.cutoff);
@@ -1097,42 +1105,42 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     const int ccap = nl->clusters_cap;
     if (host_rebuild)
     {
-        k_set_need<<<1, 1, 0, s>>>(nl->d_counters);
+        k_set_need<<<(nl->S + 255) / 256, 256, 0, s>>>(nl->S, nl->d_need, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_set_need");
     }
     else
     {
         SPGNB_CUDA(cudaMemsetAsync(nl->d_counters + kCntNeed, 0, sizeof(int), s));
+        SPGNB_CUDA(cudaMemsetAsync(nl->d_need, 0, sizeof(int) * nl->S, s));
         k_check_refresh<<<(slots_cap + 255) / 256, 256, 0, s>>>(slots_cap, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
-                                                                  d_crd, nl->d_slot_x0, nl->d_counters);
+                                                                  d_crd, nl->d_slot_x0, nl->d_need, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_check_refresh");
     }
     k_reset_list_counters<<<1, 1, 0, s>>>(nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_reset_list_counters");
     k_bin<<<(n + 255) / 256, 256, 0, s>>>(n, d_crd, nl->d_atom_sys, nl->d_sys, nl->d_atom_cell, nl->d_atom_shift,
-                                            nl->d_wrapped, nl->d_cell_count, nl->d_counters);
+                                            nl->d_wrapped, nl->d_cell_count, nl->d_need, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_bin");
-    k_scan_cells<<<1, 1024, 0, s>>>(nl->G, nl->d_cell_count, nl->d_cell_cl_start, nl->opt.max_atom_in_grid_numbers,
-                                     nl->clusters_cap, nl->d_counters);
+    k_scan_cells<<<nl->S, 1024, 0, s>>>(nl->d_sys, nl->d_cell_count, nl->d_cell_cl, nl->opt.max_atom_in_grid_numbers,
+                                         nl->d_need, nl->d_ncl, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_scan_cells");
-    k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_atom_cell, nl->d_cell_cl_start, nl->d_cell_cursor,
-                                                nl->d_tmp_atoms, slots_cap, nl->d_counters);
+    k_scatter<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_atom_sys, nl->d_atom_cell, nl->d_cell_cl, nl->d_ncl, nl->d_sys,
+                                                nl->d_cell_cursor, nl->d_tmp_atoms, nl->d_need, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_scatter");
     k_sort_cells<<<std::min(nl->G, sms * 16), 128, kMaxCellAtoms * sizeof(unsigned long long), s>>>(
-        nl->G, nl->d_cell_sys, nl->d_sys, nl->d_cell_count, nl->d_cell_cl_start, nl->d_tmp_atoms, nl->d_wrapped,
-        nl->d_slot_atom, nl->d_cl_cell, nl->d_cl_sys, nl->d_atom_slot, slots_cap, nl->d_counters);
+        nl->G, nl->d_cell_sys, nl->d_sys, nl->d_cell_count, nl->d_cell_cl, nl->d_ncl, nl->d_tmp_atoms, nl->d_wrapped,
+        nl->d_slot_atom, nl->d_cl_cell, nl->d_atom_slot, nl->d_need, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_sort_cells");
-    k_cluster_props<<<(slots_cap + 255) / 256, 256, 0, s>>>(d_crd, nl->d_slot_atom, nl->d_atom_shift, d_atom_local,
-                                                             nl->d_cl_sys, nl->d_sys, nl->d_counters, nl->d_cl_u,
-                                                             nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0,
-                                                             nl->d_slot_ex, ex_start, ex_list, ex_num, ccap);
+    k_cluster_props<<<(slots_cap + 255) / 256, 256, 0, s>>>(
+        d_crd, nl->d_slot_atom, nl->d_atom_shift, d_atom_local, nl->d_cl_sys, nl->d_sys, nl->d_counters, nl->d_cl_u,
+        nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex, ex_start, ex_list, ex_num, ccap,
+        nl->d_need, nl->d_ncl, nl->d_tcount, nl->d_slot_count, nl->d_pcount);
     SPGNB_CHECK_LAUNCH("k_cluster_props");
     const int search_blocks = std::max(1, std::min((ccap + kSearchWarps - 1) / kSearchWarps, sms * 8));
     k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
-        nl->d_sys, nl->table_cap, nl->d_run_start, nl->d_runs, nl->d_cell_cl_start, nl->d_cl_cell, nl->d_cl_sys,
-        nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex, ex_start, ex_list, ex_num,
-        nl->d_tcount,
-        nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_counters);
+        nl->d_sys, ccap, nl->table_cap, nl->d_need, nl->d_ncl, nl->d_run_start, nl->d_runs, nl->d_cell_cl,
+        nl->d_cl_cell, nl->d_cl_sys, nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex,
+        ex_start, ex_list, ex_num, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_search");
     if (nl->opt.export_atom_groups)
     {
@@ -1143,7 +1151,9 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
             nl->d_temp, nl->opt.max_neighbor_numbers, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_export");
     }
-    k_finish<<<(nl->G + 255) / 256, 256, 0, s>>>(nl->G, nl->d_cell_count, nl->d_cell_cursor, nl->d_counters);
+    const int fin = std::max(nl->G, nl->S);
+    k_finish<<<(fin + 255) / 256, 256, 0, s>>>(nl->G, nl->S, nl->d_cell_sys, nl->d_need, nl->d_prune,
+                                                  nl->d_cell_count, nl->d_cell_cursor, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_finish");
     nl->built = true;
     nl->local_atoms = n;
@@ -1160,6 +1170,8 @@ int nl_set_prune_rc(spgnb_nl* nl, float rc, cudaStream_t s)
     for (auto& d : nl->h_desc) d.prune_r2 = prune_r2_of(rc, nl->opt.prune_buffer);
     SPGNB_CUDA(cudaMemcpyAsync(nl->d_sys, nl->h_desc.data(), sizeof(SysDesc) * nl->S, cudaMemcpyHostToDevice, s));
     SPGNB_CUDA(cudaStreamSynchronize(s));
+    const std::vector<int> ones(nl->S, 1);
+    SPGNB_CUDA(cudaMemcpyAsync(nl->d_prune, ones.data(), sizeof(int) * nl->S, cudaMemcpyHostToDevice, s));
     const int one = 1;
     SPGNB_CUDA(cudaMemcpyAsync(nl->d_counters + kCntPrune, &one, sizeof(int), cudaMemcpyHostToDevice, s));
     SPGNB_CUDA(cudaStreamSynchronize(s));
@@ -1297,11 +1309,15 @@ int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out)
     out->grid_dims[0] = nl->dims[0];
     out->grid_dims[1] = nl->dims[1];
     out->grid_dims[2] = nl->dims[2];
-    out->clusters = h[kCntClusters];
+    std::vector<int> ncl(nl->S);
+    SPGNB_CUDA(cudaMemcpy(ncl.data(), nl->d_ncl, sizeof(int) * nl->S, cudaMemcpyDeviceToHost));
+    long long nclt = 0;
+    for (int v : ncl) nclt += v;
+    out->clusters = (int)nclt;
     long long e;
     memcpy(&e, &h[kCntEntries], sizeof(e));
     out->entries = e;
-    out->work_items = h[kCntClusters];
+    out->work_items = (int)nclt;
     out->builds = h[kCntBuilds];
     out->overflow = h[kCntOverflow];
     memcpy(&out->full_list_words, &h[kCntWords], sizeof(long long));

@@ -80,25 +80,6 @@ __device__ __forceinline__ void red_fixed(long long* acc, float v)
     if (q != 0) atomicAdd((unsigned long long*)acc, (unsigned long long)q);
 }
 
-struct OwnerMap
-{
-    const int* atom_local;   // global index of each local atom
-    int solvent_start;       // first local atom of the water tail (n when none)
-    int water_points;
-    __device__ __forceinline__ int remap(int a) const
-    {
-        return a >= solvent_start ? solvent_start + ((a - solvent_start) / water_points) * water_points : a;
-    }
-};
-
-struct PerAtomOut
-{
-    float* energy;       // caller's atom_energy (+=)
-    float* lj_energy;    // module's per-atom LJ energy
-    float* direct;       // atom_direct_pme_energy
-    float* virial;       // caller's LTMatrix3 array (+=), 6 floats per atom
-};
-
 // Per-step slot pack: each slot's offset from the build-time cluster centre
 // moved by the displacement since the build (minimum image in the system's
 // box, so a caller that wraps coordinates between builds is fine), with the
@@ -111,7 +92,7 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
                              const float4* __restrict__ x0, const float4* __restrict__ d0,
                              const float3* __restrict__ crd, const float* __restrict__ charge,
                              const int* __restrict__ local_type, float4* __restrict__ pos, int* __restrict__ ptype,
-                             const float4* __restrict__ pref, float half_buffer2)
+                             const float4* __restrict__ pref, float half_buffer2, int* __restrict__ prune)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     bool moved = false;
@@ -120,7 +101,7 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
         pos[s] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
         ptype[s] = 0;
     }
-    else if (s < slots_cap && s < counters[kCntClusters] * kClusterSize)
+    else if (s < slots_cap)
     {
         const int a = slot_atom[s];
         const float4 d = d0[s];
@@ -145,12 +126,13 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
                 const float4 r = pref[s];
                 const float ex = p.x - r.x, ey = p.y - r.y, ez = p.z - r.z;
                 moved = ex * ex + ey * ey + ez * ez > half_buffer2;
+                if (moved) prune[cl_sys[s >> 3]] = 1;
             }
         }
         pos[s] = p;
         ptype[s] = t;
     }
-    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) atomicExch(&counters[kCntPrune], 1);
+    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) counters[kCntPrune] = 1;
 }
 
 // Pruning (no reference counterpart; results unchanged).  Runs after every
@@ -171,14 +153,14 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
             int table_cap, int slot_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
             const int* __restrict__ tcount, const float4* __restrict__ tab, const uint2* __restrict__ tmask,
             const float4* __restrict__ pos, const int* __restrict__ ptype, float4* __restrict__ pref,
-            int* __restrict__ pcount, unsigned* __restrict__ pwords)
+            int* __restrict__ pcount, unsigned* __restrict__ pwords, int n_sys, int* __restrict__ prune)
 {
     if (counters[kCntPrune] == 0) return;
     __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];  // {partner slot | image flag, element}
     __shared__ unsigned long long kept_total;
     const int lane = threadIdx.x & 31;
     const int a = threadIdx.x >> 5;
-    const int nc = min(counters[kCntClusters], clusters_cap);
+    const int nc = clusters_cap;
     const unsigned null_word = (unsigned)(clusters_cap * kClusterSize);
     const int usable = slot_cap - 64;
     if (threadIdx.x == 0) kept_total = 0;
@@ -186,6 +168,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
     uint2* __restrict__ mybuf = buf[a];
     for (int c = blockIdx.x; c < nc; c += gridDim.x)
     {
+        if (!prune[cl_sys[c]]) continue;
         const int s = c * kClusterSize + a;
         const float4 pi = pos[s];
         if (lane == 0) pref[s] = pi;
@@ -280,20 +263,24 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
             atomicAdd(&kept_total, (unsigned long long)kept);
         }
     }
+    __shared__ int is_last;
     __syncthreads();
     if (threadIdx.x == 0)
     {
         atomicAdd((unsigned long long*)&counters[kCntPWords], kept_total);
         __threadfence();
-        const int done = atomicAdd(&counters[kCntPruneDone], 1);
-        if (done == gridDim.x - 1)
-        {
-            unsigned long long* w = (unsigned long long*)&counters[kCntPWords];
-            *(unsigned long long*)&counters[kCntPWordsLast] = atomicExch(w, 0ull);
-            counters[kCntPruneDone] = 0;
-            counters[kCntPrune] = 0;
-            counters[kCntPrunes] += 1;
-        }
+        is_last = atomicAdd(&counters[kCntPruneDone], 1) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return;
+    for (int q = threadIdx.x; q < n_sys; q += blockDim.x) prune[q] = 0;
+    if (threadIdx.x == 0)
+    {
+        unsigned long long* w = (unsigned long long*)&counters[kCntPWords];
+        *(unsigned long long*)&counters[kCntPWordsLast] = atomicExch(w, 0ull);
+        counters[kCntPruneDone] = 0;
+        counters[kCntPrune] = 0;
+        counters[kCntPrunes] += 1;
     }
 }
 
@@ -400,7 +387,7 @@ __device__ __forceinline__ float centre_step(int qj, int qi)
 template <int MODE, int FIT, bool TRI>
 __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ? 3 : 2))
     k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
-                const int* __restrict__ counters, int clusters_cap, int slot_cap,
+                int n_clusters, int slot_cap,
                 const int* __restrict__ cl_sys, const int* __restrict__ pcount, const unsigned* __restrict__ pwords,
                 const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0, const int4* __restrict__ cl_q,
                 const float4* __restrict__ pos, const int* __restrict__ ptype,
@@ -420,14 +407,29 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
     constexpr bool PA = MODE >= 2;
     const int lane = threadIdx.x & 31;
     const int a = threadIdx.x >> 5;
-    const int nc = min(counters[kCntClusters], clusters_cap);
+    int cur_sys = -1;  // the system red[a] accumulates for (the same sequence in every warp)
 
-    for (int c = blockIdx.x; c < nc; c += gridDim.x)
+    // clusters strided over the blocks: at any moment the blocks are spread
+    // over all systems and the whole of each box (contiguous runs per block
+    // measured slower)
+    for (int c = blockIdx.x; c < n_clusters; c += gridDim.x)
     {
         const int s = c * kClusterSize + a;
         const int n = pcount[s];  // a multiple of 64
         if (n == 0) continue;
         const int sy = cl_sys[c];
+        if (EN && sy != cur_sys)
+        {
+            // totals belong to one system each: flush this warp's share
+            if (lane == 0 && cur_sys >= 0)
+                for (int q = 0; q < 8; q++)
+                {
+                    const long long v = red[a][q];
+                    if (v) atomicAdd((unsigned long long*)&totals[8 * cur_sys + q], (unsigned long long)v);
+                    red[a][q] = 0;
+                }
+            cur_sys = sy;
+        }
         const ForceParams P = fps ? fps[sy] : p0;
         const Cell qc = sys[sy].qcell;
         const float4 pi = pos[s];
@@ -591,12 +593,27 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
     }
     if (EN)
     {
+        // the warps end on the same cluster, or on no cluster at all
+        __shared__ int end_sys[kForceWarps];
+        if (lane == 0) end_sys[a] = cur_sys;
         __syncthreads();
         if (threadIdx.x < 8)
         {
             long long t = 0;
-            for (int w = 0; w < kForceWarps; w++) t += red[w][threadIdx.x];
-            if (t) atomicAdd((unsigned long long*)&totals[threadIdx.x], (unsigned long long)t);
+            int sys_end = -1;
+            for (int w = 0; w < kForceWarps; w++)
+                if (end_sys[w] >= 0)
+                {
+                    if (sys_end >= 0 && end_sys[w] != sys_end)
+                    {
+                        const long long v = red[w][threadIdx.x];
+                        if (v) atomicAdd((unsigned long long*)&totals[8 * end_sys[w] + threadIdx.x], (unsigned long long)v);
+                        continue;
+                    }
+                    sys_end = end_sys[w];
+                    t += red[w][threadIdx.x];
+                }
+            if (t && sys_end >= 0) atomicAdd((unsigned long long*)&totals[8 * sys_end + threadIdx.x], (unsigned long long)t);
         }
     }
 }
@@ -972,8 +989,7 @@ int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
     const spgnb_nl* nl = x.nl;
     const int grid = std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T>, kForceWarps * 32, smem), nl->clusters_cap));
     k_pair_fast<M, F, T><<<grid, kForceWarps * 32, smem, s>>>(
-        x.p0, x.fps, nl->d_sys, nl->d_counters, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount,
-        nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table,
+        x.p0, x.fps, nl->d_sys, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table,
         x.table_size, x.frc, x.totals, x.om, x.pa);
     SPGNB_CHECK_LAUNCH("k_pair_fast");
     return SPGNB_OK;
@@ -997,6 +1013,51 @@ int launch_fast_any(const FastArgs& x, int mode, bool fit, bool tri, size_t smem
     if (mode == 1) return launch_fast_ft<1>(x, fit, tri, smem, s);
     return launch_fast_ft<2>(x, fit, tri, smem, s);
 }
+
+}  // namespace
+
+int force_kernels_init(int table_size)
+{
+    const size_t smem = sizeof(float2) * table_size;
+    if (smem > 48 * 1024)
+    {
+        set_fast_smem<0>(smem);
+        set_fast_smem<1>(smem);
+        set_fast_smem<2>(smem);
+    }
+    return SPGNB_OK;
+}
+
+int force_pipeline(const ForceInputs& in, cudaStream_t s)
+{
+    spgnb_nl* nl = in.nl;
+    const int slots = nl->clusters_cap * kClusterSize;
+    const bool track = nl->opt.prune_buffer > 0.0f;
+    const float half = 0.5f * nl->opt.prune_buffer;
+    k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
+                                                     nl->d_slot_x0, nl->d_slot_d0, in.crd, in.charge, in.atom_type,
+                                                     in.slot_pos, in.slot_type, track ? nl->d_pref : nullptr,
+                                                     half * half, nl->d_prune);
+    SPGNB_CHECK_LAUNCH("k_pack_slots");
+    const int grid = std::max(1, std::min(num_sms() * 4, nl->clusters_cap));
+    k_prune<<<grid, kPruneWarps * 32, 0, s>>>(in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters, nl->clusters_cap,
+                                              nl->table_cap, nl->slot_cap, nl->d_cl_sys, nl->d_sys, nl->d_tcount,
+                                              nl->d_tab, nl->d_tmask, in.slot_pos, in.slot_type, nl->d_pref,
+                                              nl->d_pcount, nl->d_pwords, nl->S, nl->d_prune);
+    SPGNB_CHECK_LAUNCH("k_prune");
+    cudaEvent_t ev0, ev1;
+    pair_events(&ev0, &ev1);
+    if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
+    const FastArgs fa{in.p0, in.d_fps, nl, in.slot_pos, in.slot_type, in.table, in.table_size, in.frc,
+                      in.totals, in.om, in.pa};
+    const int st = launch_fast_any(fa, in.mode, in.fit, nl->triclinic, sizeof(float2) * in.table_size, s);
+    if (st) return st;
+    if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
+    return SPGNB_OK;
+}
+
+namespace
+{
 
 int check_common(spgnb_lj* lj, int local_atom_numbers, int ghost_numbers, const spgnb_vector* d_crd,
                  const float* d_charge, spgnb_vector* d_frc)
@@ -1064,13 +1125,7 @@ int spgnb_lj_create(int atom_numbers, int atom_type_numbers, const int* h_atom_t
         spgnb_lj_destroy(lj);
         return st;
     }
-    const int smem = (int)(sizeof(float2) * T * T);
-    if (smem > 48 * 1024)
-    {
-        set_fast_smem<0>(smem);
-        set_fast_smem<1>(smem);
-        set_fast_smem<2>(smem);
-    }
+    force_kernels_init(T * T);
     cudaMemcpy(lj->d_atom_type, h_atom_type, sizeof(int) * atom_numbers, cudaMemcpyHostToDevice);
     cudaMemcpy(lj->d_table, table.data(), sizeof(float2) * table.size(), cudaMemcpyHostToDevice);
     cudaMemset(lj->d_frc_acc, 0, sizeof(long long) * 4 * (size_t)atom_numbers);
@@ -1133,45 +1188,39 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
             SPGNB_CUDA(cudaMemsetAsync(d_atom_direct_pme_energy, 0, sizeof(float) * lj->atom_numbers, s));
     }
     if ((st = nl_set_prune_rc(const_cast<spgnb_nl*>(nl), lj->cutoff, s))) return st;
-    const bool track = nl->opt.prune_buffer > 0.0f;
-    const float half = 0.5f * nl->opt.prune_buffer;
-    k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_cl_sys,
-                                                     nl->d_sys, nl->d_slot_x0, nl->d_slot_d0, (const float3*)d_crd,
-                                                     d_charge, lj->d_local_type, lj->d_sdata, lj->d_slot_type,
-                                                     track ? nl->d_pref : nullptr, half * half);
-    SPGNB_CHECK_LAUNCH("k_pack_slots");
-    const ForceParams fp = make_pair_const(lj, pme_beta);
-    const int grid = std::max(1, std::min(num_sms() * 4, nl->clusters_cap));
-    k_prune<<<grid, kPruneWarps * 32, 0, s>>>(fp, nullptr, nl->opt.prune_buffer, nl->d_counters, nl->clusters_cap,
-                                              nl->table_cap, nl->slot_cap, nl->d_cl_sys, nl->d_sys, nl->d_tcount,
-                                              nl->d_tab, nl->d_tmask, lj->d_sdata, lj->d_slot_type, nl->d_pref,
-                                              nl->d_pcount, nl->d_pwords);
-    SPGNB_CHECK_LAUNCH("k_prune");
-    OwnerMap om{nullptr, local_atom_numbers, 3};
-    PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
+    ForceInputs in;
+    in.nl = const_cast<spgnb_nl*>(nl);
+    in.crd = (const float3*)d_crd;
+    in.charge = d_charge;
+    in.atom_type = lj->d_local_type;
+    in.slot_pos = lj->d_sdata;
+    in.slot_type = lj->d_slot_type;
+    in.p0 = make_pair_const(lj, pme_beta);
+    in.fit = in.p0.use_fit != 0;
+    in.table = lj->d_table;
+    in.table_size = lj->n_types * lj->n_types;
+    in.frc = (float3*)d_frc;
+    in.totals = lj->d_totals;
     int mode = 0;
     if (need_atom_energy || need_virial) mode = 1;
     if ((need_atom_energy && (d_atom_energy || d_atom_direct_pme_energy)) || (need_virial && d_atom_virial))
         mode = 2;
+    in.mode = mode;
     if (mode == 2)
     {
-        om.atom_local = lj->d_atom_local;
-        om.solvent_start = local_atom_numbers - (solvent_numbers > 0 ? solvent_numbers : 0);
-        om.water_points = 3;
-        pa.energy = need_atom_energy ? d_atom_energy : nullptr;
-        pa.lj_energy = need_atom_energy ? lj->d_lj_energy_atom : nullptr;
-        pa.direct = need_atom_energy ? d_atom_direct_pme_energy : nullptr;
-        pa.virial = need_virial ? (float*)d_atom_virial : nullptr;
+        in.om.atom_local = lj->d_atom_local;
+        in.om.solvent_start = local_atom_numbers - (solvent_numbers > 0 ? solvent_numbers : 0);
+        in.om.water_points = 3;
+        in.pa.energy = need_atom_energy ? d_atom_energy : nullptr;
+        in.pa.lj_energy = need_atom_energy ? lj->d_lj_energy_atom : nullptr;
+        in.pa.direct = need_atom_energy ? d_atom_direct_pme_energy : nullptr;
+        in.pa.virial = need_virial ? (float*)d_atom_virial : nullptr;
     }
-    const int table_size = lj->n_types * lj->n_types;
-    const size_t smem = sizeof(float2) * table_size;
-    cudaEvent_t ev0, ev1;
-    pair_events(&ev0, &ev1);
-    if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
-    const FastArgs fa{fp, nullptr, nl, lj->d_sdata, lj->d_slot_type, lj->d_table, table_size, (float3*)d_frc,
-                      lj->d_totals, om, pa};
-    if ((st = launch_fast_any(fa, mode, fp.use_fit != 0, nl->triclinic, smem, s))) return st;
-    if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
+    else
+    {
+        in.om.solvent_start = local_atom_numbers;
+    }
+    if ((st = force_pipeline(in, s))) return st;
     lj->have_energy = need_atom_energy != 0;
     lj->have_virial = need_virial != 0;
     return SPGNB_OK;

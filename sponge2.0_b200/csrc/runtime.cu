@@ -3,6 +3,8 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <stdlib.h>
+
 #include "common.cuh"
 
 namespace spgnb
@@ -16,6 +18,17 @@ unsigned long long g_launches = 0;
 }  // namespace
 
 void count_launch() { __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAXED); }
+
+// SPGNB_SYNC_CHECK=1: every launch is followed by a device synchronisation so
+// that an execution error is reported against the kernel that caused it.
+bool sync_check()
+{
+    static const bool on = [] {
+        const char* v = getenv("SPGNB_SYNC_CHECK");
+        return v && v[0] == '1';
+    }();
+    return on;
+}
 
 void pair_events(cudaEvent_t* start, cudaEvent_t* stop)
 {

@@ -27,6 +27,8 @@ EXPORTED = [
     "spgnb_solvent_create", "spgnb_solvent_get_local", "spgnb_solvent_pme_direct_force", "spgnb_solvent_destroy",
     "spgnb_launch_count", "spgnb_debug_set_pair_events", "spgnb_nl_count_pairs", "spgnb_probe_fp32_fma_tflops",
     "spgnb_lj_pme_direct_force_noalloc",
+    "spgnb_batch_default_options", "spgnb_batch_create", "spgnb_batch_run", "spgnb_batch_energies",
+    "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_destroy",
 ]
 
 
@@ -52,6 +54,20 @@ class NLOptions(C.Structure):
                 ("skin_permit", C.c_float), ("check_overflow_interval", C.c_int),
                 ("throw_error_when_overflow", C.c_int), ("export_atom_groups", C.c_int),
                 ("max_entries_per_cluster", C.c_int), ("prune_buffer", C.c_float)]
+
+
+class BatchSystem(C.Structure):
+    _fields_ = [("atom_numbers", C.c_int), ("cutoff", C.c_float), ("skin", C.c_float), ("pme_beta", C.c_float),
+                ("cell", LTMatrix3), ("rcell", LTMatrix3), ("h_crd", C.c_void_p), ("h_vel", C.c_void_p),
+                ("h_charge", C.c_void_p), ("h_mass", C.c_void_p), ("h_atom_type", C.c_void_p),
+                ("h_excluded_start", C.c_void_p), ("h_excluded_numbers", C.c_void_p),
+                ("h_excluded_list", C.c_void_p), ("excluded_total", C.c_int), ("water_begin", C.c_int),
+                ("water_numbers", C.c_int)]
+
+
+class BatchOptions(C.Structure):
+    _fields_ = [("dt", C.c_float), ("water_doh", C.c_float), ("water_dhh", C.c_float), ("skin_permit", C.c_float),
+                ("prune_buffer", C.c_float), ("steps_per_graph", C.c_int), ("use_graphs", C.c_int)]
 
 
 class NLStats(C.Structure):
@@ -89,6 +105,16 @@ def lib():
     L.spgnb_nl_copy_atom_groups.argtypes = [vp, vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]
     L.spgnb_nl_get_stats.argtypes = [vp, C.POINTER(NLStats)]
     L.spgnb_nl_destroy.argtypes = [vp]
+    L.spgnb_batch_default_options.argtypes = [C.POINTER(BatchOptions)]
+    L.spgnb_batch_default_options.restype = None
+    L.spgnb_batch_create.argtypes = [i, C.POINTER(BatchSystem), i, vp, vp, C.POINTER(BatchOptions), C.POINTER(vp)]
+    L.spgnb_batch_run.argtypes = [vp, i, i]
+    L.spgnb_batch_energies.argtypes = [vp, vp]
+    L.spgnb_batch_download.argtypes = [vp, i, vp, vp, vp]
+    L.spgnb_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                    C.POINTER(C.c_int)]
+    L.spgnb_batch_autotune.argtypes = [vp, i, C.POINTER(C.c_float)]
+    L.spgnb_batch_destroy.argtypes = [vp]
     L.spgnb_lj_create.argtypes = [i, i, vp, vp, vp, f, C.POINTER(vp)]
     L.spgnb_lj_get_local.argtypes = [vp, vp, i, i]
     L.spgnb_lj_pme_direct_force.argtypes = [vp, i, i, i, i, vp, vp, vp, M, M, vp, f, i, vp, i, vp, vp]

@@ -197,7 +197,7 @@ def _solute_types(rng, n_types=20):
 
 def water_system(n_waters, box, seed, n_solute=0, cutoff=10.0, skin=2.0,
                  tolerance=1e-5, jitter=0.3, angles=(90.0, 90.0, 90.0),
-                 temperature=300.0, n_solute_types=20, name=""):
+                 temperature=300.0, n_solute_types=20, name="", solute_types=None):
     """Water (+ optional LJ solute) box on a jittered lattice.
 
     Lattice sites fill the box; waters sit on jittered sites with uniformly
@@ -221,10 +221,14 @@ def water_system(n_waters, box, seed, n_solute=0, cutoff=10.0, skin=2.0,
     centers[:n_solute] = lattice[:n_solute]
 
     sol_sig = sol_eps = None
-    if n_solute:
+    if solute_types is not None:
+        # a type table shared with other systems (all types present even
+        # without solutes, so every such system has the same table)
+        sol_sig, sol_eps = solute_types
+    elif n_solute:
         sol_sig, sol_eps = _solute_types(rng, n_solute_types)
-    sigma_all = np.concatenate([[SIGMA_O, 0.0], sol_sig if n_solute else []])
-    eps_all = np.concatenate([[EPS_O, 0.0], sol_eps if n_solute else []])
+    sigma_all = np.concatenate([[SIGMA_O, 0.0], sol_sig if sol_sig is not None else []])
+    eps_all = np.concatenate([[EPS_O, 0.0], sol_eps if sol_eps is not None else []])
     n_types = len(sigma_all)
     pair_A, pair_B = lj_pair_tables(sigma_all, eps_all)
 
@@ -360,6 +364,8 @@ def batch_systems(n_systems=256, seed=4, n_min=1500, n_max=24000, skin=2.0):
     rc + skin <= L/2, so each pair has a single minimum image.
     """
     rng = np.random.default_rng(seed)
+    # one solute type table for the whole batch
+    types = shared_solute_types(seed)
     out = []
     for k in range(n_systems):
         n_atoms = int(math.exp(rng.uniform(math.log(n_min), math.log(n_max))))
@@ -372,7 +378,7 @@ def batch_systems(n_systems=256, seed=4, n_min=1500, n_max=24000, skin=2.0):
             allowed = [max(4.0, L / 2 - skin)]
         rc = float(rng.choice(allowed))
         out.append(water_system(n_w, L, int(rng.integers(1 << 31)), n_solute=n_sol, cutoff=rc,
-                                skin=skin, name=f"batch-{k}"))
+                                skin=skin, name=f"batch-{k}", solute_types=types))
     return out
 
 
@@ -403,6 +409,11 @@ def request_stream(duration_s=600.0, rate_per_s=40.0, seed=5, n_min=1000, n_max=
     return out
 
 
+def shared_solute_types(seed=4):
+    """The one solute type table of the batched and served workloads."""
+    return _solute_types(np.random.default_rng(seed + 1000), 20)
+
+
 def request_system(req: Request, skin=2.0):
     rng = np.random.default_rng(req.seed)
     frac_sol = rng.uniform(0.0, 0.15)
@@ -414,4 +425,4 @@ def request_system(req: Request, skin=2.0):
         allowed = [max(4.0, L / 2 - skin)]
     rc = float(rng.choice(allowed))
     return water_system(n_w, L, int(rng.integers(1 << 31)), n_solute=n_sol, cutoff=rc, skin=skin,
-                        name=f"req-{req.rid}")
+                        name=f"req-{req.rid}", solute_types=shared_solute_types())

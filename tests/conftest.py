@@ -26,3 +26,11 @@ def rel_rms(a, b):
     a = np.asarray(a, np.float64)
     b = np.asarray(b, np.float64)
     return float(np.sqrt(((a - b) ** 2).sum(axis=-1).mean()) / np.sqrt((b ** 2).sum(axis=-1).mean()))
+
+
+@pytest.fixture(scope="session")
+def torch_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return torch

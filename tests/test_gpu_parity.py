@@ -31,14 +31,6 @@ def _systems():
 SYSTEMS = _systems()
 
 
-@pytest.fixture(scope="module")
-def torch_cuda():
-    import torch
-    if not torch.cuda.is_available():
-        pytest.skip("no CUDA device")
-    return torch
-
-
 def _path(system, **kw):
     from spgnb.engine import PlainPath
     return PlainPath(system, **kw)
