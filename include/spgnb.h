@@ -338,6 +338,10 @@ typedef struct
     float prune_buffer;            /* as spgnb_nl_options.prune_buffer, 1.0 */
     int steps_per_graph;           /* steps per captured graph, 10 */
     int use_graphs;                /* 1 = replay captured graphs, 0 = launch each step */
+    float thermostat_tau;          /* Berendsen coupling time (ps) per system, 0 = off */
+    float temperature;             /* its target (K), 300 */
+    int refresh_interval;          /* > 0: rebuild every system's list every this many steps
+                                      (neighbor_list_refresh_interval); 0: per-system skin trigger */
 } spgnb_batch_options;
 
 void spgnb_batch_default_options(spgnb_batch_options* opt);
@@ -359,11 +363,18 @@ int spgnb_batch_energies(spgnb_batch* b, double* out);
 /* Coordinates, velocities and forces of system `sys` (3N floats each, NULL
  * to skip).  Synchronises. */
 int spgnb_batch_download(spgnb_batch* b, int sys, float* h_crd, float* h_vel, float* h_frc);
+/* Changes the per-system Berendsen thermostat (tau 0 = off) for later steps. */
+int spgnb_batch_set_thermostat(spgnb_batch* b, float tau, float temperature);
+/* Reads the overflow flags (synchronises); on overflow regrows the buffers,
+ * rebuilds every list and sets *regrown. */
+int spgnb_batch_check_overflow(spgnb_batch* b, int* regrown);
 /* Steps done, list rebuilds (all systems), prunings, overflow flags. */
 int spgnb_batch_stats(spgnb_batch* b, long long* steps, long long* rebuilds, long long* prunings, int* overflow);
 /* Picks the prune buffer with the fastest step for this batch by timing a
  * few steps of each candidate (the systems advance meanwhile). */
 int spgnb_batch_autotune(spgnb_batch* b, int steps_per_candidate, float* chosen_buffer);
+/* The batch's CUDA stream (a cudaStream_t), for events around its work. */
+void* spgnb_batch_stream(spgnb_batch* b);
 int spgnb_batch_destroy(spgnb_batch* b);
 
 /* ------------------------------------------------------------ diagnostics */

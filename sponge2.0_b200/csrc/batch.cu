@@ -52,6 +52,10 @@ struct spgnb_batch
     std::vector<spgnb::ForceParams> h_fps;
     bool fit = true;
     long long* d_totals = nullptr;  // 8 per system
+    int* d_atom_sys = nullptr;      // system of each atom (thermostat)
+    double* d_kin = nullptr;        // per system: sum of m v^2
+    int* d_step = nullptr;          // steps done, on the device (interval refresh)
+    float* d_ndof = nullptr;        // per system: degrees of freedom
     float4* d_slot_pos = nullptr;
     int* d_slot_type = nullptr;
     // per system, host
@@ -60,6 +64,7 @@ struct spgnb_batch
     // stepping
     float ra = 0, rb = 0, rc = 0, mO = 0, mH = 0;
     cudaGraphExec_t g_plain = nullptr, g_energy = nullptr;
+    long long kernels_plain = 0, kernels_energy = 0;  // kernel launches inside each graph
     long long steps_done = 0;
 };
 
@@ -152,6 +157,30 @@ __global__ void k_settle(int n_waters, const int* __restrict__ waters, float3* _
     vel[o + 2] = mul3(sub3(c3, c0), inv_dt);
 }
 
+// Berendsen weak coupling per system: twice the kinetic energy, then every
+// velocity scaled by sqrt(1 + dt/tau (T0/T - 1)) (clamped to [0.8, 1.25]).
+__global__ void k_kinetic(int n, const float3* __restrict__ vel, const float* __restrict__ inv_mass,
+                          const int* __restrict__ atom_sys, double* __restrict__ kin)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || inv_mass[i] == 0.0f) return;
+    const float3 v = vel[i];
+    atomicAdd(&kin[atom_sys[i]], (double)((v.x * v.x + v.y * v.y + v.z * v.z) / inv_mass[i]));
+}
+
+__global__ void k_rescale(int n, float3* __restrict__ vel, const int* __restrict__ atom_sys,
+                          const double* __restrict__ kin, const float* __restrict__ ndof, float kT0, float coupling)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int s = atom_sys[i];
+    const double kT = kin[s] / fmax((double)ndof[s], 1.0);  // k_B T = 2 E_kin / dof
+    const float lam2 = kT > 0.0 ? 1.0f + coupling * (float)(kT0 / kT - 1.0) : 1.0f;
+    const float lam = sqrtf(fminf(fmaxf(lam2, 0.64f), 1.5625f));
+    float3 v = vel[i];
+    vel[i] = make_float3(v.x * lam, v.y * lam, v.z * lam);
+}
+
 int batch_force(spgnb_batch* b, int mode, cudaStream_t s)
 {
     SPGNB_CUDA(cudaMemsetAsync(b->d_frc, 0, sizeof(float3) * b->n, s));
@@ -189,8 +218,19 @@ int batch_step(spgnb_batch* b, bool energy, cudaStream_t s)
                                                             1.0f / dt);
         SPGNB_CHECK_LAUNCH("k_settle");
     }
-    int st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num, false,
-                            s);
+    if (b->opt.thermostat_tau > 0.0f)
+    {
+        SPGNB_CUDA(cudaMemsetAsync(b->d_kin, 0, sizeof(double) * b->S, s));
+        k_kinetic<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_vel, b->d_inv_mass, b->d_atom_sys, b->d_kin);
+        SPGNB_CHECK_LAUNCH("k_kinetic");
+        const float kT0 = 0.00198716f * b->opt.temperature;  // kcal/mol
+        k_rescale<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_vel, b->d_atom_sys, b->d_kin, b->d_ndof, kT0,
+                                                      b->opt.dt / b->opt.thermostat_tau);
+        SPGNB_CHECK_LAUNCH("k_rescale");
+    }
+    int st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num,
+                            b->opt.refresh_interval > 0 ? kBuildInterval : kBuildSkin, s, b->d_step,
+                            b->opt.refresh_interval);
     if (st) return st;
     return batch_force(b, energy ? 1 : 0, s);
 }
@@ -202,13 +242,17 @@ void free_graphs(spgnb_batch* b)
     b->g_plain = b->g_energy = nullptr;
 }
 
-int capture(spgnb_batch* b, bool energy_last, cudaGraphExec_t* out)
+int capture(spgnb_batch* b, bool energy_last, cudaGraphExec_t* out, long long* kernels)
 {
     cudaGraph_t g = nullptr;
     SPGNB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     int st = SPGNB_OK;
+    const unsigned long long c0 = launches_so_far();
     for (int k = 0; k < b->opt.steps_per_graph && !st; k++)
         st = batch_step(b, energy_last && k == b->opt.steps_per_graph - 1, b->stream);
+    // captured, not run: counted when the graph is launched
+    *kernels = (long long)(launches_so_far() - c0);
+    count_launches(-*kernels);
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     if (st)
     {
@@ -226,8 +270,8 @@ int ensure_graphs(spgnb_batch* b)
 {
     if (!b->opt.use_graphs || (b->g_plain && b->g_energy)) return SPGNB_OK;
     free_graphs(b);
-    int st = capture(b, false, &b->g_plain);
-    if (!st) st = capture(b, true, &b->g_energy);
+    int st = capture(b, false, &b->g_plain, &b->kernels_plain);
+    if (!st) st = capture(b, true, &b->g_energy, &b->kernels_energy);
     return st;
 }
 
@@ -251,6 +295,10 @@ void free_batch(spgnb_batch* b)
     dfree(b->d_table);
     dfree(b->d_fps);
     dfree(b->d_totals);
+    dfree(b->d_atom_sys);
+    dfree(b->d_kin);
+    dfree(b->d_ndof);
+    dfree(b->d_step);
     dfree(b->d_slot_pos);
     dfree(b->d_slot_type);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -283,6 +331,19 @@ void spgnb_batch_default_options(spgnb_batch_options* o)
     o->prune_buffer = 1.0f;
     o->steps_per_graph = 10;
     o->use_graphs = 1;
+    o->thermostat_tau = 0.0f;
+    o->temperature = 300.0f;
+    o->refresh_interval = 0;
+}
+
+int spgnb_batch_set_thermostat(spgnb_batch* b, float tau, float temperature)
+{
+    if (!b) return fail(SPGNB_E_ARG, "spgnb_batch_set_thermostat: NULL handle");
+    if (!(tau >= 0.0f) || !(temperature >= 0.0f)) return fail(SPGNB_E_ARG, "spgnb_batch_set_thermostat: bad values");
+    b->opt.thermostat_tau = tau;
+    b->opt.temperature = temperature;
+    free_graphs(b);
+    return SPGNB_OK;
 }
 
 int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int atom_type_numbers,
@@ -329,7 +390,8 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
     std::vector<float3> crd(b->n), vel(b->n);
     std::vector<float> charge(b->n), inv_mass(b->n);
     std::vector<int> type(b->n), iota(b->n), ex_start(b->n), ex_num(b->n), ex_list, waters;
-    std::vector<int> counts(n_systems);
+    std::vector<int> counts(n_systems), atom_sys(b->n);
+    std::vector<float> ndof(n_systems);
     std::vector<spgnb_ltmatrix3> cells(n_systems), rcells(n_systems);
     std::vector<float> cutoffs(n_systems), skins(n_systems);
     b->h_fps.resize(n_systems);
@@ -362,6 +424,10 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
                 ex_list.push_back(a0 + y.h_excluded_list[y.h_excluded_start[i] + k]);
         }
         for (int w = 0; w < y.water_numbers; w++) waters.push_back(a0 + y.water_begin + 3 * w);
+        for (int i = 0; i < y.atom_numbers; i++) atom_sys[a0 + i] = s;
+        int moving = 0;
+        for (int i = 0; i < y.atom_numbers; i++) moving += y.h_mass[i] > 0.0f;
+        ndof[s] = (float)std::max(1, 3 * moving - 3 * y.water_numbers - 3);
         counts[s] = y.atom_numbers;
         cells[s] = y.cell;
         rcells[s] = y.rcell;
@@ -431,6 +497,8 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
         (st = upload(&b->d_ex_num, ex_num)) || (st = upload(&b->d_ex_list, ex_list)) ||
         (st = upload(&b->d_waters, waters)) || (st = upload(&b->d_table, table)) ||
         (st = upload(&b->d_fps, b->h_fps)) || (st = dalloc(&b->d_totals, 8 * (size_t)n_systems)) ||
+        (st = upload(&b->d_atom_sys, atom_sys)) || (st = upload(&b->d_ndof, ndof)) ||
+        (st = dalloc(&b->d_kin, (size_t)n_systems)) || (st = dalloc(&b->d_step, 1)) ||
         (st = dalloc(&b->d_slot_pos, (size_t)b->nl->clusters_cap * kClusterSize + 1)) ||
         (st = dalloc(&b->d_slot_type, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
     {
@@ -439,6 +507,7 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
         return st;
     }
     force_kernels_init(T * T);
+    cudaMemset(b->d_step, 0, sizeof(int));
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess)
     {
@@ -447,7 +516,7 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
         return cuda_fail(e, "cudaStreamCreate");
     }
     // first lists and F(0) with energies
-    if ((st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num, true,
+    if ((st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num, kBuildForced,
                              b->stream)) ||
         (st = batch_force(b, 1, b->stream)))
     {
@@ -487,7 +556,7 @@ int spgnb_batch_run(spgnb_batch* b, int steps, int energy_interval)
             if (!any_inside)
             {
                 SPGNB_CUDA(cudaGraphLaunch(en ? b->g_energy : b->g_plain, b->stream));
-                count_launch();
+                count_launches(en ? b->kernels_energy : b->kernels_plain);
                 b->steps_done += K;
                 done += K;
                 continue;
@@ -593,6 +662,39 @@ int spgnb_batch_autotune(spgnb_batch* b, int steps_per_candidate, float* chosen_
     SPGNB_CUDA(cudaMemcpyAsync(b->nl->d_counters + kCntPrune, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
     SPGNB_CUDA(cudaStreamSynchronize(b->stream));
     if (chosen_buffer) *chosen_buffer = best;
+    return SPGNB_OK;
+}
+
+void* spgnb_batch_stream(spgnb_batch* b) { return b ? (void*)b->stream : nullptr; }
+
+int spgnb_batch_check_overflow(spgnb_batch* b, int* regrown)
+{
+    if (!b) return fail(SPGNB_E_ARG, "spgnb_batch_check_overflow: NULL handle");
+    if (regrown) *regrown = 0;
+    int flags = 0;
+    SPGNB_CUDA(cudaMemcpyAsync(&flags, b->nl->d_counters + kCntOverflow, sizeof(int), cudaMemcpyDeviceToHost,
+                               b->stream));
+    SPGNB_CUDA(cudaStreamSynchronize(b->stream));
+    if (!flags) return SPGNB_OK;
+    if (flags & kOvfCellHard)
+        return fail(SPGNB_E_OVERFLOW, "batch: a grid cell holds more than %d atoms (a system collapsed?)",
+                    kMaxCellAtoms);
+    int st = nl_regrow(b->nl, flags);
+    if (st) return st;
+    free_graphs(b);
+    const int S = b->S;
+    if (b->d_slot_pos) dfree(b->d_slot_pos);
+    if (b->d_slot_type) dfree(b->d_slot_type);
+    if ((st = dalloc(&b->d_slot_pos, (size_t)b->nl->clusters_cap * kClusterSize + 1)) ||
+        (st = dalloc(&b->d_slot_type, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
+        return st;
+    (void)S;
+    if ((st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num, kBuildForced,
+                             b->stream)) ||
+        (st = batch_force(b, 0, b->stream)))
+        return st;
+    SPGNB_CUDA(cudaStreamSynchronize(b->stream));
+    if (regrown) *regrown = 1;
     return SPGNB_OK;
 }
 

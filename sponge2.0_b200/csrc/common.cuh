@@ -27,6 +27,8 @@ int num_sms();
     } while (0)
 
 void count_launch();
+void count_launches(long long n);  // kernels of a replayed graph; negative to undo captured ones
+unsigned long long launches_so_far();
 bool sync_check();
 
 #define SPGNB_CHECK_LAUNCH(name)                                        \
@@ -366,8 +368,15 @@ int force_kernels_init(int table_size);
 int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,
                     const spgnb_ltmatrix3* rcells, const float* cutoffs, const float* skins,
                     const spgnb_nl_options* opt, spgnb_nl** out);
+enum BuildHow
+{
+    kBuildSkin = 0,
+    kBuildForced = 1,
+    kBuildInterval = 2
+};
 int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
-                   const int* ex_list, const int* ex_num, bool host_rebuild, cudaStream_t s);
+                   const int* ex_list, const int* ex_num, int how, cudaStream_t s, int* d_step = nullptr,
+                   int interval = 0);
 int nl_regrow(spgnb_nl* nl, int flags);
 int nl_set_prune_rc(spgnb_nl* nl, float rc, cudaStream_t s);
 

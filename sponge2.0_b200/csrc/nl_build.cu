@@ -676,6 +676,21 @@ __global__ void k_finish(int G, int S, const int* __restrict__ cell_sys, const i
     }
 }
 
+// Refresh by a fixed interval of steps (NEIGHBOR_LIST::Update with
+// refresh_interval > 0), counted on the device: every system rebuilds when
+// the step counter, advanced here, reaches a multiple of the interval.
+__global__ void k_interval_need(int S, int interval, int* __restrict__ step, int* __restrict__ need, int* counters)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    const int now = step[0] + 1;
+    const bool due = interval > 0 && now % interval == 0;
+    if (s < S) need[s] = due ? 1 : 0;
+    __syncthreads();
+    if (blockIdx.x == 0 && threadIdx.x == 0) counters[kCntNeed] = due ? 1 : 0;
+}
+
+__global__ void k_step_tick(int* __restrict__ step) { step[0] += 1; }
+
 __global__ void k_set_need(int S, int* __restrict__ need, int* counters)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1096,17 +1111,27 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
 }
 
 // Queues one rebuild, or the device-side decision about one, on stream s.
-// host_rebuild: rebuild unconditionally; otherwise the skin check decides.
+// how: kBuildForced rebuilds every system, kBuildSkin lets each system's
+// skin check decide, kBuildInterval rebuilds all when the device step counter
+// (advanced by this call) reaches a multiple of `interval`.
 int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
-                   const int* ex_list, const int* ex_num, bool host_rebuild, cudaStream_t s)
+                   const int* ex_list, const int* ex_num, int how, cudaStream_t s, int* d_step, int interval)
 {
     const int sms = num_sms();
     const int slots_cap = nl->clusters_cap * kClusterSize;
     const int ccap = nl->clusters_cap;
-    if (host_rebuild)
+    if (how == kBuildForced)
     {
         k_set_need<<<(nl->S + 255) / 256, 256, 0, s>>>(nl->S, nl->d_need, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_set_need");
+    }
+    else if (how == kBuildInterval)
+    {
+        if (nl->S > 1024) return fail(SPGNB_E_UNSUPPORTED, "interval refresh: more than 1024 systems");
+        k_interval_need<<<1, 1024, 0, s>>>(nl->S, interval, d_step, nl->d_need, nl->d_counters);
+        SPGNB_CHECK_LAUNCH("k_interval_need");
+        k_step_tick<<<1, 1, 0, s>>>(d_step);
+        SPGNB_CHECK_LAUNCH("k_step_tick");
     }
     else
     {
@@ -1295,7 +1320,8 @@ int spgnb_nl_update(spgnb_nl* nl, const int* d_atom_local, int local_atom_number
         if (!rebuild) return SPGNB_OK;
     }
     return nl_queue_build(nl, local_atom_numbers, (const float3*)d_crd, d_atom_local, d_excluded_list_start,
-                          d_excluded_list, d_excluded_numbers, host_knows, s);
+                          d_excluded_list, d_excluded_numbers, host_knows ? kBuildForced : kBuildSkin, s, nullptr,
+                          0);
 }
 
 int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out)

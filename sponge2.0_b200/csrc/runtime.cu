@@ -18,6 +18,8 @@ unsigned long long g_launches = 0;
 }  // namespace
 
 void count_launch() { __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAXED); }
+void count_launches(long long n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
+unsigned long long launches_so_far() { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
 // SPGNB_SYNC_CHECK=1: every launch is followed by a device synchronisation so
 // that an execution error is reported against the kernel that caused it.

@@ -28,7 +28,9 @@ EXPORTED = [
     "spgnb_launch_count", "spgnb_debug_set_pair_events", "spgnb_nl_count_pairs", "spgnb_probe_fp32_fma_tflops",
     "spgnb_lj_pme_direct_force_noalloc",
     "spgnb_batch_default_options", "spgnb_batch_create", "spgnb_batch_run", "spgnb_batch_energies",
-    "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_destroy",
+    "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_stream",
+    "spgnb_batch_check_overflow", "spgnb_batch_set_thermostat",
+    "spgnb_batch_destroy",
 ]
 
 
@@ -67,7 +69,8 @@ class BatchSystem(C.Structure):
 
 class BatchOptions(C.Structure):
     _fields_ = [("dt", C.c_float), ("water_doh", C.c_float), ("water_dhh", C.c_float), ("skin_permit", C.c_float),
-                ("prune_buffer", C.c_float), ("steps_per_graph", C.c_int), ("use_graphs", C.c_int)]
+                ("prune_buffer", C.c_float), ("steps_per_graph", C.c_int), ("use_graphs", C.c_int),
+                ("thermostat_tau", C.c_float), ("temperature", C.c_float), ("refresh_interval", C.c_int)]
 
 
 class NLStats(C.Structure):
@@ -114,6 +117,10 @@ def lib():
     L.spgnb_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                     C.POINTER(C.c_int)]
     L.spgnb_batch_autotune.argtypes = [vp, i, C.POINTER(C.c_float)]
+    L.spgnb_batch_check_overflow.argtypes = [vp, C.POINTER(i)]
+    L.spgnb_batch_set_thermostat.argtypes = [vp, f, f]
+    L.spgnb_batch_stream.argtypes = [vp]
+    L.spgnb_batch_stream.restype = vp
     L.spgnb_batch_destroy.argtypes = [vp]
     L.spgnb_lj_create.argtypes = [i, i, vp, vp, vp, f, C.POINTER(vp)]
     L.spgnb_lj_get_local.argtypes = [vp, vp, i, i]

@@ -96,10 +96,24 @@ class Batch:
         check(lib().spgnb_batch_stats(self.handle, C.byref(steps), C.byref(builds), C.byref(prunes), C.byref(ovf)))
         return {"steps": steps.value, "rebuilds": builds.value, "prunings": prunes.value, "overflow": ovf.value}
 
+    def set_thermostat(self, tau, temperature=300.0):
+        check(lib().spgnb_batch_set_thermostat(self.handle, float(tau), float(temperature)))
+
+    def check_overflow(self):
+        """True when buffers overflowed and were regrown (the lists rebuilt)."""
+        r = C.c_int()
+        check(lib().spgnb_batch_check_overflow(self.handle, C.byref(r)))
+        return bool(r.value)
+
     def autotune(self, steps_per_candidate=20):
         best = C.c_float()
         check(lib().spgnb_batch_autotune(self.handle, int(steps_per_candidate), C.byref(best)))
         return best.value
+
+    @property
+    def stream_ptr(self):
+        """The batch's cudaStream_t as an integer (torch.cuda.ExternalStream)."""
+        return lib().spgnb_batch_stream(self.handle)
 
     def close(self):
         if getattr(self, "handle", None):
