@@ -48,10 +48,15 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     p.add_argument("--profile", action="store_true",
                    help="profiling run for ncu: warm-up and --steps plain steps, no L2 flush, no e2e, no baseline")
-    p.add_argument("--workload", choices=["mixed96k", "batched"], default="mixed96k",
+    p.add_argument("--workload", choices=["mixed96k", "batched", "served"], default="mixed96k",
                    help="mixed96k: the plain path on the 96k box (default); batched: 256 systems, batched engine "
-                        "against the plain per-system path")
+                        "against the plain per-system path; served: Poisson stream of MD segments into a pool")
     p.add_argument("--systems", type=int, default=256, help="batched: number of systems")
+    p.add_argument("--serve-seconds", type=float, default=60.0, help="served: length of the request stream")
+    p.add_argument("--rate", type=float, default=40.0, help="served: mean arrivals per second")
+    p.add_argument("--max-resident-atoms", type=int, default=2_500_000,
+                   help="served: atoms on the device at once (0 = as many as the HBM budget holds)")
+    p.add_argument("--hbm-budget-gb", type=float, default=120.0, help="served: device memory of the pool")
     return p.parse_args()
 
 
@@ -156,19 +161,6 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def shard_systems(systems, world, rank):
-    """Greedy bin packing of independent systems over ranks by estimated pair
-    work (atoms x cutoff^3), largest first; rank r takes bin r."""
-    order = sorted(range(len(systems)), key=lambda k: -systems[k].n * systems[k].cutoff ** 3)
-    loads = [0.0] * world
-    bins = [[] for _ in range(world)]
-    for k in order:
-        r = min(range(world), key=lambda q: loads[q])
-        bins[r].append(k)
-        loads[r] += systems[k].n * systems[k].cutoff ** 3
-    return sorted(bins[rank])
-
-
 def run_batched(args, world, rank, local):
     """Config 3: independent systems (log-uniform 1,500-24,000 atoms, 0-15 %
     solute, rc from {8, 10, 12}, skin 2) stepped by the batched engine
@@ -179,6 +171,7 @@ def run_batched(args, world, rank, local):
     from spgnb import systems as S
     from spgnb._lib import lib
     from spgnb.batch import Batch
+    from spgnb.shard import shard_systems
     dist = None
     if world > 1:
         import datetime
@@ -205,7 +198,8 @@ def run_batched(args, world, rank, local):
     opts = dict(refresh_interval=REFRESH_INTERVAL, thermostat_tau=0.1, temperature=300.0)
     # the synthetic boxes start strained: relax them with a strongly coupled
     # thermostat first (not timed), then production coupling
-    B = Batch(mine, **dict(opts, thermostat_tau=0.002))
+    # lists sized for a 1.6 A prune buffer: the autotuner tries buffers up to it
+    B = Batch(mine, **dict(opts, thermostat_tau=0.002, prune_buffer=1.6))
     B.run(200)
     B.check_overflow()
     B.set_thermostat(0.1, 300.0)
@@ -213,6 +207,19 @@ def run_batched(args, world, rank, local):
     B.run(W * B.options.steps_per_graph)
     B.check_overflow()
     torch.cuda.synchronize()
+    if args.profile:
+        # kernels of K steps inside the NVTX range "timed" (ncu --nvtx --nvtx-include timed/)
+        torch.cuda.nvtx.range_push("timed")
+        B.run(K, 100)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "workload": "batched", "steps": K,
+                              "atoms": sum(s.n for s in mine)}), flush=True)
+        B.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     sampler = ClockSampler(local)
     sampler.start()
     if dist is not None:
@@ -233,7 +240,7 @@ def run_batched(args, world, rank, local):
         crd, vel, _ = B.download(k)
         s2 = copy.copy(s)
         s2.crd, s2.vel = crd, vel
-        b = Batch([s2], use_graphs=0, **opts)
+        b = Batch([s2], use_graphs=0, **dict(opts, prune_buffer=tuned))
         b.run(W)
         plain_ms += timed(b, k_plain)
         plain_as += s.n * k_plain
@@ -277,11 +284,109 @@ def run_batched(args, world, rank, local):
         dist.destroy_process_group()
 
 
+def run_served(args, world, rank, local):
+    """Config 4: Poisson arrivals (40/s) of MD segments, each a system made as
+    in the batched workload with 1,000-50,000 atoms and 500-5,000 steps,
+    admitted into a pool under the HBM budget as room frees up (continuous
+    batching), state resident on the device.  Ranks serve independent
+    streams (no collective in the data path)."""
+    import torch
+    from spgnb import systems as S
+    from spgnb._lib import lib
+    from spgnb.batch import Pool, pool_options
+    from spgnb.serve import Server
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    L = lib()
+    reqs = S.request_stream(duration_s=args.serve_seconds, rate_per_s=args.rate, seed=5 + 1000 * rank)
+    warm = S.request_stream(duration_s=1.0, rate_per_s=8.0, seed=99 + rank, steps_min=40, steps_max=60)
+    template = S.request_system(reqs[0])
+    pool = Pool(template, pool_options(max_systems=1024, hbm_budget_bytes=args.hbm_budget_gb * 1e9),
+                steps_per_graph=10, thermostat_tau=0.1, temperature=300.0)
+    cap = pool.capacity()
+    # warm-up: graph capture and first launches on a few short segments (not timed)
+    Server(pool, S.request_system, chunk_steps=10).run([type(r)(r.rid, 0.0, r.n_atoms, r.steps, r.seed)
+                                                       for r in warm[:max(3, args.warmup)]])
+    torch.cuda.synchronize()
+    st = torch.cuda.ExternalStream(pool.stream_ptr)
+    sampler = ClockSampler(local)
+    sampler.start()
+    if dist is not None:
+        dist.barrier()
+    launches0 = L.spgnb_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    srv = Server(pool, S.request_system, chunk_steps=10, max_resident_atoms=args.max_resident_atoms)
+    rep = srv.run(reqs, duration_s=args.serve_seconds, drain=False)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    launches = L.spgnb_launch_count() - launches0
+    clocks = sampler.stop()
+    pst = pool.stats()
+    lat = [x.latency_s for x in srv.finished]
+    que = [x.queueing_s for x in srv.finished]
+    admitted = [x for x in srv.finished] + list(srv.resident.values())
+    h2d = sum(x.request.n_atoms * 40 for x in admitted)   # crd vel (12+12) charge mass type (12) exclusions (~4)
+    d2h = sum(x.request.n_atoms * 36 + 72 for x in srv.finished)
+    steps_chunks = max(1, srv.chunks * 10)
+    from spgnb.shard import gather, merge_served
+    mine = {"latencies_s": lat, "queueing_s": que, "finished": rep["finished"], "atom_steps": rep["atom_steps"],
+            "elapsed_s": rep["elapsed_s"], "device_ms": ms}
+    ranks = gather(mine, dist)
+    merged = merge_served(ranks)
+    ms = max(r["device_ms"] for r in ranks)
+    wall, atom_steps = merged["elapsed_s"], float(merged["atom_steps"])
+    if rank == 0:
+        value = atom_steps / (ms * 1e-3)
+        offered = world * sum(r.n_atoms * r.steps for r in reqs) / args.serve_seconds
+        line = {"metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world,
+                "steps": steps_chunks, "warmup": max(3, args.warmup), "ms_per_step": ms / steps_chunks,
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+                "data": "synthetic",
+                "config": {"workload": f"served: Poisson {args.rate}/s for {args.serve_seconds:.0f} s, segments of "
+                                       "1000-50000 atoms (log-uniform) x 500-5000 steps, systems as in the batched "
+                                       "workload, leap-frog + SETTLE, 2 fs, Berendsen 300 K (tau 0.1 ps), "
+                                       "skin-triggered lists",
+                           "hbm_budget_gb": args.hbm_budget_gb, "pool_atoms": cap["max_atoms"],
+                           "pool_device_gb": cap["device_bytes"] / 1e9, "max_resident_atoms": args.max_resident_atoms,
+                           "chunk_steps": 10, "l2": "inputs larger than L2",
+                           "parallelism": f"independent streams on {world} GPUs" if world > 1 else "single GPU"},
+                "served": {"arrivals_per_gpu": len(reqs), "finished": merged["finished"], "rejected": rep["rejected"],
+                           "resident_at_end": rep["resident_at_end"], "queued_at_end": rep["queued_at_end"],
+                           "latency_p50_s": merged["latency_p50_s"], "latency_p99_s": merged["latency_p99_s"],
+                           "queueing_p50_s": merged["queueing_p50_s"], "queueing_p99_s": merged["queueing_p99_s"],
+                           "max_resident_segments": rep["max_resident_segments"],
+                           "max_resident_atoms": rep["max_resident_atoms"],
+                           "offered_atom_steps_per_s": offered, "wall_s": wall,
+                           "wall_atom_steps_per_s": atom_steps / wall,
+                           "rebuilds": pst["rebuilds"], "prunings": pst["prunings"], "overflow": pst["overflow"],
+                           "host_s": srv.host_times()},
+                "clocks": clocks, "gpu_launches": int(launches),
+                "e2e": {"value": atom_steps / wall, "unit": "atom-steps/s",
+                        "h2d_bytes_per_step": h2d / steps_chunks, "d2h_bytes_per_step": d2h / steps_chunks,
+                        "note": "host clock over the serving loop: uploads of admitted systems, downloads of results"}}
+        print(json.dumps(line), flush=True)
+    pool.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup()
     if args.workload == "batched" and args.impl != "reference":
         run_batched(args, world, rank, local)
+        return
+    if args.workload == "served" and args.impl != "reference":
+        run_served(args, world, rank, local)
         return
     if args.impl == "reference":
         # the reference arm is the reference's CPU path: rank 0 alone, no GPU work

@@ -356,7 +356,7 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
  * and virials are evaluated on steps whose count is a multiple of it (the
  * last ones are kept).  Returns without synchronising. */
 int spgnb_batch_run(spgnb_batch* b, int steps, int energy_interval);
-/* Per system, 9 doubles: LJ short-range, LJ long-range correction, PME
+/* Per system id, 9 doubles: LJ short-range, LJ long-range correction, PME
  * direct-space Coulomb (kcal/mol), virial a11 a21 a22 a31 a32 a33 of the
  * last energy evaluation.  Synchronises. */
 int spgnb_batch_energies(spgnb_batch* b, double* out);
@@ -376,6 +376,45 @@ int spgnb_batch_autotune(spgnb_batch* b, int steps_per_candidate, float* chosen_
 /* The batch's CUDA stream (a cudaStream_t), for events around its work. */
 void* spgnb_batch_stream(spgnb_batch* b);
 int spgnb_batch_destroy(spgnb_batch* b);
+
+/* ------------------------------------------------------ POOL (serving) */
+/* A batch created empty with fixed capacities, into which systems are
+ * admitted and from which they are retired while the others keep running
+ * (continuous batching).  Every system owns ranges of the pool's arrays, so
+ * admitting or retiring one changes nothing for the others: a system's
+ * trajectory is bitwise the same alone and in any mix.  A system admitted
+ * with a step count stops (its state frozen) after that many steps. */
+typedef struct
+{
+    int max_systems;            /* system ids [0, max_systems) */
+    int max_atoms;              /* 0: as many as hbm_budget_bytes allows */
+    long long max_excluded;     /* exclusion entries; 0: 2 per atom */
+    int max_waters;             /* 0: max_atoms / 3 */
+    float max_cutoff;           /* largest cutoff admitted (list sizes), 12 */
+    float min_cutoff;           /* smallest (cells per atom), 8 */
+    float skin;                 /* 2 */
+    float density;              /* atoms per A^3 of the systems admitted, 0.1003 */
+    double hbm_budget_bytes;    /* device memory for the pool when max_atoms is 0 */
+} spgnb_batch_pool_options;
+
+void spgnb_batch_pool_default_options(spgnb_batch_pool_options* opt);
+int spgnb_batch_create_pool(const spgnb_batch_pool_options* pool, int atom_type_numbers, const float* h_pair_A,
+                            const float* h_pair_B, const spgnb_batch_options* opt, spgnb_batch** out);
+/* Copies a system in (stream-ordered after the work already queued) and
+ * gives it an id; `steps` > 0 = the system stops after that many steps, 0 =
+ * runs until retired.  Its lists, forces and energies at step 0 are made
+ * before the next run.  SPGNB_E_OOM: no room now (nothing changed). */
+int spgnb_batch_admit(spgnb_batch* b, const spgnb_batch_system* sys, int steps, int* id);
+/* Returns a system's ranges to the pool (its results must have been read). */
+int spgnb_batch_retire(spgnb_batch* b, int id);
+/* Evaluates forces, energies and virial now for the listed systems only. */
+int spgnb_batch_evaluate(spgnb_batch* b, const int* ids, int n);
+/* Per system id (max_systems entries, NULL to skip): steps done and steps
+ * left (-1 = unlimited; a retired id reads 0 and 0).  Synchronises. */
+int spgnb_batch_progress(spgnb_batch* b, int* steps_done, int* steps_left);
+/* Capacity: system ids, atoms in the pool and free now, device bytes held. */
+int spgnb_batch_capacity(spgnb_batch* b, int* max_systems, long long* max_atoms, long long* free_atoms,
+                         double* device_bytes);
 
 /* ------------------------------------------------------------ diagnostics */
 /* Kernel launches issued by the library so far (all threads). */

@@ -24,15 +24,29 @@
 // (AKMA), in which F/m is an acceleration in A per unit^2
 static constexpr float kTimeUnitsPerPs = 20.455f;
 
+struct SysRec
+{
+    bool live = false;
+    int atom_begin = 0, atom_count = 0;
+    long long ex_begin = 0, ex_count = 0;
+    int w_begin = 0, w_count = 0;
+    double lr_factor = 0, volume = 0;
+};
+
+// A pool of systems: fixed capacities, every system in ranges of its own.
 struct spgnb_batch
 {
-    int S = 0;
-    int n = 0;
-    int n_waters = 0;
+    int S = 0;          // system ids
+    int n = 0;          // atom capacity
+    long long ex_cap = 0;
+    int w_cap = 0;
+    RangePool atom_pool, ex_pool, water_pool;
+    std::vector<SysRec> rec;
+    std::vector<float> h_pair_A, h_pair_B;  // the type table, reference layout
     spgnb_batch_options opt{};
     spgnb_nl* nl = nullptr;
     cudaStream_t stream = nullptr;
-    // per atom
+    // per atom (parked atoms: zero velocity and inverse mass)
     float3* d_crd = nullptr;
     float3* d_vel = nullptr;
     float3* d_frc = nullptr;
@@ -40,32 +54,34 @@ struct spgnb_batch
     float* d_charge = nullptr;
     float* d_inv_mass = nullptr;
     int* d_type = nullptr;
-    int* d_atom_local = nullptr;
+    int* d_atom_local = nullptr;  // the atom's own index (exclusions hold pool indices)
     int* d_ex_start = nullptr;
     int* d_ex_num = nullptr;
     int* d_ex_list = nullptr;
-    int* d_waters = nullptr;  // oxygen of each rigid water
+    int* d_waters = nullptr;  // oxygen of each rigid water, -1 for a free entry
     // force field
     int T = 0;
     float2* d_table = nullptr;
-    spgnb::ForceParams* d_fps = nullptr;
+    spgnb::ForceParams* d_fps = nullptr;  // S + 1
     std::vector<spgnb::ForceParams> h_fps;
-    bool fit = true;
-    long long* d_totals = nullptr;  // 8 per system
-    int* d_atom_sys = nullptr;      // system of each atom (thermostat)
-    double* d_kin = nullptr;        // per system: sum of m v^2
-    int* d_step = nullptr;          // steps done, on the device (interval refresh)
-    float* d_ndof = nullptr;        // per system: degrees of freedom
+    bool fit = true;                  // the rational fits (every admitted system inside their range)
+    long long* d_totals = nullptr;    // 8 per system id
+    long long* d_kin = nullptr;       // per system: sum of m v^2, fixed point
+    float* d_ndof = nullptr;          // per system: degrees of freedom
+    int* d_steps = nullptr;           // per system: steps done
+    int* d_left = nullptr;            // per system: steps left (-1 unlimited, 0 stopped or parked)
+    int* d_flags = nullptr;           // per system: evaluate now
+    std::vector<int> h_flags;
     float4* d_slot_pos = nullptr;
     int* d_slot_type = nullptr;
-    // per system, host
-    std::vector<int> atom_begin, atom_count;
-    std::vector<double> lr_factor, volume;
     // stepping
+    bool have_water = false;
     float ra = 0, rb = 0, rc = 0, mO = 0, mH = 0;
     cudaGraphExec_t g_plain = nullptr, g_energy = nullptr;
     long long kernels_plain = 0, kernels_energy = 0;  // kernel launches inside each graph
+    bool graph_tri = false;
     long long steps_done = 0;
+    bool pending = false;  // admitted systems wait for their first lists and forces
 };
 
 namespace spgnb
@@ -73,11 +89,12 @@ namespace spgnb
 namespace
 {
 
-__global__ void k_leapfrog(int n, float3* __restrict__ crd, float3* __restrict__ vel, const float3* __restrict__ frc,
+__global__ void k_leapfrog(int n, const int* __restrict__ atom_sys, const int* __restrict__ left,
+                           float3* __restrict__ crd, float3* __restrict__ vel, const float3* __restrict__ frc,
                            const float* __restrict__ inv_mass, float3* __restrict__ crd_old, float dt)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+    if (i >= n || left[atom_sys[i]] == 0) return;  // parked, or its steps are done
     const float3 x = crd[i];
     const float3 f = frc[i];
     const float im = inv_mass[i] * dt;
@@ -105,13 +122,15 @@ __device__ __forceinline__ float3 unit3(float3 a) { return mul3(a, rsqrtf(dot3(a
 // triangle in its own frame has O at (0, ra, 0) and the hydrogens at
 // (-+rc, -rb, 0); the new plane orientation comes from rotations about the
 // frame axes solved in closed form.  Velocities follow from the displacement.
-__global__ void k_settle(int n_waters, const int* __restrict__ waters, float3* __restrict__ crd,
-                         float3* __restrict__ vel, const float3* __restrict__ crd_old, float mO, float mH, float ra,
-                         float rb, float rc, float inv_dt)
+__global__ void k_settle(int n_waters, const int* __restrict__ waters, const int* __restrict__ atom_sys,
+                         const int* __restrict__ left, float3* __restrict__ crd, float3* __restrict__ vel,
+                         const float3* __restrict__ crd_old, float mO, float mH, float ra, float rb, float rc,
+                         float inv_dt)
 {
     const int w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= n_waters) return;
     const int o = waters[w];
+    if (o < 0 || left[atom_sys[o]] == 0) return;
     const float3 origin = crd_old[o];
     // everything relative to the old oxygen, for precision
     const float3 b0 = sub3(crd_old[o + 1], origin), c0 = sub3(crd_old[o + 2], origin);
@@ -157,34 +176,89 @@ __global__ void k_settle(int n_waters, const int* __restrict__ waters, float3* _
     vel[o + 2] = mul3(sub3(c3, c0), inv_dt);
 }
 
-// Berendsen weak coupling per system: twice the kinetic energy, then every
-// velocity scaled by sqrt(1 + dt/tau (T0/T - 1)) (clamped to [0.8, 1.25]).
+// Berendsen weak coupling per system: twice the kinetic energy (summed in
+// fixed point, so the same in any order), then every velocity scaled by
+// sqrt(1 + dt/tau (T0/T - 1)) (clamped to [0.8, 1.25]).
 __global__ void k_kinetic(int n, const float3* __restrict__ vel, const float* __restrict__ inv_mass,
-                          const int* __restrict__ atom_sys, double* __restrict__ kin)
+                          const int* __restrict__ atom_sys, const int* __restrict__ left, long long* __restrict__ kin)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || inv_mass[i] == 0.0f) return;
-    const float3 v = vel[i];
-    atomicAdd(&kin[atom_sys[i]], (double)((v.x * v.x + v.y * v.y + v.z * v.z) / inv_mass[i]));
+    int s = -1;
+    long long q = 0;
+    if (i < n && inv_mass[i] != 0.0f)
+    {
+        s = atom_sys[i];
+        if (left[s] == 0)
+            s = -1;
+        else
+        {
+            const float3 v = vel[i];
+            const double mv2 = (double)((v.x * v.x + v.y * v.y + v.z * v.z) / inv_mass[i]);
+            q = __double2ll_rn(mv2 * kEnergyScale);
+        }
+    }
+    // a warp's atoms nearly always belong to one system (atoms are
+    // contiguous per system): one atomic per warp then, per lane otherwise
+    const unsigned valid = __ballot_sync(0xffffffffu, s >= 0);
+    if (!valid) return;
+    const int s0 = __shfl_sync(0xffffffffu, s, __ffs(valid) - 1);
+    if (__all_sync(0xffffffffu, s < 0 || s == s0))
+    {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+        if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long*)&kin[s0], (unsigned long long)q);
+    }
+    else if (s >= 0)
+        atomicAdd((unsigned long long*)&kin[s], (unsigned long long)q);
 }
 
 __global__ void k_rescale(int n, float3* __restrict__ vel, const int* __restrict__ atom_sys,
-                          const double* __restrict__ kin, const float* __restrict__ ndof, float kT0, float coupling)
+                          const int* __restrict__ left, const long long* __restrict__ kin,
+                          const float* __restrict__ ndof, float kT0, float coupling)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const int s = atom_sys[i];
-    const double kT = kin[s] / fmax((double)ndof[s], 1.0);  // k_B T = 2 E_kin / dof
+    if (left[s] == 0) return;
+    const double kT = (double)kin[s] / kEnergyScale / fmax((double)ndof[s], 1.0);  // k_B T = 2 E_kin / dof
     const float lam2 = kT > 0.0 ? 1.0f + coupling * (float)(kT0 / kT - 1.0) : 1.0f;
     const float lam = sqrtf(fminf(fmaxf(lam2, 0.64f), 1.5625f));
     float3 v = vel[i];
     vel[i] = make_float3(v.x * lam, v.y * lam, v.z * lam);
 }
 
-int batch_force(spgnb_batch* b, int mode, cudaStream_t s)
+// End of a step: per live system, one more step done, one fewer left.
+__global__ void k_tick(int S, const int* __restrict__ live, int* __restrict__ left, int* __restrict__ steps)
 {
-    SPGNB_CUDA(cudaMemsetAsync(b->d_frc, 0, sizeof(float3) * b->n, s));
-    if (mode) SPGNB_CUDA(cudaMemsetAsync(b->d_totals, 0, sizeof(long long) * 8 * b->S, s));
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S || !live[s] || left[s] == 0) return;
+    steps[s] += 1;
+    if (left[s] > 0) left[s] -= 1;
+}
+
+// Zero the forces of the flagged systems' atoms and their totals.
+__global__ void k_clear_flagged(int n, const int* __restrict__ atom_sys, const int* __restrict__ flags,
+                                float3* __restrict__ frc, int S, long long* __restrict__ totals)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && flags[atom_sys[i]]) frc[i] = make_float3(0.0f, 0.0f, 0.0f);
+    if (totals && i < 8 * S && flags[i >> 3]) totals[i] = 0;
+}
+
+int batch_force(spgnb_batch* b, int mode, cudaStream_t s, const int* only = nullptr)
+{
+    if (!only)
+    {
+        SPGNB_CUDA(cudaMemsetAsync(b->d_frc, 0, sizeof(float3) * b->n, s));
+        if (mode) SPGNB_CUDA(cudaMemsetAsync(b->d_totals, 0, sizeof(long long) * 8 * b->S, s));
+    }
+    else
+    {
+        const int m = std::max(b->n, 8 * b->S);
+        k_clear_flagged<<<(m + 255) / 256, 256, 0, s>>>(b->n, b->nl->d_atom_sys, only, b->d_frc, b->S,
+                                                         mode ? b->d_totals : nullptr);
+        SPGNB_CHECK_LAUNCH("k_clear_flagged");
+    }
     ForceInputs in;
     in.nl = b->nl;
     in.crd = b->d_crd;
@@ -193,7 +267,7 @@ int batch_force(spgnb_batch* b, int mode, cudaStream_t s)
     in.slot_pos = b->d_slot_pos;
     in.slot_type = b->d_slot_type;
     in.p0 = b->h_fps[0];
-    in.d_fps = b->S > 1 ? b->d_fps : nullptr;
+    in.d_fps = b->d_fps;
     in.fit = b->fit;
     in.table = b->d_table;
     in.table_size = b->T * b->T;
@@ -201,38 +275,60 @@ int batch_force(spgnb_batch* b, int mode, cudaStream_t s)
     in.totals = b->d_totals;
     in.mode = mode;
     in.om.solvent_start = b->n;
+    in.only = only;
     return force_pipeline(in, s);
 }
 
-// One step: kick-drift, SETTLE, list update, forces.
+// One step: kick-drift, SETTLE, thermostat, list update, forces, counters.
 int batch_step(spgnb_batch* b, bool energy, cudaStream_t s)
 {
     const float dt = b->opt.dt * kTimeUnitsPerPs;
-    k_leapfrog<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_crd, b->d_vel, b->d_frc, b->d_inv_mass, b->d_crd_old,
-                                                   dt);
+    const int* atom_sys = b->nl->d_atom_sys;
+    k_leapfrog<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, atom_sys, b->d_left, b->d_crd, b->d_vel, b->d_frc,
+                                                   b->d_inv_mass, b->d_crd_old, dt);
     SPGNB_CHECK_LAUNCH("k_leapfrog");
-    if (b->n_waters > 0)
+    if (b->have_water)
     {
-        k_settle<<<(b->n_waters + 127) / 128, 128, 0, s>>>(b->n_waters, b->d_waters, b->d_crd, b->d_vel,
-                                                            b->d_crd_old, b->mO, b->mH, b->ra, b->rb, b->rc,
-                                                            1.0f / dt);
+        k_settle<<<(b->w_cap + 127) / 128, 128, 0, s>>>(b->w_cap, b->d_waters, atom_sys, b->d_left, b->d_crd,
+                                                         b->d_vel, b->d_crd_old, b->mO, b->mH, b->ra, b->rb, b->rc,
+                                                         1.0f / dt);
         SPGNB_CHECK_LAUNCH("k_settle");
     }
     if (b->opt.thermostat_tau > 0.0f)
     {
-        SPGNB_CUDA(cudaMemsetAsync(b->d_kin, 0, sizeof(double) * b->S, s));
-        k_kinetic<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_vel, b->d_inv_mass, b->d_atom_sys, b->d_kin);
+        SPGNB_CUDA(cudaMemsetAsync(b->d_kin, 0, sizeof(long long) * b->S, s));
+        k_kinetic<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_vel, b->d_inv_mass, atom_sys, b->d_left, b->d_kin);
         SPGNB_CHECK_LAUNCH("k_kinetic");
         const float kT0 = 0.00198716f * b->opt.temperature;  // kcal/mol
-        k_rescale<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_vel, b->d_atom_sys, b->d_kin, b->d_ndof, kT0,
+        k_rescale<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_vel, atom_sys, b->d_left, b->d_kin, b->d_ndof, kT0,
                                                       b->opt.dt / b->opt.thermostat_tau);
         SPGNB_CHECK_LAUNCH("k_rescale");
     }
     int st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num,
-                            b->opt.refresh_interval > 0 ? kBuildInterval : kBuildSkin, s, b->d_step,
-                            b->opt.refresh_interval);
+                            b->opt.refresh_interval > 0 ? kBuildInterval : kBuildSkin, s, b->d_steps,
+                            b->opt.refresh_interval, b->d_left);
     if (st) return st;
-    return batch_force(b, energy ? 1 : 0, s);
+    if ((st = batch_force(b, energy ? 1 : 0, s))) return st;
+    k_tick<<<(b->S + 255) / 256, 256, 0, s>>>(b->S, b->nl->d_live, b->d_left, b->d_steps);
+    SPGNB_CHECK_LAUNCH("k_tick");
+    return SPGNB_OK;
+}
+
+// Lists and forces (with energies) of the systems admitted since the last
+// run; the other systems' state is untouched.
+int settle_pending(spgnb_batch* b)
+{
+    if (!b->pending) return SPGNB_OK;
+    cudaStream_t s = b->stream;
+    SPGNB_CUDA(cudaMemcpyAsync(b->d_flags, b->h_flags.data(), sizeof(int) * b->S, cudaMemcpyHostToDevice, s));
+    int st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num,
+                            kBuildPreset, s, b->d_flags);
+    if (!st) st = batch_force(b, 1, s, b->d_flags);
+    if (st) return st;
+    SPGNB_CUDA(cudaMemsetAsync(b->d_flags, 0, sizeof(int) * b->S, s));
+    std::fill(b->h_flags.begin(), b->h_flags.end(), 0);
+    b->pending = false;
+    return SPGNB_OK;
 }
 
 void free_graphs(spgnb_batch* b)
@@ -268,8 +364,10 @@ int capture(spgnb_batch* b, bool energy_last, cudaGraphExec_t* out, long long* k
 
 int ensure_graphs(spgnb_batch* b)
 {
-    if (!b->opt.use_graphs || (b->g_plain && b->g_energy)) return SPGNB_OK;
+    if (!b->opt.use_graphs) return SPGNB_OK;
+    if (b->g_plain && b->g_energy && b->graph_tri == b->nl->triclinic) return SPGNB_OK;
     free_graphs(b);
+    b->graph_tri = b->nl->triclinic;
     int st = capture(b, false, &b->g_plain, &b->kernels_plain);
     if (!st) st = capture(b, true, &b->g_energy, &b->kernels_energy);
     return st;
@@ -295,10 +393,11 @@ void free_batch(spgnb_batch* b)
     dfree(b->d_table);
     dfree(b->d_fps);
     dfree(b->d_totals);
-    dfree(b->d_atom_sys);
     dfree(b->d_kin);
     dfree(b->d_ndof);
-    dfree(b->d_step);
+    dfree(b->d_steps);
+    dfree(b->d_left);
+    dfree(b->d_flags);
     dfree(b->d_slot_pos);
     dfree(b->d_slot_type);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -306,12 +405,288 @@ void free_batch(spgnb_batch* b)
 }
 
 template <typename T>
-int upload(T** d, const std::vector<T>& h)
+int zalloc(T** d, size_t count)
 {
-    int st = dalloc(d, h.size());
+    int st = dalloc(d, count);
     if (st) return st;
-    if (!h.empty()) SPGNB_CUDA(cudaMemcpy(*d, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice));
+    SPGNB_CUDA(cudaMemset(*d, 0, sizeof(T) * std::max<size_t>(count, 1)));
     return SPGNB_OK;
+}
+
+template <typename T>
+int put(T* d, size_t offset, const std::vector<T>& h, cudaStream_t s)
+{
+    if (h.empty()) return SPGNB_OK;
+    SPGNB_CUDA(cudaMemcpyAsync(d + offset, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
+    return SPGNB_OK;
+}
+
+// One system checked and laid out on the host, indices local to it.
+struct Staged
+{
+    int N = 0;
+    std::vector<float3> crd, vel;
+    std::vector<float> charge, inv_mass;
+    std::vector<int> type, ex_start, ex_num, ex_list;
+    int water_begin = 0, water_numbers = 0;
+    float mO = 0, mH = 0;
+    ForceParams fp{};
+    double lr_factor = 0, volume = 0;
+    float ndof = 1;
+    SysHost sh;
+    std::vector<int> run_start;
+    std::vector<int2> runs;
+};
+
+int stage(const spgnb_batch_system& y, int T, const std::vector<float>& pair_A, const std::vector<float>& pair_B,
+          int index, Staged& z)
+{
+    if (y.atom_numbers <= 0 || !y.h_crd || !y.h_charge || !y.h_mass || !y.h_atom_type || !y.h_excluded_start ||
+        !y.h_excluded_numbers || (y.excluded_total > 0 && !y.h_excluded_list) || y.water_begin < 0 ||
+        y.water_numbers < 0 || y.water_begin + 3LL * y.water_numbers > y.atom_numbers || y.excluded_total < 0)
+        return fail(SPGNB_E_ARG, "batch: system %d is incomplete", index);
+    const int N = y.atom_numbers;
+    z.N = N;
+    z.crd.resize(N);
+    z.vel.resize(N);
+    z.charge.resize(N);
+    z.inv_mass.resize(N);
+    z.type.resize(N);
+    z.ex_start.resize(N);
+    z.ex_num.resize(N);
+    std::vector<double> hist(T, 0.0);
+    int moving = 0;
+    for (int i = 0; i < N; i++)
+    {
+        z.crd[i] = make_float3(y.h_crd[3 * i], y.h_crd[3 * i + 1], y.h_crd[3 * i + 2]);
+        z.vel[i] = y.h_vel ? make_float3(y.h_vel[3 * i], y.h_vel[3 * i + 1], y.h_vel[3 * i + 2]) : make_float3(0, 0, 0);
+        z.charge[i] = y.h_charge[i];
+        z.inv_mass[i] = y.h_mass[i] > 0.0f ? 1.0f / y.h_mass[i] : 0.0f;
+        moving += y.h_mass[i] > 0.0f;
+        const int t = y.h_atom_type[i];
+        if (t < 0 || t >= T) return fail(SPGNB_E_ARG, "batch: system %d atom %d has type %d outside [0,%d)", index, i, t, T);
+        z.type[i] = t;
+        hist[t] += 1.0;
+        const int cnt = y.h_excluded_numbers[i], st0 = y.h_excluded_start[i];
+        if (cnt < 0 || (cnt > 0 && (st0 < 0 || st0 + cnt > y.excluded_total)))
+            return fail(SPGNB_E_ARG, "batch: system %d atom %d has a bad exclusion range", index, i);
+        z.ex_num[i] = cnt;
+        z.ex_start[i] = (int)z.ex_list.size();
+        for (int k = 0; k < cnt; k++)
+        {
+            const int j = y.h_excluded_list[st0 + k];
+            if (j < 0 || j >= N) return fail(SPGNB_E_ARG, "batch: system %d excludes atom %d outside it", index, j);
+            z.ex_list.push_back(j);
+        }
+    }
+    z.water_begin = y.water_begin;
+    z.water_numbers = y.water_numbers;
+    if (y.water_numbers > 0)
+    {
+        z.mO = y.h_mass[y.water_begin];
+        z.mH = y.h_mass[y.water_begin + 1];
+    }
+    z.ndof = (float)std::max(1, 3 * moving - 3 * y.water_numbers - 3);
+    ForceParams& f = z.fp;
+    f.rc2 = y.cutoff * y.cutoff;
+    f.beta = y.pme_beta;
+    f.beta3 = y.pme_beta * y.pme_beta * y.pme_beta;
+    f.w_scale = y.pme_beta * y.pme_beta * SPGNB_EWALD_INV_W_MAX;
+    const float zz = y.pme_beta * y.cutoff;
+    f.use_fit = (zz * zz <= SPGNB_EWALD_W_MAX * 0.999f) ? 1 : 0;
+    f.n_types = T;
+    f.table_begin = 0;
+    f.pad = 0;
+    // Total_C6_Get and the factor of Lennard_Jones_force.cpp:263-268
+    double c6 = 0.0;
+    for (int p = 0; p < T; p++)
+        for (int q = 0; q < T; q++)
+        {
+            const int hi = p > q ? p : q, lo = p > q ? q : p;
+            c6 += hist[p] * hist[q] * (double)pair_B[hi * (hi + 1) / 2 + lo];
+        }
+    float fac = (float)c6;
+    fac *= -2.0f / 3.0f * 3.1415926535897932f / y.cutoff / y.cutoff / y.cutoff / 6.0f;
+    z.lr_factor = fac;
+    z.volume = (double)y.cell.a11 * y.cell.a22 * y.cell.a33;
+    int st = nl_init_system(z.sh, N, y.cell, y.rcell, y.cutoff, y.skin, index);
+    if (st) return st;
+    return nl_system_runs(z.sh, z.run_start, z.runs);
+}
+
+// Device arrays for the capacities; every range free.
+int create_common(spgnb_batch* b, const NLPoolSpec& spec, long long ex_cap, int w_cap, int T, const float* pair_A,
+                  const float* pair_B)
+{
+    int st;
+    b->S = spec.systems;
+    b->n = spec.atoms;
+    b->ex_cap = std::max(1LL, ex_cap);
+    b->w_cap = std::max(1, w_cap);
+    b->T = T;
+    b->atom_pool.reset(b->n);
+    b->ex_pool.reset(b->ex_cap);
+    b->water_pool.reset(b->w_cap);
+    b->rec.assign(b->S, SysRec{});
+    b->h_flags.assign(b->S, 0);
+    b->h_fps.assign(b->S + 1, ForceParams{});
+    std::vector<float2> table((size_t)T * T);
+    for (int p = 0; p < T; p++)
+        for (int q = 0; q < T; q++)
+        {
+            const int hi = p > q ? p : q, lo = p > q ? q : p;
+            table[(size_t)p * T + q] = make_float2(pair_A[hi * (hi + 1) / 2 + lo], pair_B[hi * (hi + 1) / 2 + lo]);
+        }
+    spgnb_nl_options nlo;
+    spgnb_nl_default_options(&nlo);
+    nlo.refresh_interval = 0;
+    nlo.skin_permit = b->opt.skin_permit;
+    nlo.export_atom_groups = 0;
+    nlo.prune_buffer = b->opt.prune_buffer;
+    const size_t n = b->n, S1 = b->S + 1;
+    if ((st = nl_create_pool(spec, &nlo, &b->nl)) || (st = zalloc(&b->d_crd, n)) || (st = zalloc(&b->d_vel, n)) ||
+        (st = zalloc(&b->d_frc, n)) || (st = zalloc(&b->d_crd_old, n)) || (st = zalloc(&b->d_charge, n)) ||
+        (st = zalloc(&b->d_inv_mass, n)) || (st = zalloc(&b->d_type, n)) || (st = zalloc(&b->d_atom_local, n)) ||
+        (st = zalloc(&b->d_ex_start, n)) || (st = zalloc(&b->d_ex_num, n)) ||
+        (st = zalloc(&b->d_ex_list, (size_t)b->ex_cap)) || (st = dalloc(&b->d_waters, (size_t)b->w_cap)) ||
+        (st = dalloc(&b->d_table, table.size())) || (st = zalloc(&b->d_fps, S1)) ||
+        (st = zalloc(&b->d_totals, 8 * S1)) || (st = zalloc(&b->d_kin, S1)) || (st = zalloc(&b->d_ndof, S1)) ||
+        (st = zalloc(&b->d_steps, S1)) || (st = zalloc(&b->d_left, S1)) || (st = zalloc(&b->d_flags, S1)) ||
+        (st = dalloc(&b->d_slot_pos, (size_t)b->nl->clusters_cap * kClusterSize + 1)) ||
+        (st = dalloc(&b->d_slot_type, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
+        return st;
+    SPGNB_CUDA(cudaMemcpy(b->d_table, table.data(), sizeof(float2) * table.size(), cudaMemcpyHostToDevice));
+    SPGNB_CUDA(cudaMemset(b->d_waters, 0xff, sizeof(int) * b->w_cap));
+    force_kernels_init(T * T);
+    SPGNB_CUDA(cudaDeviceSynchronize());
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
+    return SPGNB_OK;
+}
+
+int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
+{
+    int st;
+    if (b->fit && !z.fp.use_fit)
+        return fail(SPGNB_E_UNSUPPORTED, "batch: beta * cutoff of this system is outside the pool's fitted range");
+    if (z.water_numbers > 0 && b->have_water && (z.mO != b->mO || z.mH != b->mH))
+        return fail(SPGNB_E_ARG, "batch: the rigid waters of a pool share one mass pair");
+    cudaStream_t s = b->stream;
+    const long long ab = b->atom_pool.alloc(z.N);
+    if (ab < 0) return fail(SPGNB_E_OOM, "batch: no room for %d atoms now", z.N);
+    const long long ne = (long long)z.ex_list.size();
+    const long long eb = b->ex_pool.alloc(ne);
+    const long long wb = eb < 0 ? -1 : b->water_pool.alloc(z.water_numbers);
+    if (eb < 0 || wb < 0)
+    {
+        if (eb >= 0) b->ex_pool.release(eb, ne);
+        b->atom_pool.release(ab, z.N);
+        return fail(SPGNB_E_OOM, "batch: no room for the exclusions or waters now");
+    }
+    z.sh.atom_begin = (int)ab;
+    int sid = -1;
+    st = nl_admit(b->nl, z.sh, &z.run_start, &z.runs, s, &sid);
+    if (st)
+    {
+        b->water_pool.release(wb, z.water_numbers);
+        b->ex_pool.release(eb, ne);
+        b->atom_pool.release(ab, z.N);
+        return st == SPGNB_E_OOM ? fail(SPGNB_E_OOM, "batch: no free system id, cells or clusters now") : st;
+    }
+    if (z.water_numbers > 0 && !b->have_water)
+    {
+        b->have_water = true;
+        b->mO = z.mO;
+        b->mH = z.mH;
+        b->rc = 0.5f * b->opt.water_dhh;
+        const float h = sqrtf(b->opt.water_doh * b->opt.water_doh - b->rc * b->rc);
+        b->ra = 2.0f * b->mH * h / (b->mO + 2.0f * b->mH);
+        b->rb = h - b->ra;
+        free_graphs(b);  // the step now includes SETTLE
+    }
+    const int a0 = (int)ab;
+    std::vector<int> own(z.N), ex_start(z.N), ex_list(ne), waters(z.water_numbers);
+    for (int i = 0; i < z.N; i++)
+    {
+        own[i] = a0 + i;
+        ex_start[i] = (int)eb + z.ex_start[i];
+    }
+    for (long long k = 0; k < ne; k++) ex_list[k] = a0 + z.ex_list[k];
+    for (int w = 0; w < z.water_numbers; w++) waters[w] = a0 + z.water_begin + 3 * w;
+    const std::vector<ForceParams> fp(1, z.fp);
+    const std::vector<float> ndof(1, z.ndof);
+    const std::vector<int> left(1, steps > 0 ? steps : -1);
+    if ((st = put(b->d_crd, ab, z.crd, s)) || (st = put(b->d_vel, ab, z.vel, s)) ||
+        (st = put(b->d_charge, ab, z.charge, s)) || (st = put(b->d_inv_mass, ab, z.inv_mass, s)) ||
+        (st = put(b->d_type, ab, z.type, s)) || (st = put(b->d_atom_local, ab, own, s)) ||
+        (st = put(b->d_ex_start, ab, ex_start, s)) || (st = put(b->d_ex_num, ab, z.ex_num, s)) ||
+        (st = put(b->d_ex_list, eb, ex_list, s)) || (st = put(b->d_waters, wb, waters, s)) ||
+        (st = put(b->d_fps, sid, fp, s)) || (st = put(b->d_ndof, sid, ndof, s)) || (st = put(b->d_left, sid, left, s)))
+        return st;
+    SPGNB_CUDA(cudaMemsetAsync(b->d_frc + ab, 0, sizeof(float3) * z.N, s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_steps + sid, 0, sizeof(int), s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_kin + sid, 0, sizeof(long long), s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_totals + 8 * (size_t)sid, 0, sizeof(long long) * 8, s));
+    // the host vectors above are about to go: wait for the copies
+    SPGNB_CUDA(cudaStreamSynchronize(s));
+    b->h_fps[sid] = z.fp;
+    SysRec& r = b->rec[sid];
+    r.live = true;
+    r.atom_begin = a0;
+    r.atom_count = z.N;
+    r.ex_begin = eb;
+    r.ex_count = ne;
+    r.w_begin = (int)wb;
+    r.w_count = z.water_numbers;
+    r.lr_factor = z.lr_factor;
+    r.volume = z.volume;
+    b->h_flags[sid] = 1;
+    b->pending = true;
+    *id = sid;
+    return SPGNB_OK;
+}
+
+// Batch-side device bytes for the capacities.
+double batch_bytes(long long atoms, long long ex, long long waters, long long slots, int S, int T)
+{
+    return (double)atoms * (12 * 4 + 4 * 6) + ex * 4.0 + waters * 4.0 + slots * 20.0 + (S + 1.0) * (32 + 64 + 8 + 16) +
+           T * (double)T * 8;
+}
+
+// Pool capacities for `atoms` atoms under the pool options.
+NLPoolSpec pool_spec(const spgnb_batch_pool_options& po, float prune_buffer, int atoms)
+{
+    NLPoolSpec sp;
+    const double gl = 0.5 * (po.min_cutoff + po.skin);
+    const double cells_per_atom = 1.25 / (po.density * gl * gl * gl);
+    sp.systems = po.max_systems;
+    sp.atoms = atoms;
+    sp.cells = (int)std::min<double>(atoms * cells_per_atom + 2.0 * po.max_systems + 64, (1 << 28) - 1);
+    sp.clusters = (int)std::min<double>(atoms / (double)kClusterSize + sp.cells + po.max_systems, 0x7fffffff);
+    sp.runs = (long long)sp.cells * 48;
+    double pc, pa;
+    nl_capacity_for(po.density * 1.1, 1e30, po.max_cutoff, po.skin, prune_buffer, &pc, &pa);
+    sp.table_cap = std::max((int)(pc * 1.3) + 64, 128);
+    sp.slot_cap = (((int)(pa * 1.3) + 63) & ~63) + 128;
+    sp.prune_rc = po.max_cutoff;
+    return sp;
+}
+
+double pool_bytes(const spgnb_batch_pool_options& po, float prune_buffer, int atoms, int T)
+{
+    const NLPoolSpec sp = pool_spec(po, prune_buffer, atoms);
+    spgnb_nl probe;
+    probe.S = sp.systems;
+    probe.n_cap = sp.atoms;
+    probe.G = sp.cells;
+    probe.clusters_cap = sp.clusters;
+    probe.runs_cap = sp.runs;
+    probe.table_cap = sp.table_cap;
+    probe.slot_cap = sp.slot_cap;
+    probe.opt.export_atom_groups = 0;
+    const long long ex = po.max_excluded > 0 ? po.max_excluded : 2LL * atoms;
+    const long long w = po.max_waters > 0 ? po.max_waters : atoms / 3;
+    return (double)nl_device_bytes(&probe) + batch_bytes(atoms, ex, w, (long long)sp.clusters * kClusterSize, sp.systems, T);
 }
 
 }  // namespace
@@ -336,6 +711,20 @@ void spgnb_batch_default_options(spgnb_batch_options* o)
     o->refresh_interval = 0;
 }
 
+void spgnb_batch_pool_default_options(spgnb_batch_pool_options* o)
+{
+    if (!o) return;
+    o->max_systems = 1024;
+    o->max_atoms = 0;
+    o->max_excluded = 0;
+    o->max_waters = 0;
+    o->max_cutoff = 12.0f;
+    o->min_cutoff = 8.0f;
+    o->skin = 2.0f;
+    o->density = 0.1003f;
+    o->hbm_budget_bytes = 120e9;
+}
+
 int spgnb_batch_set_thermostat(spgnb_batch* b, float tau, float temperature)
 {
     if (!b) return fail(SPGNB_E_ARG, "spgnb_batch_set_thermostat: NULL handle");
@@ -346,201 +735,262 @@ int spgnb_batch_set_thermostat(spgnb_batch* b, float tau, float temperature)
     return SPGNB_OK;
 }
 
-int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int atom_type_numbers,
-                       const float* h_pair_A, const float* h_pair_B, const spgnb_batch_options* opt,
-                       spgnb_batch** out)
+static int check_type_table(int T, const float* A, const float* B)
 {
-    if (!out) return fail(SPGNB_E_ARG, "spgnb_batch_create: out is NULL");
-    *out = nullptr;
-    if (n_systems <= 0 || !systems || atom_type_numbers <= 0 || !h_pair_A || !h_pair_B)
-        return fail(SPGNB_E_ARG, "spgnb_batch_create: bad arguments");
-    const int T = atom_type_numbers;
+    if (T <= 0 || !A || !B) return fail(SPGNB_E_ARG, "batch: bad LJ type table");
     if (T > kMaxTypes || T * T * (int)sizeof(float2) > 96 * 1024)
-        return fail(SPGNB_E_UNSUPPORTED, "spgnb_batch_create: %d LJ types exceed the shared-memory pair table", T);
+        return fail(SPGNB_E_UNSUPPORTED, "batch: %d LJ types exceed the shared-memory pair table", T);
+    return SPGNB_OK;
+}
+
+static spgnb_batch* new_batch(const spgnb_batch_options* opt, int T, const float* A, const float* B)
+{
     spgnb_batch* b = new spgnb_batch();
     if (opt)
         b->opt = *opt;
     else
         spgnb_batch_default_options(&b->opt);
     if (b->opt.steps_per_graph <= 0) b->opt.steps_per_graph = 1;
-    b->S = n_systems;
-    b->T = T;
-    // host staging
-    long long ntot = 0;
-    for (int s = 0; s < n_systems; s++)
-    {
-        const spgnb_batch_system& y = systems[s];
-        if (y.atom_numbers <= 0 || !y.h_crd || !y.h_charge || !y.h_mass || !y.h_atom_type || !y.h_excluded_start ||
-            !y.h_excluded_numbers || (y.excluded_total > 0 && !y.h_excluded_list) || y.water_begin < 0 ||
-            y.water_numbers < 0 || y.water_begin + 3LL * y.water_numbers > y.atom_numbers)
-        {
-            delete b;
-            return fail(SPGNB_E_ARG, "spgnb_batch_create: system %d is incomplete", s);
-        }
-        b->atom_begin.push_back((int)ntot);
-        b->atom_count.push_back(y.atom_numbers);
-        ntot += y.atom_numbers;
-    }
-    if (ntot > (1LL << 28))
-    {
-        delete b;
-        return fail(SPGNB_E_UNSUPPORTED, "spgnb_batch_create: %lld atoms in total", ntot);
-    }
-    b->n = (int)ntot;
-    std::vector<float3> crd(b->n), vel(b->n);
-    std::vector<float> charge(b->n), inv_mass(b->n);
-    std::vector<int> type(b->n), iota(b->n), ex_start(b->n), ex_num(b->n), ex_list, waters;
-    std::vector<int> counts(n_systems), atom_sys(b->n);
-    std::vector<float> ndof(n_systems);
-    std::vector<spgnb_ltmatrix3> cells(n_systems), rcells(n_systems);
-    std::vector<float> cutoffs(n_systems), skins(n_systems);
-    b->h_fps.resize(n_systems);
-    b->lr_factor.resize(n_systems);
-    b->volume.resize(n_systems);
-    for (int s = 0; s < n_systems; s++)
-    {
-        const spgnb_batch_system& y = systems[s];
-        const int a0 = b->atom_begin[s];
-        std::vector<double> hist(T, 0.0);
-        for (int i = 0; i < y.atom_numbers; i++)
-        {
-            const int g = a0 + i;
-            crd[g] = make_float3(y.h_crd[3 * i], y.h_crd[3 * i + 1], y.h_crd[3 * i + 2]);
-            vel[g] = y.h_vel ? make_float3(y.h_vel[3 * i], y.h_vel[3 * i + 1], y.h_vel[3 * i + 2]) : make_float3(0, 0, 0);
-            charge[g] = y.h_charge[i];
-            inv_mass[g] = y.h_mass[i] > 0.0f ? 1.0f / y.h_mass[i] : 0.0f;
-            const int t = y.h_atom_type[i];
-            if (t < 0 || t >= T)
-            {
-                delete b;
-                return fail(SPGNB_E_ARG, "spgnb_batch_create: system %d atom %d has type %d outside [0,%d)", s, i, t, T);
-            }
-            type[g] = t;
-            hist[t] += 1.0;
-            iota[g] = g;
-            ex_num[g] = y.h_excluded_numbers[i];
-            ex_start[g] = (int)ex_list.size();
-            for (int k = 0; k < y.h_excluded_numbers[i]; k++)
-                ex_list.push_back(a0 + y.h_excluded_list[y.h_excluded_start[i] + k]);
-        }
-        for (int w = 0; w < y.water_numbers; w++) waters.push_back(a0 + y.water_begin + 3 * w);
-        for (int i = 0; i < y.atom_numbers; i++) atom_sys[a0 + i] = s;
-        int moving = 0;
-        for (int i = 0; i < y.atom_numbers; i++) moving += y.h_mass[i] > 0.0f;
-        ndof[s] = (float)std::max(1, 3 * moving - 3 * y.water_numbers - 3);
-        counts[s] = y.atom_numbers;
-        cells[s] = y.cell;
-        rcells[s] = y.rcell;
-        cutoffs[s] = y.cutoff;
-        skins[s] = y.skin;
-        ForceParams& f = b->h_fps[s];
-        f.rc2 = y.cutoff * y.cutoff;
-        f.beta = y.pme_beta;
-        f.beta3 = y.pme_beta * y.pme_beta * y.pme_beta;
-        f.w_scale = y.pme_beta * y.pme_beta * SPGNB_EWALD_INV_W_MAX;
-        const float z = y.pme_beta * y.cutoff;
-        f.use_fit = (z * z <= SPGNB_EWALD_W_MAX * 0.999f) ? 1 : 0;
-        f.n_types = T;
-        f.table_begin = 0;
-        f.pad = 0;
-        if (!f.use_fit) b->fit = false;
-        // Total_C6_Get and the factor of Lennard_Jones_force.cpp:263-268
-        double c6 = 0.0;
-        for (int p = 0; p < T; p++)
-            for (int q = 0; q < T; q++)
-            {
-                const int hi = p > q ? p : q, lo = p > q ? q : p;
-                c6 += hist[p] * hist[q] * (double)h_pair_B[hi * (hi + 1) / 2 + lo];
-            }
-        float fac = (float)c6;
-        fac *= -2.0f / 3.0f * 3.1415926535897932f / y.cutoff / y.cutoff / y.cutoff / 6.0f;
-        b->lr_factor[s] = fac;
-        b->volume[s] = (double)y.cell.a11 * y.cell.a22 * y.cell.a33;
-    }
-    if (ex_list.empty()) ex_list.push_back(0);
-    b->n_waters = (int)waters.size();
-    std::vector<float2> table((size_t)T * T);
-    for (int p = 0; p < T; p++)
-        for (int q = 0; q < T; q++)
-        {
-            const int hi = p > q ? p : q, lo = p > q ? q : p;
-            table[(size_t)p * T + q] = make_float2(h_pair_A[hi * (hi + 1) / 2 + lo], h_pair_B[hi * (hi + 1) / 2 + lo]);
-        }
-    // rigid water geometry (first water's masses)
-    b->mO = 16.0f;
-    b->mH = 1.008f;
-    for (int s = 0; s < n_systems; s++)
-        if (systems[s].water_numbers > 0)
-        {
-            b->mO = systems[s].h_mass[systems[s].water_begin];
-            b->mH = systems[s].h_mass[systems[s].water_begin + 1];
-            break;
-        }
-    b->rc = 0.5f * b->opt.water_dhh;
-    const float h = sqrtf(b->opt.water_doh * b->opt.water_doh - b->rc * b->rc);
-    b->ra = 2.0f * b->mH * h / (b->mO + 2.0f * b->mH);
-    b->rb = h - b->ra;
+    const int P = T * (T + 1) / 2;
+    b->h_pair_A.assign(A, A + P);
+    b->h_pair_B.assign(B, B + P);
+    return b;
+}
 
-    int st = SPGNB_OK;
-    spgnb_nl_options nlo;
-    spgnb_nl_default_options(&nlo);
-    nlo.refresh_interval = 0;
-    nlo.skin_permit = b->opt.skin_permit;
-    nlo.export_atom_groups = 0;
-    nlo.prune_buffer = b->opt.prune_buffer;
-    if ((st = nl_create_multi(n_systems, counts.data(), cells.data(), rcells.data(), cutoffs.data(), skins.data(),
-                              &nlo, &b->nl)) ||
-        (st = upload(&b->d_crd, crd)) || (st = upload(&b->d_vel, vel)) || (st = dalloc(&b->d_frc, b->n)) ||
-        (st = dalloc(&b->d_crd_old, b->n)) || (st = upload(&b->d_charge, charge)) ||
-        (st = upload(&b->d_inv_mass, inv_mass)) || (st = upload(&b->d_type, type)) ||
-        (st = upload(&b->d_atom_local, iota)) || (st = upload(&b->d_ex_start, ex_start)) ||
-        (st = upload(&b->d_ex_num, ex_num)) || (st = upload(&b->d_ex_list, ex_list)) ||
-        (st = upload(&b->d_waters, waters)) || (st = upload(&b->d_table, table)) ||
-        (st = upload(&b->d_fps, b->h_fps)) || (st = dalloc(&b->d_totals, 8 * (size_t)n_systems)) ||
-        (st = upload(&b->d_atom_sys, atom_sys)) || (st = upload(&b->d_ndof, ndof)) ||
-        (st = dalloc(&b->d_kin, (size_t)n_systems)) || (st = dalloc(&b->d_step, 1)) ||
-        (st = dalloc(&b->d_slot_pos, (size_t)b->nl->clusters_cap * kClusterSize + 1)) ||
-        (st = dalloc(&b->d_slot_type, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
+int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int atom_type_numbers,
+                       const float* h_pair_A, const float* h_pair_B, const spgnb_batch_options* opt,
+                       spgnb_batch** out)
+{
+    if (!out) return fail(SPGNB_E_ARG, "spgnb_batch_create: out is NULL");
+    *out = nullptr;
+    if (n_systems <= 0 || !systems) return fail(SPGNB_E_ARG, "spgnb_batch_create: bad arguments");
+    const int T = atom_type_numbers;
+    int st = check_type_table(T, h_pair_A, h_pair_B);
+    if (st) return st;
+    spgnb_batch* b = new_batch(opt, T, h_pair_A, h_pair_B);
+    const std::vector<float>& pa = b->h_pair_A;
+    const std::vector<float>& pb = b->h_pair_B;
+    std::vector<Staged> z(n_systems);
+    long long atoms = 0, ex = 0, waters = 0, cells = 0, clusters = 0, runs = 0;
+    double per_cluster = 0, per_atom = 0;
+    float rcmax = 0;
+    for (int k = 0; k < n_systems && !st; k++)
+    {
+        if ((st = stage(systems[k], T, pa, pb, k, z[k]))) break;
+        const Staged& y = z[k];
+        atoms += y.N;
+        ex += (long long)y.ex_list.size();
+        waters += y.water_numbers;
+        const int G = y.sh.cells();
+        cells += G + 1;
+        clusters += y.N / kClusterSize + G + 1;
+        runs += (long long)y.runs.size();
+        double pc, pw;
+        nl_capacity_for(y.N / y.volume, y.N, systems[k].cutoff, systems[k].skin, b->opt.prune_buffer, &pc, &pw);
+        per_cluster = std::max(per_cluster, pc);
+        per_atom = std::max(per_atom, pw);
+        rcmax = std::max(rcmax, systems[k].cutoff);
+        if (!y.fp.use_fit) b->fit = false;
+    }
+    if (!st && atoms > (1LL << 28)) st = fail(SPGNB_E_UNSUPPORTED, "spgnb_batch_create: %lld atoms in total", atoms);
+    if (!st && (clusters + 1) * kClusterSize > kMaxSlots)
+        st = fail(SPGNB_E_UNSUPPORTED, "batch: %lld atoms in %lld cells exceed the %d-slot limit of the lists", atoms,
+                  cells, kMaxSlots);
+    if (st)
+    {
+        delete b;
+        return st;
+    }
+    NLPoolSpec spec;
+    spec.systems = n_systems;
+    spec.atoms = (int)atoms;
+    spec.cells = (int)cells;
+    spec.clusters = (int)clusters;
+    spec.runs = std::max(1LL, runs);
+    spec.table_cap = std::max((int)(per_cluster * 1.3) + 64, 128);
+    spec.slot_cap = (((int)(per_atom * 1.3) + 63) & ~63) + 128;
+    spec.prune_rc = rcmax;
+    if (!(st = create_common(b, spec, ex, (int)waters, T, pa.data(), pb.data())))
+        for (int k = 0; k < n_systems && !st; k++)
+        {
+            int id = -1;
+            st = admit_staged(b, z[k], 0, &id);
+            if (!st && id != k) st = fail(SPGNB_E_STATE, "spgnb_batch_create: system %d got id %d", k, id);
+            z[k] = Staged{};
+        }
+    if (!st) st = settle_pending(b);
+    if (!st)
+    {
+        cudaError_t e = cudaStreamSynchronize(b->stream);
+        if (e != cudaSuccess) st = cuda_fail(e, "spgnb_batch_create");
+    }
+    if (st)
     {
         free_batch(b);
         delete b;
         return st;
-    }
-    force_kernels_init(T * T);
-    cudaMemset(b->d_step, 0, sizeof(int));
-    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
-    if (e != cudaSuccess)
-    {
-        free_batch(b);
-        delete b;
-        return cuda_fail(e, "cudaStreamCreate");
-    }
-    // first lists and F(0) with energies
-    if ((st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num, kBuildForced,
-                             b->stream)) ||
-        (st = batch_force(b, 1, b->stream)))
-    {
-        free_batch(b);
-        delete b;
-        return st;
-    }
-    e = cudaStreamSynchronize(b->stream);
-    if (e != cudaSuccess)
-    {
-        free_batch(b);
-        delete b;
-        return cuda_fail(e, "spgnb_batch_create");
     }
     *out = b;
+    return SPGNB_OK;
+}
+
+int spgnb_batch_create_pool(const spgnb_batch_pool_options* pool, int atom_type_numbers, const float* h_pair_A,
+                            const float* h_pair_B, const spgnb_batch_options* opt, spgnb_batch** out)
+{
+    if (!out) return fail(SPGNB_E_ARG, "spgnb_batch_create_pool: out is NULL");
+    *out = nullptr;
+    const int T = atom_type_numbers;
+    int st = check_type_table(T, h_pair_A, h_pair_B);
+    if (st) return st;
+    spgnb_batch_pool_options po;
+    if (pool)
+        po = *pool;
+    else
+        spgnb_batch_pool_default_options(&po);
+    if (po.max_systems <= 0 || !(po.max_cutoff > 0.0f) || !(po.min_cutoff > 0.0f) || po.min_cutoff > po.max_cutoff ||
+        !(po.skin >= 0.0f) || !(po.density > 0.0f) || (po.max_atoms <= 0 && !(po.hbm_budget_bytes > 0.0)))
+        return fail(SPGNB_E_ARG, "spgnb_batch_create_pool: bad pool options");
+    spgnb_batch* b = new_batch(opt, T, h_pair_A, h_pair_B);
+    int atoms = po.max_atoms;
+    // the largest atom count whose clusters fit the slot field of the lists
+    {
+        int lo = 1024, hi = 1 << 28;
+        while (hi - lo > 1024)
+        {
+            const int mid = lo + (hi - lo) / 2;
+            const NLPoolSpec sp = pool_spec(po, b->opt.prune_buffer, mid);
+            if (((long long)sp.clusters + 1) * kClusterSize <= kMaxSlots)
+                lo = mid;
+            else
+                hi = mid;
+        }
+        const int slot_limit = lo;
+        if (atoms <= 0)
+        {
+            // linear in the atom count: solve bytes(atoms) = budget
+            const double b1 = pool_bytes(po, b->opt.prune_buffer, 1 << 20, T);
+            const double b2 = pool_bytes(po, b->opt.prune_buffer, 1 << 21, T);
+            const double per_atom = (b2 - b1) / (double)(1 << 20);
+            const double fixed = b1 - per_atom * (1 << 20);
+            atoms = (int)std::min<double>((po.hbm_budget_bytes - fixed) / per_atom, (double)(1 << 28));
+        }
+        atoms = std::min(atoms, slot_limit);
+        atoms &= ~1023;
+    }
+    if (atoms < 1024)
+    {
+        delete b;
+        return fail(SPGNB_E_ARG, "spgnb_batch_create_pool: the budget holds fewer than 1024 atoms");
+    }
+    const NLPoolSpec spec = pool_spec(po, b->opt.prune_buffer, atoms);
+    const long long ex = po.max_excluded > 0 ? po.max_excluded : 2LL * atoms;
+    const int w = po.max_waters > 0 ? po.max_waters : atoms / 3;
+    b->fit = true;
+    if ((st = create_common(b, spec, ex, w, T, b->h_pair_A.data(), b->h_pair_B.data())))
+    {
+        free_batch(b);
+        delete b;
+        return st;
+    }
+    *out = b;
+    return SPGNB_OK;
+}
+
+int spgnb_batch_admit(spgnb_batch* b, const spgnb_batch_system* sys, int steps, int* id)
+{
+    if (!b || !sys || !id) return fail(SPGNB_E_ARG, "spgnb_batch_admit: NULL argument");
+    *id = -1;
+    Staged z;
+    int st = stage(*sys, b->T, b->h_pair_A, b->h_pair_B, -1, z);
+    if (st) return st;
+    return admit_staged(b, z, steps, id);
+}
+
+int spgnb_batch_retire(spgnb_batch* b, int id)
+{
+    if (!b || id < 0 || id >= b->S || !b->rec[id].live) return fail(SPGNB_E_ARG, "spgnb_batch_retire: bad system id");
+    cudaStream_t s = b->stream;
+    SysRec& r = b->rec[id];
+    int st = nl_retire(b->nl, id, s);
+    if (st) return st;
+    // parked atoms: at rest, massless, no force; free water entries -1
+    SPGNB_CUDA(cudaMemsetAsync(b->d_vel + r.atom_begin, 0, sizeof(float3) * r.atom_count, s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_frc + r.atom_begin, 0, sizeof(float3) * r.atom_count, s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_inv_mass + r.atom_begin, 0, sizeof(float) * r.atom_count, s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_charge + r.atom_begin, 0, sizeof(float) * r.atom_count, s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_ex_num + r.atom_begin, 0, sizeof(int) * r.atom_count, s));
+    if (r.w_count) SPGNB_CUDA(cudaMemsetAsync(b->d_waters + r.w_begin, 0xff, sizeof(int) * r.w_count, s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_left + id, 0, sizeof(int), s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_steps + id, 0, sizeof(int), s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_totals + 8 * (size_t)id, 0, sizeof(long long) * 8, s));
+    b->atom_pool.release(r.atom_begin, r.atom_count);
+    b->ex_pool.release(r.ex_begin, r.ex_count);
+    b->water_pool.release(r.w_begin, r.w_count);
+    b->h_flags[id] = 0;
+    r = SysRec{};
+    return SPGNB_OK;
+}
+
+int spgnb_batch_evaluate(spgnb_batch* b, const int* ids, int n)
+{
+    if (!b || (n > 0 && !ids)) return fail(SPGNB_E_ARG, "spgnb_batch_evaluate: NULL argument");
+    int st = settle_pending(b);
+    if (st) return st;
+    bool any = false;
+    for (int k = 0; k < n; k++)
+    {
+        if (ids[k] < 0 || ids[k] >= b->S || !b->rec[ids[k]].live)
+            return fail(SPGNB_E_ARG, "spgnb_batch_evaluate: system %d is not in the pool", ids[k]);
+        b->h_flags[ids[k]] = 1;
+        any = true;
+    }
+    if (!any) return SPGNB_OK;
+    cudaStream_t s = b->stream;
+    SPGNB_CUDA(cudaMemcpyAsync(b->d_flags, b->h_flags.data(), sizeof(int) * b->S, cudaMemcpyHostToDevice, s));
+    st = batch_force(b, 1, s, b->d_flags);
+    if (st) return st;
+    SPGNB_CUDA(cudaMemsetAsync(b->d_flags, 0, sizeof(int) * b->S, s));
+    SPGNB_CUDA(cudaStreamSynchronize(s));  // h_flags is the copy's source
+    std::fill(b->h_flags.begin(), b->h_flags.end(), 0);
+    return SPGNB_OK;
+}
+
+int spgnb_batch_progress(spgnb_batch* b, int* steps_done, int* steps_left)
+{
+    if (!b) return fail(SPGNB_E_ARG, "spgnb_batch_progress: NULL handle");
+    std::vector<int> d(b->S), l(b->S);
+    SPGNB_CUDA(cudaMemcpyAsync(d.data(), b->d_steps, sizeof(int) * b->S, cudaMemcpyDeviceToHost, b->stream));
+    SPGNB_CUDA(cudaMemcpyAsync(l.data(), b->d_left, sizeof(int) * b->S, cudaMemcpyDeviceToHost, b->stream));
+    SPGNB_CUDA(cudaStreamSynchronize(b->stream));
+    for (int k = 0; k < b->S; k++)
+    {
+        const bool live = b->rec[k].live;
+        if (steps_done) steps_done[k] = live ? d[k] : 0;
+        if (steps_left) steps_left[k] = live ? l[k] : 0;
+    }
+    return SPGNB_OK;
+}
+
+int spgnb_batch_capacity(spgnb_batch* b, int* max_systems, long long* max_atoms, long long* free_atoms,
+                         double* device_bytes)
+{
+    if (!b) return fail(SPGNB_E_ARG, "spgnb_batch_capacity: NULL handle");
+    if (max_systems) *max_systems = b->S;
+    if (max_atoms) *max_atoms = b->n;
+    if (free_atoms) *free_atoms = b->atom_pool.available();
+    if (device_bytes)
+        *device_bytes = (double)nl_device_bytes(b->nl) +
+                        batch_bytes(b->n, b->ex_cap, b->w_cap, (long long)b->nl->clusters_cap * kClusterSize, b->S, b->T);
     return SPGNB_OK;
 }
 
 int spgnb_batch_run(spgnb_batch* b, int steps, int energy_interval)
 {
     if (!b) return fail(SPGNB_E_ARG, "spgnb_batch_run: NULL handle");
-    if (steps <= 0) return SPGNB_OK;
-    int st = ensure_graphs(b);
+    int st = settle_pending(b);
     if (st) return st;
+    if (steps <= 0) return SPGNB_OK;
+    if ((st = ensure_graphs(b))) return st;
     const int K = b->opt.steps_per_graph;
     int done = 0;
     while (done < steps)
@@ -573,6 +1023,8 @@ int spgnb_batch_run(spgnb_batch* b, int steps, int energy_interval)
 int spgnb_batch_energies(spgnb_batch* b, double* out)
 {
     if (!b || !out) return fail(SPGNB_E_ARG, "spgnb_batch_energies: NULL argument");
+    int st = settle_pending(b);
+    if (st) return st;
     std::vector<long long> h(8 * (size_t)b->S);
     SPGNB_CUDA(cudaMemcpyAsync(h.data(), b->d_totals, sizeof(long long) * h.size(), cudaMemcpyDeviceToHost, b->stream));
     SPGNB_CUDA(cudaStreamSynchronize(b->stream));
@@ -580,8 +1032,9 @@ int spgnb_batch_energies(spgnb_batch* b, double* out)
     {
         const long long* t = &h[8 * (size_t)s];
         double* o = out + 9 * (size_t)s;
+        const SysRec& r = b->rec[s];
         o[0] = (double)t[0] / kEnergyScale;
-        o[1] = b->lr_factor[s] / b->volume[s];
+        o[1] = r.live ? r.lr_factor / r.volume : 0.0;
         o[2] = (double)t[1] / kEnergyScale;
         for (int q = 0; q < 6; q++) o[3 + q] = (double)t[2 + q] / kEnergyScale;
     }
@@ -590,8 +1043,10 @@ int spgnb_batch_energies(spgnb_batch* b, double* out)
 
 int spgnb_batch_download(spgnb_batch* b, int sys, float* h_crd, float* h_vel, float* h_frc)
 {
-    if (!b || sys < 0 || sys >= b->S) return fail(SPGNB_E_ARG, "spgnb_batch_download: bad system");
-    const size_t off = b->atom_begin[sys], cnt = b->atom_count[sys];
+    if (!b || sys < 0 || sys >= b->S || !b->rec[sys].live) return fail(SPGNB_E_ARG, "spgnb_batch_download: bad system");
+    int st = settle_pending(b);
+    if (st) return st;
+    const size_t off = b->rec[sys].atom_begin, cnt = b->rec[sys].atom_count;
     if (h_crd)
         SPGNB_CUDA(cudaMemcpyAsync(h_crd, b->d_crd + off, sizeof(float3) * cnt, cudaMemcpyDeviceToHost, b->stream));
     if (h_vel)
@@ -632,10 +1087,7 @@ int spgnb_batch_autotune(spgnb_batch* b, int steps_per_candidate, float* chosen_
     {
         if (c > maxb + 1e-6f) continue;
         b->nl->opt.prune_buffer = c;
-        const std::vector<int> ones(b->S, 1);
-        SPGNB_CUDA(cudaMemcpyAsync(b->nl->d_prune, ones.data(), sizeof(int) * b->S, cudaMemcpyHostToDevice, b->stream));
-        const int one = 1;
-        SPGNB_CUDA(cudaMemcpyAsync(b->nl->d_counters + kCntPrune, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+        if ((st = nl_prune_all(b->nl, b->stream))) break;
         free_graphs(b);
         if ((st = spgnb_batch_run(b, b->opt.steps_per_graph, 0))) break;  // warm-up, includes the pruning
         SPGNB_CUDA(cudaEventRecord(e0, b->stream));
@@ -656,10 +1108,7 @@ int spgnb_batch_autotune(spgnb_batch* b, int steps_per_candidate, float* chosen_
     b->nl->opt.prune_buffer = best;
     b->opt.prune_buffer = best;
     free_graphs(b);
-    const std::vector<int> ones(b->S, 1);
-    SPGNB_CUDA(cudaMemcpyAsync(b->nl->d_prune, ones.data(), sizeof(int) * b->S, cudaMemcpyHostToDevice, b->stream));
-    const int one = 1;
-    SPGNB_CUDA(cudaMemcpyAsync(b->nl->d_counters + kCntPrune, &one, sizeof(int), cudaMemcpyHostToDevice, b->stream));
+    if ((st = nl_prune_all(b->nl, b->stream))) return st;
     SPGNB_CUDA(cudaStreamSynchronize(b->stream));
     if (chosen_buffer) *chosen_buffer = best;
     return SPGNB_OK;
@@ -682,15 +1131,8 @@ int spgnb_batch_check_overflow(spgnb_batch* b, int* regrown)
     int st = nl_regrow(b->nl, flags);
     if (st) return st;
     free_graphs(b);
-    const int S = b->S;
-    if (b->d_slot_pos) dfree(b->d_slot_pos);
-    if (b->d_slot_type) dfree(b->d_slot_type);
-    if ((st = dalloc(&b->d_slot_pos, (size_t)b->nl->clusters_cap * kClusterSize + 1)) ||
-        (st = dalloc(&b->d_slot_type, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
-        return st;
-    (void)S;
-    if ((st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num, kBuildForced,
-                             b->stream)) ||
+    if ((st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num,
+                             kBuildForced, b->stream)) ||
         (st = batch_force(b, 0, b->stream)))
         return st;
     SPGNB_CUDA(cudaStreamSynchronize(b->stream));

@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -151,24 +153,85 @@ constexpr int kMaxTypes = 256;       // LJ type field of a pruned-list word
 }  // namespace spgnb
 
 // ----------------------------------------------------------- host handles
+// First-fit allocator of index ranges in [0, cap), for the pool of systems.
+struct RangePool
+{
+    long long cap = 0;
+    std::map<long long, long long> free_;  // begin -> length
+    void reset(long long c)
+    {
+        cap = c;
+        free_.clear();
+        if (c > 0) free_[0] = c;
+    }
+    // first range of n indices, or -1 (n = 0 is an empty range at 0)
+    long long alloc(long long n)
+    {
+        if (n <= 0) return 0;
+        for (auto it = free_.begin(); it != free_.end(); ++it)
+            if (it->second >= n)
+            {
+                const long long b = it->first, len = it->second;
+                free_.erase(it);
+                if (len > n) free_[b + n] = len - n;
+                return b;
+            }
+        return -1;
+    }
+    void release(long long b, long long n)
+    {
+        if (n <= 0) return;
+        auto it = free_.emplace(b, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first)
+        {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin())
+        {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first)
+            {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    long long available() const
+    {
+        long long t = 0;
+        for (const auto& f : free_) t += f.second;
+        return t;
+    }
+};
+
 struct SysHost
 {
     int atom_begin = 0, atom_count = 0;
     spgnb_ltmatrix3 cell{}, rcell{};
     float cutoff = 0, skin = 0, gl = 0, cs2 = 0;
     int dims[3] = {0, 0, 0};
-    int cell_begin = 0;
+    int cell_begin = 0;     // cells [cell_begin, cell_begin + G]; the extra one ends the run table
     int cl_begin = 0, cl_cap = 0;
+    long long run_begin = 0, run_count = 0;
     bool triclinic = false;
+    int cells() const { return dims[0] * dims[1] * dims[2]; }
 };
 
-// A neighbour list over one or more independent periodic systems whose atoms
-// are concatenated.  The C ABI's NEIGHBOR_LIST is the one-system case; the
-// batched engine uses many.
+// A neighbour list over one or more independent periodic systems.  Every
+// system owns ranges of the atom, cell, cluster and run arrays; ranges no
+// system owns map to the parking descriptor (index S), which never rebuilds
+// or prunes.  The C ABI's NEIGHBOR_LIST is the one-system case; the batched
+// engine uses many, admitted and retired while the others run.
 struct spgnb_nl
 {
-    int S = 1;
+    int S = 1;             // system ids [0, S); descriptor S parks unused ranges
     std::vector<SysHost> sys;
+    std::vector<char> live;
+    std::set<int> free_ids;
+    RangePool cell_pool, cl_pool, run_pool;
+    long long runs_cap = 0;
     int n_cap = 0;         // atoms, all systems
     int G = 0;             // cells, all systems
     float cutoff = 0, skin = 0, grid_length = 0, cs2 = 0;   // system 0 (one-system API)
@@ -194,6 +257,7 @@ struct spgnb_nl
     int* d_cell_cursor = nullptr; // G
     int2* d_cell_cl = nullptr;    // G: the cell's clusters [x, y)
     // per system: rebuild and prune requests, clusters of the last build
+    int* d_live = nullptr;
     int* d_need = nullptr;
     int* d_prune = nullptr;
     int* d_ncl = nullptr;
@@ -357,6 +421,7 @@ struct ForceInputs
     int table_size = 0;
     float3* frc = nullptr;             // += forces
     long long* totals = nullptr;       // 8 fixed-point sums per system (mode >= 1)
+    const int* only = nullptr;         // per-system flags: evaluate these systems only (null: all)
     int mode = 0;                      // 0 forces, 1 + totals, 2 + per-atom outputs
     OwnerMap om{nullptr, 0, 3};
     PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
@@ -368,16 +433,53 @@ int force_kernels_init(int table_size);
 int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,
                     const spgnb_ltmatrix3* rcells, const float* cutoffs, const float* skins,
                     const spgnb_nl_options* opt, spgnb_nl** out);
+// Capacities of an empty pool of systems.
+struct NLPoolSpec
+{
+    int systems = 0;
+    int atoms = 0;
+    int cells = 0;        // including one extra cell per system
+    int clusters = 0;
+    long long runs = 0;
+    int table_cap = 0;    // neighbour-table elements per cluster
+    int slot_cap = 0;     // pruned-list words per slot
+    float prune_rc = 0;   // the largest cutoff
+};
+int nl_create_pool(const NLPoolSpec& spec, const spgnb_nl_options* opt, spgnb_nl** out);
+// Fills a system's grid geometry from its box, cutoff and skin; checks them.
+int nl_init_system(SysHost& sh, int atom_count, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, float cutoff,
+                   float skin, int index);
+// Candidate-cell runs of a system with cell ids from 0: run_start has G + 1
+// entries.
+int nl_system_runs(const SysHost& sh, std::vector<int>& run_start, std::vector<int2>& runs);
+// Table and pruned-list capacities for a system of this density and cutoff.
+void nl_capacity_for(double atoms_per_A3, double atom_count, float cutoff, float skin, float prune_buffer,
+                     double* table_per_cluster, double* words_per_atom);
+// Takes a free system id and the cell, cluster and run ranges of a system
+// whose atoms occupy [sh.atom_begin, + sh.atom_count); SPGNB_E_OOM (no
+// message) when the pool has no room now.  The system rebuilds when the
+// caller sets its flag for a kBuildPreset update.
+int nl_admit(spgnb_nl* nl, SysHost sh, const std::vector<int>* run_start, const std::vector<int2>* runs,
+             cudaStream_t s, int* id);
+// Returns a system's ranges to the pool; its atoms map to the parking descriptor.
+int nl_retire(spgnb_nl* nl, int id, cudaStream_t s);
+// Every live system re-prunes before the next force evaluation.
+int nl_prune_all(spgnb_nl* nl, cudaStream_t s);
 enum BuildHow
 {
     kBuildSkin = 0,
     kBuildForced = 1,
-    kBuildInterval = 2
+    kBuildInterval = 2,
+    kBuildPreset = 3
 };
+// aux: kBuildInterval - per-system steps done; kBuildPreset - per-system
+// flags of the systems to rebuild.  active (optional): per system, 0 = frozen
+// (no forced or interval rebuild).
 int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
-                   const int* ex_list, const int* ex_num, int how, cudaStream_t s, int* d_step = nullptr,
-                   int interval = 0);
+                   const int* ex_list, const int* ex_num, int how, cudaStream_t s, const int* d_aux = nullptr,
+                   int interval = 0, const int* d_active = nullptr);
 int nl_regrow(spgnb_nl* nl, int flags);
 int nl_set_prune_rc(spgnb_nl* nl, float rc, cudaStream_t s);
+size_t nl_device_bytes(const spgnb_nl* nl);
 
 }  // namespace spgnb

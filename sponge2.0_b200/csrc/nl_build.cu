@@ -677,25 +677,51 @@ __global__ void k_finish(int G, int S, const int* __restrict__ cell_sys, const i
 }
 
 // Refresh by a fixed interval of steps (NEIGHBOR_LIST::Update with
-// refresh_interval > 0), counted on the device: every system rebuilds when
-// the step counter, advanced here, reaches a multiple of the interval.
-__global__ void k_interval_need(int S, int interval, int* __restrict__ step, int* __restrict__ need, int* counters)
+// refresh_interval > 0), counted on the device per system: a system rebuilds
+// when its own step count reaches a multiple of the interval, so a system's
+// rebuilds do not depend on when it joined a batch.
+__global__ void k_interval_need(int S, int interval, const int* __restrict__ steps, const int* __restrict__ live,
+                                const int* __restrict__ active, int* __restrict__ need, int* counters)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    const int now = step[0] + 1;
-    const bool due = interval > 0 && now % interval == 0;
-    if (s < S) need[s] = due ? 1 : 0;
-    __syncthreads();
-    if (blockIdx.x == 0 && threadIdx.x == 0) counters[kCntNeed] = due ? 1 : 0;
+    if (s >= S) return;
+    const bool due = interval > 0 && live[s] && (!active || active[s] != 0) && (steps[s] + 1) % interval == 0;
+    need[s] = due ? 1 : 0;
+    if (due) counters[kCntNeed] = 1;
 }
 
-__global__ void k_step_tick(int* __restrict__ step) { step[0] += 1; }
-
-__global__ void k_set_need(int S, int* __restrict__ need, int* counters)
+__global__ void k_set_need(int S, const int* __restrict__ live, const int* __restrict__ active,
+                           int* __restrict__ need, int* counters)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s < S) need[s] = 1;
-    if (s == 0) counters[kCntNeed] = 1;
+    if (s >= S) return;
+    const bool due = live[s] && (!active || active[s] != 0);
+    need[s] = due ? 1 : 0;
+    if (due) counters[kCntNeed] = 1;
+}
+
+__global__ void k_need_preset(int S, const int* __restrict__ flags, const int* __restrict__ live,
+                              int* __restrict__ need, int* counters)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    const bool due = live[s] && flags[s];
+    need[s] = due ? 1 : 0;
+    if (due) counters[kCntNeed] = 1;
+}
+
+__global__ void k_prune_live(int S, const int* __restrict__ live, int* __restrict__ prune, int* counters)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= S) return;
+    prune[s] = live[s] ? 1 : 0;
+    if (live[s]) counters[kCntPrune] = 1;
+}
+
+__global__ void k_fill_int(int* __restrict__ p, long long n, int v)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = v;
 }
 
 __global__ void k_reset_list_counters(int* counters)
@@ -736,10 +762,12 @@ void grid_dims(const spgnb_ltmatrix3& cell, float cutoff, float skin, int dims[3
 // cell by enumerating the offsets instead of the O(G^2) scan.  A cell's
 // candidates are the cells B with B in stencil(A) (flag 1) or A in
 // stencil(B) (flag 2), grouped into runs of consecutive cell ids with equal
-// flags: {first | flags << 28, last + 1}.  Cell ids are global (the system's
-// first cell added).
+// flags: {first | flags << 28, last + 1}.  Cell ids count from the system's
+// first cell; start gets G + 1 entries.
 int build_runs(const SysHost& sh, std::vector<int>& start, std::vector<int2>& runs)
 {
+    start.assign(1, 0);
+    runs.clear();
     const int Nx = sh.dims[0], Ny = sh.dims[1], Nz = sh.dims[2];
     const int G = Nx * Ny * Nz;
     const float gl = sh.gl;
@@ -797,14 +825,30 @@ int build_runs(const SysHost& sh, std::vector<int>& start, std::vector<int2>& ru
         {
             size_t e = i + 1;
             while (e < touched.size() && touched[e] == touched[e - 1] + 1 && flag[touched[e]] == flag[touched[i]]) e++;
-            runs.push_back(make_int2((sh.cell_begin + touched[i]) | (flag[touched[i]] << 28),
-                                     sh.cell_begin + touched[e - 1] + 1));
+            runs.push_back(make_int2(touched[i] | (flag[touched[i]] << 28), touched[e - 1] + 1));
             i = e;
         }
         for (int j : touched) flag[j] = 0;
         start.push_back((int)runs.size());
     }
     return SPGNB_OK;
+}
+
+int fill_int(int* p, long long n, int v, cudaStream_t s)
+{
+    if (n <= 0) return SPGNB_OK;
+    const long long blocks = std::min<long long>((n + 255) / 256, 4096);
+    k_fill_int<<<(int)blocks, 256, 0, s>>>(p, n, v);
+    SPGNB_CHECK_LAUNCH("k_fill_int");
+    return SPGNB_OK;
+}
+
+__global__ void k_sys_flags(int id, int live_value, int* live, int* need, int* prune, int* ncl)
+{
+    live[id] = live_value;
+    need[id] = 0;
+    prune[id] = 0;
+    ncl[id] = 0;
 }
 
 void free_nl(spgnb_nl* nl)
@@ -817,6 +861,7 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_cell_count);
     dfree(nl->d_cell_cursor);
     dfree(nl->d_cell_cl);
+    dfree(nl->d_live);
     dfree(nl->d_need);
     dfree(nl->d_prune);
     dfree(nl->d_ncl);
@@ -910,67 +955,47 @@ SysDesc make_desc(const SysHost& sh, float skin_permit)
     return d;
 }
 
+// Arrays for the pool's capacities, every range parked.
 int alloc_nl(spgnb_nl* nl)
 {
     int st;
-    const int n = nl->n_cap;
-    int G = 0;
-    for (auto& sh : nl->sys)
-    {
-        sh.cell_begin = G;
-        G += sh.dims[0] * sh.dims[1] * sh.dims[2];
-    }
-    nl->G = G;
-    // each system owns a fixed cluster range: its atoms/8 + its cells + 1
-    long long ccap = 0;
-    for (auto& sh : nl->sys)
-    {
-        sh.cl_begin = (int)std::min<long long>(ccap, 0x7fffffff);
-        sh.cl_cap = sh.atom_count / kClusterSize + sh.dims[0] * sh.dims[1] * sh.dims[2] + 1;
-        ccap += sh.cl_cap;
-    }
-    nl->clusters_cap = (int)std::min<long long>(ccap, 0x7fffffff);
-    if ((ccap + 1) * kClusterSize > kMaxSlots)
-        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d atoms in %d cells exceed the %d-slot limit of the lists",
-                    n, G, kMaxSlots);
+    const int n = nl->n_cap, G = nl->G, S = nl->S;
+    if (((long long)nl->clusters_cap + 1) * kClusterSize > kMaxSlots)
+        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d clusters exceed the %d-slot limit of the lists",
+                    nl->clusters_cap, kMaxSlots);
     const size_t slots = (size_t)nl->clusters_cap * kClusterSize;
-    std::vector<int> start(1, 0);
-    std::vector<int2> runs;
-    for (auto& sh : nl->sys)
-        if ((st = build_runs(sh, start, runs))) return st;
-    nl->h_desc.resize(nl->S);
-    std::vector<int> atom_sys(n, 0), cell_sys(G, 0), cl_sys(nl->clusters_cap, 0);
-    for (int s = 0; s < nl->S; s++)
-    {
-        const SysHost& sh = nl->sys[s];
-        nl->h_desc[s] = make_desc(sh, nl->opt.skin_permit);
-        nl->h_desc[s].prune_r2 = prune_r2_of(nl->prune_rc, nl->opt.prune_buffer);
-        for (int i = sh.atom_begin; i < sh.atom_begin + sh.atom_count && i < n; i++) atom_sys[i] = s;
-        for (int c = 0; c < sh.dims[0] * sh.dims[1] * sh.dims[2]; c++) cell_sys[sh.cell_begin + c] = s;
-        for (int k = 0; k < sh.cl_cap; k++) cl_sys[sh.cl_begin + k] = s;
-    }
-    if ((st = dalloc(&nl->d_sys, nl->S))) return st;
+    nl->sys.assign(S, SysHost{});
+    nl->live.assign(S, 0);
+    nl->free_ids.clear();
+    for (int i = 0; i < S; i++) nl->free_ids.insert(i);
+    nl->cell_pool.reset(G);
+    nl->cl_pool.reset(nl->clusters_cap);
+    nl->run_pool.reset(nl->runs_cap);
+    nl->h_desc.assign(S + 1, SysDesc{});
+    cudaStream_t s0 = nullptr;
+    if ((st = dalloc(&nl->d_sys, S + 1))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_sys, 0, sizeof(SysDesc) * (S + 1)));
     if ((st = dalloc(&nl->d_atom_sys, n))) return st;
+    if ((st = fill_int(nl->d_atom_sys, n, S, s0))) return st;
     if ((st = dalloc(&nl->d_cell_sys, G))) return st;
-    SPGNB_CUDA(cudaMemcpy(nl->d_sys, nl->h_desc.data(), sizeof(SysDesc) * nl->S, cudaMemcpyHostToDevice));
-    SPGNB_CUDA(cudaMemcpy(nl->d_atom_sys, atom_sys.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
-    SPGNB_CUDA(cudaMemcpy(nl->d_cell_sys, cell_sys.data(), sizeof(int) * G, cudaMemcpyHostToDevice));
+    if ((st = fill_int(nl->d_cell_sys, G, S, s0))) return st;
     if ((st = dalloc(&nl->d_run_start, G + 1))) return st;
-    if ((st = dalloc(&nl->d_runs, runs.size()))) return st;
-    SPGNB_CUDA(cudaMemcpy(nl->d_run_start, start.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice));
-    SPGNB_CUDA(cudaMemcpy(nl->d_runs, runs.data(), sizeof(int2) * runs.size(), cudaMemcpyHostToDevice));
+    SPGNB_CUDA(cudaMemset(nl->d_run_start, 0, sizeof(int) * (G + 1)));
+    if ((st = dalloc(&nl->d_runs, nl->runs_cap))) return st;
     if ((st = dalloc(&nl->d_cell_count, G))) return st;
     if ((st = dalloc(&nl->d_cell_cursor, G))) return st;
     if ((st = dalloc(&nl->d_cell_cl, G))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_cell_cl, 0, sizeof(int2) * G));
-    if ((st = dalloc(&nl->d_need, nl->S))) return st;
-    if ((st = dalloc(&nl->d_prune, nl->S))) return st;
-    if ((st = dalloc(&nl->d_ncl, nl->S))) return st;
-    SPGNB_CUDA(cudaMemset(nl->d_need, 0, sizeof(int) * nl->S));
-    SPGNB_CUDA(cudaMemset(nl->d_prune, 0, sizeof(int) * nl->S));
-    SPGNB_CUDA(cudaMemset(nl->d_ncl, 0, sizeof(int) * nl->S));
     SPGNB_CUDA(cudaMemset(nl->d_cell_count, 0, sizeof(int) * G));
     SPGNB_CUDA(cudaMemset(nl->d_cell_cursor, 0, sizeof(int) * G));
+    if ((st = dalloc(&nl->d_live, S + 1))) return st;
+    if ((st = dalloc(&nl->d_need, S + 1))) return st;
+    if ((st = dalloc(&nl->d_prune, S + 1))) return st;
+    if ((st = dalloc(&nl->d_ncl, S + 1))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_live, 0, sizeof(int) * (S + 1)));
+    SPGNB_CUDA(cudaMemset(nl->d_need, 0, sizeof(int) * (S + 1)));
+    SPGNB_CUDA(cudaMemset(nl->d_prune, 0, sizeof(int) * (S + 1)));
+    SPGNB_CUDA(cudaMemset(nl->d_ncl, 0, sizeof(int) * (S + 1)));
     if ((st = dalloc(&nl->d_atom_cell, n))) return st;
     if ((st = dalloc(&nl->d_atom_shift, n))) return st;
     if ((st = dalloc(&nl->d_wrapped, n))) return st;
@@ -981,6 +1006,7 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemset(nl->d_slot_atom, 0xff, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_slot_x0, slots))) return st;
     if ((st = dalloc(&nl->d_slot_d0, slots))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_slot_d0, 0, sizeof(float4) * slots));
     if ((st = dalloc(&nl->d_slot_ex, slots))) return st;
     if ((st = dalloc(&nl->d_slot_count, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_slot_count, 0, sizeof(int) * slots));
@@ -989,7 +1015,7 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemset(nl->d_pcount, 0, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_cl_cell, nl->clusters_cap))) return st;
     if ((st = dalloc(&nl->d_cl_sys, nl->clusters_cap))) return st;
-    SPGNB_CUDA(cudaMemcpy(nl->d_cl_sys, cl_sys.data(), sizeof(int) * nl->clusters_cap, cudaMemcpyHostToDevice));
+    if ((st = fill_int(nl->d_cl_sys, nl->clusters_cap, S, s0))) return st;
     if ((st = dalloc(&nl->d_cl_u, nl->clusters_cap))) return st;
     // one more: the null cluster of the padding slot (centre 0)
     if ((st = dalloc(&nl->d_cl_q, nl->clusters_cap + 1))) return st;
@@ -1012,93 +1038,79 @@ int alloc_nl(spgnb_nl* nl)
     return SPGNB_OK;
 }
 
-// Capacities from the densest system: neighbour clusters within
-// rc + skin + 6 A of an 8-atom cluster (the table, 1.3x margin), and pruned
-// partners per atom within rc + buffer + 1 A (the lists, 1.3x margin, whole
-// 64-word windows plus one window for the padding).
-void estimate_capacities(spgnb_nl* nl)
-{
-    double per_cluster = 0, per_atom = 0;
-    for (const auto& sh : nl->sys)
-    {
-        const double vol = (double)sh.cell.a11 * sh.cell.a22 * sh.cell.a33;
-        const double rho = sh.atom_count / vol;
-        const double R = sh.cutoff + sh.skin + 6.0;
-        per_cluster = std::max(per_cluster, std::min(4.18879 * R * R * R * rho, (double)sh.atom_count) / kClusterSize);
-        const double buf = nl->opt.prune_buffer > 0.0f ? nl->opt.prune_buffer + 1.0 : sh.skin;
-        const double Rl = sh.cutoff + buf;
-        per_atom = std::max(per_atom, std::min(4.18879 * Rl * Rl * Rl * rho, (double)sh.atom_count));
-    }
-    nl->table_cap = nl->opt.max_entries_per_cluster > 0 ? nl->opt.max_entries_per_cluster
-                                                        : std::max((int)(per_cluster * 1.3) + 64, 128);
-    nl->slot_cap = (((int)(per_atom * 1.3) + 63) & ~63) + 128;
-}
+int table_cap_for(double per_cluster) { return std::max((int)(per_cluster * 1.3) + 64, 128); }
+int slot_cap_for(double per_atom) { return (((int)(per_atom * 1.3) + 63) & ~63) + 128; }
 
+void resolve_options(const spgnb_nl_options* opt, spgnb_nl_options* o)
+{
+    if (opt)
+        *o = *opt;
+    else
+        spgnb_nl_default_options(o);
+    if (o->max_neighbor_numbers <= 0) o->max_neighbor_numbers = 1200;
+    if (!(o->prune_buffer >= 0.0f)) o->prune_buffer = 0.0f;
+}
 
 }  // namespace
 
-int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,
-                    const spgnb_ltmatrix3* rcells, const float* cutoffs, const float* skins,
-                    const spgnb_nl_options* opt, spgnb_nl** out)
+void nl_capacity_for(double atoms_per_A3, double atom_count, float cutoff, float skin, float prune_buffer,
+                     double* table_per_cluster, double* words_per_atom)
+{
+    // neighbour clusters within rc + skin + 6 A of an 8-atom cluster; pruned
+    // partners per atom within rc + buffer + 1 A
+    const double R = cutoff + skin + 6.0;
+    *table_per_cluster = std::min(4.18879 * R * R * R * atoms_per_A3, atom_count) / kClusterSize;
+    const double buf = prune_buffer > 0.0f ? prune_buffer + 1.0 : skin;
+    const double Rl = cutoff + buf;
+    *words_per_atom = std::min(4.18879 * Rl * Rl * Rl * atoms_per_A3, atom_count);
+}
+
+int nl_init_system(SysHost& sh, int atom_count, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, float cutoff,
+                   float skin, int index)
+{
+    if (atom_count <= 0 || !(cutoff > 0.0f) || !(skin >= 0.0f) ||
+        !(cell.a11 > 0.0f && cell.a22 > 0.0f && cell.a33 > 0.0f))
+        return fail(SPGNB_E_ARG, "neighbour list: system %d has bad atoms/cutoff/skin/cell", index);
+    sh = SysHost{};
+    sh.atom_count = atom_count;
+    sh.cell = cell;
+    sh.rcell = rcell;
+    sh.cutoff = cutoff;
+    sh.skin = skin;
+    sh.triclinic = cell.a21 != 0.0f || cell.a31 != 0.0f || cell.a32 != 0.0f;
+    grid_dims(cell, cutoff, skin, sh.dims, &sh.gl);
+    sh.cs2 = sh.gl * sh.gl * 4.0f;
+    if (sh.dims[0] <= 2 || sh.dims[1] <= 2 || sh.dims[2] <= 2)
+        return fail(SPGNB_E_ARG,
+                    "NEIGHBOR_LIST: the box is too small (system %d: grid %dx%dx%d, need >= 3 per dimension)", index,
+                    sh.dims[0], sh.dims[1], sh.dims[2]);
+    return SPGNB_OK;
+}
+
+int nl_system_runs(const SysHost& sh, std::vector<int>& run_start, std::vector<int2>& runs)
+{
+    return build_runs(sh, run_start, runs);
+}
+
+int nl_create_pool(const NLPoolSpec& spec, const spgnb_nl_options* opt, spgnb_nl** out)
 {
     *out = nullptr;
-    if (n_systems <= 0) return fail(SPGNB_E_ARG, "neighbour list: no systems");
+    if (spec.systems <= 0 || spec.atoms <= 0 || spec.cells <= 0 || spec.clusters <= 0 || spec.runs <= 0 ||
+        spec.table_cap <= 0 || spec.slot_cap <= 0)
+        return fail(SPGNB_E_ARG, "neighbour list: empty pool capacities");
+    if (spec.atoms > (1 << 28) || spec.cells >= (1 << 28))
+        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d atoms / %d cells exceed the 2^28 limit", spec.atoms,
+                    spec.cells);
     spgnb_nl* nl = new spgnb_nl();
-    if (opt)
-        nl->opt = *opt;
-    else
-        spgnb_nl_default_options(&nl->opt);
-    if (nl->opt.max_neighbor_numbers <= 0) nl->opt.max_neighbor_numbers = 1200;
-    if (!(nl->opt.prune_buffer >= 0.0f)) nl->opt.prune_buffer = 0.0f;
-    nl->S = n_systems;
-    nl->sys.resize(n_systems);
-    long long begin = 0;
-    for (int s = 0; s < n_systems; s++)
-    {
-        SysHost& sh = nl->sys[s];
-        if (atom_counts[s] <= 0 || !(cutoffs[s] > 0.0f) || !(skins[s] >= 0.0f) ||
-            !(cells[s].a11 > 0.0f && cells[s].a22 > 0.0f && cells[s].a33 > 0.0f))
-        {
-            delete nl;
-            return fail(SPGNB_E_ARG, "neighbour list: system %d has bad atoms/cutoff/skin/cell", s);
-        }
-        sh.atom_begin = (int)begin;
-        sh.atom_count = atom_counts[s];
-        begin += atom_counts[s];
-        sh.cell = cells[s];
-        sh.rcell = rcells[s];
-        sh.cutoff = cutoffs[s];
-        sh.skin = skins[s];
-        sh.triclinic = cells[s].a21 != 0.0f || cells[s].a31 != 0.0f || cells[s].a32 != 0.0f;
-        grid_dims(cells[s], cutoffs[s], skins[s], sh.dims, &sh.gl);
-        sh.cs2 = sh.gl * sh.gl * 4.0f;
-        if (sh.dims[0] <= 2 || sh.dims[1] <= 2 || sh.dims[2] <= 2)
-        {
-            const int d0 = sh.dims[0], d1 = sh.dims[1], d2 = sh.dims[2];
-            delete nl;
-            return fail(SPGNB_E_ARG,
-                        "NEIGHBOR_LIST: the box is too small (system %d: grid %dx%dx%d, need >= 3 per dimension)", s,
-                        d0, d1, d2);
-        }
-    }
-    if (begin > (1LL << 28))
-    {
-        delete nl;
-        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %lld atoms exceed the 2^28 limit", begin);
-    }
-    nl->n_cap = (int)begin;
-    nl->cutoff = nl->sys[0].cutoff;
-    nl->skin = nl->sys[0].skin;
-    nl->grid_length = nl->sys[0].gl;
-    nl->cs2 = nl->sys[0].cs2;
-    nl->cell = nl->sys[0].cell;
-    nl->rcell = nl->sys[0].rcell;
-    nl->triclinic = false;  // any system: the force kernel's box-shape variant
-    for (const auto& sh : nl->sys) nl->triclinic = nl->triclinic || sh.triclinic;
-    memcpy(nl->dims, nl->sys[0].dims, sizeof(nl->dims));
-    nl->prune_rc = 0.0f;
-    for (const auto& sh : nl->sys) nl->prune_rc = std::max(nl->prune_rc, sh.cutoff);
-    estimate_capacities(nl);
+    resolve_options(opt, &nl->opt);
+    nl->S = spec.systems;
+    nl->n_cap = spec.atoms;
+    nl->G = spec.cells;
+    nl->clusters_cap = spec.clusters;
+    nl->runs_cap = spec.runs;
+    nl->table_cap = nl->opt.max_entries_per_cluster > 0 ? nl->opt.max_entries_per_cluster : spec.table_cap;
+    nl->slot_cap = spec.slot_cap;
+    nl->prune_rc = spec.prune_rc;
     const int st = alloc_nl(nl);
     if (st)
     {
@@ -1110,28 +1122,226 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
     return SPGNB_OK;
 }
 
+int nl_admit(spgnb_nl* nl, SysHost sh, const std::vector<int>* run_start, const std::vector<int2>* runs,
+             cudaStream_t s, int* id)
+{
+    int st;
+    std::vector<int> start_own;
+    std::vector<int2> runs_own;
+    if (!run_start || !runs)
+    {
+        if ((st = build_runs(sh, start_own, runs_own))) return st;
+        run_start = &start_own;
+        runs = &runs_own;
+    }
+    const int G = sh.cells();
+    if ((int)run_start->size() != G + 1) return fail(SPGNB_E_ARG, "nl_admit: run table of the wrong size");
+    if (sh.atom_begin < 0 || (long long)sh.atom_begin + sh.atom_count > nl->n_cap)
+        return fail(SPGNB_E_ARG, "nl_admit: atoms outside the pool");
+    if (nl->free_ids.empty()) return SPGNB_E_OOM;
+    const long long cl_cap = sh.atom_count / kClusterSize + G + 1;
+    const long long cb = nl->cell_pool.alloc(G + 1);
+    if (cb < 0) return SPGNB_E_OOM;
+    const long long clb = nl->cl_pool.alloc(cl_cap);
+    if (clb < 0)
+    {
+        nl->cell_pool.release(cb, G + 1);
+        return SPGNB_E_OOM;
+    }
+    const long long nr = (long long)runs->size();
+    const long long rb = nl->run_pool.alloc(nr);
+    if (rb < 0)
+    {
+        nl->cl_pool.release(clb, cl_cap);
+        nl->cell_pool.release(cb, G + 1);
+        return SPGNB_E_OOM;
+    }
+    const int sid = *nl->free_ids.begin();
+    nl->free_ids.erase(nl->free_ids.begin());
+    sh.cell_begin = (int)cb;
+    sh.cl_begin = (int)clb;
+    sh.cl_cap = (int)cl_cap;
+    sh.run_begin = rb;
+    sh.run_count = nr;
+    std::vector<int2> ra(nr);
+    for (long long k = 0; k < nr; k++) ra[k] = make_int2((*runs)[k].x + (int)cb, (*runs)[k].y + (int)cb);
+    std::vector<int> sa(G + 1);
+    for (int g = 0; g <= G; g++) sa[g] = (*run_start)[g] + (int)rb;
+    nl->h_desc[sid] = make_desc(sh, nl->opt.skin_permit);
+    nl->h_desc[sid].prune_r2 = prune_r2_of(nl->prune_rc, nl->opt.prune_buffer);
+    // (pageable sources: the copies are staged before these calls return)
+    SPGNB_CUDA(cudaMemcpyAsync(nl->d_sys + sid, &nl->h_desc[sid], sizeof(SysDesc), cudaMemcpyHostToDevice, s));
+    if (nr) SPGNB_CUDA(cudaMemcpyAsync(nl->d_runs + rb, ra.data(), sizeof(int2) * nr, cudaMemcpyHostToDevice, s));
+    SPGNB_CUDA(cudaMemcpyAsync(nl->d_run_start + cb, sa.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, s));
+    if ((st = fill_int(nl->d_atom_sys + sh.atom_begin, sh.atom_count, sid, s))) return st;
+    if ((st = fill_int(nl->d_cell_sys + cb, G, sid, s))) return st;
+    if ((st = fill_int(nl->d_cl_sys + clb, cl_cap, sid, s))) return st;
+    k_sys_flags<<<1, 1, 0, s>>>(sid, 1, nl->d_live, nl->d_need, nl->d_prune, nl->d_ncl);
+    SPGNB_CHECK_LAUNCH("k_sys_flags");
+    nl->sys[sid] = sh;
+    nl->live[sid] = 1;
+    nl->triclinic = nl->triclinic || sh.triclinic;
+    *id = sid;
+    return SPGNB_OK;
+}
+
+int nl_retire(spgnb_nl* nl, int id, cudaStream_t s)
+{
+    int st;
+    if (id < 0 || id >= nl->S || !nl->live[id]) return fail(SPGNB_E_ARG, "nl_retire: system %d is not in the list", id);
+    const SysHost sh = nl->sys[id];
+    const int G = sh.cells();
+    const size_t slot0 = (size_t)sh.cl_begin * kClusterSize, nslots = (size_t)sh.cl_cap * kClusterSize;
+    if ((st = fill_int(nl->d_atom_sys + sh.atom_begin, sh.atom_count, nl->S, s))) return st;
+    SPGNB_CUDA(cudaMemsetAsync(nl->d_atom_slot + sh.atom_begin, 0xff, sizeof(int) * sh.atom_count, s));
+    if ((st = fill_int(nl->d_cell_sys + sh.cell_begin, G, nl->S, s))) return st;
+    SPGNB_CUDA(cudaMemsetAsync(nl->d_cell_count + sh.cell_begin, 0, sizeof(int) * (G + 1), s));
+    SPGNB_CUDA(cudaMemsetAsync(nl->d_cell_cursor + sh.cell_begin, 0, sizeof(int) * (G + 1), s));
+    if ((st = fill_int(nl->d_cl_sys + sh.cl_begin, sh.cl_cap, nl->S, s))) return st;
+    SPGNB_CUDA(cudaMemsetAsync(nl->d_slot_atom + slot0, 0xff, sizeof(int) * nslots, s));
+    SPGNB_CUDA(cudaMemsetAsync(nl->d_slot_count + slot0, 0, sizeof(int) * nslots, s));
+    SPGNB_CUDA(cudaMemsetAsync(nl->d_pcount + slot0, 0, sizeof(int) * nslots, s));
+    SPGNB_CUDA(cudaMemsetAsync(nl->d_tcount + sh.cl_begin, 0, sizeof(int) * sh.cl_cap, s));
+    k_sys_flags<<<1, 1, 0, s>>>(id, 0, nl->d_live, nl->d_need, nl->d_prune, nl->d_ncl);
+    SPGNB_CHECK_LAUNCH("k_sys_flags");
+    nl->cell_pool.release(sh.cell_begin, G + 1);
+    nl->cl_pool.release(sh.cl_begin, sh.cl_cap);
+    nl->run_pool.release(sh.run_begin, sh.run_count);
+    nl->free_ids.insert(id);
+    nl->live[id] = 0;
+    nl->sys[id] = SysHost{};
+    nl->h_desc[id] = SysDesc{};
+    nl->triclinic = false;
+    for (int k = 0; k < nl->S; k++) nl->triclinic = nl->triclinic || (nl->live[k] && nl->sys[k].triclinic);
+    return SPGNB_OK;
+}
+
+int nl_prune_all(spgnb_nl* nl, cudaStream_t s)
+{
+    k_prune_live<<<(nl->S + 255) / 256, 256, 0, s>>>(nl->S, nl->d_live, nl->d_prune, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_prune_live");
+    return SPGNB_OK;
+}
+
+size_t nl_device_bytes(const spgnb_nl* nl)
+{
+    const size_t n = nl->n_cap, G = nl->G, S = nl->S + 1, C = nl->clusters_cap, slots = C * kClusterSize;
+    size_t b = 0;
+    b += n * (4 + 4 + 4 + 16 + 4);                                   // atom system, cell, shift, wrapped, slot
+    b += slots * (4 + 4 + 16 + 16 + 8 + 4 + 4 + 16);                 // per-slot arrays
+    b += slots * (size_t)nl->slot_cap * 4;                           // pruned lists
+    b += C * (4 + 4 + 16 + 16 + 16 + 4) + 16;                        // per-cluster arrays
+    b += C * (size_t)nl->table_cap * (16 + 8);                       // neighbour tables
+    b += G * (4 + 4 + 4 + 8 + 4) + 4 + (size_t)nl->runs_cap * 8;     // cells and runs
+    b += S * (sizeof(SysDesc) + 16);
+    if (nl->opt.export_atom_groups) b += n * sizeof(spgnb_atom_group) + n * (size_t)nl->opt.max_neighbor_numbers * 4;
+    return b;
+}
+
+int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,
+                    const spgnb_ltmatrix3* rcells, const float* cutoffs, const float* skins,
+                    const spgnb_nl_options* opt, spgnb_nl** out)
+{
+    *out = nullptr;
+    if (n_systems <= 0) return fail(SPGNB_E_ARG, "neighbour list: no systems");
+    int st;
+    spgnb_nl_options o;
+    resolve_options(opt, &o);
+    std::vector<SysHost> hs(n_systems);
+    std::vector<std::vector<int>> starts(n_systems);
+    std::vector<std::vector<int2>> runs(n_systems);
+    long long atoms = 0, cellsum = 0, clsum = 0, runsum = 0;
+    double per_cluster = 0, per_atom = 0;
+    float rcmax = 0;
+    for (int s = 0; s < n_systems; s++)
+    {
+        if ((st = nl_init_system(hs[s], atom_counts[s], cells[s], rcells[s], cutoffs[s], skins[s], s))) return st;
+        hs[s].atom_begin = (int)std::min<long long>(atoms, 0x7fffffff);
+        atoms += atom_counts[s];
+        if ((st = build_runs(hs[s], starts[s], runs[s]))) return st;
+        const int G = hs[s].cells();
+        cellsum += G + 1;
+        clsum += atom_counts[s] / kClusterSize + G + 1;
+        runsum += (long long)runs[s].size();
+        const double vol = (double)cells[s].a11 * cells[s].a22 * cells[s].a33;
+        double pc, pa;
+        nl_capacity_for(atom_counts[s] / vol, atom_counts[s], cutoffs[s], skins[s], o.prune_buffer, &pc, &pa);
+        per_cluster = std::max(per_cluster, pc);
+        per_atom = std::max(per_atom, pa);
+        rcmax = std::max(rcmax, cutoffs[s]);
+    }
+    if (atoms > (1LL << 28)) return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %lld atoms exceed the 2^28 limit", atoms);
+    if ((clsum + 1) * kClusterSize > kMaxSlots)
+        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %lld atoms in %lld cells exceed the %d-slot limit of the lists",
+                    atoms, cellsum, kMaxSlots);
+    NLPoolSpec spec;
+    spec.systems = n_systems;
+    spec.atoms = (int)atoms;
+    spec.cells = (int)cellsum;
+    spec.clusters = (int)clsum;
+    spec.runs = std::max(1LL, runsum);
+    spec.table_cap = table_cap_for(per_cluster);
+    spec.slot_cap = slot_cap_for(per_atom);
+    spec.prune_rc = rcmax;
+    spgnb_nl* nl = nullptr;
+    if ((st = nl_create_pool(spec, &o, &nl))) return st;
+    cudaStream_t s0 = stream();
+    for (int s = 0; s < n_systems; s++)
+    {
+        int id = -1;
+        st = nl_admit(nl, hs[s], &starts[s], &runs[s], s0, &id);
+        if (st || id != s)
+        {
+            free_nl(nl);
+            delete nl;
+            return st ? (st == SPGNB_E_OOM ? fail(st, "neighbour list: pool sizing error") : st)
+                      : fail(SPGNB_E_STATE, "neighbour list: unexpected system id");
+        }
+    }
+    cudaError_t e = cudaStreamSynchronize(s0);
+    if (e != cudaSuccess)
+    {
+        free_nl(nl);
+        delete nl;
+        return cuda_fail(e, "nl_create_multi");
+    }
+    nl->cutoff = nl->sys[0].cutoff;
+    nl->skin = nl->sys[0].skin;
+    nl->grid_length = nl->sys[0].gl;
+    nl->cs2 = nl->sys[0].cs2;
+    nl->cell = nl->sys[0].cell;
+    nl->rcell = nl->sys[0].rcell;
+    memcpy(nl->dims, nl->sys[0].dims, sizeof(nl->dims));
+    *out = nl;
+    return SPGNB_OK;
+}
+
 // Queues one rebuild, or the device-side decision about one, on stream s.
-// how: kBuildForced rebuilds every system, kBuildSkin lets each system's
-// skin check decide, kBuildInterval rebuilds all when the device step counter
-// (advanced by this call) reaches a multiple of `interval`.
+// how: kBuildForced rebuilds every live system, kBuildSkin lets each
+// system's skin check decide, kBuildInterval rebuilds a system when its step
+// count (aux) reaches a multiple of `interval`, kBuildPreset rebuilds the
+// systems flagged in aux.
 int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
-                   const int* ex_list, const int* ex_num, int how, cudaStream_t s, int* d_step, int interval)
+                   const int* ex_list, const int* ex_num, int how, cudaStream_t s, const int* d_aux, int interval,
+                   const int* d_active)
 {
     const int sms = num_sms();
     const int slots_cap = nl->clusters_cap * kClusterSize;
     const int ccap = nl->clusters_cap;
-    if (how == kBuildForced)
+    const int sb = (nl->S + 255) / 256;
+    if (how != kBuildSkin)
     {
-        k_set_need<<<(nl->S + 255) / 256, 256, 0, s>>>(nl->S, nl->d_need, nl->d_counters);
-        SPGNB_CHECK_LAUNCH("k_set_need");
-    }
-    else if (how == kBuildInterval)
-    {
-        if (nl->S > 1024) return fail(SPGNB_E_UNSUPPORTED, "interval refresh: more than 1024 systems");
-        k_interval_need<<<1, 1024, 0, s>>>(nl->S, interval, d_step, nl->d_need, nl->d_counters);
-        SPGNB_CHECK_LAUNCH("k_interval_need");
-        k_step_tick<<<1, 1, 0, s>>>(d_step);
-        SPGNB_CHECK_LAUNCH("k_step_tick");
+        if ((how == kBuildInterval || how == kBuildPreset) && !d_aux)
+            return fail(SPGNB_E_ARG, "nl_queue_build: per-system steps or flags missing");
+        SPGNB_CUDA(cudaMemsetAsync(nl->d_counters + kCntNeed, 0, sizeof(int), s));
+        if (how == kBuildForced)
+            k_set_need<<<sb, 256, 0, s>>>(nl->S, nl->d_live, d_active, nl->d_need, nl->d_counters);
+        else if (how == kBuildInterval)
+            k_interval_need<<<sb, 256, 0, s>>>(nl->S, interval, d_aux, nl->d_live, d_active, nl->d_need,
+                                               nl->d_counters);
+        else
+            k_need_preset<<<sb, 256, 0, s>>>(nl->S, d_aux, nl->d_live, nl->d_need, nl->d_counters);
+        SPGNB_CHECK_LAUNCH("k_need");
     }
     else
     {
@@ -1192,13 +1402,11 @@ int nl_set_prune_rc(spgnb_nl* nl, float rc, cudaStream_t s)
 {
     if (!(rc > nl->prune_rc)) return SPGNB_OK;
     nl->prune_rc = rc;
-    for (auto& d : nl->h_desc) d.prune_r2 = prune_r2_of(rc, nl->opt.prune_buffer);
+    for (int k = 0; k < nl->S; k++)
+        if (nl->live[k]) nl->h_desc[k].prune_r2 = prune_r2_of(rc, nl->opt.prune_buffer);
     SPGNB_CUDA(cudaMemcpyAsync(nl->d_sys, nl->h_desc.data(), sizeof(SysDesc) * nl->S, cudaMemcpyHostToDevice, s));
-    SPGNB_CUDA(cudaStreamSynchronize(s));
-    const std::vector<int> ones(nl->S, 1);
-    SPGNB_CUDA(cudaMemcpyAsync(nl->d_prune, ones.data(), sizeof(int) * nl->S, cudaMemcpyHostToDevice, s));
-    const int one = 1;
-    SPGNB_CUDA(cudaMemcpyAsync(nl->d_counters + kCntPrune, &one, sizeof(int), cudaMemcpyHostToDevice, s));
+    int st = nl_prune_all(nl, s);
+    if (st) return st;
     SPGNB_CUDA(cudaStreamSynchronize(s));
     return SPGNB_OK;
 }

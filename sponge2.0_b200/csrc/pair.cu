@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
                 const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0, const int4* __restrict__ cl_q,
                 const float4* __restrict__ pos, const int* __restrict__ ptype,
                 const float2* __restrict__ gtable, int table_size, float3* __restrict__ frc,
-                long long* __restrict__ totals, OwnerMap om, PerAtomOut pa)
+                long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, const int* __restrict__ only)
 {
     extern __shared__ float2 table[];           // {-A, B}
     __shared__ long long red[kForceWarps][8];  // per-warp fixed-point totals
@@ -418,6 +418,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
         const int n = pcount[s];  // a multiple of 64
         if (n == 0) continue;
         const int sy = cl_sys[c];
+        if (only && !only[sy]) continue;
         if (EN && sy != cur_sys)
         {
             // totals belong to one system each: flush this warp's share
@@ -981,6 +982,7 @@ struct FastArgs
     long long* totals;
     OwnerMap om;
     PerAtomOut pa;
+    const int* only;
 };
 
 template <int M, int F, bool T>
@@ -990,7 +992,7 @@ int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
     const int grid = std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T>, kForceWarps * 32, smem), nl->clusters_cap));
     k_pair_fast<M, F, T><<<grid, kForceWarps * 32, smem, s>>>(
         x.p0, x.fps, nl->d_sys, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table,
-        x.table_size, x.frc, x.totals, x.om, x.pa);
+        x.table_size, x.frc, x.totals, x.om, x.pa, x.only);
     SPGNB_CHECK_LAUNCH("k_pair_fast");
     return SPGNB_OK;
 }
@@ -1049,7 +1051,7 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
     pair_events(&ev0, &ev1);
     if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
     const FastArgs fa{in.p0, in.d_fps, nl, in.slot_pos, in.slot_type, in.table, in.table_size, in.frc,
-                      in.totals, in.om, in.pa};
+                      in.totals, in.om, in.pa, in.only};
     const int st = launch_fast_any(fa, in.mode, in.fit, nl->triclinic, sizeof(float2) * in.table_size, s);
     if (st) return st;
     if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));

@@ -31,6 +31,8 @@ EXPORTED = [
     "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_stream",
     "spgnb_batch_check_overflow", "spgnb_batch_set_thermostat",
     "spgnb_batch_destroy",
+    "spgnb_batch_pool_default_options", "spgnb_batch_create_pool", "spgnb_batch_admit", "spgnb_batch_retire",
+    "spgnb_batch_evaluate", "spgnb_batch_progress", "spgnb_batch_capacity",
 ]
 
 
@@ -71,6 +73,12 @@ class BatchOptions(C.Structure):
     _fields_ = [("dt", C.c_float), ("water_doh", C.c_float), ("water_dhh", C.c_float), ("skin_permit", C.c_float),
                 ("prune_buffer", C.c_float), ("steps_per_graph", C.c_int), ("use_graphs", C.c_int),
                 ("thermostat_tau", C.c_float), ("temperature", C.c_float), ("refresh_interval", C.c_int)]
+
+
+class PoolOptions(C.Structure):
+    _fields_ = [("max_systems", C.c_int), ("max_atoms", C.c_int), ("max_excluded", C.c_longlong),
+                ("max_waters", C.c_int), ("max_cutoff", C.c_float), ("min_cutoff", C.c_float), ("skin", C.c_float),
+                ("density", C.c_float), ("hbm_budget_bytes", C.c_double)]
 
 
 class NLStats(C.Structure):
@@ -122,6 +130,15 @@ def lib():
     L.spgnb_batch_stream.argtypes = [vp]
     L.spgnb_batch_stream.restype = vp
     L.spgnb_batch_destroy.argtypes = [vp]
+    L.spgnb_batch_pool_default_options.argtypes = [C.POINTER(PoolOptions)]
+    L.spgnb_batch_pool_default_options.restype = None
+    L.spgnb_batch_create_pool.argtypes = [C.POINTER(PoolOptions), i, vp, vp, C.POINTER(BatchOptions), C.POINTER(vp)]
+    L.spgnb_batch_admit.argtypes = [vp, C.POINTER(BatchSystem), i, C.POINTER(i)]
+    L.spgnb_batch_retire.argtypes = [vp, i]
+    L.spgnb_batch_evaluate.argtypes = [vp, vp, i]
+    L.spgnb_batch_progress.argtypes = [vp, vp, vp]
+    L.spgnb_batch_capacity.argtypes = [vp, C.POINTER(i), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
+                                       C.POINTER(d)]
     L.spgnb_lj_create.argtypes = [i, i, vp, vp, vp, f, C.POINTER(vp)]
     L.spgnb_lj_get_local.argtypes = [vp, vp, i, i]
     L.spgnb_lj_pme_direct_force.argtypes = [vp, i, i, i, i, vp, vp, vp, M, M, vp, f, i, vp, i, vp, vp]

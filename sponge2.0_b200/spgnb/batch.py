@@ -1,10 +1,13 @@
 """Batched engine: many independent systems stepped together on one GPU.
 
-``Batch`` wraps the ``spgnb_batch_*`` C ABI.  Every system keeps its own box,
-cutoff, skin, Ewald beta, exclusions and rigid waters; all share one LJ type
-table.  A step is leap-frog velocity Verlet with SETTLE, the per-system
-skin-triggered neighbour-list update and one LJ + PME direct-space force
-launch over all systems, replayed from captured CUDA graphs.
+``Batch`` wraps the ``spgnb_batch_*`` C ABI for a fixed set of systems and
+``Pool`` for a pool into which systems are admitted and from which they are
+retired while the others run (continuous batching).  Every system keeps its
+own box, cutoff, skin, Ewald beta, exclusions and rigid waters; all share one
+LJ type table.  A step is leap-frog velocity Verlet with SETTLE, the
+per-system skin-triggered neighbour-list update and one LJ + PME direct-space
+force launch over all systems, replayed from captured CUDA graphs.  A
+system's results are bitwise the same alone and in any mix.
 """
 from __future__ import annotations
 
@@ -12,7 +15,9 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import BatchOptions, BatchSystem, LTMatrix3, check, lib
+from ._lib import SPGNB_OK, BatchOptions, BatchSystem, LTMatrix3, PoolOptions, SpgnbError, check, lib
+
+SPGNB_E_OOM = 2
 
 
 def default_options(**kw):
@@ -23,67 +28,64 @@ def default_options(**kw):
     return o
 
 
+def pool_options(**kw):
+    o = PoolOptions()
+    lib().spgnb_batch_pool_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
 def _ptr(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
 
-class Batch:
-    """Systems from ``spgnb.systems`` (same ``pair_A``/``pair_B`` table)."""
+def _fill(y, s, keep):
+    """Fill a BatchSystem from a ``spgnb.systems`` system; arrays go to keep."""
+    crd = np.ascontiguousarray(s.crd, np.float32)
+    vel = np.ascontiguousarray(s.vel if s.vel is not None else np.zeros_like(s.crd), np.float32)
+    charge = np.ascontiguousarray(s.charge, np.float32)
+    mass = np.ascontiguousarray(s.mass, np.float32)
+    atype = np.ascontiguousarray(s.atom_type, np.int32)
+    es = np.ascontiguousarray(s.excl_start, np.int32)
+    en = np.ascontiguousarray(s.excl_numbers, np.int32)
+    el = np.ascontiguousarray(s.excl_list if len(s.excl_list) else np.zeros(1, np.int32), np.int32)
+    keep += [crd, vel, charge, mass, atype, es, en, el]
+    y.atom_numbers = s.n
+    y.cutoff = s.cutoff
+    y.skin = s.skin
+    y.pme_beta = s.beta
+    y.cell = LTMatrix3.of(s.cell)
+    y.rcell = LTMatrix3.of(s.rcell)
+    y.h_crd, y.h_vel, y.h_charge, y.h_mass = _ptr(crd), _ptr(vel), _ptr(charge), _ptr(mass)
+    y.h_atom_type, y.h_excluded_start, y.h_excluded_numbers = _ptr(atype), _ptr(es), _ptr(en)
+    y.h_excluded_list = _ptr(el)
+    y.excluded_total = len(s.excl_list)
+    y.water_begin = s.n_solute
+    y.water_numbers = s.n_waters
 
-    def __init__(self, systems, options=None, **kw):
-        L = lib()
-        self.systems = list(systems)
-        s0 = self.systems[0]
-        for s in self.systems[1:]:
-            if s.n_types != s0.n_types or not np.array_equal(s.pair_A, s0.pair_A) or \
-                    not np.array_equal(s.pair_B, s0.pair_B):
-                raise ValueError("the systems of a batch share one LJ type table")
-        self._keep = []
-        arr = (BatchSystem * len(self.systems))()
-        for k, s in enumerate(self.systems):
-            crd = np.ascontiguousarray(s.crd, np.float32)
-            vel = np.ascontiguousarray(s.vel if s.vel is not None else np.zeros_like(s.crd), np.float32)
-            charge = np.ascontiguousarray(s.charge, np.float32)
-            mass = np.ascontiguousarray(s.mass, np.float32)
-            atype = np.ascontiguousarray(s.atom_type, np.int32)
-            es = np.ascontiguousarray(s.excl_start, np.int32)
-            en = np.ascontiguousarray(s.excl_numbers, np.int32)
-            el = np.ascontiguousarray(s.excl_list if len(s.excl_list) else np.zeros(1, np.int32), np.int32)
-            self._keep += [crd, vel, charge, mass, atype, es, en, el]
-            y = arr[k]
-            y.atom_numbers = s.n
-            y.cutoff = s.cutoff
-            y.skin = s.skin
-            y.pme_beta = s.beta
-            y.cell = LTMatrix3.of(s.cell)
-            y.rcell = LTMatrix3.of(s.rcell)
-            y.h_crd, y.h_vel, y.h_charge, y.h_mass = _ptr(crd), _ptr(vel), _ptr(charge), _ptr(mass)
-            y.h_atom_type, y.h_excluded_start, y.h_excluded_numbers = _ptr(atype), _ptr(es), _ptr(en)
-            y.h_excluded_list = _ptr(el)
-            y.excluded_total = len(s.excl_list)
-            y.water_begin = s.n_solute
-            y.water_numbers = s.n_waters
-        self.options = options if options is not None else default_options(**kw)
-        pa = np.ascontiguousarray(s0.pair_A, np.float32)
-        pb = np.ascontiguousarray(s0.pair_B, np.float32)
-        self._keep += [pa, pb]
-        h = C.c_void_p()
-        check(L.spgnb_batch_create(len(self.systems), arr, s0.n_types, _ptr(pa), _ptr(pb),
-                                   C.byref(self.options), C.byref(h)))
-        self.handle = h
-        self.atoms = sum(s.n for s in self.systems)
+
+def _same_table(systems):
+    s0 = systems[0]
+    for s in systems[1:]:
+        if s.n_types != s0.n_types or not np.array_equal(s.pair_A, s0.pair_A) or \
+                not np.array_equal(s.pair_B, s0.pair_B):
+            raise ValueError("the systems of a batch share one LJ type table")
+
+
+class _Common:
+    """Methods shared by Batch and Pool (``self.handle``, ``self.n_ids``)."""
 
     def run(self, steps, energy_interval=0):
         check(lib().spgnb_batch_run(self.handle, int(steps), int(energy_interval)))
 
     def energies(self):
-        """(S, 9): LJ short, LJ long, Coulomb direct, virial a11 a21 a22 a31 a32 a33."""
-        out = np.zeros((len(self.systems), 9), np.float64)
+        """(ids, 9): LJ short, LJ long, Coulomb direct, virial a11 a21 a22 a31 a32 a33."""
+        out = np.zeros((self.n_ids, 9), np.float64)
         check(lib().spgnb_batch_energies(self.handle, _ptr(out)))
         return out
 
-    def download(self, k):
-        n = self.systems[k].n
+    def _download(self, k, n):
         crd = np.zeros((n, 3), np.float32)
         vel = np.zeros((n, 3), np.float32)
         frc = np.zeros((n, 3), np.float32)
@@ -110,6 +112,23 @@ class Batch:
         check(lib().spgnb_batch_autotune(self.handle, int(steps_per_candidate), C.byref(best)))
         return best.value
 
+    def evaluate(self, ids):
+        """Forces, energies and virial now for these systems only."""
+        arr = np.ascontiguousarray(list(ids), np.int32)
+        check(lib().spgnb_batch_evaluate(self.handle, _ptr(arr), len(arr)))
+
+    def progress(self):
+        """(steps done, steps left) per system id; -1 left = unlimited."""
+        d = np.zeros(self.n_ids, np.int32)
+        left = np.zeros(self.n_ids, np.int32)
+        check(lib().spgnb_batch_progress(self.handle, _ptr(d), _ptr(left)))
+        return d, left
+
+    def capacity(self):
+        ms, ma, fa, by = C.c_int(), C.c_longlong(), C.c_longlong(), C.c_double()
+        check(lib().spgnb_batch_capacity(self.handle, C.byref(ms), C.byref(ma), C.byref(fa), C.byref(by)))
+        return {"max_systems": ms.value, "max_atoms": ma.value, "free_atoms": fa.value, "device_bytes": by.value}
+
     @property
     def stream_ptr(self):
         """The batch's cudaStream_t as an integer (torch.cuda.ExternalStream)."""
@@ -125,3 +144,71 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+class Batch(_Common):
+    """Systems from ``spgnb.systems`` (same ``pair_A``/``pair_B`` table), ids 0..n-1."""
+
+    def __init__(self, systems, options=None, **kw):
+        L = lib()
+        self.systems = list(systems)
+        _same_table(self.systems)
+        s0 = self.systems[0]
+        self._keep = []
+        arr = (BatchSystem * len(self.systems))()
+        for k, s in enumerate(self.systems):
+            _fill(arr[k], s, self._keep)
+        self.options = options if options is not None else default_options(**kw)
+        pa = np.ascontiguousarray(s0.pair_A, np.float32)
+        pb = np.ascontiguousarray(s0.pair_B, np.float32)
+        h = C.c_void_p()
+        check(L.spgnb_batch_create(len(self.systems), arr, s0.n_types, _ptr(pa), _ptr(pb),
+                                   C.byref(self.options), C.byref(h)))
+        self._keep = []
+        self.handle = h
+        self.n_ids = len(self.systems)
+        self.atoms = sum(s.n for s in self.systems)
+
+    def download(self, k):
+        return self._download(k, self.systems[k].n)
+
+
+class Pool(_Common):
+    """An empty pool for systems sharing the type table of ``template``.
+
+    ``admit`` returns an id, or None when the pool has no room now."""
+
+    def __init__(self, template, pool=None, options=None, **kw):
+        L = lib()
+        self.pool_options = pool if pool is not None else pool_options()
+        self.options = options if options is not None else default_options(**kw)
+        self.template = template
+        pa = np.ascontiguousarray(template.pair_A, np.float32)
+        pb = np.ascontiguousarray(template.pair_B, np.float32)
+        h = C.c_void_p()
+        check(L.spgnb_batch_create_pool(C.byref(self.pool_options), template.n_types, _ptr(pa), _ptr(pb),
+                                        C.byref(self.options), C.byref(h)))
+        self.handle = h
+        self.n_ids = self.pool_options.max_systems
+        self.members = {}
+
+    def admit(self, system, steps=0):
+        _same_table([self.template, system])
+        keep = []
+        y = BatchSystem()
+        _fill(y, system, keep)
+        i = C.c_int(-1)
+        st = lib().spgnb_batch_admit(self.handle, C.byref(y), int(steps), C.byref(i))
+        if st == SPGNB_E_OOM:
+            return None
+        if st != SPGNB_OK:
+            raise SpgnbError(st, lib().spgnb_last_error().decode())
+        self.members[i.value] = system
+        return i.value
+
+    def retire(self, k):
+        check(lib().spgnb_batch_retire(self.handle, int(k)))
+        self.members.pop(k, None)
+
+    def download(self, k):
+        return self._download(k, self.members[k].n)

@@ -424,5 +424,12 @@ def request_system(req: Request, skin=2.0):
     if not allowed:
         allowed = [max(4.0, L / 2 - skin)]
     rc = float(rng.choice(allowed))
-    return water_system(n_w, L, int(rng.integers(1 << 31)), n_solute=n_sol, cutoff=rc, skin=skin,
-                        name=f"req-{req.rid}", solute_types=shared_solute_types())
+    # a small box can draw a solute arrangement the lattice cannot clear:
+    # draw the placement again (deterministically) until one fits
+    for attempt in range(50):
+        try:
+            return water_system(n_w, L, int(rng.integers(1 << 31)), n_solute=n_sol, cutoff=rc, skin=skin,
+                                name=f"req-{req.rid}", solute_types=shared_solute_types())
+        except RuntimeError:
+            if attempt == 49:
+                raise
