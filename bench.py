@@ -517,7 +517,7 @@ def main():
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None,
                          "traffic": prof.get("bytes_per_launch"),
-                         "kernel": "k_pair_full", "kernel_ms": pair_avg_ms,
+                         "kernel": "k_pair_fast", "kernel_ms": pair_avg_ms,
                          "flop_per_launch": flop_per_launch, "listed_pairs": listed.value,
                          "pairs_in_cutoff": inside.value,
                          "full_list_words": st.full_list_words, "pruned_list_words": st.pruned_list_words,
@@ -551,7 +551,7 @@ def _ltm(m):
 
 def _profile_traffic():
     """DRAM bytes per pair-kernel launch from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_pair_full_mixed96k.json")
+    p = os.path.join(ROOT, "profiles", "k_pair_fast_mixed96k.json")
     if not os.path.exists(p):
         return {}
     try:

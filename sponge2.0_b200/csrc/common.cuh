@@ -147,8 +147,9 @@ struct ForceParams
     int use_fit, n_types, table_begin, pad;
 };
 
-constexpr int kMaxSlots = 1 << 23;   // slot index field of a pruned-list word
-constexpr int kMaxTypes = 256;       // LJ type field of a pruned-list word
+constexpr int kMaxSlots = 1 << 23;   // slots of one list (int offsets into the per-slot regions)
+constexpr int kMaxSystemSlots = 1 << 22;  // slots of one system: the partner field of a pruned-list word
+constexpr int kMaxTypes = 128;       // LJ type field (7 bits) of a pruned-list word
 
 }  // namespace spgnb
 

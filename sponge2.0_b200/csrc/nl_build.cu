@@ -1138,8 +1138,11 @@ int nl_admit(spgnb_nl* nl, SysHost sh, const std::vector<int>* run_start, const 
     if ((int)run_start->size() != G + 1) return fail(SPGNB_E_ARG, "nl_admit: run table of the wrong size");
     if (sh.atom_begin < 0 || (long long)sh.atom_begin + sh.atom_count > nl->n_cap)
         return fail(SPGNB_E_ARG, "nl_admit: atoms outside the pool");
-    if (nl->free_ids.empty()) return SPGNB_E_OOM;
     const long long cl_cap = sh.atom_count / kClusterSize + G + 1;
+    if (cl_cap * kClusterSize > kMaxSystemSlots)
+        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: a system of %d atoms in %d cells exceeds the %d slots of one "
+                                         "system's lists", sh.atom_count, G, kMaxSystemSlots);
+    if (nl->free_ids.empty()) return SPGNB_E_OOM;
     const long long cb = nl->cell_pool.alloc(G + 1);
     if (cb < 0) return SPGNB_E_OOM;
     const long long clb = nl->cl_pool.alloc(cl_cap);

@@ -83,8 +83,8 @@ __device__ __forceinline__ void red_fixed(long long* acc, float v)
 // Per-step slot pack: each slot's offset from the build-time cluster centre
 // moved by the displacement since the build (minimum image in the system's
 // box, so a caller that wraps coordinates between builds is fine), with the
-// charge, and its LJ type.  Slot slots_cap is the null partner that pads the
-// pruned lists: 10^4 A away from everything, charge 0.  With pruning on
+// charge, and its LJ type.  Slot slots_cap is a null slot: 10^4 A away from
+// everything, charge 0.  With pruning on
 // (pref set) the kernel also flags a re-pruning when some atom moved more
 // than half the prune buffer since the last one.
 __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict__ slot_atom,
@@ -136,17 +136,50 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
 }
 
 // Pruning (no reference counterpart; results unchanged).  Runs after every
-// rebuild and whenever some atom moved more than buffer/2 since the last run
-// (the pack kernel checks).  For each atom (one warp) it walks its cluster's neighbour table,
-// expands the atom's partners (mask row) of 32 elements at a time into shared
-// memory, keeps those whose distance is below cutoff + buffer now, in table
-// order, as 32-bit words {partner slot | LJ type << 23 | per-pair image flag
-// << 31}, pads the
-// list to a multiple of 64 words with the null slot, and records the slot
-// offsets it saw.  Any pair within the cutoff before the next pruning was
-// within cutoff + buffer at this one, so the copy misses none.  buffer <= 0
-// keeps every listed pair.  The last block to finish clears the flag.
+// rebuild and whenever some atom of a system moved more than buffer/2 since
+// its last one (the pack kernel checks).  The lists belong to slot pairs: the
+// two atoms of slots 2p and 2p+1 of a cluster share one list, the union of
+// their partners within cutoff + buffer, so the force kernel evaluates both
+// atoms against each partner it loads.  One warp per slot pair walks the
+// cluster's neighbour table, expands the two atoms' mask rows 32 elements at
+// a time into shared memory and keeps, in table order, every partner within
+// cutoff + buffer of either atom, as a 32-bit word
+//   {partner slot - system's first slot (22 bits) | LJ type << 22 |
+//    pairs with the first atom << 29 | with the second << 30 | image flag << 31}
+// (an atom's bit is clear for itself, its exclusions and other
+// non-partners).  The list is padded to a multiple of 32 words with words
+// whose atom bits are clear.  Any pair within the cutoff before the next
+// pruning was within cutoff + buffer at this one, so the copy misses none.
+// buffer <= 0 keeps every listed pair.  The last block to finish clears the
+// flags.
 constexpr int kPruneWarps = 8;
+#ifndef SPGNB_PAIR_WPL
+#define SPGNB_PAIR_WPL 1
+#endif
+constexpr int kWordsPerLane = SPGNB_PAIR_WPL;  // list words a force-kernel lane takes per iteration
+constexpr int kWindow = 32 * kWordsPerLane;    // lists are padded to whole windows
+constexpr int kWordSlotBits = 22;                  // partner slot field of a list word
+constexpr unsigned kWordSlotMask = (1u << kWordSlotBits) - 1u;
+constexpr int kWordTypeShift = 22;                 // 7-bit LJ type
+constexpr unsigned kWordFirst = 1u << 29, kWordSecond = 1u << 30, kWordImage = 1u << 31;
+
+__device__ __forceinline__ float3 pair_offset(float ex, float ey, float ez, float4 pi, float4 pj, bool image,
+                                              const SysDesc& D)
+{
+    float dx = (ex - pi.x) + pj.x;
+    float dy = (ey - pi.y) + pj.y;
+    float dz = (ez - pi.z) + pj.z;
+    if (image)
+    {
+        const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
+        const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
+        const float sz = rintf(dz * D.rcell.a33);
+        dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
+        dy -= sy * D.cell.a22 + sz * D.cell.a32;
+        dz -= sz * D.cell.a33;
+    }
+    return make_float3(dx, dy, dz);
+}
 
 __global__ void __launch_bounds__(kPruneWarps * 32)
     k_prune(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, int clusters_cap,
@@ -156,110 +189,113 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
             int* __restrict__ pcount, unsigned* __restrict__ pwords, int n_sys, int* __restrict__ prune)
 {
     if (counters[kCntPrune] == 0) return;
-    __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];  // {partner slot | image flag, element}
+    __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];  // {partner slot | image flag, element | atom bits}
     __shared__ unsigned long long kept_total;
     const int lane = threadIdx.x & 31;
-    const int a = threadIdx.x >> 5;
-    const int nc = clusters_cap;
-    const unsigned null_word = (unsigned)(clusters_cap * kClusterSize);
-    const int usable = slot_cap - 64;
+    const int w = threadIdx.x >> 5;
+    const int items = clusters_cap * 4;
     if (threadIdx.x == 0) kept_total = 0;
     __syncthreads();
-    uint2* __restrict__ mybuf = buf[a];
-    for (int c = blockIdx.x; c < nc; c += gridDim.x)
+    uint2* __restrict__ mybuf = buf[w];
+    for (int it = blockIdx.x * kPruneWarps + w; it < items; it += gridDim.x * kPruneWarps)
     {
-        if (!prune[cl_sys[c]]) continue;
-        const int s = c * kClusterSize + a;
-        const float4 pi = pos[s];
-        if (lane == 0) pref[s] = pi;
+        const int c = it >> 2, p = it & 3;
+        const int sy = cl_sys[c];
+        if (!prune[sy]) continue;
+        const int s1 = c * kClusterSize + 2 * p;
+        const float4 pi1 = pos[s1], pi2 = pos[s1 + 1];
+        if (lane == 0) pref[s1] = pi1;
+        if (lane == 1) pref[s1 + 1] = pi2;
+        const SysDesc& D = sys[sy];
+        const unsigned slot0 = (unsigned)D.cl_begin * kClusterSize;
+        const ForceParams P = fps ? fps[sy] : p0;
+        const float rp = sqrtf(P.rc2) + buffer + 1e-3f;
+        const float rp2 = buffer > 0.0f ? rp * rp : 3.0e38f;
+        const int T = tcount[c];
+        const float4* __restrict__ tb = tab + (size_t)c * table_cap;
+        const uint2* __restrict__ tm = tmask + (size_t)c * table_cap;
+        unsigned* __restrict__ out_words = pwords + (size_t)s1 * slot_cap;
+        const int usable = 2 * slot_cap - kWindow;
+        const int sh1 = 8 * ((2 * p) & 3), sh2 = 8 * ((2 * p + 1) & 3);
         int kept = 0;
-        unsigned* __restrict__ out_words = pwords + (size_t)s * slot_cap;
+        for (int t0 = 0; t0 < T; t0 += 32)
         {
-            const ForceParams P = fps ? fps[cl_sys[c]] : p0;
-            const float rp = sqrtf(P.rc2) + buffer + 1e-3f;
-            const float rp2 = buffer > 0.0f ? rp * rp : 3.0e38f;
-            const int T = tcount[c];
-            const float4* __restrict__ tb = tab + (size_t)c * table_cap;
-            const uint2* __restrict__ tm = tmask + (size_t)c * table_cap;
-            for (int t0 = 0; t0 < T; t0 += 32)
+            const int t = t0 + lane;
+            unsigned r1 = 0, r2 = 0;
+            float4 e = make_float4(0, 0, 0, 0);
+            if (t < T)
             {
-                const int t = t0 + lane;
-                unsigned row = 0;
-                float4 e = make_float4(0, 0, 0, 0);
-                if (t < T)
-                {
-                    e = tb[t];
-                    const uint2 mm = tm[t];
-                    row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
-                }
-                const int cnt = __popc(row);
-                int incl = cnt;
-                for (int o = 1; o < 32; o <<= 1)
-                {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                const int total = __shfl_sync(0xffffffffu, incl, 31);
-                const int eb = __float_as_int(e.w);
-                const unsigned flag = (eb & (1 << 30)) ? 0x80000000u : 0u;
-                const unsigned base = (unsigned)(eb & 0x3fffffff) | flag;
-                int k = incl - cnt;
-#pragma unroll
-                for (int b = 0; b < kClusterSize; b++)
-                    if ((row >> b) & 1u) mybuf[k++] = make_uint2(base + b, (unsigned)lane);
-                __syncwarp();
-                for (int q0 = 0; q0 < total; q0 += 32)
-                {
-                    const int q = q0 + lane;
-                    const uint2 w = mybuf[q < total ? q : 0];
-                    // the element's centre difference from the lane that read it
-                    const float ex = __shfl_sync(0xffffffffu, e.x, (int)w.y);
-                    const float ey = __shfl_sync(0xffffffffu, e.y, (int)w.y);
-                    const float ez = __shfl_sync(0xffffffffu, e.z, (int)w.y);
-                    bool keep = false;
-                    unsigned out = 0;
-                    if (q < total)
-                    {
-                        const int js = (int)(w.x & 0x7fffffffu);
-                        const float4 pj = pos[js];
-                        const int tj = ptype[js];
-                        float dx = (ex - pi.x) + pj.x;
-                        float dy = (ey - pi.y) + pj.y;
-                        float dz = (ez - pi.z) + pj.z;
-                        if (w.x & 0x80000000u)
-                        {
-                            const SysDesc& D = sys[cl_sys[c]];
-                            const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
-                            const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
-                            const float sz = rintf(dz * D.rcell.a33);
-                            dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
-                            dy -= sy * D.cell.a22 + sz * D.cell.a32;
-                            dz -= sz * D.cell.a33;
-                        }
-                        keep = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, dx * dx)) < rp2;
-                        out = (unsigned)js | ((unsigned)tj << 23) | (w.x & 0x80000000u);
-                    }
-                    const unsigned m = __ballot_sync(0xffffffffu, keep);
-                    if (keep)
-                    {
-                        const int k = kept + __popc(m & ((1u << lane) - 1u));
-                        if (k < usable)
-                            out_words[k] = out;
-                        else
-                            atomicOr(&counters[kCntOverflow], kOvfWords);
-                    }
-                    kept += __popc(m);
-                }
-                __syncwarp();
+                e = tb[t];
+                const uint2 mm = tm[t];
+                const unsigned half = p < 2 ? mm.x : mm.y;
+                r1 = (half >> sh1) & 0xffu;
+                r2 = (half >> sh2) & 0xffu;
             }
+            const unsigned row = r1 | r2;
+            const int cnt = __popc(row);
+            int incl = cnt;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const int eb = __float_as_int(e.w);
+            const unsigned flag = (eb & (1 << 30)) ? kWordImage : 0u;
+            const unsigned base = (unsigned)(eb & 0x3fffffff) | flag;
+            int k = incl - cnt;
+#pragma unroll
+            for (int b = 0; b < kClusterSize; b++)
+                if ((row >> b) & 1u)
+                    mybuf[k++] = make_uint2(base + b, (unsigned)lane | (((r1 >> b) & 1u) << 5) | (((r2 >> b) & 1u) << 6));
+            __syncwarp();
+            for (int q0 = 0; q0 < total; q0 += 32)
+            {
+                const int q = q0 + lane;
+                const uint2 wv = mybuf[q < total ? q : 0];
+                // the element's centre difference from the lane that read it
+                const int src = (int)(wv.y & 31u);
+                const float ex = __shfl_sync(0xffffffffu, e.x, src);
+                const float ey = __shfl_sync(0xffffffffu, e.y, src);
+                const float ez = __shfl_sync(0xffffffffu, e.z, src);
+                bool keep = false;
+                unsigned out = 0;
+                if (q < total)
+                {
+                    const int js = (int)(wv.x & 0x7fffffffu);
+                    const bool img = (wv.x & 0x80000000u) != 0;
+                    const float4 pj = pos[js];
+                    const int tj = ptype[js];
+                    const bool m1 = (wv.y >> 5) & 1u, m2 = (wv.y >> 6) & 1u;
+                    const float3 d1 = pair_offset(ex, ey, ez, pi1, pj, img, D);
+                    const float3 d2 = pair_offset(ex, ey, ez, pi2, pj, img, D);
+                    const float q1 = __fmaf_rn(d1.z, d1.z, __fmaf_rn(d1.y, d1.y, d1.x * d1.x));
+                    const float q2 = __fmaf_rn(d2.z, d2.z, __fmaf_rn(d2.y, d2.y, d2.x * d2.x));
+                    keep = (m1 && q1 < rp2) || (m2 && q2 < rp2);
+                    out = ((unsigned)js - slot0) | ((unsigned)tj << kWordTypeShift) | (m1 ? kWordFirst : 0u) |
+                          (m2 ? kWordSecond : 0u) | (img ? kWordImage : 0u);
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, keep);
+                if (keep)
+                {
+                    const int kk = kept + __popc(m & ((1u << lane) - 1u));
+                    if (kk < usable)
+                        out_words[kk] = out;
+                    else
+                        atomicOr(&counters[kCntOverflow], kOvfWords);
+                }
+                kept += __popc(m);
+            }
+            __syncwarp();
         }
-        // pad to a multiple of 64 words with the null partner
+        // pad to whole windows: the first atom against itself, no atom bit set
         kept = min(kept, usable);
-        const int padded = (kept + 63) & ~63;
-        for (int k = kept + lane; k < padded; k += 32) out_words[k] = null_word;
+        const int padded = (kept + kWindow - 1) & ~(kWindow - 1);
+        for (int k = kept + lane; k < padded; k += 32) out_words[k] = (unsigned)s1 - slot0;
         if (lane == 0)
         {
-            pcount[s] = padded;
+            pcount[s1] = padded;
+            pcount[s1 + 1] = 0;
             atomicAdd(&kept_total, (unsigned long long)kept);
         }
     }
@@ -276,8 +312,8 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
     for (int q = threadIdx.x; q < n_sys; q += blockDim.x) prune[q] = 0;
     if (threadIdx.x == 0)
     {
-        unsigned long long* w = (unsigned long long*)&counters[kCntPWords];
-        *(unsigned long long*)&counters[kCntPWordsLast] = atomicExch(w, 0ull);
+        unsigned long long* wp = (unsigned long long*)&counters[kCntPWords];
+        *(unsigned long long*)&counters[kCntPWordsLast] = atomicExch(wp, 0ull);
         counters[kCntPruneDone] = 0;
         counters[kCntPrune] = 0;
         counters[kCntPrunes] += 1;
@@ -287,14 +323,27 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
 // ------------------------------------------------ packed FP32x2 pair math
 __device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
 
-__device__ __forceinline__ float2 poly5x2(float2 x, const float* c)
+// Fixed (c, c) constants of the packed arithmetic in constant memory, so the
+// FP32x2 instructions read them as constant-bank operands instead of
+// building register pairs each time.
+static __constant__ float2 kPk[5] = {{-0.5f, -0.5f}, {1.5f, 1.5f}, {-1.0f, -1.0f},
+                                     {-1.0f / 12.0f, -1.0f / 12.0f}, {-1.0f / 6.0f, -1.0f / 6.0f}};
+enum PackedConst
 {
-    float2 p = f2(c[5]);
-    p = __ffma2_rn(p, x, f2(c[4]));
-    p = __ffma2_rn(p, x, f2(c[3]));
-    p = __ffma2_rn(p, x, f2(c[2]));
-    p = __ffma2_rn(p, x, f2(c[1]));
-    return __ffma2_rn(p, x, f2(c[0]));
+    kPkMinusHalf = 0,
+    kPkThreeHalves = 1,
+    kPkMinusOne = 2,
+    kPkMinusTwelfth = 3,
+    kPkMinusSixth = 4
+};
+
+__device__ __forceinline__ float2 poly5x2(float2 x, const float2* c)
+{
+    float2 p = __ffma2_rn(c[5], x, c[4]);
+    p = __ffma2_rn(p, x, c[3]);
+    p = __ffma2_rn(p, x, c[2]);
+    p = __ffma2_rn(p, x, c[1]);
+    return __ffma2_rn(p, x, c[0]);
 }
 
 __device__ __forceinline__ float ex2_approx(float x)
@@ -304,40 +353,78 @@ __device__ __forceinline__ float ex2_approx(float x)
     return y;
 }
 
+// The hardware approximations with subnormals flushed (PTX rsqrt.approx.ftz,
+// rcp.approx.ftz): r^2 of a listed pair and the fits' denominators (>= 1)
+// are far from the subnormal range, so the range handling of rsqrtf and
+// __fdividef is not needed.
+__device__ __forceinline__ float rsqrt_approx(float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// One system's pair-function parameters as (v, v) pairs, made once per atom
+// pair and kept in registers over its list.
+struct PairParams2
+{
+    float2 w_scale, nbeta3, nbeta, beta_2_sqrtpi, nb2_log2e;
+    float rc2, beta;
+};
+
+__device__ __forceinline__ PairParams2 pack_params(const ForceParams& pc)
+{
+    PairParams2 q;
+    q.w_scale = f2(pc.w_scale);
+    q.nbeta3 = f2(-pc.beta3);
+    q.nbeta = f2(-pc.beta);
+    q.beta_2_sqrtpi = f2(pc.beta * 1.1283791670955126f);
+    q.nb2_log2e = f2(-pc.beta * pc.beta * 1.4426950408889634f);  // -w log2(e) = -beta^2 r^2 log2(e)
+    q.rc2 = pc.rc2;
+    q.beta = pc.beta;
+    return q;
+}
+
 // pair_scalar for two pairs at once; nA = -A.  Without energies the screened
 // Coulomb force uses the K fit; with energies it uses the M fit and
 // exp(-w): beta^3 K(w) = beta (M(w) - 2/sqrt(pi) exp(-w)) / r^2, so
 //   F_c/qq = (t + beta 2/sqrt(pi) exp(-w)) / r^2,  E_c/qq = t,  t = 1/r - beta M(w).
 template <bool ENERGY, int FIT>
-__device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, float2 B, const ForceParams& pc,
+__device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, float2 B, const PairParams2& pc,
                                                float2& e_lj, float2& e_c)
 {
-    float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
-    const float2 h = __fmul2_rn(__fmul2_rn(r2, f2(-0.5f)), rinv);
-    rinv = __fmul2_rn(rinv, __ffma2_rn(h, rinv, f2(1.5f)));  // one Newton step
+    float2 rinv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
+    const float2 h = __fmul2_rn(__fmul2_rn(r2, kPk[kPkMinusHalf]), rinv);
+    rinv = __fmul2_rn(rinv, __ffma2_rn(h, rinv, kPk[kPkThreeHalves]));  // one Newton step
     const float2 r2inv = __fmul2_rn(rinv, rinv);
     const float2 r6inv = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
     const float2 flj = __fmul2_rn(__fmul2_rn(__ffma2_rn(nA, r6inv, B), r6inv), r2inv);
     float2 fc;
     if (FIT == 1)
     {
-        const float2 x = __fmul2_rn(r2, f2(pc.w_scale));
+        const float2 x = __fmul2_rn(r2, pc.w_scale);
         if (!ENERGY)
         {
-            const float2 kp = poly5x2(x, kEwaldKP), kq = poly5x2(x, kEwaldKQ);
-            const float2 K = make_float2(__fdividef(kp.x, kq.x), __fdividef(kp.y, kq.y));
-            fc = __fmul2_rn(qq, __ffma2_rn(f2(-pc.beta3), K, __fmul2_rn(rinv, r2inv)));
+            const float2 kp = poly5x2(x, kEwaldKP2), kq = poly5x2(x, kEwaldKQ2);
+            const float2 K = __fmul2_rn(kp, make_float2(rcp_approx(kq.x), rcp_approx(kq.y)));
+            fc = __fmul2_rn(qq, __ffma2_rn(pc.nbeta3, K, __fmul2_rn(rinv, r2inv)));
         }
         else
         {
-            const float2 mp = poly5x2(x, kEwaldMP), mq = poly5x2(x, kEwaldMQ);
-            const float2 M = make_float2(__fdividef(mp.x, mq.x), __fdividef(mp.y, mq.y));
-            // -w log2(e) = -beta^2 r^2 log2(e)
-            const float2 wl = __fmul2_rn(r2, f2(-pc.beta * pc.beta * 1.4426950408889634f));
+            const float2 mp = poly5x2(x, kEwaldMP2), mq = poly5x2(x, kEwaldMQ2);
+            const float2 M = __fmul2_rn(mp, make_float2(rcp_approx(mq.x), rcp_approx(mq.y)));
+            const float2 wl = __fmul2_rn(r2, pc.nb2_log2e);
             const float2 E = make_float2(ex2_approx(wl.x), ex2_approx(wl.y));
-            const float2 t = __ffma2_rn(f2(-pc.beta), M, rinv);
+            const float2 t = __ffma2_rn(pc.nbeta, M, rinv);
             e_c = __fmul2_rn(qq, t);
-            fc = __fmul2_rn(__fmul2_rn(qq, r2inv), __ffma2_rn(f2(pc.beta * 1.1283791670955126f), E, t));
+            fc = __fmul2_rn(__fmul2_rn(qq, r2inv), __ffma2_rn(pc.beta_2_sqrtpi, E, t));
         }
     }
     else
@@ -355,8 +442,10 @@ __device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, 
         fc = make_float2(c[0], c[1]);
         if (ENERGY) e_c = make_float2(e[0], e[1]);
     }
-    if (ENERGY) e_lj = __fmul2_rn(__ffma2_rn(nA, __fmul2_rn(r6inv, f2(-1.0f / 12.0f)), __fmul2_rn(B, f2(-1.0f / 6.0f))), r6inv);
-    return __ffma2_rn(fc, f2(-1.0f), flj);
+    if (ENERGY)
+        e_lj = __fmul2_rn(__ffma2_rn(nA, __fmul2_rn(r6inv, kPk[kPkMinusTwelfth]), __fmul2_rn(B, kPk[kPkMinusSixth])),
+                          r6inv);
+    return __ffma2_rn(fc, kPk[kPkMinusOne], flj);
 }
 
 // A difference of two 22-bit cluster-centre coordinates, wrapped to
@@ -368,54 +457,66 @@ __device__ __forceinline__ float centre_step(int qj, int qi)
     return __int_as_float(((qj - qi + 0x200000) & 0x3fffff) | 0x4b000000) - 10485760.0f;
 }
 
-// Pruned-list force kernel.  A block takes one cluster per pass and each of
-// its eight warps one slot (atom); per iteration a lane takes two adjacent
-// words of a 64-word window (one 8-byte load; the lists are padded to whole
-// windows with the null partner, so no bounds checks) and evaluates both
-// pairs with packed FP32x2 arithmetic, with the next window's words already
-// in flight.  A word names the partner slot, so its offset
-// {delta + displacement, q} and its cluster's 22-bit centre load side by
-// side; dr = (c_j - c_i) * cell / 2^22 + p_j - p_i.  Each lane's partial force is
-// converted to int64 fixed point (2^-32 kcal/mol/A) and reduced over the
-// lanes, so the atom's force does not depend on the reduction order; one
-// lane adds it to the caller's array: no atomics, bitwise reproducible.
+// Pruned-list force kernel.  A warp takes one slot pair (the two atoms of
+// slots 2p, 2p+1 of a cluster) at a time, strided over the grid's warps, and
+// walks the pair's shared list, one word per lane per iteration (32-word
+// windows, the next window's words already in flight).  A word names the
+// partner slot, so its offset {delta + displacement, q} and its cluster's
+// 22-bit centre load side by side, once for both atoms:
+//   dr = (c_j - c_i) * cell / 2^22 + p_j - p_{i1,i2},
+// and the two pairs are evaluated with packed FP32x2 arithmetic; the LJ
+// coefficients of both come from the warp's shared-memory row for the two
+// atoms' types {-A1, -A2, B1, B2} indexed by the partner's type.  Each
+// lane's partial forces are converted to int64 fixed point (2^-32
+// kcal/mol/A) and reduced over the lanes, so an atom's force does not depend
+// on the reduction order; one lane adds it to the caller's array: no
+// atomics, bitwise reproducible.
 //
 // MODE 0: forces.  MODE 1: + energy and virial totals (each pair is seen
 // from both atoms, so the sums are halved).  MODE 2: + per-atom energy and
 // virial of the pairs the atom owns (the lower global index; water sites
 // hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES does).
+#ifndef SPGNB_PAIR_MINB0
+#define SPGNB_PAIR_MINB0 4
+#endif
+#ifndef SPGNB_PAIR_CHUNKED
+#define SPGNB_PAIR_CHUNKED 0
+#endif
 template <int MODE, int FIT, bool TRI>
-__global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ? 3 : 2))
+__global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0 : (MODE == 1 ? 3 : 2))
     k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
                 int n_clusters, int slot_cap,
                 const int* __restrict__ cl_sys, const int* __restrict__ pcount, const unsigned* __restrict__ pwords,
                 const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0, const int4* __restrict__ cl_q,
                 const float4* __restrict__ pos, const int* __restrict__ ptype,
-                const float2* __restrict__ gtable, int table_size, float3* __restrict__ frc,
+                const float2* __restrict__ gtable, int n_types, float3* __restrict__ frc,
                 long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, const int* __restrict__ only)
 {
-    extern __shared__ float2 table[];           // {-A, B}
-    __shared__ long long red[kForceWarps][8];  // per-warp fixed-point totals
-    for (int k = threadIdx.x; k < table_size; k += blockDim.x)
-    {
-        const float2 g = gtable[k];
-        table[k] = make_float2(-g.x, g.y);
-    }
-    if (threadIdx.x < kForceWarps * 8) red[threadIdx.x >> 3][threadIdx.x & 7] = 0;
-    __syncthreads();
+    extern __shared__ float4 rows_all[];        // per warp: n_types rows {-A1, -A2, B1, B2}
+    __shared__ long long red[kForceWarps][8];  // per-warp fixed-point totals (lane 0)
+    __shared__ int row_of[kForceWarps][2];     // table rows the warp's shared row was built from
     constexpr bool EN = MODE >= 1;
     constexpr bool PA = MODE >= 2;
     const int lane = threadIdx.x & 31;
-    const int a = threadIdx.x >> 5;
-    int cur_sys = -1;  // the system red[a] accumulates for (the same sequence in every warp)
-
-    // clusters strided over the blocks: at any moment the blocks are spread
-    // over all systems and the whole of each box (contiguous runs per block
-    // measured slower)
-    for (int c = blockIdx.x; c < n_clusters; c += gridDim.x)
+    const int w = threadIdx.x >> 5;
+    float4* __restrict__ rows = rows_all + w * n_types;
+    if (EN && lane < 8) red[w][lane] = 0;
+    if (lane < 2) row_of[w][lane] = -1;
+    __syncwarp();
+    int cur_sys = -1;              // the system red[w] accumulates for
+    const int items = n_clusters * 4;
+#if SPGNB_PAIR_CHUNKED
+    // each block a contiguous run of clusters (neighbouring clusters share partners in L1)
+    const int per = (items + gridDim.x - 1) / gridDim.x;
+    const int it_end = min(items, (blockIdx.x + 1) * per);
+    for (int it = blockIdx.x * per + w; it < it_end; it += kForceWarps)
+#else
+    for (int it = blockIdx.x * kForceWarps + w; it < items; it += gridDim.x * kForceWarps)
+#endif
     {
-        const int s = c * kClusterSize + a;
-        const int n = pcount[s];  // a multiple of 64
+        const int c = it >> 2;
+        const int s1 = c * kClusterSize + 2 * (it & 3);
+        const int n = pcount[s1];  // a multiple of the window
         if (n == 0) continue;
         const int sy = cl_sys[c];
         if (only && !only[sy]) continue;
@@ -425,22 +526,44 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
             if (lane == 0 && cur_sys >= 0)
                 for (int q = 0; q < 8; q++)
                 {
-                    const long long v = red[a][q];
+                    const long long v = red[w][q];
                     if (v) atomicAdd((unsigned long long*)&totals[8 * cur_sys + q], (unsigned long long)v);
-                    red[a][q] = 0;
+                    red[w][q] = 0;
                 }
             cur_sys = sy;
         }
         const ForceParams P = fps ? fps[sy] : p0;
-        const Cell qc = sys[sy].qcell;
-        const float4 pi = pos[s];
+        const PairParams2 pp = pack_params(P);
+        const SysDesc& D = sys[sy];
+        const Cell qc = D.qcell;
+        const int slot0 = D.cl_begin * kClusterSize;
+        const float4 pi1 = pos[s1], pi2 = pos[s1 + 1];
         const int4 ci = cl_q[c];
-        const int qix = ci.x, qiy = ci.y, qiz = ci.z;
-        int gi = 0;
-        if (PA) gi = __float_as_int(slot_x0[s].w);
-        const int ti = ptype[s] * P.n_types + P.table_begin;
-        const uint2* __restrict__ wl = reinterpret_cast<const uint2*>(pwords + (size_t)s * slot_cap);
-        const float2 npx = f2(-pi.x), npy = f2(-pi.y), npz = f2(-pi.z), qi2 = f2(pi.w);
+        const int r1 = ptype[s1] * n_types + P.table_begin, r2i = ptype[s1 + 1] * n_types + P.table_begin;
+        if (r1 != row_of[w][0] || r2i != row_of[w][1])
+        {
+            __syncwarp();
+            for (int t = lane; t < n_types; t += 32)
+            {
+                const float2 g1 = gtable[r1 + t], g2 = gtable[r2i + t];
+                rows[t] = make_float4(-g1.x, -g2.x, g1.y, g2.y);
+            }
+            if (lane == 0)
+            {
+                row_of[w][0] = r1;
+                row_of[w][1] = r2i;
+            }
+            __syncwarp();
+        }
+        int gi1 = 0, gi2 = 0;
+        if (PA)
+        {
+            gi1 = __float_as_int(slot_x0[s1].w);
+            gi2 = __float_as_int(slot_x0[s1 + 1].w);
+        }
+        const unsigned* __restrict__ wl = pwords + (size_t)s1 * slot_cap;
+        const float2 npx = make_float2(-pi1.x, -pi2.x), npy = make_float2(-pi1.y, -pi2.y),
+                     npz = make_float2(-pi1.z, -pi2.z), qi2 = make_float2(pi1.w, pi2.w);
         float2 fx = f2(0.0f), fy = f2(0.0f), fz = f2(0.0f);
         float2 acc[8], own[8];
 #pragma unroll
@@ -449,61 +572,60 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
             acc[q] = f2(0.0f);
             own[q] = f2(0.0f);
         }
-        uint2 w = wl[lane];
-#pragma unroll 1
-        for (int k0 = 0; k0 < n; k0 += 64)
-        {
-            const uint2 cw = w;
-            if (k0 + 64 < n) w = wl[(k0 + 64) / 2 + lane];
-            const int jA = (int)(cw.x & 0x7fffffu), jB = (int)(cw.y & 0x7fffffu);
-            const float4 pA = pos[jA], pB = pos[jB];
-            const int4 cA = cl_q[jA >> 3], cB = cl_q[jB >> 3];
-            const float2 abA = table[ti + (int)((cw.x >> 23) & 0xffu)];
-            const float2 abB = table[ti + (int)((cw.y >> 23) & 0xffu)];
-            const float2 ux = make_float2(centre_step(cA.x, qix), centre_step(cB.x, qix));
-            const float2 uy = make_float2(centre_step(cA.y, qiy), centre_step(cB.y, qiy));
-            const float2 uz = make_float2(centre_step(cA.z, qiz), centre_step(cB.z, qiz));
-            float2 dx = __ffma2_rn(ux, f2(qc.a11), __fadd2_rn(make_float2(pA.x, pB.x), npx));
-            float2 dy = __ffma2_rn(uy, f2(qc.a22), __fadd2_rn(make_float2(pA.y, pB.y), npy));
-            float2 dz = __ffma2_rn(uz, f2(qc.a33), __fadd2_rn(make_float2(pA.z, pB.z), npz));
+        // one list word: the partner against both atoms
+        auto eval_word = [&](unsigned cw) {
+            const int j = slot0 + (int)(cw & kWordSlotMask);
+            const float4 pj = pos[j];
+            const int4 cj = cl_q[j >> 3];
+            const float4 ab = rows[(cw >> kWordTypeShift) & 0x7fu];
+            const float ux = centre_step(cj.x, ci.x), uy = centre_step(cj.y, ci.y), uz = centre_step(cj.z, ci.z);
+            // the partner in the frame of the pair's cluster centre
+            float sx = __fmaf_rn(ux, qc.a11, pj.x);
+            float sy2 = __fmaf_rn(uy, qc.a22, pj.y);
+            const float sz = __fmaf_rn(uz, qc.a33, pj.z);
             if (TRI)
             {
-                dx = __ffma2_rn(uy, f2(qc.a21), dx);
-                dx = __ffma2_rn(uz, f2(qc.a31), dx);
-                dy = __ffma2_rn(uz, f2(qc.a32), dy);
+                sx = __fmaf_rn(uy, qc.a21, sx);
+                sx = __fmaf_rn(uz, qc.a31, sx);
+                sy2 = __fmaf_rn(uz, qc.a32, sy2);
             }
-            if ((cw.x | cw.y) & 0x80000000u)
+            float2 dx = __fadd2_rn(f2(sx), npx), dy = __fadd2_rn(f2(sy2), npy), dz = __fadd2_rn(f2(sz), npz);
+            if (cw & kWordImage)
             {
-                // small box: these partners need a per-pair image
-                const SysDesc& D = sys[sy];
+                // small box: these pairs need their own image
                 float ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
-                const unsigned wv[2] = {cw.x, cw.y};
                 for (int h = 0; h < 2; h++)
                 {
-                    if (!(wv[h] & 0x80000000u)) continue;
-                    const float sx = rintf(ddx[h] * D.rcell.a11 + ddy[h] * D.rcell.a21 + ddz[h] * D.rcell.a31);
-                    const float sy2 = rintf(ddy[h] * D.rcell.a22 + ddz[h] * D.rcell.a32);
-                    const float sz = rintf(ddz[h] * D.rcell.a33);
-                    ddx[h] -= sx * D.cell.a11 + sy2 * D.cell.a21 + sz * D.cell.a31;
-                    ddy[h] -= sy2 * D.cell.a22 + sz * D.cell.a32;
-                    ddz[h] -= sz * D.cell.a33;
+                    const float tx = rintf(ddx[h] * D.rcell.a11 + ddy[h] * D.rcell.a21 + ddz[h] * D.rcell.a31);
+                    const float ty = rintf(ddy[h] * D.rcell.a22 + ddz[h] * D.rcell.a32);
+                    const float tz = rintf(ddz[h] * D.rcell.a33);
+                    ddx[h] -= tx * D.cell.a11 + ty * D.cell.a21 + tz * D.cell.a31;
+                    ddy[h] -= ty * D.cell.a22 + tz * D.cell.a32;
+                    ddz[h] -= tz * D.cell.a33;
                 }
                 dx = make_float2(ddx[0], ddx[1]);
                 dy = make_float2(ddy[0], ddy[1]);
                 dz = make_float2(ddz[0], ddz[1]);
             }
             const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-            const bool inA = r2.x < P.rc2, inB = r2.y < P.rc2;
+            const bool inA = (cw & kWordFirst) && r2.x < pp.rc2;
+            const bool inB = (cw & kWordSecond) && r2.y < pp.rc2;
             float2 elj, ec;
-            float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(make_float2(pA.w, pB.w), qi2), make_float2(abA.x, abB.x),
-                                             make_float2(abA.y, abB.y), P, elj, ec);
+            float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(f2(pj.w), qi2), make_float2(ab.x, ab.y),
+                                             make_float2(ab.z, ab.w), pp, elj, ec);
             f = make_float2(inA ? f.x : 0.0f, inB ? f.y : 0.0f);
-            const float2 gx = __fmul2_rn(f, dx), gy = __fmul2_rn(f, dy), gz = __fmul2_rn(f, dz);
-            fx = __fadd2_rn(fx, gx);
-            fy = __fadd2_rn(fy, gy);
-            fz = __fadd2_rn(fz, gz);
-            if (EN)
+            if (!EN)
             {
+                fx = __ffma2_rn(f, dx, fx);
+                fy = __ffma2_rn(f, dy, fy);
+                fz = __ffma2_rn(f, dz, fz);
+            }
+            else
+            {
+                const float2 gx = __fmul2_rn(f, dx), gy = __fmul2_rn(f, dy), gz = __fmul2_rn(f, dz);
+                fx = __fadd2_rn(fx, gx);
+                fy = __fadd2_rn(fy, gy);
+                fz = __fadd2_rn(fz, gz);
                 elj = make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f);
                 ec = make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f);
                 acc[0] = __fadd2_rn(acc[0], elj);
@@ -516,8 +638,8 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
                 acc[7] = __ffma2_rn(gz, dz, acc[7]);
                 if (PA)
                 {
-                    const int gjA = __float_as_int(slot_x0[jA].w), gjB = __float_as_int(slot_x0[jB].w);
-                    const float2 m = make_float2(gi < gjA ? 1.0f : 0.0f, gi < gjB ? 1.0f : 0.0f);
+                    const int gj = __float_as_int(slot_x0[j].w);
+                    const float2 m = make_float2(gi1 < gj ? 1.0f : 0.0f, gi2 < gj ? 1.0f : 0.0f);
                     own[0] = __ffma2_rn(m, elj, own[0]);
                     own[1] = __ffma2_rn(m, ec, own[1]);
                     const float2 mgx = __fmul2_rn(m, gx), mgy = __fmul2_rn(m, gy), mgz = __fmul2_rn(m, gz);
@@ -529,94 +651,115 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? 4 : (MODE == 1 ?
                     own[7] = __ffma2_rn(mgz, dz, own[7]);
                 }
             }
+        };
+        if (kWordsPerLane == 2)
+        {
+            const uint2* __restrict__ wl2 = reinterpret_cast<const uint2*>(wl);
+            uint2 wn = wl2[lane];
+#pragma unroll 1
+            for (int k0 = 0; k0 < n; k0 += 64)
+            {
+                const uint2 cw = wn;
+                if (k0 + 64 < n) wn = wl2[(k0 + 64) / 2 + lane];
+                eval_word(cw.x);
+                eval_word(cw.y);
+            }
         }
-        long long qx = __float2ll_rn((fx.x + fx.y) * kTwoPow32), qy = __float2ll_rn((fy.x + fy.y) * kTwoPow32),
-                  qz = __float2ll_rn((fz.x + fz.y) * kTwoPow32);
-        float accs[8], owns[8];
+        else
+        {
+            unsigned wn = wl[lane];
+#pragma unroll 1
+            for (int k0 = 0; k0 < n; k0 += 32)
+            {
+                const unsigned cw = wn;
+                if (k0 + 32 < n) wn = wl[k0 + 32 + lane];
+                eval_word(cw);
+            }
+        }
+        long long q1x = __float2ll_rn(fx.x * kTwoPow32), q1y = __float2ll_rn(fy.x * kTwoPow32),
+                  q1z = __float2ll_rn(fz.x * kTwoPow32);
+        long long q2x = __float2ll_rn(fx.y * kTwoPow32), q2y = __float2ll_rn(fy.y * kTwoPow32),
+                  q2z = __float2ll_rn(fz.y * kTwoPow32);
+        float accs[8], own1[8], own2[8];
 #pragma unroll
         for (int q = 0; q < 8; q++)
         {
             // the virial terms were accumulated as +g (x) d: the virial is -g (x) d
             const float sg = q >= 2 ? -1.0f : 1.0f;
             accs[q] = sg * (acc[q].x + acc[q].y);
-            owns[q] = sg * (own[q].x + own[q].y);
+            own1[q] = sg * own[q].x;
+            own2[q] = sg * own[q].y;
         }
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1)
         {
-            qx += __shfl_xor_sync(0xffffffffu, qx, o);
-            qy += __shfl_xor_sync(0xffffffffu, qy, o);
-            qz += __shfl_xor_sync(0xffffffffu, qz, o);
+            q1x += __shfl_xor_sync(0xffffffffu, q1x, o);
+            q1y += __shfl_xor_sync(0xffffffffu, q1y, o);
+            q1z += __shfl_xor_sync(0xffffffffu, q1z, o);
+            q2x += __shfl_xor_sync(0xffffffffu, q2x, o);
+            q2y += __shfl_xor_sync(0xffffffffu, q2y, o);
+            q2z += __shfl_xor_sync(0xffffffffu, q2z, o);
             if (EN)
 #pragma unroll
                 for (int q = 0; q < 8; q++) accs[q] += __shfl_xor_sync(0xffffffffu, accs[q], o);
             if (PA)
 #pragma unroll
-                for (int q = 0; q < 8; q++) owns[q] += __shfl_xor_sync(0xffffffffu, owns[q], o);
-        }
-        if (lane == 0)
-        {
-            const int ai = slot_atom[s];
-            float3 F = frc[ai];
-            F.x += (float)((double)qx * kForceUnscale);
-            F.y += (float)((double)qy * kForceUnscale);
-            F.z += (float)((double)qz * kForceUnscale);
-            frc[ai] = F;
-            if (EN)
-            {
-                // halve the double-counted sums; the symmetric off-diagonal
-                // terms (xy + yx etc.) are twice the one accumulated
-#pragma unroll
                 for (int q = 0; q < 8; q++)
                 {
-                    const double sc = (q == 3 || q == 5 || q == 6) ? 1.0 : 0.5;
-                    red[a][q] += __double2ll_rn((double)accs[q] * sc * kEnergyScale);
+                    own1[q] += __shfl_xor_sync(0xffffffffu, own1[q], o);
+                    own2[q] += __shfl_xor_sync(0xffffffffu, own2[q], o);
                 }
-            }
-            if (PA)
-            {
-                const int o = om.remap(ai);
-                if (pa.energy) atomicAdd(pa.energy + o, owns[0] + owns[1]);
-                if (pa.lj_energy) atomicAdd(pa.lj_energy + o, owns[0]);
-                if (pa.direct) atomicAdd(pa.direct + o, owns[1]);
-                if (pa.virial)
-                {
-                    float* v = pa.virial + 6 * (size_t)o;
-                    atomicAdd(v + 0, owns[2]);
-                    atomicAdd(v + 1, 2.0f * owns[3]);
-                    atomicAdd(v + 2, owns[4]);
-                    atomicAdd(v + 3, 2.0f * owns[5]);
-                    atomicAdd(v + 4, 2.0f * owns[6]);
-                    atomicAdd(v + 5, owns[7]);
-                }
-            }
         }
-    }
-    if (EN)
-    {
-        // the warps end on the same cluster, or on no cluster at all
-        __shared__ int end_sys[kForceWarps];
-        if (lane == 0) end_sys[a] = cur_sys;
-        __syncthreads();
-        if (threadIdx.x < 8)
+        if (lane < 2)
         {
-            long long t = 0;
-            int sys_end = -1;
-            for (int w = 0; w < kForceWarps; w++)
-                if (end_sys[w] >= 0)
+            // lane 0 writes the first atom, lane 1 the second
+            const int ai = slot_atom[s1 + lane];
+            if (ai >= 0)
+            {
+                const long long qx = lane ? q2x : q1x, qy = lane ? q2y : q1y, qz = lane ? q2z : q1z;
+                float3 F = frc[ai];
+                F.x += (float)((double)qx * kForceUnscale);
+                F.y += (float)((double)qy * kForceUnscale);
+                F.z += (float)((double)qz * kForceUnscale);
+                frc[ai] = F;
+                if (PA)
                 {
-                    if (sys_end >= 0 && end_sys[w] != sys_end)
+                    const float* ow = lane ? own2 : own1;
+                    const int o = om.remap(ai);
+                    if (pa.energy) atomicAdd(pa.energy + o, ow[0] + ow[1]);
+                    if (pa.lj_energy) atomicAdd(pa.lj_energy + o, ow[0]);
+                    if (pa.direct) atomicAdd(pa.direct + o, ow[1]);
+                    if (pa.virial)
                     {
-                        const long long v = red[w][threadIdx.x];
-                        if (v) atomicAdd((unsigned long long*)&totals[8 * end_sys[w] + threadIdx.x], (unsigned long long)v);
-                        continue;
+                        float* v = pa.virial + 6 * (size_t)o;
+                        atomicAdd(v + 0, ow[2]);
+                        atomicAdd(v + 1, 2.0f * ow[3]);
+                        atomicAdd(v + 2, ow[4]);
+                        atomicAdd(v + 3, 2.0f * ow[5]);
+                        atomicAdd(v + 4, 2.0f * ow[6]);
+                        atomicAdd(v + 5, ow[7]);
                     }
-                    sys_end = end_sys[w];
-                    t += red[w][threadIdx.x];
                 }
-            if (t && sys_end >= 0) atomicAdd((unsigned long long*)&totals[8 * sys_end + threadIdx.x], (unsigned long long)t);
+            }
+        }
+        if (EN && lane == 0)
+        {
+            // halve the double-counted sums; the symmetric off-diagonal
+            // terms (xy + yx etc.) are twice the one accumulated
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+            {
+                const double sc = (q == 3 || q == 5 || q == 6) ? 1.0 : 0.5;
+                red[w][q] += __double2ll_rn((double)accs[q] * sc * kEnergyScale);
+            }
         }
     }
+    if (EN && lane == 0 && cur_sys >= 0)
+        for (int q = 0; q < 8; q++)
+        {
+            const long long v = red[w][q];
+            if (v) atomicAdd((unsigned long long*)&totals[8 * cur_sys + q], (unsigned long long)v);
+        }
 }
 
 // Fixed point -> caller's float force (+=) for the reference-layout path,
@@ -958,14 +1101,6 @@ int pair_blocks(K kernel, int threads, size_t smem)
     return per_sm * num_sms();
 }
 
-template <int M>
-void set_fast_smem(size_t smem)
-{
-    cudaFuncSetAttribute(k_pair_fast<M, 0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_pair_fast<M, 1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_pair_fast<M, 0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_pair_fast<M, 1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
 
 // Launches the pruned-list force kernel for the given mode / pair-function /
 // box-shape variant.
@@ -977,7 +1112,7 @@ struct FastArgs
     const float4* pos;
     const int* ptype;
     const float2* table;
-    int table_size;
+    int n_types;
     float3* frc;
     long long* totals;
     OwnerMap om;
@@ -991,8 +1126,9 @@ int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
     const spgnb_nl* nl = x.nl;
     const int grid = std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T>, kForceWarps * 32, smem), nl->clusters_cap));
     k_pair_fast<M, F, T><<<grid, kForceWarps * 32, smem, s>>>(
-        x.p0, x.fps, nl->d_sys, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords, nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table,
-        x.table_size, x.frc, x.totals, x.om, x.pa, x.only);
+        x.p0, x.fps, nl->d_sys, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords,
+        nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table, x.n_types, x.frc, x.totals, x.om, x.pa,
+        x.only);
     SPGNB_CHECK_LAUNCH("k_pair_fast");
     return SPGNB_OK;
 }
@@ -1020,13 +1156,7 @@ int launch_fast_any(const FastArgs& x, int mode, bool fit, bool tri, size_t smem
 
 int force_kernels_init(int table_size)
 {
-    const size_t smem = sizeof(float2) * table_size;
-    if (smem > 48 * 1024)
-    {
-        set_fast_smem<0>(smem);
-        set_fast_smem<1>(smem);
-        set_fast_smem<2>(smem);
-    }
+    (void)table_size;  // the pair kernel's rows take at most kForceWarps * kMaxTypes * 16 bytes
     return SPGNB_OK;
 }
 
@@ -1050,9 +1180,12 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
     cudaEvent_t ev0, ev1;
     pair_events(&ev0, &ev1);
     if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
-    const FastArgs fa{in.p0, in.d_fps, nl, in.slot_pos, in.slot_type, in.table, in.table_size, in.frc,
+    const int T = (int)lrint(sqrt((double)in.table_size));
+    if (T <= 0 || T * T != in.table_size || T > kMaxTypes)
+        return fail(SPGNB_E_UNSUPPORTED, "force: the LJ table is not square or has more than %d types", kMaxTypes);
+    const FastArgs fa{in.p0, in.d_fps, nl, in.slot_pos, in.slot_type, in.table, T, in.frc,
                       in.totals, in.om, in.pa, in.only};
-    const int st = launch_fast_any(fa, in.mode, in.fit, nl->triclinic, sizeof(float2) * in.table_size, s);
+    const int st = launch_fast_any(fa, in.mode, in.fit, nl->triclinic, sizeof(float4) * kForceWarps * T, s);
     if (st) return st;
     if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
     return SPGNB_OK;
