@@ -476,11 +476,41 @@ __device__ __forceinline__ float centre_step(int qj, int qi)
 // from both atoms, so the sums are halved).  MODE 2: + per-atom energy and
 // virial of the pairs the atom owns (the lower global index; water sites
 // hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES does).
+// Sums eight per-lane values over the warp: after three halving exchanges
+// (lane bit 4, 3, 2 picks the half it keeps) and two full ones, lanes
+// 4v..4v+3 hold the total of value v.  Nine shuffles instead of forty.
+template <typename T>
+__device__ __forceinline__ T reduce_scatter8(const T (&v)[8], int lane)
+{
+    const bool h4 = (lane & 16) != 0, h3 = (lane & 8) != 0, h2 = (lane & 4) != 0;
+    T u[4], x[2];
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+    {
+        const T send = h4 ? v[k] : v[k + 4];
+        u[k] = (h4 ? v[k + 4] : v[k]) + __shfl_xor_sync(0xffffffffu, send, 16);
+    }
+#pragma unroll
+    for (int k = 0; k < 2; k++)
+    {
+        const T send = h3 ? u[k] : u[k + 2];
+        x[k] = (h3 ? u[k + 2] : u[k]) + __shfl_xor_sync(0xffffffffu, send, 8);
+    }
+    const T send = h2 ? x[0] : x[1];
+    T y = (h2 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
+    y += __shfl_xor_sync(0xffffffffu, y, 2);
+    y += __shfl_xor_sync(0xffffffffu, y, 1);
+    return y;
+}
+
 #ifndef SPGNB_PAIR_MINB0
 #define SPGNB_PAIR_MINB0 4
 #endif
 #ifndef SPGNB_PAIR_CHUNKED
 #define SPGNB_PAIR_CHUNKED 0
+#endif
+#ifndef SPGNB_PAIR_GP
+#define SPGNB_PAIR_GP 0
 #endif
 template <int MODE, int FIT, bool TRI>
 __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0 : (MODE == 1 ? 3 : 2))
@@ -523,6 +553,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
         if (EN && sy != cur_sys)
         {
             // totals belong to one system each: flush this warp's share
+            __syncwarp();
             if (lane == 0 && cur_sys >= 0)
                 for (int q = 0; q < 8; q++)
                 {
@@ -530,6 +561,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
                     if (v) atomicAdd((unsigned long long*)&totals[8 * cur_sys + q], (unsigned long long)v);
                     red[w][q] = 0;
                 }
+            __syncwarp();
             cur_sys = sy;
         }
         const ForceParams P = fps ? fps[sy] : p0;
@@ -573,10 +605,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             own[q] = f2(0.0f);
         }
         // one list word: the partner against both atoms
-        auto eval_word = [&](unsigned cw) {
-            const int j = slot0 + (int)(cw & kWordSlotMask);
-            const float4 pj = pos[j];
-            const int4 cj = cl_q[j >> 3];
+        auto eval_word = [&](unsigned cw, int j, float4 pj, int4 cj) {
             const float4 ab = rows[(cw >> kWordTypeShift) & 0x7fu];
             const float ux = centre_step(cj.x, ci.x), uy = centre_step(cj.y, ci.y), uz = centre_step(cj.z, ci.z);
             // the partner in the frame of the pair's cluster centre
@@ -652,6 +681,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
                 }
             }
         };
+        auto partner = [&](unsigned cw) { return slot0 + (int)(cw & kWordSlotMask); };
         if (kWordsPerLane == 2)
         {
             const uint2* __restrict__ wl2 = reinterpret_cast<const uint2*>(wl);
@@ -661,8 +691,35 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             {
                 const uint2 cw = wn;
                 if (k0 + 64 < n) wn = wl2[(k0 + 64) / 2 + lane];
-                eval_word(cw.x);
-                eval_word(cw.y);
+                const int ja = partner(cw.x), jb = partner(cw.y);
+                eval_word(cw.x, ja, pos[ja], cl_q[ja >> 3]);
+                eval_word(cw.y, jb, pos[jb], cl_q[jb >> 3]);
+            }
+        }
+        else if (SPGNB_PAIR_GP)
+        {
+            // partner data one window ahead, words two windows ahead
+            unsigned w1 = wl[lane];
+            unsigned w2 = 32 < n ? wl[32 + lane] : w1;
+            int j1 = partner(w1);
+            float4 p1 = pos[j1];
+            int4 c1 = cl_q[j1 >> 3];
+#pragma unroll 1
+            for (int k0 = 0; k0 < n; k0 += 32)
+            {
+                const unsigned cw = w1;
+                const int j = j1;
+                const float4 pj = p1;
+                const int4 cj = c1;
+                w1 = w2;
+                if (k0 + 64 < n) w2 = wl[k0 + 64 + lane];
+                if (k0 + 32 < n)
+                {
+                    j1 = partner(w1);
+                    p1 = pos[j1];
+                    c1 = cl_q[j1 >> 3];
+                }
+                eval_word(cw, j, pj, cj);
             }
         }
         else
@@ -673,56 +730,63 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             {
                 const unsigned cw = wn;
                 if (k0 + 32 < n) wn = wl[k0 + 32 + lane];
-                eval_word(cw);
+                const int j = partner(cw);
+                eval_word(cw, j, pos[j], cl_q[j >> 3]);
             }
         }
-        long long q1x = __float2ll_rn(fx.x * kTwoPow32), q1y = __float2ll_rn(fy.x * kTwoPow32),
-                  q1z = __float2ll_rn(fz.x * kTwoPow32);
-        long long q2x = __float2ll_rn(fx.y * kTwoPow32), q2y = __float2ll_rn(fy.y * kTwoPow32),
-                  q2z = __float2ll_rn(fz.y * kTwoPow32);
-        float accs[8], own1[8], own2[8];
-#pragma unroll
-        for (int q = 0; q < 8; q++)
+        // forces of both atoms: int64 fixed point per lane, summed over the
+        // lanes by a reduce-scatter (lanes 4v..4v+3 end with value v)
+        long long fq[8] = {__float2ll_rn(fx.x * kTwoPow32), __float2ll_rn(fy.x * kTwoPow32),
+                           __float2ll_rn(fz.x * kTwoPow32), __float2ll_rn(fx.y * kTwoPow32),
+                           __float2ll_rn(fy.y * kTwoPow32), __float2ll_rn(fz.y * kTwoPow32), 0, 0};
+        const long long fsum = reduce_scatter8(fq, lane);
+        const int vidx = lane >> 2;  // the value this lane holds
+        if ((lane & 3) == 0 && vidx < 6)
         {
-            // the virial terms were accumulated as +g (x) d: the virial is -g (x) d
-            const float sg = q >= 2 ? -1.0f : 1.0f;
-            accs[q] = sg * (acc[q].x + acc[q].y);
-            own1[q] = sg * own[q].x;
-            own2[q] = sg * own[q].y;
+            const int ai = slot_atom[s1 + (vidx >= 3 ? 1 : 0)];
+            if (ai >= 0)
+            {
+                float* fc = &frc[ai].x + (vidx % 3);
+                *fc += (float)((double)fsum * kForceUnscale);
+            }
         }
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1)
+        if (EN)
         {
-            q1x += __shfl_xor_sync(0xffffffffu, q1x, o);
-            q1y += __shfl_xor_sync(0xffffffffu, q1y, o);
-            q1z += __shfl_xor_sync(0xffffffffu, q1z, o);
-            q2x += __shfl_xor_sync(0xffffffffu, q2x, o);
-            q2y += __shfl_xor_sync(0xffffffffu, q2y, o);
-            q2z += __shfl_xor_sync(0xffffffffu, q2z, o);
-            if (EN)
+            float ev[8];
 #pragma unroll
-                for (int q = 0; q < 8; q++) accs[q] += __shfl_xor_sync(0xffffffffu, accs[q], o);
-            if (PA)
+            for (int q = 0; q < 8; q++) ev[q] = (q >= 2 ? -1.0f : 1.0f) * (acc[q].x + acc[q].y);
+            const float esum = reduce_scatter8(ev, lane);
+            if ((lane & 3) == 0)
+            {
+                // halve the double-counted sums; the symmetric off-diagonal
+                // terms (xy + yx etc.) are twice the one accumulated
+                const double sc = (vidx == 3 || vidx == 5 || vidx == 6) ? 1.0 : 0.5;
+                red[w][vidx] += __double2ll_rn((double)esum * sc * kEnergyScale);
+            }
+        }
+        if (PA)
+        {
+            float own1[8], own2[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++)
+            {
+                // the virial terms were accumulated as +g (x) d: the virial is -g (x) d
+                const float sg = q >= 2 ? -1.0f : 1.0f;
+                own1[q] = sg * own[q].x;
+                own2[q] = sg * own[q].y;
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1)
 #pragma unroll
                 for (int q = 0; q < 8; q++)
                 {
                     own1[q] += __shfl_xor_sync(0xffffffffu, own1[q], o);
                     own2[q] += __shfl_xor_sync(0xffffffffu, own2[q], o);
                 }
-        }
-        if (lane < 2)
-        {
-            // lane 0 writes the first atom, lane 1 the second
-            const int ai = slot_atom[s1 + lane];
-            if (ai >= 0)
+            if (lane < 2)
             {
-                const long long qx = lane ? q2x : q1x, qy = lane ? q2y : q1y, qz = lane ? q2z : q1z;
-                float3 F = frc[ai];
-                F.x += (float)((double)qx * kForceUnscale);
-                F.y += (float)((double)qy * kForceUnscale);
-                F.z += (float)((double)qz * kForceUnscale);
-                frc[ai] = F;
-                if (PA)
+                const int ai = slot_atom[s1 + lane];
+                if (ai >= 0)
                 {
                     const float* ow = lane ? own2 : own1;
                     const int o = om.remap(ai);
@@ -742,18 +806,8 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
                 }
             }
         }
-        if (EN && lane == 0)
-        {
-            // halve the double-counted sums; the symmetric off-diagonal
-            // terms (xy + yx etc.) are twice the one accumulated
-#pragma unroll
-            for (int q = 0; q < 8; q++)
-            {
-                const double sc = (q == 3 || q == 5 || q == 6) ? 1.0 : 0.5;
-                red[w][q] += __double2ll_rn((double)accs[q] * sc * kEnergyScale);
-            }
-        }
     }
+    __syncwarp();
     if (EN && lane == 0 && cur_sys >= 0)
         for (int q = 0; q < 8; q++)
         {
