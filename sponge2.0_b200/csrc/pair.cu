@@ -153,11 +153,7 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
 // buffer <= 0 keeps every listed pair.  The last block to finish clears the
 // flags.
 constexpr int kPruneWarps = 8;
-#ifndef SPGNB_PAIR_WPL
-#define SPGNB_PAIR_WPL 1
-#endif
-constexpr int kWordsPerLane = SPGNB_PAIR_WPL;  // list words a force-kernel lane takes per iteration
-constexpr int kWindow = 32 * kWordsPerLane;    // lists are padded to whole windows
+constexpr int kWindow = 32;                    // lists are padded to whole 32-word windows
 constexpr int kWordSlotBits = 22;                  // partner slot field of a list word
 constexpr unsigned kWordSlotMask = (1u << kWordSlotBits) - 1u;
 constexpr int kWordTypeShift = 22;                 // 7-bit LJ type
@@ -460,7 +456,10 @@ __device__ __forceinline__ float centre_step(int qj, int qi)
 // Pruned-list force kernel.  A warp takes one slot pair (the two atoms of
 // slots 2p, 2p+1 of a cluster) at a time, strided over the grid's warps, and
 // walks the pair's shared list, one word per lane per iteration (32-word
-// windows, the next window's words already in flight).  A word names the
+// windows).  The next item's header (list length, system, types, the two
+// atoms' offsets, the cluster centre) and first window are staged in shared
+// memory by cp.async while the warp works on the current one, and the list's
+// later windows are loaded kPrefetch iterations ahead.  A word names the
 // partner slot, so its offset {delta + displacement, q} and its cluster's
 // 22-bit centre load side by side, once for both atoms:
 //   dr = (c_j - c_i) * cell / 2^22 + p_j - p_{i1,i2},
@@ -468,14 +467,38 @@ __device__ __forceinline__ float centre_step(int qj, int qi)
 // coefficients of both come from the warp's shared-memory row for the two
 // atoms' types {-A1, -A2, B1, B2} indexed by the partner's type.  Each
 // lane's partial forces are converted to int64 fixed point (2^-32
-// kcal/mol/A) and reduced over the lanes, so an atom's force does not depend
-// on the reduction order; one lane adds it to the caller's array: no
-// atomics, bitwise reproducible.
+// kcal/mol/A) and summed over the lanes exactly, so an atom's force does not
+// depend on the reduction order; one lane per component adds it to the
+// caller's array, once per call: bitwise reproducible.
 //
 // MODE 0: forces.  MODE 1: + energy and virial totals (each pair is seen
 // from both atoms, so the sums are halved).  MODE 2: + per-atom energy and
 // virial of the pairs the atom owns (the lower global index; water sites
 // hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES does).
+// One item's header and first list window, staged in shared memory by
+// asynchronous copies (cp.async) while the warp works on the item before.
+struct alignas(16) ItemStage
+{
+    int n, sy, t1, t2;     // list words, system, LJ types of the two atoms
+    int4 ci;               // the cluster's 22-bit centre
+    float4 p1, p2;         // the two atoms' slot offsets and charges
+    unsigned words[32];    // first window of the list
+};
+
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes)
+{
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    if (bytes == 16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem));
+    else if (bytes == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem));
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
+__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 // Sums eight per-lane values over the warp: after three halving exchanges
 // (lane bit 4, 3, 2 picks the half it keeps) and two full ones, lanes
 // 4v..4v+3 hold the total of value v.  Nine shuffles instead of forty.
@@ -506,12 +529,10 @@ __device__ __forceinline__ T reduce_scatter8(const T (&v)[8], int lane)
 #ifndef SPGNB_PAIR_MINB0
 #define SPGNB_PAIR_MINB0 4
 #endif
-#ifndef SPGNB_PAIR_CHUNKED
-#define SPGNB_PAIR_CHUNKED 0
+#ifndef SPGNB_PAIR_PREFETCH
+#define SPGNB_PAIR_PREFETCH 2
 #endif
-#ifndef SPGNB_PAIR_GP
-#define SPGNB_PAIR_GP 0
-#endif
+constexpr int kPrefetch = SPGNB_PAIR_PREFETCH;  // list windows in flight per warp
 template <int MODE, int FIT, bool TRI>
 __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0 : (MODE == 1 ? 3 : 2))
     k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
@@ -535,20 +556,40 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
     __syncwarp();
     int cur_sys = -1;              // the system red[w] accumulates for
     const int items = n_clusters * 4;
-#if SPGNB_PAIR_CHUNKED
-    // each block a contiguous run of clusters (neighbouring clusters share partners in L1)
-    const int per = (items + gridDim.x - 1) / gridDim.x;
-    const int it_end = min(items, (blockIdx.x + 1) * per);
-    for (int it = blockIdx.x * per + w; it < it_end; it += kForceWarps)
-#else
-    for (int it = blockIdx.x * kForceWarps + w; it < items; it += gridDim.x * kForceWarps)
-#endif
+    __shared__ ItemStage stage_all[kForceWarps][2];
+    ItemStage* stage = stage_all[w];
+    const int stride = gridDim.x * kForceWarps;
+    // stages item `it` (nothing past the end: an empty group keeps the count)
+    auto prefetch = [&](int it, ItemStage& S) {
+        if (it < items)
+        {
+            const int c = it >> 2;
+            const int s1 = c * kClusterSize + 2 * (it & 3);
+            if (lane == 0) cp_async(&S.n, pcount + s1, 4);
+            if (lane == 1) cp_async(&S.sy, cl_sys + c, 4);
+            if (lane == 2) cp_async(&S.t1, ptype + s1, 8);
+            if (lane == 3) cp_async(&S.ci, cl_q + c, 16);
+            if (lane == 4) cp_async(&S.p1, pos + s1, 16);
+            if (lane == 5) cp_async(&S.p2, pos + s1 + 1, 16);
+            cp_async(&S.words[lane], pwords + (size_t)s1 * slot_cap + lane, 4);
+        }
+        cp_async_commit();
+    };
+    int kk = 0;
+    prefetch(blockIdx.x * kForceWarps + w, stage[0]);
+    for (int it = blockIdx.x * kForceWarps + w; it < items; it += stride, kk++)
     {
+        // every lane has read the buffer the next prefetch overwrites
+        __syncwarp();
+        prefetch(it + stride, stage[(kk + 1) & 1]);
+        cp_async_wait_prior();
+        __syncwarp();
+        const ItemStage& S = stage[kk & 1];
         const int c = it >> 2;
         const int s1 = c * kClusterSize + 2 * (it & 3);
-        const int n = pcount[s1];  // a multiple of the window
+        const int n = S.n;  // a multiple of the window
         if (n == 0) continue;
-        const int sy = cl_sys[c];
+        const int sy = S.sy;
         if (only && !only[sy]) continue;
         if (EN && sy != cur_sys)
         {
@@ -569,9 +610,9 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
         const SysDesc& D = sys[sy];
         const Cell qc = D.qcell;
         const int slot0 = D.cl_begin * kClusterSize;
-        const float4 pi1 = pos[s1], pi2 = pos[s1 + 1];
-        const int4 ci = cl_q[c];
-        const int r1 = ptype[s1] * n_types + P.table_begin, r2i = ptype[s1 + 1] * n_types + P.table_begin;
+        const float4 pi1 = S.p1, pi2 = S.p2;
+        const int4 ci = S.ci;
+        const int r1 = S.t1 * n_types + P.table_begin, r2i = S.t2 * n_types + P.table_begin;
         if (r1 != row_of[w][0] || r2i != row_of[w][1])
         {
             __syncwarp();
@@ -682,57 +723,21 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             }
         };
         auto partner = [&](unsigned cw) { return slot0 + (int)(cw & kWordSlotMask); };
-        if (kWordsPerLane == 2)
-        {
-            const uint2* __restrict__ wl2 = reinterpret_cast<const uint2*>(wl);
-            uint2 wn = wl2[lane];
+        // the list streams from memory: its windows are loaded kPrefetch
+        // iterations ahead of their use (a ring of registers)
+        unsigned ring[kPrefetch];
+        ring[0] = S.words[lane];
+#pragma unroll
+        for (int q = 1; q < kPrefetch; q++) ring[q] = q * 32 < n ? wl[q * 32 + lane] : 0u;
 #pragma unroll 1
-            for (int k0 = 0; k0 < n; k0 += 64)
-            {
-                const uint2 cw = wn;
-                if (k0 + 64 < n) wn = wl2[(k0 + 64) / 2 + lane];
-                const int ja = partner(cw.x), jb = partner(cw.y);
-                eval_word(cw.x, ja, pos[ja], cl_q[ja >> 3]);
-                eval_word(cw.y, jb, pos[jb], cl_q[jb >> 3]);
-            }
-        }
-        else if (SPGNB_PAIR_GP)
+        for (int k0 = 0; k0 < n; k0 += 32)
         {
-            // partner data one window ahead, words two windows ahead
-            unsigned w1 = wl[lane];
-            unsigned w2 = 32 < n ? wl[32 + lane] : w1;
-            int j1 = partner(w1);
-            float4 p1 = pos[j1];
-            int4 c1 = cl_q[j1 >> 3];
-#pragma unroll 1
-            for (int k0 = 0; k0 < n; k0 += 32)
-            {
-                const unsigned cw = w1;
-                const int j = j1;
-                const float4 pj = p1;
-                const int4 cj = c1;
-                w1 = w2;
-                if (k0 + 64 < n) w2 = wl[k0 + 64 + lane];
-                if (k0 + 32 < n)
-                {
-                    j1 = partner(w1);
-                    p1 = pos[j1];
-                    c1 = cl_q[j1 >> 3];
-                }
-                eval_word(cw, j, pj, cj);
-            }
-        }
-        else
-        {
-            unsigned wn = wl[lane];
-#pragma unroll 1
-            for (int k0 = 0; k0 < n; k0 += 32)
-            {
-                const unsigned cw = wn;
-                if (k0 + 32 < n) wn = wl[k0 + 32 + lane];
-                const int j = partner(cw);
-                eval_word(cw, j, pos[j], cl_q[j >> 3]);
-            }
+            const unsigned cw = ring[0];
+#pragma unroll
+            for (int q = 0; q + 1 < kPrefetch; q++) ring[q] = ring[q + 1];
+            if (k0 + kPrefetch * 32 < n) ring[kPrefetch - 1] = wl[k0 + kPrefetch * 32 + lane];
+            const int j = partner(cw);
+            eval_word(cw, j, pos[j], cl_q[j >> 3]);
         }
         // forces of both atoms: int64 fixed point per lane, summed over the
         // lanes by a reduce-scatter (lanes 4v..4v+3 end with value v)
@@ -744,11 +749,8 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
         if ((lane & 3) == 0 && vidx < 6)
         {
             const int ai = slot_atom[s1 + (vidx >= 3 ? 1 : 0)];
-            if (ai >= 0)
-            {
-                float* fc = &frc[ai].x + (vidx % 3);
-                *fc += (float)((double)fsum * kForceUnscale);
-            }
+            if (ai >= 0)  // one add per component and call: the same as a read-modify-write, without the wait
+                atomicAdd(&frc[ai].x + (vidx % 3), (float)((double)fsum * kForceUnscale));
         }
         if (EN)
         {
@@ -807,6 +809,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             }
         }
     }
+    cp_async_wait_all();
     __syncwarp();
     if (EN && lane == 0 && cur_sys >= 0)
         for (int q = 0; q < 8; q++)
