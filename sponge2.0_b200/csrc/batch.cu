@@ -82,6 +82,7 @@ struct spgnb_batch
     bool graph_tri = false;
     long long steps_done = 0;
     bool pending = false;  // admitted systems wait for their first lists and forces
+    std::vector<spgnb::PinnedStage> stages;  // upload buffers of admissions, reused when their copies are done
 };
 
 namespace spgnb
@@ -320,7 +321,7 @@ int settle_pending(spgnb_batch* b)
 {
     if (!b->pending) return SPGNB_OK;
     cudaStream_t s = b->stream;
-    SPGNB_CUDA(cudaMemcpyAsync(b->d_flags, b->h_flags.data(), sizeof(int) * b->S, cudaMemcpyHostToDevice, s));
+    // d_flags: set for each admitted system by its admission
     int st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num,
                             kBuildPreset, s, b->d_flags);
     if (!st) st = batch_force(b, 1, s, b->d_flags);
@@ -400,9 +401,52 @@ void free_batch(spgnb_batch* b)
     dfree(b->d_flags);
     dfree(b->d_slot_pos);
     dfree(b->d_slot_type);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    for (PinnedStage& ps : b->stages)
+    {
+        if (ps.ev) cudaEventDestroy(ps.ev);
+        if (ps.p) cudaFreeHost(ps.p);
+    }
+    b->stages.clear();
     if (b->stream) cudaStreamDestroy(b->stream);
     b->stream = nullptr;
 }
+
+// A pinned upload buffer of at least `bytes` whose earlier copies are done.
+int take_stage(spgnb_batch* b, size_t bytes, PinnedStage** out)
+{
+    PinnedStage* pick = nullptr;
+    for (PinnedStage& ps : b->stages)
+    {
+        if (ps.busy && cudaEventQuery(ps.ev) == cudaSuccess) ps.busy = false;
+        if (!ps.busy && ps.cap >= bytes && (!pick || ps.cap < pick->cap)) pick = &ps;
+    }
+    if (!pick)
+    {
+        for (PinnedStage& ps : b->stages)
+            if (!ps.busy && (!pick || ps.cap > pick->cap)) pick = &ps;
+        if (!pick)
+        {
+            b->stages.emplace_back();
+            pick = &b->stages.back();
+            SPGNB_CUDA(cudaEventCreateWithFlags(&pick->ev, cudaEventDisableTiming));
+        }
+        if (pick->p) SPGNB_CUDA(cudaFreeHost(pick->p));
+        pick->p = nullptr;
+        pick->cap = std::max(bytes, (size_t)1 << 20);
+        cudaError_t e = cudaHostAlloc((void**)&pick->p, pick->cap, cudaHostAllocDefault);
+        if (e != cudaSuccess)
+        {
+            pick->cap = 0;
+            return cuda_fail(e, "cudaHostAlloc (upload staging)");
+        }
+    }
+    pick->used = 0;
+    *out = pick;
+    return SPGNB_OK;
+}
+
+__global__ void k_set_flag(int* flags, int id) { flags[id] = 1; }
 
 template <typename T>
 int zalloc(T** d, size_t count)
@@ -413,13 +457,6 @@ int zalloc(T** d, size_t count)
     return SPGNB_OK;
 }
 
-template <typename T>
-int put(T* d, size_t offset, const std::vector<T>& h, cudaStream_t s)
-{
-    if (h.empty()) return SPGNB_OK;
-    SPGNB_CUDA(cudaMemcpyAsync(d + offset, h.data(), sizeof(T) * h.size(), cudaMemcpyHostToDevice, s));
-    return SPGNB_OK;
-}
 
 // One system checked and laid out on the host, indices local to it.
 struct Staged
@@ -584,8 +621,23 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
         return fail(SPGNB_E_OOM, "batch: no room for the exclusions or waters now");
     }
     z.sh.atom_begin = (int)ab;
+    // every upload of this admission goes through one pinned buffer, so the
+    // copies queue behind the work in flight instead of waiting for it
+    const size_t N = z.N;
+    const size_t need = N * (2 * sizeof(float3) + 6 * sizeof(int)) + ne * sizeof(int) +
+                        z.water_numbers * sizeof(int) + sizeof(ForceParams) + 3 * sizeof(int) + 16 * 20 +
+                        nl_admit_upload_bytes(z.sh, z.runs.size());
+    PinnedStage* ps = nullptr;
+    if ((st = take_stage(b, need, &ps)))
+    {
+        b->water_pool.release(wb, z.water_numbers);
+        b->ex_pool.release(eb, ne);
+        b->atom_pool.release(ab, z.N);
+        return st;
+    }
+    Uploader up{ps};
     int sid = -1;
-    st = nl_admit(b->nl, z.sh, &z.run_start, &z.runs, s, &sid);
+    st = nl_admit(b->nl, z.sh, &z.run_start, &z.runs, s, &sid, up);
     if (st)
     {
         b->water_pool.release(wb, z.water_numbers);
@@ -616,19 +668,22 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
     const std::vector<ForceParams> fp(1, z.fp);
     const std::vector<float> ndof(1, z.ndof);
     const std::vector<int> left(1, steps > 0 ? steps : -1);
-    if ((st = put(b->d_crd, ab, z.crd, s)) || (st = put(b->d_vel, ab, z.vel, s)) ||
-        (st = put(b->d_charge, ab, z.charge, s)) || (st = put(b->d_inv_mass, ab, z.inv_mass, s)) ||
-        (st = put(b->d_type, ab, z.type, s)) || (st = put(b->d_atom_local, ab, own, s)) ||
-        (st = put(b->d_ex_start, ab, ex_start, s)) || (st = put(b->d_ex_num, ab, z.ex_num, s)) ||
-        (st = put(b->d_ex_list, eb, ex_list, s)) || (st = put(b->d_waters, wb, waters, s)) ||
-        (st = put(b->d_fps, sid, fp, s)) || (st = put(b->d_ndof, sid, ndof, s)) || (st = put(b->d_left, sid, left, s)))
+    auto putv = [&](auto* dst, size_t off, const auto& v) { return up.put(dst + off, v.data(), sizeof(v[0]) * v.size(), s); };
+    if ((st = putv(b->d_crd, ab, z.crd)) || (st = putv(b->d_vel, ab, z.vel)) ||
+        (st = putv(b->d_charge, ab, z.charge)) || (st = putv(b->d_inv_mass, ab, z.inv_mass)) ||
+        (st = putv(b->d_type, ab, z.type)) || (st = putv(b->d_atom_local, ab, own)) ||
+        (st = putv(b->d_ex_start, ab, ex_start)) || (st = putv(b->d_ex_num, ab, z.ex_num)) ||
+        (st = putv(b->d_ex_list, eb, ex_list)) || (st = putv(b->d_waters, wb, waters)) ||
+        (st = putv(b->d_fps, sid, fp)) || (st = putv(b->d_ndof, sid, ndof)) || (st = putv(b->d_left, sid, left)))
         return st;
     SPGNB_CUDA(cudaMemsetAsync(b->d_frc + ab, 0, sizeof(float3) * z.N, s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_steps + sid, 0, sizeof(int), s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_kin + sid, 0, sizeof(long long), s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_totals + 8 * (size_t)sid, 0, sizeof(long long) * 8, s));
-    // the host vectors above are about to go: wait for the copies
-    SPGNB_CUDA(cudaStreamSynchronize(s));
+    k_set_flag<<<1, 1, 0, s>>>(b->d_flags, sid);
+    SPGNB_CHECK_LAUNCH("k_set_flag");
+    SPGNB_CUDA(cudaEventRecord(ps->ev, s));
+    ps->busy = true;
     b->h_fps[sid] = z.fp;
     SysRec& r = b->rec[sid];
     r.live = true;

@@ -434,6 +434,23 @@ int force_kernels_init(int table_size);
 int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,
                     const spgnb_ltmatrix3* rcells, const float* cutoffs, const float* skins,
                     const spgnb_nl_options* opt, spgnb_nl** out);
+// Host-to-device uploads from one pinned staging buffer, so the copies are
+// asynchronous: the caller keeps the buffer until an event recorded after
+// them has completed.  Without a buffer the copies read the caller's memory
+// directly (pageable: the copy completes before the call returns).
+struct PinnedStage
+{
+    char* p = nullptr;
+    size_t cap = 0, used = 0;
+    cudaEvent_t ev = nullptr;
+    bool busy = false;
+};
+struct Uploader
+{
+    PinnedStage* st = nullptr;
+    int put(void* dst, const void* src, size_t bytes, cudaStream_t s);
+};
+
 // Capacities of an empty pool of systems.
 struct NLPoolSpec
 {
@@ -461,7 +478,9 @@ void nl_capacity_for(double atoms_per_A3, double atom_count, float cutoff, float
 // message) when the pool has no room now.  The system rebuilds when the
 // caller sets its flag for a kBuildPreset update.
 int nl_admit(spgnb_nl* nl, SysHost sh, const std::vector<int>* run_start, const std::vector<int2>* runs,
-             cudaStream_t s, int* id);
+             cudaStream_t s, int* id, Uploader up = Uploader{});
+// Bytes an Uploader needs for a system's list data (runs, run table, descriptor).
+size_t nl_admit_upload_bytes(const SysHost& sh, size_t n_runs);
 // Returns a system's ranges to the pool; its atoms map to the parking descriptor.
 int nl_retire(spgnb_nl* nl, int id, cudaStream_t s);
 // Every live system re-prunes before the next force evaluation.

@@ -1122,8 +1122,28 @@ int nl_create_pool(const NLPoolSpec& spec, const spgnb_nl_options* opt, spgnb_nl
     return SPGNB_OK;
 }
 
+int Uploader::put(void* dst, const void* src, size_t bytes, cudaStream_t s)
+{
+    if (bytes == 0) return SPGNB_OK;
+    const void* from = src;
+    if (st)
+    {
+        if (st->used + bytes > st->cap) return fail(SPGNB_E_STATE, "upload staging buffer too small");
+        memcpy(st->p + st->used, src, bytes);
+        from = st->p + st->used;
+        st->used += (bytes + 15) & ~(size_t)15;
+    }
+    SPGNB_CUDA(cudaMemcpyAsync(dst, from, bytes, cudaMemcpyHostToDevice, s));
+    return SPGNB_OK;
+}
+
+size_t nl_admit_upload_bytes(const SysHost& sh, size_t n_runs)
+{
+    return sizeof(SysDesc) + 16 + n_runs * sizeof(int2) + 16 + (size_t)(sh.cells() + 1) * sizeof(int) + 16;
+}
+
 int nl_admit(spgnb_nl* nl, SysHost sh, const std::vector<int>* run_start, const std::vector<int2>* runs,
-             cudaStream_t s, int* id)
+             cudaStream_t s, int* id, Uploader up)
 {
     int st;
     std::vector<int> start_own;
@@ -1172,10 +1192,10 @@ int nl_admit(spgnb_nl* nl, SysHost sh, const std::vector<int>* run_start, const 
     for (int g = 0; g <= G; g++) sa[g] = (*run_start)[g] + (int)rb;
     nl->h_desc[sid] = make_desc(sh, nl->opt.skin_permit);
     nl->h_desc[sid].prune_r2 = prune_r2_of(nl->prune_rc, nl->opt.prune_buffer);
-    // (pageable sources: the copies are staged before these calls return)
-    SPGNB_CUDA(cudaMemcpyAsync(nl->d_sys + sid, &nl->h_desc[sid], sizeof(SysDesc), cudaMemcpyHostToDevice, s));
-    if (nr) SPGNB_CUDA(cudaMemcpyAsync(nl->d_runs + rb, ra.data(), sizeof(int2) * nr, cudaMemcpyHostToDevice, s));
-    SPGNB_CUDA(cudaMemcpyAsync(nl->d_run_start + cb, sa.data(), sizeof(int) * (G + 1), cudaMemcpyHostToDevice, s));
+    if ((st = up.put(nl->d_sys + sid, &nl->h_desc[sid], sizeof(SysDesc), s)) ||
+        (st = up.put(nl->d_runs + rb, ra.data(), sizeof(int2) * nr, s)) ||
+        (st = up.put(nl->d_run_start + cb, sa.data(), sizeof(int) * (G + 1), s)))
+        return st;
     if ((st = fill_int(nl->d_atom_sys + sh.atom_begin, sh.atom_count, sid, s))) return st;
     if ((st = fill_int(nl->d_cell_sys + cb, G, sid, s))) return st;
     if ((st = fill_int(nl->d_cl_sys + clb, cl_cap, sid, s))) return st;

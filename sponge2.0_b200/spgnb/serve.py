@@ -5,8 +5,9 @@ system id and free ranges for their atoms, cells, clusters, exclusions and
 waters (the pool's capacities come from its device-memory budget); admitted
 segments run together, every step one launch sequence over all of them, and
 a segment leaves the pool when its own step count is reached.  Admission and
-retirement happen between chunks of ``chunk_steps`` steps (one captured
-graph each); a segment that reaches its count inside a chunk is frozen on
+retirement happen while a chunk of ``chunk_steps`` steps (one captured
+graph) runs: admitted systems' uploads queue behind it and they start with
+the next chunk; a segment that reaches its count inside a chunk is frozen on
 the device until the chunk ends, so it runs exactly its steps.  A segment's
 result is bitwise the one it gets alone.
 
@@ -160,22 +161,32 @@ class Server:
             over = duration_s is not None and now >= duration_s
             if over and not drain:
                 break
-            if not over or drain:
-                self._admit(now)
+            admitting = not over or drain
             if not self.resident:
-                if self.queue and not over:
+                if admitting:
+                    self._admit(now)
+                if not self.resident:
+                    if self.queue and not over:
+                        continue
+                    if nxt >= len(pending) or over:
+                        break
+                    wait = pending[nxt].arrival_s - now
+                    if duration_s is not None:
+                        wait = min(wait, duration_s - now)
+                    if wait > 0:
+                        self.sleep(wait)
                     continue
-                if nxt >= len(pending) or over:
-                    break
-                wait = pending[nxt].arrival_s - now
-                if duration_s is not None:
-                    wait = min(wait, duration_s - now)
-                if wait > 0:
-                    self.sleep(wait)
-                continue
             self.pool.run(self.chunk_steps)
             self.chunks += 1
-            # while the chunk runs: make the systems of the next requests in line
+            # while the chunk runs: admit what fits (its uploads queue behind
+            # the chunk; it starts with the next one) and make the systems of
+            # the next requests in line
+            if admitting:
+                now = self.clock() - t0
+                while nxt < len(pending) and pending[nxt].arrival_s <= now:
+                    self.queue.append(Segment(pending[nxt]))
+                    nxt += 1
+                self._admit(now)
             for seg in self.queue[:self.prefetch]:
                 self._make(seg)
             self._collect(self.clock() - t0)

@@ -12,9 +12,9 @@ def _systems(k, seed):
     return S.batch_systems(k, seed=seed, n_min=1500, n_max=4000)
 
 
-def _alone(system, steps):
+def _alone(system, steps, **kw):
     from spgnb.batch import Batch
-    b = Batch([system])
+    b = Batch([system], **kw)
     b.run(steps)
     b.evaluate([0])
     crd, vel, frc = b.download(0)
@@ -28,11 +28,14 @@ def _assert_same(got, ref, what):
         assert np.array_equal(x, y), f"{what}: {name} differs alone vs in the pool"
 
 
-def test_pool_same_alone_and_in_the_mix(torch_cuda):
+@pytest.mark.parametrize("tau", [0.0, 0.05])
+def test_pool_same_alone_and_in_the_mix(torch_cuda, tau):
+    """Systems join and leave a running pool; each ends bitwise where it ends
+    alone (with the per-system thermostat on too: its sums are fixed point)."""
     from spgnb.batch import Pool, pool_options
     systems = _systems(4, seed=21)
     steps = [60, 40, 30, 20]
-    pool = Pool(systems[0], pool_options(max_systems=8, max_atoms=40000))
+    pool = Pool(systems[0], pool_options(max_systems=8, max_atoms=40000), thermostat_tau=tau)
     ids = {0: pool.admit(systems[0], steps[0]), 1: pool.admit(systems[1], steps[1])}
     pool.run(20)
     ids[2] = pool.admit(systems[2], steps[2])       # joins two running systems
@@ -55,7 +58,7 @@ def test_pool_same_alone_and_in_the_mix(torch_cuda):
     assert pool.stats()["overflow"] == 0
     pool.close()
     for k in range(4):
-        _assert_same(results[k], _alone(systems[k], steps[k]), f"system {k}")
+        _assert_same(results[k], _alone(systems[k], steps[k], thermostat_tau=tau), f"system {k}")
 
 
 def test_pool_refuses_then_admits(torch_cuda):
