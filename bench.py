@@ -491,6 +491,27 @@ def main():
         e2e_ms.append(a.elapsed_time(b))
     e2e_total = sum(e2e_ms)
 
+    # the PME excluded-pair correction (PM_force.cpp:918-997), timed on its own
+    # (not part of the step above: SPONGE runs it in the PME module)
+    ex_frc = torch.zeros_like(path.frc)
+    ex_ene = torch.zeros_like(path.atom_energy)
+    ex_vir = torch.zeros_like(path.atom_virial)
+
+    def excluded():
+        path.lj.PME_Excluded_Force_With_Atom_Energy(s.n, path.crd, s.cell, s.rcell, path.charge, s.beta,
+                                                    path.excl_start, path.excl_list, path.excl_numbers, ex_frc,
+                                                    1, ex_ene, ex_vir)
+
+    for _ in range(3):
+        excluded()
+    xa, xb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    xa.record(stream)
+    for _ in range(20):
+        excluded()
+    xb.record(stream)
+    xb.synchronize()
+    excluded_ms = xa.elapsed_time(xb) / 20
+
     if dist is not None:
         t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -526,6 +547,7 @@ def main():
                          "traffic_source": prof.get("source")},
             "clocks": clocks,
             "gpu_launches": int(launches),
+            "pme_excluded_correction_ms": excluded_ms,
             "e2e": {"value": world * s.n * K / (e2e_total * 1e-3), "unit": "atom-steps/s",
                     "h2d_bytes_per_step": s.n * 12, "d2h_bytes_per_step": s.n * 12 + (64 if fe else 0)},
         }

@@ -243,6 +243,21 @@ int spgnb_lj_atom_lj_energy(spgnb_lj* lj, float** d_atom_lj_energy);
 int spgnb_lj_export_vector_lj(spgnb_lj* lj, const spgnb_vector* d_crd, const float* d_charge, void* d_vector_lj,
                               int n);
 
+/* The PME excluded-pair correction, Particle_Mesh::PME_Excluded_Force_With_Atom_Energy
+ * (PM_force.cpp:918-997): for every excluded pair (the exclusion CSR, upper
+ * triangular) the smooth part q_i q_j erf(beta r)/r that reciprocal space
+ * counted is taken back out.  Forces are added to d_frc (int64 fixed-point
+ * accumulation, the same in any order), the per-atom energy to
+ * d_atom_energy when need_energy, the per-atom virial to d_atom_virial when
+ * it is not NULL.  The total of the last call: spgnb_lj_pme_excluded_energy
+ * (synchronises). */
+int spgnb_lj_pme_excluded_force(spgnb_lj* lj, int atom_numbers, const spgnb_vector* d_crd, spgnb_ltmatrix3 cell,
+                                spgnb_ltmatrix3 rcell, const float* d_charge, float pme_beta,
+                                const int* d_excluded_list_start, const int* d_excluded_list,
+                                const int* d_excluded_numbers, spgnb_vector* d_frc, int need_energy,
+                                float* d_atom_energy, spgnb_ltmatrix3* d_atom_virial);
+int spgnb_lj_pme_excluded_energy(spgnb_lj* lj, double* energy);
+
 int spgnb_lj_destroy(spgnb_lj* lj);
 
 /* --------------------------------------------------- SOLVENT_LENNARD_JONES */

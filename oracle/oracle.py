@@ -110,6 +110,49 @@ class Oracle:
                                               frc, ptr(elj), ptr(ec), ptr(vir), tot)
         return _result(frc, elj, ec, vir, tot, npairs)
 
+    @staticmethod
+    def pme_excluded(s):
+        """FP64 PME excluded-pair correction (PM_force.cpp:918-974): for each
+        excluded pair i < j of the CSR, dr = min image(r_j - r_i) and
+        F_i += -q_i q_j (2/sqrt(pi) x exp(-x^2) + erfc(x) - 1) / r^3 dr,
+        F_j -= the same, E_i -= q_i q_j erf(x)/r (x = beta r), and
+        W_i -= Get_Virial_From_Force_Dis(F, dr)."""
+        from scipy.special import erf, erfc
+        n = s.n
+        crd = np.asarray(s.crd, np.float64)
+        q = np.asarray(s.charge, np.float64)
+        start, num = np.asarray(s.excl_start), np.asarray(s.excl_numbers)
+        lst = np.asarray(s.excl_list)
+        ii = np.repeat(np.arange(n), num)
+        jj = np.concatenate([lst[start[k]:start[k] + num[k]] for k in range(n) if num[k] > 0]) if num.sum() else \
+            np.zeros(0, int)
+        a11, a21, a22, a31, a32, a33 = (float(v) for v in s.cell)
+        r11, r21, r22, r31, r32, r33 = (float(v) for v in s.rcell)
+        d = crd[jj] - crd[ii]
+        sx = np.floor(d[:, 0] * r11 + d[:, 1] * r21 + d[:, 2] * r31 + 0.5)
+        sy = np.floor(d[:, 1] * r22 + d[:, 2] * r32 + 0.5)
+        sz = np.floor(d[:, 2] * r33 + 0.5)
+        d[:, 0] -= sx * a11 + sy * a21 + sz * a31
+        d[:, 1] -= sy * a22 + sz * a32
+        d[:, 2] -= sz * a33
+        r2 = (d * d).sum(1)
+        r = np.sqrt(r2)
+        x = s.beta * r
+        qq = q[ii] * q[jj]
+        fa = -qq * (x * 2.0 / np.sqrt(np.pi) * np.exp(-x * x) + erfc(x) - 1.0) / r2 / r
+        g = fa[:, None] * d
+        frc = np.zeros((n, 3))
+        np.add.at(frc, ii, g)
+        np.add.at(frc, jj, -g)
+        e_atom = np.zeros(n)
+        np.add.at(e_atom, ii, -qq * erf(x) / r)
+        w = -np.stack([g[:, 0] * d[:, 0], g[:, 0] * d[:, 1] + g[:, 1] * d[:, 0], g[:, 1] * d[:, 1],
+                       g[:, 0] * d[:, 2] + g[:, 2] * d[:, 0], g[:, 1] * d[:, 2] + g[:, 2] * d[:, 1],
+                       g[:, 2] * d[:, 2]], 1)
+        vir = np.zeros((n, 6))
+        np.add.at(vir, ii, w)
+        return {"frc": frc, "e_atom": e_atom, "energy": float(e_atom.sum()), "virial_atom": vir, "pairs": len(ii)}
+
     def long_range_factor(self, s):
         return float(self.lib.orc_long_range_factor(s.n, _ci32(s.atom_type), s.n_types, _c32(s.pair_B),
                                                     s.cutoff))

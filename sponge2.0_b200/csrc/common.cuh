@@ -311,6 +311,7 @@ struct spgnb_lj
     float* d_lj_energy_atom = nullptr;
     long long* d_frc_acc = nullptr;  // 4 x int64 per local atom (reference-layout path)
     long long* d_totals = nullptr;   // 8 x int64 fixed point
+    long long* d_excl_total = nullptr;  // PME excluded-pair correction energy, int64 fixed point
     float4* d_pos = nullptr;         // per slot (spgnb list) or per atom (atom-group path)
     int* d_pos_type = nullptr;
     int pos_cap = 0;

@@ -819,6 +819,102 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
         }
 }
 
+// PME excluded-pair correction (Particle_Mesh::PME_Excluded_Force_With_Atom_Energy,
+// PM_force.cpp:918-997): reciprocal space includes every pair, excluded ones
+// too, so their smooth part erf(beta r)/r is taken back out.  One thread per
+// atom walks its (upper-triangular) exclusion list, as the reference does:
+//   dr = min image(r_j - r_i),  x = beta r,
+//   F_i += q_i q_j beta^3 h(x) dr,  F_j -= the same,  E_i -= q_i q_j erf(x)/r,
+//   W_i -= F (x) dr (the reference's symmetric virial form),
+// with h(x) = (erf(x) - 2/sqrt(pi) x exp(-x^2)) / x^3.  Below x = 0.7, h is
+// summed from its Taylor series (the series of erf and of x exp(-x^2)
+// combined: h = 2/sqrt(pi) sum_{n>=1} (-1)^(n+1) 2n x^(2n-2) / ((2n+1) n!))
+// instead of the difference of two nearly equal numbers, so the correction
+// keeps FP32 precision at bonded distances.  Forces accumulate in int64 fixed
+// point (the partner's share by atomics), the energy total likewise, so the
+// result does not depend on the order.
+__device__ __forceinline__ float excl_h(float x)
+{
+    const float x2 = x * x;
+    if (x < 0.7f)
+    {
+        // 2/sqrt(pi) * (2/3 - 2/5 x^2 + 1/7 x^4 - 1/27 x^6 + 1/132 x^8 - 1/780 x^10 + 1/5400 x^12
+        //               - 1/42840 x^14)
+        float p = -1.0f / 42840.0f;
+        p = __fmaf_rn(p, x2, 1.0f / 5400.0f);
+        p = __fmaf_rn(p, x2, -1.0f / 780.0f);
+        p = __fmaf_rn(p, x2, 1.0f / 132.0f);
+        p = __fmaf_rn(p, x2, -1.0f / 27.0f);
+        p = __fmaf_rn(p, x2, 1.0f / 7.0f);
+        p = __fmaf_rn(p, x2, -0.4f);
+        p = __fmaf_rn(p, x2, 2.0f / 3.0f);
+        return 1.1283791670955126f * p;
+    }
+    return (erff(x) - 1.1283791670955126f * x * expf(-x2)) / (x2 * x);
+}
+
+__global__ void k_pme_excluded(int n, const float3* __restrict__ crd, Cell cell, Cell rcell,
+                               const float* __restrict__ charge, float beta, const int* __restrict__ ex_start,
+                               const int* __restrict__ ex_list, const int* __restrict__ ex_num,
+                               long long* __restrict__ acc, float* __restrict__ atom_ene,
+                               float* __restrict__ atom_virial, long long* __restrict__ total)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    float ene = 0.0f;
+    if (i < n && ex_num[i] > 0)
+    {
+        const int k0 = ex_start[i], k1 = k0 + ex_num[i];
+        const float3 ri = crd[i];
+        const float qi = charge[i];
+        const float beta3 = beta * beta * beta;
+        float fx = 0.0f, fy = 0.0f, fz = 0.0f;
+        float w[6] = {0, 0, 0, 0, 0, 0};
+        for (int t = k0; t < k1; t++)
+        {
+            const int j = ex_list[t];
+            const float3 rj = crd[j];
+            // Get_Periodic_Displacement(r_j, r_i) (utils/vector.hpp:322-327)
+            float dx = rj.x - ri.x, dy = rj.y - ri.y, dz = rj.z - ri.z;
+            const float sx = floorf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31 + 0.5f);
+            const float sy = floorf(dy * rcell.a22 + dz * rcell.a32 + 0.5f);
+            const float sz = floorf(dz * rcell.a33 + 0.5f);
+            dx -= sx * cell.a11 + sy * cell.a21 + sz * cell.a31;
+            dy -= sy * cell.a22 + sz * cell.a32;
+            dz -= sz * cell.a33;
+            const float r2 = dx * dx + dy * dy + dz * dz;
+            const float r = sqrtf(r2);
+            const float x = beta * r;
+            const float qq = qi * charge[j];
+            const float fa = qq * beta3 * excl_h(x);
+            const float gx = fa * dx, gy = fa * dy, gz = fa * dz;
+            ene -= qq * erff(x) / r;
+            fx += gx;
+            fy += gy;
+            fz += gz;
+            atomicAdd((unsigned long long*)&acc[4 * (size_t)j + 0], (unsigned long long)__float2ll_rn(-gx * kTwoPow32));
+            atomicAdd((unsigned long long*)&acc[4 * (size_t)j + 1], (unsigned long long)__float2ll_rn(-gy * kTwoPow32));
+            atomicAdd((unsigned long long*)&acc[4 * (size_t)j + 2], (unsigned long long)__float2ll_rn(-gz * kTwoPow32));
+            // Get_Virial_From_Force_Dis(F, dr), subtracted
+            w[0] -= gx * dx;
+            w[1] -= gx * dy + gy * dx;
+            w[2] -= gy * dy;
+            w[3] -= gx * dz + gz * dx;
+            w[4] -= gy * dz + gz * dy;
+            w[5] -= gz * dz;
+        }
+        atomicAdd((unsigned long long*)&acc[4 * (size_t)i + 0], (unsigned long long)__float2ll_rn(fx * kTwoPow32));
+        atomicAdd((unsigned long long*)&acc[4 * (size_t)i + 1], (unsigned long long)__float2ll_rn(fy * kTwoPow32));
+        atomicAdd((unsigned long long*)&acc[4 * (size_t)i + 2], (unsigned long long)__float2ll_rn(fz * kTwoPow32));
+        if (atom_virial)
+            for (int q = 0; q < 6; q++) atom_virial[6 * (size_t)i + q] += w[q];
+        if (atom_ene) atom_ene[i] += ene;
+    }
+    // the energy total: one atomic per warp
+    long long qe = __double2ll_rn((double)ene * kEnergyScale);
+    for (int o = 16; o > 0; o >>= 1) qe += __shfl_xor_sync(0xffffffffu, qe, o);
+    if ((threadIdx.x & 31) == 0 && qe) atomicAdd((unsigned long long*)total, (unsigned long long)qe);
+}
+
 // Fixed point -> caller's float force (+=) for the reference-layout path,
 // accumulators cleared for the next call.
 __global__ void k_finalize(int n, long long* __restrict__ acc, float3* __restrict__ frc)
@@ -1312,11 +1408,12 @@ int spgnb_lj_create(int atom_numbers, int atom_type_numbers, const int* h_atom_t
     int st;
     if ((st = dalloc(&lj->d_atom_type, atom_numbers)) || (st = dalloc(&lj->d_table, table.size())) ||
         (st = dalloc(&lj->d_lj_energy_atom, atom_numbers)) || (st = dalloc(&lj->d_frc_acc, 4 * (size_t)atom_numbers)) ||
-        (st = dalloc(&lj->d_totals, 8)))
+        (st = dalloc(&lj->d_totals, 8)) || (st = dalloc(&lj->d_excl_total, 1)))
     {
         spgnb_lj_destroy(lj);
         return st;
     }
+    cudaMemset(lj->d_excl_total, 0, sizeof(long long));
     force_kernels_init(T * T);
     cudaMemcpy(lj->d_atom_type, h_atom_type, sizeof(int) * atom_numbers, cudaMemcpyHostToDevice);
     cudaMemcpy(lj->d_table, table.data(), sizeof(float2) * table.size(), cudaMemcpyHostToDevice);
@@ -1484,6 +1581,44 @@ int spgnb_lj_long_range_correction(spgnb_lj* lj, int need_pressure, spgnb_ltmatr
     return SPGNB_OK;
 }
 
+int spgnb_lj_pme_excluded_force(spgnb_lj* lj, int atom_numbers, const spgnb_vector* d_crd, spgnb_ltmatrix3 cell,
+                                spgnb_ltmatrix3 rcell, const float* d_charge, float pme_beta,
+                                const int* d_excluded_list_start, const int* d_excluded_list,
+                                const int* d_excluded_numbers, spgnb_vector* d_frc, int need_energy,
+                                float* d_atom_energy, spgnb_ltmatrix3* d_atom_virial)
+{
+    if (!lj) return fail(SPGNB_E_ARG, "spgnb_lj_pme_excluded_force: NULL handle");
+    if (atom_numbers < 0 || atom_numbers > lj->atom_numbers)
+        return fail(SPGNB_E_ARG, "spgnb_lj_pme_excluded_force: %d atoms, the module holds %d", atom_numbers,
+                    lj->atom_numbers);
+    if (atom_numbers == 0) return SPGNB_OK;
+    if (!d_crd || !d_charge || !d_frc || !d_excluded_list_start || !d_excluded_list || !d_excluded_numbers)
+        return fail(SPGNB_E_ARG, "spgnb_lj_pme_excluded_force: NULL device pointer");
+    if (need_energy && !d_atom_energy) return fail(SPGNB_E_ARG, "spgnb_lj_pme_excluded_force: NULL atom_energy");
+    cudaStream_t s = stream();
+    SPGNB_CUDA(cudaMemsetAsync(lj->d_excl_total, 0, sizeof(long long), s));
+    const int n = atom_numbers;
+    k_pme_excluded<<<(n + 255) / 256, 256, 0, s>>>(n, (const float3*)d_crd, make_cell(cell), make_cell(rcell),
+                                                   d_charge, pme_beta, d_excluded_list_start, d_excluded_list,
+                                                   d_excluded_numbers, lj->d_frc_acc,
+                                                   need_energy ? d_atom_energy : nullptr, (float*)d_atom_virial,
+                                                   lj->d_excl_total);
+    SPGNB_CHECK_LAUNCH("k_pme_excluded");
+    k_finalize<<<(n + 255) / 256, 256, 0, s>>>(n, lj->d_frc_acc, (float3*)d_frc);
+    SPGNB_CHECK_LAUNCH("k_finalize");
+    return SPGNB_OK;
+}
+
+int spgnb_lj_pme_excluded_energy(spgnb_lj* lj, double* energy)
+{
+    if (!lj || !energy) return fail(SPGNB_E_ARG, "spgnb_lj_pme_excluded_energy: NULL argument");
+    long long h = 0;
+    SPGNB_CUDA(cudaMemcpyAsync(&h, lj->d_excl_total, sizeof(h), cudaMemcpyDeviceToHost, stream()));
+    SPGNB_CUDA(cudaStreamSynchronize(stream()));
+    *energy = (double)h / kEnergyScale;
+    return SPGNB_OK;
+}
+
 int spgnb_lj_totals(spgnb_lj* lj, double out[8])
 {
     if (!lj || !out) return fail(SPGNB_E_ARG, "spgnb_lj_totals: NULL argument");
@@ -1538,6 +1673,7 @@ int spgnb_lj_destroy(spgnb_lj* lj)
     dfree(lj->d_lj_energy_atom);
     dfree(lj->d_frc_acc);
     dfree(lj->d_totals);
+    dfree(lj->d_excl_total);
     dfree(lj->d_pos);
     dfree(lj->d_pos_type);
     dfree(lj->d_sdata);

@@ -207,6 +207,26 @@ class LENNARD_JONES_INFORMATION:
         check(lib().spgnb_lj_long_range_correction(self.handle, int(need_pressure), _ptr(d_virial),
                                                    int(need_potential), _ptr(d_potential), float(volume)))
 
+    def PME_Excluded_Force_With_Atom_Energy(self, atom_numbers, crd, cell, rcell, charge, pme_beta,
+                                           excluded_list_start, excluded_list, excluded_numbers, frc,
+                                           need_energy, atom_energy, atom_virial=None):
+        """Particle_Mesh::PME_Excluded_Force_With_Atom_Energy (PM_force.cpp:918-997):
+        the erf(beta r)/r part of every excluded pair taken back out of the
+        forces (+=), per-atom energies (+=) and per-atom virials (+=)."""
+        _bind_stream()
+        check(lib().spgnb_lj_pme_excluded_force(self.handle, int(atom_numbers), _ptr(crd), LTMatrix3.of(cell),
+                                                LTMatrix3.of(rcell), _ptr(charge), float(pme_beta),
+                                                _ptr(excluded_list_start), _ptr(excluded_list),
+                                                _ptr(excluded_numbers), _ptr(frc), int(need_energy),
+                                                _ptr(atom_energy), _ptr(atom_virial)))
+
+    def excluded_energy(self):
+        """FP64 total of the last excluded-pair correction."""
+        _bind_stream()
+        e = C.c_double()
+        check(lib().spgnb_lj_pme_excluded_energy(self.handle, C.byref(e)))
+        return e.value
+
     def totals(self):
         """FP64 totals of the last call: E_lj, E_coulomb_direct, virial (6)."""
         _bind_stream()

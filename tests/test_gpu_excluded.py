@@ -1,0 +1,52 @@
+"""PME excluded-pair correction (Particle_Mesh::PME_Excluded_Force_With_Atom_Energy,
+PM_force.cpp:918-997) on the GPU against the FP64 oracle: forces within the
+force tolerance of the parity tests, per-atom and total energies, per-atom
+virials; two calls give bitwise the same forces."""
+import numpy as np
+import pytest
+
+from conftest import rel_rms
+
+pytestmark = pytest.mark.gpu
+
+FORCE_REL_RMS_TOL = 1e-5
+ENERGY_REL_TOL = 1e-6
+
+
+def _systems():
+    from spgnb import systems as S
+    return {
+        "water-1944": S.water_system(648, 26.9, 21, cutoff=8.0, skin=2.0, name="water-1944"),
+        "mixed-small": S.water_system(900, 31.0, 22, n_solute=300, cutoff=10.0, skin=2.0, name="mixed-small"),
+        "triclinic": S.water_system(1000, (33.0, 33.0, 33.0), 23, cutoff=8.0, skin=2.0,
+                                    angles=(80.0, 95.0, 105.0), name="triclinic"),
+    }
+
+
+@pytest.mark.parametrize("name", ["water-1944", "mixed-small", "triclinic"])
+def test_pme_excluded_correction_vs_fp64(torch_cuda, name):
+    import oracle as O
+    from spgnb.engine import PlainPath
+    torch = torch_cuda
+    s = _systems()[name]
+    p = PlainPath(s, export_atom_groups=False, device="cuda:0")
+    ref = O.Oracle.pme_excluded(s)
+    assert ref["pairs"] > 0
+    outs = []
+    for _ in range(2):
+        frc = torch.zeros_like(p.frc)
+        ene = torch.zeros_like(p.atom_energy)
+        vir = torch.zeros_like(p.atom_virial)
+        p.lj.PME_Excluded_Force_With_Atom_Energy(s.n, p.crd, s.cell, s.rcell, p.charge, s.beta, p.excl_start,
+                                                 p.excl_list, p.excl_numbers, frc, 1, ene, vir)
+        torch.cuda.synchronize()
+        outs.append((frc.cpu().numpy(), ene.cpu().numpy(), vir.cpu().numpy(), p.lj.excluded_energy()))
+    (frc, ene, vir, tot), (frc2, _, _, tot2) = outs
+    assert np.array_equal(frc, frc2) and tot == tot2, "not reproducible"
+    err = rel_rms(frc, ref["frc"])
+    assert err <= FORCE_REL_RMS_TOL, f"{name}: force rel RMS {err:.3e}"
+    assert abs(tot - ref["energy"]) <= ENERGY_REL_TOL * abs(ref["energy"]) + 1e-3
+    e_scale = np.abs(ref["e_atom"]).max()
+    assert np.abs(ene - ref["e_atom"]).max() <= 1e-5 * e_scale
+    v_scale = np.abs(ref["virial_atom"]).max()
+    assert np.abs(vir - ref["virial_atom"]).max() <= 1e-5 * v_scale
