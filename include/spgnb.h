@@ -169,6 +169,18 @@ typedef struct
 int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out);
 
 /* NEIGHBOR_LIST::Clear (neighbor_list.h:26, neighbor_list.cpp:967-981). */
+/* FULL_NEIGHBOR_LIST::Build_From_Half / Build_From_Half_With_Cutoff
+ * (full_neighbor_list.cpp:27-147), called where NEIGHBOR_LIST::Update calls
+ * them (neighbor_list.cpp:871-882): every pair of the current list in both
+ * atoms' lists, written into the caller's ATOM_GROUP array (atom_serial
+ * pointers set by the caller, max_neighbor_numbers entries each).  cutoff > 0
+ * keeps the pairs within it at d_crd (the reference passes cutoff_full +
+ * skin).  A list longer than max_neighbor_numbers gets its full count and
+ * sets *d_overflow to 1.  Lists come in a fixed order (no atomics). */
+int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector* d_crd, spgnb_ltmatrix3 cell,
+                        spgnb_ltmatrix3 rcell, float cutoff, spgnb_atom_group* d_full_nl, int max_neighbor_numbers,
+                        int* d_overflow);
+
 int spgnb_nl_destroy(spgnb_nl* nl);
 
 /* ----------------------------------------------- LENNARD_JONES_INFORMATION */

@@ -657,6 +657,102 @@ __global__ void k_export(int clusters_cap, int table_cap, const int* __restrict_
     }
 }
 
+// FULL_NEIGHBOR_LIST::Build_From_Half / Build_From_Half_With_Cutoff
+// (full_neighbor_list.cpp:27-147): every listed pair in both atoms' lists, in
+// the caller's ATOM_GROUP arrays.  Built from the cluster tables, where each
+// atom's partners on both sides already sit with its own cluster, so one warp
+// per cluster writes its atoms' complete lists in table order: no atomics,
+// the same order on every call.  With a cutoff, a pair is kept when its
+// distance at d_crd is within it, measured from the lower-index atom as the
+// reference does (Get_Periodic_Displacement(r_i, r_j)).
+__global__ void k_export_full(int clusters_cap, int table_cap, const int* __restrict__ tcount,
+                              const float4* __restrict__ tab, const uint2* __restrict__ tmask,
+                              const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0,
+                              const float3* __restrict__ crd, Cell cell, Cell rcell, float cut2,
+                              spgnb_atom_group* __restrict__ full, int max_nb, int* __restrict__ overflow)
+{
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < clusters_cap; c += warps)
+    {
+        const int T = tcount[c];
+        if (T == 0) continue;
+        // lane a < 8: own atom a, its global index, list and running count
+        const int own_atom = lane < 8 ? slot_atom[c * kClusterSize + lane] : -1;
+        const int own_g = lane < 8 ? __float_as_int(slot_x0[c * kClusterSize + lane].w) : -1;
+        int* own_list = own_atom >= 0 ? full[own_atom].atom_serial : nullptr;
+        int count = 0;
+        for (int t0 = 0; t0 < T; t0 += 32)
+        {
+            const int t = t0 + lane;
+            unsigned long long m = 0;
+            int base = 0;
+            if (t < T)
+            {
+                const uint2 mm = tmask[(size_t)c * table_cap + t];
+                m = ((unsigned long long)mm.y << 32) | mm.x;
+                base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
+            }
+            for (int a = 0; a < kClusterSize; a++)
+            {
+                const int ia = __shfl_sync(0xffffffffu, own_atom, a);
+                if (ia < 0) continue;  // warp-uniform
+                const int gia = __shfl_sync(0xffffffffu, own_g, a);
+                const unsigned row = (unsigned)(m >> (8 * a)) & 0xffu;
+                unsigned keep = row;
+                if (cut2 >= 0.0f && row)
+                {
+                    const float3 xi = crd[ia];
+                    keep = 0;
+                    for (unsigned r = row; r; r &= r - 1)
+                    {
+                        const int b = __ffs(r) - 1;
+                        const int jb = slot_atom[base + b];
+                        const float3 xj = crd[jb];
+                        const bool i_lo = gia < __float_as_int(slot_x0[base + b].w);
+                        const float d2 = i_lo ? ref_pair_dr2(xi, xj, cell, rcell) : ref_pair_dr2(xj, xi, cell, rcell);
+                        if (d2 <= cut2) keep |= 1u << b;
+                    }
+                }
+                const int k = __popc(keep);
+                int incl = k;
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                int pos = __shfl_sync(0xffffffffu, count, a) + incl - k;
+                int* list = (int*)__shfl_sync(0xffffffffu, (unsigned long long)own_list, a);
+                for (unsigned r = keep; r; r &= r - 1, pos++)
+                {
+                    const int b = __ffs(r) - 1;
+                    if (pos < max_nb)
+                        list[pos] = slot_atom[base + b];
+                    else
+                        atomicExch(overflow, 1);
+                }
+                if (lane == a) count += total;
+            }
+        }
+        if (own_atom >= 0)
+        {
+            full[own_atom].atom_numbers = count;
+            full[own_atom].ghost_numbers = 0;
+        }
+    }
+}
+
+__global__ void k_zero_groups(int n, spgnb_atom_group* __restrict__ g)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        g[i].atom_numbers = 0;
+        g[i].ghost_numbers = 0;
+    }
+}
+
 __global__ void k_finish(int G, int S, const int* __restrict__ cell_sys, const int* __restrict__ need,
                          int* __restrict__ prune, int* __restrict__ cell_count, int* __restrict__ cell_cursor,
                          int* counters)
@@ -1648,6 +1744,32 @@ int spgnb_nl_copy_atom_groups(spgnb_nl* nl, int* h_counts, int* h_lists, long lo
             off += h[i].atom_numbers;
         }
     }
+    return SPGNB_OK;
+}
+
+int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector* d_crd, spgnb_ltmatrix3 cell,
+                        spgnb_ltmatrix3 rcell, float cutoff, spgnb_atom_group* d_full_nl, int max_neighbor_numbers,
+                        int* d_overflow)
+{
+    if (!nl || !d_full_nl) return fail(SPGNB_E_ARG, "spgnb_nl_build_full: NULL argument");
+    if (!nl->built) return fail(SPGNB_E_STATE, "spgnb_nl_build_full: the list was never built");
+    if (local_atom_numbers != nl->local_atoms)
+        return fail(SPGNB_E_ARG, "spgnb_nl_build_full: %d local atoms, the list was built for %d", local_atom_numbers,
+                    nl->local_atoms);
+    if (max_neighbor_numbers <= 0) return fail(SPGNB_E_ARG, "spgnb_nl_build_full: max_neighbor_numbers must be positive");
+    if (cutoff > 0.0f && !d_crd) return fail(SPGNB_E_ARG, "spgnb_nl_build_full: a cutoff needs coordinates");
+    if (!d_overflow) return fail(SPGNB_E_ARG, "spgnb_nl_build_full: NULL overflow flag");
+    cudaStream_t s = stream();
+    const int n = local_atom_numbers;
+    // atoms in no cluster with a table (none, normally) keep a zero count
+    k_zero_groups<<<(n + 255) / 256, 256, 0, s>>>(n, d_full_nl);
+    SPGNB_CHECK_LAUNCH("k_zero_groups");
+    const int ccap = nl->clusters_cap;
+    k_export_full<<<std::max(1, std::min((ccap + 3) / 4, num_sms() * 8)), 128, 0, s>>>(
+        ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0,
+        (const float3*)d_crd, make_cell(cell), make_cell(rcell), cutoff > 0.0f ? cutoff * cutoff : -1.0f, d_full_nl,
+        max_neighbor_numbers, d_overflow);
+    SPGNB_CHECK_LAUNCH("k_export_full");
     return SPGNB_OK;
 }
 

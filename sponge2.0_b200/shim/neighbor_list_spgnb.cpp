@@ -144,11 +144,14 @@ void NEIGHBOR_LIST::Update(int* atom_local, int local_atom_numbers, int ghost_nu
           "NEIGHBOR_LIST::Update");
     if (this->is_needed_full && full_neighbor_list.is_initialized)
     {
-        if (this->cutoff_full > 0.0f)
-            full_neighbor_list.Build_From_Half_With_Cutoff(this->d_nl, local_atom_numbers, crd, cell, rcell,
-                                                           this->cutoff_full + skin);
-        else
-            full_neighbor_list.Build_From_Half(this->d_nl, local_atom_numbers);
+        // FULL_NEIGHBOR_LIST::Build_From_Half[_With_Cutoff], from the cluster
+        // tables into the full list's own arrays
+        raise(spgnb_shim::default_controller(),
+              spgnb_nl_build_full(h, local_atom_numbers, (const spgnb_vector*)crd, ltm(cell), ltm(rcell),
+                                  this->cutoff_full > 0.0f ? this->cutoff_full + skin : 0.0f,
+                                  (spgnb_atom_group*)full_neighbor_list.d_nl, full_neighbor_list.max_neighbor_numbers,
+                                  full_neighbor_list.d_overflow),
+              "FULL_NEIGHBOR_LIST::Build_From_Half");
     }
     updator.time_recorder->Stop();
 }

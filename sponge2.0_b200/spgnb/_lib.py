@@ -24,7 +24,7 @@ EXPORTED = [
     "spgnb_lj_create", "spgnb_lj_get_local", "spgnb_lj_pme_direct_force", "spgnb_lj_pme_direct_force_atom_groups",
     "spgnb_lj_long_range_correction", "spgnb_lj_energies", "spgnb_lj_totals", "spgnb_lj_long_range_factor",
     "spgnb_lj_destroy", "spgnb_lj_atom_lj_energy", "spgnb_lj_export_vector_lj",
-    "spgnb_lj_pme_excluded_force", "spgnb_lj_pme_excluded_energy",
+    "spgnb_lj_pme_excluded_force", "spgnb_lj_pme_excluded_energy", "spgnb_nl_build_full",
     "spgnb_solvent_create", "spgnb_solvent_get_local", "spgnb_solvent_pme_direct_force", "spgnb_solvent_destroy",
     "spgnb_launch_count", "spgnb_debug_set_pair_events", "spgnb_nl_count_pairs", "spgnb_probe_fp32_fma_tflops",
     "spgnb_lj_pme_direct_force_noalloc",
@@ -117,6 +117,7 @@ def lib():
     L.spgnb_nl_copy_atom_groups.argtypes = [vp, vp, vp, C.c_longlong, C.POINTER(C.c_longlong)]
     L.spgnb_nl_get_stats.argtypes = [vp, C.POINTER(NLStats)]
     L.spgnb_nl_destroy.argtypes = [vp]
+    L.spgnb_nl_build_full.argtypes = [vp, i, vp, M, M, f, vp, i, vp]
     L.spgnb_batch_default_options.argtypes = [C.POINTER(BatchOptions)]
     L.spgnb_batch_default_options.restype = None
     L.spgnb_batch_create.argtypes = [i, C.POINTER(BatchSystem), i, vp, vp, C.POINTER(BatchOptions), C.POINTER(vp)]
