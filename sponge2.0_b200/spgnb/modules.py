@@ -141,17 +141,22 @@ class NEIGHBOR_LIST:
                 "clusters": s.clusters, "entries": s.entries, "work_items": s.work_items, "builds": s.builds,
                 "overflow": s.overflow}
 
-    def build_full(self, local_atom_numbers, crd, cell, rcell, cutoff_full, max_neighbor_numbers):
+    def build_full(self, local_atom_numbers, crd, cell, rcell, cutoff_full, max_neighbor_numbers, out=None):
         """FULL_NEIGHBOR_LIST::Build_From_Half[_With_Cutoff] (full_neighbor_list.cpp:27-147):
-        returns (counts, lists) device tensors, lists[i, :counts[i]] the
-        partners of atom i; cutoff_full <= 0 keeps every listed pair."""
+        returns (counts, lists, overflow) device tensors, lists[i, :counts[i]]
+        the partners of atom i; cutoff_full <= 0 keeps every listed pair.
+        ``out`` = the (lists, groups, overflow) of an earlier call, reused."""
         _bind_stream()
         n, m = int(local_atom_numbers), int(max_neighbor_numbers)
         dev = crd.device
-        temp = torch.zeros((n, m), dtype=torch.int32, device=dev)
-        groups = torch.zeros((n, 2), dtype=torch.int64, device=dev)  # {count, ghost}, atom_serial
-        groups[:, 1] = temp.data_ptr() + 4 * m * torch.arange(n, dtype=torch.int64, device=dev)
-        overflow = torch.zeros(1, dtype=torch.int32, device=dev)
+        if out is None:
+            temp = torch.zeros((n, m), dtype=torch.int32, device=dev)
+            groups = torch.zeros((n, 2), dtype=torch.int64, device=dev)  # {count, ghost}, atom_serial
+            groups[:, 1] = temp.data_ptr() + 4 * m * torch.arange(n, dtype=torch.int64, device=dev)
+            overflow = torch.zeros(1, dtype=torch.int32, device=dev)
+        else:
+            temp, groups, overflow = out
+        self._full_out = (temp, groups, overflow)
         check(lib().spgnb_nl_build_full(self.handle, n, _ptr(crd), LTMatrix3.of(cell), LTMatrix3.of(rcell),
                                         float(cutoff_full), groups.data_ptr(), m, overflow.data_ptr()))
         counts = groups.view(torch.int32)[:, 0]
