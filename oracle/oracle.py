@@ -189,7 +189,7 @@ class Reference:
         lib.ref_time_rebuild.restype = C.c_double
         lib.ref_time_rebuild.argtypes = [_f32p, C.c_int]
         lib.ref_long_range_factor.restype = C.c_double
-        lib.ref_enable_solvent.argtypes = [C.c_int, _i32p, C.c_int, C.c_int]
+        lib.ref_enable_solvent.argtypes = [C.c_int, _i32p, C.c_int, C.c_int, C.c_int]
         lib.ref_set_threads.argtypes = [C.c_int]
         self.lib = lib
         self.gpu = bool(lib.ref_is_gpu())
@@ -207,7 +207,8 @@ class Reference:
                           _ci32(s.excl_numbers), ex, len(s.excl_list))
         if solvent:
             first_res = len(s.res_start) - s.n_waters
-            rc = self.lib.ref_enable_solvent(len(s.res_start), _ci32(s.res_start), first_res, 3 * s.n_waters)
+            wp = getattr(s, "water_points", 3)
+            rc = self.lib.ref_enable_solvent(len(s.res_start), _ci32(s.res_start), first_res, wp * s.n_waters, wp)
             if rc != 0 and not self.shim:
                 raise RuntimeError("the solvent module exists only in the reference's GPU build")
 

@@ -224,17 +224,18 @@ long long ref_nl_get(int* counts, int* lists, long long capacity, int* overflow_
 }
 
 // The water-residue module, configured the way SOLVENT_LENNARD_JONES::Initial
-// and Get_Local leave it for a trailing run of 3-site waters
+// and Get_Local leave it for a trailing run of 3- or 4-site waters
 // (solvent_LJ.cpp:186-228, :469-482).  GPU build only: the reference disables
 // the module on CPU builds (solvent_LJ.cpp:183-185).
-int ref_enable_solvent(int res_numbers, const int* res_start, int first_water_residue, int solvent_atoms)
+int ref_enable_solvent(int res_numbers, const int* res_start, int first_water_residue, int solvent_atoms,
+                       int water_points)
 {
 #if defined(USE_GPU) && !defined(REF_HARNESS_SHIM)
     S.lj_soft = new LJ_SOFT_CORE();
     S.slj = new SOLVENT_LENNARD_JONES();
     S.slj->lj_info = S.lj;
     S.slj->lj_soft_info = S.lj_soft;
-    S.slj->water_points = 3;
+    S.slj->water_points = water_points;
     S.slj->solvent_numbers = solvent_atoms;
     S.slj->solvent_start = first_water_residue;
     S.slj->solvent_start_local = first_water_residue;
@@ -250,6 +251,7 @@ int ref_enable_solvent(int res_numbers, const int* res_start, int first_water_re
     (void)res_start;
     (void)first_water_residue;
     (void)solvent_atoms;
+    (void)water_points;
     return -1;
 #endif
 }

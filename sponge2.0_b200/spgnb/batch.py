@@ -42,6 +42,8 @@ def _ptr(a):
 
 def _fill(y, s, keep):
     """Fill a BatchSystem from a ``spgnb.systems`` system; arrays go to keep."""
+    if getattr(s, "water_points", 3) != 3:
+        raise ValueError("the batched engine constrains 3-site waters (SETTLE) only")
     crd = np.ascontiguousarray(s.crd, np.float32)
     vel = np.ascontiguousarray(s.vel if s.vel is not None else np.zeros_like(s.crd), np.float32)
     charge = np.ascontiguousarray(s.charge, np.float32)

@@ -45,7 +45,7 @@ class PlainPath:
         self.solvent_numbers = 0
         self.solvent = SOLVENT_LENNARD_JONES()
         if solvent and s.n_waters > 0:
-            self.solvent.Initial(controller, self.lj, 3, default_enable=True)
+            self.solvent.Initial(controller, self.lj, s.water_points, default_enable=True)
             res_len = torch.from_numpy(np.ascontiguousarray(s.res_len, np.int32)).to(dev)
             mass = torch.from_numpy(np.ascontiguousarray(s.mass, np.float32)).to(dev)
             self.res_start = torch.from_numpy(np.ascontiguousarray(s.res_start, np.int32)).to(dev)

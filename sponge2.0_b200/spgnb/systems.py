@@ -40,6 +40,13 @@ EPS_O = 0.1521
 MASS_O = 16.00
 MASS_H = 1.008
 MASS_SOLUTE = 12.011
+# 4-site water (TIP4P, Jorgensen et al. 1983): the negative charge on a
+# massless site M on the bisector, 0.15 A from O; LJ on O
+OM_DIST_4 = 0.15
+Q_H_4 = 0.52
+Q_M_4 = -1.04
+SIGMA_O_4 = 3.15365
+EPS_O_4 = 0.1550
 
 
 def cell_from_box(a, b, c, alpha=90.0, beta=90.0, gamma=90.0):
@@ -153,6 +160,7 @@ class System:
     vel: np.ndarray = field(default=None)
     n_solute: int = 0
     name: str = ""
+    water_points: int = 3      # sites per water residue (3, or 4 with a massless charge site)
 
     @property
     def n(self):
@@ -160,7 +168,7 @@ class System:
 
     @property
     def n_waters(self):
-        return (self.n - self.n_solute) // 3
+        return (self.n - self.n_solute) // self.water_points
 
     @property
     def volume(self):
@@ -168,8 +176,8 @@ class System:
 
     @property
     def solvent_atoms(self):
-        """Atoms in the trailing run of 3-site water residues."""
-        return 3 * self.n_waters
+        """Atoms in the trailing run of water residues."""
+        return self.water_points * self.n_waters
 
 
 def _random_rotations(rng, n):
@@ -197,8 +205,11 @@ def _solute_types(rng, n_types=20):
 
 def water_system(n_waters, box, seed, n_solute=0, cutoff=10.0, skin=2.0,
                  tolerance=1e-5, jitter=0.3, angles=(90.0, 90.0, 90.0),
-                 temperature=300.0, n_solute_types=20, name="", solute_types=None):
+                 temperature=300.0, n_solute_types=20, name="", solute_types=None, water_points=3):
     """Water (+ optional LJ solute) box on a jittered lattice.
+
+    water_points = 4 makes 4-site waters O, H, H, M (the TIP4P geometry and
+    charges, M massless, LJ on O) for the 4-point solvent path.
 
     Lattice sites fill the box; waters sit on jittered sites with uniformly
     random orientations, solutes (if any) take other sites unjittered, and
@@ -227,8 +238,11 @@ def water_system(n_waters, box, seed, n_solute=0, cutoff=10.0, skin=2.0,
         sol_sig, sol_eps = solute_types
     elif n_solute:
         sol_sig, sol_eps = _solute_types(rng, n_solute_types)
-    sigma_all = np.concatenate([[SIGMA_O, 0.0], sol_sig if sol_sig is not None else []])
-    eps_all = np.concatenate([[EPS_O, 0.0], sol_eps if sol_eps is not None else []])
+    if water_points not in (3, 4):
+        raise ValueError("water_points must be 3 or 4")
+    w4 = water_points == 4
+    sigma_all = np.concatenate([[SIGMA_O_4 if w4 else SIGMA_O, 0.0], sol_sig if sol_sig is not None else []])
+    eps_all = np.concatenate([[EPS_O_4 if w4 else EPS_O, 0.0], sol_eps if sol_eps is not None else []])
     n_types = len(sigma_all)
     pair_A, pair_B = lj_pair_tables(sigma_all, eps_all)
 
@@ -241,13 +255,17 @@ def water_system(n_waters, box, seed, n_solute=0, cutoff=10.0, skin=2.0,
 
     # water geometry in its body frame, O at the origin
     half = math.radians(HOH_ANGLE_DEG) / 2
-    body = np.array([[0.0, 0.0, 0.0],
-                     [OH_BOND * math.sin(half), 0.0, OH_BOND * math.cos(half)],
-                     [-OH_BOND * math.sin(half), 0.0, OH_BOND * math.cos(half)]])
+    sites = [[0.0, 0.0, 0.0],
+             [OH_BOND * math.sin(half), 0.0, OH_BOND * math.cos(half)],
+             [-OH_BOND * math.sin(half), 0.0, OH_BOND * math.cos(half)]]
+    if w4:
+        sites.append([0.0, 0.0, OM_DIST_4])
+    body = np.array(sites)
     R = _random_rotations(rng, n_waters)
     wat = wat_center[:, None, :] + np.einsum("nij,kj->nki", R, body)
 
-    n = n_solute + 3 * n_waters
+    wp = water_points
+    n = n_solute + wp * n_waters
     crd = np.empty((n, 3), np.float64)
     crd[:n_solute] = sol_center
     crd[n_solute:] = wat.reshape(-1, 3)
@@ -258,40 +276,41 @@ def water_system(n_waters, box, seed, n_solute=0, cutoff=10.0, skin=2.0,
         q = rng.normal(0.0, 0.4, n_solute)
         q -= q.mean()
         charge[:n_solute] = q
-    charge[n_solute:] = np.tile([Q_O, Q_H, Q_H], n_waters)
+    charge[n_solute:] = np.tile([0.0, Q_H_4, Q_H_4, Q_M_4] if w4 else [Q_O, Q_H, Q_H], n_waters)
     charge = (charge.astype(np.float32) * CHARGE_SCALE).astype(np.float32)
 
     atom_type = np.empty(n, np.int32)
     atom_type[:n_solute] = sol_type
-    atom_type[n_solute:] = np.tile([0, 1, 1], n_waters)
+    atom_type[n_solute:] = np.tile([0, 1, 1, 1] if w4 else [0, 1, 1], n_waters)
 
     mass = np.empty(n, np.float32)
     mass[:n_solute] = MASS_SOLUTE
-    mass[n_solute:] = np.tile([MASS_O, MASS_H, MASS_H], n_waters)
+    mass[n_solute:] = np.tile([MASS_O, MASS_H, MASS_H, 0.0] if w4 else [MASS_O, MASS_H, MASS_H], n_waters)
 
-    # exclusions: intra-water O-H1, O-H2, H1-H2 (upper triangular)
+    # exclusions: every intra-water pair (upper triangular)
     excl_numbers = np.zeros(n, np.int32)
-    o = n_solute + 3 * np.arange(n_waters)
-    excl_numbers[o] = 2
-    excl_numbers[o + 1] = 1
+    o = n_solute + wp * np.arange(n_waters)
+    for k in range(wp - 1):
+        excl_numbers[o + k] = wp - 1 - k
     excl_start = np.zeros(n, np.int32)
     excl_start[1:] = np.cumsum(excl_numbers)[:-1]
     excl_list = np.empty(int(excl_numbers.sum()), np.int32)
-    s = excl_start[o]
-    excl_list[s] = o + 1
-    excl_list[s + 1] = o + 2
-    excl_list[excl_start[o + 1]] = o + 2
+    for k in range(wp - 1):
+        for t, partner in enumerate(range(k + 1, wp)):
+            excl_list[excl_start[o + k] + t] = o + partner
 
-    res_len = np.concatenate([np.ones(n_solute, np.int32), np.full(n_waters, 3, np.int32)])
+    res_len = np.concatenate([np.ones(n_solute, np.int32), np.full(n_waters, wp, np.int32)])
     res_start = np.zeros(len(res_len), np.int32)
     res_start[1:] = np.cumsum(res_len)[:-1]
 
-    vel = (rng.normal(size=(n, 3)) * np.sqrt(KB * temperature / mass)[:, None]).astype(np.float32)
+    vel = (rng.normal(size=(n, 3)) * np.sqrt(KB * temperature / np.maximum(mass, 1e-30))[:, None]).astype(np.float32)
+    vel[mass == 0] = 0.0
     return System(crd=crd, charge=charge, atom_type=atom_type, pair_A=pair_A, pair_B=pair_B,
                   n_types=n_types, excl_start=excl_start, excl_numbers=excl_numbers,
                   excl_list=excl_list, mass=mass, res_start=res_start, res_len=res_len,
                   cell=cell, rcell=rcell, cutoff=float(cutoff), skin=float(skin),
-                  beta=get_beta(cutoff, tolerance), vel=vel, n_solute=n_solute, name=name)
+                  beta=get_beta(cutoff, tolerance), vel=vel, n_solute=n_solute, name=name,
+                  water_points=wp)
 
 
 def _resolve_solute_overlaps(rng, sol_center, sol_type, wat_center, sigma, cell, box, jitter,
