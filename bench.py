@@ -527,6 +527,11 @@ def main():
         fb.synchronize()
         full_ms.append(fa.elapsed_time(fb))
 
+    # the alchemical path on the same box: LJ_SOFT_CORE with a 40-atom perturbed
+    # ligand (main.cpp:379-385), per step the list update and the soft-core
+    # force, timed on its own; and one dH/dlambda evaluation (it reads back)
+    soft = _time_soft_core(s, fe, dev, stream, flush)
+
     if dist is not None:
         t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
@@ -564,6 +569,7 @@ def main():
             "gpu_launches": int(launches),
             "pme_excluded_correction_ms": excluded_ms,
             "full_neighbor_list_ms": min(full_ms),
+            "soft_core": soft,
             "e2e": {"value": world * s.n * K / (e2e_total * 1e-3), "unit": "atom-steps/s",
                     "h2d_bytes_per_step": s.n * 12, "d2h_bytes_per_step": s.n * 12 + (64 if fe else 0)},
         }
@@ -580,6 +586,35 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _time_soft_core(s, fe, dev, stream, flush, steps=50):
+    import torch
+    from spgnb import systems as S
+    from spgnb.engine import SoftCorePath
+    f = S.fep_system(s, n_perturbed=40, seed=11, lam=0.6)
+    p = SoftCorePath(f, refresh_interval=REFRESH_INTERVAL, device=dev)
+    for k in range(5):
+        p.step(k, need_energy=fe, need_virial=fe, per_atom=False)
+    torch.cuda.synchronize()
+    ms = []
+    for k in range(steps):
+        flush.fill_(k & 0xff)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        p.step(5 + k, need_energy=fe, need_virial=fe, per_atom=False)
+        b.record(stream)
+        b.synchronize()
+        ms.append(a.elapsed_time(b))
+    import time
+    p.dhdl(charge_perturbated=True)
+    t0 = time.perf_counter()
+    for _ in range(5):
+        p.dhdl(charge_perturbated=True)
+    dh_ms = (time.perf_counter() - t0) * 1e3 / 5
+    return {"ligand_atoms": int(len(p.lj.perturbed_atoms())), "lambda": f.lam, "steps": steps,
+            "ms_per_step": sum(ms) / steps, "atom_steps_per_s": s.n * steps / (sum(ms) * 1e-3),
+            "dhdl_ms_host": dh_ms}
 
 
 def _ltm(m):

@@ -8,6 +8,7 @@
  *   NEIGHBOR_LIST               SPONGE/neighbor_list/neighbor_list.h:7-128
  *   LENNARD_JONES_INFORMATION   SPONGE/Lennard_Jones_force/Lennard_Jones_force.h:86-173
  *   SOLVENT_LENNARD_JONES       SPONGE/Lennard_Jones_force/solvent_LJ.h:9-43
+ *   LJ_SOFT_CORE                SPONGE/Lennard_Jones_force/LJ_soft_core.h:162-276
  *
  * Conventions (same as the reference):
  *   - coordinates, charges, forces, energies and virials are DEVICE pointers
@@ -271,6 +272,101 @@ int spgnb_lj_pme_excluded_force(spgnb_lj* lj, int atom_numbers, const spgnb_vect
 int spgnb_lj_pme_excluded_energy(spgnb_lj* lj, double* energy);
 
 int spgnb_lj_destroy(spgnb_lj* lj);
+
+/* ------------------------------------------------------------ LJ_SOFT_CORE */
+/* Alchemical (FEP) LJ + PME direct space with soft cores, LJ_SOFT_CORE
+ * (LJ_soft_core.h:162-276, LJ_soft_core.cpp:198-436).  Every atom has a
+ * state-A and a state-B LJ type, each state its own triangular pair tables
+ * (AA, AB: state A's r^-12 and r^-6 coefficients; BA, BB: state B's).  Per
+ * pair inside the cutoff (dr = r_j - r_i, lambda' = 1 - lambda):
+ *   - when BA*AA != 0 or BA + AA == 0, the states are mixed linearly:
+ *       F/r = lambda' LJ(r; AA, AB) + lambda LJ(r; BA, BB) - Coulomb(r);
+ *   - otherwise (one state has no r^-12 term) each state is evaluated at its
+ *     soft-core distance r_X = (r^6 + alpha lambda_X^p sigma_X)^(1/6),
+ *     lambda_A = lambda, lambda_B = lambda', sigma_X = sigma^6 when the
+ *     state's A or B is zero, else max(A / (2 B), sigma_min^6).
+ * B200 layout: atoms whose pairs can differ between the states (a minimal
+ * vertex cover of the pair-type combinations that differ, found at creation)
+ * are the "perturbed" atoms.  The regular pruned-list pair kernel evaluates
+ * every pair with the perturbed atoms given a null LJ type and no charge; a
+ * warp per perturbed atom then walks the atom's cluster-table neighbours and
+ * adds its pairs with the formula above, in int64 fixed point. */
+typedef struct spgnb_lj_soft spgnb_lj_soft;
+
+/* LJ_SOFT_CORE::Initial's parameters (LJ_soft_core.cpp:464-531):
+ * lambda_lj, soft_core_alpha, soft_core_powfer, soft_core_sigma,
+ * soft_core_sigma_min. */
+typedef struct
+{
+    float lambda;     /* required */
+    float alpha;      /* default 0.5 */
+    float p;          /* default 1.0 */
+    float sigma;      /* default 3.0 */
+    float sigma_min;  /* default 0.0 */
+} spgnb_soft_core_params;
+
+void spgnb_lj_soft_default_params(spgnb_soft_core_params* prm);
+
+/* LJ_SOFT_CORE::Initial (LJ_soft_core.cpp:438-641) from host arrays: per-atom
+ * state-A / state-B types and the four triangular pair tables (index
+ * hi*(hi+1)/2 + lo).  Also the long-range factors of Total_C6_Get and
+ * Total_C6_B_A_Get (:83-181, :605-635), through a histogram of (type A, type
+ * B) combinations instead of the O(N^2) loop.  At most 127 state-A types. */
+int spgnb_lj_soft_create(int atom_numbers, int atom_type_numbers_A, int atom_type_numbers_B,
+                         const int* h_atom_LJ_type_A, const int* h_atom_LJ_type_B, const float* h_LJ_AA,
+                         const float* h_LJ_AB, const float* h_LJ_BA, const float* h_LJ_BB,
+                         const spgnb_soft_core_params* prm, float cutoff, spgnb_lj_soft** out);
+
+/* LJ_SOFT_CORE::Get_Local (LJ_soft_core.cpp:905-919).  Reads d_atom_local
+ * back once (synchronises) to list the perturbed local atoms. */
+int spgnb_lj_soft_get_local(spgnb_lj_soft* lj, const int* d_atom_local, int local_atom_numbers, int ghost_numbers);
+
+/* LJ_SOFT_CORE::LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial
+ * (LJ_soft_core.cpp:721-784) over the spgnb list, every pair of the system
+ * (water included; no solvent-module call follows).  Same outputs and owner
+ * rule as spgnb_lj_pme_direct_force; the module's per-atom LJ energy array
+ * (spgnb_lj_soft_atom_lj_energy) is d_LJ_energy_atom. */
+int spgnb_lj_soft_pme_direct_force(spgnb_lj_soft* lj, int atom_numbers, int local_atom_numbers,
+                                   int solvent_numbers, int ghost_numbers, const spgnb_vector* d_crd,
+                                   const float* d_charge, spgnb_vector* d_frc, spgnb_ltmatrix3 cell,
+                                   spgnb_ltmatrix3 rcell, const spgnb_nl* nl, float pme_beta, int need_atom_energy,
+                                   float* d_atom_energy, int need_virial, spgnb_ltmatrix3* d_atom_virial,
+                                   float* d_atom_direct_pme_energy);
+
+/* LJ_SOFT_CORE::Get_Partial_H_Partial_Lambda_With_Columb_Direct
+ * (LJ_soft_core.cpp:786-846): dH/dlambda of the LJ part plus the long-range
+ * term long_range_factor_TI / (a11 a22 a33) to *dh_dlambda, and, when
+ * charge_perturbated, the direct-space Coulomb part to *dh_dlambda_direct
+ * (d_charge_B_A = q_B - q_A per local atom; NULL when not perturbed).  Sums
+ * are int64 fixed point.  Synchronises. */
+int spgnb_lj_soft_partial_h_partial_lambda(spgnb_lj_soft* lj, int solvent_numbers, const spgnb_vector* d_crd,
+                                           spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, const float* d_charge,
+                                           const spgnb_nl* nl, const float* d_charge_B_A, float pme_beta,
+                                           int charge_perturbated, double* dh_dlambda, double* dh_dlambda_direct);
+
+/* LJ_SOFT_CORE::Long_Range_Correction (LJ_soft_core.cpp:872-889). */
+int spgnb_lj_soft_long_range_correction(spgnb_lj_soft* lj, int need_pressure, spgnb_ltmatrix3* d_virial,
+                                        int need_potential, float* d_potential, float volume);
+
+/* Step_Print (LJ_soft_core.cpp:848-862): LJ_soft_short, LJ_soft_long,
+ * LJ_soft, plus the direct-space Coulomb energy.  Synchronises. */
+int spgnb_lj_soft_energies(spgnb_lj_soft* lj, double* lj_short, double* lj_long, double* lj_total,
+                           double* direct_coulomb);
+
+/* FP64 totals of the last force call, as spgnb_lj_totals. */
+int spgnb_lj_soft_totals(spgnb_lj_soft* lj, double out[8]);
+
+/* The long-range factors (long_range_factor, long_range_factor_TI). */
+int spgnb_lj_soft_long_range_factors(const spgnb_lj_soft* lj, double* factor, double* factor_ti);
+
+/* The module's per-atom LJ energy array (d_LJ_energy_atom). */
+int spgnb_lj_soft_atom_lj_energy(spgnb_lj_soft* lj, float** d_atom_lj_energy);
+
+/* The perturbed atoms (global indices, ascending): *count always, the
+ * indices when capacity suffices. */
+int spgnb_lj_soft_perturbed_atoms(const spgnb_lj_soft* lj, int* count, int* h_atoms, int capacity);
+
+int spgnb_lj_soft_destroy(spgnb_lj_soft* lj);
 
 /* --------------------------------------------------- SOLVENT_LENNARD_JONES */
 typedef struct spgnb_solvent spgnb_solvent;

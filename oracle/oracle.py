@@ -57,6 +57,13 @@ class Oracle:
                                             C.c_void_p, _f64p]
         lib.orc_long_range_factor.restype = C.c_double
         lib.orc_long_range_factor.argtypes = [C.c_int, _i32p, C.c_int, _f32p, C.c_float]
+        lib.orc_soft_core_fp64.restype = C.c_longlong
+        lib.orc_soft_core_fp64.argtypes = [C.c_int, _f32p, _f32p, C.c_void_p, _i32p, _i32p, _f32p, _f32p, _f32p,
+                                           _f32p, _f32p, _f32p, C.c_float, C.c_float, _i32p, _i32p, _i32p, _f64p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p, _f64p]
+        lib.orc_soft_long_range.restype = None
+        lib.orc_soft_long_range.argtypes = [C.c_int, _i32p, _i32p, _f32p, _f32p, C.c_float, C.c_float,
+                                            C.POINTER(C.c_double), C.POINTER(C.c_double)]
         lib.orc_pair_dr2.restype = C.c_float
         lib.orc_pair_dr2.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int]
         self.lib = lib
@@ -157,6 +164,38 @@ class Oracle:
         return float(self.lib.orc_long_range_factor(s.n, _ci32(s.atom_type), s.n_types, _c32(s.pair_B),
                                                     s.cutoff))
 
+    def soft_core(self, f, lam=None, crd=None, charge_ba=True, per_atom=True):
+        """FP64 two-state soft-core pair sum of an FepSystem (orc_soft_core_fp64):
+        forces, owner energies and virial as direct_sum, plus dh_lj and dh_c
+        (dH/dlambda of LJ and of the direct-space Coulomb term, pair part)."""
+        s = f.base
+        crd = _c32(s.crd if crd is None else crd)
+        n = s.n
+        q = _c32(f.charge(lam))
+        qba = _c32(f.charge_ba()) if charge_ba else None
+        frc = np.zeros(3 * n, np.float64)
+        elj = np.zeros(n, np.float64) if per_atom else None
+        ec = np.zeros(n, np.float64) if per_atom else None
+        vir = np.zeros(6 * n, np.float64) if per_atom else None
+        tot = np.zeros(10, np.float64)
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        npairs = self.lib.orc_soft_core_fp64(n, crd, q, ptr(qba), _ci32(f.type_a), _ci32(f.type_b), _c32(f.AA),
+                                             _c32(f.AB), _c32(f.BA), _c32(f.BB), _c32(f.params(lam)), _c32(s.cell),
+                                             s.cutoff, s.beta, _ci32(s.excl_start), _ci32(s.excl_numbers),
+                                             _ci32(s.excl_list if len(s.excl_list) else np.zeros(1, np.int32)),
+                                             frc, ptr(elj), ptr(ec), ptr(vir), tot)
+        out = _result(frc, elj, ec, vir, tot[:8], npairs)
+        out["dh_lj"] = float(tot[8])
+        out["dh_c"] = float(tot[9])
+        return out
+
+    def soft_long_range(self, f, lam=None):
+        """(factor, factor_TI) of LJ_SOFT_CORE's long-range correction."""
+        a, b = C.c_double(), C.c_double()
+        self.lib.orc_soft_long_range(f.base.n, _ci32(f.type_a), _ci32(f.type_b), _c32(f.AB), _c32(f.BB),
+                                     float(f.lam if lam is None else lam), f.base.cutoff, C.byref(a), C.byref(b))
+        return a.value, b.value
+
 
 def _result(frc, elj, ec, vir, tot, npairs):
     return {
@@ -191,6 +230,17 @@ class Reference:
         lib.ref_long_range_factor.restype = C.c_double
         lib.ref_enable_solvent.argtypes = [C.c_int, _i32p, C.c_int, C.c_int, C.c_int]
         lib.ref_set_threads.argtypes = [C.c_int]
+        if hasattr(lib, "ref_soft_init"):
+            lib.ref_soft_init.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p,
+                                          _f32p, C.c_float]
+            lib.ref_soft_force.argtypes = [_f32p, _f32p, C.c_float, C.c_int, C.c_int, _f32p, C.c_void_p,
+                                           C.c_void_p, C.c_void_p, C.c_void_p]
+            lib.ref_soft_dhdl.restype = C.c_double
+            lib.ref_soft_dhdl.argtypes = [_f32p, _f32p, C.c_void_p, C.c_float, C.c_int, C.POINTER(C.c_double)]
+            lib.ref_soft_long_range.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_double)]
+            lib.ref_soft_long_range.restype = None
+            lib.ref_soft_time_steps.restype = C.c_double
+            lib.ref_soft_time_steps.argtypes = [_f32p, _f32p, C.c_float, C.c_int, C.c_int, C.c_int, C.c_int]
         self.lib = lib
         self.gpu = bool(lib.ref_is_gpu())
         self.shim = shim
@@ -255,6 +305,49 @@ class Reference:
 
     def long_range_factor(self):
         return float(self.lib.ref_long_range_factor())
+
+    def soft_init(self, f, lam=None):
+        """LJ_SOFT_CORE::Initial + Get_Local for an FepSystem (after init())."""
+        self.fep = f
+        self.fep_lam = f.lam if lam is None else lam
+        rc = self.lib.ref_soft_init(f.base.n, f.n_types_a, f.n_types_b, _ci32(f.type_a), _ci32(f.type_b),
+                                    _c32(f.AA), _c32(f.AB), _c32(f.BA), _c32(f.BB), _c32(f.params(lam)),
+                                    f.base.cutoff)
+        if rc != 0:
+            raise RuntimeError("LJ_SOFT_CORE did not initialise")
+
+    def soft_force(self, crd=None, need_energy=True, need_virial=True):
+        s, f = self.s, self.fep
+        n = s.n
+        frc = np.zeros(3 * n, np.float32)
+        e = np.zeros(n, np.float32)
+        v = np.zeros(6 * n, np.float32)
+        d = np.zeros(n, np.float32)
+        lj = np.zeros(n, np.float32)
+        p = lambda a: a.ctypes.data_as(C.c_void_p)
+        self.lib.ref_soft_force(_c32(s.crd if crd is None else crd), _c32(f.charge(self.fep_lam)), s.beta,
+                                int(need_energy), int(need_virial), frc, p(e), p(v), p(d), p(lj))
+        return {"frc": frc.reshape(-1, 3), "atom_energy": e, "atom_virial": v.reshape(-1, 6),
+                "atom_direct": d, "atom_lj": lj}
+
+    def soft_dhdl(self, crd=None, charge_perturbated=True):
+        """(dH/dlambda LJ incl. the long-range term, direct-space Coulomb part)."""
+        s, f = self.s, self.fep
+        qba = _c32(f.charge_ba())
+        direct = C.c_double()
+        v = self.lib.ref_soft_dhdl(_c32(s.crd if crd is None else crd), _c32(f.charge(self.fep_lam)),
+                                   qba.ctypes.data_as(C.c_void_p), s.beta, int(charge_perturbated), C.byref(direct))
+        return float(v), float(direct.value)
+
+    def soft_long_range(self):
+        a, b = C.c_double(), C.c_double()
+        self.lib.ref_soft_long_range(C.byref(a), C.byref(b))
+        return a.value, b.value
+
+    def soft_time_steps(self, steps, first_step=0, need_energy=False, need_virial=False, crd=None):
+        s, f = self.s, self.fep
+        return float(self.lib.ref_soft_time_steps(_c32(s.crd if crd is None else crd), _c32(f.charge(self.fep_lam)),
+                                                  s.beta, first_step, steps, int(need_energy), int(need_virial)))
 
     def clear(self):
         self.lib.ref_clear()

@@ -1,7 +1,8 @@
 // Reference harness -- TEST INFRASTRUCTURE ONLY.
 //
 // Plain C entry points over the reference's own module classes
-// (NEIGHBOR_LIST, LENNARD_JONES_INFORMATION, SOLVENT_LENNARD_JONES), compiled
+// (NEIGHBOR_LIST, LENNARD_JONES_INFORMATION, SOLVENT_LENNARD_JONES,
+// LJ_SOFT_CORE), compiled
 // from the reference sources where they lie (oracle/Makefile).  The CPU build
 // generates golden fixtures and is the timed CPU baseline; the CUDA build runs
 // the reference's own kernels on a B200 for the reference-kernel parity check
@@ -15,6 +16,7 @@
 
 #include <chrono>
 
+#include "Lennard_Jones_force/LJ_soft_core.h"
 #include "Lennard_Jones_force/Lennard_Jones_force.h"
 #include "Lennard_Jones_force/solvent_LJ.h"
 #include "common.h"
@@ -74,6 +76,7 @@ struct State
     float* d_direct = nullptr;
     int *d_excl_start = nullptr, *d_excl_list = nullptr, *d_excl_num = nullptr;
     int* d_res_start = nullptr;
+    float* d_charge_ba = nullptr;
     int res_numbers = 0;
     int solvent_atoms = 0;
 } S;
@@ -334,6 +337,164 @@ double ref_time_rebuild(const float* crd, int reps)
     return std::chrono::duration<double>(t1 - t0).count() / (reps > 0 ? reps : 1);
 }
 
+#ifndef REF_HARNESS_SHIM
+// LJ_SOFT_CORE::Initial (LJ_soft_core.cpp:438-641) from arrays given the way
+// Xponge hands them over (Xponge::LJSoftCore, xponge/ir/forcefield.h:82-94),
+// the control keys set from prm = {lambda_lj, soft_core_alpha,
+// soft_core_powfer, soft_core_sigma, soft_core_sigma_min}, then Get_Local
+// with the identity map.  ref_init must have run first (it owns the list).
+int ref_soft_init(int n, int nA, int nB, const int* type_a, const int* type_b, const float* AA, const float* AB,
+                  const float* BA, const float* BB, const float* prm, float cutoff)
+{
+    Quiet q;
+    auto& ls = Xponge::system.classical_force_field.lj_soft_core;
+    ls.atom_numbers = n;
+    ls.atom_type_numbers_A = nA;
+    ls.atom_type_numbers_B = nB;
+    const int pa = nA * (nA + 1) / 2, pb = nB * (nB + 1) / 2;
+    ls.LJ_AA.assign(AA, AA + pa);
+    ls.LJ_AB.assign(AB, AB + pa);
+    ls.LJ_BA.assign(BA, BA + pb);
+    ls.LJ_BB.assign(BB, BB + pb);
+    ls.atom_LJ_type_A.assign(type_a, type_a + n);
+    ls.atom_LJ_type_B.assign(type_b, type_b + n);
+    ls.subsystem_division.clear();
+    const char* keys[5] = {"lambda_lj", "soft_core_alpha", "soft_core_powfer", "soft_core_sigma",
+                           "soft_core_sigma_min"};
+    for (int k = 0; k < 5; k++)
+    {
+        char buf[64];
+        snprintf(buf, sizeof buf, "%.9g", prm[k]);
+        controller.commands[keys[k]] = buf;
+    }
+    delete S.lj_soft;
+    S.lj_soft = new LJ_SOFT_CORE();
+    if (S.slj) S.slj->lj_soft_info = S.lj_soft;
+    S.lj_soft->Initial(&controller, cutoff, NULL);
+    if (!S.lj_soft->is_initialized) return -1;
+    S.lj_soft->Get_Local(S.d_atom_local, n, 0);
+#ifdef USE_GPU
+    if (S.slj)
+    {
+        // An alchemical run has no plain LJ module (the system carries
+        // LJ_soft_core only), so the solvent module takes its soft-core
+        // branch (solvent_LJ.cpp:310-349), which reads the soft_to_hard_crd
+        // buffer SOLVENT_LENNARD_JONES::Initial allocates when LJ_SOFT_CORE
+        // is on (:220-225).
+        S.lj->is_initialized = 0;
+        S.slj->soft_to_hard_crd = dev_alloc<VECTOR_LJ>(n);
+    }
+#endif
+    if (S.d_charge_ba) Free_Single_Device_Pointer((void**)&S.d_charge_ba);
+    S.d_charge_ba = dev_alloc<float>(n);
+    sync_device();
+    return 0;
+}
+
+void ref_soft_long_range(double* factor, double* factor_ti)
+{
+    *factor = S.lj_soft ? (double)S.lj_soft->long_range_factor : 0.0;
+    *factor_ti = S.lj_soft ? (double)S.lj_soft->long_range_factor_TI : 0.0;
+}
+
+// The soft-core force the way Main_Calculate_Force runs it in an alchemical
+// run (main.cpp:379-392): LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial
+// for the atoms before the water tail, then the solvent module for the waters
+// when it is enabled (without it every atom owns its half list).  Outputs
+// zeroed first as ref_force does.
+static void soft_step(float beta, int need_energy, int need_virial)
+{
+    const int solvent = S.slj ? S.slj->local_solvent_numbers : 0;
+    S.lj_soft->LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial(
+        S.n, S.n, solvent, 0, S.d_crd, S.d_charge, S.d_frc, S.cell, S.rcell, S.nl->d_nl, beta, need_energy,
+        S.d_energy, need_virial, S.d_virial, S.d_direct);
+    if (S.slj)
+        S.slj->LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(S.n, S.res_numbers, S.d_res_start, S.d_crd,
+                                                                S.d_charge, S.d_frc, S.cell, S.rcell, S.nl->d_nl,
+                                                                beta, need_energy, S.d_energy, need_virial,
+                                                                S.d_virial, S.d_direct);
+}
+
+int ref_soft_force(const float* crd, const float* charge, float beta, int need_energy, int need_virial, float* frc,
+                   float* atom_energy, float* atom_virial, float* atom_direct, float* atom_lj)
+{
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    to_dev(S.d_charge, charge, S.n);
+    deviceMemset(S.d_frc, 0, sizeof(VECTOR) * S.n);
+    deviceMemset(S.d_energy, 0, sizeof(float) * S.n);
+    deviceMemset(S.d_virial, 0, sizeof(LTMatrix3) * S.n);
+    deviceMemset(S.d_direct, 0, sizeof(float) * S.n);
+    soft_step(beta, need_energy, need_virial);
+    sync_device();
+    to_host((VECTOR*)frc, S.d_frc, S.n);
+    if (atom_energy) to_host(atom_energy, S.d_energy, S.n);
+    if (atom_virial) to_host((LTMatrix3*)atom_virial, S.d_virial, S.n);
+    if (atom_direct) to_host(atom_direct, S.d_direct, S.n);
+    if (atom_lj) to_host(atom_lj, S.lj_soft->d_LJ_energy_atom, S.n);
+    return 0;
+}
+
+// Get_Partial_H_Partial_Lambda_With_Columb_Direct (LJ_soft_core.cpp:786-846).
+// Its kernel reads coordinates, charges and charge_BA from
+// crd_with_LJ_parameters_local, but the method copies them into
+// crd_with_parameters (:790-797): the local buffer keeps the coordinates and
+// charges of the last force call and a charge_BA field nothing writes.  The
+// harness writes the given crd, charge and charge_BA into the local buffer
+// first, so the reference evaluates its formula at this state.  Returns the
+// method's value (LJ part + long-range term); *direct = the direct-space
+// Coulomb part it leaves in h_sigma_of_dH_dlambda_direct.
+double ref_soft_dhdl(const float* crd, const float* charge, const float* charge_ba, float beta,
+                     int charge_perturbated, double* direct)
+{
+    std::vector<VECTOR_LJ_SOFT_TYPE> h(S.n);
+    to_host(h.data(), S.lj_soft->crd_with_LJ_parameters_local, S.n);
+    for (int i = 0; i < S.n; i++)
+    {
+        h[i].crd = ((const VECTOR*)crd)[i];
+        h[i].charge = charge[i];
+        h[i].charge_BA = charge_ba ? charge_ba[i] : 0.0f;
+    }
+    to_dev(S.lj_soft->crd_with_LJ_parameters_local, h.data(), S.n);
+    std::vector<float> cba(S.n, 0.0f);
+    if (charge_ba) cba.assign(charge_ba, charge_ba + S.n);
+    to_dev(S.d_charge_ba, cba.data(), S.n);
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    to_dev(S.d_charge, charge, S.n);
+    float r;
+    {
+        Quiet q;
+        r = S.lj_soft->Get_Partial_H_Partial_Lambda_With_Columb_Direct(0, S.d_crd, S.cell, S.rcell, S.d_charge,
+                                                                       S.nl->d_nl, S.d_charge_ba, beta,
+                                                                       charge_perturbated);
+    }
+    if (direct) *direct = charge_perturbated ? (double)*S.lj_soft->h_sigma_of_dH_dlambda_direct : 0.0;
+    return (double)r;
+}
+
+// Timed loop of the soft-core path: per step a conditional list update and
+// soft_step.
+double ref_soft_time_steps(const float* crd, const float* charge, float beta, int first_step, int steps,
+                           int need_energy, int need_virial)
+{
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    to_dev(S.d_charge, charge, S.n);
+    sync_device();
+    auto t0 = std::chrono::steady_clock::now();
+    {
+        Quiet q;
+        for (int s = first_step; s < first_step + steps; s++)
+        {
+            S.nl->Update(S.d_atom_local, S.n, 0, S.d_crd, S.cell, S.rcell, s, NEIGHBOR_LIST::CONDITIONAL_UPDATE,
+                         S.d_excl_start, S.d_excl_list, S.d_excl_num);
+            soft_step(beta, need_energy, need_virial);
+        }
+        sync_device();
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+#endif
+
 void ref_clear()
 {
     Quiet q;
@@ -349,6 +510,8 @@ void ref_clear()
     S.slj = nullptr;
     delete S.lj_soft;
     S.lj_soft = nullptr;
+    if (S.d_charge_ba) Free_Single_Device_Pointer((void**)&S.d_charge_ba);
+    S.d_charge_ba = nullptr;
 }
 
 }  // extern "C"

@@ -27,6 +27,10 @@
  *   orc_direct_sum_fp64 the same pair function over every pair within rc
  *                       (no neighbour list): the FP64 direct pair sum
  *   orc_long_range      Lennard_Jones_force.cpp:146-184,267-268,312-341
+ *   orc_soft_core_fp64  SPONGE/Lennard_Jones_force/LJ_soft_core.cpp:198-414 and
+ *                       LJ_soft_core.h:33-150 (the two-state pair, soft cores,
+ *                       dH/dlambda), evaluated in double over every pair within rc
+ *   orc_soft_long_range LJ_soft_core.cpp:83-181, :605-635
  */
 #include <math.h>
 #include <stdint.h>
@@ -414,23 +418,16 @@ long long orc_pair_force_fp64(int n, const float* crd, const float* charge, cons
     return t.pairs_in_cutoff;
 }
 
-/* FP64 direct pair sum: every pair with double minimum-image distance < rc,
- * exclusions removed, found by a cell sweep independent of the neighbour
- * list.  Same outputs as orc_pair_force_fp64. */
-long long orc_direct_sum_fp64(int n, const float* crd, const float* charge, const int* type, const float* A,
-                              const float* B, const float* cell, float cutoff, float beta, const int* excl_start,
-                              const int* excl_numbers, const int* excl_list, double* frc, double* e_atom_lj,
-                              double* e_atom_c, double* vir_atom, double* totals)
+/* Calls fn(i, j, ctx) for every pair i < j whose atoms sit in neighbouring
+ * coarse cells (cells of at least rc in every fractional direction; every
+ * cell when a dimension has fewer than 3), exclusions removed.  The caller
+ * applies the distance test. */
+typedef void (*orc_pair_fn)(int i, int j, void* ctx);
+
+static void sweep_pairs(int n, const float* crd, const double* c, const double* ri, float cutoff,
+                        const int* excl_start, const int* excl_numbers, const int* excl_list, orc_pair_fn fn,
+                        void* ctx)
 {
-    double c[6], ri[6];
-    cell_inverse_fp64(cell, c, ri);
-    memset(frc, 0, sizeof(double) * 3 * (size_t)n);
-    if (e_atom_lj) memset(e_atom_lj, 0, sizeof(double) * (size_t)n);
-    if (e_atom_c) memset(e_atom_c, 0, sizeof(double) * (size_t)n);
-    if (vir_atom) memset(vir_atom, 0, sizeof(double) * 6 * (size_t)n);
-    orc_totals t;
-    memset(&t, 0, sizeof(t));
-    /* coarse cells of at least rc in every fractional direction */
     double h[3] = {c[0], c[2], c[5]};
     int m[3];
     for (int d = 0; d < 3; d++)
@@ -463,7 +460,6 @@ long long orc_direct_sum_fp64(int n, const float* crd, const float* charge, cons
         for (int i = 0; i < n; i++) catoms[fill[cell_of[i]]++] = i;
         free(fill);
     }
-    /* neighbour cells: +-1 (or every cell when a dimension has < 3) */
     for (int i = 0; i < n; i++)
     {
         int g = cell_of[i];
@@ -482,18 +478,242 @@ long long orc_direct_sum_fp64(int n, const float* crd, const float* charge, cons
                         int j = catoms[b];
                         if (j <= i) continue;
                         if (excluded_upper(i, j, excl_start, excl_numbers, excl_list)) continue;
-                        pair_fp64(i, j, crd, charge, type, A, B, c, ri, cutoff, beta, frc, e_atom_lj, e_atom_c,
-                                  vir_atom, &t);
+                        fn(i, j, ctx);
                     }
                 }
     }
     free(cell_of);
     free(cstart);
     free(catoms);
-    totals[0] = t.e_lj;
-    totals[1] = t.e_coul;
-    for (int k = 0; k < 6; k++) totals[2 + k] = t.vir[k];
-    return t.pairs_in_cutoff;
+}
+
+typedef struct
+{
+    const float *crd, *charge, *A, *B;
+    const int* type;
+    const double *c, *ri;
+    double rc, beta;
+    double *frc, *e_atom_lj, *e_atom_c, *vir_atom;
+    orc_totals t;
+} plain_ctx;
+
+static void plain_pair(int i, int j, void* ctx)
+{
+    plain_ctx* p = (plain_ctx*)ctx;
+    pair_fp64(i, j, p->crd, p->charge, p->type, p->A, p->B, p->c, p->ri, p->rc, p->beta, p->frc, p->e_atom_lj,
+              p->e_atom_c, p->vir_atom, &p->t);
+}
+
+/* FP64 direct pair sum: every pair with double minimum-image distance < rc,
+ * exclusions removed, found by a cell sweep independent of the neighbour
+ * list.  Same outputs as orc_pair_force_fp64. */
+long long orc_direct_sum_fp64(int n, const float* crd, const float* charge, const int* type, const float* A,
+                              const float* B, const float* cell, float cutoff, float beta, const int* excl_start,
+                              const int* excl_numbers, const int* excl_list, double* frc, double* e_atom_lj,
+                              double* e_atom_c, double* vir_atom, double* totals)
+{
+    double c[6], ri[6];
+    cell_inverse_fp64(cell, c, ri);
+    memset(frc, 0, sizeof(double) * 3 * (size_t)n);
+    if (e_atom_lj) memset(e_atom_lj, 0, sizeof(double) * (size_t)n);
+    if (e_atom_c) memset(e_atom_c, 0, sizeof(double) * (size_t)n);
+    if (vir_atom) memset(vir_atom, 0, sizeof(double) * 6 * (size_t)n);
+    plain_ctx p = {crd, charge, A, B, type, c, ri, cutoff, beta, frc, e_atom_lj, e_atom_c, vir_atom, {0}};
+    sweep_pairs(n, crd, c, ri, cutoff, excl_start, excl_numbers, excl_list, plain_pair, &p);
+    totals[0] = p.t.e_lj;
+    totals[1] = p.t.e_coul;
+    for (int k = 0; k < 6; k++) totals[2 + k] = p.t.vir[k];
+    return p.t.pairs_in_cutoff;
+}
+
+/* ------------------------------------------------- FP64 soft-core pair sum */
+/* LJ_SOFT_CORE's pair (SPONGE/Lennard_Jones_force/LJ_soft_core.cpp:198-414,
+ * pair functions LJ_soft_core.h:33-150) in double.  Owner i < j,
+ * dr = r_j - r_i (minimum image in double), r < rc.  With l = lambda,
+ * l' = 1 - l, the state tables AA/AB (state A) and BA/BB (state B):
+ *   linear branch (BA*AA != 0 or BA + AA == 0):
+ *     F/r = l' LJF(r; AA, AB) + l LJF(r; BA, BB) - CF(r),
+ *     E_lj = l' LJE(r; AA, AB) + l LJE(r; BA, BB), E_c = q_i q_j erfc(beta r)/r,
+ *     dH_lj = LJE(r; BA, BB) - LJE(r; AA, AB), dH_c = erfc(beta r) dq / r;
+ *   soft-core branch: sigma_X = sigma^6 if the state's A or B is 0, else
+ *     max(A/(2B), sigma_min^6); r_A^6 = r^6 + alpha l^p sigma_A,
+ *     r_B^6 = r^6 + alpha l'^p sigma_B;
+ *     F/r = l' r^4 (AB - AA r_A^-6) r_A^-12 + l r^4 (BB - BA r_B^-6) r_B^-12
+ *           - [l' SCF(r_A) + l SCF(r_B)] r^4,  SCF(s) = q_i q_j (2/sqrt(pi) beta
+ *           e^-(beta s)^2 + erfc(beta s)/s) s^-6,
+ *     E_lj = l' LJE(r_A) + l LJE(r_B), E_c = l' CE(r_A) + l CE(r_B),
+ *     dH_lj = LJE(r_B) - LJE(r_A) + D_A LJF(r_A) r_A^-4 sigma_A
+ *             - D_B LJF(r_B) r_B^-4 sigma_B,
+ *     dH_c = CE(r_B) - CE(r_A) + D_B CF(r_B) r_B^-4 sigma_B
+ *            - D_A CF(r_A) r_A^-4 sigma_A + l dq erfc(beta r_B)/r_B
+ *            + l' dq erfc(beta r_A)/r_A,
+ *   with LJF(s; A, B) = (B - A s^-6) s^-8, LJE(s; A, B) = (A/12 s^-6 - B/6) s^-6,
+ *   CF(s) = q_i q_j s^-3 (2/sqrt(pi) beta s e^-(beta s)^2 + erfc(beta s)),
+ *   CE(s) = q_i q_j erfc(beta s)/s, dq = q_i^BA q_j + q_i q_j^BA,
+ *   D_A = p alpha l' (l + FLT_MIN)^(p-1) / 6, D_B = p alpha l (l' + FLT_MIN)^(p-1) / 6.
+ * Forces, owner energies and virial as pair_fp64; dh[0] += dH_lj, dh[1] += dH_c. */
+typedef struct
+{
+    const float *crd, *charge, *charge_ba, *AA, *AB, *BA, *BB;
+    const int *ta, *tb;
+    const double *c, *ri;
+    double rc, beta, l, l_, alp_a, alp_b, d_a, d_b, s6, s6min;
+    double *frc, *e_atom_lj, *e_atom_c, *vir_atom, dh[2];
+    orc_totals t;
+} soft_ctx;
+
+static double lje(double s, double a, double b)
+{
+    double s6 = pow(s, -6.0);
+    return (a / 12.0 * s6 - b / 6.0) * s6;
+}
+
+static double ljf(double s, double a, double b) { return (b - a * pow(s, -6.0)) * pow(s, -8.0); }
+
+static void soft_pair(int i, int j, void* ctx)
+{
+    soft_ctx* p = (soft_ctx*)ctx;
+    const double* cell = p->c;
+    const double* ri = p->ri;
+    double dx = (double)p->crd[3 * j] - p->crd[3 * i];
+    double dy = (double)p->crd[3 * j + 1] - p->crd[3 * i + 1];
+    double dz = (double)p->crd[3 * j + 2] - p->crd[3 * i + 2];
+    double sx = floor(dx * ri[0] + dy * ri[1] + dz * ri[3] + 0.5);
+    double sy = floor(dy * ri[2] + dz * ri[4] + 0.5);
+    double sz = floor(dz * ri[5] + 0.5);
+    dx -= sx * cell[0] + sy * cell[1] + sz * cell[3];
+    dy -= sy * cell[2] + sz * cell[4];
+    dz -= sz * cell[5];
+    double r2 = dx * dx + dy * dy + dz * dz;
+    double r = sqrt(r2);
+    if (!(r < p->rc)) return;
+    int pa = lj_index(p->ta[i], p->ta[j]), pb = lj_index(p->tb[i], p->tb[j]);
+    double AA = p->AA[pa], AB = p->AB[pa], BA = p->BA[pb], BB = p->BB[pb];
+    double qq = (double)p->charge[i] * p->charge[j];
+    double dq = p->charge_ba ? (double)p->charge_ba[i] * p->charge[j] + (double)p->charge[i] * p->charge_ba[j] : 0.0;
+    double beta = p->beta, l = p->l, l_ = p->l_;
+    double f, elj, ec, dlj, dc;
+    if ((float)BA * (float)AA != 0.0f || BA + AA == 0.0)
+    {
+        double br = beta * r, erfc_r = erfc(br);
+        double cf = qq / (r2 * r) * (br * 1.1283791670955126 * exp(-br * br) + erfc_r);
+        f = l_ * ljf(r, AA, AB) + l * ljf(r, BA, BB) - cf;
+        elj = l_ * lje(r, AA, AB) + l * lje(r, BA, BB);
+        ec = qq * erfc_r / r;
+        dlj = lje(r, BA, BB) - lje(r, AA, AB);
+        dc = erfc_r * dq / r;
+    }
+    else
+    {
+        double sa = (AA == 0.0 || AB == 0.0) ? p->s6 : fmax(0.5 * AA / AB, p->s6min);
+        double sb = (BA == 0.0 || BB == 0.0) ? p->s6 : fmax(0.5 * BA / BB, p->s6min);
+        double r6 = r2 * r2 * r2, r4 = r2 * r2;
+        double ra = pow(r6 + p->alp_a * sa, 1.0 / 6.0), rb = pow(r6 + p->alp_b * sb, 1.0 / 6.0);
+        double bra = beta * ra, brb = beta * rb;
+        double erfc_a = erfc(bra), erfc_b = erfc(brb), exp_a = exp(-bra * bra), exp_b = exp(-brb * brb);
+        double scf_a = qq * (exp_a * 1.1283791670955126 * beta + erfc_a / ra) * pow(ra, -6.0);
+        double scf_b = qq * (exp_b * 1.1283791670955126 * beta + erfc_b / rb) * pow(rb, -6.0);
+        f = l_ * r4 * (AB - AA * pow(ra, -6.0)) * pow(ra, -12.0) + l * r4 * (BB - BA * pow(rb, -6.0)) * pow(rb, -12.0) -
+            (l_ * scf_a + l * scf_b) * r4;
+        double cea = qq * erfc_a / ra, ceb = qq * erfc_b / rb;
+        elj = l_ * lje(ra, AA, AB) + l * lje(rb, BA, BB);
+        ec = l_ * cea + l * ceb;
+        dlj = lje(rb, BA, BB) - lje(ra, AA, AB) + p->d_a * ljf(ra, AA, AB) * pow(ra, -4.0) * sa -
+              p->d_b * ljf(rb, BA, BB) * pow(rb, -4.0) * sb;
+        double cf_a = qq * pow(ra, -3.0) * (bra * 1.1283791670955126 * exp_a + erfc_a);
+        double cf_b = qq * pow(rb, -3.0) * (brb * 1.1283791670955126 * exp_b + erfc_b);
+        dc = ceb - cea + p->d_b * cf_b * pow(rb, -4.0) * sb - p->d_a * cf_a * pow(ra, -4.0) * sa +
+             l * dq * erfc_b / rb + l_ * dq * erfc_a / ra;
+    }
+    double fx = f * dx, fy = f * dy, fz = f * dz;
+    p->frc[3 * i] += fx;
+    p->frc[3 * i + 1] += fy;
+    p->frc[3 * i + 2] += fz;
+    p->frc[3 * j] -= fx;
+    p->frc[3 * j + 1] -= fy;
+    p->frc[3 * j + 2] -= fz;
+    double v[6] = {-fx * dx, -(fx * dy + fy * dx), -fy * dy, -(fx * dz + fz * dx), -(fy * dz + fz * dy), -fz * dz};
+    if (p->e_atom_lj) p->e_atom_lj[i] += elj;
+    if (p->e_atom_c) p->e_atom_c[i] += ec;
+    if (p->vir_atom)
+        for (int k = 0; k < 6; k++) p->vir_atom[6 * i + k] += v[k];
+    p->t.e_lj += elj;
+    p->t.e_coul += ec;
+    for (int k = 0; k < 6; k++) p->t.vir[k] += v[k];
+    p->t.pairs_in_cutoff++;
+    p->dh[0] += dlj;
+    p->dh[1] += dc;
+}
+
+/* prm = {lambda, alpha, p, sigma, sigma_min}; charge_ba may be NULL (no
+ * charge perturbation).  totals = {E_lj, E_c, virial[6], dH_lj, dH_c}.
+ * Returns the number of pairs inside rc. */
+long long orc_soft_core_fp64(int n, const float* crd, const float* charge, const float* charge_ba,
+                             const int* type_a, const int* type_b, const float* AA, const float* AB,
+                             const float* BA, const float* BB, const float* prm, const float* cell, float cutoff,
+                             float beta, const int* excl_start, const int* excl_numbers, const int* excl_list,
+                             double* frc, double* e_atom_lj, double* e_atom_c, double* vir_atom, double* totals)
+{
+    double c[6], ri[6];
+    cell_inverse_fp64(cell, c, ri);
+    memset(frc, 0, sizeof(double) * 3 * (size_t)n);
+    if (e_atom_lj) memset(e_atom_lj, 0, sizeof(double) * (size_t)n);
+    if (e_atom_c) memset(e_atom_c, 0, sizeof(double) * (size_t)n);
+    if (vir_atom) memset(vir_atom, 0, sizeof(double) * 6 * (size_t)n);
+    soft_ctx p;
+    memset(&p, 0, sizeof(p));
+    p.crd = crd;
+    p.charge = charge;
+    p.charge_ba = charge_ba;
+    p.AA = AA;
+    p.AB = AB;
+    p.BA = BA;
+    p.BB = BB;
+    p.ta = type_a;
+    p.tb = type_b;
+    p.c = c;
+    p.ri = ri;
+    p.rc = cutoff;
+    p.beta = beta;
+    double lam = prm[0], alpha = prm[1], pw = prm[2];
+    p.l = lam;
+    p.l_ = 1.0 - lam;
+    p.alp_a = alpha * pow(lam, pw);
+    p.alp_b = alpha * pow(1.0 - lam, pw);
+    p.d_a = pw * alpha * (1.0 - lam) * pow(lam + 1.1754943508222875e-38, pw - 1.0) / 6.0;
+    p.d_b = pw * alpha * lam * pow(1.0 - lam + 1.1754943508222875e-38, pw - 1.0) / 6.0;
+    p.s6 = pow(prm[3], 6.0);
+    p.s6min = pow(prm[4], 6.0);
+    p.frc = frc;
+    p.e_atom_lj = e_atom_lj;
+    p.e_atom_c = e_atom_c;
+    p.vir_atom = vir_atom;
+    sweep_pairs(n, crd, c, ri, cutoff, excl_start, excl_numbers, excl_list, soft_pair, &p);
+    totals[0] = p.t.e_lj;
+    totals[1] = p.t.e_coul;
+    for (int k = 0; k < 6; k++) totals[2 + k] = p.t.vir[k];
+    totals[8] = p.dh[0];
+    totals[9] = p.dh[1];
+    return p.t.pairs_in_cutoff;
+}
+
+/* LJ_SOFT_CORE's long-range factors (LJ_soft_core.cpp:83-181, :605-635):
+ * sum over ordered atom pairs (i == j included) of (1 - l) AB + l BB and of
+ * BB - AB, times -2/3 pi / rc^3 / 6. */
+void orc_soft_long_range(int n, const int* type_a, const int* type_b, const float* AB, const float* BB, float lambda,
+                         float cutoff, double* factor, double* factor_ti)
+{
+    double s = 0.0, st = 0.0;
+    for (int i = 0; i < n; i++)
+        for (int j = 0; j < n; j++)
+        {
+            double ab = AB[lj_index(type_a[i], type_a[j])], bb = BB[lj_index(type_b[i], type_b[j])];
+            s += (1.0 - lambda) * ab + lambda * bb;
+            st += bb - ab;
+        }
+    double k = -2.0 / 3.0 * 3.14159265358979323846 / cutoff / cutoff / cutoff / 6.0;
+    *factor = s * k;
+    *factor_ti = st * k;
 }
 
 /* Tail correction.  factor = -2/3 pi sum_{i,j} B(type_i,type_j) / rc^3 / 6,

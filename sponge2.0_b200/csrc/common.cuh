@@ -430,6 +430,9 @@ struct ForceInputs
 };
 int force_pipeline(const ForceInputs& in, cudaStream_t s);
 int force_kernels_init(int table_size);
+// Adds the module's int64 force accumulators of atoms [0, n) to frc and
+// clears them (the reference-layout and correction paths end with it).
+int lj_finalize_forces(spgnb_lj* lj, int n, float3* frc, cudaStream_t s);
 
 // Neighbour-list internals shared with the force and batch code.
 int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3* cells,

@@ -1313,6 +1313,14 @@ int force_kernels_init(int table_size)
     return SPGNB_OK;
 }
 
+int lj_finalize_forces(spgnb_lj* lj, int n, float3* frc, cudaStream_t s)
+{
+    if (n <= 0) return SPGNB_OK;
+    k_finalize<<<(n + 255) / 256, 256, 0, s>>>(n, lj->d_frc_acc, frc);
+    SPGNB_CHECK_LAUNCH("k_finalize");
+    return SPGNB_OK;
+}
+
 int force_pipeline(const ForceInputs& in, cudaStream_t s)
 {
     spgnb_nl* nl = in.nl;

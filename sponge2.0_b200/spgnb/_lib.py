@@ -28,6 +28,11 @@ EXPORTED = [
     "spgnb_solvent_create", "spgnb_solvent_get_local", "spgnb_solvent_pme_direct_force", "spgnb_solvent_destroy",
     "spgnb_launch_count", "spgnb_debug_set_pair_events", "spgnb_nl_count_pairs", "spgnb_probe_fp32_fma_tflops",
     "spgnb_lj_pme_direct_force_noalloc",
+    "spgnb_lj_soft_default_params", "spgnb_lj_soft_create", "spgnb_lj_soft_get_local",
+    "spgnb_lj_soft_pme_direct_force", "spgnb_lj_soft_partial_h_partial_lambda",
+    "spgnb_lj_soft_long_range_correction", "spgnb_lj_soft_energies", "spgnb_lj_soft_totals",
+    "spgnb_lj_soft_long_range_factors", "spgnb_lj_soft_atom_lj_energy", "spgnb_lj_soft_perturbed_atoms",
+    "spgnb_lj_soft_destroy",
     "spgnb_batch_default_options", "spgnb_batch_create", "spgnb_batch_run", "spgnb_batch_energies",
     "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_stream",
     "spgnb_batch_check_overflow", "spgnb_batch_set_thermostat",
@@ -80,6 +85,11 @@ class PoolOptions(C.Structure):
     _fields_ = [("max_systems", C.c_int), ("max_atoms", C.c_int), ("max_excluded", C.c_longlong),
                 ("max_waters", C.c_int), ("max_cutoff", C.c_float), ("min_cutoff", C.c_float), ("skin", C.c_float),
                 ("density", C.c_float), ("hbm_budget_bytes", C.c_double)]
+
+
+class SoftCoreParams(C.Structure):
+    _fields_ = [("lambda_", C.c_float), ("alpha", C.c_float), ("p", C.c_float), ("sigma", C.c_float),
+                ("sigma_min", C.c_float)]
 
 
 class NLStats(C.Structure):
@@ -164,6 +174,21 @@ def lib():
     L.spgnb_nl_count_pairs.argtypes = [vp, vp, M, M, f, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     L.spgnb_probe_fp32_fma_tflops.argtypes = [i, C.POINTER(d)]
     L.spgnb_lj_pme_direct_force_noalloc.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, M, M, vp, f, f]
+    SP = C.POINTER(SoftCoreParams)
+    L.spgnb_lj_soft_default_params.argtypes = [SP]
+    L.spgnb_lj_soft_default_params.restype = None
+    L.spgnb_lj_soft_create.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, SP, f, C.POINTER(vp)]
+    L.spgnb_lj_soft_get_local.argtypes = [vp, vp, i, i]
+    L.spgnb_lj_soft_pme_direct_force.argtypes = [vp, i, i, i, i, vp, vp, vp, M, M, vp, f, i, vp, i, vp, vp]
+    L.spgnb_lj_soft_partial_h_partial_lambda.argtypes = [vp, i, vp, M, M, vp, vp, vp, f, i, C.POINTER(d),
+                                                         C.POINTER(d)]
+    L.spgnb_lj_soft_long_range_correction.argtypes = [vp, i, vp, i, vp, f]
+    L.spgnb_lj_soft_energies.argtypes = [vp, C.POINTER(d), C.POINTER(d), C.POINTER(d), C.POINTER(d)]
+    L.spgnb_lj_soft_totals.argtypes = [vp, C.POINTER(d)]
+    L.spgnb_lj_soft_long_range_factors.argtypes = [vp, C.POINTER(d), C.POINTER(d)]
+    L.spgnb_lj_soft_atom_lj_energy.argtypes = [vp, C.POINTER(vp)]
+    L.spgnb_lj_soft_perturbed_atoms.argtypes = [vp, C.POINTER(i), vp, i]
+    L.spgnb_lj_soft_destroy.argtypes = [vp]
     _lib = L
     return L
 

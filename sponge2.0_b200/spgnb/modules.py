@@ -3,7 +3,8 @@
 Same class names, method names, argument order and meaning as the reference
 structs (``SPONGE/neighbor_list/neighbor_list.h:7-128``,
 ``SPONGE/Lennard_Jones_force/Lennard_Jones_force.h:86-173``,
-``SPONGE/Lennard_Jones_force/solvent_LJ.h:9-43``).  Device arrays are
+``SPONGE/Lennard_Jones_force/solvent_LJ.h:9-43``,
+``SPONGE/Lennard_Jones_force/LJ_soft_core.h:162-276``).  Device arrays are
 ``torch`` CUDA tensors (``crd``/``frc`` float32 (N,3), virials float32 (N,6));
 control keys come from a dict shaped like ``CONTROLLER::commands``
 (``"neighbor_list_refresh_interval"`` and so on, ``control.cpp:137-145``).
@@ -16,7 +17,7 @@ import ctypes as C
 import numpy as np
 import torch
 
-from ._lib import LTMatrix3, NLOptions, NLStats, SpgnbError, check, lib
+from ._lib import LTMatrix3, NLOptions, NLStats, SoftCoreParams, SpgnbError, check, lib
 
 
 def _ptr(t):
@@ -330,3 +331,132 @@ class SOLVENT_LENNARD_JONES:
             lib().spgnb_solvent_destroy(self.handle)
             self.handle = None
         self.is_initialized = False
+
+
+class LJ_SOFT_CORE:
+    """Alchemical LJ + PME direct space with soft cores (LJ_soft_core.h:162-276)
+    over the spgnb list: every pair of the system in one call, water included."""
+
+    def __init__(self):
+        self.handle = None
+        self.is_initialized = False
+        self.h_LJ_energy_sum = 0.0
+        self.h_LJ_long_energy = 0.0
+        self.h_sigma_of_dH_dlambda_direct = 0.0
+
+    def Initial(self, controller, cutoff, atom_type_A, atom_type_B, LJ_AA, LJ_AB, LJ_BA, LJ_BB,
+                atom_type_numbers_A, atom_type_numbers_B, module_name=None):
+        """LJ_SOFT_CORE::Initial (LJ_soft_core.cpp:438-641).  ``lambda_lj`` is
+        required; ``soft_core_alpha`` (0.5), ``soft_core_powfer`` (1.0),
+        ``soft_core_sigma`` (3.0), ``soft_core_sigma_min`` (0.0) as the
+        reference.  Tables in the internal convention (A*12, B*6, triangular)."""
+        self.module_name = module_name or "LJ_soft_core"
+        if (controller or {}).get("lambda_lj") is None:
+            raise SpgnbError(1, "'lambda_lj' is required for the calculation of LJ_soft_core")
+        prm = SoftCoreParams()
+        lib().spgnb_lj_soft_default_params(C.byref(prm))
+        prm.lambda_ = _controller_float(controller, "lambda_lj", 0.0)
+        prm.alpha = _controller_float(controller, "soft_core_alpha", prm.alpha)
+        prm.p = _controller_float(controller, "soft_core_powfer", prm.p)
+        prm.sigma = _controller_float(controller, "soft_core_sigma", prm.sigma)
+        prm.sigma_min = _controller_float(controller, "soft_core_sigma_min", prm.sigma_min)
+        self.lambda_, self.alpha, self.p = prm.lambda_, prm.alpha, prm.p
+        self.sigma, self.sigma_min = prm.sigma, prm.sigma_min
+        ta = np.ascontiguousarray(atom_type_A, np.int32)
+        tb = np.ascontiguousarray(atom_type_B, np.int32)
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (LJ_AA, LJ_AB, LJ_BA, LJ_BB)]
+        self.atom_numbers = len(ta)
+        self.cutoff = float(cutoff)
+        h = C.c_void_p()
+        ptr = lambda a: a.ctypes.data_as(C.c_void_p)
+        check(lib().spgnb_lj_soft_create(self.atom_numbers, int(atom_type_numbers_A), int(atom_type_numbers_B),
+                                         ptr(ta), ptr(tb), *[ptr(a) for a in arrs], C.byref(prm), self.cutoff,
+                                         C.byref(h)))
+        self.handle = h
+        f, fti = C.c_double(), C.c_double()
+        check(lib().spgnb_lj_soft_long_range_factors(h, C.byref(f), C.byref(fti)))
+        self.long_range_factor, self.long_range_factor_TI = f.value, fti.value
+        self.is_initialized = True
+
+    def Get_Local(self, atom_local, local_atom_numbers, ghost_numbers):
+        """LJ_SOFT_CORE::Get_Local (LJ_soft_core.cpp:905-919)."""
+        _bind_stream()
+        check(lib().spgnb_lj_soft_get_local(self.handle, _ptr(atom_local), int(local_atom_numbers),
+                                            int(ghost_numbers)))
+
+    def LJ_Soft_Core_PME_Direct_Force_With_Atom_Energy_And_Virial(self, atom_numbers, local_atom_numbers,
+                                                                   solvent_numbers, ghost_numbers, crd, charge, frc,
+                                                                   cell, rcell, nl, pme_beta, need_atom_energy,
+                                                                   atom_energy, need_virial, atom_lj_virial,
+                                                                   atom_direct_pme_energy):
+        """LJ_soft_core.cpp:721-784 over a NEIGHBOR_LIST."""
+        if not self.is_initialized:
+            return
+        if not isinstance(nl, NEIGHBOR_LIST):
+            raise SpgnbError(1, "the soft-core module evaluates over an spgnb NEIGHBOR_LIST")
+        _bind_stream()
+        check(lib().spgnb_lj_soft_pme_direct_force(self.handle, int(atom_numbers), int(local_atom_numbers),
+                                                   int(solvent_numbers), int(ghost_numbers), _ptr(crd),
+                                                   _ptr(charge), _ptr(frc), LTMatrix3.of(cell), LTMatrix3.of(rcell),
+                                                   nl.handle, float(pme_beta), int(need_atom_energy),
+                                                   _ptr(atom_energy), int(need_virial), _ptr(atom_lj_virial),
+                                                   _ptr(atom_direct_pme_energy)))
+
+    def Get_Partial_H_Partial_Lambda_With_Columb_Direct(self, solvent_numbers, crd, cell, rcell, charge, nl,
+                                                        charge_B_A, pme_beta, charge_perturbated):
+        """LJ_soft_core.cpp:786-846: dH/dlambda of LJ (+ the long-range term);
+        the direct-space Coulomb part is left in h_sigma_of_dH_dlambda_direct."""
+        if not self.is_initialized:
+            return float("nan")
+        _bind_stream()
+        v, vd = C.c_double(), C.c_double()
+        check(lib().spgnb_lj_soft_partial_h_partial_lambda(self.handle, int(solvent_numbers), _ptr(crd),
+                                                           LTMatrix3.of(cell), LTMatrix3.of(rcell), _ptr(charge),
+                                                           nl.handle, _ptr(charge_B_A), float(pme_beta),
+                                                           int(charge_perturbated), C.byref(v), C.byref(vd)))
+        self.h_sigma_of_dH_dlambda_direct = vd.value
+        return v.value
+
+    def Long_Range_Correction(self, need_pressure, d_virial, need_potential, d_potential, volume):
+        _bind_stream()
+        check(lib().spgnb_lj_soft_long_range_correction(self.handle, int(need_pressure), _ptr(d_virial),
+                                                        int(need_potential), _ptr(d_potential), float(volume)))
+
+    def totals(self):
+        """FP64 totals of the last call: E_lj, E_coulomb_direct, virial (6)."""
+        _bind_stream()
+        out = (C.c_double * 8)()
+        check(lib().spgnb_lj_soft_totals(self.handle, out))
+        return np.array(out[:], np.float64)
+
+    def perturbed_atoms(self):
+        """Atoms whose pairs the two-state kernel evaluates (global indices)."""
+        n = C.c_int()
+        check(lib().spgnb_lj_soft_perturbed_atoms(self.handle, C.byref(n), None, 0))
+        out = np.zeros(max(n.value, 1), np.int32)
+        check(lib().spgnb_lj_soft_perturbed_atoms(self.handle, C.byref(n), out.ctypes.data_as(C.c_void_p), n.value))
+        return out[:n.value]
+
+    def Step_Print(self, controller=None):
+        """LJ_soft_core.cpp:848-862: LJ_soft_short, LJ_soft_long and LJ_soft."""
+        _bind_stream()
+        s, l, t, d = C.c_double(), C.c_double(), C.c_double(), C.c_double()
+        check(lib().spgnb_lj_soft_energies(self.handle, C.byref(s), C.byref(l), C.byref(t), C.byref(d)))
+        self.h_LJ_energy_sum = s.value
+        self.h_LJ_long_energy = l.value
+        out = {"LJ_soft_short": s.value, "LJ_soft_long": l.value, "LJ_soft": t.value}
+        if controller is not None and hasattr(controller, "update"):
+            controller.update({f"print_{k}": v for k, v in out.items()})
+        return out
+
+    def Clear(self):
+        if self.handle is not None:
+            lib().spgnb_lj_soft_destroy(self.handle)
+            self.handle = None
+        self.is_initialized = False
+
+    def __del__(self):
+        try:
+            self.Clear()
+        except Exception:
+            pass

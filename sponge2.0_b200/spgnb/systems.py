@@ -452,3 +452,170 @@ def request_system(req: Request, skin=2.0):
         except RuntimeError:
             if attempt == 49:
                 raise
+
+
+# ---------------------------------------------------------------------------
+# Two-state (alchemical) variants for LJ_SOFT_CORE
+# ---------------------------------------------------------------------------
+
+@dataclass
+class FepSystem:
+    """A two-state copy of a System: per-atom state-A / state-B LJ types, the
+    four triangular tables (AA, AB of state A; BA, BB of state B, internal
+    convention), state charges, and the soft-core parameters
+    (lambda_lj, soft_core_alpha, soft_core_powfer, soft_core_sigma,
+    soft_core_sigma_min)."""
+    base: System
+    type_a: np.ndarray
+    type_b: np.ndarray
+    n_types_a: int
+    n_types_b: int
+    AA: np.ndarray
+    AB: np.ndarray
+    BA: np.ndarray
+    BB: np.ndarray
+    charge_a: np.ndarray
+    charge_b: np.ndarray
+    lam: float
+    alpha: float = 0.5
+    p: float = 1.0
+    sigma: float = 3.0
+    sigma_min: float = 0.0
+    changed: np.ndarray = field(default=None)   # the atoms the generator perturbed
+
+    def charge(self, lam=None):
+        """Charges at lambda, q = (1 - lambda) q_A + lambda q_B (float32)."""
+        lam = self.lam if lam is None else lam
+        return ((1.0 - lam) * self.charge_a.astype(np.float64) +
+                lam * self.charge_b.astype(np.float64)).astype(np.float32)
+
+    def charge_ba(self):
+        return (self.charge_b.astype(np.float64) - self.charge_a.astype(np.float64)).astype(np.float32)
+
+    def params(self, lam=None):
+        return np.array([self.lam if lam is None else lam, self.alpha, self.p, self.sigma, self.sigma_min],
+                        np.float32)
+
+    def system(self, lam=None):
+        """The base System with the charges at lambda."""
+        from dataclasses import replace
+        return replace(self.base, charge=self.charge(lam))
+
+    def controller(self, lam=None):
+        return {"lambda_lj": float(self.lam if lam is None else lam), "soft_core_alpha": self.alpha,
+                "soft_core_powfer": self.p, "soft_core_sigma": self.sigma, "soft_core_sigma_min": self.sigma_min}
+
+
+def _with_dummy_type(A, B, n_types):
+    """Tables of n_types + 1 types, the last one interacting with nothing."""
+    m = n_types + 1
+    A2 = np.zeros(m * (m + 1) // 2, np.float32)
+    B2 = np.zeros_like(A2)
+    A2[:len(A)] = A
+    B2[:len(B)] = B
+    return A2, B2
+
+
+def _permute_table(T, perm):
+    """Table re-indexed so that new type perm[t] is old type t."""
+    m = len(perm)
+    out = np.zeros_like(T)
+    for a in range(m):
+        for b in range(a + 1):
+            out[lj_type_index(perm[a], perm[b])] = T[lj_type_index(a, b)]
+    return out
+
+
+def fep_system(base: System, n_perturbed=24, seed=7, lam=0.5, alpha=0.5, p=1.0, sigma=3.0, sigma_min=0.0,
+               kinds=("vanish", "appear", "mutate"), permute_b=True, bond_perturbed=True):
+    """Perturbs the n_perturbed solutes nearest a random solute (a ligand):
+    "vanish" atoms lose their LJ type (a dummy type that interacts with
+    nothing) and charge in state B, "appear" atoms have them only in state
+    B, "mutate" atoms take another solute type and the opposite half charge.
+    permute_b renumbers state B's types (its own index space, as the
+    reference allows); bond_perturbed adds exclusions between consecutive
+    perturbed atoms closer than 5 A, so excluded pairs run through the
+    perturbed set too."""
+    if base.n_solute < n_perturbed:
+        raise ValueError("not enough solute atoms to perturb")
+    rng = np.random.default_rng(seed)
+    T = base.n_types
+    dummy = T
+    AA, AB = _with_dummy_type(base.pair_A, base.pair_B, T)
+    BA, BB = AA.copy(), AB.copy()
+    # the ligand: solutes nearest a random one (minimum image in fractional space)
+    c0 = int(rng.integers(base.n_solute))
+    sol = base.crd[:base.n_solute].astype(np.float64)
+    r = np.asarray(base.rcell, np.float64)
+    c = np.asarray(base.cell, np.float64)
+    d = sol - sol[c0]
+    fx = d[:, 0] * r[0] + d[:, 1] * r[1] + d[:, 2] * r[3]
+    fy = d[:, 1] * r[2] + d[:, 2] * r[4]
+    fz = d[:, 2] * r[5]
+    fx -= np.round(fx)
+    fy -= np.round(fy)
+    fz -= np.round(fz)
+    dist = np.sqrt((fx * c[0] + fy * c[1] + fz * c[3]) ** 2 + (fy * c[2] + fz * c[4]) ** 2 + (fz * c[5]) ** 2)
+    chosen = np.sort(np.argsort(dist, kind="stable")[:n_perturbed])
+    ta = base.atom_type.astype(np.int32).copy()
+    tb = ta.copy()
+    qa = base.charge.astype(np.float32).copy()
+    qb = qa.copy()
+    n_solute_types = T - 2
+    for k, a in enumerate(chosen):
+        kind = kinds[k % len(kinds)]
+        if kind == "vanish":
+            tb[a] = dummy
+            qb[a] = 0.0
+        elif kind == "appear":
+            ta[a] = dummy
+            qa[a] = 0.0
+        elif kind == "mutate":
+            old = int(ta[a]) - 2
+            tb[a] = 2 + (old + 1 + int(rng.integers(n_solute_types - 1))) % n_solute_types
+            qb[a] = np.float32(-0.5) * qa[a]
+        else:
+            raise ValueError(kind)
+    n_b = T + 1
+    if permute_b:
+        perm = rng.permutation(n_b)
+        BA, BB = _permute_table(BA, perm), _permute_table(BB, perm)
+        tb = perm[tb].astype(np.int32)
+    s = base
+    if bond_perturbed and len(chosen) > 1:
+        # each perturbed atom bonded to its nearest perturbed neighbour within 5 A
+        g = base.crd[chosen].astype(np.float64)
+        dd = g[:, None, :] - g[None, :, :]
+        f0 = dd[..., 0] * r[0] + dd[..., 1] * r[1] + dd[..., 2] * r[3]
+        f1 = dd[..., 1] * r[2] + dd[..., 2] * r[4]
+        f2 = dd[..., 2] * r[5]
+        f0 -= np.round(f0)
+        f1 -= np.round(f1)
+        f2 -= np.round(f2)
+        dm = np.sqrt((f0 * c[0] + f1 * c[1] + f2 * c[3]) ** 2 + (f1 * c[2] + f2 * c[4]) ** 2 + (f2 * c[5]) ** 2)
+        np.fill_diagonal(dm, np.inf)
+        pairs = set()
+        for k in range(len(chosen)):
+            m = int(np.argmin(dm[k]))
+            if dm[k, m] < 5.0:
+                u, v = int(chosen[k]), int(chosen[m])
+                pairs.add((min(u, v), max(u, v)))
+        if pairs:
+            lists = [list(base.excl_list[base.excl_start[i]:base.excl_start[i] + base.excl_numbers[i]])
+                     for i in range(base.n)]
+            for lo, hi in pairs:
+                lists[lo].append(hi)
+            num = np.array([len(x) for x in lists], np.int32)
+            start = np.zeros(base.n, np.int32)
+            start[1:] = np.cumsum(num)[:-1]
+            flat = np.array([j for x in lists for j in sorted(x)], np.int32)
+            from dataclasses import replace
+            s = replace(base, excl_start=start, excl_numbers=num, excl_list=flat)
+    return FepSystem(base=s, type_a=ta, type_b=tb, n_types_a=T + 1, n_types_b=n_b, AA=AA, AB=AB, BA=BA, BB=BB,
+                     charge_a=qa, charge_b=qb, lam=_f32(lam), alpha=_f32(alpha), p=_f32(p), sigma=_f32(sigma),
+                     sigma_min=_f32(sigma_min), changed=chosen)
+
+
+def _f32(v):
+    """A parameter as the float32 value the modules receive."""
+    return float(np.float32(v))
