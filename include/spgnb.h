@@ -394,6 +394,12 @@ int spgnb_solvent_pme_direct_force(spgnb_solvent* s, int atom_numbers, int resid
                                    int need_atom_energy, float* d_atom_energy, int need_virial,
                                    spgnb_ltmatrix3* d_atom_virial, float* d_atom_direct_pme_energy);
 
+/* The same module next to LJ_SOFT_CORE (an alchemical run has no plain LJ
+ * module; solvent_LJ.cpp:310-349 takes the waters with the soft-core
+ * module's state-A table): over an spgnb list the soft-core force call
+ * evaluates the water pairs and this module's call returns at once. */
+int spgnb_solvent_create_soft(spgnb_lj_soft* lj, int water_points, spgnb_solvent** out);
+
 int spgnb_solvent_destroy(spgnb_solvent* s);
 
 /* ------------------------------------------------ no-allocation force call */

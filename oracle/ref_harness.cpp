@@ -337,7 +337,6 @@ double ref_time_rebuild(const float* crd, int reps)
     return std::chrono::duration<double>(t1 - t0).count() / (reps > 0 ? reps : 1);
 }
 
-#ifndef REF_HARNESS_SHIM
 // LJ_SOFT_CORE::Initial (LJ_soft_core.cpp:438-641) from arrays given the way
 // Xponge hands them over (Xponge::LJSoftCore, xponge/ir/forcefield.h:82-94),
 // the control keys set from prm = {lambda_lj, soft_core_alpha,
@@ -493,7 +492,6 @@ double ref_soft_time_steps(const float* crd, const float* charge, float beta, in
     auto t1 = std::chrono::steady_clock::now();
     return std::chrono::duration<double>(t1 - t0).count();
 }
-#endif
 
 void ref_clear()
 {

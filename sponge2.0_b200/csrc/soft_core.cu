@@ -795,6 +795,12 @@ int spgnb_lj_soft_perturbed_atoms(const spgnb_lj_soft* lj, int* count, int* h_at
     return SPGNB_OK;
 }
 
+int spgnb_solvent_create_soft(spgnb_lj_soft* lj, int water_points, spgnb_solvent** out)
+{
+    if (!lj) return fail(SPGNB_E_ARG, "spgnb_solvent_create_soft: NULL handle");
+    return spgnb_solvent_create(lj->inner, water_points, out);
+}
+
 int spgnb_lj_soft_destroy(spgnb_lj_soft* lj)
 {
     if (!lj) return SPGNB_OK;

@@ -42,9 +42,9 @@ void SOLVENT_LENNARD_JONES::Initial(CONTROLLER* controller, LENNARD_JONES_INFORM
         enable = controller->Get_Bool(this->module_name, "SOLVENT_LENNARD_JONES::Initial");
     if (enable) water_points = md_info->ug.ug[md_info->ug.ug_numbers - 1].atom_numbers;
     if (water_points != 3 && water_points != 4) enable = false;
-    if (enable && !lj->is_initialized && lj_soft->is_initialized)
-        controller->Throw_SPONGE_Error(spongeErrorNotImplemented, "SOLVENT_LENNARD_JONES::Initial",
-                                       "the soft-core water path is not part of spgnb");
+    // an alchemical run has the soft-core module instead of the plain one
+    // (solvent_LJ.cpp:310-349): the waters go with it
+    const bool soft = !lj->is_initialized && lj_soft->is_initialized;
     if (enable)
     {
         lj_info = lj;
@@ -71,7 +71,9 @@ void SOLVENT_LENNARD_JONES::Initial(CONTROLLER* controller, LENNARD_JONES_INFORM
         if (solvent_numbers > 0)
         {
             spgnb_solvent* h = nullptr;
-            raise(controller, spgnb_solvent_create(spgnb_shim::lj_of(lj), water_points, &h),
+            raise(controller,
+                  soft ? spgnb_solvent_create_soft(spgnb_shim::lj_soft_of(lj_soft), water_points, &h)
+                       : spgnb_solvent_create(spgnb_shim::lj_of(lj), water_points, &h),
                   "SOLVENT_LENNARD_JONES::Initial");
             std::lock_guard<std::mutex> lk(g_mu);
             handles()[this] = h;

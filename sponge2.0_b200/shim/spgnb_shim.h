@@ -61,4 +61,8 @@ CONTROLLER* default_controller();
 // Lennard_Jones_force_spgnb.cpp), NULL before its Initial.
 spgnb_lj* lj_of(const void* lj_information);
 
+// The spgnb soft-core module behind an LJ_SOFT_CORE (defined in
+// LJ_soft_core_spgnb.cpp), NULL before its Initial.
+spgnb_lj_soft* lj_soft_of(const void* lj_soft_core);
+
 }  // namespace spgnb_shim

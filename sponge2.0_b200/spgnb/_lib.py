@@ -32,7 +32,7 @@ EXPORTED = [
     "spgnb_lj_soft_pme_direct_force", "spgnb_lj_soft_partial_h_partial_lambda",
     "spgnb_lj_soft_long_range_correction", "spgnb_lj_soft_energies", "spgnb_lj_soft_totals",
     "spgnb_lj_soft_long_range_factors", "spgnb_lj_soft_atom_lj_energy", "spgnb_lj_soft_perturbed_atoms",
-    "spgnb_lj_soft_destroy",
+    "spgnb_lj_soft_destroy", "spgnb_solvent_create_soft",
     "spgnb_batch_default_options", "spgnb_batch_create", "spgnb_batch_run", "spgnb_batch_energies",
     "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_stream",
     "spgnb_batch_check_overflow", "spgnb_batch_set_thermostat",
@@ -189,6 +189,7 @@ def lib():
     L.spgnb_lj_soft_atom_lj_energy.argtypes = [vp, C.POINTER(vp)]
     L.spgnb_lj_soft_perturbed_atoms.argtypes = [vp, C.POINTER(i), vp, i]
     L.spgnb_lj_soft_destroy.argtypes = [vp]
+    L.spgnb_solvent_create_soft.argtypes = [vp, i, C.POINTER(vp)]
     _lib = L
     return L
 

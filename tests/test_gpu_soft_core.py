@@ -157,3 +157,35 @@ def test_soft_core_vs_reference_cuda_kernels(torch_cuda, name, solvent):
     v, vd = p.dhdl(charge_perturbated=True)
     assert abs(v - dh) <= 2e-5 * (abs(v) + 10.0)
     assert abs(vd - dh_c) <= 2e-5 * (abs(vd) + 10.0)
+
+
+REF_SHIM = os.path.join(ROOT, "oracle", "_ref", "libspgref_shim.so")
+
+
+@pytest.mark.skipif(not os.path.exists(REF_SHIM), reason="drop-in harness not built")
+@pytest.mark.parametrize("name", CASES)
+def test_soft_core_through_sponge_module_api(torch_cuda, oracle, name):
+    """SPONGE's own LJ_SOFT_CORE class, built with the drop-in shim over
+    libspgnb (sponge2.0_b200/shim/LJ_soft_core_spgnb.cpp), driven by the same
+    C++ harness as the reference: Initial from Xponge's arrays, Get_Local,
+    the force and dH/dlambda, against the FP64 oracle."""
+    import oracle as O
+    f, z, m = load_soft(name)
+    ref = O.Reference(shim=True)
+    ref.init(f.system())
+    ref.nl_update(forced=True)
+    ref.soft_init(f)
+    r = ref.soft_force(need_energy=True, need_virial=True)
+    dh, dh_c = ref.soft_dhdl(charge_perturbated=True)
+    lr, lr_ti = ref.soft_long_range()
+    ref.clear()
+    o = oracle.soft_core(f)
+    assert rel_rms(r["frc"], o["frc"]) <= FORCE_REL_RMS_TOL
+    scale = abs(o["e_lj"]) + abs(o["e_coul"])
+    assert abs(r["atom_lj"].astype(np.float64).sum() - o["e_lj"]) <= ENERGY_REL_TOL * scale
+    assert abs(r["atom_direct"].astype(np.float64).sum() - o["e_coul"]) <= ENERGY_REL_TOL * scale
+    olr, olr_ti = oracle.soft_long_range(f)
+    assert abs(lr - olr) <= 1e-6 * abs(olr) and abs(lr_ti - olr_ti) <= 1e-6 * abs(olr_ti)
+    want = o["dh_lj"] + olr_ti / f.base.volume
+    assert abs(dh - want) <= 2e-5 * (abs(want) + 10.0)
+    assert abs(dh_c - o["dh_c"]) <= 2e-5 * (abs(o["dh_c"]) + 10.0)
