@@ -607,138 +607,97 @@ __global__ void k_export_zero(int n, spgnb_atom_group* __restrict__ nl, const in
     }
 }
 
-__global__ void k_export(int clusters_cap, int table_cap, const int* __restrict__ tcount, const float4* __restrict__ tab,
-                         const uint2* __restrict__ tmask, const int* __restrict__ slot_atom,
-                         const float4* __restrict__ slot_x0, spgnb_atom_group* __restrict__ nl,
-                         int* __restrict__ temp, int max_nb, int* counters)
+// ATOM_GROUP lists from the cluster tables, where each atom's partners on
+// both sides already sit with its own cluster, so one warp per atom writes
+// its list in table order: no atomics, the same order on every call.
+//   HALF: the reference-layout half list of NEIGHBOR_LIST::d_nl, each listed
+//   pair with its owner (the lower atom_local index) as the reference stores
+//   it; runs after a rebuild only (need: the device's rebuild flag).
+//   full: FULL_NEIGHBOR_LIST::Build_From_Half / Build_From_Half_With_Cutoff
+//   (full_neighbor_list.cpp:27-147), every listed pair in both atoms' lists.
+//   With a cutoff, a pair is kept when its distance at d_crd is within it,
+//   measured from the lower-index atom as the reference does
+//   (Get_Periodic_Displacement(r_i, r_j)).
+// A list longer than max_nb is cut and ovf_bits set in *overflow.
+template <bool HALF>
+__global__ void k_export_lists(int clusters_cap, int table_cap, const int* __restrict__ tcount,
+                               const float4* __restrict__ tab, const uint2* __restrict__ tmask,
+                               const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0,
+                               const float3* __restrict__ crd, Cell cell, Cell rcell, float cut2,
+                               spgnb_atom_group* __restrict__ full, int max_nb, int* __restrict__ overflow,
+                               int ovf_bits, const int* __restrict__ need)
 {
-    if (counters[kCntNeed] == 0) return;
+    if (HALF && *need == 0) return;
     const int lane = threadIdx.x & 31;
     const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < clusters_cap; c += warps)
+    // one warp per own slot (cluster c, atom a): its list in table order
+    for (int item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < clusters_cap * kClusterSize;
+         item += warps)
     {
-        // own atoms and global indices, lane a holds slot a
-        const int own_atom = lane < 8 ? slot_atom[c * kClusterSize + lane] : -1;
-        const int own_g = lane < 8 ? __float_as_int(slot_x0[c * kClusterSize + lane].w) : -1;
+        const int c = item / kClusterSize, a = item % kClusterSize;
+        const int ia = slot_atom[item];
+        if (ia < 0) continue;  // warp-uniform
         const int T = tcount[c];
-        for (int t0 = 0; t0 < T; t0 += 32)
-        {
-            const int t = t0 + lane;
-            unsigned long long m = 0;
-            int base = 0;
-            if (t < T)
-            {
-                const uint2 mm = tmask[(size_t)c * table_cap + t];
-                m = ((unsigned long long)mm.y << 32) | mm.x;
-                base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
-            }
-            for (int a = 0; a < kClusterSize; a++)
-            {
-                const int ia = __shfl_sync(0xffffffffu, own_atom, a);
-                const int gia = __shfl_sync(0xffffffffu, own_g, a);
-                unsigned row = (unsigned)(m >> (8 * a)) & 0xffu;
-                while (row)
-                {
-                    const int b = __ffs(row) - 1;
-                    row &= row - 1;
-                    const float4 xb = slot_x0[base + b];
-                    if (gia < __float_as_int(xb.w))
-                    {
-                        const int jb = slot_atom[base + b];
-                        const int k = atomicAdd(&nl[ia].atom_numbers, 1);
-                        if (k < max_nb)
-                            temp[(size_t)ia * max_nb + k] = jb;
-                        else
-                            atomicOr(&counters[kCntOverflow], kOvfList);
-                    }
-                }
-            }
-        }
-    }
-}
-
-// FULL_NEIGHBOR_LIST::Build_From_Half / Build_From_Half_With_Cutoff
-// (full_neighbor_list.cpp:27-147): every listed pair in both atoms' lists, in
-// the caller's ATOM_GROUP arrays.  Built from the cluster tables, where each
-// atom's partners on both sides already sit with its own cluster, so one warp
-// per cluster writes its atoms' complete lists in table order: no atomics,
-// the same order on every call.  With a cutoff, a pair is kept when its
-// distance at d_crd is within it, measured from the lower-index atom as the
-// reference does (Get_Periodic_Displacement(r_i, r_j)).
-__global__ void k_export_full(int clusters_cap, int table_cap, const int* __restrict__ tcount,
-                              const float4* __restrict__ tab, const uint2* __restrict__ tmask,
-                              const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0,
-                              const float3* __restrict__ crd, Cell cell, Cell rcell, float cut2,
-                              spgnb_atom_group* __restrict__ full, int max_nb, int* __restrict__ overflow)
-{
-    const int lane = threadIdx.x & 31;
-    const int warps = gridDim.x * (blockDim.x >> 5);
-    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < clusters_cap; c += warps)
-    {
-        const int T = tcount[c];
-        if (T == 0) continue;
-        // lane a < 8: own atom a, its global index, list and running count
-        const int own_atom = lane < 8 ? slot_atom[c * kClusterSize + lane] : -1;
-        const int own_g = lane < 8 ? __float_as_int(slot_x0[c * kClusterSize + lane].w) : -1;
-        int* own_list = own_atom >= 0 ? full[own_atom].atom_serial : nullptr;
+        const int gia = __float_as_int(slot_x0[item].w);
+        int* list = full[ia].atom_serial;
+        const float3 xi = (!HALF && cut2 >= 0.0f) ? crd[ia] : make_float3(0.0f, 0.0f, 0.0f);
         int count = 0;
         for (int t0 = 0; t0 < T; t0 += 32)
         {
             const int t = t0 + lane;
-            unsigned long long m = 0;
+            unsigned row = 0;
             int base = 0;
             if (t < T)
             {
                 const uint2 mm = tmask[(size_t)c * table_cap + t];
-                m = ((unsigned long long)mm.y << 32) | mm.x;
+                row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
                 base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
             }
-            for (int a = 0; a < kClusterSize; a++)
+            unsigned keep = row;
+            if (HALF)
             {
-                const int ia = __shfl_sync(0xffffffffu, own_atom, a);
-                if (ia < 0) continue;  // warp-uniform
-                const int gia = __shfl_sync(0xffffffffu, own_g, a);
-                const unsigned row = (unsigned)(m >> (8 * a)) & 0xffu;
-                unsigned keep = row;
-                if (cut2 >= 0.0f && row)
-                {
-                    const float3 xi = crd[ia];
-                    keep = 0;
-                    for (unsigned r = row; r; r &= r - 1)
-                    {
-                        const int b = __ffs(r) - 1;
-                        const int jb = slot_atom[base + b];
-                        const float3 xj = crd[jb];
-                        const bool i_lo = gia < __float_as_int(slot_x0[base + b].w);
-                        const float d2 = i_lo ? ref_pair_dr2(xi, xj, cell, rcell) : ref_pair_dr2(xj, xi, cell, rcell);
-                        if (d2 <= cut2) keep |= 1u << b;
-                    }
-                }
-                const int k = __popc(keep);
-                int incl = k;
-                for (int o = 1; o < 32; o <<= 1)
-                {
-                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                    if (lane >= o) incl += y;
-                }
-                const int total = __shfl_sync(0xffffffffu, incl, 31);
-                int pos = __shfl_sync(0xffffffffu, count, a) + incl - k;
-                int* list = (int*)__shfl_sync(0xffffffffu, (unsigned long long)own_list, a);
-                for (unsigned r = keep; r; r &= r - 1, pos++)
+                keep = 0;
+                for (unsigned r = row; r; r &= r - 1)
                 {
                     const int b = __ffs(r) - 1;
-                    if (pos < max_nb)
-                        list[pos] = slot_atom[base + b];
-                    else
-                        atomicExch(overflow, 1);
+                    if (gia < __float_as_int(slot_x0[base + b].w)) keep |= 1u << b;
                 }
-                if (lane == a) count += total;
             }
+            else if (cut2 >= 0.0f && row)
+            {
+                keep = 0;
+                for (unsigned r = row; r; r &= r - 1)
+                {
+                    const int b = __ffs(r) - 1;
+                    const int jb = slot_atom[base + b];
+                    const float3 xj = crd[jb];
+                    const bool i_lo = gia < __float_as_int(slot_x0[base + b].w);
+                    const float d2 = i_lo ? ref_pair_dr2(xi, xj, cell, rcell) : ref_pair_dr2(xj, xi, cell, rcell);
+                    if (d2 <= cut2) keep |= 1u << b;
+                }
+            }
+            const int k = __popc(keep);
+            int incl = k;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            int pos = count + incl - k;
+            for (unsigned r = keep; r; r &= r - 1, pos++)
+            {
+                const int b = __ffs(r) - 1;
+                if (pos < max_nb)
+                    list[pos] = slot_atom[base + b];
+                else
+                    atomicOr(overflow, ovf_bits);
+            }
+            count += __shfl_sync(0xffffffffu, incl, 31);
         }
-        if (own_atom >= 0)
+        if (lane == 0)
         {
-            full[own_atom].atom_numbers = count;
-            full[own_atom].ghost_numbers = 0;
+            full[ia].atom_numbers = count;
+            full[ia].ghost_numbers = 0;
         }
     }
 }
@@ -1500,10 +1459,11 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     {
         k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_export_zero");
-        k_export<<<std::max(1, std::min((ccap + 3) / 4, sms * 8)), 128, 0, s>>>(
-            ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_nl,
-            nl->d_temp, nl->opt.max_neighbor_numbers, nl->d_counters);
-        SPGNB_CHECK_LAUNCH("k_export");
+        k_export_lists<true><<<std::max(1, std::min((ccap * kClusterSize + 3) / 4, sms * 16)), 128, 0, s>>>(
+            ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nullptr,
+            Cell{}, Cell{}, -1.0f, nl->d_nl, nl->opt.max_neighbor_numbers, nl->d_counters + kCntOverflow, kOvfList,
+            nl->d_counters + kCntNeed);
+        SPGNB_CHECK_LAUNCH("k_export_lists");
     }
     const int fin = std::max(nl->G, nl->S);
     k_finish<<<(fin + 255) / 256, 256, 0, s>>>(nl->G, nl->S, nl->d_cell_sys, nl->d_need, nl->d_prune,
@@ -1765,11 +1725,11 @@ int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector
     k_zero_groups<<<(n + 255) / 256, 256, 0, s>>>(n, d_full_nl);
     SPGNB_CHECK_LAUNCH("k_zero_groups");
     const int ccap = nl->clusters_cap;
-    k_export_full<<<std::max(1, std::min((ccap + 3) / 4, num_sms() * 8)), 128, 0, s>>>(
+    k_export_lists<false><<<std::max(1, std::min((ccap * kClusterSize + 3) / 4, num_sms() * 16)), 128, 0, s>>>(
         ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0,
         (const float3*)d_crd, make_cell(cell), make_cell(rcell), cutoff > 0.0f ? cutoff * cutoff : -1.0f, d_full_nl,
-        max_neighbor_numbers, d_overflow);
-    SPGNB_CHECK_LAUNCH("k_export_full");
+        max_neighbor_numbers, d_overflow, 1, nullptr);
+    SPGNB_CHECK_LAUNCH("k_export_lists");
     return SPGNB_OK;
 }
 

@@ -474,7 +474,8 @@ __device__ __forceinline__ float centre_step(int qj, int qi)
 // MODE 0: forces.  MODE 1: + energy and virial totals (each pair is seen
 // from both atoms, so the sums are halved).  MODE 2: + per-atom energy and
 // virial of the pairs the atom owns (the lower global index; water sites
-// hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES does).
+// hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES does),
+// and the totals summed from those (each pair once).
 // One item's header and first list window, staged in shared memory by
 // asynchronous copies (cp.async) while the warp works on the item before.
 struct alignas(16) ItemStage
@@ -526,6 +527,9 @@ __device__ __forceinline__ T reduce_scatter8(const T (&v)[8], int lane)
     return y;
 }
 
+#ifndef SPGNB_PAIR_MINB2
+#define SPGNB_PAIR_MINB2 3
+#endif
 #ifndef SPGNB_PAIR_MINB0
 #define SPGNB_PAIR_MINB0 4
 #endif
@@ -534,7 +538,7 @@ __device__ __forceinline__ T reduce_scatter8(const T (&v)[8], int lane)
 #endif
 constexpr int kPrefetch = SPGNB_PAIR_PREFETCH;  // list windows in flight per warp
 template <int MODE, int FIT, bool TRI>
-__global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0 : (MODE == 1 ? 3 : 2))
+__global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0 : (MODE == 1 ? 3 : SPGNB_PAIR_MINB2))
     k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
                 int n_clusters, int slot_cap,
                 const int* __restrict__ cl_sys, const int* __restrict__ pcount, const unsigned* __restrict__ pwords,
@@ -638,13 +642,11 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
         const float2 npx = make_float2(-pi1.x, -pi2.x), npy = make_float2(-pi1.y, -pi2.y),
                      npz = make_float2(-pi1.z, -pi2.z), qi2 = make_float2(pi1.w, pi2.w);
         float2 fx = f2(0.0f), fy = f2(0.0f), fz = f2(0.0f);
-        float2 acc[8], own[8];
+        float2 acc[PA ? 1 : 8], own[PA ? 8 : 1];  // totals (MODE 1) or owned sums (MODE 2)
 #pragma unroll
-        for (int q = 0; q < 8; q++)
-        {
-            acc[q] = f2(0.0f);
-            own[q] = f2(0.0f);
-        }
+        for (int q = 0; q < (PA ? 1 : 8); q++) acc[q] = f2(0.0f);
+#pragma unroll
+        for (int q = 0; q < (PA ? 8 : 1); q++) own[q] = f2(0.0f);
         // one list word: the partner against both atoms
         auto eval_word = [&](unsigned cw, int j, float4 pj, int4 cj) {
             const float4 ab = rows[(cw >> kWordTypeShift) & 0x7fu];
@@ -696,23 +698,31 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
                 fx = __fadd2_rn(fx, gx);
                 fy = __fadd2_rn(fy, gy);
                 fz = __fadd2_rn(fz, gz);
-                elj = make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f);
-                ec = make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f);
-                acc[0] = __fadd2_rn(acc[0], elj);
-                acc[1] = __fadd2_rn(acc[1], ec);
-                acc[2] = __ffma2_rn(gx, dx, acc[2]);
-                acc[3] = __ffma2_rn(gx, dy, acc[3]);
-                acc[4] = __ffma2_rn(gy, dy, acc[4]);
-                acc[5] = __ffma2_rn(gx, dz, acc[5]);
-                acc[6] = __ffma2_rn(gy, dz, acc[6]);
-                acc[7] = __ffma2_rn(gz, dz, acc[7]);
-                if (PA)
+                if (!PA)
                 {
-                    const int gj = __float_as_int(slot_x0[j].w);
-                    const float2 m = make_float2(gi1 < gj ? 1.0f : 0.0f, gi2 < gj ? 1.0f : 0.0f);
-                    own[0] = __ffma2_rn(m, elj, own[0]);
-                    own[1] = __ffma2_rn(m, ec, own[1]);
-                    const float2 mgx = __fmul2_rn(m, gx), mgy = __fmul2_rn(m, gy), mgz = __fmul2_rn(m, gz);
+                    elj = make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f);
+                    ec = make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f);
+                    acc[0] = __fadd2_rn(acc[0], elj);
+                    acc[1] = __fadd2_rn(acc[1], ec);
+                    acc[2] = __ffma2_rn(gx, dx, acc[2]);
+                    acc[3] = __ffma2_rn(gx, dy, acc[3]);
+                    acc[4] = __ffma2_rn(gy, dy, acc[4]);
+                    acc[5] = __ffma2_rn(gx, dz, acc[5]);
+                    acc[6] = __ffma2_rn(gy, dz, acc[6]);
+                    acc[7] = __ffma2_rn(gz, dz, acc[7]);
+                }
+                else
+                {
+                    // only the pair's owner (the lower global index) keeps its
+                    // energy and virial; the totals are summed from these, so
+                    // every pair counts once
+                    const int gj = __ldg(reinterpret_cast<const int*>(slot_x0) + 4 * (size_t)j + 3);
+                    const bool oA = inA && gi1 < gj, oB = inB && gi2 < gj;
+                    own[0] = __fadd2_rn(own[0], make_float2(oA ? elj.x : 0.0f, oB ? elj.y : 0.0f));
+                    own[1] = __fadd2_rn(own[1], make_float2(oA ? ec.x : 0.0f, oB ? ec.y : 0.0f));
+                    const float2 mgx = make_float2(oA ? gx.x : 0.0f, oB ? gx.y : 0.0f);
+                    const float2 mgy = make_float2(oA ? gy.x : 0.0f, oB ? gy.y : 0.0f);
+                    const float2 mgz = make_float2(oA ? gz.x : 0.0f, oB ? gz.y : 0.0f);
                     own[2] = __ffma2_rn(mgx, dx, own[2]);
                     own[3] = __ffma2_rn(mgx, dy, own[3]);
                     own[4] = __ffma2_rn(mgy, dy, own[4]);
@@ -752,7 +762,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             if (ai >= 0)  // one add per component and call: the same as a read-modify-write, without the wait
                 atomicAdd(&frc[ai].x + (vidx % 3), (float)((double)fsum * kForceUnscale));
         }
-        if (EN)
+        if (EN && !PA)
         {
             float ev[8];
 #pragma unroll
@@ -785,6 +795,17 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
                     own1[q] += __shfl_xor_sync(0xffffffffu, own1[q], o);
                     own2[q] += __shfl_xor_sync(0xffffffffu, own2[q], o);
                 }
+            if (lane == 0)
+            {
+                // the item's totals: each pair once; the symmetric off-diagonal
+                // terms (xy + yx etc.) are twice the one accumulated
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                {
+                    const double sc = (q == 3 || q == 5 || q == 6) ? 2.0 : 1.0;
+                    red[w][q] += __double2ll_rn((double)(own1[q] + own2[q]) * sc * kEnergyScale);
+                }
+            }
             if (lane < 2)
             {
                 const int ai = slot_atom[s1 + lane];

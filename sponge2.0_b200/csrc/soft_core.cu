@@ -161,110 +161,109 @@ __device__ __forceinline__ SoftPair soft_pair(const SoftConst& k, float r2, floa
     return o;
 }
 
-// One warp per listed atom i (list == nullptr: items are local atoms, flag
-// selects).  The warp walks the table of i's cluster; lane t takes element t
-// and, from its pair mask, i's partners in that neighbour cluster.  A partner
-// that is itself flagged and has the lower global index owns the pair and
-// skips it here.  Forces go to int64 accumulators; energy and virial to the
-// pair's owner (lower global index), the totals in fixed point.
+// One thread per candidate pair: a warp takes a listed atom i and four
+// elements of the table of i's cluster (list == nullptr: the atoms are the
+// local atoms, flag selects), lane 8e + b the neighbour slot b of element e,
+// kept when the element's pair mask pairs it with i.  So an atom's pairs
+// spread over many warps and no lane evaluates more than one: the kernel's
+// time is one pair's latency, not a list's.  A partner that is itself
+// flagged and has the lower global index owns the pair and skips it here.
+// Forces go to int64 accumulators; energy and virial to the pair's owner
+// (lower global index), the totals in fixed point.
+constexpr int kSoftElems = 4;   // table elements per warp
+
 template <bool FORCE, bool EN, bool PA, bool DH, bool DHC>
 __global__ void __launch_bounds__(kSoftWarps * 32)
-    k_soft_pairs(SoftConst k, Cell cell, Cell rcell, int n_items, const int* __restrict__ list,
-                 const unsigned char* __restrict__ flag, const int* __restrict__ atom_local,
-                 const int* __restrict__ atom_slot, const int* __restrict__ slot_atom, const int* __restrict__ tcount,
-                 const float4* __restrict__ tab, const uint2* __restrict__ tmask, int table_cap,
-                 const float3* __restrict__ crd, const float* __restrict__ charge,
-                 const float* __restrict__ charge_ba, const int2* __restrict__ types,
-                 const float* __restrict__ tAA, const float* __restrict__ tAB, const float* __restrict__ tBA,
-                 const float* __restrict__ tBB, long long* __restrict__ acc, long long* __restrict__ totals,
-                 PerAtomOut pa, long long* __restrict__ dh)
+    k_soft_pairs(SoftConst k, Cell cell, Cell rcell, long long n_items, int chunks, const int* __restrict__ list,
+                 const unsigned char* __restrict__ flag,
+                 const int* __restrict__ atom_local, const int* __restrict__ atom_slot,
+                 const int* __restrict__ slot_atom, const int* __restrict__ tcount, const float4* __restrict__ tab,
+                 const uint2* __restrict__ tmask, int table_cap, const float3* __restrict__ crd,
+                 const float* __restrict__ charge, const float* __restrict__ charge_ba,
+                 const int2* __restrict__ types, const float* __restrict__ tAA, const float* __restrict__ tAB,
+                 const float* __restrict__ tBA, const float* __restrict__ tBB, long long* __restrict__ acc,
+                 long long* __restrict__ totals, PerAtomOut pa, long long* __restrict__ dh)
 {
     const int lane = threadIdx.x & 31;
-    const int item = blockIdx.x * kSoftWarps + (threadIdx.x >> 5);
+    const long long item = (long long)blockIdx.x * kSoftWarps + (threadIdx.x >> 5);
     if (item >= n_items) return;  // whole warps
-    const int i = list ? list[item] : item;
+    const int ia = (int)(item / chunks);
+    const int t0 = (int)(item % chunks) * kSoftElems;
+    const int i = list ? list[ia] : ia;
     if (!flag[i]) return;
     const int s = atom_slot[i];
     if (s < 0) return;
     const int c = s / kClusterSize, a = s % kClusterSize;
     const int T = tcount[c];
+    if (t0 >= T) return;
     const float3 ri = crd[i];
     const float qi = charge[i];
     const float qbi = DHC ? charge_ba[i] : 0.0f;
     const int2 ti = types[i];
     const int gi = atom_local[i];
     float fx = 0.0f, fy = 0.0f, fz = 0.0f;
-    float tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // this lane's pairs: E_lj, E_c, virial
+    float tot[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // this lane's pair: E_lj, E_c, virial
     float own[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // the part owned by i
     float dl = 0.0f, dc = 0.0f;
-    for (int t0 = 0; t0 < T; t0 += 32)
+    do
     {
-        const int t = t0 + lane;
-        unsigned row = 0;
-        int base = 0;
-        if (t < T)
+        const int t = t0 + (lane >> 3), b = lane & 7;
+        if (t >= T) break;
+        const uint2 mm = tmask[(size_t)c * table_cap + t];
+        if (!((((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) >> b) & 1u)) break;
+        const int base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
+        const int j = slot_atom[base + b];
+        if (j < 0 || j == i) break;
+        const int gj = atom_local[j];
+        if (flag[j] && gj < gi) break;
+        const float3 rj = crd[j];
+        float dx = rj.x - ri.x, dy = rj.y - ri.y, dz = rj.z - ri.z;
+        min_image(dx, dy, dz, cell, rcell);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (!(r2 < k.rc2)) break;
+        const int2 tj = types[j];
+        const int pa_ = tri_index(ti.x, tj.x), pb_ = tri_index(ti.y, tj.y);
+        const float qj = charge[j];
+        const float dq = DHC ? qbi * qj + qi * charge_ba[j] : 0.0f;
+        const SoftPair o = soft_pair<EN, DH, DHC>(k, r2, qi * qj, dq, tAA[pa_], tAB[pa_], tBA[pb_], tBB[pb_]);
+        if (DH)
         {
-            const uint2 mm = tmask[(size_t)c * table_cap + t];
-            row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
-            base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
+            dl = o.dlj;
+            dc = o.dc;
         }
-        for (; row; row &= row - 1)
+        if (!FORCE) break;
+        const float gx = o.f * dx, gy = o.f * dy, gz = o.f * dz;
+        fx = gx;
+        fy = gy;
+        fz = gz;
+        red_fixed(acc + 4 * (size_t)j + 0, -gx);
+        red_fixed(acc + 4 * (size_t)j + 1, -gy);
+        red_fixed(acc + 4 * (size_t)j + 2, -gz);
+        if (EN)
         {
-            const int b = __ffs(row) - 1;
-            const int j = slot_atom[base + b];
-            if (j < 0 || j == i) continue;
-            const int gj = atom_local[j];
-            if (flag[j] && gj < gi) continue;
-            const float3 rj = crd[j];
-            float dx = rj.x - ri.x, dy = rj.y - ri.y, dz = rj.z - ri.z;
-            min_image(dx, dy, dz, cell, rcell);
-            const float r2 = dx * dx + dy * dy + dz * dz;
-            if (!(r2 < k.rc2)) continue;
-            const int2 tj = types[j];
-            const int pa_ = tri_index(ti.x, tj.x), pb_ = tri_index(ti.y, tj.y);
-            const float qj = charge[j];
-            const float dq = DHC ? qbi * qj + qi * charge_ba[j] : 0.0f;
-            const SoftPair o =
-                soft_pair<EN, DH, DHC>(k, r2, qi * qj, dq, tAA[pa_], tAB[pa_], tBA[pb_], tBB[pb_]);
-            if (DH)
-            {
-                dl += o.dlj;
-                dc += o.dc;
-            }
-            if (!FORCE) continue;
-            const float gx = o.f * dx, gy = o.f * dy, gz = o.f * dz;
-            fx += gx;
-            fy += gy;
-            fz += gz;
-            red_fixed(acc + 4 * (size_t)j + 0, -gx);
-            red_fixed(acc + 4 * (size_t)j + 1, -gy);
-            red_fixed(acc + 4 * (size_t)j + 2, -gz);
-            if (EN)
-            {
-                // Get_Virial_From_Force_Dis(F, dr) (vector.hpp:337-347), subtracted
-                const float w[8] = {o.elj, o.ec, -gx * dx, -(gx * dy + gy * dx), -gy * dy, -(gx * dz + gz * dx),
-                                    -(gy * dz + gz * dy), -gz * dz};
+            // Get_Virial_From_Force_Dis(F, dr) (vector.hpp:337-347), subtracted
+            const float w[8] = {o.elj, o.ec, -gx * dx, -(gx * dy + gy * dx), -gy * dy, -(gx * dz + gz * dx),
+                                -(gy * dz + gz * dy), -gz * dz};
 #pragma unroll
-                for (int q = 0; q < 8; q++) tot[q] += w[q];
-                if (PA)
+            for (int q = 0; q < 8; q++) tot[q] = w[q];
+            if (PA)
+            {
+                if (gi < gj)
                 {
-                    if (gi < gj)
-                    {
 #pragma unroll
-                        for (int q = 0; q < 8; q++) own[q] += w[q];
-                    }
-                    else
-                    {
-                        if (pa.energy) atomicAdd(pa.energy + j, w[0] + w[1]);
-                        if (pa.lj_energy) atomicAdd(pa.lj_energy + j, w[0]);
-                        if (pa.direct) atomicAdd(pa.direct + j, w[1]);
-                        if (pa.virial)
-                            for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)j + q, w[2 + q]);
-                    }
+                    for (int q = 0; q < 8; q++) own[q] = w[q];
+                }
+                else
+                {
+                    if (pa.energy) atomicAdd(pa.energy + j, w[0] + w[1]);
+                    if (pa.lj_energy) atomicAdd(pa.lj_energy + j, w[0]);
+                    if (pa.direct) atomicAdd(pa.direct + j, w[1]);
+                    if (pa.virial)
+                        for (int q = 0; q < 6; q++) atomicAdd(pa.virial + 6 * (size_t)j + q, w[2 + q]);
                 }
             }
         }
-    }
+    } while (false);
     if (FORCE)
     {
         for (int o = 16; o > 0; o >>= 1)
@@ -342,12 +341,16 @@ __global__ void k_mask_charge(int n, const float* __restrict__ q, const unsigned
 }
 
 // Atoms whose pairs enter dH/dlambda with charge perturbation on: the
-// perturbed ones and every atom whose charge changes.
+// perturbed ones and every atom whose charge changes; flagged and listed (in
+// any order: the sums are fixed point).
 __global__ void k_dh_flags(int n, const unsigned char* __restrict__ flag, const float* __restrict__ charge_ba,
-                           unsigned char* __restrict__ out)
+                           unsigned char* __restrict__ out, int* __restrict__ list, int* __restrict__ count)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) out[i] = (flag[i] || charge_ba[i] != 0.0f) ? 1 : 0;
+    if (i >= n) return;
+    const bool on = flag[i] || charge_ba[i] != 0.0f;
+    out[i] = on ? 1 : 0;
+    if (on) list[atomicAdd(count, 1)] = i;
 }
 
 template <bool FORCE, bool EN, bool PA, bool DH, bool DHC>
@@ -358,9 +361,13 @@ int launch_soft(const SoftConst& k, const spgnb_ltmatrix3& cell, const spgnb_ltm
                 PerAtomOut pa, long long* dh, cudaStream_t s)
 {
     if (n_items <= 0) return SPGNB_OK;
-    const int grid = (n_items + kSoftWarps - 1) / kSoftWarps;
-    k_soft_pairs<FORCE, EN, PA, DH, DHC><<<grid, kSoftWarps * 32, 0, s>>>(
-        k, make_cell(cell), make_cell(rcell), n_items, list, flag, atom_local, nl->d_atom_slot, nl->d_slot_atom,
+    const int chunks = (nl->table_cap + kSoftElems - 1) / kSoftElems;
+    const long long warps = (long long)n_items * chunks;
+    const long long grid = (warps + kSoftWarps - 1) / kSoftWarps;
+    if (grid > 0x7fffffffLL) return fail(SPGNB_E_UNSUPPORTED, "soft-core kernel: %lld blocks", grid);
+    k_soft_pairs<FORCE, EN, PA, DH, DHC><<<(unsigned)grid, kSoftWarps * 32, 0, s>>>(
+        k, make_cell(cell), make_cell(rcell), warps, chunks, list, flag, atom_local, nl->d_atom_slot,
+        nl->d_slot_atom,
         nl->d_tcount, nl->d_tab, nl->d_tmask, nl->table_cap, crd, charge, charge_ba, types, AA, AB, BA, BB, acc,
         totals, pa, dh);
     SPGNB_CHECK_LAUNCH("k_soft_pairs");
@@ -434,6 +441,8 @@ struct spgnb_lj_soft
     int2* d_types = nullptr;             // per local atom
     unsigned char* d_flag = nullptr;
     unsigned char* d_dh_flag = nullptr;
+    int* d_dh_list = nullptr;            // atoms of the charge-perturbed dH/dlambda
+    int* d_dh_count = nullptr;
     float* d_masked_q = nullptr;
     int* d_list = nullptr;               // perturbed local atoms
     int n_list = 0;
@@ -617,7 +626,8 @@ int spgnb_lj_soft_get_local(spgnb_lj_soft* lj, const int* d_atom_local, int loca
     {
         const int N = lj->atom_numbers;
         if ((st = dalloc(&lj->d_types, N)) || (st = dalloc(&lj->d_flag, N)) || (st = dalloc(&lj->d_dh_flag, N)) ||
-            (st = dalloc(&lj->d_masked_q, N)) || (st = dalloc(&lj->d_list, N)))
+            (st = dalloc(&lj->d_masked_q, N)) || (st = dalloc(&lj->d_list, N)) || (st = dalloc(&lj->d_dh_list, N)) ||
+            (st = dalloc(&lj->d_dh_count, 1)))
             return st;
     }
     cudaStream_t s = stream();
@@ -728,9 +738,15 @@ int spgnb_lj_soft_partial_h_partial_lambda(spgnb_lj_soft* lj, int solvent_number
     const int n = lj->local_atoms;
     if (charge_perturbated)
     {
-        k_dh_flags<<<(n + 255) / 256, 256, 0, s>>>(n, lj->d_flag, d_charge_B_A, lj->d_dh_flag);
+        SPGNB_CUDA(cudaMemsetAsync(lj->d_dh_count, 0, sizeof(int), s));
+        k_dh_flags<<<(n + 255) / 256, 256, 0, s>>>(n, lj->d_flag, d_charge_B_A, lj->d_dh_flag, lj->d_dh_list,
+                                                   lj->d_dh_count);
         SPGNB_CHECK_LAUNCH("k_dh_flags");
-        st = launch_soft<false, false, false, true, true>(k, cell, rcell, n, nullptr, lj->d_dh_flag, lj->d_atom_local,
+        int m = 0;
+        SPGNB_CUDA(cudaMemcpyAsync(&m, lj->d_dh_count, sizeof(int), cudaMemcpyDeviceToHost, s));
+        SPGNB_CUDA(cudaStreamSynchronize(s));
+        st = launch_soft<false, false, false, true, true>(k, cell, rcell, m, lj->d_dh_list, lj->d_dh_flag,
+                                                          lj->d_atom_local,
                                                           nl, crd, d_charge, d_charge_B_A, lj->d_types, lj->d_AA,
                                                           lj->d_AB, lj->d_BA, lj->d_BB, nullptr, nullptr, pa, lj->d_dh,
                                                           s);
@@ -814,6 +830,8 @@ int spgnb_lj_soft_destroy(spgnb_lj_soft* lj)
     dfree(lj->d_types);
     dfree(lj->d_flag);
     dfree(lj->d_dh_flag);
+    dfree(lj->d_dh_list);
+    dfree(lj->d_dh_count);
     dfree(lj->d_masked_q);
     dfree(lj->d_list);
     dfree(lj->d_dh);
