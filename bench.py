@@ -512,6 +512,24 @@ def main():
     xb.synchronize()
     excluded_ms = xa.elapsed_time(xb) / 20
 
+    # the same correction fused into the pair pass (spgnb_lj_fuse_pme_excluded):
+    # a force call with it against one without, each the mean of 20 calls
+    def force_calls(n=20):
+        for _ in range(3):
+            path.force(need_energy=fe, need_virial=fe, per_atom=False)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            path.force(need_energy=fe, need_virial=fe, per_atom=False)
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / n
+
+    force_only_ms = force_calls()
+    path.lj.Fuse_PME_Excluded(s.n, path.excl_start, path.excl_list, path.excl_numbers, len(s.excl_list))
+    force_fused_ms = force_calls()
+    path.lj.Fuse_PME_Excluded(s.n, None, None, None, 0)
+
     # the full neighbour list for many-body modules (FULL_NEIGHBOR_LIST, rebuilt
     # every update in SPONGE when a module asks for it), timed on its own
     for _ in range(2):
@@ -531,6 +549,7 @@ def main():
     # ligand (main.cpp:379-385), per step the list update and the soft-core
     # force, timed on its own; and one dH/dlambda evaluation (it reads back)
     soft = _time_soft_core(s, fe, dev, stream, flush)
+    graph = _time_graph_resident(s)
 
     if dist is not None:
         t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=dev)
@@ -568,8 +587,11 @@ def main():
             "clocks": clocks,
             "gpu_launches": int(launches),
             "pme_excluded_correction_ms": excluded_ms,
+            "pme_excluded_fused": {"force_call_ms": force_only_ms, "force_call_with_correction_ms": force_fused_ms,
+                                   "extra_ms": force_fused_ms - force_only_ms},
             "full_neighbor_list_ms": min(full_ms),
             "soft_core": soft,
+            "graph_resident": graph,
             "e2e": {"value": world * s.n * K / (e2e_total * 1e-3), "unit": "atom-steps/s",
                     "h2d_bytes_per_step": s.n * 12, "d2h_bytes_per_step": s.n * 12 + (64 if fe else 0)},
         }
@@ -615,6 +637,35 @@ def _time_soft_core(s, fe, dev, stream, flush, steps=50):
     return {"ligand_atoms": int(len(p.lj.perturbed_atoms())), "lambda": f.lam, "steps": steps,
             "ms_per_step": sum(ms) / steps, "atom_steps_per_s": s.n * steps / (sum(ms) * 1e-3),
             "dhdl_ms_host": dh_ms}
+
+
+def _time_graph_resident(s, steps=400):
+    """The same box as dynamics with the whole step on the device: leap-frog +
+    SETTLE + the skin/interval list check + list update + force, replayed from
+    captured CUDA graphs (the batched engine with one system); energies every
+    100 steps.  The box is relaxed first (strongly coupled thermostat, not
+    timed)."""
+    import torch
+    from spgnb.batch import Batch
+    b = Batch([s], refresh_interval=REFRESH_INTERVAL, thermostat_tau=0.002, temperature=300.0, prune_buffer=1.0)
+    b.run(200)
+    b.check_overflow()
+    b.set_thermostat(0.1, 300.0)
+    b.run(3 * b.options.steps_per_graph)
+    st = torch.cuda.ExternalStream(b.stream_ptr)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    b.run(steps, 100)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    stats = b.stats()
+    b.close()
+    return {"steps": steps, "ms_per_step": ms / steps, "atom_steps_per_s": s.n * steps / (ms * 1e-3),
+            "ns_per_day": steps * 86.4 * DT_PS / (ms * 1e-3), "rebuilds": stats["rebuilds"],
+            "prunings": stats["prunings"], "overflow": stats["overflow"],
+            "how": "leap-frog + SETTLE + list check/update + force in captured CUDA graphs, 2 fs, "
+                   "Berendsen 300 K, energies every 100 steps"}
 
 
 def _ltm(m):

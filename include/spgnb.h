@@ -271,6 +271,20 @@ int spgnb_lj_pme_excluded_force(spgnb_lj* lj, int atom_numbers, const spgnb_vect
                                 float* d_atom_energy, spgnb_ltmatrix3* d_atom_virial);
 int spgnb_lj_pme_excluded_energy(spgnb_lj* lj, double* energy);
 
+/* The same correction fused into this module's pair pass: after this call
+ * every spgnb_lj_pme_direct_force also applies PME_Excluded_Force_With_Atom_Energy
+ * (PM_force.cpp:918-997) for these exclusions, in the pair kernel's warps
+ * (each atom walks its excluded partners on both sides after its list), so
+ * the caller drops its separate excluded-correction call.  Outputs as
+ * spgnb_lj_pme_excluded_force: forces (+=), the correction's per-atom energy
+ * (+= d_atom_energy) and per-atom virial (+= d_atom_virial) when the force
+ * call asks for per-atom outputs, its energy total (spgnb_lj_pme_excluded_energy)
+ * on energy calls.  The exclusion CSR (upper triangular, the indices of
+ * d_crd) is read once here (synchronises) and turned into a symmetric one;
+ * call again after it changes.  NULL lists switch the fused correction off. */
+int spgnb_lj_fuse_pme_excluded(spgnb_lj* lj, int atom_numbers, const int* d_excluded_list_start,
+                               const int* d_excluded_list, const int* d_excluded_numbers, int excluded_total);
+
 int spgnb_lj_destroy(spgnb_lj* lj);
 
 /* ------------------------------------------------------------ LJ_SOFT_CORE */

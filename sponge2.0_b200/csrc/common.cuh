@@ -312,6 +312,10 @@ struct spgnb_lj
     long long* d_frc_acc = nullptr;  // 4 x int64 per local atom (reference-layout path)
     long long* d_totals = nullptr;   // 8 x int64 fixed point
     long long* d_excl_total = nullptr;  // PME excluded-pair correction energy, int64 fixed point
+    int* d_xs_start = nullptr;          // symmetric exclusion CSR of the fused correction (local indices)
+    int* d_xs_num = nullptr;
+    int* d_xs_list = nullptr;
+    bool xs_on = false;
     float4* d_pos = nullptr;         // per slot (spgnb list) or per atom (atom-group path)
     int* d_pos_type = nullptr;
     int pos_cap = 0;
@@ -406,6 +410,23 @@ struct PerAtomOut
     float* virial;       // caller's LTMatrix3 array (+=), 6 floats per atom
 };
 
+// PME's excluded-pair correction fused into the pair kernel: each atom's
+// excluded partners on both sides (a symmetric CSR in local indices), walked
+// by the atom's warp after its list.  list == nullptr: off.
+struct ExclFuse
+{
+    const int* start = nullptr;
+    const int* num = nullptr;
+    const int* list = nullptr;
+    const float3* crd = nullptr;       // per local atom
+    const float* charge = nullptr;
+    const int* atom_local = nullptr;   // global index of each local atom (the energy owner rule)
+    float beta = 0.0f, beta3 = 0.0f;
+    long long* total = nullptr;        // energy total, int64 fixed point (energy modes)
+    float* energy = nullptr;           // per-atom energy (+=), per-atom mode
+    float* virial = nullptr;           // per-atom virial (+=), per-atom mode
+};
+
 // One force evaluation over an spgnb list: slot pack (with the per-system
 // prune trigger), pruning when due, and the pruned-list force kernel.
 struct ForceInputs
@@ -427,6 +448,7 @@ struct ForceInputs
     int mode = 0;                      // 0 forces, 1 + totals, 2 + per-atom outputs
     OwnerMap om{nullptr, 0, 3};
     PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
+    ExclFuse xf{};                     // one system only
 };
 int force_pipeline(const ForceInputs& in, cudaStream_t s);
 int force_kernels_init(int table_size);

@@ -537,7 +537,9 @@ __device__ __forceinline__ T reduce_scatter8(const T (&v)[8], int lane)
 #define SPGNB_PAIR_PREFETCH 2
 #endif
 constexpr int kPrefetch = SPGNB_PAIR_PREFETCH;  // list windows in flight per warp
-template <int MODE, int FIT, bool TRI>
+__device__ __forceinline__ float excl_h(float x);
+
+template <int MODE, int FIT, bool TRI, bool EXCL>
 __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0 : (MODE == 1 ? 3 : SPGNB_PAIR_MINB2))
     k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
                 int n_clusters, int slot_cap,
@@ -545,7 +547,8 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
                 const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0, const int4* __restrict__ cl_q,
                 const float4* __restrict__ pos, const int* __restrict__ ptype,
                 const float2* __restrict__ gtable, int n_types, float3* __restrict__ frc,
-                long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, const int* __restrict__ only)
+                long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, const int* __restrict__ only,
+                ExclFuse xf)
 {
     extern __shared__ float4 rows_all[];        // per warp: n_types rows {-A1, -A2, B1, B2}
     __shared__ long long red[kForceWarps][8];  // per-warp fixed-point totals (lane 0)
@@ -748,6 +751,73 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             if (k0 + kPrefetch * 32 < n) ring[kPrefetch - 1] = wl[k0 + kPrefetch * 32 + lane];
             const int j = partner(cw);
             eval_word(cw, j, pos[j], cl_q[j >> 3]);
+        }
+        if (EXCL)
+        {
+            // PME's excluded-pair correction for the two atoms (each atom's
+            // excluded partners on both sides, one pair per lane), as
+            // k_pme_excluded computes it; the force joins the lane's partial
+            // sums, the energy and per-atom outputs go to the pair's owner
+            // (lower global index)
+            const int a1 = slot_atom[s1], a2 = slot_atom[s1 + 1];
+            const int n1 = a1 >= 0 ? xf.num[a1] : 0, n2 = a2 >= 0 ? xf.num[a2] : 0;
+            float eown = 0.0f;
+            for (int k = lane; k < n1 + n2; k += 32)
+            {
+                const bool sec = k >= n1;
+                const int ia = sec ? a2 : a1;
+                const int jx = xf.list[xf.start[ia] + (sec ? k - n1 : k)];
+                const float3 ri = xf.crd[ia], rj = xf.crd[jx];
+                float ex = rj.x - ri.x, ey = rj.y - ri.y, ez = rj.z - ri.z;
+                const float tx = floorf(ex * D.rcell.a11 + ey * D.rcell.a21 + ez * D.rcell.a31 + 0.5f);
+                const float ty = floorf(ey * D.rcell.a22 + ez * D.rcell.a32 + 0.5f);
+                const float tz = floorf(ez * D.rcell.a33 + 0.5f);
+                ex -= tx * D.cell.a11 + ty * D.cell.a21 + tz * D.cell.a31;
+                ey -= ty * D.cell.a22 + tz * D.cell.a32;
+                ez -= tz * D.cell.a33;
+                const float er = sqrtf(ex * ex + ey * ey + ez * ez);
+                const float x = xf.beta * er;
+                const float qq = xf.charge[ia] * xf.charge[jx];
+                const float fa = qq * xf.beta3 * excl_h(x);
+                const float gx = fa * ex, gy = fa * ey, gz = fa * ez;
+                if (sec)
+                {
+                    fx.y += gx;
+                    fy.y += gy;
+                    fz.y += gz;
+                }
+                else
+                {
+                    fx.x += gx;
+                    fy.x += gy;
+                    fz.x += gz;
+                }
+                if (EN && xf.atom_local[ia] < xf.atom_local[jx])
+                {
+                    const float e = -qq * erff(x) / er;
+                    eown += e;
+                    if (PA)
+                    {
+                        if (xf.energy) atomicAdd(xf.energy + ia, e);
+                        if (xf.virial)
+                        {
+                            float* v = xf.virial + 6 * (size_t)ia;
+                            atomicAdd(v + 0, -gx * ex);
+                            atomicAdd(v + 1, -(gx * ey + gy * ex));
+                            atomicAdd(v + 2, -gy * ey);
+                            atomicAdd(v + 3, -(gx * ez + gz * ex));
+                            atomicAdd(v + 4, -(gy * ez + gz * ey));
+                            atomicAdd(v + 5, -gz * ez);
+                        }
+                    }
+                }
+            }
+            if (EN && n1 + n2 > 0)
+            {
+                long long qe = __double2ll_rn((double)eown * kEnergyScale);
+                for (int o = 16; o > 0; o >>= 1) qe += __shfl_xor_sync(0xffffffffu, qe, o);
+                if (lane == 0 && qe) atomicAdd((unsigned long long*)xf.total, (unsigned long long)qe);
+            }
         }
         // forces of both atoms: int64 fixed point per lane, summed over the
         // lanes by a reduce-scatter (lanes 4v..4v+3 end with value v)
@@ -1292,17 +1362,19 @@ struct FastArgs
     OwnerMap om;
     PerAtomOut pa;
     const int* only;
+    ExclFuse xf;
 };
 
-template <int M, int F, bool T>
+template <int M, int F, bool T, bool E>
 int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
 {
     const spgnb_nl* nl = x.nl;
-    const int grid = std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T>, kForceWarps * 32, smem), nl->clusters_cap));
-    k_pair_fast<M, F, T><<<grid, kForceWarps * 32, smem, s>>>(
+    const int grid =
+        std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T, E>, kForceWarps * 32, smem), nl->clusters_cap));
+    k_pair_fast<M, F, T, E><<<grid, kForceWarps * 32, smem, s>>>(
         x.p0, x.fps, nl->d_sys, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords,
         nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table, x.n_types, x.frc, x.totals, x.om, x.pa,
-        x.only);
+        x.only, x.xf);
     SPGNB_CHECK_LAUNCH("k_pair_fast");
     return SPGNB_OK;
 }
@@ -1310,7 +1382,8 @@ int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
 template <int M, int F>
 int launch_fast_t(const FastArgs& x, bool tri, size_t smem, cudaStream_t s)
 {
-    return tri ? launch_fast<M, F, true>(x, smem, s) : launch_fast<M, F, false>(x, smem, s);
+    if (x.xf.list) return tri ? launch_fast<M, F, true, true>(x, smem, s) : launch_fast<M, F, false, true>(x, smem, s);
+    return tri ? launch_fast<M, F, true, false>(x, smem, s) : launch_fast<M, F, false, false>(x, smem, s);
 }
 
 template <int M>
@@ -1366,7 +1439,7 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
     if (T <= 0 || T * T != in.table_size || T > kMaxTypes)
         return fail(SPGNB_E_UNSUPPORTED, "force: the LJ table is not square or has more than %d types", kMaxTypes);
     const FastArgs fa{in.p0, in.d_fps, nl, in.slot_pos, in.slot_type, in.table, T, in.frc,
-                      in.totals, in.om, in.pa, in.only};
+                      in.totals, in.om, in.pa, in.only, in.xf};
     const int st = launch_fast_any(fa, in.mode, in.fit, nl->triclinic, sizeof(float4) * kForceWarps * T, s);
     if (st) return st;
     if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
@@ -1538,9 +1611,96 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     {
         in.om.solvent_start = local_atom_numbers;
     }
+    if (lj->xs_on)
+    {
+        // PME's excluded-pair correction in the same pass
+        in.xf.start = lj->d_xs_start;
+        in.xf.num = lj->d_xs_num;
+        in.xf.list = lj->d_xs_list;
+        in.xf.crd = in.crd;
+        in.xf.charge = d_charge;
+        in.xf.atom_local = lj->d_atom_local;
+        in.xf.beta = pme_beta;
+        in.xf.beta3 = pme_beta * pme_beta * pme_beta;
+        in.xf.total = lj->d_excl_total;
+        if (mode == 2)
+        {
+            in.xf.energy = need_atom_energy ? d_atom_energy : nullptr;
+            in.xf.virial = need_virial ? (float*)d_atom_virial : nullptr;
+        }
+        if (mode >= 1) SPGNB_CUDA(cudaMemsetAsync(lj->d_excl_total, 0, sizeof(long long), s));
+    }
     if ((st = force_pipeline(in, s))) return st;
     lj->have_energy = need_atom_energy != 0;
     lj->have_virial = need_virial != 0;
+    return SPGNB_OK;
+}
+
+int spgnb_lj_fuse_pme_excluded(spgnb_lj* lj, int atom_numbers, const int* d_excluded_list_start,
+                               const int* d_excluded_list, const int* d_excluded_numbers, int excluded_total)
+{
+    if (!lj) return fail(SPGNB_E_ARG, "spgnb_lj_fuse_pme_excluded: NULL handle");
+    lj->xs_on = false;
+    if (atom_numbers <= 0 || !d_excluded_list_start || !d_excluded_list || !d_excluded_numbers) return SPGNB_OK;
+    if (atom_numbers > lj->atom_numbers)
+        return fail(SPGNB_E_ARG, "spgnb_lj_fuse_pme_excluded: %d atoms, the module holds %d", atom_numbers,
+                    lj->atom_numbers);
+    if (excluded_total < 0) return fail(SPGNB_E_ARG, "spgnb_lj_fuse_pme_excluded: negative list size");
+    const int n = atom_numbers;
+    std::vector<int> start(n), num(n), list(std::max(excluded_total, 1));
+    cudaStream_t s = stream();
+    SPGNB_CUDA(cudaMemcpyAsync(start.data(), d_excluded_list_start, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    SPGNB_CUDA(cudaMemcpyAsync(num.data(), d_excluded_numbers, sizeof(int) * n, cudaMemcpyDeviceToHost, s));
+    if (excluded_total > 0)
+        SPGNB_CUDA(cudaMemcpyAsync(list.data(), d_excluded_list, sizeof(int) * excluded_total, cudaMemcpyDeviceToHost,
+                                   s));
+    SPGNB_CUDA(cudaStreamSynchronize(s));
+    // both directions of every excluded pair, each atom's partners ascending
+    std::vector<int> cnt(n, 0);
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < num[i]; k++)
+        {
+            const int e = start[i] + k;
+            if (num[i] < 0 || start[i] < 0 || e >= excluded_total)
+                return fail(SPGNB_E_ARG, "spgnb_lj_fuse_pme_excluded: atom %d's list runs past the %d entries", i,
+                            excluded_total);
+            const int j = list[e];
+            if (j < 0 || j >= n || j == i)
+                return fail(SPGNB_E_ARG, "spgnb_lj_fuse_pme_excluded: atom %d excludes %d", i, j);
+            cnt[i]++;
+            cnt[j]++;
+        }
+    std::vector<int> sym_start(n), fill(n);
+    int total = 0;
+    for (int i = 0; i < n; i++)
+    {
+        sym_start[i] = total;
+        fill[i] = total;
+        total += cnt[i];
+    }
+    std::vector<int> sym(std::max(total, 1));
+    for (int i = 0; i < n; i++)
+        for (int k = 0; k < num[i]; k++)
+        {
+            const int j = list[start[i] + k];
+            sym[fill[i]++] = j;
+            sym[fill[j]++] = i;
+        }
+    for (int i = 0; i < n; i++) std::sort(sym.begin() + sym_start[i], sym.begin() + sym_start[i] + cnt[i]);
+    dfree(lj->d_xs_start);
+    dfree(lj->d_xs_num);
+    dfree(lj->d_xs_list);
+    int st;
+    if ((st = dalloc(&lj->d_xs_start, lj->atom_numbers)) || (st = dalloc(&lj->d_xs_num, lj->atom_numbers)) ||
+        (st = dalloc(&lj->d_xs_list, sym.size())))
+        return st;
+    SPGNB_CUDA(cudaMemsetAsync(lj->d_xs_num, 0, sizeof(int) * lj->atom_numbers, s));
+    SPGNB_CUDA(cudaMemsetAsync(lj->d_xs_start, 0, sizeof(int) * lj->atom_numbers, s));
+    SPGNB_CUDA(cudaMemcpyAsync(lj->d_xs_start, sym_start.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    SPGNB_CUDA(cudaMemcpyAsync(lj->d_xs_num, cnt.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    SPGNB_CUDA(cudaMemcpyAsync(lj->d_xs_list, sym.data(), sizeof(int) * sym.size(), cudaMemcpyHostToDevice, s));
+    SPGNB_CUDA(cudaStreamSynchronize(s));
+    lj->xs_on = true;
     return SPGNB_OK;
 }
 
@@ -1703,6 +1863,9 @@ int spgnb_lj_destroy(spgnb_lj* lj)
     dfree(lj->d_frc_acc);
     dfree(lj->d_totals);
     dfree(lj->d_excl_total);
+    dfree(lj->d_xs_start);
+    dfree(lj->d_xs_num);
+    dfree(lj->d_xs_list);
     dfree(lj->d_pos);
     dfree(lj->d_pos_type);
     dfree(lj->d_sdata);

@@ -24,7 +24,8 @@ EXPORTED = [
     "spgnb_lj_create", "spgnb_lj_get_local", "spgnb_lj_pme_direct_force", "spgnb_lj_pme_direct_force_atom_groups",
     "spgnb_lj_long_range_correction", "spgnb_lj_energies", "spgnb_lj_totals", "spgnb_lj_long_range_factor",
     "spgnb_lj_destroy", "spgnb_lj_atom_lj_energy", "spgnb_lj_export_vector_lj",
-    "spgnb_lj_pme_excluded_force", "spgnb_lj_pme_excluded_energy", "spgnb_nl_build_full",
+    "spgnb_lj_pme_excluded_force", "spgnb_lj_pme_excluded_energy", "spgnb_lj_fuse_pme_excluded",
+    "spgnb_nl_build_full",
     "spgnb_solvent_create", "spgnb_solvent_get_local", "spgnb_solvent_pme_direct_force", "spgnb_solvent_destroy",
     "spgnb_launch_count", "spgnb_debug_set_pair_events", "spgnb_nl_count_pairs", "spgnb_probe_fp32_fma_tflops",
     "spgnb_lj_pme_direct_force_noalloc",
@@ -165,6 +166,7 @@ def lib():
     L.spgnb_lj_export_vector_lj.argtypes = [vp, vp, vp, vp, i]
     L.spgnb_lj_pme_excluded_force.argtypes = [vp, i, vp, M, M, vp, f, vp, vp, vp, vp, i, vp, vp]
     L.spgnb_lj_pme_excluded_energy.argtypes = [vp, C.POINTER(d)]
+    L.spgnb_lj_fuse_pme_excluded.argtypes = [vp, i, vp, vp, vp, i]
     L.spgnb_solvent_create.argtypes = [vp, i, C.POINTER(vp)]
     L.spgnb_solvent_get_local.argtypes = [vp, i, vp, i, vp, C.POINTER(i)]
     L.spgnb_solvent_pme_direct_force.argtypes = [vp, i, i, vp, vp, vp, vp, M, M, vp, vp, f, i, vp, i, vp, vp]

@@ -242,6 +242,16 @@ class LENNARD_JONES_INFORMATION:
                                                 _ptr(excluded_numbers), _ptr(frc), int(need_energy),
                                                 _ptr(atom_energy), _ptr(atom_virial)))
 
+    def Fuse_PME_Excluded(self, atom_numbers, excluded_list_start, excluded_list, excluded_numbers,
+                          excluded_total):
+        """Applies the PME excluded-pair correction inside every later
+        LJ_PME_Direct_Force_With_Atom_Energy_And_Virial call over an spgnb list
+        (the separate PME_Excluded_Force_With_Atom_Energy call is then left
+        out).  None lists switch it off."""
+        _bind_stream()
+        check(lib().spgnb_lj_fuse_pme_excluded(self.handle, int(atom_numbers), _ptr(excluded_list_start),
+                                               _ptr(excluded_list), _ptr(excluded_numbers), int(excluded_total)))
+
     def excluded_energy(self):
         """FP64 total of the last excluded-pair correction."""
         _bind_stream()

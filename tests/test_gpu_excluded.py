@@ -50,3 +50,45 @@ def test_pme_excluded_correction_vs_fp64(torch_cuda, name):
     assert np.abs(ene - ref["e_atom"]).max() <= 1e-5 * e_scale
     v_scale = np.abs(ref["virial_atom"]).max()
     assert np.abs(vir - ref["virial_atom"]).max() <= 1e-5 * v_scale
+
+
+@pytest.mark.parametrize("name", ["mixed-small", "triclinic"])
+def test_fused_excluded_correction(torch_cuda, oracle, name):
+    """The correction fused into the pair pass (spgnb_lj_fuse_pme_excluded)
+    gives what the pair call followed by the separate correction call gives:
+    forces, per-atom energy and virial, the totals and the correction's own
+    energy; against FP64 it is the direct pair sum minus the excluded pairs'
+    erf part; switched off, the pair call is back to its own forces bit for bit."""
+    import oracle as O
+    from spgnb.engine import PlainPath
+    torch = torch_cuda
+    s = _systems()[name]
+    p = PlainPath(s, device="cuda:0")
+    frc_plain = p.force(need_energy=True, need_virial=True).clone()
+    p.lj.PME_Excluded_Force_With_Atom_Energy(s.n, p.crd, s.cell, s.rcell, p.charge, s.beta, p.excl_start,
+                                             p.excl_list, p.excl_numbers, p.frc, 1, p.atom_energy, p.atom_virial)
+    torch.cuda.synchronize()
+    sep = (p.frc.cpu().numpy(), p.atom_energy.cpu().numpy(), p.atom_virial.cpu().numpy(), p.lj.totals(),
+           p.lj.excluded_energy())
+    p.lj.Fuse_PME_Excluded(s.n, p.excl_start, p.excl_list, p.excl_numbers, len(s.excl_list))
+    p.force(need_energy=True, need_virial=True)
+    torch.cuda.synchronize()
+    fused = (p.frc.cpu().numpy(), p.atom_energy.cpu().numpy(), p.atom_virial.cpu().numpy(), p.lj.totals(),
+             p.lj.excluded_energy())
+    assert rel_rms(fused[0], sep[0]) <= 1e-6
+    assert np.abs(fused[1] - sep[1]).max() <= 1e-5 * np.abs(sep[1]).max()
+    assert np.abs(fused[2] - sep[2]).max() <= 1e-5 * np.abs(sep[2]).max()
+    assert np.abs(fused[3] - sep[3]).max() <= 1e-6 * np.abs(sep[3]).max()
+    assert abs(fused[4] - sep[4]) <= 1e-6 * abs(sep[4]) + 1e-3
+    ref = oracle.direct_sum(s)
+    ex = O.Oracle.pme_excluded(s)
+    assert rel_rms(fused[0], ref["frc"] + ex["frc"]) <= FORCE_REL_RMS_TOL
+    assert abs(fused[4] - ex["energy"]) <= ENERGY_REL_TOL * abs(ex["energy"]) + 1e-3
+    # force only: the same forces
+    p.force()
+    torch.cuda.synchronize()
+    assert rel_rms(p.frc.cpu().numpy(), fused[0]) <= 1e-6
+    # off again
+    p.lj.Fuse_PME_Excluded(s.n, None, None, None, 0)
+    p.force(need_energy=True, need_virial=True)
+    assert np.array_equal(p.frc.cpu().numpy(), frc_plain.cpu().numpy())
