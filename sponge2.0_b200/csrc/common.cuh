@@ -271,6 +271,7 @@ struct spgnb_nl
     // per slot
     int* d_slot_atom = nullptr;
     float4* d_slot_x0 = nullptr;  // raw coordinates at the build, w = global index
+    int* d_slot_gid = nullptr;    // the same global index, compact (-1: empty slot)
     float4* d_slot_d0 = nullptr;  // offset from the cluster centre at the build
     int2* d_slot_ex = nullptr;    // first and last entry of the atom's exclusion list
     int* d_slot_count = nullptr;  // full-list length of each slot

@@ -251,7 +251,7 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, int* __restrict_
                                 const int* __restrict__ atom_shift, const int* __restrict__ atom_local,
                                 const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys, int* counters,
                                 uint4* __restrict__ cl_u, int4* __restrict__ cl_q, float4* __restrict__ cl_c,
-                                float4* __restrict__ slot_x0, float4* __restrict__ slot_d0,
+                                float4* __restrict__ slot_x0, int* __restrict__ slot_gid, float4* __restrict__ slot_d0,
                                 int2* __restrict__ slot_ex, const int* __restrict__ ex_start,
                                 const int* __restrict__ ex_list, const int* __restrict__ ex_num, int clusters_cap,
                                 const int* __restrict__ need, const int* __restrict__ ncl, int* __restrict__ tcount,
@@ -334,6 +334,7 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, int* __restrict_
         slot_d0[s] = make_float4((float)d0, (float)d1, (float)d2, 0.0f);
         const int g = atom_local[a];
         slot_x0[s] = make_float4(x.x, x.y, x.z, __int_as_float(g));
+        slot_gid[s] = g;
         // [first, last] of the atom's (sorted) exclusion list, empty when none
         const int k = ex_num[g];
         slot_ex[s] = k > 0 ? make_int2(ex_list[ex_start[g]], ex_list[ex_start[g] + k - 1]) : make_int2(0x7fffffff, -1);
@@ -343,6 +344,7 @@ __global__ void k_cluster_props(const float3* __restrict__ crd, int* __restrict_
         const float p = kPadCoordinate + (float)s;
         slot_d0[s] = make_float4(p, p, p, 0.0f);
         slot_x0[s] = make_float4(0.0f, 0.0f, 0.0f, __int_as_float(-1));
+        slot_gid[s] = -1;
         slot_ex[s] = make_int2(0x7fffffff, -1);
     }
     for (int o = 1; o < 8; o <<= 1) r2 = fmax(r2, __shfl_xor_sync(0xffffffffu, r2, o));
@@ -623,12 +625,17 @@ template <bool HALF>
 __global__ void k_export_lists(int clusters_cap, int table_cap, const int* __restrict__ tcount,
                                const float4* __restrict__ tab, const uint2* __restrict__ tmask,
                                const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0,
-                               const float3* __restrict__ crd, Cell cell, Cell rcell, float cut2,
+                               const int* __restrict__ slot_gid, const float3* __restrict__ crd, Cell cell,
+                               Cell rcell, float cut2,
                                spgnb_atom_group* __restrict__ full, int max_nb, int* __restrict__ overflow,
                                int ovf_bits, const int* __restrict__ need)
 {
     if (HALF && *need == 0) return;
+    // a chunk's kept partners, compacted here so that the list is written
+    // with contiguous stores (blocks of 128 threads)
+    __shared__ int staged[4][32 * kClusterSize];
     const int lane = threadIdx.x & 31;
+    int* const stage = staged[threadIdx.x >> 5];
     const int warps = gridDim.x * (blockDim.x >> 5);
     // one warp per own slot (cluster c, atom a): its list in table order
     for (int item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < clusters_cap * kClusterSize;
@@ -647,23 +654,34 @@ __global__ void k_export_lists(int clusters_cap, int table_cap, const int* __res
             const int t = t0 + lane;
             unsigned row = 0;
             int base = 0;
+            // the neighbour cluster's eight atoms (and global indices), in two
+            // 16-byte loads each: a cluster's slots start on an 8-slot boundary
+            int4 na0 = make_int4(-1, -1, -1, -1), na1 = na0;
             if (t < T)
             {
                 const uint2 mm = tmask[(size_t)c * table_cap + t];
                 row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
                 base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
-            }
-            unsigned keep = row;
-            if (HALF)
-            {
-                keep = 0;
-                for (unsigned r = row; r; r &= r - 1)
+                if (row)
                 {
-                    const int b = __ffs(r) - 1;
-                    if (gia < __float_as_int(slot_x0[base + b].w)) keep |= 1u << b;
+                    const int4* sa = reinterpret_cast<const int4*>(slot_atom + base);
+                    na0 = sa[0];
+                    na1 = sa[1];
                 }
             }
-            else if (cut2 >= 0.0f && row)
+            const int nb[kClusterSize] = {na0.x, na0.y, na0.z, na0.w, na1.x, na1.y, na1.z, na1.w};
+            unsigned keep = row;
+            if (HALF && row)
+            {
+                const int4* sg = reinterpret_cast<const int4*>(slot_gid + base);
+                const int4 g0 = sg[0], g1 = sg[1];
+                const int gb[kClusterSize] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
+                unsigned above = 0;
+#pragma unroll
+                for (int b = 0; b < kClusterSize; b++) above |= (gia < gb[b] ? 1u : 0u) << b;
+                keep = row & above;
+            }
+            else if (!HALF && cut2 >= 0.0f && row)
             {
                 keep = 0;
                 for (unsigned r = row; r; r &= r - 1)
@@ -683,16 +701,21 @@ __global__ void k_export_lists(int clusters_cap, int table_cap, const int* __res
                 const int y = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += y;
             }
-            int pos = count + incl - k;
-            for (unsigned r = keep; r; r &= r - 1, pos++)
+            int pos = incl - k;
+#pragma unroll
+            for (int b = 0; b < kClusterSize; b++)
+                if ((keep >> b) & 1u) stage[pos++] = nb[b];
+            __syncwarp();
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            for (int q = lane; q < total; q += 32)
             {
-                const int b = __ffs(r) - 1;
-                if (pos < max_nb)
-                    list[pos] = slot_atom[base + b];
+                if (count + q < max_nb)
+                    list[count + q] = stage[q];
                 else
                     atomicOr(overflow, ovf_bits);
             }
-            count += __shfl_sync(0xffffffffu, incl, 31);
+            __syncwarp();
+            count += total;
         }
         if (lane == 0)
         {
@@ -927,6 +950,7 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_atom_slot);
     dfree(nl->d_slot_atom);
     dfree(nl->d_slot_x0);
+    dfree(nl->d_slot_gid);
     dfree(nl->d_slot_d0);
     dfree(nl->d_slot_ex);
     dfree(nl->d_slot_count);
@@ -1060,6 +1084,8 @@ int alloc_nl(spgnb_nl* nl)
     if ((st = dalloc(&nl->d_slot_atom, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_slot_atom, 0xff, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_slot_x0, slots))) return st;
+    if ((st = dalloc(&nl->d_slot_gid, slots))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_slot_gid, 0xff, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_slot_d0, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_slot_d0, 0, sizeof(float4) * slots));
     if ((st = dalloc(&nl->d_slot_ex, slots))) return st;
@@ -1446,8 +1472,8 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     SPGNB_CHECK_LAUNCH("k_sort_cells");
     k_cluster_props<<<(slots_cap + 255) / 256, 256, 0, s>>>(
         d_crd, nl->d_slot_atom, nl->d_atom_shift, d_atom_local, nl->d_cl_sys, nl->d_sys, nl->d_counters, nl->d_cl_u,
-        nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex, ex_start, ex_list, ex_num, ccap,
-        nl->d_need, nl->d_ncl, nl->d_tcount, nl->d_slot_count, nl->d_pcount);
+        nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_gid, nl->d_slot_d0, nl->d_slot_ex, ex_start, ex_list, ex_num,
+        ccap, nl->d_need, nl->d_ncl, nl->d_tcount, nl->d_slot_count, nl->d_pcount);
     SPGNB_CHECK_LAUNCH("k_cluster_props");
     const int search_blocks = std::max(1, std::min((ccap + kSearchWarps - 1) / kSearchWarps, sms * 8));
     k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
@@ -1460,7 +1486,8 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
         k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_export_zero");
         k_export_lists<true><<<std::max(1, std::min((ccap * kClusterSize + 3) / 4, sms * 16)), 128, 0, s>>>(
-            ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nullptr,
+            ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_gid,
+            nullptr,
             Cell{}, Cell{}, -1.0f, nl->d_nl, nl->opt.max_neighbor_numbers, nl->d_counters + kCntOverflow, kOvfList,
             nl->d_counters + kCntNeed);
         SPGNB_CHECK_LAUNCH("k_export_lists");
@@ -1726,7 +1753,7 @@ int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector
     SPGNB_CHECK_LAUNCH("k_zero_groups");
     const int ccap = nl->clusters_cap;
     k_export_lists<false><<<std::max(1, std::min((ccap * kClusterSize + 3) / 4, num_sms() * 16)), 128, 0, s>>>(
-        ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0,
+        ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_gid,
         (const float3*)d_crd, make_cell(cell), make_cell(rcell), cutoff > 0.0f ? cutoff * cutoff : -1.0f, d_full_nl,
         max_neighbor_numbers, d_overflow, 1, nullptr);
     SPGNB_CHECK_LAUNCH("k_export_lists");
