@@ -644,13 +644,14 @@ def _time_graph_resident(s, steps=400):
     SETTLE + the skin/interval list check + list update + force, replayed from
     captured CUDA graphs (the batched engine with one system); energies every
     100 steps.  The box is relaxed first (strongly coupled thermostat, not
-    timed)."""
+    timed) and the prune buffer autotuned as in the batched workload."""
     import torch
     from spgnb.batch import Batch
-    b = Batch([s], refresh_interval=REFRESH_INTERVAL, thermostat_tau=0.002, temperature=300.0, prune_buffer=1.0)
+    b = Batch([s], refresh_interval=REFRESH_INTERVAL, thermostat_tau=0.002, temperature=300.0, prune_buffer=1.6)
     b.run(200)
     b.check_overflow()
     b.set_thermostat(0.1, 300.0)
+    tuned = b.autotune(10)
     b.run(3 * b.options.steps_per_graph)
     st = torch.cuda.ExternalStream(b.stream_ptr)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -663,7 +664,7 @@ def _time_graph_resident(s, steps=400):
     b.close()
     return {"steps": steps, "ms_per_step": ms / steps, "atom_steps_per_s": s.n * steps / (ms * 1e-3),
             "ns_per_day": steps * 86.4 * DT_PS / (ms * 1e-3), "rebuilds": stats["rebuilds"],
-            "prunings": stats["prunings"], "overflow": stats["overflow"],
+            "prunings": stats["prunings"], "overflow": stats["overflow"], "prune_buffer_autotuned": tuned,
             "how": "leap-frog + SETTLE + list check/update + force in captured CUDA graphs, 2 fs, "
                    "Berendsen 300 K, energies every 100 steps"}
 

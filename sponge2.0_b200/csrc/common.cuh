@@ -313,9 +313,8 @@ struct spgnb_lj
     long long* d_frc_acc = nullptr;  // 4 x int64 per local atom (reference-layout path)
     long long* d_totals = nullptr;   // 8 x int64 fixed point
     long long* d_excl_total = nullptr;  // PME excluded-pair correction energy, int64 fixed point
-    int* d_xs_start = nullptr;          // symmetric exclusion CSR of the fused correction (local indices)
-    int* d_xs_num = nullptr;
-    int* d_xs_list = nullptr;
+    int2* d_xs_sn = nullptr;            // symmetric exclusion CSR of the fused correction (local indices):
+    int* d_xs_list = nullptr;           //   {first entry, count} per atom, the partners
     bool xs_on = false;
     float4* d_pos = nullptr;         // per slot (spgnb list) or per atom (atom-group path)
     int* d_pos_type = nullptr;
@@ -416,8 +415,7 @@ struct PerAtomOut
 // by the atom's warp after its list.  list == nullptr: off.
 struct ExclFuse
 {
-    const int* start = nullptr;
-    const int* num = nullptr;
+    const int2* sn = nullptr;          // per local atom {first entry, count}
     const int* list = nullptr;
     const float3* crd = nullptr;       // per local atom
     const float* charge = nullptr;

@@ -760,13 +760,14 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             // sums, the energy and per-atom outputs go to the pair's owner
             // (lower global index)
             const int a1 = slot_atom[s1], a2 = slot_atom[s1 + 1];
-            const int n1 = a1 >= 0 ? xf.num[a1] : 0, n2 = a2 >= 0 ? xf.num[a2] : 0;
+            const int2 sn1 = a1 >= 0 ? xf.sn[a1] : make_int2(0, 0), sn2 = a2 >= 0 ? xf.sn[a2] : make_int2(0, 0);
+            const int n1 = sn1.y, n2 = sn2.y;
             float eown = 0.0f;
             for (int k = lane; k < n1 + n2; k += 32)
             {
                 const bool sec = k >= n1;
                 const int ia = sec ? a2 : a1;
-                const int jx = xf.list[xf.start[ia] + (sec ? k - n1 : k)];
+                const int jx = xf.list[sec ? sn2.x + k - n1 : sn1.x + k];
                 const float3 ri = xf.crd[ia], rj = xf.crd[jx];
                 float ex = rj.x - ri.x, ey = rj.y - ri.y, ez = rj.z - ri.z;
                 const float tx = floorf(ex * D.rcell.a11 + ey * D.rcell.a21 + ez * D.rcell.a31 + 0.5f);
@@ -1614,8 +1615,7 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     if (lj->xs_on)
     {
         // PME's excluded-pair correction in the same pass
-        in.xf.start = lj->d_xs_start;
-        in.xf.num = lj->d_xs_num;
+        in.xf.sn = lj->d_xs_sn;
         in.xf.list = lj->d_xs_list;
         in.xf.crd = in.crd;
         in.xf.charge = d_charge;
@@ -1687,17 +1687,13 @@ int spgnb_lj_fuse_pme_excluded(spgnb_lj* lj, int atom_numbers, const int* d_excl
             sym[fill[j]++] = i;
         }
     for (int i = 0; i < n; i++) std::sort(sym.begin() + sym_start[i], sym.begin() + sym_start[i] + cnt[i]);
-    dfree(lj->d_xs_start);
-    dfree(lj->d_xs_num);
+    dfree(lj->d_xs_sn);
     dfree(lj->d_xs_list);
     int st;
-    if ((st = dalloc(&lj->d_xs_start, lj->atom_numbers)) || (st = dalloc(&lj->d_xs_num, lj->atom_numbers)) ||
-        (st = dalloc(&lj->d_xs_list, sym.size())))
-        return st;
-    SPGNB_CUDA(cudaMemsetAsync(lj->d_xs_num, 0, sizeof(int) * lj->atom_numbers, s));
-    SPGNB_CUDA(cudaMemsetAsync(lj->d_xs_start, 0, sizeof(int) * lj->atom_numbers, s));
-    SPGNB_CUDA(cudaMemcpyAsync(lj->d_xs_start, sym_start.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
-    SPGNB_CUDA(cudaMemcpyAsync(lj->d_xs_num, cnt.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s));
+    if ((st = dalloc(&lj->d_xs_sn, lj->atom_numbers)) || (st = dalloc(&lj->d_xs_list, sym.size()))) return st;
+    std::vector<int2> sn(lj->atom_numbers, make_int2(0, 0));
+    for (int i = 0; i < n; i++) sn[i] = make_int2(sym_start[i], cnt[i]);
+    SPGNB_CUDA(cudaMemcpyAsync(lj->d_xs_sn, sn.data(), sizeof(int2) * sn.size(), cudaMemcpyHostToDevice, s));
     SPGNB_CUDA(cudaMemcpyAsync(lj->d_xs_list, sym.data(), sizeof(int) * sym.size(), cudaMemcpyHostToDevice, s));
     SPGNB_CUDA(cudaStreamSynchronize(s));
     lj->xs_on = true;
@@ -1863,8 +1859,7 @@ int spgnb_lj_destroy(spgnb_lj* lj)
     dfree(lj->d_frc_acc);
     dfree(lj->d_totals);
     dfree(lj->d_excl_total);
-    dfree(lj->d_xs_start);
-    dfree(lj->d_xs_num);
+    dfree(lj->d_xs_sn);
     dfree(lj->d_xs_list);
     dfree(lj->d_pos);
     dfree(lj->d_pos_type);

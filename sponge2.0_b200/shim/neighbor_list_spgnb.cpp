@@ -101,6 +101,13 @@ void NEIGHBOR_LIST::Initial(CONTROLLER* controller, int atom_numbers, float cuto
     }
     o.skin_permit = updator.skin_permit;
     o.export_atom_groups = 1;
+    // spgnb's own key: the margin of the pruned list the force kernel walks
+    // (re-pruned when an atom has moved half of it); 0 turns pruning off
+    if (controller->Command_Exist("neighbor_list", "prune_buffer"))
+    {
+        controller->Check_Float("neighbor_list", "prune_buffer", "NEIGHBOR_LIST::Initial");
+        o.prune_buffer = atof(controller->Command("neighbor_list", "prune_buffer"));
+    }
     controller->printf("    Max number of neighbors for one atom: %d\n", max_neighbor_numbers);
     controller->printf("    The interval to refresh the neighbor list: %d\n", o.refresh_interval);
     spgnb_nl* h = nullptr;

@@ -78,6 +78,7 @@ class NEIGHBOR_LIST:
                                                              False))
         opt.export_atom_groups = int(bool(export_atom_groups))
         opt.max_entries_per_cluster = _controller_int(controller, "neighbor_list_max_entries_per_cluster", 0)
+        opt.prune_buffer = _controller_float(controller, "neighbor_list_prune_buffer", opt.prune_buffer)
         self.atom_numbers = int(atom_numbers)
         self.cutoff = float(cutoff)
         self.skin = float(skin)
