@@ -140,10 +140,11 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
 // its last one (the pack kernel checks).  The lists belong to slot pairs: the
 // two atoms of slots 2p and 2p+1 of a cluster share one list, the union of
 // their partners within cutoff + buffer, so the force kernel evaluates both
-// atoms against each partner it loads.  One warp per slot pair walks the
-// cluster's neighbour table, expands the two atoms' mask rows 32 elements at
-// a time into shared memory and keeps, in table order, every partner within
-// cutoff + buffer of either atom, as a 32-bit word
+// atoms against each partner it loads.  One warp per cluster walks its
+// neighbour table, expands the union of the eight atoms' mask rows 32
+// elements at a time into shared memory, loads each candidate partner once
+// and keeps, for each of the four slot pairs in table order, every partner
+// within cutoff + buffer of either of the pair's atoms, as a 32-bit word
 //   {partner slot - system's first slot (22 bits) | LJ type << 22 |
 //    pairs with the first atom << 29 | with the second << 30 | image flag << 31}
 // (an atom's bit is clear for itself, its exclusions and other
@@ -185,23 +186,30 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
             int* __restrict__ pcount, unsigned* __restrict__ pwords, int n_sys, int* __restrict__ prune)
 {
     if (counters[kCntPrune] == 0) return;
-    __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];  // {partner slot | image flag, element | atom bits}
+    // a chunk's candidates {partner slot | image flag, element lane | own-atom bits << 5}
+    __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];
+    __shared__ float4 own_all[kPruneWarps][kClusterSize];
     __shared__ unsigned long long kept_total;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
-    const int items = clusters_cap * 4;
     if (threadIdx.x == 0) kept_total = 0;
     __syncthreads();
     uint2* __restrict__ mybuf = buf[w];
-    for (int it = blockIdx.x * kPruneWarps + w; it < items; it += gridDim.x * kPruneWarps)
+    float4* __restrict__ own = own_all[w];
+    // one warp per cluster: each candidate partner is loaded once and tested
+    // against the cluster's eight atoms, feeding the four slot pairs' lists
+    for (int c = blockIdx.x * kPruneWarps + w; c < clusters_cap; c += gridDim.x * kPruneWarps)
     {
-        const int c = it >> 2, p = it & 3;
         const int sy = cl_sys[c];
         if (!prune[sy]) continue;
-        const int s1 = c * kClusterSize + 2 * p;
-        const float4 pi1 = pos[s1], pi2 = pos[s1 + 1];
-        if (lane == 0) pref[s1] = pi1;
-        if (lane == 1) pref[s1 + 1] = pi2;
+        const int s0 = c * kClusterSize;
+        if (lane < kClusterSize)
+        {
+            const float4 pl = pos[s0 + lane];
+            own[lane] = pl;
+            pref[s0 + lane] = pl;
+        }
+        __syncwarp();
         const SysDesc& D = sys[sy];
         const unsigned slot0 = (unsigned)D.cl_begin * kClusterSize;
         const ForceParams P = fps ? fps[sy] : p0;
@@ -210,24 +218,23 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
         const int T = tcount[c];
         const float4* __restrict__ tb = tab + (size_t)c * table_cap;
         const uint2* __restrict__ tm = tmask + (size_t)c * table_cap;
-        unsigned* __restrict__ out_words = pwords + (size_t)s1 * slot_cap;
         const int usable = 2 * slot_cap - kWindow;
-        const int sh1 = 8 * ((2 * p) & 3), sh2 = 8 * ((2 * p + 1) & 3);
-        int kept = 0;
+        int kept[4] = {0, 0, 0, 0};
         for (int t0 = 0; t0 < T; t0 += 32)
         {
             const int t = t0 + lane;
-            unsigned r1 = 0, r2 = 0;
+            uint2 mm = make_uint2(0u, 0u);
             float4 e = make_float4(0, 0, 0, 0);
             if (t < T)
             {
                 e = tb[t];
-                const uint2 mm = tm[t];
-                const unsigned half = p < 2 ? mm.x : mm.y;
-                r1 = (half >> sh1) & 0xffu;
-                r2 = (half >> sh2) & 0xffu;
+                mm = tm[t];
             }
-            const unsigned row = r1 | r2;
+            // partners of any of the eight atoms
+            unsigned u = mm.x | mm.y;
+            u |= u >> 16;
+            u |= u >> 8;
+            const unsigned row = u & 0xffu;
             const int cnt = __popc(row);
             int incl = cnt;
             for (int o = 1; o < 32; o <<= 1)
@@ -243,7 +250,13 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
 #pragma unroll
             for (int b = 0; b < kClusterSize; b++)
                 if ((row >> b) & 1u)
-                    mybuf[k++] = make_uint2(base + b, (unsigned)lane | (((r1 >> b) & 1u) << 5) | (((r2 >> b) & 1u) << 6));
+                {
+                    // own atom a pairs with neighbour slot b when bit 8a + b is set
+                    const unsigned x = (mm.x >> b) & 0x01010101u, y = (mm.y >> b) & 0x01010101u;
+                    const unsigned am = ((x | (x >> 7) | (x >> 14) | (x >> 21)) & 0xfu) |
+                                        (((y | (y >> 7) | (y >> 14) | (y >> 21)) & 0xfu) << 4);
+                    mybuf[k++] = make_uint2(base + b, (unsigned)lane | (am << 5));
+                }
             __syncwarp();
             for (int q0 = 0; q0 < total; q0 += 32)
             {
@@ -254,46 +267,66 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
                 const float ex = __shfl_sync(0xffffffffu, e.x, src);
                 const float ey = __shfl_sync(0xffffffffu, e.y, src);
                 const float ez = __shfl_sync(0xffffffffu, e.z, src);
-                bool keep = false;
-                unsigned out = 0;
-                if (q < total)
+                const unsigned am = q < total ? (wv.y >> 5) & 0xffu : 0u;
+                const int js = (int)(wv.x & 0x7fffffffu);
+                const bool img = (wv.x & 0x80000000u) != 0;
+                float4 pj = make_float4(0, 0, 0, 0);
+                int tj = 0;
+                if (am)
                 {
-                    const int js = (int)(wv.x & 0x7fffffffu);
-                    const bool img = (wv.x & 0x80000000u) != 0;
-                    const float4 pj = pos[js];
-                    const int tj = ptype[js];
-                    const bool m1 = (wv.y >> 5) & 1u, m2 = (wv.y >> 6) & 1u;
-                    const float3 d1 = pair_offset(ex, ey, ez, pi1, pj, img, D);
-                    const float3 d2 = pair_offset(ex, ey, ez, pi2, pj, img, D);
-                    const float q1 = __fmaf_rn(d1.z, d1.z, __fmaf_rn(d1.y, d1.y, d1.x * d1.x));
-                    const float q2 = __fmaf_rn(d2.z, d2.z, __fmaf_rn(d2.y, d2.y, d2.x * d2.x));
-                    keep = (m1 && q1 < rp2) || (m2 && q2 < rp2);
-                    out = ((unsigned)js - slot0) | ((unsigned)tj << kWordTypeShift) | (m1 ? kWordFirst : 0u) |
-                          (m2 ? kWordSecond : 0u) | (img ? kWordImage : 0u);
+                    pj = pos[js];
+                    tj = ptype[js];
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, keep);
-                if (keep)
+                const unsigned wbase =
+                    ((unsigned)js - slot0) | ((unsigned)tj << kWordTypeShift) | (img ? kWordImage : 0u);
+#pragma unroll
+                for (int p = 0; p < 4; p++)
                 {
-                    const int kk = kept + __popc(m & ((1u << lane) - 1u));
-                    if (kk < usable)
-                        out_words[kk] = out;
-                    else
-                        atomicOr(&counters[kCntOverflow], kOvfWords);
+                    const bool m1 = (am >> (2 * p)) & 1u, m2 = (am >> (2 * p + 1)) & 1u;
+                    bool keep = false;
+                    if (m1)
+                    {
+                        const float3 d1 = pair_offset(ex, ey, ez, own[2 * p], pj, img, D);
+                        keep = __fmaf_rn(d1.z, d1.z, __fmaf_rn(d1.y, d1.y, d1.x * d1.x)) < rp2;
+                    }
+                    if (m2 && !keep)
+                    {
+                        const float3 d2 = pair_offset(ex, ey, ez, own[2 * p + 1], pj, img, D);
+                        keep = __fmaf_rn(d2.z, d2.z, __fmaf_rn(d2.y, d2.y, d2.x * d2.x)) < rp2;
+                    }
+                    const unsigned m = __ballot_sync(0xffffffffu, keep);
+                    if (keep)
+                    {
+                        const int kk = kept[p] + __popc(m & ((1u << lane) - 1u));
+                        if (kk < usable)
+                            pwords[(size_t)(s0 + 2 * p) * slot_cap + kk] =
+                                wbase | (m1 ? kWordFirst : 0u) | (m2 ? kWordSecond : 0u);
+                        else
+                            atomicOr(&counters[kCntOverflow], kOvfWords);
+                    }
+                    kept[p] += __popc(m);
                 }
-                kept += __popc(m);
             }
             __syncwarp();
         }
         // pad to whole windows: the first atom against itself, no atom bit set
-        kept = min(kept, usable);
-        const int padded = (kept + kWindow - 1) & ~(kWindow - 1);
-        for (int k = kept + lane; k < padded; k += 32) out_words[k] = (unsigned)s1 - slot0;
-        if (lane == 0)
+        unsigned long long kept_sum = 0;
+#pragma unroll
+        for (int p = 0; p < 4; p++)
         {
-            pcount[s1] = padded;
-            pcount[s1 + 1] = 0;
-            atomicAdd(&kept_total, (unsigned long long)kept);
+            const int s1 = s0 + 2 * p;
+            const int kp = min(kept[p], usable);
+            const int padded = (kp + kWindow - 1) & ~(kWindow - 1);
+            for (int k2 = kp + lane; k2 < padded; k2 += 32) pwords[(size_t)s1 * slot_cap + k2] = (unsigned)s1 - slot0;
+            if (lane == 0)
+            {
+                pcount[s1] = padded;
+                pcount[s1 + 1] = 0;
+            }
+            kept_sum += (unsigned long long)kp;
         }
+        if (lane == 0) atomicAdd(&kept_total, kept_sum);
+        __syncwarp();
     }
     __shared__ int is_last;
     __syncthreads();
