@@ -8,7 +8,13 @@ shim = SPONGE's module classes built with the drop-in shim over libspgnb
 (oracle/_ref/libspgref_cuda.so).  The 96,000-atom mixed box, rebuild every 20
 steps, energy and virial with per-atom arrays every step; plain = list update
 + LJ + solvent modules, soft = list update + LJ_SOFT_CORE (40-atom perturbed
-ligand) + solvent module.  Prints the wall-clock ms per step of the loop."""
+ligand) + solvent module.  Prints the wall-clock ms per step of the loop.
+
+    python tests/speed_loops.py graph [steps]
+
+runs the same box as dynamics through the batched engine with one system
+(leap-frog + SETTLE + list check/update + force replayed from CUDA graphs,
+prune margin autotuned), the timed steps inside the NVTX range "timed"."""
 import json
 import os
 import sys
@@ -23,6 +29,9 @@ def main():
     from spgnb import systems as S
     which = sys.argv[1]
     steps = int(sys.argv[2]) if len(sys.argv) > 2 else 30
+    if which == "graph":
+        graph_loop(steps)
+        return
     lib, path = which.split("_")
     s = S.mixed_box_96k()
     ref = O.Reference(gpu=lib == "ref", shim=lib == "shim")
@@ -40,6 +49,32 @@ def main():
         t = ref.time_steps(steps, first_step=10, need_energy=True, need_virial=True)
     ref.clear()
     print(json.dumps({"loop": which, "steps": steps, "ms_per_step": t * 1e3 / steps}))
+
+
+def graph_loop(steps):
+    import time
+    import torch
+    from spgnb import systems as S
+    from spgnb.batch import Batch
+    s = S.mixed_box_96k()
+    b = Batch([s], refresh_interval=20, thermostat_tau=0.002, temperature=300.0, prune_buffer=1.6)
+    b.run(200)
+    b.check_overflow()
+    b.set_thermostat(0.1, 300.0)
+    tuned = b.autotune(10)
+    b.run(3 * b.options.steps_per_graph)
+    torch.cuda.synchronize()
+    st0 = b.stats()
+    torch.cuda.nvtx.range_push("timed")
+    t0 = time.perf_counter()
+    b.run(steps, 100)
+    torch.cuda.synchronize()
+    t = time.perf_counter() - t0
+    torch.cuda.nvtx.range_pop()
+    st1 = b.stats()
+    b.close()
+    print(json.dumps({"loop": "graph", "steps": steps, "ms_per_step": t * 1e3 / steps, "prune_buffer": tuned,
+                      "rebuilds": st1["rebuilds"] - st0["rebuilds"], "prunings": st1["prunings"] - st0["prunings"]}))
 
 
 if __name__ == "__main__":
