@@ -1,12 +1,13 @@
 """The C++ harness loops of tests/test_gpu_speed_vs_reference.py as a script,
 for timing one of them alone or under a profiler's launch list:
 
-    python tests/speed_loops.py {shim|ref}_{plain|soft} [steps]
+    python tests/speed_loops.py {shim|ref}_{plain|soft} [steps] [f]
 
 shim = SPONGE's module classes built with the drop-in shim over libspgnb
 (oracle/_ref/libspgref_shim.so); ref = built from the reference's sources
 (oracle/_ref/libspgref_cuda.so).  The 96,000-atom mixed box, rebuild every 20
-steps, energy and virial with per-atom arrays every step; plain = list update
+steps, energy and virial with per-atom arrays every step (forces only with a
+trailing "f"); plain = list update
 + LJ + solvent modules, soft = list update + LJ_SOFT_CORE (40-atom perturbed
 ligand) + solvent module.  Prints the wall-clock ms per step of the loop.
 
@@ -33,6 +34,7 @@ def main():
         graph_loop(steps)
         return
     lib, path = which.split("_")
+    ev = not (len(sys.argv) > 3 and sys.argv[3] == "f")
     s = S.mixed_box_96k()
     ref = O.Reference(gpu=lib == "ref", shim=lib == "shim")
     if path == "soft":
@@ -40,15 +42,15 @@ def main():
         ref.init(f.system(), refresh_interval=20, solvent=True)
         ref.nl_update(forced=True)
         ref.soft_init(f)
-        ref.soft_time_steps(10, need_energy=True, need_virial=True)
-        t = ref.soft_time_steps(steps, first_step=10, need_energy=True, need_virial=True)
+        ref.soft_time_steps(10, need_energy=ev, need_virial=ev)
+        t = ref.soft_time_steps(steps, first_step=10, need_energy=ev, need_virial=ev)
     else:
         ref.init(s, refresh_interval=20, solvent=True)
         ref.nl_update(forced=True)
-        ref.time_steps(10, need_energy=True, need_virial=True)
-        t = ref.time_steps(steps, first_step=10, need_energy=True, need_virial=True)
+        ref.time_steps(10, need_energy=ev, need_virial=ev)
+        t = ref.time_steps(steps, first_step=10, need_energy=ev, need_virial=ev)
     ref.clear()
-    print(json.dumps({"loop": which, "steps": steps, "ms_per_step": t * 1e3 / steps}))
+    print(json.dumps({"loop": which, "steps": steps, "energy_virial": ev, "ms_per_step": t * 1e3 / steps}))
 
 
 def graph_loop(steps):
