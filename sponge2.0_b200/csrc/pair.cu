@@ -142,8 +142,9 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
 // their partners within cutoff + buffer, so the force kernel evaluates both
 // atoms against each partner it loads.  One warp per cluster walks its
 // neighbour table, expands the union of the eight atoms' mask rows 32
-// elements at a time into shared memory, loads each candidate partner once
-// and keeps, for each of the four slot pairs in table order, every partner
+// elements at a time into shared memory, loads each candidate partner once,
+// tests it against all eight atoms without branches (packed FP32x2, two atoms
+// an instruction) and keeps, for each of the four slot pairs in table order, every partner
 // within cutoff + buffer of either of the pair's atoms, as a 32-bit word
 //   {partner slot - system's first slot (22 bits) | LJ type << 22 |
 //    pairs with the first atom << 29 | with the second << 30 | image flag << 31}
@@ -189,6 +190,9 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
     // a chunk's candidates {partner slot | image flag, element lane | own-atom bits << 5}
     __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];
     __shared__ float4 own_all[kPruneWarps][kClusterSize];
+    // the cluster's atoms negated, per coordinate, as the four slot pairs'
+    // {first, second} float2
+    __shared__ __align__(16) float nown_all[kPruneWarps][3][kClusterSize];
     __shared__ unsigned long long kept_total;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -196,6 +200,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
     __syncthreads();
     uint2* __restrict__ mybuf = buf[w];
     float4* __restrict__ own = own_all[w];
+    const float2* __restrict__ nown = reinterpret_cast<const float2*>(&nown_all[w][0][0]);
     // one warp per cluster: each candidate partner is loaded once and tested
     // against the cluster's eight atoms, feeding the four slot pairs' lists
     for (int c = blockIdx.x * kPruneWarps + w; c < clusters_cap; c += gridDim.x * kPruneWarps)
@@ -207,6 +212,9 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
         {
             const float4 pl = pos[s0 + lane];
             own[lane] = pl;
+            nown_all[w][0][lane] = -pl.x;
+            nown_all[w][1][lane] = -pl.y;
+            nown_all[w][2][lane] = -pl.z;
             pref[s0 + lane] = pl;
         }
         __syncwarp();
@@ -279,28 +287,47 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
                 }
                 const unsigned wbase =
                     ((unsigned)js - slot0) | ((unsigned)tj << kWordTypeShift) | (img ? kWordImage : 0u);
+                // bit a: own atom a lies within the pruning radius of the
+                // partner.  All eight are tested without branches; the
+                // minimum-image path (small boxes) only when a lane needs it.
+                unsigned hit = 0;
+                if (!__any_sync(0xffffffffu, img && am != 0u))
+                {
+                    // the partner in the cluster's frame, then two own atoms
+                    // at a time in packed FP32x2
+                    const float2 cx = make_float2(ex + pj.x, ex + pj.x), cy = make_float2(ey + pj.y, ey + pj.y),
+                                 cz = make_float2(ez + pj.z, ez + pj.z);
+#pragma unroll
+                    for (int p = 0; p < 4; p++)
+                    {
+                        const float2 dx = __fadd2_rn(cx, nown[p]), dy = __fadd2_rn(cy, nown[4 + p]),
+                                     dz = __fadd2_rn(cz, nown[8 + p]);
+                        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                        hit |= ((r2.x < rp2 ? 1u : 0u) | (r2.y < rp2 ? 2u : 0u)) << (2 * p);
+                    }
+                }
+                else
+                {
+#pragma unroll 1
+                    for (int a = 0; a < kClusterSize; a++)
+                    {
+                        const float3 d = pair_offset(ex, ey, ez, own[a], pj, img, D);
+                        if (__fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, d.x * d.x)) < rp2) hit |= 1u << a;
+                    }
+                }
+                hit &= am;
 #pragma unroll
                 for (int p = 0; p < 4; p++)
                 {
-                    const bool m1 = (am >> (2 * p)) & 1u, m2 = (am >> (2 * p + 1)) & 1u;
-                    bool keep = false;
-                    if (m1)
-                    {
-                        const float3 d1 = pair_offset(ex, ey, ez, own[2 * p], pj, img, D);
-                        keep = __fmaf_rn(d1.z, d1.z, __fmaf_rn(d1.y, d1.y, d1.x * d1.x)) < rp2;
-                    }
-                    if (m2 && !keep)
-                    {
-                        const float3 d2 = pair_offset(ex, ey, ez, own[2 * p + 1], pj, img, D);
-                        keep = __fmaf_rn(d2.z, d2.z, __fmaf_rn(d2.y, d2.y, d2.x * d2.x)) < rp2;
-                    }
+                    // kept when either atom of the slot pair is in range; the
+                    // word's atom bits stay those of the full list
+                    const bool keep = ((hit >> (2 * p)) & 3u) != 0u;
                     const unsigned m = __ballot_sync(0xffffffffu, keep);
                     if (keep)
                     {
                         const int kk = kept[p] + __popc(m & ((1u << lane) - 1u));
                         if (kk < usable)
-                            pwords[(size_t)(s0 + 2 * p) * slot_cap + kk] =
-                                wbase | (m1 ? kWordFirst : 0u) | (m2 ? kWordSecond : 0u);
+                            pwords[(size_t)(s0 + 2 * p) * slot_cap + kk] = wbase | (((am >> (2 * p)) & 3u) << 29);
                         else
                             atomicOr(&counters[kCntOverflow], kOvfWords);
                     }
