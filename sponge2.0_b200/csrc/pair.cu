@@ -179,6 +179,20 @@ __device__ __forceinline__ float3 pair_offset(float ex, float ey, float ez, floa
     return make_float3(dx, dy, dz);
 }
 
+// Transpose of an 8x8 bit matrix held as 64 bits, row r in byte r (bit 8r + c
+// moves to bit 8c + r): three rounds of swapping off-diagonal blocks of
+// 1x1, 2x2 and 4x4 bits (H. S. Warren, Hacker's Delight, 2nd ed., section 7-3).
+__device__ __forceinline__ unsigned long long transpose8x8(unsigned long long x)
+{
+    unsigned long long t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
+    x ^= t ^ (t << 7);
+    t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
+    x ^= t ^ (t << 14);
+    t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
+    x ^= t ^ (t << 28);
+    return x;
+}
+
 __global__ void __launch_bounds__(kPruneWarps * 32)
     k_prune(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, int clusters_cap,
             int table_cap, int slot_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
@@ -193,6 +207,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
     // the cluster's atoms negated, per coordinate, as the four slot pairs'
     // {first, second} float2
     __shared__ __align__(16) float nown_all[kPruneWarps][3][kClusterSize];
+    __shared__ float4 ent_all[kPruneWarps][32];  // the window's table elements (centre differences)
     __shared__ unsigned long long kept_total;
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
@@ -201,6 +216,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
     uint2* __restrict__ mybuf = buf[w];
     float4* __restrict__ own = own_all[w];
     const float2* __restrict__ nown = reinterpret_cast<const float2*>(&nown_all[w][0][0]);
+    float4* __restrict__ ent = ent_all[w];
     // one warp per cluster: each candidate partner is loaded once and tested
     // against the cluster's eight atoms, feeding the four slot pairs' lists
     for (int c = blockIdx.x * kPruneWarps + w; c < clusters_cap; c += gridDim.x * kPruneWarps)
@@ -255,14 +271,15 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
             const unsigned flag = (eb & (1 << 30)) ? kWordImage : 0u;
             const unsigned base = (unsigned)(eb & 0x3fffffff) | flag;
             int k = incl - cnt;
+            // own atom a pairs with neighbour slot b when bit 8a + b is set;
+            // transposed, byte b holds neighbour b's own-atom bits
+            const unsigned long long tm8 = transpose8x8(((unsigned long long)mm.y << 32) | mm.x);
+            ent[lane] = e;
 #pragma unroll
             for (int b = 0; b < kClusterSize; b++)
                 if ((row >> b) & 1u)
                 {
-                    // own atom a pairs with neighbour slot b when bit 8a + b is set
-                    const unsigned x = (mm.x >> b) & 0x01010101u, y = (mm.y >> b) & 0x01010101u;
-                    const unsigned am = ((x | (x >> 7) | (x >> 14) | (x >> 21)) & 0xfu) |
-                                        (((y | (y >> 7) | (y >> 14) | (y >> 21)) & 0xfu) << 4);
+                    const unsigned am = (unsigned)(tm8 >> (8 * b)) & 0xffu;
                     mybuf[k++] = make_uint2(base + b, (unsigned)lane | (am << 5));
                 }
             __syncwarp();
@@ -270,11 +287,9 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
             {
                 const int q = q0 + lane;
                 const uint2 wv = mybuf[q < total ? q : 0];
-                // the element's centre difference from the lane that read it
-                const int src = (int)(wv.y & 31u);
-                const float ex = __shfl_sync(0xffffffffu, e.x, src);
-                const float ey = __shfl_sync(0xffffffffu, e.y, src);
-                const float ez = __shfl_sync(0xffffffffu, e.z, src);
+                // the element's centre difference, staged by the lane that read it
+                const float4 es = ent[wv.y & 31u];
+                const float ex = es.x, ey = es.y, ez = es.z;
                 const unsigned am = q < total ? (wv.y >> 5) & 0xffu : 0u;
                 const int js = (int)(wv.x & 0x7fffffffu);
                 const bool img = (wv.x & 0x80000000u) != 0;
