@@ -217,10 +217,15 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
     float4* __restrict__ own = own_all[w];
     const float2* __restrict__ nown = reinterpret_cast<const float2*>(&nown_all[w][0][0]);
     float4* __restrict__ ent = ent_all[w];
-    // one warp per cluster: each candidate partner is loaded once and tested
-    // against the cluster's eight atoms, feeding the four slot pairs' lists
-    for (int c = blockIdx.x * kPruneWarps + w; c < clusters_cap; c += gridDim.x * kPruneWarps)
+    // one warp per cluster, taken from a shared counter (tables differ in
+    // length): each candidate partner is loaded once and tested against the
+    // cluster's eight atoms, feeding the four slot pairs' lists
+    for (;;)
     {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(&counters[kCntPruneNext], 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= clusters_cap) break;
         const int sy = cl_sys[c];
         if (!prune[sy]) continue;
         const int s0 = c * kClusterSize;
@@ -386,6 +391,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
         unsigned long long* wp = (unsigned long long*)&counters[kCntPWords];
         *(unsigned long long*)&counters[kCntPWordsLast] = atomicExch(wp, 0ull);
         counters[kCntPruneDone] = 0;
+        counters[kCntPruneNext] = 0;
         counters[kCntPrune] = 0;
         counters[kCntPrunes] += 1;
     }
@@ -1500,7 +1506,7 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
                                                      in.slot_pos, in.slot_type, track ? nl->d_pref : nullptr,
                                                      half * half, nl->d_prune);
     SPGNB_CHECK_LAUNCH("k_pack_slots");
-    const int grid = std::max(1, std::min(num_sms() * 4, nl->clusters_cap));
+    const int grid = std::max(1, std::min(num_sms() * 5, (nl->clusters_cap + kPruneWarps - 1) / kPruneWarps));
     k_prune<<<grid, kPruneWarps * 32, 0, s>>>(in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters, nl->clusters_cap,
                                               nl->table_cap, nl->slot_cap, nl->d_cl_sys, nl->d_sys, nl->d_tcount,
                                               nl->d_tab, nl->d_tmask, in.slot_pos, in.slot_type, nl->d_pref,
