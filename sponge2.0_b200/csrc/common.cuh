@@ -95,6 +95,7 @@ enum Counter
     kCntPWords = 14,    // 64-bit: words of the running pruning (slots 14,15)
     kCntPWordsLast = 16,  // 64-bit: words of the last completed pruning (slots 16,17)
     kCntPruneNext = 18,   // the next cluster a warp of the running prune kernel takes
+    kCntSearchNext = 19,  // the next cluster a warp of the running search kernel takes
     kCntSize = 24
 };
 

@@ -418,11 +418,15 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
     __shared__ uint2 stage_m[kSearchWarps][kChunk];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    const int total_warps = gridDim.x * kSearchWarps;
     unsigned long long elements = 0, listed = 0;
 
-    for (int c = blockIdx.x * kSearchWarps + wib; c < clusters_cap; c += total_warps)
+    // clusters are taken from a counter (their tables differ in length)
+    for (;;)
     {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(&counters[kCntSearchNext], 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= clusters_cap) break;
         const int sy = cl_sys[c];
         if (!need[sy] || c - sys[sy].cl_begin >= ncl[sy]) continue;
         const SysDesc& p = sys[sy];
@@ -812,6 +816,7 @@ __global__ void k_reset_list_counters(int* counters)
     counters[kCntWords + 1] = 0;
     counters[kCntPWordsLast] = 0;
     counters[kCntPWordsLast + 1] = 0;
+    counters[kCntSearchNext] = 0;
 }
 
 __global__ void k_init_atom_groups(int n, spgnb_atom_group* nl, int* temp, int max_nb)
@@ -1475,7 +1480,8 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
         nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_gid, nl->d_slot_d0, nl->d_slot_ex, ex_start, ex_list, ex_num,
         ccap, nl->d_need, nl->d_ncl, nl->d_tcount, nl->d_slot_count, nl->d_pcount);
     SPGNB_CHECK_LAUNCH("k_cluster_props");
-    const int search_blocks = std::max(1, std::min((ccap + kSearchWarps - 1) / kSearchWarps, sms * 8));
+    // one resident wave (five blocks per SM)
+    const int search_blocks = std::max(1, std::min((ccap + kSearchWarps - 1) / kSearchWarps, sms * 5));
     k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
         nl->d_sys, ccap, nl->table_cap, nl->d_need, nl->d_ncl, nl->d_run_start, nl->d_runs, nl->d_cell_cl,
         nl->d_cl_cell, nl->d_cl_sys, nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex,
