@@ -623,7 +623,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
     k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
                 int n_clusters, int slot_cap,
                 const int* __restrict__ cl_sys, const int* __restrict__ pcount, const unsigned* __restrict__ pwords,
-                const int* __restrict__ slot_atom, const float4* __restrict__ slot_x0, const int4* __restrict__ cl_q,
+                const int* __restrict__ slot_atom, const int* __restrict__ slot_gid, const int4* __restrict__ cl_q,
                 const float4* __restrict__ pos, const int* __restrict__ ptype,
                 const float2* __restrict__ gtable, int n_types, float3* __restrict__ frc,
                 long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, const int* __restrict__ only,
@@ -717,8 +717,8 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
         int gi1 = 0, gi2 = 0;
         if (PA)
         {
-            gi1 = __float_as_int(slot_x0[s1].w);
-            gi2 = __float_as_int(slot_x0[s1 + 1].w);
+            gi1 = slot_gid[s1];
+            gi2 = slot_gid[s1 + 1];
         }
         const unsigned* __restrict__ wl = pwords + (size_t)s1 * slot_cap;
         const float2 npx = make_float2(-pi1.x, -pi2.x), npy = make_float2(-pi1.y, -pi2.y),
@@ -798,7 +798,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
                     // only the pair's owner (the lower global index) keeps its
                     // energy and virial; the totals are summed from these, so
                     // every pair counts once
-                    const int gj = __ldg(reinterpret_cast<const int*>(slot_x0) + 4 * (size_t)j + 3);
+                    const int gj = __ldg(slot_gid + j);
                     const bool oA = inA && gi1 < gj, oB = inB && gi2 < gj;
                     own[0] = __fadd2_rn(own[0], make_float2(oA ? elj.x : 0.0f, oB ? elj.y : 0.0f));
                     own[1] = __fadd2_rn(own[1], make_float2(oA ? ec.x : 0.0f, oB ? ec.y : 0.0f));
@@ -1453,7 +1453,7 @@ int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
         std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T, E>, kForceWarps * 32, smem), nl->clusters_cap));
     k_pair_fast<M, F, T, E><<<grid, kForceWarps * 32, smem, s>>>(
         x.p0, x.fps, nl->d_sys, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords,
-        nl->d_slot_atom, nl->d_slot_x0, nl->d_cl_q, x.pos, x.ptype, x.table, x.n_types, x.frc, x.totals, x.om, x.pa,
+        nl->d_slot_atom, nl->d_slot_gid, nl->d_cl_q, x.pos, x.ptype, x.table, x.n_types, x.frc, x.totals, x.om, x.pa,
         x.only, x.xf);
     SPGNB_CHECK_LAUNCH("k_pair_fast");
     return SPGNB_OK;
