@@ -937,45 +937,34 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
                 own1[q] = sg * own[q].x;
                 own2[q] = sg * own[q].y;
             }
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-                for (int q = 0; q < 8; q++)
-                {
-                    own1[q] += __shfl_xor_sync(0xffffffffu, own1[q], o);
-                    own2[q] += __shfl_xor_sync(0xffffffffu, own2[q], o);
-                }
-            if (lane == 0)
+            // both atoms' sums over the lanes: lanes 4q..4q+3 end with value q
+            const float a = reduce_scatter8(own1, lane), b = reduce_scatter8(own2, lane);
+            // an atom's energy is value 0 + value 1 (lanes 0 and 4)
+            const float a1 = __shfl_down_sync(0xffffffffu, a, 4), b1 = __shfl_down_sync(0xffffffffu, b, 4);
+            if ((lane & 3) == 0)
             {
                 // the item's totals: each pair once; the symmetric off-diagonal
                 // terms (xy + yx etc.) are twice the one accumulated
+                const bool twice = vidx == 3 || vidx == 5 || vidx == 6;
+                red[w][vidx] += __double2ll_rn((double)(a + b) * (twice ? 2.0 : 1.0) * kEnergyScale);
 #pragma unroll
-                for (int q = 0; q < 8; q++)
+                for (int h = 0; h < 2; h++)
                 {
-                    const double sc = (q == 3 || q == 5 || q == 6) ? 2.0 : 1.0;
-                    red[w][q] += __double2ll_rn((double)(own1[q] + own2[q]) * sc * kEnergyScale);
-                }
-            }
-            if (lane < 2)
-            {
-                const int ai = slot_atom[s1 + lane];
-                if (ai >= 0)
-                {
-                    const float* ow = lane ? own2 : own1;
+                    const int ai = slot_atom[s1 + h];
+                    if (ai < 0) continue;
+                    const float val = h ? b : a;
                     const int o = om.remap(ai);
-                    if (pa.energy) atomicAdd(pa.energy + o, ow[0] + ow[1]);
-                    if (pa.lj_energy) atomicAdd(pa.lj_energy + o, ow[0]);
-                    if (pa.direct) atomicAdd(pa.direct + o, ow[1]);
-                    if (pa.virial)
+                    if (vidx == 0)
                     {
-                        float* v = pa.virial + 6 * (size_t)o;
-                        atomicAdd(v + 0, ow[2]);
-                        atomicAdd(v + 1, 2.0f * ow[3]);
-                        atomicAdd(v + 2, ow[4]);
-                        atomicAdd(v + 3, 2.0f * ow[5]);
-                        atomicAdd(v + 4, 2.0f * ow[6]);
-                        atomicAdd(v + 5, ow[7]);
+                        if (pa.energy) atomicAdd(pa.energy + o, val + (h ? b1 : a1));
+                        if (pa.lj_energy) atomicAdd(pa.lj_energy + o, val);
                     }
+                    else if (vidx == 1)
+                    {
+                        if (pa.direct) atomicAdd(pa.direct + o, val);
+                    }
+                    else if (pa.virial)
+                        atomicAdd(pa.virial + 6 * (size_t)o + (vidx - 2), twice ? 2.0f * val : val);
                 }
             }
         }
