@@ -403,13 +403,14 @@ __device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
 // Fixed (c, c) constants of the packed arithmetic in constant memory, so the
 // FP32x2 instructions read them as constant-bank operands instead of
 // building register pairs each time.
-static __constant__ float2 kPk[3] = {{-1.0f, -1.0f}, {-1.0f / 12.0f, -1.0f / 12.0f}, {-1.0f / 6.0f, -1.0f / 6.0f}};
+static __constant__ float2 kPk[1] = {{-1.0f, -1.0f}};
 enum PackedConst
 {
-    kPkMinusOne = 0,
-    kPkMinusTwelfth = 1,
-    kPkMinusSixth = 2
+    kPkMinusOne = 0
 };
+// pair_scalar2's LJ energy is -12 times the energy (A/(12 r^12) - B/(6 r^6)):
+// the kernels scale the sums once
+constexpr float kLjEnergyScale = -1.0f / 12.0f;
 
 __device__ __forceinline__ float2 poly5x2(float2 x, const float2* c)
 {
@@ -480,7 +481,9 @@ __device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, 
     const float2 rinv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
     const float2 r2inv = __fmul2_rn(rinv, rinv);
     const float2 r6inv = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
-    const float2 flj = __fmul2_rn(__fmul2_rn(__ffma2_rn(nA, r6inv, B), r6inv), r2inv);
+    // u = (-A/r^6 + B)/r^6 serves the force and, plus B/r^6, the energy
+    const float2 u = __fmul2_rn(__ffma2_rn(nA, r6inv, B), r6inv);
+    const float2 flj = __fmul2_rn(u, r2inv);
     float2 fc;
     if (FIT == 1)
     {
@@ -517,9 +520,7 @@ __device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, 
         fc = make_float2(c[0], c[1]);
         if (ENERGY) e_c = make_float2(e[0], e[1]);
     }
-    if (ENERGY)
-        e_lj = __fmul2_rn(__ffma2_rn(nA, __fmul2_rn(r6inv, kPk[kPkMinusTwelfth]), __fmul2_rn(B, kPk[kPkMinusSixth])),
-                          r6inv);
+    if (ENERGY) e_lj = __ffma2_rn(B, r6inv, u);  // -A/r^12 + 2B/r^6 = -12 E_lj
     return __ffma2_rn(fc, kPk[kPkMinusOne], flj);
 }
 
@@ -916,7 +917,8 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
         {
             float ev[8];
 #pragma unroll
-            for (int q = 0; q < 8; q++) ev[q] = (q >= 2 ? -1.0f : 1.0f) * (acc[q].x + acc[q].y);
+            for (int q = 0; q < 8; q++)
+                ev[q] = (q >= 2 ? -1.0f : (q == 0 ? kLjEnergyScale : 1.0f)) * (acc[q].x + acc[q].y);
             const float esum = reduce_scatter8(ev, lane);
             if ((lane & 3) == 0)
             {
@@ -933,7 +935,7 @@ __global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0
             for (int q = 0; q < 8; q++)
             {
                 // the virial terms were accumulated as +g (x) d: the virial is -g (x) d
-                const float sg = q >= 2 ? -1.0f : 1.0f;
+                const float sg = q >= 2 ? -1.0f : (q == 0 ? kLjEnergyScale : 1.0f);
                 own1[q] = sg * own[q].x;
                 own2[q] = sg * own[q].y;
             }
