@@ -62,6 +62,7 @@ struct spgnb_batch
     // force field
     int T = 0;
     float2* d_table = nullptr;
+    float4* d_t4 = nullptr;       // the force kernel's T^3 table
     spgnb::ForceParams* d_fps = nullptr;  // S + 1
     std::vector<spgnb::ForceParams> h_fps;
     bool fit = true;                  // the rational fits (every admitted system inside their range)
@@ -73,7 +74,7 @@ struct spgnb_batch
     int* d_flags = nullptr;           // per system: evaluate now
     std::vector<int> h_flags;
     float4* d_slot_pos = nullptr;
-    int* d_slot_type = nullptr;
+    int4* d_slot_aux = nullptr;
     // stepping
     bool have_water = false;
     float ra = 0, rb = 0, rc = 0, mO = 0, mH = 0;
@@ -266,12 +267,11 @@ int batch_force(spgnb_batch* b, int mode, cudaStream_t s, const int* only = null
     in.charge = b->d_charge;
     in.atom_type = b->d_type;
     in.slot_pos = b->d_slot_pos;
-    in.slot_type = b->d_slot_type;
+    in.slot_aux = b->d_slot_aux;
     in.p0 = b->h_fps[0];
     in.d_fps = b->d_fps;
     in.fit = b->fit;
-    in.table = b->d_table;
-    in.table_size = b->T * b->T;
+    in.t4 = b->d_t4;
     in.frc = b->d_frc;
     in.totals = b->d_totals;
     in.mode = mode;
@@ -400,7 +400,8 @@ void free_batch(spgnb_batch* b)
     dfree(b->d_left);
     dfree(b->d_flags);
     dfree(b->d_slot_pos);
-    dfree(b->d_slot_type);
+    dfree(b->d_slot_aux);
+    dfree(b->d_t4);
     if (b->stream) cudaStreamSynchronize(b->stream);
     for (PinnedStage& ps : b->stages)
     {
@@ -533,7 +534,7 @@ int stage(const spgnb_batch_system& y, int T, const std::vector<float>& pair_A, 
     f.use_fit = (zz * zz <= SPGNB_EWALD_W_MAX * 0.999f) ? 1 : 0;
     f.n_types = T;
     f.table_begin = 0;
-    f.pad = 0;
+    f.t4_begin = 0;
     // Total_C6_Get and the factor of Lennard_Jones_force.cpp:263-268
     double c6 = 0.0;
     for (int p = 0; p < T; p++)
@@ -590,11 +591,11 @@ int create_common(spgnb_batch* b, const NLPoolSpec& spec, long long ex_cap, int 
         (st = zalloc(&b->d_totals, 8 * S1)) || (st = zalloc(&b->d_kin, S1)) || (st = zalloc(&b->d_ndof, S1)) ||
         (st = zalloc(&b->d_steps, S1)) || (st = zalloc(&b->d_left, S1)) || (st = zalloc(&b->d_flags, S1)) ||
         (st = dalloc(&b->d_slot_pos, (size_t)b->nl->clusters_cap * kClusterSize + 1)) ||
-        (st = dalloc(&b->d_slot_type, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
+        (st = dalloc(&b->d_slot_aux, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
         return st;
     SPGNB_CUDA(cudaMemcpy(b->d_table, table.data(), sizeof(float2) * table.size(), cudaMemcpyHostToDevice));
     SPGNB_CUDA(cudaMemset(b->d_waters, 0xff, sizeof(int) * b->w_cap));
-    force_kernels_init(T * T);
+    if ((st = build_t4(table.data(), T, &b->d_t4))) return st;
     SPGNB_CUDA(cudaDeviceSynchronize());
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");

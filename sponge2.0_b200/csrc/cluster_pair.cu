@@ -1,0 +1,893 @@
+// Short-range force over the cluster lists: the per-step slot pack, the
+// pruning of the neighbour tables into per-cluster partner lists, the
+// cluster-pair force kernel and its finishing pass.  Together they are the
+// B200 form of Lennard_Jones_And_Direct_Coulomb_Device and its dispatcher
+// (SPONGE/Lennard_Jones_force/Lennard_Jones_force.cpp:43-136, 359-417) and of
+// the solvent kernel (solvent_LJ.cpp:25-145), which evaluate the same pairs.
+//
+// List layout.  A cluster is 8 slots.  Each cluster I has one partner list:
+// 32-bit words {partner slot - system's first slot (22 bits) | mask of the
+// cluster's atoms the partner pairs with (8 bits) << 22 | image flag << 30}.
+// A word's partner is evaluated against all eight atoms of I at once, so the
+// partner's gathers and the word's decoding are paid once per eight pairs.
+// The list has two parts:
+//   upper: partners in clusters J > I, and in I itself the pairs a < b;
+//   lower: partners in clusters J < I, and in I itself the pairs a > b.
+// The upper part alone holds every pair once (a half list); both parts hold
+// every pair from both sides (a full list).  Words are kept when the partner
+// lies within rc + buffer of one of the atoms at the last pruning, and a
+// pruning is redone when an atom has moved half the buffer since, so no pair
+// within rc is ever missing.
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "common.cuh"
+#include "pairfn.cuh"
+
+namespace spgnb
+{
+namespace
+{
+
+constexpr int kPruneWarps = 8;
+constexpr int kWindow = 32;                        // list parts are padded to whole 32-word windows
+constexpr unsigned kWordSlotMask = (1u << 22) - 1u; // partner slot field of a list word
+constexpr int kWordMaskShift = 22;                  // the 8-bit atom mask
+constexpr unsigned kWordImage = 1u << 30;           // the pair needs its own periodic image
+constexpr int kPairWarps = 4;                       // warps per block of the force kernel
+
+// Per-step slot pack: each slot's offset from the build-time cluster centre
+// moved by the displacement since the build (minimum image in the system's
+// box, so a caller that wraps coordinates between builds is fine), with the
+// charge; and the slot's aux record {cluster centre x | LJ type << 22, centre
+// y, centre z, global index}, the 22-bit centre the force kernel takes
+// differences of (its high bits are masked off there).  Slot slots_cap is a
+// null slot: 10^4 A away from everything, charge 0.  With pruning on (pref
+// set) the kernel also flags a re-pruning when some atom moved more than half
+// the prune buffer since the last one.
+__global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict__ slot_atom,
+                             const int* __restrict__ slot_gid, const int* __restrict__ cl_sys,
+                             const SysDesc* __restrict__ sys, const int4* __restrict__ cl_q,
+                             const float4* __restrict__ x0, const float4* __restrict__ d0,
+                             const float3* __restrict__ crd, const float* __restrict__ charge,
+                             const int* __restrict__ local_type, float4* __restrict__ pos, int4* __restrict__ aux,
+                             const float4* __restrict__ pref, float half_buffer2, int* __restrict__ prune)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    bool moved = false;
+    if (s == slots_cap)
+    {
+        pos[s] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
+        aux[s] = make_int4(0, 0, 0, -1);
+    }
+    else if (s < slots_cap)
+    {
+        const int a = slot_atom[s];
+        const float4 d = d0[s];
+        const int4 q = cl_q[s >> 3];
+        float4 p = make_float4(d.x, d.y, d.z, 0.0f);
+        int t = 0;
+        if (a >= 0)
+        {
+            const SysDesc& D = sys[cl_sys[s >> 3]];
+            const float3 c = crd[a];
+            const float4 o = x0[s];
+            float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+            const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
+            const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
+            const float sz = rintf(dz * D.rcell.a33);
+            dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
+            dy -= sy * D.cell.a22 + sz * D.cell.a32;
+            dz -= sz * D.cell.a33;
+            p = make_float4(d.x + dx, d.y + dy, d.z + dz, charge[a]);
+            t = local_type[a];
+            if (pref)
+            {
+                const float4 r = pref[s];
+                const float ex = p.x - r.x, ey = p.y - r.y, ez = p.z - r.z;
+                moved = ex * ex + ey * ey + ez * ez > half_buffer2;
+                if (moved) prune[cl_sys[s >> 3]] = 1;
+            }
+        }
+        pos[s] = p;
+        aux[s] = make_int4((q.x & 0x3fffff) | (t << 22), q.y, q.z, a >= 0 ? slot_gid[s] : -1);
+    }
+    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) counters[kCntPrune] = 1;
+}
+
+// Pruning (no reference counterpart; results unchanged).  Runs after every
+// rebuild and whenever some atom of a system moved more than buffer/2 since
+// its last one (the pack kernel checks).  One warp per cluster I walks its
+// neighbour table, expands the union of the eight atoms' mask rows 32
+// elements at a time into shared memory, loads each candidate partner once,
+// tests it against all eight atoms without branches (packed FP32x2, two atoms
+// an instruction) and writes one word per partner within cutoff + buffer of
+// any of them: to the upper part (from the start of the cluster's region,
+// ascending) or the lower part (from its end, descending).  Both parts are
+// padded to whole windows with words whose mask is empty.  The last block to
+// finish clears the flags.
+__global__ void __launch_bounds__(kPruneWarps * 32)
+    k_prune8(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, int clusters_cap,
+             int table_cap, int list_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
+             const int* __restrict__ tcount, const float4* __restrict__ tab, const uint2* __restrict__ tmask,
+             const float4* __restrict__ pos, float4* __restrict__ pref, int* __restrict__ lcount,
+             unsigned* __restrict__ words, int n_sys, int* __restrict__ prune)
+{
+    if (counters[kCntPrune] == 0) return;
+    // a chunk's candidates {partner slot | image flag, element lane | own-atom bits << 5}
+    __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];
+    __shared__ float4 own_all[kPruneWarps][kClusterSize];
+    // the cluster's atoms negated, per coordinate, as four {even, odd} float2
+    __shared__ __align__(16) float nown_all[kPruneWarps][3][kClusterSize];
+    __shared__ float4 ent_all[kPruneWarps][32];  // the window's table elements (centre differences)
+    __shared__ unsigned long long kept_total;
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    if (threadIdx.x == 0) kept_total = 0;
+    __syncthreads();
+    uint2* __restrict__ mybuf = buf[w];
+    float4* __restrict__ own = own_all[w];
+    const float2* __restrict__ nown = reinterpret_cast<const float2*>(&nown_all[w][0][0]);
+    float4* __restrict__ ent = ent_all[w];
+    const unsigned below = (1u << lane) - 1u;
+    for (;;)
+    {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(&counters[kCntPruneNext], 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= clusters_cap) break;
+        const int sy = cl_sys[c];
+        if (!prune[sy]) continue;
+        const int s0 = c * kClusterSize;
+        if (lane < kClusterSize)
+        {
+            const float4 pl = pos[s0 + lane];
+            own[lane] = pl;
+            nown_all[w][0][lane] = -pl.x;
+            nown_all[w][1][lane] = -pl.y;
+            nown_all[w][2][lane] = -pl.z;
+            pref[s0 + lane] = pl;
+        }
+        __syncwarp();
+        const SysDesc& D = sys[sy];
+        const unsigned slot0 = (unsigned)D.cl_begin * kClusterSize;
+        const ForceParams P = fps ? fps[sy] : p0;
+        const float rp = sqrtf(P.rc2) + buffer + 1e-3f;
+        const float rp2 = buffer > 0.0f ? rp * rp : 3.0e38f;
+        const int T = tcount[c];
+        const float4* __restrict__ tb = tab + (size_t)c * table_cap;
+        const uint2* __restrict__ tm = tmask + (size_t)c * table_cap;
+        unsigned* __restrict__ wc = words + (size_t)c * list_cap;
+        const int usable = list_cap - 2 * kWindow;  // room left for both parts' padding
+        int kh = 0, kl = 0;
+        for (int t0 = 0; t0 < T; t0 += 32)
+        {
+            const int t = t0 + lane;
+            uint2 mm = make_uint2(0u, 0u);
+            float4 e = make_float4(0, 0, 0, 0);
+            if (t < T)
+            {
+                e = tb[t];
+                mm = tm[t];
+            }
+            // partners of any of the eight atoms
+            unsigned u = mm.x | mm.y;
+            u |= u >> 16;
+            u |= u >> 8;
+            const unsigned row = u & 0xffu;
+            const int cnt = __popc(row);
+            int incl = cnt;
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += y;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const int eb = __float_as_int(e.w);
+            const unsigned flag = (eb & (1 << 30)) ? 0x80000000u : 0u;
+            const unsigned base = (unsigned)(eb & 0x3fffffff) | flag;
+            int k = incl - cnt;
+            // own atom a pairs with neighbour slot b when bit 8a + b is set;
+            // transposed, byte b holds neighbour b's own-atom bits
+            const unsigned long long tm8 = transpose8x8(((unsigned long long)mm.y << 32) | mm.x);
+            ent[lane] = e;
+#pragma unroll
+            for (int b = 0; b < kClusterSize; b++)
+                if ((row >> b) & 1u)
+                {
+                    const unsigned am = (unsigned)(tm8 >> (8 * b)) & 0xffu;
+                    mybuf[k++] = make_uint2(base + b, (unsigned)lane | (am << 5));
+                }
+            __syncwarp();
+            for (int q0 = 0; q0 < total; q0 += 32)
+            {
+                const int q = q0 + lane;
+                const uint2 wv = mybuf[q < total ? q : 0];
+                // the element's centre difference, staged by the lane that read it
+                const float4 es = ent[wv.y & 31u];
+                const float ex = es.x, ey = es.y, ez = es.z;
+                const unsigned am = q < total ? (wv.y >> 5) & 0xffu : 0u;
+                const int js = (int)(wv.x & 0x7fffffffu);
+                const bool img = (wv.x & 0x80000000u) != 0;
+                float4 pj = make_float4(0, 0, 0, 0);
+                if (am) pj = pos[js];
+                // bit a: own atom a lies within the pruning radius of the
+                // partner.  All eight are tested without branches; the
+                // minimum-image path (small boxes) only when a lane needs it.
+                unsigned hit = 0;
+                if (!__any_sync(0xffffffffu, img && am != 0u))
+                {
+                    // the partner in the cluster's frame, then two own atoms
+                    // at a time in packed FP32x2
+                    const float2 cx = make_float2(ex + pj.x, ex + pj.x), cy = make_float2(ey + pj.y, ey + pj.y),
+                                 cz = make_float2(ez + pj.z, ez + pj.z);
+#pragma unroll
+                    for (int p = 0; p < 4; p++)
+                    {
+                        const float2 dx = __fadd2_rn(cx, nown[p]), dy = __fadd2_rn(cy, nown[4 + p]),
+                                     dz = __fadd2_rn(cz, nown[8 + p]);
+                        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                        hit |= ((r2.x < rp2 ? 1u : 0u) | (r2.y < rp2 ? 2u : 0u)) << (2 * p);
+                    }
+                }
+                else
+                {
+#pragma unroll 1
+                    for (int a = 0; a < kClusterSize; a++)
+                    {
+                        const float3 d = pair_offset(ex, ey, ez, own[a], pj, img, D);
+                        if (__fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, d.x * d.x)) < rp2) hit |= 1u << a;
+                    }
+                }
+                hit &= am;
+                // the upper part takes the pairs of later clusters and, within
+                // the cluster, those with a < b; the lower part the others
+                const int J = js >> 3;
+                unsigned hb, lb;
+                if (J > c)
+                {
+                    hb = hit;
+                    lb = 0u;
+                }
+                else if (J < c)
+                {
+                    hb = 0u;
+                    lb = hit;
+                }
+                else
+                {
+                    const unsigned b = (unsigned)js & 7u;
+                    hb = hit & ((1u << b) - 1u);
+                    lb = hit & (0xfeu << b) & 0xffu;
+                }
+                const unsigned wb = ((unsigned)js - slot0) | (img ? kWordImage : 0u);
+                const unsigned mh = __ballot_sync(0xffffffffu, hb != 0u);
+                const unsigned ml = __ballot_sync(0xffffffffu, lb != 0u);
+                const int kh_next = kh + __popc(mh), kl_next = kl + __popc(ml);
+                // the parts grow towards each other: [0, kh) and [cap - kl, cap)
+                if (kh_next + kl_next <= usable)
+                {
+                    if (hb) wc[kh + __popc(mh & below)] = wb | (hb << kWordMaskShift);
+                    if (lb) wc[list_cap - 1 - (kl + __popc(ml & below))] = wb | (lb << kWordMaskShift);
+                }
+                else if (lane == 0)
+                    atomicOr(&counters[kCntOverflow], kOvfWords);
+                kh = kh_next;
+                kl = kl_next;
+            }
+            __syncwarp();
+        }
+        // an overflowed cluster keeps no list (the flag makes the caller regrow
+        // and rebuild); otherwise pad both parts to whole windows
+        if (kh + kl > usable) kh = kl = 0;
+        const int hp = (kh + kWindow - 1) & ~(kWindow - 1), lp = (kl + kWindow - 1) & ~(kWindow - 1);
+        const unsigned null_word = (unsigned)s0 - slot0;
+        for (int k2 = kh + lane; k2 < hp; k2 += 32) wc[k2] = null_word;
+        for (int k2 = kl + lane; k2 < lp; k2 += 32) wc[list_cap - 1 - k2] = null_word;
+        if (lane == 0)
+        {
+            lcount[s0] = hp;
+            lcount[s0 + 1] = lp;
+            atomicAdd(&kept_total, (unsigned long long)(kh + kl));
+        }
+        __syncwarp();
+    }
+    __shared__ int is_last;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        atomicAdd((unsigned long long*)&counters[kCntPWords], kept_total);
+        __threadfence();
+        is_last = atomicAdd(&counters[kCntPruneDone], 1) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return;
+    for (int q = threadIdx.x; q < n_sys; q += blockDim.x) prune[q] = 0;
+    if (threadIdx.x == 0)
+    {
+        unsigned long long* wp = (unsigned long long*)&counters[kCntPWords];
+        *(unsigned long long*)&counters[kCntPWordsLast] = atomicExch(wp, 0ull);
+        counters[kCntPruneDone] = 0;
+        counters[kCntPruneNext] = 0;
+        counters[kCntPrune] = 0;
+        counters[kCntPrunes] += 1;
+    }
+}
+
+// Cluster-pair force kernel.  A warp takes clusters from a counter and walks
+// the cluster's list, one word per lane per iteration; the partner's offset
+// {delta + displacement, q} and aux record {22-bit centre, LJ type, global
+// index} load once for all of the cluster's atoms the lane holds, and
+//   dr = (c_J - c_I) * cell / 2^22 + p_j - p_i
+// is formed with the exact integer centre difference.  The atoms are held in
+// registers as packed pairs, so every instruction of the pair function
+// serves two pairs (FP32x2).  The LJ coefficients of a pair of cluster atoms
+// against the partner's type come as one float4 {-A_a, -A_b, B_a, B_b} of
+// the T^3 table.  Partner gathers run one iteration ahead of their use, list
+// words two.
+//
+// HALF (forces, and forces with energy/virial totals): the upper part only,
+// each pair once; a lane holds all 8 atoms, the partner's force (summed over
+// the 8 in a fixed order) goes to its int64 fixed-point accumulator by one
+// atomic add per component and word, and the cluster's forces are summed
+// over the lanes as int64 and added the same way.  Integer addition does not
+// depend on order, so the forces are bitwise reproducible; the finishing pass
+// converts them.
+//
+// Full (per-atom energy and virial, MODE 2): both parts, each pair from both
+// sides.  Half-warps take four atoms each, over the same words; an atom's
+// force and its owned energy and virial (pairs whose other atom has the
+// higher global index, as the reference's half list credits them to the
+// owner; water sites hand theirs to the residue's first atom, as
+// SOLVENT_LENNARD_JONES does) are complete in the warp and added once.
+//
+// MODE 0: forces.  MODE 1: + energy and virial totals.  MODE 2: + per-atom
+// outputs, totals summed from them.
+template <int MODE, int FIT, bool TRI, bool HALF>
+__global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
+    k_pair8(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys, int n_clusters,
+            int list_cap, const int* __restrict__ cl_sys, const int* __restrict__ lcount,
+            const unsigned* __restrict__ words, const int* __restrict__ slot_atom, const int4* __restrict__ cl_q,
+            const float4* __restrict__ pos, const int4* __restrict__ aux, const float4* __restrict__ t4,
+            float3* __restrict__ frc, long long* __restrict__ facc, long long* __restrict__ totals, OwnerMap om,
+            PerAtomOut pa, const int* __restrict__ only, int* __restrict__ counters)
+{
+    constexpr bool EN = MODE >= 1;
+    constexpr bool PA = MODE >= 2;
+    static_assert(!(PA && HALF), "per-atom outputs use the full list");
+    constexpr int NI = HALF ? 8 : 4;  // cluster atoms a lane holds
+    constexpr int NP = NI / 2;        // as packed pairs
+    constexpr int WPI = 4 * NI;       // words an iteration takes (32, or 16 twice)
+    __shared__ long long red[kPairWarps][8];  // per-warp fixed-point totals
+    __shared__ int is_last;
+    const int lane = threadIdx.x & 31;
+    const int w = threadIdx.x >> 5;
+    const int sub = HALF ? 0 : lane >> 4;  // the half of the cluster this lane holds (full list)
+    const int lw = lane & (WPI - 1);      // the word of an iteration this lane takes
+    if (EN && lane < 8) red[w][lane] = 0;
+    __syncwarp();
+    int cur_sys = -1;  // the system red[w] accumulates for
+    for (;;)
+    {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(&counters[kCntPairNext], 1);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= n_clusters) break;
+        const int s0 = c * kClusterSize;
+        const int nh = lcount[s0];
+        const int nlo = HALF ? 0 : lcount[s0 + 1];
+        const int total = nh + nlo;  // multiples of the window
+        if (total == 0) continue;
+        const int sy = cl_sys[c];
+        if (only && !only[sy]) continue;
+        if (EN && sy != cur_sys)
+        {
+            // totals belong to one system each: flush this warp's share
+            __syncwarp();
+            if (lane == 0 && cur_sys >= 0)
+                for (int q = 0; q < 8; q++)
+                {
+                    const long long v = red[w][q];
+                    if (v) atomicAdd((unsigned long long*)&totals[8 * cur_sys + q], (unsigned long long)v);
+                    red[w][q] = 0;
+                }
+            __syncwarp();
+            cur_sys = sy;
+        }
+        const ForceParams P = fps ? fps[sy] : p0;
+        const PairParams2 pp = pack_params(P);
+        const SysDesc& D = sys[sy];
+        const Cell qc = D.qcell;
+        const int slot0 = D.cl_begin * kClusterSize;
+        const int4 ci = cl_q[c];
+        const int nt = P.n_types;
+        // this lane's cluster atoms, negated, as packed pairs
+        float2 npx[NP], npy[NP], npz[NP], qi[NP];
+        int rowb[NP];
+        int gi[NI];
+#pragma unroll
+        for (int p = 0; p < NP; p++)
+        {
+            const int a = sub * NI + 2 * p;
+            const float4 u0 = pos[s0 + a], u1 = pos[s0 + a + 1];
+            const int4 x0 = aux[s0 + a], x1 = aux[s0 + a + 1];
+            npx[p] = make_float2(-u0.x, -u1.x);
+            npy[p] = make_float2(-u0.y, -u1.y);
+            npz[p] = make_float2(-u0.z, -u1.z);
+            qi[p] = make_float2(u0.w, u1.w);
+            rowb[p] = P.t4_begin + (((x0.x >> 22) & 0x7f) * nt + ((x1.x >> 22) & 0x7f)) * nt;
+            gi[2 * p] = x0.w;
+            gi[2 * p + 1] = x1.w;
+        }
+        float2 fx[NP], fy[NP], fz[NP];
+#pragma unroll
+        for (int p = 0; p < NP; p++) fx[p] = fy[p] = fz[p] = f2(0.0f);
+        float2 acc[(EN && !PA) ? 8 : 1];
+#pragma unroll
+        for (int q = 0; q < ((EN && !PA) ? 8 : 1); q++) acc[q] = f2(0.0f);
+        float2 own[PA ? NP : 1][PA ? 8 : 1];
+#pragma unroll
+        for (int p = 0; p < (PA ? NP : 1); p++)
+#pragma unroll
+            for (int q = 0; q < (PA ? 8 : 1); q++) own[p][q] = f2(0.0f);
+
+        const unsigned* __restrict__ wb = words + (size_t)c * list_cap;
+        // the k-th word of the list: the upper part, then the lower part
+        auto word_at = [&](int k) { return __ldg(k < nh ? wb + k : wb + (list_cap - nlo) + (k - nh)); };
+        unsigned wc = word_at(lw);
+        unsigned wn = WPI < total ? word_at(WPI + lw) : wc;
+        int jc = slot0 + (int)(wc & kWordSlotMask);
+        float4 pjc = pos[jc];
+        int4 xjc = aux[jc];
+#pragma unroll 1
+        for (int k0 = 0; k0 < total; k0 += WPI)
+        {
+            // the next iteration's partner and the word after it
+            const unsigned wnn = k0 + 2 * WPI < total ? word_at(k0 + 2 * WPI + lw) : wn;
+            const int jn = slot0 + (int)(wn & kWordSlotMask);
+            const float4 pjn = pos[jn];
+            const int4 xjn = aux[jn];
+
+            const unsigned m8 = (wc >> kWordMaskShift) & 0xffu;
+            const unsigned mi = HALF ? m8 : (m8 >> (4 * sub)) & 0xfu;
+            const float ux = centre_step(xjc.x, ci.x), uy = centre_step(xjc.y, ci.y), uz = centre_step(xjc.z, ci.z);
+            // the partner in the frame of the cluster's centre
+            float sx = __fmaf_rn(ux, qc.a11, pjc.x);
+            float sy2 = __fmaf_rn(uy, qc.a22, pjc.y);
+            const float sz = __fmaf_rn(uz, qc.a33, pjc.z);
+            if (TRI)
+            {
+                sx = __fmaf_rn(uy, qc.a21, sx);
+                sx = __fmaf_rn(uz, qc.a31, sx);
+                sy2 = __fmaf_rn(uz, qc.a32, sy2);
+            }
+            const bool img = (wc & kWordImage) != 0u;
+            const bool any_img = __any_sync(0xffffffffu, img);
+            const int tj = (xjc.x >> 22) & 0x7f;
+            const int gj = xjc.w;
+            const float2 qj = f2(pjc.w);
+            float2 hx = f2(0.0f), hy = f2(0.0f), hz = f2(0.0f);  // the partner's force, negated
+#pragma unroll
+            for (int p = 0; p < NP; p++)
+            {
+                float2 dx = __fadd2_rn(f2(sx), npx[p]), dy = __fadd2_rn(f2(sy2), npy[p]),
+                       dz = __fadd2_rn(f2(sz), npz[p]);
+                if (any_img && img)
+                {
+                    // small box: the pair takes its own minimum image
+                    float ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+                    {
+                        const float tx = rintf(ddx[h] * D.rcell.a11 + ddy[h] * D.rcell.a21 + ddz[h] * D.rcell.a31);
+                        const float ty = rintf(ddy[h] * D.rcell.a22 + ddz[h] * D.rcell.a32);
+                        const float tz = rintf(ddz[h] * D.rcell.a33);
+                        ddx[h] -= tx * D.cell.a11 + ty * D.cell.a21 + tz * D.cell.a31;
+                        ddy[h] -= ty * D.cell.a22 + tz * D.cell.a32;
+                        ddz[h] -= tz * D.cell.a33;
+                    }
+                    dx = make_float2(ddx[0], ddx[1]);
+                    dy = make_float2(ddy[0], ddy[1]);
+                    dz = make_float2(ddz[0], ddz[1]);
+                }
+                const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
+                const bool inA = ((mi >> (2 * p)) & 1u) && r2.x < pp.rc2;
+                const bool inB = ((mi >> (2 * p + 1)) & 1u) && r2.y < pp.rc2;
+                const float4 ab = __ldg(t4 + rowb[p] + tj);
+                float2 elj, ec;
+                float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(qj, qi[p]), make_float2(ab.x, ab.y),
+                                                 make_float2(ab.z, ab.w), pp, elj, ec);
+                f = make_float2(inA ? f.x : 0.0f, inB ? f.y : 0.0f);
+                const float2 gx = __fmul2_rn(f, dx), gy = __fmul2_rn(f, dy), gz = __fmul2_rn(f, dz);
+                fx[p] = __fadd2_rn(fx[p], gx);
+                fy[p] = __fadd2_rn(fy[p], gy);
+                fz[p] = __fadd2_rn(fz[p], gz);
+                if (HALF)
+                {
+                    hx = __fadd2_rn(hx, gx);
+                    hy = __fadd2_rn(hy, gy);
+                    hz = __fadd2_rn(hz, gz);
+                }
+                if (EN && !PA)
+                {
+                    acc[0] = __fadd2_rn(acc[0], make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f));
+                    acc[1] = __fadd2_rn(acc[1], make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f));
+                    acc[2] = __ffma2_rn(gx, dx, acc[2]);
+                    acc[3] = __ffma2_rn(gx, dy, acc[3]);
+                    acc[4] = __ffma2_rn(gy, dy, acc[4]);
+                    acc[5] = __ffma2_rn(gx, dz, acc[5]);
+                    acc[6] = __ffma2_rn(gy, dz, acc[6]);
+                    acc[7] = __ffma2_rn(gz, dz, acc[7]);
+                }
+                if (PA)
+                {
+                    // the pair's owner is the lower global index
+                    const bool oA = inA && gi[2 * p] < gj, oB = inB && gi[2 * p + 1] < gj;
+                    own[p][0] = __fadd2_rn(own[p][0], make_float2(oA ? elj.x : 0.0f, oB ? elj.y : 0.0f));
+                    own[p][1] = __fadd2_rn(own[p][1], make_float2(oA ? ec.x : 0.0f, oB ? ec.y : 0.0f));
+                    const float2 mgx = make_float2(oA ? gx.x : 0.0f, oB ? gx.y : 0.0f);
+                    const float2 mgy = make_float2(oA ? gy.x : 0.0f, oB ? gy.y : 0.0f);
+                    const float2 mgz = make_float2(oA ? gz.x : 0.0f, oB ? gz.y : 0.0f);
+                    own[p][2] = __ffma2_rn(mgx, dx, own[p][2]);
+                    own[p][3] = __ffma2_rn(mgx, dy, own[p][3]);
+                    own[p][4] = __ffma2_rn(mgy, dy, own[p][4]);
+                    own[p][5] = __ffma2_rn(mgx, dz, own[p][5]);
+                    own[p][6] = __ffma2_rn(mgy, dz, own[p][6]);
+                    own[p][7] = __ffma2_rn(mgz, dz, own[p][7]);
+                }
+            }
+            if (HALF)
+            {
+                // the partner's force: minus the sum over the cluster's atoms
+                const long long qx = __float2ll_rn(-(hx.x + hx.y) * kTwoPow32);
+                const long long qy = __float2ll_rn(-(hy.x + hy.y) * kTwoPow32);
+                const long long qz = __float2ll_rn(-(hz.x + hz.y) * kTwoPow32);
+                unsigned long long* fa = (unsigned long long*)(facc + 3 * (size_t)jc);
+                if (qx) atomicAdd(fa + 0, (unsigned long long)qx);
+                if (qy) atomicAdd(fa + 1, (unsigned long long)qy);
+                if (qz) atomicAdd(fa + 2, (unsigned long long)qz);
+            }
+            wc = wn;
+            wn = wnn;
+            jc = jn;
+            pjc = pjn;
+            xjc = xjn;
+        }
+
+        // the cluster's forces: int64 per lane, summed over the lanes by a
+        // reduce-scatter (lanes 4a..4a+3 end with atom a)
+        long long vx[8], vy[8], vz[8];
+#pragma unroll
+        for (int a = 0; a < 8; a++)
+        {
+            const int p = (a % NI) / 2;
+            const bool mine = HALF || (a / NI) == sub;
+            const float sxv = (a & 1) ? fx[p].y : fx[p].x, syv = (a & 1) ? fy[p].y : fy[p].x,
+                        szv = (a & 1) ? fz[p].y : fz[p].x;
+            vx[a] = mine ? __float2ll_rn(sxv * kTwoPow32) : 0ll;
+            vy[a] = mine ? __float2ll_rn(syv * kTwoPow32) : 0ll;
+            vz[a] = mine ? __float2ll_rn(szv * kTwoPow32) : 0ll;
+        }
+        const long long Fx = reduce_scatter8(vx, lane), Fy = reduce_scatter8(vy, lane),
+                        Fz = reduce_scatter8(vz, lane);
+        const int va = lane >> 2;
+        if ((lane & 3) == 0)
+        {
+            if (HALF)
+            {
+                unsigned long long* fa = (unsigned long long*)(facc + 3 * (size_t)(s0 + va));
+                if (Fx) atomicAdd(fa + 0, (unsigned long long)Fx);
+                if (Fy) atomicAdd(fa + 1, (unsigned long long)Fy);
+                if (Fz) atomicAdd(fa + 2, (unsigned long long)Fz);
+            }
+            else
+            {
+                const int ai = slot_atom[s0 + va];
+                if (ai >= 0)
+                {
+                    // complete: one add per component and call
+                    atomicAdd(&frc[ai].x, (float)((double)Fx * kForceUnscale));
+                    atomicAdd(&frc[ai].y, (float)((double)Fy * kForceUnscale));
+                    atomicAdd(&frc[ai].z, (float)((double)Fz * kForceUnscale));
+                }
+            }
+        }
+        if (EN && !PA)
+        {
+            float ev[8];
+#pragma unroll
+            for (int q = 0; q < 8; q++) ev[q] = acc[q].x + acc[q].y;
+            const float esum = reduce_scatter8(ev, lane);
+            if ((lane & 3) == 0)
+            {
+                // each pair once; the virial is -g (x) d, its symmetric
+                // off-diagonal terms (xy + yx etc.) twice the one accumulated
+                const double sc = va == 0 ? (double)kLjEnergyScale
+                                          : (va == 1 ? 1.0 : ((va == 3 || va == 5 || va == 6) ? -2.0 : -1.0));
+                red[w][va] += __double2ll_rn((double)esum * sc * kEnergyScale);
+            }
+        }
+        if (PA)
+        {
+#pragma unroll
+            for (int a = 0; a < 8; a++)
+            {
+                const int p = (a % NI) / 2;
+                const bool mine = (a / NI) == sub;
+                float v[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                {
+                    const float sg = q >= 2 ? -1.0f : (q == 0 ? kLjEnergyScale : 1.0f);
+                    v[q] = mine ? sg * ((a & 1) ? own[p][q].y : own[p][q].x) : 0.0f;
+                }
+                // lanes 4q..4q+3 end with value q of atom a; an atom's energy is
+                // value 0 + value 1 (lanes 0 and 4)
+                const float val = reduce_scatter8(v, lane);
+                const float ec_val = __shfl_down_sync(0xffffffffu, val, 4);
+                if ((lane & 3) == 0)
+                {
+                    const bool twice = va == 3 || va == 5 || va == 6;
+                    red[w][va] += __double2ll_rn((double)val * (twice ? 2.0 : 1.0) * kEnergyScale);
+                    const int ai = slot_atom[s0 + a];
+                    if (ai >= 0)
+                    {
+                        const int o = om.remap(ai);
+                        if (va == 0)
+                        {
+                            if (pa.energy) atomicAdd(pa.energy + o, val + ec_val);
+                            if (pa.lj_energy) atomicAdd(pa.lj_energy + o, val);
+                        }
+                        else if (va == 1)
+                        {
+                            if (pa.direct) atomicAdd(pa.direct + o, val);
+                        }
+                        else if (pa.virial)
+                            atomicAdd(pa.virial + 6 * (size_t)o + (va - 2), twice ? 2.0f * val : val);
+                    }
+                }
+            }
+        }
+    }
+    __syncwarp();
+    if (EN && lane == 0 && cur_sys >= 0)
+        for (int q = 0; q < 8; q++)
+        {
+            const long long v = red[w][q];
+            if (v) atomicAdd((unsigned long long*)&totals[8 * cur_sys + q], (unsigned long long)v);
+        }
+    // the last block resets the cluster counter for the next launch
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        is_last = atomicAdd(&counters[kCntPairDone], 1) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (is_last && threadIdx.x == 0)
+    {
+        counters[kCntPairNext] = 0;
+        counters[kCntPairDone] = 0;
+    }
+}
+
+// Finishing pass, one thread per slot: the half-list kernel's int64 force
+// sums go to the caller's float array (and are cleared for the next call),
+// and with the fused PME excluded-pair correction each atom adds its excluded
+// pairs' terms (Particle_Mesh::PME_Excluded_Force_With_Atom_Energy,
+// PM_force.cpp:918-997): its symmetric exclusion list holds both sides of
+// every pair, so each atom computes its own share, F_a += q_a q_x beta^3
+// h(beta r) dr with dr = the reference's minimum image of r_x - r_a, and the
+// pair's owner (lower global index) adds -q_a q_x erf(beta r)/r to the energy
+// and -F (x) dr to its virial.  A thread touches only its own atom's entries.
+template <bool EXCL, bool EN>
+__global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* __restrict__ cl_sys,
+                       const SysDesc* __restrict__ sys, long long* __restrict__ facc, float3* __restrict__ frc,
+                       ExclFuse xf)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    float ene = 0.0f;
+    if (s < slots)
+    {
+        const int a = slot_atom[s];
+        long long x = 0, y = 0, z = 0;
+        if (facc)
+        {
+            long long* q = facc + 3 * (size_t)s;
+            x = q[0];
+            y = q[1];
+            z = q[2];
+            if (x | y | z)
+            {
+                q[0] = 0;
+                q[1] = 0;
+                q[2] = 0;
+            }
+        }
+        if (a >= 0)
+        {
+            float fx = (float)((double)x * kForceUnscale), fy = (float)((double)y * kForceUnscale),
+                  fz = (float)((double)z * kForceUnscale);
+            if (EXCL)
+            {
+                const SysDesc& D = sys[cl_sys[s >> 3]];
+                const int2 sn = xf.sn[a];
+                const float3 ri = xf.crd[a];
+                const float qa = xf.charge[a];
+                const int ga = xf.atom_local[a];
+                float wv[6] = {0, 0, 0, 0, 0, 0};
+                float eown = 0.0f;
+                for (int k = 0; k < sn.y; k++)
+                {
+                    const int jx = xf.list[sn.x + k];
+                    const float3 rj = xf.crd[jx];
+                    float ex = rj.x - ri.x, ey = rj.y - ri.y, ez = rj.z - ri.z;
+                    const float tx = floorf(ex * D.rcell.a11 + ey * D.rcell.a21 + ez * D.rcell.a31 + 0.5f);
+                    const float ty = floorf(ey * D.rcell.a22 + ez * D.rcell.a32 + 0.5f);
+                    const float tz = floorf(ez * D.rcell.a33 + 0.5f);
+                    ex -= tx * D.cell.a11 + ty * D.cell.a21 + tz * D.cell.a31;
+                    ey -= ty * D.cell.a22 + tz * D.cell.a32;
+                    ez -= tz * D.cell.a33;
+                    const float er = sqrtf(ex * ex + ey * ey + ez * ez);
+                    const float xb = xf.beta * er;
+                    const float qq = qa * xf.charge[jx];
+                    const float fa = qq * xf.beta3 * excl_h(xb);
+                    const float gx = fa * ex, gy = fa * ey, gz = fa * ez;
+                    fx += gx;
+                    fy += gy;
+                    fz += gz;
+                    if (EN && ga < xf.atom_local[jx])
+                    {
+                        eown -= qq * erff(xb) / er;
+                        wv[0] -= gx * ex;
+                        wv[1] -= gx * ey + gy * ex;
+                        wv[2] -= gy * ey;
+                        wv[3] -= gx * ez + gz * ex;
+                        wv[4] -= gy * ez + gz * ey;
+                        wv[5] -= gz * ez;
+                    }
+                }
+                if (EN)
+                {
+                    ene = eown;
+                    if (xf.energy && eown != 0.0f) atomicAdd(xf.energy + a, eown);
+                    if (xf.virial && sn.y > 0)
+                        for (int q = 0; q < 6; q++) atomicAdd(xf.virial + 6 * (size_t)a + q, wv[q]);
+                }
+            }
+            if (fx != 0.0f || fy != 0.0f || fz != 0.0f)
+            {
+                float3 f = frc[a];
+                f.x += fx;
+                f.y += fy;
+                f.z += fz;
+                frc[a] = f;
+            }
+        }
+    }
+    if (EXCL && EN)
+    {
+        // the correction's energy total: one atomic per warp
+        long long qe = __double2ll_rn((double)ene * kEnergyScale);
+        for (int o = 16; o > 0; o >>= 1) qe += __shfl_xor_sync(0xffffffffu, qe, o);
+        if ((threadIdx.x & 31) == 0 && qe) atomicAdd((unsigned long long*)xf.total, (unsigned long long)qe);
+    }
+}
+
+// A persistent grid: as many blocks as can be resident on every SM.
+template <typename K>
+int resident_blocks(K kernel, int threads, size_t smem)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+        per_sm <= 0)
+    {
+        cudaGetLastError();
+        per_sm = 4;
+    }
+    return per_sm * num_sms();
+}
+
+template <int M, int F, bool T, bool H>
+int launch_pair(const ForceInputs& in, cudaStream_t s)
+{
+    const spgnb_nl* nl = in.nl;
+    const int grid = std::max(1, std::min(resident_blocks(k_pair8<M, F, T, H>, kPairWarps * 32, 0),
+                                          (nl->clusters_cap + kPairWarps - 1) / kPairWarps));
+    k_pair8<M, F, T, H><<<grid, kPairWarps * 32, 0, s>>>(
+        in.p0, in.d_fps, nl->d_sys, nl->clusters_cap, kClusterSize * nl->slot_cap, nl->d_cl_sys, nl->d_pcount,
+        nl->d_pwords, nl->d_slot_atom, nl->d_cl_q, in.slot_pos, in.slot_aux, in.t4, in.frc, nl->d_facc, in.totals,
+        in.om, in.pa, in.only, nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_pair8");
+    return SPGNB_OK;
+}
+
+template <int M, int F>
+int launch_pair_t(const ForceInputs& in, bool tri, cudaStream_t s)
+{
+    constexpr bool H = M < 2;
+    return tri ? launch_pair<M, F, true, H>(in, s) : launch_pair<M, F, false, H>(in, s);
+}
+
+template <int M>
+int launch_pair_ft(const ForceInputs& in, bool tri, cudaStream_t s)
+{
+    return in.fit ? launch_pair_t<M, 1>(in, tri, s) : launch_pair_t<M, 0>(in, tri, s);
+}
+
+}  // namespace
+
+int build_t4(const float2* table, int T, float4** d_t4)
+{
+    std::vector<float4> t4((size_t)T * T * T);
+    for (int a = 0; a < T; a++)
+        for (int b = 0; b < T; b++)
+            for (int j = 0; j < T; j++)
+            {
+                const float2 ga = table[(size_t)a * T + j], gb = table[(size_t)b * T + j];
+                t4[((size_t)a * T + b) * T + j] = make_float4(-ga.x, -gb.x, ga.y, gb.y);
+            }
+    dfree(*d_t4);
+    int st = dalloc(d_t4, t4.size());
+    if (st) return st;
+    SPGNB_CUDA(cudaMemcpy(*d_t4, t4.data(), sizeof(float4) * t4.size(), cudaMemcpyHostToDevice));
+    return SPGNB_OK;
+}
+
+int force_pipeline(const ForceInputs& in, cudaStream_t s)
+{
+    spgnb_nl* nl = in.nl;
+    const int slots = nl->clusters_cap * kClusterSize;
+    const bool track = nl->opt.prune_buffer > 0.0f;
+    const float half = 0.5f * nl->opt.prune_buffer;
+    if (!in.t4) return fail(SPGNB_E_STATE, "force: the LJ module has no pair table");
+    if (in.p0.n_types <= 0 || in.p0.n_types > kMaxTypes)
+        return fail(SPGNB_E_UNSUPPORTED, "force: %d LJ types (at most %d)", in.p0.n_types, kMaxTypes);
+    k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_slot_gid,
+                                                     nl->d_cl_sys, nl->d_sys, nl->d_cl_q, nl->d_slot_x0,
+                                                     nl->d_slot_d0, in.crd, in.charge, in.atom_type, in.slot_pos,
+                                                     in.slot_aux, track ? nl->d_pref : nullptr, half * half,
+                                                     nl->d_prune);
+    SPGNB_CHECK_LAUNCH("k_pack_slots");
+    const int grid = std::max(1, std::min(num_sms() * 5, (nl->clusters_cap + kPruneWarps - 1) / kPruneWarps));
+    k_prune8<<<grid, kPruneWarps * 32, 0, s>>>(in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters,
+                                               nl->clusters_cap, nl->table_cap, kClusterSize * nl->slot_cap,
+                                               nl->d_cl_sys, nl->d_sys, nl->d_tcount, nl->d_tab, nl->d_tmask,
+                                               in.slot_pos, nl->d_pref, nl->d_pcount, nl->d_pwords, nl->S,
+                                               nl->d_prune);
+    SPGNB_CHECK_LAUNCH("k_prune8");
+    cudaEvent_t ev0, ev1;
+    pair_events(&ev0, &ev1);
+    if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
+    int st;
+    if (in.mode == 0)
+        st = launch_pair_ft<0>(in, nl->triclinic, s);
+    else if (in.mode == 1)
+        st = launch_pair_ft<1>(in, nl->triclinic, s);
+    else
+        st = launch_pair_ft<2>(in, nl->triclinic, s);
+    if (st) return st;
+    if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
+    const bool half_list = in.mode < 2;
+    const bool excl = in.xf.list != nullptr;
+    if (half_list || excl)
+    {
+        long long* facc = half_list ? nl->d_facc : nullptr;
+        const int blocks = (slots + 255) / 256;
+        if (excl && in.mode >= 1)
+            k_fin8<true, true><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, facc, in.frc,
+                                                      in.xf);
+        else if (excl)
+            k_fin8<true, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, facc,
+                                                       in.frc, in.xf);
+        else
+            k_fin8<false, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, facc,
+                                                        in.frc, in.xf);
+        SPGNB_CHECK_LAUNCH("k_fin8");
+    }
+    return SPGNB_OK;
+}
+
+}  // namespace spgnb

@@ -96,6 +96,8 @@ enum Counter
     kCntPWordsLast = 16,  // 64-bit: words of the last completed pruning (slots 16,17)
     kCntPruneNext = 18,   // the next cluster a warp of the running prune kernel takes
     kCntSearchNext = 19,  // the next cluster a warp of the running search kernel takes
+    kCntPairNext = 20,    // the next cluster a warp of the running force kernel takes
+    kCntPairDone = 21,    // blocks of the running force kernel that finished
     kCntSize = 24
 };
 
@@ -146,12 +148,12 @@ struct SysDesc
 struct ForceParams
 {
     float rc2, beta, beta3, w_scale;
-    int use_fit, n_types, table_begin, pad;
+    int use_fit, n_types, table_begin, t4_begin;  // t4_begin: first element of the system's T^3 table
 };
 
 constexpr int kMaxSlots = 1 << 23;   // slots of one list (int offsets into the per-slot regions)
 constexpr int kMaxSystemSlots = 1 << 22;  // slots of one system: the partner field of a pruned-list word
-constexpr int kMaxTypes = 128;       // LJ type field (7 bits) of a pruned-list word
+constexpr int kMaxTypes = 128;       // LJ type field (7 bits) of a slot's aux record
 
 }  // namespace spgnb
 
@@ -288,10 +290,13 @@ struct spgnb_nl
     int* d_tcount = nullptr;      // elements of each cluster's table
     float4* d_tab = nullptr;      // {D = centre difference (minimum image), neighbour slot base | image flag << 30}
     uint2* d_tmask = nullptr;     // 64-bit pair mask: bit a*8 + b = own slot a with neighbour slot b
-    // pruned per-atom lists, slot_cap words reserved per slot, one 32-bit word
-    // per pair: partner slot | image flag << 31, padded to 64-word windows
+    // pruned per-cluster partner lists, 8 * slot_cap words reserved per
+    // cluster: {partner slot | atom mask << 22 | image flag << 30}, an upper
+    // part from the start and a lower part from the end, each padded to
+    // 32-word windows; their lengths at d_pcount[8c], d_pcount[8c + 1]
     unsigned* d_pwords = nullptr;
     int* d_pcount = nullptr;
+    long long* d_facc = nullptr;  // per slot: the half-list kernel's int64 force sums (3), cleared after use
     float4* d_pref = nullptr;     // slot offsets at the last pruning
     int* d_counters = nullptr;
     // reference-layout export
@@ -311,6 +316,7 @@ struct spgnb_lj
     int* d_local_type = nullptr;     // types of local atoms (Get_Local)
     const int* d_atom_local = nullptr;  // caller's local -> global map (Get_Local)
     float2* d_table = nullptr;       // T*T square table {A, B}
+    float4* d_t4 = nullptr;          // T^3 table: {-A(a,j), -A(b,j), B(a,j), B(b,j)} at (a*T + b)*T + j
     float* d_lj_energy_atom = nullptr;
     long long* d_frc_acc = nullptr;  // 4 x int64 per local atom (reference-layout path)
     long long* d_totals = nullptr;   // 8 x int64 fixed point
@@ -322,7 +328,7 @@ struct spgnb_lj
     int* d_pos_type = nullptr;
     int pos_cap = 0;
     float4* d_sdata = nullptr;       // spgnb list: per-step slot offsets and charges (+ the null slot)
-    int* d_slot_type = nullptr;
+    int4* d_slot_aux = nullptr;      // per slot: {centre x | LJ type << 22, centre y, centre z, global index}
     int sdata_cap = 0;
     int local_atoms = 0;
     bool have_energy = false, have_virial = false;
@@ -437,12 +443,11 @@ struct ForceInputs
     const float* charge = nullptr;
     const int* atom_type = nullptr;    // into the LJ table
     float4* slot_pos = nullptr;        // scratch, slots + 1
-    int* slot_type = nullptr;          // scratch, slots + 1
+    int4* slot_aux = nullptr;          // scratch, slots + 1
     ForceParams p0{};                  // the one system's parameters (d_fps null)
     const ForceParams* d_fps = nullptr;  // per system (several systems)
     bool fit = true;                   // every system inside the rational fits' range
-    const float2* table = nullptr;     // T x T {A, B}
-    int table_size = 0;
+    const float4* t4 = nullptr;        // the T^3 pair table (build_t4)
     float3* frc = nullptr;             // += forces
     long long* totals = nullptr;       // 8 fixed-point sums per system (mode >= 1)
     const int* only = nullptr;         // per-system flags: evaluate these systems only (null: all)
@@ -452,7 +457,9 @@ struct ForceInputs
     ExclFuse xf{};                     // one system only
 };
 int force_pipeline(const ForceInputs& in, cudaStream_t s);
-int force_kernels_init(int table_size);
+// Uploads the T^3 table the force kernel reads from a T x T {A, B} table:
+// element (a*T + b)*T + j is {-A(a,j), -A(b,j), B(a,j), B(b,j)}.
+int build_t4(const float2* table, int T, float4** d_t4);
 // Adds the module's int64 force accumulators of atoms [0, n) to frc and
 // clears them (the reference-layout and correction paths end with it).
 int lj_finalize_forces(spgnb_lj* lj, int n, float3* frc, cudaStream_t s);

@@ -969,6 +969,7 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_tmask);
     dfree(nl->d_pwords);
     dfree(nl->d_pcount);
+    dfree(nl->d_facc);
     dfree(nl->d_pref);
     dfree(nl->d_counters);
     dfree(nl->d_nl);
@@ -1097,6 +1098,8 @@ int alloc_nl(spgnb_nl* nl)
     if ((st = dalloc(&nl->d_slot_count, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_slot_count, 0, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_pcount, slots))) return st;
+    if ((st = dalloc(&nl->d_facc, 3 * (size_t)slots))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_facc, 0, sizeof(long long) * 3 * (size_t)slots));
     if ((st = dalloc(&nl->d_pref, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_pcount, 0, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_cl_cell, nl->clusters_cap))) return st;

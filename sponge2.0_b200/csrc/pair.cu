@@ -17,14 +17,12 @@
 #include <vector>
 
 #include "common.cuh"
+#include "pairfn.cuh"
 
 namespace spgnb
 {
 namespace
 {
-
-constexpr int kForceWarps = 8;  // warps per block of the full-list kernel: one cluster per block pass
-constexpr float kTwoPow32 = 4294967296.0f;
 
 using PairConst = ForceParams;
 
@@ -78,941 +76,6 @@ __device__ __forceinline__ void red_fixed(long long* acc, float v)
 {
     long long q = __float2ll_rn(v * kTwoPow32);
     if (q != 0) atomicAdd((unsigned long long*)acc, (unsigned long long)q);
-}
-
-// Per-step slot pack: each slot's offset from the build-time cluster centre
-// moved by the displacement since the build (minimum image in the system's
-// box, so a caller that wraps coordinates between builds is fine), with the
-// charge, and its LJ type.  Slot slots_cap is a null slot: 10^4 A away from
-// everything, charge 0.  With pruning on
-// (pref set) the kernel also flags a re-pruning when some atom moved more
-// than half the prune buffer since the last one.
-__global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict__ slot_atom,
-                             const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
-                             const float4* __restrict__ x0, const float4* __restrict__ d0,
-                             const float3* __restrict__ crd, const float* __restrict__ charge,
-                             const int* __restrict__ local_type, float4* __restrict__ pos, int* __restrict__ ptype,
-                             const float4* __restrict__ pref, float half_buffer2, int* __restrict__ prune)
-{
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    bool moved = false;
-    if (s == slots_cap)
-    {
-        pos[s] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
-        ptype[s] = 0;
-    }
-    else if (s < slots_cap)
-    {
-        const int a = slot_atom[s];
-        const float4 d = d0[s];
-        float4 p = make_float4(d.x, d.y, d.z, 0.0f);
-        int t = 0;
-        if (a >= 0)
-        {
-            const SysDesc& D = sys[cl_sys[s >> 3]];
-            const float3 c = crd[a];
-            const float4 o = x0[s];
-            float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
-            const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
-            const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
-            const float sz = rintf(dz * D.rcell.a33);
-            dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
-            dy -= sy * D.cell.a22 + sz * D.cell.a32;
-            dz -= sz * D.cell.a33;
-            p = make_float4(d.x + dx, d.y + dy, d.z + dz, charge[a]);
-            t = local_type[a];
-            if (pref)
-            {
-                const float4 r = pref[s];
-                const float ex = p.x - r.x, ey = p.y - r.y, ez = p.z - r.z;
-                moved = ex * ex + ey * ey + ez * ez > half_buffer2;
-                if (moved) prune[cl_sys[s >> 3]] = 1;
-            }
-        }
-        pos[s] = p;
-        ptype[s] = t;
-    }
-    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) counters[kCntPrune] = 1;
-}
-
-// Pruning (no reference counterpart; results unchanged).  Runs after every
-// rebuild and whenever some atom of a system moved more than buffer/2 since
-// its last one (the pack kernel checks).  The lists belong to slot pairs: the
-// two atoms of slots 2p and 2p+1 of a cluster share one list, the union of
-// their partners within cutoff + buffer, so the force kernel evaluates both
-// atoms against each partner it loads.  One warp per cluster walks its
-// neighbour table, expands the union of the eight atoms' mask rows 32
-// elements at a time into shared memory, loads each candidate partner once,
-// tests it against all eight atoms without branches (packed FP32x2, two atoms
-// an instruction) and keeps, for each of the four slot pairs in table order, every partner
-// within cutoff + buffer of either of the pair's atoms, as a 32-bit word
-//   {partner slot - system's first slot (22 bits) | LJ type << 22 |
-//    pairs with the first atom << 29 | with the second << 30 | image flag << 31}
-// (an atom's bit is clear for itself, its exclusions and other
-// non-partners).  The list is padded to a multiple of 32 words with words
-// whose atom bits are clear.  Any pair within the cutoff before the next
-// pruning was within cutoff + buffer at this one, so the copy misses none.
-// buffer <= 0 keeps every listed pair.  The last block to finish clears the
-// flags.
-constexpr int kPruneWarps = 8;
-constexpr int kWindow = 32;                    // lists are padded to whole 32-word windows
-constexpr int kWordSlotBits = 22;                  // partner slot field of a list word
-constexpr unsigned kWordSlotMask = (1u << kWordSlotBits) - 1u;
-constexpr int kWordTypeShift = 22;                 // 7-bit LJ type
-constexpr unsigned kWordFirst = 1u << 29, kWordSecond = 1u << 30, kWordImage = 1u << 31;
-
-__device__ __forceinline__ float3 pair_offset(float ex, float ey, float ez, float4 pi, float4 pj, bool image,
-                                              const SysDesc& D)
-{
-    float dx = (ex - pi.x) + pj.x;
-    float dy = (ey - pi.y) + pj.y;
-    float dz = (ez - pi.z) + pj.z;
-    if (image)
-    {
-        const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
-        const float sy = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
-        const float sz = rintf(dz * D.rcell.a33);
-        dx -= sx * D.cell.a11 + sy * D.cell.a21 + sz * D.cell.a31;
-        dy -= sy * D.cell.a22 + sz * D.cell.a32;
-        dz -= sz * D.cell.a33;
-    }
-    return make_float3(dx, dy, dz);
-}
-
-// Transpose of an 8x8 bit matrix held as 64 bits, row r in byte r (bit 8r + c
-// moves to bit 8c + r): three rounds of swapping off-diagonal blocks of
-// 1x1, 2x2 and 4x4 bits (H. S. Warren, Hacker's Delight, 2nd ed., section 7-3).
-__device__ __forceinline__ unsigned long long transpose8x8(unsigned long long x)
-{
-    unsigned long long t = (x ^ (x >> 7)) & 0x00AA00AA00AA00AAull;
-    x ^= t ^ (t << 7);
-    t = (x ^ (x >> 14)) & 0x0000CCCC0000CCCCull;
-    x ^= t ^ (t << 14);
-    t = (x ^ (x >> 28)) & 0x00000000F0F0F0F0ull;
-    x ^= t ^ (t << 28);
-    return x;
-}
-
-__global__ void __launch_bounds__(kPruneWarps * 32)
-    k_prune(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, int clusters_cap,
-            int table_cap, int slot_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
-            const int* __restrict__ tcount, const float4* __restrict__ tab, const uint2* __restrict__ tmask,
-            const float4* __restrict__ pos, const int* __restrict__ ptype, float4* __restrict__ pref,
-            int* __restrict__ pcount, unsigned* __restrict__ pwords, int n_sys, int* __restrict__ prune)
-{
-    if (counters[kCntPrune] == 0) return;
-    // a chunk's candidates {partner slot | image flag, element lane | own-atom bits << 5}
-    __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];
-    __shared__ float4 own_all[kPruneWarps][kClusterSize];
-    // the cluster's atoms negated, per coordinate, as the four slot pairs'
-    // {first, second} float2
-    __shared__ __align__(16) float nown_all[kPruneWarps][3][kClusterSize];
-    __shared__ float4 ent_all[kPruneWarps][32];  // the window's table elements (centre differences)
-    __shared__ unsigned long long kept_total;
-    const int lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;
-    if (threadIdx.x == 0) kept_total = 0;
-    __syncthreads();
-    uint2* __restrict__ mybuf = buf[w];
-    float4* __restrict__ own = own_all[w];
-    const float2* __restrict__ nown = reinterpret_cast<const float2*>(&nown_all[w][0][0]);
-    float4* __restrict__ ent = ent_all[w];
-    // one warp per cluster, taken from a shared counter (tables differ in
-    // length): each candidate partner is loaded once and tested against the
-    // cluster's eight atoms, feeding the four slot pairs' lists
-    for (;;)
-    {
-        int c = 0;
-        if (lane == 0) c = atomicAdd(&counters[kCntPruneNext], 1);
-        c = __shfl_sync(0xffffffffu, c, 0);
-        if (c >= clusters_cap) break;
-        const int sy = cl_sys[c];
-        if (!prune[sy]) continue;
-        const int s0 = c * kClusterSize;
-        if (lane < kClusterSize)
-        {
-            const float4 pl = pos[s0 + lane];
-            own[lane] = pl;
-            nown_all[w][0][lane] = -pl.x;
-            nown_all[w][1][lane] = -pl.y;
-            nown_all[w][2][lane] = -pl.z;
-            pref[s0 + lane] = pl;
-        }
-        __syncwarp();
-        const SysDesc& D = sys[sy];
-        const unsigned slot0 = (unsigned)D.cl_begin * kClusterSize;
-        const ForceParams P = fps ? fps[sy] : p0;
-        const float rp = sqrtf(P.rc2) + buffer + 1e-3f;
-        const float rp2 = buffer > 0.0f ? rp * rp : 3.0e38f;
-        const int T = tcount[c];
-        const float4* __restrict__ tb = tab + (size_t)c * table_cap;
-        const uint2* __restrict__ tm = tmask + (size_t)c * table_cap;
-        const int usable = 2 * slot_cap - kWindow;
-        int kept[4] = {0, 0, 0, 0};
-        for (int t0 = 0; t0 < T; t0 += 32)
-        {
-            const int t = t0 + lane;
-            uint2 mm = make_uint2(0u, 0u);
-            float4 e = make_float4(0, 0, 0, 0);
-            if (t < T)
-            {
-                e = tb[t];
-                mm = tm[t];
-            }
-            // partners of any of the eight atoms
-            unsigned u = mm.x | mm.y;
-            u |= u >> 16;
-            u |= u >> 8;
-            const unsigned row = u & 0xffu;
-            const int cnt = __popc(row);
-            int incl = cnt;
-            for (int o = 1; o < 32; o <<= 1)
-            {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            const int eb = __float_as_int(e.w);
-            const unsigned flag = (eb & (1 << 30)) ? kWordImage : 0u;
-            const unsigned base = (unsigned)(eb & 0x3fffffff) | flag;
-            int k = incl - cnt;
-            // own atom a pairs with neighbour slot b when bit 8a + b is set;
-            // transposed, byte b holds neighbour b's own-atom bits
-            const unsigned long long tm8 = transpose8x8(((unsigned long long)mm.y << 32) | mm.x);
-            ent[lane] = e;
-#pragma unroll
-            for (int b = 0; b < kClusterSize; b++)
-                if ((row >> b) & 1u)
-                {
-                    const unsigned am = (unsigned)(tm8 >> (8 * b)) & 0xffu;
-                    mybuf[k++] = make_uint2(base + b, (unsigned)lane | (am << 5));
-                }
-            __syncwarp();
-            for (int q0 = 0; q0 < total; q0 += 32)
-            {
-                const int q = q0 + lane;
-                const uint2 wv = mybuf[q < total ? q : 0];
-                // the element's centre difference, staged by the lane that read it
-                const float4 es = ent[wv.y & 31u];
-                const float ex = es.x, ey = es.y, ez = es.z;
-                const unsigned am = q < total ? (wv.y >> 5) & 0xffu : 0u;
-                const int js = (int)(wv.x & 0x7fffffffu);
-                const bool img = (wv.x & 0x80000000u) != 0;
-                float4 pj = make_float4(0, 0, 0, 0);
-                int tj = 0;
-                if (am)
-                {
-                    pj = pos[js];
-                    tj = ptype[js];
-                }
-                const unsigned wbase =
-                    ((unsigned)js - slot0) | ((unsigned)tj << kWordTypeShift) | (img ? kWordImage : 0u);
-                // bit a: own atom a lies within the pruning radius of the
-                // partner.  All eight are tested without branches; the
-                // minimum-image path (small boxes) only when a lane needs it.
-                unsigned hit = 0;
-                if (!__any_sync(0xffffffffu, img && am != 0u))
-                {
-                    // the partner in the cluster's frame, then two own atoms
-                    // at a time in packed FP32x2
-                    const float2 cx = make_float2(ex + pj.x, ex + pj.x), cy = make_float2(ey + pj.y, ey + pj.y),
-                                 cz = make_float2(ez + pj.z, ez + pj.z);
-#pragma unroll
-                    for (int p = 0; p < 4; p++)
-                    {
-                        const float2 dx = __fadd2_rn(cx, nown[p]), dy = __fadd2_rn(cy, nown[4 + p]),
-                                     dz = __fadd2_rn(cz, nown[8 + p]);
-                        const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-                        hit |= ((r2.x < rp2 ? 1u : 0u) | (r2.y < rp2 ? 2u : 0u)) << (2 * p);
-                    }
-                }
-                else
-                {
-#pragma unroll 1
-                    for (int a = 0; a < kClusterSize; a++)
-                    {
-                        const float3 d = pair_offset(ex, ey, ez, own[a], pj, img, D);
-                        if (__fmaf_rn(d.z, d.z, __fmaf_rn(d.y, d.y, d.x * d.x)) < rp2) hit |= 1u << a;
-                    }
-                }
-                hit &= am;
-#pragma unroll
-                for (int p = 0; p < 4; p++)
-                {
-                    // kept when either atom of the slot pair is in range; the
-                    // word's atom bits stay those of the full list
-                    const bool keep = ((hit >> (2 * p)) & 3u) != 0u;
-                    const unsigned m = __ballot_sync(0xffffffffu, keep);
-                    if (keep)
-                    {
-                        const int kk = kept[p] + __popc(m & ((1u << lane) - 1u));
-                        if (kk < usable)
-                            pwords[(size_t)(s0 + 2 * p) * slot_cap + kk] = wbase | (((am >> (2 * p)) & 3u) << 29);
-                        else
-                            atomicOr(&counters[kCntOverflow], kOvfWords);
-                    }
-                    kept[p] += __popc(m);
-                }
-            }
-            __syncwarp();
-        }
-        // pad to whole windows: the first atom against itself, no atom bit set
-        unsigned long long kept_sum = 0;
-#pragma unroll
-        for (int p = 0; p < 4; p++)
-        {
-            const int s1 = s0 + 2 * p;
-            const int kp = min(kept[p], usable);
-            const int padded = (kp + kWindow - 1) & ~(kWindow - 1);
-            for (int k2 = kp + lane; k2 < padded; k2 += 32) pwords[(size_t)s1 * slot_cap + k2] = (unsigned)s1 - slot0;
-            if (lane == 0)
-            {
-                pcount[s1] = padded;
-                pcount[s1 + 1] = 0;
-            }
-            kept_sum += (unsigned long long)kp;
-        }
-        if (lane == 0) atomicAdd(&kept_total, kept_sum);
-        __syncwarp();
-    }
-    __shared__ int is_last;
-    __syncthreads();
-    if (threadIdx.x == 0)
-    {
-        atomicAdd((unsigned long long*)&counters[kCntPWords], kept_total);
-        __threadfence();
-        is_last = atomicAdd(&counters[kCntPruneDone], 1) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!is_last) return;
-    for (int q = threadIdx.x; q < n_sys; q += blockDim.x) prune[q] = 0;
-    if (threadIdx.x == 0)
-    {
-        unsigned long long* wp = (unsigned long long*)&counters[kCntPWords];
-        *(unsigned long long*)&counters[kCntPWordsLast] = atomicExch(wp, 0ull);
-        counters[kCntPruneDone] = 0;
-        counters[kCntPruneNext] = 0;
-        counters[kCntPrune] = 0;
-        counters[kCntPrunes] += 1;
-    }
-}
-
-// ------------------------------------------------ packed FP32x2 pair math
-__device__ __forceinline__ float2 f2(float x) { return make_float2(x, x); }
-
-// Fixed (c, c) constants of the packed arithmetic in constant memory, so the
-// FP32x2 instructions read them as constant-bank operands instead of
-// building register pairs each time.
-static __constant__ float2 kPk[1] = {{-1.0f, -1.0f}};
-enum PackedConst
-{
-    kPkMinusOne = 0
-};
-// pair_scalar2's LJ energy is -12 times the energy (A/(12 r^12) - B/(6 r^6)):
-// the kernels scale the sums once
-constexpr float kLjEnergyScale = -1.0f / 12.0f;
-
-__device__ __forceinline__ float2 poly5x2(float2 x, const float2* c)
-{
-    float2 p = __ffma2_rn(c[5], x, c[4]);
-    p = __ffma2_rn(p, x, c[3]);
-    p = __ffma2_rn(p, x, c[2]);
-    p = __ffma2_rn(p, x, c[1]);
-    return __ffma2_rn(p, x, c[0]);
-}
-
-__device__ __forceinline__ float ex2_approx(float x)
-{
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-// The hardware approximations with subnormals flushed (PTX rsqrt.approx.ftz,
-// rcp.approx.ftz): r^2 of a listed pair and the fits' denominators (>= 1)
-// are far from the subnormal range, so the range handling of rsqrtf and
-// __fdividef is not needed.
-__device__ __forceinline__ float rsqrt_approx(float x)
-{
-    float y;
-    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-__device__ __forceinline__ float rcp_approx(float x)
-{
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-// One system's pair-function parameters as (v, v) pairs, made once per atom
-// pair and kept in registers over its list.
-struct PairParams2
-{
-    float2 w_scale, nbeta3, nbeta, beta_2_sqrtpi, nb2_log2e;
-    float rc2, beta;
-};
-
-__device__ __forceinline__ PairParams2 pack_params(const ForceParams& pc)
-{
-    PairParams2 q;
-    q.w_scale = f2(pc.w_scale);
-    q.nbeta3 = f2(-pc.beta3);
-    q.nbeta = f2(-pc.beta);
-    q.beta_2_sqrtpi = f2(pc.beta * 1.1283791670955126f);
-    q.nb2_log2e = f2(-pc.beta * pc.beta * 1.4426950408889634f);  // -w log2(e) = -beta^2 r^2 log2(e)
-    q.rc2 = pc.rc2;
-    q.beta = pc.beta;
-    return q;
-}
-
-// pair_scalar for two pairs at once; nA = -A.  Without energies the screened
-// Coulomb force uses the K fit; with energies it uses the M fit and
-// exp(-w): beta^3 K(w) = beta (M(w) - 2/sqrt(pi) exp(-w)) / r^2, so
-//   F_c/qq = (t + beta 2/sqrt(pi) exp(-w)) / r^2,  E_c/qq = t,  t = 1/r - beta M(w).
-template <bool ENERGY, int FIT>
-__device__ __forceinline__ float2 pair_scalar2(float2 r2, float2 qq, float2 nA, float2 B, const PairParams2& pc,
-                                               float2& e_lj, float2& e_c)
-{
-    // the hardware reciprocal square root alone: a Newton step on top of it
-    // moves the forces' error against FP64 by 1e-8 relative RMS and costs
-    // four packed instructions a word
-    const float2 rinv = make_float2(rsqrt_approx(r2.x), rsqrt_approx(r2.y));
-    const float2 r2inv = __fmul2_rn(rinv, rinv);
-    const float2 r6inv = __fmul2_rn(__fmul2_rn(r2inv, r2inv), r2inv);
-    // u = (-A/r^6 + B)/r^6 serves the force and, plus B/r^6, the energy
-    const float2 u = __fmul2_rn(__ffma2_rn(nA, r6inv, B), r6inv);
-    const float2 flj = __fmul2_rn(u, r2inv);
-    float2 fc;
-    if (FIT == 1)
-    {
-        const float2 x = __fmul2_rn(r2, pc.w_scale);
-        if (!ENERGY)
-        {
-            const float2 kp = poly5x2(x, kEwaldKP2), kq = poly5x2(x, kEwaldKQ2);
-            const float2 K = __fmul2_rn(kp, make_float2(rcp_approx(kq.x), rcp_approx(kq.y)));
-            fc = __fmul2_rn(qq, __ffma2_rn(pc.nbeta3, K, __fmul2_rn(rinv, r2inv)));
-        }
-        else
-        {
-            const float2 mp = poly5x2(x, kEwaldMP2), mq = poly5x2(x, kEwaldMQ2);
-            const float2 M = __fmul2_rn(mp, make_float2(rcp_approx(mq.x), rcp_approx(mq.y)));
-            const float2 wl = __fmul2_rn(r2, pc.nb2_log2e);
-            const float2 E = make_float2(ex2_approx(wl.x), ex2_approx(wl.y));
-            const float2 t = __ffma2_rn(pc.nbeta, M, rinv);
-            e_c = __fmul2_rn(qq, t);
-            fc = __fmul2_rn(__fmul2_rn(qq, r2inv), __ffma2_rn(pc.beta_2_sqrtpi, E, t));
-        }
-    }
-    else
-    {
-        float c[2], e[2];
-        const float rr[2] = {r2.x, r2.y}, ri[2] = {rinv.x, rinv.y}, q[2] = {qq.x, qq.y};
-        for (int h2 = 0; h2 < 2; h2++)
-        {
-            const float r = rr[h2] * ri[h2];
-            const float br = pc.beta * r;
-            const float erfcv = erfcf(br);
-            c[h2] = q[h2] * ri[h2] * ri[h2] * ri[h2] * __fmaf_rn(br * 1.1283791670955126f, __expf(-br * br), erfcv);
-            e[h2] = q[h2] * erfcv * ri[h2];
-        }
-        fc = make_float2(c[0], c[1]);
-        if (ENERGY) e_c = make_float2(e[0], e[1]);
-    }
-    if (ENERGY) e_lj = __ffma2_rn(B, r6inv, u);  // -A/r^12 + 2B/r^6 = -12 E_lj
-    return __ffma2_rn(fc, kPk[kPkMinusOne], flj);
-}
-
-// A difference of two 22-bit cluster-centre coordinates, wrapped to
-// [-2^21, 2^21) (minimum image of the centres) and converted exactly: the
-// wrapped value plus 2^23 + 2^21 is an integer below 2^23 + 2^22, whose float
-// bit pattern is 0x4B000000 | value.
-__device__ __forceinline__ float centre_step(int qj, int qi)
-{
-    return __int_as_float(((qj - qi + 0x200000) & 0x3fffff) | 0x4b000000) - 10485760.0f;
-}
-
-// Pruned-list force kernel.  A warp takes one slot pair (the two atoms of
-// slots 2p, 2p+1 of a cluster) at a time, strided over the grid's warps, and
-// walks the pair's shared list, one word per lane per iteration (32-word
-// windows).  The next item's header (list length, system, types, the two
-// atoms' offsets, the cluster centre) and first window are staged in shared
-// memory by cp.async while the warp works on the current one, and the list's
-// later windows are loaded kPrefetch iterations ahead.  A word names the
-// partner slot, so its offset {delta + displacement, q} and its cluster's
-// 22-bit centre load side by side, once for both atoms:
-//   dr = (c_j - c_i) * cell / 2^22 + p_j - p_{i1,i2},
-// and the two pairs are evaluated with packed FP32x2 arithmetic; the LJ
-// coefficients of both come from the warp's shared-memory row for the two
-// atoms' types {-A1, -A2, B1, B2} indexed by the partner's type.  Each
-// lane's partial forces are converted to int64 fixed point (2^-32
-// kcal/mol/A) and summed over the lanes exactly, so an atom's force does not
-// depend on the reduction order; one lane per component adds it to the
-// caller's array, once per call: bitwise reproducible.
-//
-// MODE 0: forces.  MODE 1: + energy and virial totals (each pair is seen
-// from both atoms, so the sums are halved).  MODE 2: + per-atom energy and
-// virial of the pairs the atom owns (the lower global index; water sites
-// hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES does),
-// and the totals summed from those (each pair once).
-// One item's header and first list window, staged in shared memory by
-// asynchronous copies (cp.async) while the warp works on the item before.
-struct alignas(16) ItemStage
-{
-    int n, sy, t1, t2;     // list words, system, LJ types of the two atoms
-    int4 ci;               // the cluster's 22-bit centre
-    float4 p1, p2;         // the two atoms' slot offsets and charges
-    unsigned words[32];    // first window of the list
-};
-
-__device__ __forceinline__ void cp_async(void* smem, const void* gmem, int bytes)
-{
-    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
-    if (bytes == 16)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem));
-    else if (bytes == 8)
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem));
-    else
-        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(d), "l"(gmem));
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;"); }
-__device__ __forceinline__ void cp_async_wait_prior() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
-
-// Sums eight per-lane values over the warp: after three halving exchanges
-// (lane bit 4, 3, 2 picks the half it keeps) and two full ones, lanes
-// 4v..4v+3 hold the total of value v.  Nine shuffles instead of forty.
-template <typename T>
-__device__ __forceinline__ T reduce_scatter8(const T (&v)[8], int lane)
-{
-    const bool h4 = (lane & 16) != 0, h3 = (lane & 8) != 0, h2 = (lane & 4) != 0;
-    T u[4], x[2];
-#pragma unroll
-    for (int k = 0; k < 4; k++)
-    {
-        const T send = h4 ? v[k] : v[k + 4];
-        u[k] = (h4 ? v[k + 4] : v[k]) + __shfl_xor_sync(0xffffffffu, send, 16);
-    }
-#pragma unroll
-    for (int k = 0; k < 2; k++)
-    {
-        const T send = h3 ? u[k] : u[k + 2];
-        x[k] = (h3 ? u[k + 2] : u[k]) + __shfl_xor_sync(0xffffffffu, send, 8);
-    }
-    const T send = h2 ? x[0] : x[1];
-    T y = (h2 ? x[1] : x[0]) + __shfl_xor_sync(0xffffffffu, send, 4);
-    y += __shfl_xor_sync(0xffffffffu, y, 2);
-    y += __shfl_xor_sync(0xffffffffu, y, 1);
-    return y;
-}
-
-#ifndef SPGNB_PAIR_MINB2
-#define SPGNB_PAIR_MINB2 3
-#endif
-#ifndef SPGNB_PAIR_MINB0
-#define SPGNB_PAIR_MINB0 4
-#endif
-#ifndef SPGNB_PAIR_PREFETCH
-#define SPGNB_PAIR_PREFETCH 2
-#endif
-constexpr int kPrefetch = SPGNB_PAIR_PREFETCH;  // list windows in flight per warp
-__device__ __forceinline__ float excl_h(float x);
-
-template <int MODE, int FIT, bool TRI, bool EXCL>
-__global__ void __launch_bounds__(kForceWarps * 32, MODE == 0 ? SPGNB_PAIR_MINB0 : (MODE == 1 ? 3 : SPGNB_PAIR_MINB2))
-    k_pair_fast(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys,
-                int n_clusters, int slot_cap,
-                const int* __restrict__ cl_sys, const int* __restrict__ pcount, const unsigned* __restrict__ pwords,
-                const int* __restrict__ slot_atom, const int* __restrict__ slot_gid, const int4* __restrict__ cl_q,
-                const float4* __restrict__ pos, const int* __restrict__ ptype,
-                const float2* __restrict__ gtable, int n_types, float3* __restrict__ frc,
-                long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, const int* __restrict__ only,
-                ExclFuse xf)
-{
-    extern __shared__ float4 rows_all[];        // per warp: n_types rows {-A1, -A2, B1, B2}
-    __shared__ long long red[kForceWarps][8];  // per-warp fixed-point totals (lane 0)
-    __shared__ int row_of[kForceWarps][2];     // table rows the warp's shared row was built from
-    constexpr bool EN = MODE >= 1;
-    constexpr bool PA = MODE >= 2;
-    const int lane = threadIdx.x & 31;
-    const int w = threadIdx.x >> 5;
-    float4* __restrict__ rows = rows_all + w * n_types;
-    if (EN && lane < 8) red[w][lane] = 0;
-    if (lane < 2) row_of[w][lane] = -1;
-    __syncwarp();
-    int cur_sys = -1;              // the system red[w] accumulates for
-    const int items = n_clusters * 4;
-    __shared__ ItemStage stage_all[kForceWarps][2];
-    ItemStage* stage = stage_all[w];
-    const int stride = gridDim.x * kForceWarps;
-    // stages item `it` (nothing past the end: an empty group keeps the count)
-    auto prefetch = [&](int it, ItemStage& S) {
-        if (it < items)
-        {
-            const int c = it >> 2;
-            const int s1 = c * kClusterSize + 2 * (it & 3);
-            if (lane == 0) cp_async(&S.n, pcount + s1, 4);
-            if (lane == 1) cp_async(&S.sy, cl_sys + c, 4);
-            if (lane == 2) cp_async(&S.t1, ptype + s1, 8);
-            if (lane == 3) cp_async(&S.ci, cl_q + c, 16);
-            if (lane == 4) cp_async(&S.p1, pos + s1, 16);
-            if (lane == 5) cp_async(&S.p2, pos + s1 + 1, 16);
-            cp_async(&S.words[lane], pwords + (size_t)s1 * slot_cap + lane, 4);
-        }
-        cp_async_commit();
-    };
-    int kk = 0;
-    prefetch(blockIdx.x * kForceWarps + w, stage[0]);
-    for (int it = blockIdx.x * kForceWarps + w; it < items; it += stride, kk++)
-    {
-        // every lane has read the buffer the next prefetch overwrites
-        __syncwarp();
-        prefetch(it + stride, stage[(kk + 1) & 1]);
-        cp_async_wait_prior();
-        __syncwarp();
-        const ItemStage& S = stage[kk & 1];
-        const int c = it >> 2;
-        const int s1 = c * kClusterSize + 2 * (it & 3);
-        const int n = S.n;  // a multiple of the window
-        if (n == 0) continue;
-        const int sy = S.sy;
-        if (only && !only[sy]) continue;
-        if (EN && sy != cur_sys)
-        {
-            // totals belong to one system each: flush this warp's share
-            __syncwarp();
-            if (lane == 0 && cur_sys >= 0)
-                for (int q = 0; q < 8; q++)
-                {
-                    const long long v = red[w][q];
-                    if (v) atomicAdd((unsigned long long*)&totals[8 * cur_sys + q], (unsigned long long)v);
-                    red[w][q] = 0;
-                }
-            __syncwarp();
-            cur_sys = sy;
-        }
-        const ForceParams P = fps ? fps[sy] : p0;
-        const PairParams2 pp = pack_params(P);
-        const SysDesc& D = sys[sy];
-        const Cell qc = D.qcell;
-        const int slot0 = D.cl_begin * kClusterSize;
-        const float4 pi1 = S.p1, pi2 = S.p2;
-        const int4 ci = S.ci;
-        const int r1 = S.t1 * n_types + P.table_begin, r2i = S.t2 * n_types + P.table_begin;
-        if (r1 != row_of[w][0] || r2i != row_of[w][1])
-        {
-            __syncwarp();
-            for (int t = lane; t < n_types; t += 32)
-            {
-                const float2 g1 = gtable[r1 + t], g2 = gtable[r2i + t];
-                rows[t] = make_float4(-g1.x, -g2.x, g1.y, g2.y);
-            }
-            if (lane == 0)
-            {
-                row_of[w][0] = r1;
-                row_of[w][1] = r2i;
-            }
-            __syncwarp();
-        }
-        int gi1 = 0, gi2 = 0;
-        if (PA)
-        {
-            gi1 = slot_gid[s1];
-            gi2 = slot_gid[s1 + 1];
-        }
-        const unsigned* __restrict__ wl = pwords + (size_t)s1 * slot_cap;
-        const float2 npx = make_float2(-pi1.x, -pi2.x), npy = make_float2(-pi1.y, -pi2.y),
-                     npz = make_float2(-pi1.z, -pi2.z), qi2 = make_float2(pi1.w, pi2.w);
-        float2 fx = f2(0.0f), fy = f2(0.0f), fz = f2(0.0f);
-        float2 acc[PA ? 1 : 8], own[PA ? 8 : 1];  // totals (MODE 1) or owned sums (MODE 2)
-#pragma unroll
-        for (int q = 0; q < (PA ? 1 : 8); q++) acc[q] = f2(0.0f);
-#pragma unroll
-        for (int q = 0; q < (PA ? 8 : 1); q++) own[q] = f2(0.0f);
-        // one list word: the partner against both atoms
-        auto eval_word = [&](unsigned cw, int j, float4 pj, int4 cj) {
-            const float4 ab = rows[(cw >> kWordTypeShift) & 0x7fu];
-            const float ux = centre_step(cj.x, ci.x), uy = centre_step(cj.y, ci.y), uz = centre_step(cj.z, ci.z);
-            // the partner in the frame of the pair's cluster centre
-            float sx = __fmaf_rn(ux, qc.a11, pj.x);
-            float sy2 = __fmaf_rn(uy, qc.a22, pj.y);
-            const float sz = __fmaf_rn(uz, qc.a33, pj.z);
-            if (TRI)
-            {
-                sx = __fmaf_rn(uy, qc.a21, sx);
-                sx = __fmaf_rn(uz, qc.a31, sx);
-                sy2 = __fmaf_rn(uz, qc.a32, sy2);
-            }
-            float2 dx = __fadd2_rn(f2(sx), npx), dy = __fadd2_rn(f2(sy2), npy), dz = __fadd2_rn(f2(sz), npz);
-            if (cw & kWordImage)
-            {
-                // small box: these pairs need their own image
-                float ddx[2] = {dx.x, dx.y}, ddy[2] = {dy.x, dy.y}, ddz[2] = {dz.x, dz.y};
-                for (int h = 0; h < 2; h++)
-                {
-                    const float tx = rintf(ddx[h] * D.rcell.a11 + ddy[h] * D.rcell.a21 + ddz[h] * D.rcell.a31);
-                    const float ty = rintf(ddy[h] * D.rcell.a22 + ddz[h] * D.rcell.a32);
-                    const float tz = rintf(ddz[h] * D.rcell.a33);
-                    ddx[h] -= tx * D.cell.a11 + ty * D.cell.a21 + tz * D.cell.a31;
-                    ddy[h] -= ty * D.cell.a22 + tz * D.cell.a32;
-                    ddz[h] -= tz * D.cell.a33;
-                }
-                dx = make_float2(ddx[0], ddx[1]);
-                dy = make_float2(ddy[0], ddy[1]);
-                dz = make_float2(ddz[0], ddz[1]);
-            }
-            const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
-            const bool inA = (cw & kWordFirst) && r2.x < pp.rc2;
-            const bool inB = (cw & kWordSecond) && r2.y < pp.rc2;
-            float2 elj, ec;
-            float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(f2(pj.w), qi2), make_float2(ab.x, ab.y),
-                                             make_float2(ab.z, ab.w), pp, elj, ec);
-            f = make_float2(inA ? f.x : 0.0f, inB ? f.y : 0.0f);
-            if (!EN)
-            {
-                fx = __ffma2_rn(f, dx, fx);
-                fy = __ffma2_rn(f, dy, fy);
-                fz = __ffma2_rn(f, dz, fz);
-            }
-            else
-            {
-                const float2 gx = __fmul2_rn(f, dx), gy = __fmul2_rn(f, dy), gz = __fmul2_rn(f, dz);
-                fx = __fadd2_rn(fx, gx);
-                fy = __fadd2_rn(fy, gy);
-                fz = __fadd2_rn(fz, gz);
-                if (!PA)
-                {
-                    elj = make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f);
-                    ec = make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f);
-                    acc[0] = __fadd2_rn(acc[0], elj);
-                    acc[1] = __fadd2_rn(acc[1], ec);
-                    acc[2] = __ffma2_rn(gx, dx, acc[2]);
-                    acc[3] = __ffma2_rn(gx, dy, acc[3]);
-                    acc[4] = __ffma2_rn(gy, dy, acc[4]);
-                    acc[5] = __ffma2_rn(gx, dz, acc[5]);
-                    acc[6] = __ffma2_rn(gy, dz, acc[6]);
-                    acc[7] = __ffma2_rn(gz, dz, acc[7]);
-                }
-                else
-                {
-                    // only the pair's owner (the lower global index) keeps its
-                    // energy and virial; the totals are summed from these, so
-                    // every pair counts once
-                    const int gj = __ldg(slot_gid + j);
-                    const bool oA = inA && gi1 < gj, oB = inB && gi2 < gj;
-                    own[0] = __fadd2_rn(own[0], make_float2(oA ? elj.x : 0.0f, oB ? elj.y : 0.0f));
-                    own[1] = __fadd2_rn(own[1], make_float2(oA ? ec.x : 0.0f, oB ? ec.y : 0.0f));
-                    const float2 mgx = make_float2(oA ? gx.x : 0.0f, oB ? gx.y : 0.0f);
-                    const float2 mgy = make_float2(oA ? gy.x : 0.0f, oB ? gy.y : 0.0f);
-                    const float2 mgz = make_float2(oA ? gz.x : 0.0f, oB ? gz.y : 0.0f);
-                    own[2] = __ffma2_rn(mgx, dx, own[2]);
-                    own[3] = __ffma2_rn(mgx, dy, own[3]);
-                    own[4] = __ffma2_rn(mgy, dy, own[4]);
-                    own[5] = __ffma2_rn(mgx, dz, own[5]);
-                    own[6] = __ffma2_rn(mgy, dz, own[6]);
-                    own[7] = __ffma2_rn(mgz, dz, own[7]);
-                }
-            }
-        };
-        auto partner = [&](unsigned cw) { return slot0 + (int)(cw & kWordSlotMask); };
-        // the list streams from memory: its windows are loaded kPrefetch
-        // iterations ahead of their use (a ring of registers)
-        unsigned ring[kPrefetch];
-        ring[0] = S.words[lane];
-#pragma unroll
-        for (int q = 1; q < kPrefetch; q++) ring[q] = q * 32 < n ? wl[q * 32 + lane] : 0u;
-#pragma unroll 1
-        for (int k0 = 0; k0 < n; k0 += 32)
-        {
-            const unsigned cw = ring[0];
-#pragma unroll
-            for (int q = 0; q + 1 < kPrefetch; q++) ring[q] = ring[q + 1];
-            if (k0 + kPrefetch * 32 < n) ring[kPrefetch - 1] = wl[k0 + kPrefetch * 32 + lane];
-            const int j = partner(cw);
-            eval_word(cw, j, pos[j], cl_q[j >> 3]);
-        }
-        if (EXCL)
-        {
-            // PME's excluded-pair correction for the two atoms (each atom's
-            // excluded partners on both sides, one pair per lane), as
-            // k_pme_excluded computes it; the force joins the lane's partial
-            // sums, the energy and per-atom outputs go to the pair's owner
-            // (lower global index)
-            const int a1 = slot_atom[s1], a2 = slot_atom[s1 + 1];
-            const int2 sn1 = a1 >= 0 ? xf.sn[a1] : make_int2(0, 0), sn2 = a2 >= 0 ? xf.sn[a2] : make_int2(0, 0);
-            const int n1 = sn1.y, n2 = sn2.y;
-            float eown = 0.0f;
-            for (int k = lane; k < n1 + n2; k += 32)
-            {
-                const bool sec = k >= n1;
-                const int ia = sec ? a2 : a1;
-                const int jx = xf.list[sec ? sn2.x + k - n1 : sn1.x + k];
-                const float3 ri = xf.crd[ia], rj = xf.crd[jx];
-                float ex = rj.x - ri.x, ey = rj.y - ri.y, ez = rj.z - ri.z;
-                const float tx = floorf(ex * D.rcell.a11 + ey * D.rcell.a21 + ez * D.rcell.a31 + 0.5f);
-                const float ty = floorf(ey * D.rcell.a22 + ez * D.rcell.a32 + 0.5f);
-                const float tz = floorf(ez * D.rcell.a33 + 0.5f);
-                ex -= tx * D.cell.a11 + ty * D.cell.a21 + tz * D.cell.a31;
-                ey -= ty * D.cell.a22 + tz * D.cell.a32;
-                ez -= tz * D.cell.a33;
-                const float er = sqrtf(ex * ex + ey * ey + ez * ez);
-                const float x = xf.beta * er;
-                const float qq = xf.charge[ia] * xf.charge[jx];
-                const float fa = qq * xf.beta3 * excl_h(x);
-                const float gx = fa * ex, gy = fa * ey, gz = fa * ez;
-                if (sec)
-                {
-                    fx.y += gx;
-                    fy.y += gy;
-                    fz.y += gz;
-                }
-                else
-                {
-                    fx.x += gx;
-                    fy.x += gy;
-                    fz.x += gz;
-                }
-                if (EN && xf.atom_local[ia] < xf.atom_local[jx])
-                {
-                    const float e = -qq * erff(x) / er;
-                    eown += e;
-                    if (PA)
-                    {
-                        if (xf.energy) atomicAdd(xf.energy + ia, e);
-                        if (xf.virial)
-                        {
-                            float* v = xf.virial + 6 * (size_t)ia;
-                            atomicAdd(v + 0, -gx * ex);
-                            atomicAdd(v + 1, -(gx * ey + gy * ex));
-                            atomicAdd(v + 2, -gy * ey);
-                            atomicAdd(v + 3, -(gx * ez + gz * ex));
-                            atomicAdd(v + 4, -(gy * ez + gz * ey));
-                            atomicAdd(v + 5, -gz * ez);
-                        }
-                    }
-                }
-            }
-            if (EN && n1 + n2 > 0)
-            {
-                long long qe = __double2ll_rn((double)eown * kEnergyScale);
-                for (int o = 16; o > 0; o >>= 1) qe += __shfl_xor_sync(0xffffffffu, qe, o);
-                if (lane == 0 && qe) atomicAdd((unsigned long long*)xf.total, (unsigned long long)qe);
-            }
-        }
-        // forces of both atoms: int64 fixed point per lane, summed over the
-        // lanes by a reduce-scatter (lanes 4v..4v+3 end with value v)
-        long long fq[8] = {__float2ll_rn(fx.x * kTwoPow32), __float2ll_rn(fy.x * kTwoPow32),
-                           __float2ll_rn(fz.x * kTwoPow32), __float2ll_rn(fx.y * kTwoPow32),
-                           __float2ll_rn(fy.y * kTwoPow32), __float2ll_rn(fz.y * kTwoPow32), 0, 0};
-        const long long fsum = reduce_scatter8(fq, lane);
-        const int vidx = lane >> 2;  // the value this lane holds
-        if ((lane & 3) == 0 && vidx < 6)
-        {
-            const int ai = slot_atom[s1 + (vidx >= 3 ? 1 : 0)];
-            if (ai >= 0)  // one add per component and call: the same as a read-modify-write, without the wait
-                atomicAdd(&frc[ai].x + (vidx % 3), (float)((double)fsum * kForceUnscale));
-        }
-        if (EN && !PA)
-        {
-            float ev[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++)
-                ev[q] = (q >= 2 ? -1.0f : (q == 0 ? kLjEnergyScale : 1.0f)) * (acc[q].x + acc[q].y);
-            const float esum = reduce_scatter8(ev, lane);
-            if ((lane & 3) == 0)
-            {
-                // halve the double-counted sums; the symmetric off-diagonal
-                // terms (xy + yx etc.) are twice the one accumulated
-                const double sc = (vidx == 3 || vidx == 5 || vidx == 6) ? 1.0 : 0.5;
-                red[w][vidx] += __double2ll_rn((double)esum * sc * kEnergyScale);
-            }
-        }
-        if (PA)
-        {
-            float own1[8], own2[8];
-#pragma unroll
-            for (int q = 0; q < 8; q++)
-            {
-                // the virial terms were accumulated as +g (x) d: the virial is -g (x) d
-                const float sg = q >= 2 ? -1.0f : (q == 0 ? kLjEnergyScale : 1.0f);
-                own1[q] = sg * own[q].x;
-                own2[q] = sg * own[q].y;
-            }
-            // both atoms' sums over the lanes: lanes 4q..4q+3 end with value q
-            const float a = reduce_scatter8(own1, lane), b = reduce_scatter8(own2, lane);
-            // an atom's energy is value 0 + value 1 (lanes 0 and 4)
-            const float a1 = __shfl_down_sync(0xffffffffu, a, 4), b1 = __shfl_down_sync(0xffffffffu, b, 4);
-            if ((lane & 3) == 0)
-            {
-                // the item's totals: each pair once; the symmetric off-diagonal
-                // terms (xy + yx etc.) are twice the one accumulated
-                const bool twice = vidx == 3 || vidx == 5 || vidx == 6;
-                red[w][vidx] += __double2ll_rn((double)(a + b) * (twice ? 2.0 : 1.0) * kEnergyScale);
-#pragma unroll
-                for (int h = 0; h < 2; h++)
-                {
-                    const int ai = slot_atom[s1 + h];
-                    if (ai < 0) continue;
-                    const float val = h ? b : a;
-                    const int o = om.remap(ai);
-                    if (vidx == 0)
-                    {
-                        if (pa.energy) atomicAdd(pa.energy + o, val + (h ? b1 : a1));
-                        if (pa.lj_energy) atomicAdd(pa.lj_energy + o, val);
-                    }
-                    else if (vidx == 1)
-                    {
-                        if (pa.direct) atomicAdd(pa.direct + o, val);
-                    }
-                    else if (pa.virial)
-                        atomicAdd(pa.virial + 6 * (size_t)o + (vidx - 2), twice ? 2.0f * val : val);
-                }
-            }
-        }
-    }
-    cp_async_wait_all();
-    __syncwarp();
-    if (EN && lane == 0 && cur_sys >= 0)
-        for (int q = 0; q < 8; q++)
-        {
-            const long long v = red[w][q];
-            if (v) atomicAdd((unsigned long long*)&totals[8 * cur_sys + q], (unsigned long long)v);
-        }
-}
-
-// PME excluded-pair correction (Particle_Mesh::PME_Excluded_Force_With_Atom_Energy,
-// PM_force.cpp:918-997): reciprocal space includes every pair, excluded ones
-// too, so their smooth part erf(beta r)/r is taken back out.  One thread per
-// atom walks its (upper-triangular) exclusion list, as the reference does:
-//   dr = min image(r_j - r_i),  x = beta r,
-//   F_i += q_i q_j beta^3 h(x) dr,  F_j -= the same,  E_i -= q_i q_j erf(x)/r,
-//   W_i -= F (x) dr (the reference's symmetric virial form),
-// with h(x) = (erf(x) - 2/sqrt(pi) x exp(-x^2)) / x^3.  Below x = 0.7, h is
-// summed from its Taylor series (the series of erf and of x exp(-x^2)
-// combined: h = 2/sqrt(pi) sum_{n>=1} (-1)^(n+1) 2n x^(2n-2) / ((2n+1) n!))
-// instead of the difference of two nearly equal numbers, so the correction
-// keeps FP32 precision at bonded distances.  Forces accumulate in int64 fixed
-// point (the partner's share by atomics), the energy total likewise, so the
-// result does not depend on the order.
-__device__ __forceinline__ float excl_h(float x)
-{
-    const float x2 = x * x;
-    if (x < 0.7f)
-    {
-        // 2/sqrt(pi) * (2/3 - 2/5 x^2 + 1/7 x^4 - 1/27 x^6 + 1/132 x^8 - 1/780 x^10 + 1/5400 x^12
-        //               - 1/42840 x^14)
-        float p = -1.0f / 42840.0f;
-        p = __fmaf_rn(p, x2, 1.0f / 5400.0f);
-        p = __fmaf_rn(p, x2, -1.0f / 780.0f);
-        p = __fmaf_rn(p, x2, 1.0f / 132.0f);
-        p = __fmaf_rn(p, x2, -1.0f / 27.0f);
-        p = __fmaf_rn(p, x2, 1.0f / 7.0f);
-        p = __fmaf_rn(p, x2, -0.4f);
-        p = __fmaf_rn(p, x2, 2.0f / 3.0f);
-        return 1.1283791670955126f * p;
-    }
-    return (erff(x) - 1.1283791670955126f * x * expf(-x2)) / (x2 * x);
 }
 
 __global__ void k_pme_excluded(int n, const float3* __restrict__ crd, Cell cell, Cell rcell,
@@ -1373,7 +436,7 @@ PairConst make_pair_const(const spgnb_lj* lj, float beta)
     float z = beta * lj->cutoff;
     pc.use_fit = (z * z <= SPGNB_EWALD_W_MAX * 0.999f) ? 1 : 0;
     pc.table_begin = 0;
-    pc.pad = 0;
+    pc.t4_begin = 0;
     return pc;
 }
 
@@ -1382,10 +445,10 @@ int ensure_slots(spgnb_lj* lj, int slots)
 {
     if (slots + 1 <= lj->sdata_cap) return SPGNB_OK;
     dfree(lj->d_sdata);
-    dfree(lj->d_slot_type);
+    dfree(lj->d_slot_aux);
     int st;
     if ((st = dalloc(&lj->d_sdata, (size_t)(slots + 1)))) return st;
-    if ((st = dalloc(&lj->d_slot_type, (size_t)(slots + 1)))) return st;
+    if ((st = dalloc(&lj->d_slot_aux, (size_t)(slots + 1)))) return st;
     lj->sdata_cap = slots + 1;
     return SPGNB_OK;
 }
@@ -1402,118 +465,13 @@ int ensure_pos(spgnb_lj* lj, int count)
     return SPGNB_OK;
 }
 
-// A persistent grid: as many blocks as can be resident on every SM.
-template <typename K>
-int pair_blocks(K kernel, int threads, size_t smem)
-{
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
-        per_sm <= 0)
-    {
-        cudaGetLastError();
-        per_sm = 4;
-    }
-    return per_sm * num_sms();
-}
-
-
-// Launches the pruned-list force kernel for the given mode / pair-function /
-// box-shape variant.
-struct FastArgs
-{
-    ForceParams p0;
-    const ForceParams* fps;
-    const spgnb_nl* nl;
-    const float4* pos;
-    const int* ptype;
-    const float2* table;
-    int n_types;
-    float3* frc;
-    long long* totals;
-    OwnerMap om;
-    PerAtomOut pa;
-    const int* only;
-    ExclFuse xf;
-};
-
-template <int M, int F, bool T, bool E>
-int launch_fast(const FastArgs& x, size_t smem, cudaStream_t s)
-{
-    const spgnb_nl* nl = x.nl;
-    const int grid =
-        std::max(1, std::min(pair_blocks(k_pair_fast<M, F, T, E>, kForceWarps * 32, smem), nl->clusters_cap));
-    k_pair_fast<M, F, T, E><<<grid, kForceWarps * 32, smem, s>>>(
-        x.p0, x.fps, nl->d_sys, nl->clusters_cap, nl->slot_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords,
-        nl->d_slot_atom, nl->d_slot_gid, nl->d_cl_q, x.pos, x.ptype, x.table, x.n_types, x.frc, x.totals, x.om, x.pa,
-        x.only, x.xf);
-    SPGNB_CHECK_LAUNCH("k_pair_fast");
-    return SPGNB_OK;
-}
-
-template <int M, int F>
-int launch_fast_t(const FastArgs& x, bool tri, size_t smem, cudaStream_t s)
-{
-    if (x.xf.list) return tri ? launch_fast<M, F, true, true>(x, smem, s) : launch_fast<M, F, false, true>(x, smem, s);
-    return tri ? launch_fast<M, F, true, false>(x, smem, s) : launch_fast<M, F, false, false>(x, smem, s);
-}
-
-template <int M>
-int launch_fast_ft(const FastArgs& x, bool fit, bool tri, size_t smem, cudaStream_t s)
-{
-    return fit ? launch_fast_t<M, 1>(x, tri, smem, s) : launch_fast_t<M, 0>(x, tri, smem, s);
-}
-
-int launch_fast_any(const FastArgs& x, int mode, bool fit, bool tri, size_t smem, cudaStream_t s)
-{
-    if (mode == 0) return launch_fast_ft<0>(x, fit, tri, smem, s);
-    if (mode == 1) return launch_fast_ft<1>(x, fit, tri, smem, s);
-    return launch_fast_ft<2>(x, fit, tri, smem, s);
-}
-
 }  // namespace
-
-int force_kernels_init(int table_size)
-{
-    (void)table_size;  // the pair kernel's rows take at most kForceWarps * kMaxTypes * 16 bytes
-    return SPGNB_OK;
-}
 
 int lj_finalize_forces(spgnb_lj* lj, int n, float3* frc, cudaStream_t s)
 {
     if (n <= 0) return SPGNB_OK;
     k_finalize<<<(n + 255) / 256, 256, 0, s>>>(n, lj->d_frc_acc, frc);
     SPGNB_CHECK_LAUNCH("k_finalize");
-    return SPGNB_OK;
-}
-
-int force_pipeline(const ForceInputs& in, cudaStream_t s)
-{
-    spgnb_nl* nl = in.nl;
-    const int slots = nl->clusters_cap * kClusterSize;
-    const bool track = nl->opt.prune_buffer > 0.0f;
-    const float half = 0.5f * nl->opt.prune_buffer;
-    k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
-                                                     nl->d_slot_x0, nl->d_slot_d0, in.crd, in.charge, in.atom_type,
-                                                     in.slot_pos, in.slot_type, track ? nl->d_pref : nullptr,
-                                                     half * half, nl->d_prune);
-    SPGNB_CHECK_LAUNCH("k_pack_slots");
-    const int grid = std::max(1, std::min(num_sms() * 5, (nl->clusters_cap + kPruneWarps - 1) / kPruneWarps));
-    k_prune<<<grid, kPruneWarps * 32, 0, s>>>(in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters, nl->clusters_cap,
-                                              nl->table_cap, nl->slot_cap, nl->d_cl_sys, nl->d_sys, nl->d_tcount,
-                                              nl->d_tab, nl->d_tmask, in.slot_pos, in.slot_type, nl->d_pref,
-                                              nl->d_pcount, nl->d_pwords, nl->S, nl->d_prune);
-    SPGNB_CHECK_LAUNCH("k_prune");
-    cudaEvent_t ev0, ev1;
-    pair_events(&ev0, &ev1);
-    if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
-    const int T = (int)lrint(sqrt((double)in.table_size));
-    if (T <= 0 || T * T != in.table_size || T > kMaxTypes)
-        return fail(SPGNB_E_UNSUPPORTED, "force: the LJ table is not square or has more than %d types", kMaxTypes);
-    const FastArgs fa{in.p0, in.d_fps, nl, in.slot_pos, in.slot_type, in.table, T, in.frc,
-                      in.totals, in.om, in.pa, in.only, in.xf};
-    const int st = launch_fast_any(fa, in.mode, in.fit, nl->triclinic, sizeof(float4) * kForceWarps * T, s);
-    if (st) return st;
-    if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
     return SPGNB_OK;
 }
 
@@ -1587,9 +545,13 @@ int spgnb_lj_create(int atom_numbers, int atom_type_numbers, const int* h_atom_t
         return st;
     }
     cudaMemset(lj->d_excl_total, 0, sizeof(long long));
-    force_kernels_init(T * T);
     cudaMemcpy(lj->d_atom_type, h_atom_type, sizeof(int) * atom_numbers, cudaMemcpyHostToDevice);
     cudaMemcpy(lj->d_table, table.data(), sizeof(float2) * table.size(), cudaMemcpyHostToDevice);
+    if ((st = build_t4(table.data(), T, &lj->d_t4)))
+    {
+        spgnb_lj_destroy(lj);
+        return st;
+    }
     cudaMemset(lj->d_frc_acc, 0, sizeof(long long) * 4 * (size_t)atom_numbers);
     cudaMemset(lj->d_totals, 0, sizeof(long long) * 8);
     cudaMemset(lj->d_lj_energy_atom, 0, sizeof(float) * atom_numbers);
@@ -1656,11 +618,10 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     in.charge = d_charge;
     in.atom_type = lj->d_local_type;
     in.slot_pos = lj->d_sdata;
-    in.slot_type = lj->d_slot_type;
+    in.slot_aux = lj->d_slot_aux;
     in.p0 = make_pair_const(lj, pme_beta);
     in.fit = in.p0.use_fit != 0;
-    in.table = lj->d_table;
-    in.table_size = lj->n_types * lj->n_types;
+    in.t4 = lj->d_t4;
     in.frc = (float3*)d_frc;
     in.totals = lj->d_totals;
     int mode = 0;
@@ -1934,7 +895,8 @@ int spgnb_lj_destroy(spgnb_lj* lj)
     dfree(lj->d_pos);
     dfree(lj->d_pos_type);
     dfree(lj->d_sdata);
-    dfree(lj->d_slot_type);
+    dfree(lj->d_slot_aux);
+    dfree(lj->d_t4);
     delete lj;
     return SPGNB_OK;
 }
