@@ -1,15 +1,23 @@
 #!/usr/bin/env python
-"""Benchmark of the short-range nonbonded path on the 96,000-atom mixed box.
+"""Benchmark of the short-range nonbonded path.
 
 One step is what SPONGE's Main_Calculate_Force runs on this path
-(SPONGE/main.cpp:307-397): a conditional neighbour-list update (a full
-rebuild every 20 steps), the LJ + PME direct-space force with energy and
-virial, and the long-range correction.  Workload: 30,000 rigid-geometry
-waters + 6,000 LJ solute atoms of 20 types in a 99 A box, cutoff 10 A,
-skin 2 A, beta from tolerance 1e-5, seeded synthetic coordinates (static
-between steps; the rebuild cadence is the reference's refresh_interval).
+(SPONGE/main.cpp:307-397) on an energy step: the caller zeroes the force and
+per-atom energy/virial arrays, a conditional neighbour-list update (a full
+rebuild every 20 steps), the LJ + PME direct-space force with per-atom energy
+and virial (LJ_PME_Direct_Force_With_Atom_Energy_And_Virial with
+need_atom_energy = need_virial = 1), and the long-range correction.
+``--terms f`` times the force-only step SPONGE runs between energy outputs;
+each line reports the other kind beside the headline.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl spgnb|reference]
+Workloads (seeded synthetic coordinates, static between steps; the rebuild
+cadence is the reference's refresh_interval):
+  mixed96k (default)  30,000 rigid-geometry waters + 6,000 LJ solute atoms of
+                      20 types, 99 A box, cutoff 10 A, skin 2 A
+  water1m             333,333 waters, 215 A box, cutoff 12 A, skin 2 A
+  batched / served    256 independent systems / a Poisson stream of segments
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl spgnb|reference] [--workload W]
 
 Metric: atom-steps/s (whole job, all ranks) and ns/day at dt = 2 fs.  Each
 timed step is bracketed by CUDA events on the launching stream, with L2
@@ -33,24 +41,66 @@ sys.path.insert(0, os.path.join(ROOT, "sponge2.0_b200"))
 
 DT_PS = 0.002
 REFRESH_INTERVAL = 20
-WORKLOAD = "mixed-box-96k: 30000 waters + 6000 LJ solutes (20 types), 99 A cubic, rc 10 A, skin 2 A"
+
+
+def _mixed96k():
+    from spgnb import systems as S
+    return S.mixed_box_96k()
+
+
+def _water1m():
+    from spgnb import systems as S
+    return S.water_box_1m()
+
+
+def _water1m_cpu_sample():
+    # the reference's CPU Initial is O(N^2) in the atoms (Total_C6_Get,
+    # Lennard_Jones_force.cpp:146-184) and O(G^2) in the cells (the stencil
+    # scan, neighbor_list.cpp:5-49): hours at 1M atoms.  Its CPU rate is
+    # taken on a box of the same density, cutoff and skin, 36,000 waters.
+    from spgnb import systems as S
+    n_w = 36000
+    return S.water_system(n_w, (n_w / 0.0334) ** (1.0 / 3.0), 3, cutoff=12.0, skin=2.0, name="water-108k")
+
+
+# plain-path workloads: generator, name, the box the reference's CPU path is
+# timed on (None: the workload's own)
+PLAIN = {
+    "mixed96k": (_mixed96k, "mixed-box-96k: 30000 waters + 6000 LJ solutes (20 types), 99 A cubic, rc 10 A, skin 2 A",
+                 None),
+    "water1m": (_water1m, "water-box-1m: 333333 waters (999999 atoms), 215 A cubic, rc 12 A, skin 2 A",
+                _water1m_cpu_sample),
+}
+
+
+def cpu_sample_box(workload, s):
+    """The box the reference's CPU path is timed on, and a note when it is not
+    the workload's own."""
+    gen = PLAIN[workload][2]
+    if gen is None:
+        return s, ""
+    b = gen()
+    return b, f" (a {b.n}-atom box of the same density, cutoff and skin: the reference's CPU set-up is O(N^2))"
 
 
 def parse():
     p = argparse.ArgumentParser()
     p.add_argument("--gpus", type=int, default=1)
-    p.add_argument("--steps", type=int, default=400)
-    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--steps", type=int, default=100)
+    p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["spgnb", "reference"], default="spgnb")
     p.add_argument("--terms", choices=["fev", "f"], default="fev",
-                   help="fev: force + energy + virial every step; f: force only")
+                   help="fev: force + per-atom energy + virial every step (the reference API's energy step); "
+                        "f: force only")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     p.add_argument("--profile", action="store_true",
                    help="profiling run for ncu: warm-up and --steps plain steps, no L2 flush, no e2e, no baseline")
-    p.add_argument("--workload", choices=["mixed96k", "batched", "served"], default="mixed96k",
-                   help="mixed96k: the plain path on the 96k box (default); batched: 256 systems, batched engine "
-                        "against the plain per-system path; served: Poisson stream of MD segments into a pool")
+    p.add_argument("--workload", choices=["mixed96k", "water1m", "batched", "served"], default="mixed96k",
+                   help="mixed96k: the plain path on the 96k box (default); water1m: the plain path on the "
+                        "1M-atom water box, rc 12; batched: 256 systems, batched engine against the plain "
+                        "per-system path; served: Poisson stream of MD segments into a pool")
+    p.add_argument("--no-batched", action="store_true", help="mixed96k: leave out the batched sub-measurement")
     p.add_argument("--systems", type=int, default=256, help="batched: number of systems")
     p.add_argument("--serve-seconds", type=float, default=60.0, help="served: length of the request stream")
     p.add_argument("--rate", type=float, default=40.0, help="served: mean arrivals per second")
@@ -121,10 +171,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def plain_config(args, s, world):
+    """The config dict both arms print for a plain-path workload."""
+    wl = PLAIN[args.workload][1]
+    return {"workload": wl, "atoms_per_gpu": s.n, "terms": args.terms, "refresh_interval": REFRESH_INTERVAL,
+            "l2": "flushed between steps (512 MiB write)",
+            "parallelism": f"replicas x{world}" if world > 1 else "single system"}
+
+
 def cpu_reference_rate(system, terms, budget_s, threads=None):
     """The reference's own CPU implementation of the path (oracle/_ref, built
-    from its sources) timed on this host: forced build, then conditional
-    update + force per step, refresh_interval 20."""
+    from its sources) timed on this host, on a bounded sample: one forced
+    rebuild, and force steps between rebuilds; atom-steps/s with the rebuild
+    amortised over refresh_interval steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     ref = O.Reference(gpu=False)
@@ -133,58 +192,94 @@ def cpu_reference_rate(system, terms, budget_s, threads=None):
     ref.init(system, refresh_interval=REFRESH_INTERVAL)
     ref.nl_update(forced=True)
     fe = terms == "fev"
-    probe = ref.time_steps(2, first_step=0, need_energy=fe, need_virial=fe)
-    per = probe / 2
-    steps = max(REFRESH_INTERVAL, min(200, int(budget_s / max(per, 1e-6))))
-    steps = (steps // REFRESH_INTERVAL) * REFRESH_INTERVAL
-    t = ref.time_steps(steps, first_step=2, need_energy=fe, need_virial=fe)
+    t_build = ref.time_rebuild(1)
+    probe = ref.time_steps(1, first_step=0, need_energy=fe, need_virial=fe)
+    steps = max(1, min(REFRESH_INTERVAL - 2, int(max(0.0, budget_s - t_build) / max(probe, 1e-6))))
+    t = ref.time_steps(steps, first_step=1, need_energy=fe, need_virial=fe)
     ref.clear()
-    return system.n * steps / t, threads, steps, t
+    per_step = t / steps + t_build / REFRESH_INTERVAL
+    return system.n / per_step, threads, steps, t + t_build, per_step
+
+
+def reference_cuda_times(s, W, K):
+    """The reference's own CUDA kernels (oracle/_ref/libspgref_cuda.so, built
+    unchanged from its sources for sm_100a) on this GPU: SPONGE's classes
+    driven by the harness loop (NEIGHBOR_LIST::Update, then the LJ and solvent
+    modules), per step, host clock around K steps after W warm-up steps; the
+    same step indices as the other arm, list rebuilt every 20 steps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    out = {}
+    ref = O.Reference(gpu=True)
+    ref.init(s, refresh_interval=REFRESH_INTERVAL, solvent=True)
+    ref.nl_update(forced=True)
+    for name, ev in (("per_atom_energy_virial", True), ("force_only", False)):
+        ref.time_steps(W, first_step=0, need_energy=ev, need_virial=ev)
+        t = ref.time_steps(K, first_step=W, need_energy=ev, need_virial=ev)
+        out[name] = {"ms_per_step": 1e3 * t / K, "atom_steps_per_s": s.n * K / t}
+    ref.clear()
+    out["how"] = ("reference CUDA build of NEIGHBOR_LIST + LENNARD_JONES_INFORMATION + SOLVENT_LENNARD_JONES "
+                  "(SPONGE/main.cpp:307-397 order), harness loop, host clock, no L2 flush")
+    return out
 
 
 def run_reference_arm(args, world, rank):
+    """The reference's CPU implementation of the path on this host's cores, on
+    the other arm's workload, step indices, steps and warm-up; rank 0 only.
+    Beside it, when a GPU is present, the reference's own CUDA kernels on the
+    same workload (reference_cuda)."""
     from spgnb import systems as S
     if rank != 0:
         return
-    s = S.mixed_box_96k()
-    budget = max(20.0, min(150.0, 0.5 * (args.steps + args.warmup)))
-    rate, threads, steps, t = cpu_reference_rate(s, args.terms, budget)
+    s = PLAIN[args.workload][0]()
+    cs, note = cpu_sample_box(args.workload, s)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    ref = O.Reference(gpu=False)
+    threads = os.cpu_count() or 1
+    ref.set_threads(threads)
+    fe = args.terms == "fev"
+    ref.init(cs, refresh_interval=REFRESH_INTERVAL)
+    ref.nl_update(forced=True)
+    W, K = args.warmup, args.steps
+    if W > 0:
+        ref.time_steps(W, first_step=0, need_energy=fe, need_virial=fe)
+    t = ref.time_steps(K, first_step=W, need_energy=fe, need_virial=fe)
+    ref.clear()
+    rate = cs.n * K / t
+    rebuilds = sum(1 for k in range(W, W + K) if (k + 1) % REFRESH_INTERVAL == 0)
     line = {"metric": "atom-steps/s", "value": rate, "unit": "atom-steps/s", "impl": "reference", "n_gpus": args.gpus,
-            "steps": steps, "warmup": 2, "ms_per_step": 1e3 * t / steps, "higher_is_better": True,
+            "steps": K, "warmup": W, "ms_per_step": 1e3 * t / K, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "ns_per_day": steps * 86.4 * DT_PS / t,
-            "config": {"workload": WORKLOAD, "terms": args.terms, "refresh_interval": REFRESH_INTERVAL,
-                       "atoms": s.n, "parallelism": "replicas"},
+            "ns_per_day": K * 86.4 * DT_PS / t,
+            "config": plain_config(args, s, args.gpus),
             "cpu_baseline": {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
-                             "sample": f"{steps} steps of the 96k box (incl. {steps // REFRESH_INTERVAL} rebuilds)"},
+                             "sample": f"steps {W}..{W + K - 1} of the box ({rebuilds} rebuilds), after {W} warm-up "
+                                       f"steps, {'per-atom energy + virial' if fe else 'forces only'}{note}"},
             "e2e": {"value": rate, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        import torch
+        if torch.cuda.is_available() and os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libspgref_cuda.so")):
+            line["reference_cuda"] = reference_cuda_times(s, W, K)
+    except Exception as exc:  # reported beside the CPU figure, not required
+        line["reference_cuda"] = {"unavailable": str(exc)}
     print(json.dumps(line), flush=True)
 
 
-def run_batched(args, world, rank, local):
+def batched_measure(systems_all, K, W, world, rank, local, dist, k_plain=None):
     """Config 3: independent systems (log-uniform 1,500-24,000 atoms, 0-15 %
     solute, rc from {8, 10, 12}, skin 2) stepped by the batched engine
     (leap-frog + SETTLE + per-system list updates + one force launch, graph
     replay), against the plain per-system path: the same kernels for one
-    system at a time, launched step by step."""
+    system at a time, launched step by step.  Returns the figures of rank 0's
+    line (max time and summed atoms over ranks)."""
+    import copy
     import torch
-    from spgnb import systems as S
     from spgnb._lib import lib
     from spgnb.batch import Batch
     from spgnb.shard import shard_systems
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
-    torch.cuda.set_device(local)
-    systems_all = S.batch_systems(args.systems)
     mine = [systems_all[k] for k in shard_systems(systems_all, world, rank)]
     L = lib()
-    K = args.steps
-    W = max(3, args.warmup)
 
     def timed(b, steps, energy_interval=0):
         st = torch.cuda.ExternalStream(b.stream_ptr)
@@ -197,8 +292,8 @@ def run_batched(args, world, rank, local):
 
     opts = dict(refresh_interval=REFRESH_INTERVAL, thermostat_tau=0.1, temperature=300.0)
     # the synthetic boxes start strained: relax them with a strongly coupled
-    # thermostat first (not timed), then production coupling
-    # lists sized for a 1.6 A prune buffer: the autotuner tries buffers up to it
+    # thermostat first (not timed), then production coupling; lists sized for
+    # a 1.6 A prune buffer, the largest the autotuner tries
     B = Batch(mine, **dict(opts, thermostat_tau=0.002, prune_buffer=1.6))
     B.run(200)
     B.check_overflow()
@@ -206,20 +301,8 @@ def run_batched(args, world, rank, local):
     tuned = B.autotune(10)
     B.run(W * B.options.steps_per_graph)
     B.check_overflow()
+    st0 = B.stats()
     torch.cuda.synchronize()
-    if args.profile:
-        # kernels of K steps inside the NVTX range "timed" (ncu --nvtx --nvtx-include timed/)
-        torch.cuda.nvtx.range_push("timed")
-        B.run(K, 100)
-        torch.cuda.synchronize()
-        torch.cuda.nvtx.range_pop()
-        if rank == 0:
-            print(json.dumps({"profile_run": True, "workload": "batched", "steps": K,
-                              "atoms": sum(s.n for s in mine)}), flush=True)
-        B.close()
-        if dist is not None:
-            dist.destroy_process_group()
-        return
     sampler = ClockSampler(local)
     sampler.start()
     if dist is not None:
@@ -233,8 +316,7 @@ def run_batched(args, world, rank, local):
     e = B.energies()
     # plain per-system path from the same relaxed states: each system alone,
     # the same kernels launched step by step, a bounded sample of steps
-    import copy
-    k_plain = max(5, min(20, K // 5))
+    k_plain = k_plain or max(5, min(20, K // 5))
     plain_ms, plain_as = 0.0, 0
     for k, s in enumerate(mine):
         crd, vel, _ = B.download(k)
@@ -245,6 +327,7 @@ def run_batched(args, world, rank, local):
         plain_ms += timed(b, k_plain)
         plain_as += s.n * k_plain
         b.close()
+    B.close()
     if dist is not None:
         t = torch.tensor([ms, plain_ms, float(atoms), float(plain_as)], dtype=torch.float64, device="cuda")
         tmax = t[:2].clone()
@@ -255,30 +338,52 @@ def run_batched(args, world, rank, local):
         atoms_all, plain_as_all = float(tsum[0]), float(tsum[1])
     else:
         atoms_all, plain_as_all = float(atoms), float(plain_as)
+    value = atoms_all * K / (ms * 1e-3)
+    plain = plain_as_all / (plain_ms * 1e-3)
+    return {"value": value, "ms": ms, "K": K, "W": W, "systems": len(systems_all), "systems_per_gpu": len(mine),
+            "atoms_all": int(sum(s.n for s in systems_all)), "atoms_per_gpu": atoms,
+            "plain": plain, "k_plain": k_plain, "tuned": tuned,
+            "rebuilds": st["rebuilds"] - st0["rebuilds"], "prunings": st["prunings"] - st0["prunings"],
+            "overflow": st["overflow"], "energies_finite": bool(np.isfinite(e).all()), "clocks": clocks,
+            "launches": int(launches)}
+
+
+def batched_workload_name(m):
+    return (f"batched: {m['systems']} systems, {m['atoms_all']} atoms, log-uniform 1500-24000, rc {{8,10,12}}, "
+            "skin 2, leap-frog + SETTLE, 2 fs, Berendsen 300 K (tau 0.1 ps), lists rebuilt every 20 steps")
+
+
+def run_batched(args, world, rank, local):
+    import torch
+    from spgnb import systems as S
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    torch.cuda.set_device(local)
+    m = batched_measure(S.batch_systems(args.systems), args.steps, max(3, args.warmup), world, rank, local, dist)
     if rank == 0:
-        value = atoms_all * K / (ms * 1e-3)
-        plain = plain_as_all / (plain_ms * 1e-3)
-        line = {"metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": K,
-                "warmup": W, "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak",
+        K = m["K"]
+        line = {"metric": "atom-steps/s", "value": m["value"], "unit": "atom-steps/s", "n_gpus": world, "steps": K,
+                "warmup": m["W"], "ms_per_step": m["ms"] / K, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": {"workload": f"batched: {len(systems_all)} systems, {sum(s.n for s in systems_all)} atoms, "
-                                       "log-uniform 1500-24000, rc {8,10,12}, skin 2, leap-frog + SETTLE, 2 fs, "
-                                       "Berendsen 300 K (tau 0.1 ps), lists rebuilt every 20 steps",
-                           "systems_per_gpu": len(mine), "atoms_per_gpu": atoms,
-                           "energy_interval": 100, "prune_buffer_autotuned": tuned,
-                           "l2": "inputs larger than L2",
+                "config": {"workload": batched_workload_name(m), "systems_per_gpu": m["systems_per_gpu"],
+                           "atoms_per_gpu": m["atoms_per_gpu"], "energy_interval": 100,
+                           "prune_buffer_autotuned": m["tuned"], "l2": "inputs larger than L2",
                            "parallelism": f"systems sharded over {world} GPUs" if world > 1 else "single GPU"},
-                "plain_per_system": {"value": plain, "unit": "atom-steps/s",
+                "plain_per_system": {"value": m["plain"], "unit": "atom-steps/s",
                                      "how": f"each system alone from the same relaxed state, kernels launched step "
-                                            f"by step, {k_plain} steps each"},
-                "batched_over_plain": value / plain,
-                "rebuilds": st["rebuilds"], "prunings": st["prunings"], "overflow": st["overflow"],
-                "energies_finite": bool(np.isfinite(e).all()),
-                "clocks": clocks, "gpu_launches": int(launches),
-                "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
+                                            f"by step, {m['k_plain']} steps each"},
+                "batched_over_plain": m["value"] / m["plain"],
+                "rebuilds": m["rebuilds"], "prunings": m["prunings"], "overflow": m["overflow"],
+                "energies_finite": m["energies_finite"], "clocks": m["clocks"], "gpu_launches": m["launches"],
+                "gpu_launches_per_step": m["launches"] / K,
+                "e2e": {"value": m["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                         "note": "state stays resident on the device between steps"}}
         print(json.dumps(line), flush=True)
-    B.close()
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -390,6 +495,7 @@ def main():
         return
     if args.impl == "reference":
         # the reference arm is the reference's CPU path: rank 0 alone, no GPU work
+        # besides the reference's own CUDA kernels timed beside it
         run_reference_arm(args, world, rank)
         return
     import torch
@@ -400,34 +506,39 @@ def main():
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                 device_id=torch.device("cuda", local))
-    from spgnb import systems as S
     from spgnb._lib import lib
     from spgnb.engine import PlainPath
     import ctypes as C
 
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    s = S.mixed_box_96k()
-    fe = args.terms == "fev"
+    s = PLAIN[args.workload][0]()
+    main_box = args.workload == "mixed96k"
     L = lib()
     path = PlainPath(s, refresh_interval=REFRESH_INTERVAL, export_atom_groups=False, device=dev)
     stream = torch.cuda.current_stream()
 
-    def step(k):
+    def step(k, terms):
+        # Main_Calculate_Force's part of the path: the caller zeroes the force
+        # and (on energy steps) the per-atom arrays, then list update, the LJ +
+        # PME direct force with per-atom energy and virial, the tail correction
+        fe = terms == "fev"
         path.update(k)
-        path.force(need_energy=fe, need_virial=fe, per_atom=False)
+        path.force(need_energy=fe, need_virial=fe, per_atom=True)
         if fe:
             path.lj.Long_Range_Correction(1, path.atom_virial, 1, path.atom_energy, s.volume)
 
-    for k in range(args.warmup):
-        step(k)
+    W, K = args.warmup, args.steps
+    for k in range(W):
+        step(k, args.terms)
     torch.cuda.synchronize()
     if args.profile:
-        for k in range(args.steps):
-            step(args.warmup + k)
+        for k in range(K):
+            step(W + k, args.terms)
         torch.cuda.synchronize()
         if rank == 0:
-            print(json.dumps({"profile_run": True, "steps": args.steps, "warmup": args.warmup, "atoms": s.n}))
+            print(json.dumps({"profile_run": True, "workload": args.workload, "steps": K, "warmup": W,
+                              "atoms": s.n, "terms": args.terms}))
         if dist is not None:
             dist.destroy_process_group()
         return
@@ -437,52 +548,62 @@ def main():
     listed, inside = C.c_longlong(), C.c_longlong()
     L.spgnb_nl_count_pairs(path.nl.handle, C.c_void_p(path.crd.data_ptr()), _ltm(s.cell), _ltm(s.rcell),
                            s.cutoff, C.byref(listed), C.byref(inside))
-    flop_per_launch = 20.0 * listed.value + (45.0 + (22.0 if fe else 0.0)) * inside.value
     peak = C.c_double()
     L.spgnb_probe_fp32_fma_tflops(5, C.byref(peak))
 
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
-    K = args.steps
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-    for a, b in ev + pev:
-        a.record()
-        b.record()
-    torch.cuda.synchronize()
+
+    def timed_steps(terms, first, with_pair_events):
+        """K steps, each bracketed by CUDA events on the stream, L2 flushed in
+        between (outside the events); the pair kernel's own events too."""
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        pev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        for a, b in ev + pev:
+            a.record()
+            b.record()
+        torch.cuda.synchronize()
+        launches0 = L.spgnb_launch_count()
+        for k in range(K):
+            flush.fill_(k & 0xff)
+            ev[k][0].record(stream)
+            if with_pair_events:
+                L.spgnb_debug_set_pair_events(C.c_void_p(pev[k][0].cuda_event), C.c_void_p(pev[k][1].cuda_event))
+            step(first + k, terms)
+            ev[k][1].record(stream)
+        L.spgnb_debug_set_pair_events(None, None)
+        torch.cuda.synchronize()
+        launches = L.spgnb_launch_count() - launches0
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        pair_ms = [a.elapsed_time(b) for a, b in pev] if with_pair_events else []
+        return step_ms, pair_ms, launches
+
     sampler = ClockSampler(local)
     sampler.start()
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
-    launches0 = L.spgnb_launch_count()
-    for k in range(K):
-        flush.fill_(k & 0xff)
-        ev[k][0].record(stream)
-        L.spgnb_debug_set_pair_events(C.c_void_p(pev[k][0].cuda_event), C.c_void_p(pev[k][1].cuda_event))
-        step(args.warmup + k)
-        ev[k][1].record(stream)
-    L.spgnb_debug_set_pair_events(None, None)
-    torch.cuda.synchronize()
-    launches = L.spgnb_launch_count() - launches0
+    step_ms, pair_ms, launches = timed_steps(args.terms, W, True)
     if dist is not None:
         dist.barrier()
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    pair_ms = [a.elapsed_time(b) for a, b in pev]
     total_ms = sum(step_ms)
+    other = "f" if args.terms == "fev" else "fev"
+    other_ms, other_pair_ms, _ = timed_steps(other, W + K, True)
 
     # end to end through the module API with host buffers: pinned H2D of the
-    # coordinates, the step, D2H of forces and the FP64 totals, every step
+    # coordinates, the step, D2H of the forces and the energy/virial totals
+    # (Step_Print's sums), every step
     crd_host = torch.from_numpy(s.crd.copy()).pin_memory()
     frc_host = torch.empty((s.n, 3), dtype=torch.float32).pin_memory()
+    fe = args.terms == "fev"
     e2e_ms = []
     for k in range(K):
         flush.fill_(k & 0xff)
-        a, b = ev[k]
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
         path.crd.copy_(crd_host, non_blocking=True)
-        step(args.warmup + K + k)
+        step(W + 2 * K + k, args.terms)
         frc_host.copy_(path.frc, non_blocking=True)
         if fe:
             path.lj.totals()
@@ -491,65 +612,9 @@ def main():
         e2e_ms.append(a.elapsed_time(b))
     e2e_total = sum(e2e_ms)
 
-    # the PME excluded-pair correction (PM_force.cpp:918-997), timed on its own
-    # (not part of the step above: SPONGE runs it in the PME module)
-    ex_frc = torch.zeros_like(path.frc)
-    ex_ene = torch.zeros_like(path.atom_energy)
-    ex_vir = torch.zeros_like(path.atom_virial)
-
-    def excluded():
-        path.lj.PME_Excluded_Force_With_Atom_Energy(s.n, path.crd, s.cell, s.rcell, path.charge, s.beta,
-                                                    path.excl_start, path.excl_list, path.excl_numbers, ex_frc,
-                                                    1, ex_ene, ex_vir)
-
-    for _ in range(3):
-        excluded()
-    xa, xb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    xa.record(stream)
-    for _ in range(20):
-        excluded()
-    xb.record(stream)
-    xb.synchronize()
-    excluded_ms = xa.elapsed_time(xb) / 20
-
-    # the same correction fused into the pair pass (spgnb_lj_fuse_pme_excluded):
-    # a force call with it against one without, each the mean of 20 calls
-    def force_calls(n=20):
-        for _ in range(3):
-            path.force(need_energy=fe, need_virial=fe, per_atom=False)
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
-        for _ in range(n):
-            path.force(need_energy=fe, need_virial=fe, per_atom=False)
-        b.record(stream)
-        b.synchronize()
-        return a.elapsed_time(b) / n
-
-    force_only_ms = force_calls()
-    path.lj.Fuse_PME_Excluded(s.n, path.excl_start, path.excl_list, path.excl_numbers, len(s.excl_list))
-    force_fused_ms = force_calls()
-    path.lj.Fuse_PME_Excluded(s.n, None, None, None, 0)
-
-    # the full neighbour list for many-body modules (FULL_NEIGHBOR_LIST, rebuilt
-    # every update in SPONGE when a module asks for it), timed on its own
-    for _ in range(2):
-        path.nl.build_full(s.n, path.crd, s.cell, s.rcell, 0.0, 1200)
-    full_out = path.nl._full_out
-    torch.cuda.synchronize()
-    full_ms = []
-    for _ in range(5):
-        fa, fb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        fa.record(stream)
-        path.nl.build_full(s.n, path.crd, s.cell, s.rcell, 0.0, 1200, out=full_out)
-        fb.record(stream)
-        fb.synchronize()
-        full_ms.append(fa.elapsed_time(fb))
-
-    # the alchemical path on the same box: LJ_SOFT_CORE with a 40-atom perturbed
-    # ligand (main.cpp:379-385), per step the list update and the soft-core
-    # force, timed on its own; and one dH/dlambda evaluation (it reads back)
-    soft = _time_soft_core(s, fe, dev, stream, flush)
-    graph = _time_graph_resident(s)
+    extras = {}
+    if main_box:
+        extras = _main_box_extras(path, s, dev, stream, flush, world, rank, local, dist, args)
 
     if dist is not None:
         t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=dev)
@@ -564,43 +629,48 @@ def main():
         atoms_steps = world * s.n * K
         value = atoms_steps / (total_ms * 1e-3)
         pair_avg_ms = sum(pair_ms) / len(pair_ms)
+        flop_per_launch = 20.0 * listed.value + (45.0 + (22.0 if fe else 0.0)) * inside.value
         achieved = flop_per_launch / (pair_avg_ms * 1e-3) / 1e12
-        prof = _profile_traffic()
+        prof = _profile_traffic(args.workload, args.terms)
         line = {
             "metric": "atom-steps/s", "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": K,
-            "warmup": args.warmup, "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak",
+            "warmup": W, "ms_per_step": total_ms / K, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "ns_per_day": K * 86.4 * DT_PS / (total_ms * 1e-3),
-            "config": {"workload": WORKLOAD, "atoms_per_gpu": s.n, "terms": args.terms,
-                       "refresh_interval": REFRESH_INTERVAL, "l2": "flushed between steps (512 MiB write)",
-                       "parallelism": f"replicas x{world}" if world > 1 else "single system"},
+            "config": plain_config(args, s, world),
+            "step": ("list update + LJ/PME direct force with per-atom energy and virial + tail correction "
+                     "(the reference API's energy step)") if fe else "list update + LJ/PME direct force",
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None,
                          "traffic": prof.get("bytes_per_launch"),
-                         "kernel": "k_pair_fast", "kernel_ms": pair_avg_ms,
+                         "kernel": "k_pair8", "kernel_ms": pair_avg_ms,
                          "flop_per_launch": flop_per_launch, "listed_pairs": listed.value,
                          "pairs_in_cutoff": inside.value,
-                         "full_list_words": st.full_list_words, "pruned_list_words": st.pruned_list_words,
-                         "prunings": st.prunes, "rebuilds": st.builds,
+                         "pruned_list_words": st.pruned_list_words, "prunings": st.prunes, "rebuilds": st.builds,
                          "peak_source": "measured FP32 FFMA throughput on this device (spgnb_probe_fp32_fma_tflops)",
                          "traffic_source": prof.get("source")},
+            ("force_only" if fe else "per_atom_energy_virial"): {
+                "ms_per_step": sum(other_ms) / K, "atom_steps_per_s": world * s.n * K / (sum(other_ms) * 1e-3),
+                "pair_kernel_ms": sum(other_pair_ms) / K},
+            "list_device_bytes": st.device_bytes,
+            "reference_d_temp_bytes": 4 * 1200 * s.n,
             "clocks": clocks,
             "gpu_launches": int(launches),
-            "pme_excluded_correction_ms": excluded_ms,
-            "pme_excluded_fused": {"force_call_ms": force_only_ms, "force_call_with_correction_ms": force_fused_ms,
-                                   "extra_ms": force_fused_ms - force_only_ms},
-            "full_neighbor_list_ms": min(full_ms),
-            "soft_core": soft,
-            "graph_resident": graph,
             "e2e": {"value": world * s.n * K / (e2e_total * 1e-3), "unit": "atom-steps/s",
                     "h2d_bytes_per_step": s.n * 12, "d2h_bytes_per_step": s.n * 12 + (64 if fe else 0)},
         }
+        line.update(extras)
         if world == 1 and not args.no_cpu_baseline:
             try:
-                rate, threads, steps, t = cpu_reference_rate(s, args.terms, args.cpu_seconds)
+                cs, note = cpu_sample_box(args.workload, s)
+                rate, threads, steps, t, per = cpu_reference_rate(cs, args.terms, args.cpu_seconds)
                 line["cpu_baseline"] = {"value": rate, "unit": "atom-steps/s", "cores": threads, "kind": "reference",
-                                        "sample": f"{steps} steps of the same box on the host "
-                                                  f"({steps // REFRESH_INTERVAL} rebuilds), {t:.1f} s"}
+                                        "sample": f"one rebuild + {steps} force steps on the host ({t:.1f} s), the "
+                                                  f"rebuild amortised over {REFRESH_INTERVAL} steps{note}"}
+                rate1, _, steps1, t1, _ = cpu_reference_rate(cs, args.terms, args.cpu_seconds / 2, threads=1)
+                line["cpu_baseline"]["single_core"] = {
+                    "value": rate1, "cores": 1,
+                    "sample": f"one rebuild + {steps1} force steps on one core ({t1:.1f} s)"}
             except Exception as exc:  # the baseline is reported, not required
                 line["cpu_baseline"] = {"value": None, "unit": "atom-steps/s", "cores": 0, "kind": "reference",
                                         "sample": f"unavailable: {exc}"}
@@ -608,6 +678,70 @@ def main():
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def _main_box_extras(path, s, dev, stream, flush, world, rank, local, dist, args):
+    """The 96k box's side measurements: the PME excluded-pair correction
+    alone and fused, the full neighbour list, the alchemical path, the box as
+    graph-resident dynamics, and the batched workload (config 3, all systems,
+    fewer steps)."""
+    import torch
+    from spgnb import systems as S
+    fe = args.terms == "fev"
+    out = {}
+    # the PME excluded-pair correction (PM_force.cpp:918-997), timed on its own
+    # (SPONGE runs it in the PME module)
+    ex_frc = torch.zeros_like(path.frc)
+    ex_ene = torch.zeros_like(path.atom_energy)
+    ex_vir = torch.zeros_like(path.atom_virial)
+
+    def excluded():
+        path.lj.PME_Excluded_Force_With_Atom_Energy(s.n, path.crd, s.cell, s.rcell, path.charge, s.beta,
+                                                    path.excl_start, path.excl_list, path.excl_numbers, ex_frc,
+                                                    1, ex_ene, ex_vir)
+
+    def mean_ms(fn, n=20):
+        for _ in range(3):
+            fn()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(n):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / n
+
+    out["pme_excluded_correction_ms"] = mean_ms(excluded)
+    # the same correction in the force call's finishing pass (spgnb_lj_fuse_pme_excluded)
+    force_call = lambda: path.force(need_energy=fe, need_virial=fe, per_atom=True)
+    plain_ms = mean_ms(force_call)
+    path.lj.Fuse_PME_Excluded(s.n, path.excl_start, path.excl_list, path.excl_numbers, len(s.excl_list))
+    fused_ms = mean_ms(force_call)
+    path.lj.Fuse_PME_Excluded(s.n, None, None, None, 0)
+    out["pme_excluded_fused"] = {"force_call_ms": plain_ms, "force_call_with_correction_ms": fused_ms,
+                                 "extra_ms": fused_ms - plain_ms}
+    # the full neighbour list for many-body modules (FULL_NEIGHBOR_LIST)
+    for _ in range(2):
+        path.nl.build_full(s.n, path.crd, s.cell, s.rcell, 0.0, 1200)
+    full_out = path.nl._full_out
+    out["full_neighbor_list_ms"] = mean_ms(
+        lambda: path.nl.build_full(s.n, path.crd, s.cell, s.rcell, 0.0, 1200, out=full_out), 5)
+    # the alchemical path on the same box: LJ_SOFT_CORE with a 40-atom perturbed
+    # ligand (main.cpp:379-385), per step the list update and the soft-core
+    # force; and one dH/dlambda evaluation (it reads back)
+    out["soft_core"] = _time_soft_core(s, fe, dev, stream, flush)
+    out["graph_resident"] = _time_graph_resident(s)
+    if not args.no_batched:
+        m = batched_measure(S.batch_systems(args.systems), 100, 3, world, rank, local, dist, k_plain=5)
+        out["batched"] = {"workload": batched_workload_name(m), "steps": m["K"], "ms_per_step": m["ms"] / m["K"],
+                          "atom_steps_per_s": m["value"], "plain_per_system_atom_steps_per_s": m["plain"],
+                          "batched_over_plain": m["value"] / m["plain"],
+                          "plain_how": f"each system alone from the same relaxed state, kernels launched step by "
+                                       f"step, {m['k_plain']} steps each",
+                          "gpu_launches_per_step": m["launches"] / m["K"], "prune_buffer_autotuned": m["tuned"],
+                          "rebuilds": m["rebuilds"], "prunings": m["prunings"], "overflow": m["overflow"],
+                          "energies_finite": m["energies_finite"], "clocks": m["clocks"]}
+    return out
 
 
 def _time_soft_core(s, fe, dev, stream, flush, steps=50):
@@ -674,9 +808,10 @@ def _ltm(m):
     return LTMatrix3.of(m)
 
 
-def _profile_traffic():
-    """DRAM bytes per pair-kernel launch from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "k_pair_fast_mixed96k.json")
+def _profile_traffic(workload, terms):
+    """DRAM bytes per pair-kernel launch from the committed ncu summary of
+    this workload and step kind."""
+    p = os.path.join(ROOT, "profiles", f"k_pair8_{workload}_{terms}.json")
     if not os.path.exists(p):
         return {}
     try:

@@ -164,6 +164,7 @@ typedef struct
     long long full_list_words;  /* listed partners summed over atoms (each pair twice) */
     long long prunes;       /* prunings performed so far */
     long long pruned_list_words; /* partners in the pruned lists of the last pruning */
+    long long device_bytes; /* device memory the list's arrays hold (capacities, not use) */
 } spgnb_nl_stats;
 
 /* Reads counters back (synchronises the stream). */
@@ -430,12 +431,20 @@ int spgnb_solvent_destroy(spgnb_solvent* s);
  * [0, atom_type_numbers)), the triangular pair tables A = 12*A_file and
  * B = 6*B_file on the device, coordinates, charges, the reference-layout
  * list; owners are atoms [0, local_atom_numbers - solvent_numbers) as in the
- * reference's LJ call.  All calls share the one scratch array and each call
+ * reference's LJ call.  Like spgnb_lj_pme_direct_force, it takes one rank's
+ * atoms only: ghost_numbers != 0 returns SPGNB_E_UNSUPPORTED.  A list entry
+ * outside [0, local_atom_numbers) or a type outside [0, atom_type_numbers) is
+ * a caller error: such an entry is skipped (a type is clamped into the
+ * table), nothing is read out of bounds, and the forces of those pairs are
+ * missing.  The pair evaluation adds each partner's force with one int64
+ * atomic per pair and component: correct, but slower than the cluster-list
+ * path.  All calls share the one scratch array and each call
  * clears what must start at zero; calls whose kernels overlap on the GPU race
  * on it, so serialise them.  The first call on a device looks up the array's
  * device address with that device current; make it before capturing any
  * stream on that device. */
-int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_numbers, int atom_type_numbers,
+int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_numbers, int ghost_numbers,
+                                      int atom_type_numbers,
                                       const int* d_atom_type, const float* d_pair_A, const float* d_pair_B,
                                       const spgnb_vector* d_crd, const float* d_charge, spgnb_vector* d_frc,
                                       spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, const spgnb_atom_group* d_nl,
@@ -560,6 +569,8 @@ int spgnb_batch_capacity(spgnb_batch* b, int* max_systems, long long* max_atoms,
                          double* device_bytes);
 
 /* ------------------------------------------------------------ diagnostics */
+/* Measurement hooks for benchmarks and profiling only: no SPONGE module calls
+ * these and nothing on the force path depends on them. */
 /* Kernel launches issued by the library so far (all threads). */
 unsigned long long spgnb_launch_count(void);
 /* CUDA events (cudaEvent_t, or NULL to stop) recorded around every later

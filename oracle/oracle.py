@@ -64,6 +64,9 @@ class Oracle:
         lib.orc_soft_long_range.restype = None
         lib.orc_soft_long_range.argtypes = [C.c_int, _i32p, _i32p, _f32p, _f32p, C.c_float, C.c_float,
                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        lib.orc_direct_forces_subset_fp64.restype = C.c_longlong
+        lib.orc_direct_forces_subset_fp64.argtypes = [C.c_int, _f32p, _f32p, _i32p, _f32p, _f32p, _f32p, C.c_float,
+                                                      C.c_float, _i32p, _i32p, _i32p, C.c_int, _i32p, _f64p]
         lib.orc_pair_dr2.restype = C.c_float
         lib.orc_pair_dr2.argtypes = [_f32p, _f32p, _f32p, _f32p, C.c_int]
         self.lib = lib
@@ -100,6 +103,18 @@ class Oracle:
                                               _ci32(lists if len(lists) else np.zeros(1, np.int32)), frc,
                                               ptr(elj), ptr(ec), ptr(vir), tot)
         return _result(frc, elj, ec, vir, tot, npairs)
+
+    def direct_forces_subset(self, s, atoms, crd=None):
+        """FP64 forces on the given atoms from all their partners within rc
+        (exclusions removed): (len(atoms), 3)."""
+        crd = _c32(s.crd if crd is None else crd)
+        atoms = _ci32(atoms)
+        out = np.zeros(3 * len(atoms), np.float64)
+        self.lib.orc_direct_forces_subset_fp64(
+            s.n, crd, _c32(s.charge), _ci32(s.atom_type), _c32(s.pair_A), _c32(s.pair_B), _c32(s.cell),
+            s.cutoff, s.beta, _ci32(s.excl_start), _ci32(s.excl_numbers),
+            _ci32(s.excl_list if len(s.excl_list) else np.zeros(1, np.int32)), len(atoms), atoms, out)
+        return out.reshape(-1, 3)
 
     def direct_sum(self, s, crd=None, per_atom=False):
         crd = _c32(s.crd if crd is None else crd)
@@ -230,6 +245,7 @@ class Reference:
         lib.ref_long_range_factor.restype = C.c_double
         lib.ref_enable_solvent.argtypes = [C.c_int, _i32p, C.c_int, C.c_int, C.c_int]
         lib.ref_set_threads.argtypes = [C.c_int]
+        lib.ref_set_key.argtypes = [C.c_char_p, C.c_char_p]
         if hasattr(lib, "ref_soft_init"):
             lib.ref_soft_init.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p,
                                           _f32p, C.c_float]
@@ -248,6 +264,10 @@ class Reference:
 
     def set_threads(self, t):
         self.lib.ref_set_threads(int(t))
+
+    def set_key(self, key, value):
+        """A control key for the modules of the next init() (value None removes it)."""
+        self.lib.ref_set_key(key.encode(), b"" if value is None else str(value).encode())
 
     def init(self, s, max_neighbor=1200, refresh_interval=0, solvent=False):
         self.s = s

@@ -129,6 +129,16 @@ void ref_set_threads(int threads)
 #endif
 }
 
+// Sets one control key (e.g. neighbor_list_max_atom_in_grid_numbers) for the
+// modules the next ref_init creates; an empty value removes it.
+void ref_set_key(const char* key, const char* value)
+{
+    if (value && value[0])
+        controller.commands[key] = value;
+    else
+        controller.commands.erase(key);
+}
+
 // NEIGHBOR_LIST::Initial + LENNARD_JONES_INFORMATION::Initial + Get_Local
 // (identity atom_local, one rank, no ghosts).  refresh_interval <= 0 selects
 // the skin-triggered rebuild.

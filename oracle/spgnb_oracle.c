@@ -526,6 +526,109 @@ long long orc_direct_sum_fp64(int n, const float* crd, const float* charge, cons
     return p.t.pairs_in_cutoff;
 }
 
+/* FP64 forces on a subset of atoms: for each listed atom i, the force from
+ * every partner j != i with double minimum-image distance < rc, exclusions
+ * removed (either side of the upper-triangular CSR), by the same coarse-cell
+ * sweep and the same pair function as pair_fp64 (Lennard_Jones_force.h:44-73,
+ * vector.hpp:322-327).  For checking large boxes on a sample of atoms.
+ * frc_sub gets 3 doubles per listed atom.  Returns the pairs counted. */
+long long orc_direct_forces_subset_fp64(int n, const float* crd, const float* charge, const int* type,
+                                        const float* A, const float* B, const float* cell, float cutoff, float beta,
+                                        const int* excl_start, const int* excl_numbers, const int* excl_list,
+                                        int n_sub, const int* sub, double* frc_sub)
+{
+    double c[6], ri[6];
+    cell_inverse_fp64(cell, c, ri);
+    double h[3] = {c[0], c[2], c[5]};
+    int m[3];
+    for (int d = 0; d < 3; d++)
+    {
+        m[d] = (int)floor(h[d] / cutoff);
+        if (m[d] < 1) m[d] = 1;
+    }
+    int G = m[0] * m[1] * m[2];
+    int* cell_of = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    int* cstart = (int*)calloc((size_t)G + 1, sizeof(int));
+    int* catoms = (int*)malloc(sizeof(int) * (size_t)(n > 0 ? n : 1));
+    for (int i = 0; i < n; i++)
+    {
+        double x = crd[3 * i], y = crd[3 * i + 1], z = crd[3 * i + 2];
+        double sf[3] = {x * ri[0] + y * ri[1] + z * ri[3], y * ri[2] + z * ri[4], z * ri[5]};
+        int id[3];
+        for (int d = 0; d < 3; d++)
+        {
+            double f = sf[d] - floor(sf[d]);
+            id[d] = (int)(f * m[d]);
+            if (id[d] >= m[d]) id[d] = m[d] - 1;
+        }
+        cell_of[i] = (id[0] * m[1] + id[1]) * m[2] + id[2];
+        cstart[cell_of[i] + 1]++;
+    }
+    for (int g = 0; g < G; g++) cstart[g + 1] += cstart[g];
+    {
+        int* fill = (int*)malloc(sizeof(int) * (size_t)G);
+        memcpy(fill, cstart, sizeof(int) * (size_t)G);
+        for (int i = 0; i < n; i++) catoms[fill[cell_of[i]]++] = i;
+        free(fill);
+    }
+    long long pairs = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : pairs)
+    for (int q = 0; q < n_sub; q++)
+    {
+        const int i = sub[q];
+        double fx = 0, fy = 0, fz = 0;
+        int g = cell_of[i];
+        int gx = g / (m[1] * m[2]), gy = (g / m[2]) % m[1], gz = g % m[2];
+        int rx = m[0] < 3 ? m[0] : 3, ry = m[1] < 3 ? m[1] : 3, rz = m[2] < 3 ? m[2] : 3;
+        for (int ax = 0; ax < rx; ax++)
+            for (int ay = 0; ay < ry; ay++)
+                for (int az = 0; az < rz; az++)
+                {
+                    int hx = m[0] < 3 ? ax : (gx + ax - 1 + m[0]) % m[0];
+                    int hy = m[1] < 3 ? ay : (gy + ay - 1 + m[1]) % m[1];
+                    int hz = m[2] < 3 ? az : (gz + az - 1 + m[2]) % m[2];
+                    int hcell = (hx * m[1] + hy) * m[2] + hz;
+                    for (int b = cstart[hcell]; b < cstart[hcell + 1]; b++)
+                    {
+                        int j = catoms[b];
+                        if (j == i) continue;
+                        if (excluded_upper(i < j ? i : j, i < j ? j : i, excl_start, excl_numbers, excl_list)) continue;
+                        double dx = (double)crd[3 * j] - crd[3 * i];
+                        double dy = (double)crd[3 * j + 1] - crd[3 * i + 1];
+                        double dz = (double)crd[3 * j + 2] - crd[3 * i + 2];
+                        double sx = floor(dx * ri[0] + dy * ri[1] + dz * ri[3] + 0.5);
+                        double sy = floor(dy * ri[2] + dz * ri[4] + 0.5);
+                        double sz = floor(dz * ri[5] + 0.5);
+                        dx -= sx * c[0] + sy * c[1] + sz * c[3];
+                        dy -= sy * c[2] + sz * c[4];
+                        dz -= sz * c[5];
+                        double r2 = dx * dx + dy * dy + dz * dz;
+                        double r = sqrt(r2);
+                        if (!(r < cutoff)) continue;
+                        int p = lj_index(type[i], type[j]);
+                        double a = A[p], bb = B[p];
+                        double r6 = 1.0 / (r2 * r2 * r2);
+                        double r8 = r6 / r2;
+                        double qq = (double)charge[i] * (double)charge[j];
+                        double br = beta * r;
+                        double fscal = (bb - a * r6) * r8 -
+                                       qq / (r2 * r) * (erfc(br) + 1.1283791670955126 * br * exp(-br * br));
+                        fx += fscal * dx;
+                        fy += fscal * dy;
+                        fz += fscal * dz;
+                        pairs++;
+                    }
+                }
+        frc_sub[3 * q] = fx;
+        frc_sub[3 * q + 1] = fy;
+        frc_sub[3 * q + 2] = fz;
+    }
+    free(cell_of);
+    free(cstart);
+    free(catoms);
+    return pairs;
+}
+
 /* ------------------------------------------------- FP64 soft-core pair sum */
 /* LJ_SOFT_CORE's pair (SPONGE/Lennard_Jones_force/LJ_soft_core.cpp:198-414,
  * pair functions LJ_soft_core.h:33-150) in double.  Owner i < j,

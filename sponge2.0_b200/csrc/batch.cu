@@ -578,6 +578,11 @@ int create_common(spgnb_batch* b, const NLPoolSpec& spec, long long ex_cap, int 
     spgnb_nl_options nlo;
     spgnb_nl_default_options(&nlo);
     nlo.refresh_interval = 0;
+    // the reference's grid gives each row's last cell the remainder of the
+    // box, so in small boxes edge cells hold well over the reference's
+    // 150-atom buckets; this engine has no such buckets, only the in-cell sort
+    // capacity, so the grid flag is raised at that capacity
+    nlo.max_atom_in_grid_numbers = kMaxCellAtoms;
     nlo.skin_permit = b->opt.skin_permit;
     nlo.export_atom_groups = 0;
     nlo.prune_buffer = b->opt.prune_buffer;
@@ -638,13 +643,23 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
     }
     Uploader up{ps};
     int sid = -1;
-    st = nl_admit(b->nl, z.sh, &z.run_start, &z.runs, s, &sid, up);
-    if (st)
-    {
+    // after the first queued copy a failure must keep the pinned buffer from
+    // being reused until the copies already queued from it have run, and hand
+    // back the ranges (and the system id, when one was taken)
+    auto bail = [&](int code) {
+        cudaEventRecord(ps->ev, s);
+        ps->busy = true;
+        if (sid >= 0) nl_retire(b->nl, sid, s);
         b->water_pool.release(wb, z.water_numbers);
         b->ex_pool.release(eb, ne);
         b->atom_pool.release(ab, z.N);
-        return st == SPGNB_E_OOM ? fail(SPGNB_E_OOM, "batch: no free system id, cells or clusters now") : st;
+        return code;
+    };
+    st = nl_admit(b->nl, z.sh, &z.run_start, &z.runs, s, &sid, up);
+    if (st)
+    {
+        sid = -1;  // nl_admit has released what it took
+        return bail(st == SPGNB_E_OOM ? fail(SPGNB_E_OOM, "batch: no free system id, cells or clusters now") : st);
     }
     if (z.water_numbers > 0 && !b->have_water)
     {
@@ -676,7 +691,7 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
         (st = putv(b->d_ex_start, ab, ex_start)) || (st = putv(b->d_ex_num, ab, z.ex_num)) ||
         (st = putv(b->d_ex_list, eb, ex_list)) || (st = putv(b->d_waters, wb, waters)) ||
         (st = putv(b->d_fps, sid, fp)) || (st = putv(b->d_ndof, sid, ndof)) || (st = putv(b->d_left, sid, left)))
-        return st;
+        return bail(st);
     SPGNB_CUDA(cudaMemsetAsync(b->d_frc + ab, 0, sizeof(float3) * z.N, s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_steps + sid, 0, sizeof(int), s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_kin + sid, 0, sizeof(long long), s));

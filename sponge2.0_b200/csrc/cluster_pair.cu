@@ -325,8 +325,9 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
 // registers as packed pairs, so every instruction of the pair function
 // serves two pairs (FP32x2).  The LJ coefficients of a pair of cluster atoms
 // against the partner's type come as one float4 {-A_a, -A_b, B_a, B_b} of
-// the T^3 table.  Partner gathers run one iteration ahead of their use, list
-// words two.
+// the T^3 table.  Partner records are copied into shared memory by
+// asynchronous copies (cp.async) one iteration ahead of their use, list words
+// two, so their latency overlaps the pair arithmetic.
 //
 // HALF (forces, and forces with energy/virial totals): the upper part only,
 // each pair once; a lane holds all 8 atoms, the partner's force (summed over
@@ -345,27 +346,37 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
 //
 // MODE 0: forces.  MODE 1: + energy and virial totals.  MODE 2: + per-atom
 // outputs, totals summed from them.
-template <int MODE, int FIT, bool TRI, bool HALF>
+template <int MODE, int FIT, bool TRI, bool HALF, int NI>
 __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
     k_pair8(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys, int n_clusters,
             int list_cap, const int* __restrict__ cl_sys, const int* __restrict__ lcount,
             const unsigned* __restrict__ words, const int* __restrict__ slot_atom, const int4* __restrict__ cl_q,
             const float4* __restrict__ pos, const int4* __restrict__ aux, const float4* __restrict__ t4,
-            float3* __restrict__ frc, long long* __restrict__ facc, long long* __restrict__ totals, OwnerMap om,
-            PerAtomOut pa, const int* __restrict__ only, int* __restrict__ counters)
+            float3* __restrict__ frc, long long* __restrict__ facc, long long* __restrict__ oacc,
+            long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, const int* __restrict__ only,
+            int* __restrict__ counters, int max_types)
 {
     constexpr bool EN = MODE >= 1;
     constexpr bool PA = MODE >= 2;
-    static_assert(!(PA && HALF), "per-atom outputs use the full list");
-    constexpr int NI = HALF ? 8 : 4;  // cluster atoms a lane holds
-    constexpr int NP = NI / 2;        // as packed pairs
-    constexpr int WPI = 4 * NI;       // words an iteration takes (32, or 16 twice)
+    static_assert(NI == 8 || NI == 4, "a lane holds all of the cluster's atoms or half of them");
+    // NI: cluster atoms a lane holds (with 4, two half-warps take the same
+    // words, each for half of the atoms)
+    constexpr int NP = NI / 2;   // as packed pairs
+    constexpr int WPI = 4 * NI;  // words an iteration takes
     __shared__ long long red[kPairWarps][8];  // per-warp fixed-point totals
     __shared__ int is_last;
+    extern __shared__ float4 rows_all[];      // per warp: 4 x max_types coefficient rows
+    __shared__ unsigned wring_all[kPairWarps][3][32];       // per warp: list words in flight
+    __shared__ __align__(16) float4 jpos_all[kPairWarps][2][32];  // partner offsets and charges in flight
+    __shared__ __align__(16) int4 jaux_all[kPairWarps][2][32];    // partner aux records in flight
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
-    const int sub = HALF ? 0 : lane >> 4;  // the half of the cluster this lane holds (full list)
+    const int sub = NI == 8 ? 0 : lane >> 4;  // the half of the cluster this lane holds (NI = 4)
     const int lw = lane & (WPI - 1);      // the word of an iteration this lane takes
+    float4* __restrict__ rows = rows_all + w * 4 * max_types;
+    unsigned(&wring)[3][32] = wring_all[w];
+    float4(&jpos)[2][32] = jpos_all[w];
+    int4(&jaux)[2][32] = jaux_all[w];
     if (EN && lane < 8) red[w][lane] = 0;
     __syncwarp();
     int cur_sys = -1;  // the system red[w] accumulates for
@@ -405,7 +416,6 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
         const int nt = P.n_types;
         // this lane's cluster atoms, negated, as packed pairs
         float2 npx[NP], npy[NP], npz[NP], qi[NP];
-        int rowb[NP];
         int gi[NI];
 #pragma unroll
         for (int p = 0; p < NP; p++)
@@ -417,9 +427,24 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
             npy[p] = make_float2(-u0.y, -u1.y);
             npz[p] = make_float2(-u0.z, -u1.z);
             qi[p] = make_float2(u0.w, u1.w);
-            rowb[p] = P.t4_begin + (((x0.x >> 22) & 0x7f) * nt + ((x1.x >> 22) & 0x7f)) * nt;
             gi[2 * p] = x0.w;
             gi[2 * p + 1] = x1.w;
+        }
+        // the coefficient rows of the cluster's four atom pairs against every
+        // partner type, {-A_a, -A_b, B_a, B_b}, staged in shared memory
+        {
+            int rq[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++)
+                rq[q] = P.t4_begin + (((aux[s0 + 2 * q].x >> 22) & 0x7f) * nt + ((aux[s0 + 2 * q + 1].x >> 22) & 0x7f)) * nt;
+            __syncwarp();  // the previous cluster's rows are no longer read
+            for (int e = lane; e < 4 * nt; e += 32)
+            {
+                const int q = e / nt;
+                const int r = q == 0 ? rq[0] : (q == 1 ? rq[1] : (q == 2 ? rq[2] : rq[3]));
+                rows[e] = __ldg(t4 + r + (e - q * nt));
+            }
+            __syncwarp();
         }
         float2 fx[NP], fy[NP], fz[NP];
 #pragma unroll
@@ -435,23 +460,43 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
 
         const unsigned* __restrict__ wb = words + (size_t)c * list_cap;
         // the k-th word of the list: the upper part, then the lower part
-        auto word_at = [&](int k) { return __ldg(k < nh ? wb + k : wb + (list_cap - nlo) + (k - nh)); };
-        unsigned wc = word_at(lw);
-        unsigned wn = WPI < total ? word_at(WPI + lw) : wc;
-        int jc = slot0 + (int)(wc & kWordSlotMask);
-        float4 pjc = pos[jc];
-        int4 xjc = aux[jc];
+        auto word_ptr = [&](int k) { return k < nh ? wb + k : wb + (list_cap - nlo) + (k - nh); };
+        // a three-deep ring of list words and a two-deep ring of partner
+        // records in shared memory, filled by asynchronous copies: a lane
+        // only ever reads what it copied itself, so no warp barrier is needed
+        auto stage_word = [&](int it) {
+            if (it * WPI < total) cp_async(&wring[it % 3][lane], word_ptr(it * WPI + lw), 4);
+            cp_async_commit();
+        };
+        auto stage_partner = [&](int it, unsigned w) {
+            if (it * WPI < total)
+            {
+                const int j = slot0 + (int)(w & kWordSlotMask);
+                cp_async(&jpos[it & 1][lane], pos + j, 16);
+                cp_async(&jaux[it & 1][lane], aux + j, 16);
+            }
+            cp_async_commit();
+        };
+        const int iters = total / WPI;
+        stage_word(0);
+        stage_word(1);
+        cp_async_wait_prior();
+        unsigned wc = wring[0][lane];
+        stage_partner(0, wc);
 #pragma unroll 1
-        for (int k0 = 0; k0 < total; k0 += WPI)
+        for (int it = 0; it < iters; it++)
         {
-            // the next iteration's partner and the word after it
-            const unsigned wnn = k0 + 2 * WPI < total ? word_at(k0 + 2 * WPI + lw) : wn;
-            const int jn = slot0 + (int)(wn & kWordSlotMask);
-            const float4 pjn = pos[jn];
-            const int4 xjn = aux[jn];
+            // in flight, oldest first: word it+1, partner it, then word it+2
+            stage_word(it + 2);
+            cp_async_wait_prior();
+            const unsigned wn = wring[(it + 1) % 3][lane];
+            const float4 pjc = jpos[it & 1][lane];
+            const int4 xjc = jaux[it & 1][lane];
+            const int jc = slot0 + (int)(wc & kWordSlotMask);
+            stage_partner(it + 1, wn);
 
             const unsigned m8 = (wc >> kWordMaskShift) & 0xffu;
-            const unsigned mi = HALF ? m8 : (m8 >> (4 * sub)) & 0xfu;
+            const unsigned mi = NI == 8 ? m8 : (m8 >> (4 * sub)) & 0xfu;
             const float ux = centre_step(xjc.x, ci.x), uy = centre_step(xjc.y, ci.y), uz = centre_step(xjc.z, ci.z);
             // the partner in the frame of the cluster's centre
             float sx = __fmaf_rn(ux, qc.a11, pjc.x);
@@ -469,6 +514,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
             const int gj = xjc.w;
             const float2 qj = f2(pjc.w);
             float2 hx = f2(0.0f), hy = f2(0.0f), hz = f2(0.0f);  // the partner's force, negated
+            float2 jo[(PA && HALF) ? 8 : 1];                        // the partner's owned sums
+#pragma unroll
+            for (int q = 0; q < ((PA && HALF) ? 8 : 1); q++) jo[q] = f2(0.0f);
 #pragma unroll
             for (int p = 0; p < NP; p++)
             {
@@ -495,7 +543,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
                 const bool inA = ((mi >> (2 * p)) & 1u) && r2.x < pp.rc2;
                 const bool inB = ((mi >> (2 * p + 1)) & 1u) && r2.y < pp.rc2;
-                const float4 ab = __ldg(t4 + rowb[p] + tj);
+                const float4 ab = rows[(sub * NP + p) * nt + tj];
                 float2 elj, ec;
                 float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(qj, qi[p]), make_float2(ab.x, ab.y),
                                                  make_float2(ab.z, ab.w), pp, elj, ec);
@@ -523,24 +571,62 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 }
                 if (PA)
                 {
-                    // the pair's owner is the lower global index
-                    const bool oA = inA && gi[2 * p] < gj, oB = inB && gi[2 * p + 1] < gj;
-                    own[p][0] = __fadd2_rn(own[p][0], make_float2(oA ? elj.x : 0.0f, oB ? elj.y : 0.0f));
-                    own[p][1] = __fadd2_rn(own[p][1], make_float2(oA ? ec.x : 0.0f, oB ? ec.y : 0.0f));
-                    const float2 mgx = make_float2(oA ? gx.x : 0.0f, oB ? gx.y : 0.0f);
-                    const float2 mgy = make_float2(oA ? gy.x : 0.0f, oB ? gy.y : 0.0f);
-                    const float2 mgz = make_float2(oA ? gz.x : 0.0f, oB ? gz.y : 0.0f);
-                    own[p][2] = __ffma2_rn(mgx, dx, own[p][2]);
-                    own[p][3] = __ffma2_rn(mgx, dy, own[p][3]);
-                    own[p][4] = __ffma2_rn(mgy, dy, own[p][4]);
-                    own[p][5] = __ffma2_rn(mgx, dz, own[p][5]);
-                    own[p][6] = __ffma2_rn(mgy, dz, own[p][6]);
-                    own[p][7] = __ffma2_rn(mgz, dz, own[p][7]);
+                    // the pair's owner is the lower global index: this lane's
+                    // atom (kept over the list) or, over the half list, the
+                    // partner (summed over the word's atoms)
+                    const float2 wi = make_float2(gi[2 * p] < gj ? 1.0f : 0.0f, gi[2 * p + 1] < gj ? 1.0f : 0.0f);
+                    const float2 v[8] = {make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f),
+                                         make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f),
+                                         __fmul2_rn(gx, dx), __fmul2_rn(gx, dy), __fmul2_rn(gy, dy),
+                                         __fmul2_rn(gx, dz), __fmul2_rn(gy, dz), __fmul2_rn(gz, dz)};
+#pragma unroll
+                    for (int q = 0; q < 8; q++) own[p][q] = __ffma2_rn(v[q], wi, own[p][q]);
+                    if (HALF)
+                    {
+                        const float2 wj = __fadd2_rn(f2(1.0f), __fmul2_rn(wi, kPk[kPkMinusOne]));
+#pragma unroll
+                        for (int q = 0; q < 8; q++) jo[q] = __ffma2_rn(v[q], wj, jo[q]);
+                    }
+                }
+            }
+            if (PA && HALF)
+            {
+                // the partner's owned sums over this word: raw fixed point to
+                // its staging (scaled in the finishing pass)
+                float js[8];
+                bool any = false;
+#pragma unroll
+                for (int q = 0; q < 8; q++)
+                {
+                    js[q] = jo[q].x + jo[q].y;
+                    if (NI == 4) js[q] += __shfl_xor_sync(0xffffffffu, js[q], 16);
+                    any |= js[q] != 0.0f;
+                }
+                if (any && sub == 0)
+                {
+                    unsigned long long* oa = (unsigned long long*)(oacc + 8 * (size_t)jc);
+#pragma unroll
+                    for (int q = 0; q < 8; q++)
+                    {
+                        const long long v = __float2ll_rn(js[q] * kTwoPow32);
+                        if (v) atomicAdd(oa + q, (unsigned long long)v);
+                    }
                 }
             }
             if (HALF)
             {
                 // the partner's force: minus the sum over the cluster's atoms
+                if (NI == 4)
+                {
+                    // the other half-warp holds the other four atoms' share
+                    hx = __fadd2_rn(hx, make_float2(__shfl_xor_sync(0xffffffffu, hx.x, 16),
+                                                    __shfl_xor_sync(0xffffffffu, hx.y, 16)));
+                    hy = __fadd2_rn(hy, make_float2(__shfl_xor_sync(0xffffffffu, hy.x, 16),
+                                                    __shfl_xor_sync(0xffffffffu, hy.y, 16)));
+                    hz = __fadd2_rn(hz, make_float2(__shfl_xor_sync(0xffffffffu, hz.x, 16),
+                                                    __shfl_xor_sync(0xffffffffu, hz.y, 16)));
+                    if (sub) hx = hy = hz = f2(0.0f);
+                }
                 const long long qx = __float2ll_rn(-(hx.x + hx.y) * kTwoPow32);
                 const long long qy = __float2ll_rn(-(hy.x + hy.y) * kTwoPow32);
                 const long long qz = __float2ll_rn(-(hz.x + hz.y) * kTwoPow32);
@@ -550,11 +636,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 if (qz) atomicAdd(fa + 2, (unsigned long long)qz);
             }
             wc = wn;
-            wn = wnn;
-            jc = jn;
-            pjc = pjn;
-            xjc = xjn;
         }
+        cp_async_wait_all();
 
         // the cluster's forces: int64 per lane, summed over the lanes by a
         // reduce-scatter (lanes 4a..4a+3 end with atom a)
@@ -563,7 +646,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
         for (int a = 0; a < 8; a++)
         {
             const int p = (a % NI) / 2;
-            const bool mine = HALF || (a / NI) == sub;
+            const bool mine = NI == 8 || (a / NI) == sub;
             const float sxv = (a & 1) ? fx[p].y : fx[p].x, syv = (a & 1) ? fy[p].y : fy[p].x,
                         szv = (a & 1) ? fz[p].y : fz[p].x;
             vx[a] = mine ? __float2ll_rn(sxv * kTwoPow32) : 0ll;
@@ -618,34 +701,39 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 const bool mine = (a / NI) == sub;
                 float v[8];
 #pragma unroll
-                for (int q = 0; q < 8; q++)
-                {
-                    const float sg = q >= 2 ? -1.0f : (q == 0 ? kLjEnergyScale : 1.0f);
-                    v[q] = mine ? sg * ((a & 1) ? own[p][q].y : own[p][q].x) : 0.0f;
-                }
-                // lanes 4q..4q+3 end with value q of atom a; an atom's energy is
-                // value 0 + value 1 (lanes 0 and 4)
+                for (int q = 0; q < 8; q++) v[q] = mine ? ((a & 1) ? own[p][q].y : own[p][q].x) : 0.0f;
+                // lanes 4q..4q+3 end with value q of atom a
                 const float val = reduce_scatter8(v, lane);
-                const float ec_val = __shfl_down_sync(0xffffffffu, val, 4);
+                if (HALF)
+                {
+                    // raw fixed point to the atom's staging (scaled in the finishing pass)
+                    const long long r = __float2ll_rn(val * kTwoPow32);
+                    if ((lane & 3) == 0 && r) atomicAdd((unsigned long long*)(oacc + 8 * (size_t)(s0 + a) + va), (unsigned long long)r);
+                    continue;
+                }
+                const float sg = va >= 2 ? -1.0f : (va == 0 ? kLjEnergyScale : 1.0f);
+                const float sv = sg * val;
+                // an atom's energy is value 0 + value 1 (lanes 0 and 4)
+                const float ec_val = __shfl_down_sync(0xffffffffu, sv, 4);
                 if ((lane & 3) == 0)
                 {
                     const bool twice = va == 3 || va == 5 || va == 6;
-                    red[w][va] += __double2ll_rn((double)val * (twice ? 2.0 : 1.0) * kEnergyScale);
+                    red[w][va] += __double2ll_rn((double)sv * (twice ? 2.0 : 1.0) * kEnergyScale);
                     const int ai = slot_atom[s0 + a];
                     if (ai >= 0)
                     {
                         const int o = om.remap(ai);
                         if (va == 0)
                         {
-                            if (pa.energy) atomicAdd(pa.energy + o, val + ec_val);
-                            if (pa.lj_energy) atomicAdd(pa.lj_energy + o, val);
+                            if (pa.energy) atomicAdd(pa.energy + o, sv + ec_val);
+                            if (pa.lj_energy) atomicAdd(pa.lj_energy + o, sv);
                         }
                         else if (va == 1)
                         {
-                            if (pa.direct) atomicAdd(pa.direct + o, val);
+                            if (pa.direct) atomicAdd(pa.direct + o, sv);
                         }
                         else if (pa.virial)
-                            atomicAdd(pa.virial + 6 * (size_t)o + (va - 2), twice ? 2.0f * val : val);
+                            atomicAdd(pa.virial + 6 * (size_t)o + (va - 2), twice ? 2.0f * sv : sv);
                     }
                 }
             }
@@ -674,21 +762,26 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
 }
 
 // Finishing pass, one thread per slot: the half-list kernel's int64 force
-// sums go to the caller's float array (and are cleared for the next call),
-// and with the fused PME excluded-pair correction each atom adds its excluded
-// pairs' terms (Particle_Mesh::PME_Excluded_Force_With_Atom_Energy,
-// PM_force.cpp:918-997): its symmetric exclusion list holds both sides of
-// every pair, so each atom computes its own share, F_a += q_a q_x beta^3
-// h(beta r) dr with dr = the reference's minimum image of r_x - r_a, and the
-// pair's owner (lower global index) adds -q_a q_x erf(beta r)/r to the energy
-// and -F (x) dr to its virial.  A thread touches only its own atom's entries.
-template <bool EXCL, bool EN>
+// sums go to the caller's float array, and its owned energy/virial sums
+// (per-atom mode) to the caller's per-atom arrays and the totals, the
+// staging cleared for the next call.  With the fused PME excluded-pair
+// correction each atom also adds its excluded pairs' terms
+// (Particle_Mesh::PME_Excluded_Force_With_Atom_Energy, PM_force.cpp:918-997):
+// its symmetric exclusion list holds both sides of every pair, so each atom
+// computes its own share, F_a += q_a q_x beta^3 h(beta r) dr with dr = the
+// reference's minimum image of r_x - r_a, and the pair's owner (lower global
+// index) adds -q_a q_x erf(beta r)/r to the energy and -F (x) dr to its
+// virial.  A thread touches only its own atom's force.
+template <bool EXCL, bool EN, bool PA>
 __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* __restrict__ cl_sys,
-                       const SysDesc* __restrict__ sys, long long* __restrict__ facc, float3* __restrict__ frc,
+                       const SysDesc* __restrict__ sys, long long* __restrict__ facc, long long* __restrict__ oacc,
+                       float3* __restrict__ frc, long long* __restrict__ totals, OwnerMap om, PerAtomOut pa,
                        ExclFuse xf)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     float ene = 0.0f;
+    long long tq[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // this slot's share of the totals (per-atom mode)
+    int tsys = -1;
     if (s < slots)
     {
         const int a = slot_atom[s];
@@ -704,6 +797,46 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
                 q[0] = 0;
                 q[1] = 0;
                 q[2] = 0;
+            }
+        }
+        if (PA)
+        {
+            long long* q = oacc + 8 * (size_t)s;
+            long long r[8];
+            long long any = 0;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+            {
+                r[k] = q[k];
+                any |= r[k];
+            }
+            if (any)
+            {
+#pragma unroll
+                for (int k = 0; k < 8; k++) q[k] = 0;
+                const int sy = cl_sys[s >> 3];
+                // raw sums: -12 E_lj, E_c, and +g (x) d; the virial is -g (x) d
+                // with the symmetric off-diagonal terms twice the one summed
+                double v[8];
+#pragma unroll
+                for (int k = 0; k < 8; k++)
+                {
+                    const double sg = k == 0 ? (double)kLjEnergyScale
+                                             : (k == 1 ? 1.0 : ((k == 3 || k == 5 || k == 6) ? -2.0 : -1.0));
+                    v[k] = (double)r[k] * sg;
+                    tq[k] = __double2ll_rn(v[k]);
+                }
+                tsys = sy;
+                if (a >= 0)
+                {
+                    const int o = om.remap(a);
+                    const float elj = (float)(v[0] * kForceUnscale), ec = (float)(v[1] * kForceUnscale);
+                    if (pa.energy) atomicAdd(pa.energy + o, elj + ec);
+                    if (pa.lj_energy) atomicAdd(pa.lj_energy + o, elj);
+                    if (pa.direct) atomicAdd(pa.direct + o, ec);
+                    if (pa.virial)
+                        for (int k = 0; k < 6; k++) atomicAdd(pa.virial + 6 * (size_t)o + k, (float)(v[2 + k] * kForceUnscale));
+                }
             }
         }
         if (a >= 0)
@@ -767,6 +900,36 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
             }
         }
     }
+    if (PA)
+    {
+        // the totals: summed over the block when its slots belong to one
+        // system (the usual case), else added slot by slot
+        __shared__ long long bsum[8];
+        __shared__ int bsys;
+        if (threadIdx.x == 0) bsys = -2;
+        if (threadIdx.x < 8) bsum[threadIdx.x] = 0;
+        __syncthreads();
+        if (tsys >= 0) atomicCAS(&bsys, -2, tsys);
+        __syncthreads();
+        const int bs = bsys;
+        __syncthreads();
+        if (tsys >= 0)
+        {
+            const bool same = tsys == bs;
+#pragma unroll
+            for (int k = 0; k < 8; k++)
+                if (tq[k])
+                {
+                    if (same)
+                        atomicAdd((unsigned long long*)&bsum[k], (unsigned long long)tq[k]);
+                    else
+                        atomicAdd((unsigned long long*)&totals[8 * tsys + k], (unsigned long long)tq[k]);
+                }
+        }
+        __syncthreads();
+        if (threadIdx.x < 8 && bs >= 0 && bsum[threadIdx.x])
+            atomicAdd((unsigned long long*)&totals[8 * bs + threadIdx.x], (unsigned long long)bsum[threadIdx.x]);
+    }
     if (EXCL && EN)
     {
         // the correction's energy total: one atomic per warp
@@ -790,16 +953,21 @@ int resident_blocks(K kernel, int threads, size_t smem)
     return per_sm * num_sms();
 }
 
-template <int M, int F, bool T, bool H>
+template <int M, int F, bool T, bool H, int NI>
 int launch_pair(const ForceInputs& in, cudaStream_t s)
 {
     const spgnb_nl* nl = in.nl;
-    const int grid = std::max(1, std::min(resident_blocks(k_pair8<M, F, T, H>, kPairWarps * 32, 0),
+    const int mt = in.p0.n_types;
+    const size_t smem = sizeof(float4) * kPairWarps * 4 * mt;
+    const int grid = std::max(1, std::min(resident_blocks(k_pair8<M, F, T, H, NI>, kPairWarps * 32, smem),
                                           (nl->clusters_cap + kPairWarps - 1) / kPairWarps));
-    k_pair8<M, F, T, H><<<grid, kPairWarps * 32, 0, s>>>(
+    if (smem > 48 * 1024)
+        SPGNB_CUDA(cudaFuncSetAttribute(k_pair8<M, F, T, H, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        (int)smem));
+    k_pair8<M, F, T, H, NI><<<grid, kPairWarps * 32, smem, s>>>(
         in.p0, in.d_fps, nl->d_sys, nl->clusters_cap, kClusterSize * nl->slot_cap, nl->d_cl_sys, nl->d_pcount,
-        nl->d_pwords, nl->d_slot_atom, nl->d_cl_q, in.slot_pos, in.slot_aux, in.t4, in.frc, nl->d_facc, in.totals,
-        in.om, in.pa, in.only, nl->d_counters);
+        nl->d_pwords, nl->d_slot_atom, nl->d_cl_q, in.slot_pos, in.slot_aux, in.t4, in.frc, nl->d_facc, nl->d_oacc,
+        in.totals, in.om, in.pa, in.only, nl->d_counters, mt);
     SPGNB_CHECK_LAUNCH("k_pair8");
     return SPGNB_OK;
 }
@@ -807,8 +975,9 @@ int launch_pair(const ForceInputs& in, cudaStream_t s)
 template <int M, int F>
 int launch_pair_t(const ForceInputs& in, bool tri, cudaStream_t s)
 {
-    constexpr bool H = M < 2;
-    return tri ? launch_pair<M, F, true, H>(in, s) : launch_pair<M, F, false, H>(in, s);
+    // every mode walks the half list; the per-atom mode holds four atoms a lane
+    constexpr int NI = 8;
+    return tri ? launch_pair<M, F, true, true, NI>(in, s) : launch_pair<M, F, false, true, NI>(in, s);
 }
 
 template <int M>
@@ -870,23 +1039,30 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
         st = launch_pair_ft<2>(in, nl->triclinic, s);
     if (st) return st;
     if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
-    const bool half_list = in.mode < 2;
     const bool excl = in.xf.list != nullptr;
-    if (half_list || excl)
+    const int blocks = (slots + 255) / 256;
+    if (in.mode == 2)
     {
-        long long* facc = half_list ? nl->d_facc : nullptr;
-        const int blocks = (slots + 255) / 256;
-        if (excl && in.mode >= 1)
-            k_fin8<true, true><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, facc, in.frc,
-                                                      in.xf);
-        else if (excl)
-            k_fin8<true, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, facc,
-                                                       in.frc, in.xf);
+        if (excl)
+            k_fin8<true, true, true><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
+                                                            nl->d_facc, nl->d_oacc, in.frc, in.totals, in.om, in.pa,
+                                                            in.xf);
         else
-            k_fin8<false, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, facc,
-                                                        in.frc, in.xf);
-        SPGNB_CHECK_LAUNCH("k_fin8");
+            k_fin8<false, true, true><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
+                                                             nl->d_facc, nl->d_oacc, in.frc, in.totals, in.om, in.pa,
+                                                             in.xf);
     }
+    else if (excl && in.mode == 1)
+        k_fin8<true, true, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+                                                         nullptr, in.frc, in.totals, in.om, in.pa, in.xf);
+    else if (excl)
+        k_fin8<true, false, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
+                                                          nl->d_facc, nullptr, in.frc, in.totals, in.om, in.pa, in.xf);
+    else
+        k_fin8<false, false, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
+                                                           nl->d_facc, nullptr, in.frc, in.totals, in.om, in.pa,
+                                                           in.xf);
+    SPGNB_CHECK_LAUNCH("k_fin8");
     return SPGNB_OK;
 }
 

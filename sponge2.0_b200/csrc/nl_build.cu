@@ -970,6 +970,7 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_pwords);
     dfree(nl->d_pcount);
     dfree(nl->d_facc);
+    dfree(nl->d_oacc);
     dfree(nl->d_pref);
     dfree(nl->d_counters);
     dfree(nl->d_nl);
@@ -1100,6 +1101,8 @@ int alloc_nl(spgnb_nl* nl)
     if ((st = dalloc(&nl->d_pcount, slots))) return st;
     if ((st = dalloc(&nl->d_facc, 3 * (size_t)slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_facc, 0, sizeof(long long) * 3 * (size_t)slots));
+    if ((st = dalloc(&nl->d_oacc, 8 * (size_t)slots))) return st;
+    SPGNB_CUDA(cudaMemset(nl->d_oacc, 0, sizeof(long long) * 8 * (size_t)slots));
     if ((st = dalloc(&nl->d_pref, slots))) return st;
     SPGNB_CUDA(cudaMemset(nl->d_pcount, 0, sizeof(int) * slots));
     if ((st = dalloc(&nl->d_cl_cell, nl->clusters_cap))) return st;
@@ -1281,17 +1284,20 @@ int nl_admit(spgnb_nl* nl, SysHost sh, const std::vector<int>* run_start, const 
     for (int g = 0; g <= G; g++) sa[g] = (*run_start)[g] + (int)rb;
     nl->h_desc[sid] = make_desc(sh, nl->opt.skin_permit);
     nl->h_desc[sid].prune_r2 = prune_r2_of(nl->prune_rc, nl->opt.prune_buffer);
-    if ((st = up.put(nl->d_sys + sid, &nl->h_desc[sid], sizeof(SysDesc), s)) ||
-        (st = up.put(nl->d_runs + rb, ra.data(), sizeof(int2) * nr, s)) ||
-        (st = up.put(nl->d_run_start + cb, sa.data(), sizeof(int) * (G + 1), s)))
-        return st;
-    if ((st = fill_int(nl->d_atom_sys + sh.atom_begin, sh.atom_count, sid, s))) return st;
-    if ((st = fill_int(nl->d_cell_sys + cb, G, sid, s))) return st;
-    if ((st = fill_int(nl->d_cl_sys + clb, cl_cap, sid, s))) return st;
-    k_sys_flags<<<1, 1, 0, s>>>(sid, 1, nl->d_live, nl->d_need, nl->d_prune, nl->d_ncl);
-    SPGNB_CHECK_LAUNCH("k_sys_flags");
+    // recorded before the uploads, so a failing one can hand everything back
     nl->sys[sid] = sh;
     nl->live[sid] = 1;
+    if ((st = up.put(nl->d_sys + sid, &nl->h_desc[sid], sizeof(SysDesc), s)) ||
+        (st = up.put(nl->d_runs + rb, ra.data(), sizeof(int2) * nr, s)) ||
+        (st = up.put(nl->d_run_start + cb, sa.data(), sizeof(int) * (G + 1), s)) ||
+        (st = fill_int(nl->d_atom_sys + sh.atom_begin, sh.atom_count, sid, s)) ||
+        (st = fill_int(nl->d_cell_sys + cb, G, sid, s)) || (st = fill_int(nl->d_cl_sys + clb, cl_cap, sid, s)))
+    {
+        nl_retire(nl, sid, s);
+        return st;
+    }
+    k_sys_flags<<<1, 1, 0, s>>>(sid, 1, nl->d_live, nl->d_need, nl->d_prune, nl->d_ncl);
+    SPGNB_CHECK_LAUNCH("k_sys_flags");
     nl->triclinic = nl->triclinic || sh.triclinic;
     *id = sid;
     return SPGNB_OK;
@@ -1340,7 +1346,7 @@ size_t nl_device_bytes(const spgnb_nl* nl)
     const size_t n = nl->n_cap, G = nl->G, S = nl->S + 1, C = nl->clusters_cap, slots = C * kClusterSize;
     size_t b = 0;
     b += n * (4 + 4 + 4 + 16 + 4);                                   // atom system, cell, shift, wrapped, slot
-    b += slots * (4 + 4 + 16 + 16 + 8 + 4 + 4 + 16);                 // per-slot arrays
+    b += slots * (4 + 4 + 16 + 4 + 16 + 8 + 4 + 4 + 24 + 64 + 16);   // per-slot arrays (with the int64 staging)
     b += slots * (size_t)nl->slot_cap * 4;                           // pruned lists
     b += C * (4 + 4 + 16 + 16 + 16 + 4) + 16;                        // per-cluster arrays
     b += C * (size_t)nl->table_cap * (16 + 8);                       // neighbour tables
@@ -1672,6 +1678,7 @@ int spgnb_nl_get_stats(spgnb_nl* nl, spgnb_nl_stats* out)
     memcpy(&out->full_list_words, &h[kCntWords], sizeof(long long));
     out->prunes = h[kCntPrunes];
     memcpy(&out->pruned_list_words, &h[kCntPWordsLast], sizeof(long long));
+    out->device_bytes = (long long)nl_device_bytes(nl);
     return SPGNB_OK;
 }
 

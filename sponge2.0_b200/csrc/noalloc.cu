@@ -44,6 +44,9 @@ constexpr size_t kScratchBytes = kAccBytes + kPosBytes + kTableBytes;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
+// Device address of the scratch array per device, looked up on a device's
+// first call.  Written without a lock: every writer for a device stores the
+// same address, so a racing second lookup only repeats the first.
 void* g_scratch_addr[kMaxDevices] = {nullptr};
 
 struct Params
@@ -131,8 +134,9 @@ __global__ void k_noalloc_pairs(unsigned char* scratch, Params p, Cell c, Cell r
     {
         const spgnb_atom_group g = nl[i];
         const float4 pi = pos[i];
-        // types outside [0, n_types) are clamped: the table lookups stay
-        // inside the scratch array whatever the input holds
+        // types outside [0, n_types) and partners outside [0, n) are caller
+        // errors: types are clamped and such partners skipped, so every read
+        // stays inside the scratch array and the caller's arrays
         const int ti = min(max(atom_type[i], 0), p.n_types - 1) * p.n_types;
         float fx = 0, fy = 0, fz = 0;
         for (int k = lane; k < g.atom_numbers; k += 32)
@@ -208,7 +212,8 @@ using namespace spgnb;
 
 extern "C" {
 
-int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_numbers, int atom_type_numbers,
+int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_numbers, int ghost_numbers,
+                                      int atom_type_numbers,
                                       const int* d_atom_type, const float* d_pair_A, const float* d_pair_B,
                                       const spgnb_vector* d_crd, const float* d_charge, spgnb_vector* d_frc,
                                       spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, const spgnb_atom_group* d_nl,
@@ -224,6 +229,10 @@ int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_number
                     kNoAllocMaxTypes);
     if (solvent_numbers < 0 || solvent_numbers > local_atom_numbers)
         return fail(SPGNB_E_ARG, "spgnb_lj_pme_direct_force_noalloc: bad solvent_numbers");
+    if (ghost_numbers != 0)
+        return fail(SPGNB_E_UNSUPPORTED,
+                    "spgnb_lj_pme_direct_force_noalloc: ghost atoms (multi-rank domain decomposition) are not "
+                    "supported");
     if (!d_atom_type || !d_pair_A || !d_pair_B || !d_crd || !d_charge || !d_frc || !d_nl)
         return fail(SPGNB_E_ARG, "spgnb_lj_pme_direct_force_noalloc: NULL device pointer");
     if (!(cutoff > 0.0f)) return fail(SPGNB_E_ARG, "spgnb_lj_pme_direct_force_noalloc: cutoff must be positive");

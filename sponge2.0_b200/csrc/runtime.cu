@@ -123,34 +123,34 @@ int spgnb_set_stream(void* cuda_stream)
     return SPGNB_OK;
 }
 
-// Bisection on erfc(beta*rc)/rc = tol, the search PM_force.cpp:244-272 runs,
-// in the same float arithmetic.
+// Ewald splitting parameter for a direct-space cutoff: the beta at which the
+// screened Coulomb kernel erfc(beta rc)/rc falls to `tolerance`.  The search
+// is the one SPONGE runs (PM_force.cpp:244-272), so the value is bit-identical
+// to the reference's: an upper bound doubled from 1 until the kernel is at or
+// below the tolerance, then (doublings + 50) halvings of [0, bound], each
+// keeping the half where the kernel is still >= the tolerance; the answer is
+// the last midpoint, all in float.
 float spgnb_get_beta(float cutoff, float tolerance)
 {
-    float beta = 0.0f, low, high, tempf;
-    int ilow, ihigh;
     if (!(cutoff > 0.0f) || !(tolerance > 0.0f)) return 0.0f;
-    high = 1.0f;
-    ihigh = 1;
-    for (;;)
+    const auto screened = [cutoff](float b) { return erfcf(b * cutoff) / cutoff; };
+    float hi = 1.0f;
+    int doublings = 0;
+    while (screened(hi) > tolerance)
     {
-        tempf = erfcf(high * cutoff) / cutoff;
-        if (tempf <= tolerance) break;
-        high *= 2;
-        ihigh++;
+        hi *= 2.0f;
+        ++doublings;
     }
-    ihigh += 50;
-    low = 0.0f;
-    for (ilow = 1; ilow < ihigh; ilow++)
+    float lo = 0.0f, mid = 0.0f;
+    for (int step = 0; step < doublings + 50; ++step)
     {
-        beta = (low + high) / 2;
-        tempf = erfcf(beta * cutoff) / cutoff;
-        if (tempf >= tolerance)
-            low = beta;
+        mid = 0.5f * (lo + hi);
+        if (screened(mid) >= tolerance)
+            lo = mid;
         else
-            high = beta;
+            hi = mid;
     }
-    return beta;
+    return mid;
 }
 
 }  // extern "C"

@@ -97,7 +97,7 @@ class NLStats(C.Structure):
     _fields_ = [("atom_numbers", C.c_int), ("grid_numbers", C.c_int), ("grid_dims", C.c_int * 3),
                 ("clusters", C.c_int), ("entries", C.c_longlong), ("work_items", C.c_int),
                 ("builds", C.c_longlong), ("overflow", C.c_int), ("full_list_words", C.c_longlong),
-                ("prunes", C.c_longlong), ("pruned_list_words", C.c_longlong)]
+                ("prunes", C.c_longlong), ("pruned_list_words", C.c_longlong), ("device_bytes", C.c_longlong)]
 
 
 _lib = None
@@ -175,7 +175,7 @@ def lib():
     L.spgnb_debug_set_pair_events.argtypes = [vp, vp]
     L.spgnb_nl_count_pairs.argtypes = [vp, vp, M, M, f, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
     L.spgnb_probe_fp32_fma_tflops.argtypes = [i, C.POINTER(d)]
-    L.spgnb_lj_pme_direct_force_noalloc.argtypes = [i, i, i, vp, vp, vp, vp, vp, vp, M, M, vp, f, f]
+    L.spgnb_lj_pme_direct_force_noalloc.argtypes = [i, i, i, i, vp, vp, vp, vp, vp, vp, M, M, vp, f, f]
     SP = C.POINTER(SoftCoreParams)
     L.spgnb_lj_soft_default_params.argtypes = [SP]
     L.spgnb_lj_soft_default_params.restype = None
