@@ -738,7 +738,7 @@ NLPoolSpec pool_spec(const spgnb_batch_pool_options& po, float prune_buffer, int
     double pc, pa;
     nl_capacity_for(po.density * 1.1, 1e30, po.max_cutoff, po.skin, prune_buffer, &pc, &pa);
     sp.table_cap = std::max((int)(pc * 1.3) + 64, 128);
-    sp.slot_cap = (((int)(pa * 1.3) + 63) & ~63) + 128;
+    sp.list_cap = list_cap_for(pa);
     sp.prune_rc = po.max_cutoff;
     return sp;
 }
@@ -753,7 +753,7 @@ double pool_bytes(const spgnb_batch_pool_options& po, float prune_buffer, int at
     probe.clusters_cap = sp.clusters;
     probe.runs_cap = sp.runs;
     probe.table_cap = sp.table_cap;
-    probe.slot_cap = sp.slot_cap;
+    probe.list_cap = sp.list_cap;
     probe.opt.export_atom_groups = 0;
     const long long ex = po.max_excluded > 0 ? po.max_excluded : 2LL * atoms;
     const long long w = po.max_waters > 0 ? po.max_waters : atoms / 3;
@@ -843,7 +843,7 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
     const std::vector<float>& pb = b->h_pair_B;
     std::vector<Staged> z(n_systems);
     long long atoms = 0, ex = 0, waters = 0, cells = 0, clusters = 0, runs = 0;
-    double per_cluster = 0, per_atom = 0;
+    double per_cluster = 0, per_list = 0;
     float rcmax = 0;
     for (int k = 0; k < n_systems && !st; k++)
     {
@@ -859,7 +859,7 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
         double pc, pw;
         nl_capacity_for(y.N / y.volume, y.N, systems[k].cutoff, systems[k].skin, b->opt.prune_buffer, &pc, &pw);
         per_cluster = std::max(per_cluster, pc);
-        per_atom = std::max(per_atom, pw);
+        per_list = std::max(per_list, pw);
         rcmax = std::max(rcmax, systems[k].cutoff);
         if (!y.fp.use_fit) b->fit = false;
     }
@@ -879,7 +879,7 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
     spec.clusters = (int)clusters;
     spec.runs = std::max(1LL, runs);
     spec.table_cap = std::max((int)(per_cluster * 1.3) + 64, 128);
-    spec.slot_cap = (((int)(per_atom * 1.3) + 63) & ~63) + 128;
+    spec.list_cap = list_cap_for(per_list);
     spec.prune_rc = rcmax;
     if (!(st = create_common(b, spec, ex, (int)waters, T, pa.data(), pb.data())))
         for (int k = 0; k < n_systems && !st; k++)

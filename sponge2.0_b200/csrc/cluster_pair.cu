@@ -46,17 +46,28 @@ constexpr int kPairWarps = 4;                       // warps per block of the fo
 // differences of (its high bits are masked off there).  Slot slots_cap is a
 // null slot: 10^4 A away from everything, charge 0.  With pruning on (pref
 // set) the kernel also flags a re-pruning when some atom moved more than half
-// the prune buffer since the last one.
+// the prune buffer since the last one.  It also clears the outputs the force
+// call must start from zero (totals, module-owned per-atom energies).
 __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict__ slot_atom,
                              const int* __restrict__ slot_gid, const int* __restrict__ cl_sys,
                              const SysDesc* __restrict__ sys, const int4* __restrict__ cl_q,
                              const float4* __restrict__ x0, const float4* __restrict__ d0,
                              const float3* __restrict__ crd, const float* __restrict__ charge,
                              const int* __restrict__ local_type, float4* __restrict__ pos, int4* __restrict__ aux,
-                             const float4* __restrict__ pref, float half_buffer2, int* __restrict__ prune)
+                             const float4* __restrict__ pref, float half_buffer2, int* __restrict__ prune,
+                             long long* __restrict__ clear_totals, long long* __restrict__ clear_one,
+                             float* __restrict__ clear_a, float* __restrict__ clear_b, int clear_n)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     bool moved = false;
+    // the outputs the force call zeroes first
+    if (clear_totals && s < 8) clear_totals[s] = 0;
+    if (clear_one && s == 0) *clear_one = 0;
+    for (int k = s; k < clear_n; k += gridDim.x * blockDim.x)
+    {
+        if (clear_a) clear_a[k] = 0.0f;
+        if (clear_b) clear_b[k] = 0.0f;
+    }
     if (s == slots_cap)
     {
         pos[s] = make_float4(1.0e4f, 1.0e4f, 1.0e4f, 0.0f);
@@ -362,11 +373,15 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
     // NI: cluster atoms a lane holds (with 4, two half-warps take the same
     // words, each for half of the atoms)
     constexpr int NP = NI / 2;   // as packed pairs
+    constexpr bool ISM = PA;     // the cluster's atoms in shared memory instead of registers
     constexpr int WPI = 4 * NI;  // words an iteration takes
     __shared__ long long red[kPairWarps][8];  // per-warp fixed-point totals
     __shared__ int is_last;
     extern __shared__ float4 rows_all[];      // per warp: 4 x max_types coefficient rows
     __shared__ unsigned wring_all[kPairWarps][3][32];       // per warp: list words in flight
+    // per warp, when ISM: the cluster's atom pairs {-x, -y | -z, q} and global indices
+    __shared__ float4 iat_all[kPairWarps][4][2];
+    __shared__ int2 igid_all[kPairWarps][4];
     __shared__ __align__(16) float4 jpos_all[kPairWarps][2][32];  // partner offsets and charges in flight
     __shared__ __align__(16) int4 jaux_all[kPairWarps][2][32];    // partner aux records in flight
     const int lane = threadIdx.x & 31;
@@ -375,6 +390,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
     const int lw = lane & (WPI - 1);      // the word of an iteration this lane takes
     float4* __restrict__ rows = rows_all + w * 4 * max_types;
     unsigned(&wring)[3][32] = wring_all[w];
+    float4(&iat)[4][2] = iat_all[w];
+    int2(&igid)[4] = igid_all[w];
     float4(&jpos)[2][32] = jpos_all[w];
     int4(&jaux)[2][32] = jaux_all[w];
     if (EN && lane < 8) red[w][lane] = 0;
@@ -415,20 +432,38 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
         const int4 ci = cl_q[c];
         const int nt = P.n_types;
         // this lane's cluster atoms, negated, as packed pairs
-        float2 npx[NP], npy[NP], npz[NP], qi[NP];
-        int gi[NI];
-#pragma unroll
-        for (int p = 0; p < NP; p++)
+        // (the per-atom mode keeps them in shared memory instead: its owned
+        // sums already take 64 registers)
+        float2 npx[ISM ? 1 : NP], npy[ISM ? 1 : NP], npz[ISM ? 1 : NP], qi[ISM ? 1 : NP];
+        int gi[ISM ? 1 : NI];
+        if (ISM)
         {
-            const int a = sub * NI + 2 * p;
-            const float4 u0 = pos[s0 + a], u1 = pos[s0 + a + 1];
-            const int4 x0 = aux[s0 + a], x1 = aux[s0 + a + 1];
-            npx[p] = make_float2(-u0.x, -u1.x);
-            npy[p] = make_float2(-u0.y, -u1.y);
-            npz[p] = make_float2(-u0.z, -u1.z);
-            qi[p] = make_float2(u0.w, u1.w);
-            gi[2 * p] = x0.w;
-            gi[2 * p + 1] = x1.w;
+            __syncwarp();  // the previous cluster's atoms are no longer read
+            if (lane < 4)
+            {
+                const int a = 2 * lane;
+                const float4 u0 = pos[s0 + a], u1 = pos[s0 + a + 1];
+                iat[lane][0] = make_float4(-u0.x, -u1.x, -u0.y, -u1.y);
+                iat[lane][1] = make_float4(-u0.z, -u1.z, u0.w, u1.w);
+                igid[lane] = make_int2(aux[s0 + a].w, aux[s0 + a + 1].w);
+            }
+            __syncwarp();
+        }
+        else
+        {
+#pragma unroll
+            for (int p = 0; p < NP; p++)
+            {
+                const int a = sub * NI + 2 * p;
+                const float4 u0 = pos[s0 + a], u1 = pos[s0 + a + 1];
+                const int4 x0 = aux[s0 + a], x1 = aux[s0 + a + 1];
+                npx[p] = make_float2(-u0.x, -u1.x);
+                npy[p] = make_float2(-u0.y, -u1.y);
+                npz[p] = make_float2(-u0.z, -u1.z);
+                qi[p] = make_float2(u0.w, u1.w);
+                gi[2 * p] = x0.w;
+                gi[2 * p + 1] = x1.w;
+            }
         }
         // the coefficient rows of the cluster's four atom pairs against every
         // partner type, {-A_a, -A_b, B_a, B_b}, staged in shared memory
@@ -520,8 +555,26 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
 #pragma unroll
             for (int p = 0; p < NP; p++)
             {
-                float2 dx = __fadd2_rn(f2(sx), npx[p]), dy = __fadd2_rn(f2(sy2), npy[p]),
-                       dz = __fadd2_rn(f2(sz), npz[p]);
+                float2 pnx, pny, pnz, pq;
+                int2 pg;
+                if (ISM)
+                {
+                    const float4 A = iat[sub * NP + p][0], B = iat[sub * NP + p][1];
+                    pnx = make_float2(A.x, A.y);
+                    pny = make_float2(A.z, A.w);
+                    pnz = make_float2(B.x, B.y);
+                    pq = make_float2(B.z, B.w);
+                    pg = igid[sub * NP + p];
+                }
+                else
+                {
+                    pnx = npx[p];
+                    pny = npy[p];
+                    pnz = npz[p];
+                    pq = qi[p];
+                    pg = make_int2(gi[2 * p], gi[2 * p + 1]);
+                }
+                float2 dx = __fadd2_rn(f2(sx), pnx), dy = __fadd2_rn(f2(sy2), pny), dz = __fadd2_rn(f2(sz), pnz);
                 if (any_img && img)
                 {
                     // small box: the pair takes its own minimum image
@@ -545,7 +598,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 const bool inB = ((mi >> (2 * p + 1)) & 1u) && r2.y < pp.rc2;
                 const float4 ab = rows[(sub * NP + p) * nt + tj];
                 float2 elj, ec;
-                float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(qj, qi[p]), make_float2(ab.x, ab.y),
+                float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(qj, pq), make_float2(ab.x, ab.y),
                                                  make_float2(ab.z, ab.w), pp, elj, ec);
                 f = make_float2(inA ? f.x : 0.0f, inB ? f.y : 0.0f);
                 const float2 gx = __fmul2_rn(f, dx), gy = __fmul2_rn(f, dy), gz = __fmul2_rn(f, dz);
@@ -574,7 +627,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                     // the pair's owner is the lower global index: this lane's
                     // atom (kept over the list) or, over the half list, the
                     // partner (summed over the word's atoms)
-                    const float2 wi = make_float2(gi[2 * p] < gj ? 1.0f : 0.0f, gi[2 * p + 1] < gj ? 1.0f : 0.0f);
+                    const float2 wi = make_float2(pg.x < gj ? 1.0f : 0.0f, pg.y < gj ? 1.0f : 0.0f);
                     const float2 v[8] = {make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f),
                                          make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f),
                                          __fmul2_rn(gx, dx), __fmul2_rn(gx, dy), __fmul2_rn(gy, dy),
@@ -781,7 +834,6 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     float ene = 0.0f;
     long long tq[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // this slot's share of the totals (per-atom mode)
-    int tsys = -1;
     if (s < slots)
     {
         const int a = slot_atom[s];
@@ -814,7 +866,6 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
             {
 #pragma unroll
                 for (int k = 0; k < 8; k++) q[k] = 0;
-                const int sy = cl_sys[s >> 3];
                 // raw sums: -12 E_lj, E_c, and +g (x) d; the virial is -g (x) d
                 // with the symmetric off-diagonal terms twice the one summed
                 double v[8];
@@ -826,7 +877,6 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
                     v[k] = (double)r[k] * sg;
                     tq[k] = __double2ll_rn(v[k]);
                 }
-                tsys = sy;
                 if (a >= 0)
                 {
                     const int o = om.remap(a);
@@ -902,33 +952,22 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
     }
     if (PA)
     {
-        // the totals: summed over the block when its slots belong to one
-        // system (the usual case), else added slot by slot
+        // the totals (the per-atom mode runs on one system): summed over the
+        // warp by shuffles, over the block in shared memory, one atomic per
+        // value and block
         __shared__ long long bsum[8];
-        __shared__ int bsys;
-        if (threadIdx.x == 0) bsys = -2;
         if (threadIdx.x < 8) bsum[threadIdx.x] = 0;
         __syncthreads();
-        if (tsys >= 0) atomicCAS(&bsys, -2, tsys);
-        __syncthreads();
-        const int bs = bsys;
-        __syncthreads();
-        if (tsys >= 0)
-        {
-            const bool same = tsys == bs;
 #pragma unroll
-            for (int k = 0; k < 8; k++)
-                if (tq[k])
-                {
-                    if (same)
-                        atomicAdd((unsigned long long*)&bsum[k], (unsigned long long)tq[k]);
-                    else
-                        atomicAdd((unsigned long long*)&totals[8 * tsys + k], (unsigned long long)tq[k]);
-                }
+        for (int k = 0; k < 8; k++)
+        {
+            long long v = tq[k];
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+            if ((threadIdx.x & 31) == 0 && v) atomicAdd((unsigned long long*)&bsum[k], (unsigned long long)v);
         }
         __syncthreads();
-        if (threadIdx.x < 8 && bs >= 0 && bsum[threadIdx.x])
-            atomicAdd((unsigned long long*)&totals[8 * bs + threadIdx.x], (unsigned long long)bsum[threadIdx.x]);
+        if (threadIdx.x < 8 && bsum[threadIdx.x])
+            atomicAdd((unsigned long long*)&totals[threadIdx.x], (unsigned long long)bsum[threadIdx.x]);
     }
     if (EXCL && EN)
     {
@@ -965,7 +1004,7 @@ int launch_pair(const ForceInputs& in, cudaStream_t s)
         SPGNB_CUDA(cudaFuncSetAttribute(k_pair8<M, F, T, H, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
     k_pair8<M, F, T, H, NI><<<grid, kPairWarps * 32, smem, s>>>(
-        in.p0, in.d_fps, nl->d_sys, nl->clusters_cap, kClusterSize * nl->slot_cap, nl->d_cl_sys, nl->d_pcount,
+        in.p0, in.d_fps, nl->d_sys, nl->clusters_cap, nl->list_cap, nl->d_cl_sys, nl->d_pcount,
         nl->d_pwords, nl->d_slot_atom, nl->d_cl_q, in.slot_pos, in.slot_aux, in.t4, in.frc, nl->d_facc, nl->d_oacc,
         in.totals, in.om, in.pa, in.only, nl->d_counters, mt);
     SPGNB_CHECK_LAUNCH("k_pair8");
@@ -1012,17 +1051,20 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
     const bool track = nl->opt.prune_buffer > 0.0f;
     const float half = 0.5f * nl->opt.prune_buffer;
     if (!in.t4) return fail(SPGNB_E_STATE, "force: the LJ module has no pair table");
+    if (in.mode == 2 && nl->S != 1)
+        return fail(SPGNB_E_UNSUPPORTED, "force: per-atom energy/virial outputs are for a one-system list");
     if (in.p0.n_types <= 0 || in.p0.n_types > kMaxTypes)
         return fail(SPGNB_E_UNSUPPORTED, "force: %d LJ types (at most %d)", in.p0.n_types, kMaxTypes);
     k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_slot_gid,
                                                      nl->d_cl_sys, nl->d_sys, nl->d_cl_q, nl->d_slot_x0,
                                                      nl->d_slot_d0, in.crd, in.charge, in.atom_type, in.slot_pos,
                                                      in.slot_aux, track ? nl->d_pref : nullptr, half * half,
-                                                     nl->d_prune);
+                                                     nl->d_prune, in.clear.totals, in.clear.one, in.clear.a, in.clear.b,
+                                                     in.clear.n);
     SPGNB_CHECK_LAUNCH("k_pack_slots");
     const int grid = std::max(1, std::min(num_sms() * 5, (nl->clusters_cap + kPruneWarps - 1) / kPruneWarps));
     k_prune8<<<grid, kPruneWarps * 32, 0, s>>>(in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters,
-                                               nl->clusters_cap, nl->table_cap, kClusterSize * nl->slot_cap,
+                                               nl->clusters_cap, nl->table_cap, nl->list_cap,
                                                nl->d_cl_sys, nl->d_sys, nl->d_tcount, nl->d_tab, nl->d_tmask,
                                                in.slot_pos, nl->d_pref, nl->d_pcount, nl->d_pwords, nl->S,
                                                nl->d_prune);

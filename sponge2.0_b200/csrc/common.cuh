@@ -246,7 +246,7 @@ struct spgnb_nl
     spgnb_nl_options opt{};
     int clusters_cap = 0;
     int table_cap = 0;     // neighbour-table elements per cluster
-    int slot_cap = 0;      // words reserved per atom for its pruned list (a multiple of 64)
+    int list_cap = 0;      // words reserved per cluster for its pruned partner list (a multiple of 32)
     float prune_rc = 0;    // cutoff the pruned lists are made for
     bool built = false;
     int local_atoms = 0;
@@ -290,7 +290,7 @@ struct spgnb_nl
     int* d_tcount = nullptr;      // elements of each cluster's table
     float4* d_tab = nullptr;      // {D = centre difference (minimum image), neighbour slot base | image flag << 30}
     uint2* d_tmask = nullptr;     // 64-bit pair mask: bit a*8 + b = own slot a with neighbour slot b
-    // pruned per-cluster partner lists, 8 * slot_cap words reserved per
+    // pruned per-cluster partner lists, list_cap words reserved per
     // cluster: {partner slot | atom mask << 22 | image flag << 30}, an upper
     // part from the start and a lower part from the end, each padded to
     // 32-word windows; their lengths at d_pcount[8c], d_pcount[8c + 1]
@@ -456,6 +456,16 @@ struct ForceInputs
     OwnerMap om{nullptr, 0, 3};
     PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
     ExclFuse xf{};                     // one system only
+    // cleared by the slot pack before the pair kernel runs: 8 totals, one
+    // more int64, and two float arrays of n entries (any may be null)
+    struct
+    {
+        long long* totals = nullptr;
+        long long* one = nullptr;
+        float* a = nullptr;
+        float* b = nullptr;
+        int n = 0;
+    } clear;
 };
 int force_pipeline(const ForceInputs& in, cudaStream_t s);
 // Uploads the T^3 table the force kernel reads from a T x T {A, B} table:
@@ -495,7 +505,7 @@ struct NLPoolSpec
     int clusters = 0;
     long long runs = 0;
     int table_cap = 0;    // neighbour-table elements per cluster
-    int slot_cap = 0;     // pruned-list words per slot
+    int list_cap = 0;     // pruned-list words per cluster
     float prune_rc = 0;   // the largest cutoff
 };
 int nl_create_pool(const NLPoolSpec& spec, const spgnb_nl_options* opt, spgnb_nl** out);
@@ -506,8 +516,11 @@ int nl_init_system(SysHost& sh, int atom_count, spgnb_ltmatrix3 cell, spgnb_ltma
 // entries.
 int nl_system_runs(const SysHost& sh, std::vector<int>& run_start, std::vector<int2>& runs);
 // Table and pruned-list capacities for a system of this density and cutoff.
+// Words reserved per cluster for a pruned list of per_cluster partners
+// (margin and room for padding both parts to whole windows).
+int list_cap_for(double per_cluster);
 void nl_capacity_for(double atoms_per_A3, double atom_count, float cutoff, float skin, float prune_buffer,
-                     double* table_per_cluster, double* words_per_atom);
+                     double* table_per_cluster, double* words_per_cluster);
 // Takes a free system id and the cell, cluster and run ranges of a system
 // whose atoms occupy [sh.atom_begin, + sh.atom_count); SPGNB_E_OOM (no
 // message) when the pool has no room now.  The system rebuilds when the

@@ -988,11 +988,11 @@ int alloc_tables(spgnb_nl* nl)
     return SPGNB_OK;
 }
 
-// The pruned lists: slot_cap words per slot.
+// The pruned lists: list_cap words per cluster.
 int alloc_words(spgnb_nl* nl)
 {
     dfree(nl->d_pwords);
-    return dalloc(&nl->d_pwords, (size_t)nl->clusters_cap * kClusterSize * nl->slot_cap);
+    return dalloc(&nl->d_pwords, (size_t)nl->clusters_cap * nl->list_cap);
 }
 
 // Squared radius of the pruned lists for the pruning cutoff rc.
@@ -1131,7 +1131,6 @@ int alloc_nl(spgnb_nl* nl)
 }
 
 int table_cap_for(double per_cluster) { return std::max((int)(per_cluster * 1.3) + 64, 128); }
-int slot_cap_for(double per_atom) { return (((int)(per_atom * 1.3) + 63) & ~63) + 128; }
 
 void resolve_options(const spgnb_nl_options* opt, spgnb_nl_options* o)
 {
@@ -1145,16 +1144,19 @@ void resolve_options(const spgnb_nl_options* opt, spgnb_nl_options* o)
 
 }  // namespace
 
+int list_cap_for(double per_cluster) { return (((int)(per_cluster * 1.3) + 31) & ~31) + 64; }
+
 void nl_capacity_for(double atoms_per_A3, double atom_count, float cutoff, float skin, float prune_buffer,
-                     double* table_per_cluster, double* words_per_atom)
+                     double* table_per_cluster, double* words_per_cluster)
 {
     // neighbour clusters within rc + skin + 6 A of an 8-atom cluster; pruned
-    // partners per atom within rc + buffer + 1 A
+    // partners of a cluster (any of its atoms within rc + buffer) within
+    // rc + buffer + 1 A of a sphere holding the cluster (radius 2.5 A)
     const double R = cutoff + skin + 6.0;
     *table_per_cluster = std::min(4.18879 * R * R * R * atoms_per_A3, atom_count) / kClusterSize;
     const double buf = prune_buffer > 0.0f ? prune_buffer + 1.0 : skin;
-    const double Rl = cutoff + buf;
-    *words_per_atom = std::min(4.18879 * Rl * Rl * Rl * atoms_per_A3, atom_count);
+    const double Rl = cutoff + buf + 2.5;
+    *words_per_cluster = std::min(4.18879 * Rl * Rl * Rl * atoms_per_A3, atom_count);
 }
 
 int nl_init_system(SysHost& sh, int atom_count, spgnb_ltmatrix3 cell, spgnb_ltmatrix3 rcell, float cutoff,
@@ -1188,7 +1190,7 @@ int nl_create_pool(const NLPoolSpec& spec, const spgnb_nl_options* opt, spgnb_nl
 {
     *out = nullptr;
     if (spec.systems <= 0 || spec.atoms <= 0 || spec.cells <= 0 || spec.clusters <= 0 || spec.runs <= 0 ||
-        spec.table_cap <= 0 || spec.slot_cap <= 0)
+        spec.table_cap <= 0 || spec.list_cap <= 0)
         return fail(SPGNB_E_ARG, "neighbour list: empty pool capacities");
     if (spec.atoms > (1 << 28) || spec.cells >= (1 << 28))
         return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d atoms / %d cells exceed the 2^28 limit", spec.atoms,
@@ -1201,7 +1203,7 @@ int nl_create_pool(const NLPoolSpec& spec, const spgnb_nl_options* opt, spgnb_nl
     nl->clusters_cap = spec.clusters;
     nl->runs_cap = spec.runs;
     nl->table_cap = nl->opt.max_entries_per_cluster > 0 ? nl->opt.max_entries_per_cluster : spec.table_cap;
-    nl->slot_cap = spec.slot_cap;
+    nl->list_cap = spec.list_cap;
     nl->prune_rc = spec.prune_rc;
     const int st = alloc_nl(nl);
     if (st)
@@ -1347,7 +1349,7 @@ size_t nl_device_bytes(const spgnb_nl* nl)
     size_t b = 0;
     b += n * (4 + 4 + 4 + 16 + 4);                                   // atom system, cell, shift, wrapped, slot
     b += slots * (4 + 4 + 16 + 4 + 16 + 8 + 4 + 4 + 24 + 64 + 16);   // per-slot arrays (with the int64 staging)
-    b += slots * (size_t)nl->slot_cap * 4;                           // pruned lists
+    b += C * (size_t)nl->list_cap * 4;                               // pruned lists
     b += C * (4 + 4 + 16 + 16 + 16 + 4) + 16;                        // per-cluster arrays
     b += C * (size_t)nl->table_cap * (16 + 8);                       // neighbour tables
     b += G * (4 + 4 + 4 + 8 + 4) + 4 + (size_t)nl->runs_cap * 8;     // cells and runs
@@ -1369,7 +1371,7 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
     std::vector<std::vector<int>> starts(n_systems);
     std::vector<std::vector<int2>> runs(n_systems);
     long long atoms = 0, cellsum = 0, clsum = 0, runsum = 0;
-    double per_cluster = 0, per_atom = 0;
+    double per_cluster = 0, per_list = 0;
     float rcmax = 0;
     for (int s = 0; s < n_systems; s++)
     {
@@ -1385,7 +1387,7 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
         double pc, pa;
         nl_capacity_for(atom_counts[s] / vol, atom_counts[s], cutoffs[s], skins[s], o.prune_buffer, &pc, &pa);
         per_cluster = std::max(per_cluster, pc);
-        per_atom = std::max(per_atom, pa);
+        per_list = std::max(per_list, pa);
         rcmax = std::max(rcmax, cutoffs[s]);
     }
     if (atoms > (1LL << 28)) return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %lld atoms exceed the 2^28 limit", atoms);
@@ -1399,7 +1401,7 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
     spec.clusters = (int)clsum;
     spec.runs = std::max(1LL, runsum);
     spec.table_cap = table_cap_for(per_cluster);
-    spec.slot_cap = slot_cap_for(per_atom);
+    spec.list_cap = list_cap_for(per_list);
     spec.prune_rc = rcmax;
     spgnb_nl* nl = nullptr;
     if ((st = nl_create_pool(spec, &o, &nl))) return st;
@@ -1556,7 +1558,7 @@ int nl_regrow(spgnb_nl* nl, int flags)
     }
     if (flags & kOvfWords)
     {
-        nl->slot_cap = (((int)(nl->slot_cap * 1.3)) + 63) & ~63;
+        nl->list_cap = (((int)(nl->list_cap * 1.3)) + 31) & ~31;
         if ((st = alloc_words(nl))) return st;
     }
     SPGNB_CUDA(cudaMemsetAsync(nl->d_counters + kCntOverflow, 0, sizeof(int), stream()));

@@ -604,16 +604,18 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
     cudaStream_t s = stream();
     const int slots = nl->clusters_cap * kClusterSize;
     if ((st = ensure_slots(lj, slots))) return st;
-    SPGNB_CUDA(cudaMemsetAsync(lj->d_totals, 0, sizeof(long long) * 8, s));
-    if (need_atom_energy)
-    {
-        SPGNB_CUDA(cudaMemsetAsync(lj->d_lj_energy_atom, 0, sizeof(float) * lj->atom_numbers, s));
-        if (d_atom_direct_pme_energy)
-            SPGNB_CUDA(cudaMemsetAsync(d_atom_direct_pme_energy, 0, sizeof(float) * lj->atom_numbers, s));
-    }
     if ((st = nl_set_prune_rc(const_cast<spgnb_nl*>(nl), lj->cutoff, s))) return st;
     ForceInputs in;
     in.nl = const_cast<spgnb_nl*>(nl);
+    // what the callee zeroes (Lennard_Jones_force.cpp:376-382) is cleared by
+    // the slot pack at the head of the force pass, not by separate memsets
+    in.clear.totals = lj->d_totals;
+    if (need_atom_energy)
+    {
+        in.clear.a = lj->d_lj_energy_atom;
+        in.clear.b = d_atom_direct_pme_energy;
+        in.clear.n = lj->atom_numbers;
+    }
     in.crd = (const float3*)d_crd;
     in.charge = d_charge;
     in.atom_type = lj->d_local_type;
@@ -659,7 +661,7 @@ int spgnb_lj_pme_direct_force(spgnb_lj* lj, int atom_numbers, int local_atom_num
             in.xf.energy = need_atom_energy ? d_atom_energy : nullptr;
             in.xf.virial = need_virial ? (float*)d_atom_virial : nullptr;
         }
-        if (mode >= 1) SPGNB_CUDA(cudaMemsetAsync(lj->d_excl_total, 0, sizeof(long long), s));
+        if (mode >= 1) in.clear.one = lj->d_excl_total;
     }
     if ((st = force_pipeline(in, s))) return st;
     lj->have_energy = need_atom_energy != 0;
