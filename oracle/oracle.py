@@ -246,6 +246,14 @@ class Reference:
         lib.ref_enable_solvent.argtypes = [C.c_int, _i32p, C.c_int, C.c_int, C.c_int]
         lib.ref_set_threads.argtypes = [C.c_int]
         lib.ref_set_key.argtypes = [C.c_char_p, C.c_char_p]
+        if hasattr(lib, "ref_pme_excluded"):
+            lib.ref_pme_excluded.restype = C.c_double
+            lib.ref_pme_excluded.argtypes = [_f32p, _f32p, C.c_float, C.c_int, _f32p, _f32p, _f32p]
+        if hasattr(lib, "ref_md_init"):
+            lib.ref_md_init.restype = C.c_int
+            lib.ref_md_init.argtypes = [_f32p, C.c_int, C.c_int, C.c_float, C.c_float, C.c_float]
+            lib.ref_md_run.restype = None
+            lib.ref_md_run.argtypes = [_f32p, _f32p, _f32p, C.c_float, C.c_int, C.c_int, _f64p]
         if hasattr(lib, "ref_soft_init"):
             lib.ref_soft_init.argtypes = [C.c_int, C.c_int, C.c_int, _i32p, _i32p, _f32p, _f32p, _f32p, _f32p,
                                           _f32p, C.c_float]
@@ -319,6 +327,36 @@ class Reference:
         s = self.s
         return float(self.lib.ref_time_steps(_c32(s.crd if crd is None else crd), _c32(s.charge), s.beta,
                                              first_step, steps, int(need_energy), int(need_virial)))
+
+    def pme_excluded(self, crd=None, need_energy=True):
+        """The reference's PME excluded-pair correction (CUDA build only) on
+        the system of the last init(): forces, per-atom energy and virial,
+        and the correction's energy."""
+        s = self.s
+        n = s.n
+        frc = np.zeros(3 * n, np.float32)
+        ene = np.zeros(n, np.float32)
+        vir = np.zeros(6 * n, np.float32)
+        e = self.lib.ref_pme_excluded(_c32(s.crd if crd is None else crd), _c32(s.charge), s.beta, int(need_energy),
+                                      frc, ene, vir)
+        return {"frc": frc.reshape(-1, 3), "atom_energy": ene, "atom_virial": vir.reshape(-1, 6), "energy": float(e)}
+
+    def md_init(self, dt=0.002, d_oh=0.9572, d_hh=1.5139):
+        """The reference's SETTLE for the system's trailing 3-site waters
+        (CUDA build only); returns the number of SETTLE triangles."""
+        s = self.s
+        first = s.n - 3 * s.n_waters
+        return int(self.lib.ref_md_init(_c32(s.mass), first, s.n_waters, d_oh, d_hh, dt))
+
+    def md_run(self, crd, vel, steps, first_step=0):
+        """NVE steps of the reference's force path, leap-frog and SETTLE:
+        (crd, vel) after them and (steps, 2) LJ / direct Coulomb energies at
+        each step's starting positions."""
+        crd = np.array(crd, np.float32, copy=True, order="C")
+        vel = np.array(vel, np.float32, copy=True, order="C")
+        e = np.zeros(2 * steps, np.float64)
+        self.lib.ref_md_run(crd, vel, _c32(self.s.charge), self.s.beta, first_step, steps, e)
+        return crd, vel, e.reshape(-1, 2)
 
     def time_rebuild(self, reps=1, crd=None):
         return float(self.lib.ref_time_rebuild(_c32(self.s.crd if crd is None else crd), reps))

@@ -15,6 +15,7 @@
 #include <unistd.h>
 
 #include <chrono>
+#include <vector>
 
 #include "Lennard_Jones_force/LJ_soft_core.h"
 #include "Lennard_Jones_force/Lennard_Jones_force.h"
@@ -23,6 +24,15 @@
 #include "control.h"
 #include "neighbor_list/neighbor_list.h"
 #include "xponge/xponge.h"
+#ifdef REF_HARNESS_PME
+#include "PM_force/PM_force.h"
+#endif
+#ifdef REF_HARNESS_MD
+#include "MD_core/MD_core.h"
+#include "MD_core/nve.hpp"
+#include "constrain/constrain.h"
+#include "constrain/settle.h"
+#endif
 
 CONTROLLER controller;
 namespace Xponge
@@ -521,5 +531,176 @@ void ref_clear()
     if (S.d_charge_ba) Free_Single_Device_Pointer((void**)&S.d_charge_ba);
     S.d_charge_ba = nullptr;
 }
+
+#ifdef REF_HARNESS_PME
+// Particle_Mesh::PME_Excluded_Force_With_Atom_Energy (PM_force.cpp:918-1002),
+// the reference's own kernel, on the system of the last ref_init: the
+// method needs only the members set here (its reciprocal-space set-up is not
+// run).  Outputs (overwritten): forces n x 3, per-atom energy n, per-atom
+// virial n x 6; returns the correction's energy (sum of its per-atom record).
+double ref_pme_excluded(const float* crd, const float* charge, float beta, int need_energy, float* frc,
+                        float* atom_energy, float* atom_virial)
+{
+    static Particle_Mesh* pm = nullptr;
+    if (!pm) pm = new Particle_Mesh();
+    pm->is_initialized = 1;
+    pm->calculate_excluded_part = true;
+    pm->atom_numbers = S.n;
+    pm->beta = beta;
+    static float* d_corr = nullptr;
+    static int corr_n = 0;
+    if (corr_n < S.n)
+    {
+        if (d_corr) cudaFree(d_corr);
+        d_corr = dev_alloc<float>(S.n);
+        corr_n = S.n;
+    }
+    pm->d_correction_atom_energy = d_corr;
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    to_dev(S.d_charge, charge, S.n);
+    cudaMemset(S.d_frc, 0, sizeof(VECTOR) * S.n);
+    cudaMemset(S.d_energy, 0, sizeof(float) * S.n);
+    cudaMemset(S.d_virial, 0, sizeof(LTMatrix3) * S.n);
+    cudaMemset(d_corr, 0, sizeof(float) * S.n);
+    pm->PME_Excluded_Force_With_Atom_Energy(S.d_crd, S.cell, S.rcell, S.d_charge, S.d_excl_start, S.d_excl_list,
+                                            S.d_excl_num, S.d_frc, need_energy, S.d_energy, S.d_virial);
+    sync_device();
+    to_host((VECTOR*)frc, S.d_frc, S.n);
+    to_host(atom_energy, S.d_energy, S.n);
+    to_host((LTMatrix3*)atom_virial, S.d_virial, S.n);
+    std::vector<float> corr(S.n);
+    to_host(corr.data(), d_corr, S.n);
+    double e = 0;
+    for (float v : corr) e += v;
+    return e;
+}
+#endif
+
+#ifdef REF_HARNESS_MD
+namespace
+{
+struct MdState
+{
+    CONSTRAIN* con = nullptr;
+    SETTLE* settle = nullptr;
+    VECTOR* d_vel = nullptr;
+    float* d_mass = nullptr;
+    float* d_inv_mass = nullptr;
+    int* d_local_id = nullptr;
+    char* d_local_label = nullptr;
+    float dt = 0.002f;
+} M;
+}  // namespace
+
+// Rigid 3-site waters (O, H, H at water_first + 3k) constrained by the
+// reference's SETTLE as SPONGE sets it up (settle.cpp:342-570) from the
+// constraint pairs CONSTRAIN holds -- O-H, O-H, H-H with the reduced masses
+// as constrain_k, x and v factors 1 (NVE leap-frog) -- on the system of the
+// last ref_init, with a time step of dt_ps picoseconds.  Returns the number of
+// SETTLE triangles.
+int ref_md_init(const float* mass, int water_first, int n_waters, float d_oh, float d_hh, float dt_ps)
+{
+    Quiet q;
+    // SPONGE's internal time unit (MD_core.cpp:133)
+    const float dt = dt_ps * CONSTANT_TIME_CONVERTION;
+    M.dt = dt;
+    M.con = new CONSTRAIN();
+    CONSTRAIN& c = *M.con;
+    strcpy(c.module_name, "constrain");
+    c.atom_numbers = S.n;
+    c.dt = dt;
+    c.dt_inverse = 1.0f / dt;
+    c.v_factor = 1.0f;
+    c.x_factor = 1.0f;
+    c.constrain_pair_numbers = 3 * n_waters;
+    Malloc_Safely((void**)&c.h_constrain_pair, sizeof(CONSTRAIN_PAIR) * (c.constrain_pair_numbers + 1));
+    auto pair = [&](int k, int i, int j, float r) {
+        CONSTRAIN_PAIR p;
+        p.atom_i_serial = i;
+        p.atom_j_serial = j;
+        p.constant_r = r;
+        p.constrain_k = mass[i] * mass[j] / (mass[i] + mass[j]);
+        c.h_constrain_pair[k] = p;
+    };
+    for (int w = 0; w < n_waters; w++)
+    {
+        const int o = water_first + 3 * w;
+        pair(3 * w, o, o + 1, d_oh);
+        pair(3 * w + 1, o, o + 2, d_oh);
+        pair(3 * w + 2, o + 1, o + 2, d_hh);
+    }
+    std::vector<float> h_mass(mass, mass + S.n);
+    M.settle = new SETTLE();
+    M.settle->Initial(&controller, M.con, h_mass.data());
+    std::vector<int> id(S.n);
+    for (int i = 0; i < S.n; i++) id[i] = i;
+    std::vector<char> label(S.n, 1);
+    std::vector<float> inv(S.n);
+    for (int i = 0; i < S.n; i++) inv[i] = mass[i] > 0 ? 1.0f / mass[i] : 0.0f;
+    M.d_local_id = dev_alloc<int>(S.n);
+    M.d_local_label = dev_alloc<char>(S.n);
+    M.d_vel = dev_alloc<VECTOR>(S.n);
+    M.d_mass = dev_alloc<float>(S.n);
+    M.d_inv_mass = dev_alloc<float>(S.n);
+    to_dev(M.d_local_id, id.data(), S.n);
+    to_dev(M.d_local_label, label.data(), S.n);
+    to_dev(M.d_mass, h_mass.data(), S.n);
+    to_dev(M.d_inv_mass, inv.data(), S.n);
+    M.settle->Get_Local(M.d_local_id, M.d_local_label, S.n);
+    sync_device();
+    return M.settle->is_initialized ? M.settle->num_triangle_local : -1;
+}
+
+// `steps` NVE steps in Main_Iteration's order (main.cpp:622-710), each after
+// Main_Calculate_Force's part of this path (main.cpp:307-397): the list
+// update, the LJ (+ solvent) force with per-atom energies, then
+// SETTLE::Remember_Last_Coordinates, the reference's leap-frog kernel
+// (MD_core/nve.hpp) and SETTLE::Do_SETTLE.  energies[2 s] gets the LJ energy
+// and energies[2 s + 1] the direct Coulomb energy at the positions of step s
+// (before its integration); crd and vel are updated in place.
+void ref_md_run(float* crd, float* vel, const float* charge, float beta, int first_step, int steps,
+                double* energies)
+{
+    to_dev(S.d_crd, (const VECTOR*)crd, S.n);
+    to_dev(S.d_charge, charge, S.n);
+    to_dev(M.d_vel, (const VECTOR*)vel, S.n);
+    int solvent = S.slj ? S.slj->local_solvent_numbers : 0;
+    std::vector<float> e(S.n), d(S.n);
+    {
+        Quiet q;
+        for (int s = first_step; s < first_step + steps; s++)
+        {
+            S.nl->Update(S.d_atom_local, S.n, 0, S.d_crd, S.cell, S.rcell, s, NEIGHBOR_LIST::CONDITIONAL_UPDATE,
+                         S.d_excl_start, S.d_excl_list, S.d_excl_num);
+            cudaMemset(S.d_frc, 0, sizeof(VECTOR) * S.n);
+            cudaMemset(S.d_energy, 0, sizeof(float) * S.n);
+            cudaMemset(S.d_virial, 0, sizeof(LTMatrix3) * S.n);
+            S.lj->LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(S.n, S.n, solvent, 0, S.d_crd, S.d_charge, S.d_frc,
+                                                                  S.cell, S.rcell, S.nl->d_nl, beta, 1, S.d_energy,
+                                                                  0, S.d_virial, S.d_direct);
+            if (S.slj)
+                S.slj->LJ_PME_Direct_Force_With_Atom_Energy_And_Virial(
+                    S.n, S.res_numbers, S.d_res_start, S.d_crd, S.d_charge, S.d_frc, S.cell, S.rcell, S.nl->d_nl,
+                    beta, 1, S.d_energy, 0, S.d_virial, S.d_direct);
+            to_host(e.data(), S.d_energy, S.n);
+            to_host(d.data(), S.d_direct, S.n);
+            double et = 0, ed = 0;
+            for (int i = 0; i < S.n; i++)
+            {
+                et += e[i];
+                ed += d[i];
+            }
+            energies[2 * (s - first_step)] = et - ed;
+            energies[2 * (s - first_step) + 1] = ed;
+            M.settle->Remember_Last_Coordinates(S.d_crd, S.cell, S.rcell);
+            MD_Iteration_Leap_Frog<<<(S.n + 127) / 128, 128>>>(S.n, M.d_vel, S.d_crd, S.d_frc, M.d_inv_mass, M.dt);
+            M.settle->Do_SETTLE(M.d_mass, S.d_crd, S.cell, S.rcell, M.d_vel, 0, nullptr);
+        }
+        sync_device();
+    }
+    to_host((VECTOR*)crd, S.d_crd, S.n);
+    to_host((VECTOR*)vel, M.d_vel, S.n);
+}
+#endif
 
 }  // extern "C"
