@@ -2,13 +2,14 @@
 """Benchmark of the short-range nonbonded path.
 
 One step is what SPONGE's Main_Calculate_Force runs on this path
-(SPONGE/main.cpp:307-397) on an energy step: the caller zeroes the force and
-per-atom energy/virial arrays, a conditional neighbour-list update (a full
-rebuild every 20 steps), the LJ + PME direct-space force with per-atom energy
-and virial (LJ_PME_Direct_Force_With_Atom_Energy_And_Virial with
-need_atom_energy = need_virial = 1), and the long-range correction.
-``--terms f`` times the force-only step SPONGE runs between energy outputs;
-each line reports the other kind beside the headline.
+(SPONGE/main.cpp:307-397): the caller zeroes the force array, a conditional
+neighbour-list update (a full rebuild every 20 steps), and the LJ + PME
+direct-space force (LJ_PME_Direct_Force_With_Atom_Energy_And_Virial with
+need_atom_energy = need_virial = 0: the step SPONGE runs between energy
+outputs).  ``--terms fev`` times the energy step instead (per-atom energy and
+virial, the caller also zeroes those arrays, plus the long-range
+correction); each line reports the other kind beside the headline, and the
+FP64-totals form of the energy step.
 
 Workloads (seeded synthetic coordinates, static between steps; the rebuild
 cadence is the reference's refresh_interval):
@@ -89,13 +90,18 @@ def parse():
     p.add_argument("--steps", type=int, default=100)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", choices=["spgnb", "reference"], default="spgnb")
-    p.add_argument("--terms", choices=["fev", "f"], default="fev",
-                   help="fev: force + per-atom energy + virial every step (the reference API's energy step); "
-                        "f: force only")
+    p.add_argument("--terms", choices=["f", "fev", "totals"], default="f",
+                   help="f: force only, the step SPONGE runs between energy outputs (default); fev: force + "
+                        "per-atom energy + virial every step (the reference API's energy step); totals: force + "
+                        "energy and virial as FP64 totals (the reference arm runs its energy step for it)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=20.0, help="budget of the CPU baseline sample")
     p.add_argument("--profile", action="store_true",
-                   help="profiling run for ncu: warm-up and --steps plain steps, no L2 flush, no e2e, no baseline")
+                   help="profiling run for ncu: warm-up and --steps steps (inside the NVTX range 'timed'), no L2 "
+                        "flush, no e2e, no baseline")
+    p.add_argument("--profile-path", choices=["plain", "soft_core", "graph_resident"], default="plain",
+                   help="with --profile: plain (the module API, default); soft_core (the same box with a 40-atom "
+                        "perturbed ligand); graph_resident (the box as dynamics in captured graphs)")
     p.add_argument("--workload", choices=["mixed96k", "water1m", "batched", "served"], default="mixed96k",
                    help="mixed96k: the plain path on the 96k box (default); water1m: the plain path on the "
                         "1M-atom water box, rc 12; batched: 256 systems, batched engine against the plain "
@@ -191,7 +197,7 @@ def cpu_reference_rate(system, terms, budget_s, threads=None):
     ref.set_threads(threads)
     ref.init(system, refresh_interval=REFRESH_INTERVAL)
     ref.nl_update(forced=True)
-    fe = terms == "fev"
+    fe = terms != "f"
     t_build = ref.time_rebuild(1)
     probe = ref.time_steps(1, first_step=0, need_energy=fe, need_virial=fe)
     steps = max(1, min(REFRESH_INTERVAL - 2, int(max(0.0, budget_s - t_build) / max(probe, 1e-6))))
@@ -238,7 +244,7 @@ def run_reference_arm(args, world, rank):
     ref = O.Reference(gpu=False)
     threads = os.cpu_count() or 1
     ref.set_threads(threads)
-    fe = args.terms == "fev"
+    fe = args.terms != "f"
     ref.init(cs, refresh_interval=REFRESH_INTERVAL)
     ref.nl_update(forced=True)
     W, K = args.warmup, args.steps
@@ -299,7 +305,8 @@ def batched_measure(systems_all, K, W, world, rank, local, dist, k_plain=None):
     B.check_overflow()
     B.set_thermostat(0.1, 300.0)
     tuned = B.autotune(10)
-    B.run(W * B.options.steps_per_graph)
+    tuning = B.tuning()
+    B.run(W * tuning["steps_per_graph"])
     B.check_overflow()
     st0 = B.stats()
     torch.cuda.synchronize()
@@ -342,7 +349,7 @@ def batched_measure(systems_all, K, W, world, rank, local, dist, k_plain=None):
     plain = plain_as_all / (plain_ms * 1e-3)
     return {"value": value, "ms": ms, "K": K, "W": W, "systems": len(systems_all), "systems_per_gpu": len(mine),
             "atoms_all": int(sum(s.n for s in systems_all)), "atoms_per_gpu": atoms,
-            "plain": plain, "k_plain": k_plain, "tuned": tuned,
+            "plain": plain, "k_plain": k_plain, "tuned": tuned, "tuning": tuning,
             "rebuilds": st["rebuilds"] - st0["rebuilds"], "prunings": st["prunings"] - st0["prunings"],
             "overflow": st["overflow"], "energies_finite": bool(np.isfinite(e).all()), "clocks": clocks,
             "launches": int(launches)}
@@ -372,7 +379,8 @@ def run_batched(args, world, rank, local):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": {"workload": batched_workload_name(m), "systems_per_gpu": m["systems_per_gpu"],
                            "atoms_per_gpu": m["atoms_per_gpu"], "energy_interval": 100,
-                           "prune_buffer_autotuned": m["tuned"], "l2": "inputs larger than L2",
+                           "prune_buffer_autotuned": m["tuned"], "autotuned": m["tuning"],
+                           "l2": "inputs larger than L2",
                            "parallelism": f"systems sharded over {world} GPUs" if world > 1 else "single GPU"},
                 "plain_per_system": {"value": m["plain"], "unit": "atom-steps/s",
                                      "how": f"each system alone from the same relaxed state, kernels launched step "
@@ -514,18 +522,23 @@ def main():
     dev = torch.device("cuda", local)
     s = PLAIN[args.workload][0]()
     main_box = args.workload == "mixed96k"
+    if args.profile and args.profile_path != "plain":
+        run_profile_path(args, s, dev)
+        return
     L = lib()
     path = PlainPath(s, refresh_interval=REFRESH_INTERVAL, export_atom_groups=False, device=dev)
     stream = torch.cuda.current_stream()
 
     def step(k, terms):
         # Main_Calculate_Force's part of the path: the caller zeroes the force
-        # and (on energy steps) the per-atom arrays, then list update, the LJ +
-        # PME direct force with per-atom energy and virial, the tail correction
-        fe = terms == "fev"
+        # (and on energy steps the per-atom arrays), then list update and the
+        # LJ + PME direct force; an energy step adds per-atom energy and
+        # virial and the tail correction.  "totals" is the energy step with
+        # the FP64 totals in place of the per-atom arrays.
+        fe = terms != "f"
         path.update(k)
-        path.force(need_energy=fe, need_virial=fe, per_atom=True)
-        if fe:
+        path.force(need_energy=fe, need_virial=fe, per_atom=terms == "fev")
+        if terms == "fev":
             path.lj.Long_Range_Correction(1, path.atom_virial, 1, path.atom_energy, s.volume)
 
     W, K = args.warmup, args.steps
@@ -533,9 +546,11 @@ def main():
         step(k, args.terms)
     torch.cuda.synchronize()
     if args.profile:
+        torch.cuda.nvtx.range_push("timed")
         for k in range(K):
             step(W + k, args.terms)
         torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
         if rank == 0:
             print(json.dumps({"profile_run": True, "workload": args.workload, "steps": K, "warmup": W,
                               "atoms": s.n, "terms": args.terms}))
@@ -589,15 +604,16 @@ def main():
     clocks = sampler.stop()
     total_ms = sum(step_ms)
     # the other step kind over the same step indices (the same rebuilds)
-    other = "f" if args.terms == "fev" else "fev"
+    other = "fev" if args.terms == "f" else "f"
     other_ms, other_pair_ms, _ = timed_steps(other, W, True)
+    tot_ms, tot_pair_ms, _ = timed_steps("totals", W, True)
 
     # end to end through the module API with host buffers: pinned H2D of the
     # coordinates, the step, D2H of the forces and the energy/virial totals
     # (Step_Print's sums), every step
     crd_host = torch.from_numpy(s.crd.copy()).pin_memory()
     frc_host = torch.empty((s.n, 3), dtype=torch.float32).pin_memory()
-    fe = args.terms == "fev"
+    fe = args.terms != "f"
     e2e_ms = []
     for k in range(K):
         flush.fill_(k & 0xff)
@@ -639,8 +655,10 @@ def main():
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "ns_per_day": K * 86.4 * DT_PS / (total_ms * 1e-3),
             "config": plain_config(args, s, world),
-            "step": ("list update + LJ/PME direct force with per-atom energy and virial + tail correction "
-                     "(the reference API's energy step)") if fe else "list update + LJ/PME direct force",
+            "step": {"f": "list update + LJ/PME direct force (the step SPONGE runs between energy outputs)",
+                     "fev": "list update + LJ/PME direct force with per-atom energy and virial + tail correction "
+                            "(the reference API's energy step)",
+                     "totals": "list update + LJ/PME direct force with FP64 energy and virial totals"}[args.terms],
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak.value, "unit": "TFLOP/s",
                          "frac": achieved / peak.value if peak.value else None,
                          "traffic": prof.get("bytes_per_launch"),
@@ -650,9 +668,13 @@ def main():
                          "pruned_list_words": st.pruned_list_words, "prunings": st.prunes, "rebuilds": st.builds,
                          "peak_source": "measured FP32 FFMA throughput on this device (spgnb_probe_fp32_fma_tflops)",
                          "traffic_source": prof.get("source")},
-            ("force_only" if fe else "per_atom_energy_virial"): {
+            ("per_atom_energy_virial" if other == "fev" else "force_only"): {
                 "ms_per_step": sum(other_ms) / K, "atom_steps_per_s": world * s.n * K / (sum(other_ms) * 1e-3),
                 "pair_kernel_ms": sum(other_pair_ms) / K},
+            "energy_virial_totals": {
+                "ms_per_step": sum(tot_ms) / K, "atom_steps_per_s": world * s.n * K / (sum(tot_ms) * 1e-3),
+                "pair_kernel_ms": sum(tot_pair_ms) / K,
+                "how": "force + energy and virial reduced to FP64 totals on the device, no per-atom arrays"},
             "list_device_bytes": st.device_bytes,
             "reference_d_temp_bytes": 4 * 1200 * s.n,
             "clocks": clocks,
@@ -688,7 +710,7 @@ def _main_box_extras(path, s, dev, stream, flush, world, rank, local, dist, args
     fewer steps)."""
     import torch
     from spgnb import systems as S
-    fe = args.terms == "fev"
+    fe = args.terms != "f"
     out = {}
     # the PME excluded-pair correction (PM_force.cpp:918-997), timed on its own
     # (SPONGE runs it in the PME module)
@@ -740,6 +762,7 @@ def _main_box_extras(path, s, dev, stream, flush, world, rank, local, dist, args
                           "plain_how": f"each system alone from the same relaxed state, kernels launched step by "
                                        f"step, {m['k_plain']} steps each",
                           "gpu_launches_per_step": m["launches"] / m["K"], "prune_buffer_autotuned": m["tuned"],
+                          "autotuned": m["tuning"],
                           "rebuilds": m["rebuilds"], "prunings": m["prunings"], "overflow": m["overflow"],
                           "energies_finite": m["energies_finite"], "clocks": m["clocks"]}
     return out
@@ -787,7 +810,8 @@ def _time_graph_resident(s, steps=400):
     b.check_overflow()
     b.set_thermostat(0.1, 300.0)
     tuned = b.autotune(10)
-    b.run(3 * b.options.steps_per_graph)
+    tuning = b.tuning()
+    b.run(3 * tuning["steps_per_graph"])
     st = torch.cuda.ExternalStream(b.stream_ptr)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(st)
@@ -800,8 +824,41 @@ def _time_graph_resident(s, steps=400):
     return {"steps": steps, "ms_per_step": ms / steps, "atom_steps_per_s": s.n * steps / (ms * 1e-3),
             "ns_per_day": steps * 86.4 * DT_PS / (ms * 1e-3), "rebuilds": stats["rebuilds"],
             "prunings": stats["prunings"], "overflow": stats["overflow"], "prune_buffer_autotuned": tuned,
+            "autotuned": tuning,
             "how": "leap-frog + SETTLE + list check/update + force in captured CUDA graphs, 2 fs, "
                    "Berendsen 300 K, energies every 100 steps"}
+
+
+def run_profile_path(args, s, dev):
+    """--profile on one of the side paths: set up and warm up as the timed
+    measurement does, then --steps steps inside the NVTX range 'timed' (an
+    ncu launch list takes --nvtx --nvtx-include timed/)."""
+    import torch
+    from spgnb import systems as S
+    fe = args.terms != "f"
+    W, K = args.warmup, args.steps
+    if args.profile_path == "soft_core":
+        from spgnb.engine import SoftCorePath
+        p = SoftCorePath(S.fep_system(s, n_perturbed=40, seed=11, lam=0.6), refresh_interval=REFRESH_INTERVAL,
+                         device=dev)
+        run = lambda first, n: [p.step(first + k, need_energy=fe, need_virial=fe, per_atom=args.terms == "fev")
+                                for k in range(n)]
+    elif args.profile_path == "graph_resident":
+        from spgnb.batch import Batch
+        b = Batch([s], refresh_interval=REFRESH_INTERVAL, thermostat_tau=0.002, temperature=300.0, prune_buffer=1.6)
+        b.run(200)
+        b.check_overflow()
+        b.set_thermostat(0.1, 300.0)
+        b.autotune(10)
+        run = lambda first, n: b.run(n, 100)
+    run(0, W)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_push("timed")
+    run(W, K)
+    torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
+    print(json.dumps({"profile_run": True, "path": args.profile_path, "workload": args.workload, "steps": K,
+                      "warmup": W, "atoms": s.n, "terms": args.terms}))
 
 
 def _ltm(m):

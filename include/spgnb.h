@@ -453,8 +453,9 @@ int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_number
 /* ----------------------------------------------------------------- BATCH */
 /* Many independent periodic systems stepped together (no reference
  * counterpart: the reference runs one system per process).  Every system
- * keeps its own box, cutoff, skin, Ewald beta, exclusions and rigid waters;
- * they share one LJ type table.  One step = leap-frog velocity Verlet (kick
+ * keeps its own box, cutoff, skin, Ewald beta, exclusions and rigid waters,
+ * and either the batch's LJ type table or one of its own (as each SPONGE
+ * process reads its own LJ_in_file, Lennard_Jones_force.cpp:186-231).  One step = leap-frog velocity Verlet (kick
  * with F(t), drift, SETTLE for the rigid waters) + the neighbour-list
  * update (per system, by the skin trigger of NEIGHBOR_LIST::Update) + LJ and
  * PME direct-space forces over all systems in one kernel launch.  Steps are
@@ -480,6 +481,10 @@ typedef struct
     int excluded_total;
     int water_begin;               /* rigid 3-site waters O,H,H from this local atom */
     int water_numbers;             /* how many */
+    int atom_type_numbers;         /* > 0: this system's own LJ type table below, h_atom_type indexes it;
+                                      0: the batch's table (h_pair_A / h_pair_B ignored) */
+    const float* h_pair_A;         /* its pair_A / pair_B, the reference's triangular layout (x12 / x6) */
+    const float* h_pair_B;
 } spgnb_batch_system;
 
 typedef struct
@@ -498,9 +503,10 @@ typedef struct
 
 void spgnb_batch_default_options(spgnb_batch_options* opt);
 
-/* Copies the systems to the device and builds their lists.  The type table
- * (atom_type_numbers types) is shared: pair_A / pair_B in the reference's
- * triangular layout (already x12 / x6). */
+/* Copies the systems to the device and builds their lists.  The batch's
+ * type table (atom_type_numbers types, pair_A / pair_B in the reference's
+ * triangular layout, already x12 / x6) serves every system that brings none
+ * of its own; at most 128 types per table. */
 int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int atom_type_numbers,
                        const float* h_pair_A, const float* h_pair_B, const spgnb_batch_options* opt,
                        spgnb_batch** out);
@@ -522,9 +528,27 @@ int spgnb_batch_set_thermostat(spgnb_batch* b, float tau, float temperature);
 int spgnb_batch_check_overflow(spgnb_batch* b, int* regrown);
 /* Steps done, list rebuilds (all systems), prunings, overflow flags. */
 int spgnb_batch_stats(spgnb_batch* b, long long* steps, long long* rebuilds, long long* prunings, int* overflow);
-/* Picks the prune buffer with the fastest step for this batch by timing a
- * few steps of each candidate (the systems advance meanwhile). */
+/* Picks the launch configuration with the fastest step for this batch by
+ * timing a few steps of each candidate, one setting after the other (the
+ * systems advance meanwhile): the prune buffer (up to the one the lists were
+ * sized for), the force kernel's resident blocks per SM, the pruning
+ * kernel's blocks per SM and the steps per captured graph.  Results are the
+ * same for every choice; only the time differs. */
 int spgnb_batch_autotune(spgnb_batch* b, int steps_per_candidate, float* chosen_buffer);
+typedef struct
+{
+    float prune_buffer;         /* A */
+    int pair_blocks_per_sm;     /* force kernel, 0 = as many as are resident */
+    int prune_blocks_per_sm;    /* pruning kernel */
+    int steps_per_graph;
+    float ms_per_step;          /* of the chosen configuration, 0 before any tuning */
+} spgnb_batch_tuning;
+/* The launch configuration in use (chosen by spgnb_batch_autotune). */
+int spgnb_batch_get_tuning(spgnb_batch* b, spgnb_batch_tuning* in_use);
+/* Applies a launch configuration (one saved from an earlier tuning, say);
+ * the prune buffer at most the one the lists were sized for.  ms_per_step
+ * is ignored. */
+int spgnb_batch_set_tuning(spgnb_batch* b, const spgnb_batch_tuning* tuning);
 /* The batch's CUDA stream (a cudaStream_t), for events around its work. */
 void* spgnb_batch_stream(spgnb_batch* b);
 int spgnb_batch_destroy(spgnb_batch* b);
@@ -547,6 +571,9 @@ typedef struct
     float skin;                 /* 2 */
     float density;              /* atoms per A^3 of the systems admitted, 0.1003 */
     double hbm_budget_bytes;    /* device memory for the pool when max_atoms is 0 */
+    int max_types;              /* most LJ types of an admitted system's own table; 0: the pool's table's */
+    double type_table_bytes;    /* device memory for admitted systems' own tables (16 B x types^3 each),
+                                   64 MiB */
 } spgnb_batch_pool_options;
 
 void spgnb_batch_pool_default_options(spgnb_batch_pool_options* opt);
@@ -555,7 +582,8 @@ int spgnb_batch_create_pool(const spgnb_batch_pool_options* pool, int atom_type_
 /* Copies a system in (stream-ordered after the work already queued) and
  * gives it an id; `steps` > 0 = the system stops after that many steps, 0 =
  * runs until retired.  Its lists, forces and energies at step 0 are made
- * before the next run.  SPGNB_E_OOM: no room now (nothing changed). */
+ * before the next run.  SPGNB_E_OOM: no room now (nothing changed); a table
+ * of its own with more than max_types types: SPGNB_E_UNSUPPORTED. */
 int spgnb_batch_admit(spgnb_batch* b, const spgnb_batch_system* sys, int steps, int* id);
 /* Returns a system's ranges to the pool (its results must have been read). */
 int spgnb_batch_retire(spgnb_batch* b, int id);

@@ -31,6 +31,7 @@ struct SysRec
     long long ex_begin = 0, ex_count = 0;
     int w_begin = 0, w_count = 0;
     double lr_factor = 0, volume = 0;
+    long long t4_begin = 0, t4_count = 0;  // the system's own coefficient table, when it has one
 };
 
 // A pool of systems: fixed capacities, every system in ranges of its own.
@@ -41,8 +42,9 @@ struct spgnb_batch
     long long ex_cap = 0;
     int w_cap = 0;
     RangePool atom_pool, ex_pool, water_pool;
+    RangePool t4_pool;  // coefficient-table elements: the batch's table first, then systems' own
     std::vector<SysRec> rec;
-    std::vector<float> h_pair_A, h_pair_B;  // the type table, reference layout
+    std::vector<float> h_pair_A, h_pair_B;  // the batch's type table, reference layout
     spgnb_batch_options opt{};
     spgnb_nl* nl = nullptr;
     cudaStream_t stream = nullptr;
@@ -60,9 +62,10 @@ struct spgnb_batch
     int* d_ex_list = nullptr;
     int* d_waters = nullptr;  // oxygen of each rigid water, -1 for a free entry
     // force field
-    int T = 0;
-    float2* d_table = nullptr;
-    float4* d_t4 = nullptr;       // the force kernel's T^3 table
+    int T = 0;                    // types of the batch's table
+    int max_T = 0;                // most types of any table (the force kernel's shared rows)
+    long long t4_cap = 0;
+    float4* d_t4 = nullptr;       // the force kernel's T^3 tables
     spgnb::ForceParams* d_fps = nullptr;  // S + 1
     std::vector<spgnb::ForceParams> h_fps;
     bool fit = true;                  // the rational fits (every admitted system inside their range)
@@ -82,6 +85,9 @@ struct spgnb_batch
     long long kernels_plain = 0, kernels_energy = 0;  // kernel launches inside each graph
     bool graph_tri = false;
     long long steps_done = 0;
+    // launch configuration (spgnb_batch_autotune)
+    int pair_bps = 0, prune_bps = 0;
+    float tuned_ms = 0.0f;
     bool pending = false;  // admitted systems wait for their first lists and forces
     std::vector<spgnb::PinnedStage> stages;  // upload buffers of admissions, reused when their copies are done
 };
@@ -272,9 +278,12 @@ int batch_force(spgnb_batch* b, int mode, cudaStream_t s, const int* only = null
     in.d_fps = b->d_fps;
     in.fit = b->fit;
     in.t4 = b->d_t4;
+    in.max_types = b->max_T;
     in.frc = b->d_frc;
     in.totals = b->d_totals;
     in.mode = mode;
+    in.pair_blocks_per_sm = b->pair_bps;
+    in.prune_blocks_per_sm = b->prune_bps;
     in.om.solvent_start = b->n;
     in.only = only;
     return force_pipeline(in, s);
@@ -391,7 +400,6 @@ void free_batch(spgnb_batch* b)
     dfree(b->d_ex_num);
     dfree(b->d_ex_list);
     dfree(b->d_waters);
-    dfree(b->d_table);
     dfree(b->d_fps);
     dfree(b->d_totals);
     dfree(b->d_kin);
@@ -469,6 +477,7 @@ struct Staged
     int water_begin = 0, water_numbers = 0;
     float mO = 0, mH = 0;
     ForceParams fp{};
+    std::vector<float4> t4;  // the system's own coefficient table (empty: the batch's)
     double lr_factor = 0, volume = 0;
     float ndof = 1;
     SysHost sh;
@@ -476,9 +485,40 @@ struct Staged
     std::vector<int2> runs;
 };
 
-int stage(const spgnb_batch_system& y, int T, const std::vector<float>& pair_A, const std::vector<float>& pair_B,
-          int index, Staged& z)
+int check_type_table(int T, const float* A, const float* B)
 {
+    if (T <= 0 || !A || !B) return fail(SPGNB_E_ARG, "batch: bad LJ type table");
+    if (T > kMaxTypes) return fail(SPGNB_E_UNSUPPORTED, "batch: %d LJ types (at most %d)", T, kMaxTypes);
+    return SPGNB_OK;
+}
+
+// The reference's triangular pair_A / pair_B as the square table.
+std::vector<float2> square_table(int T, const float* A, const float* B)
+{
+    std::vector<float2> table((size_t)T * T);
+    for (int p = 0; p < T; p++)
+        for (int q = 0; q < T; q++)
+        {
+            const int hi = p > q ? p : q, lo = p > q ? q : p;
+            table[(size_t)p * T + q] = make_float2(A[hi * (hi + 1) / 2 + lo], B[hi * (hi + 1) / 2 + lo]);
+        }
+    return table;
+}
+
+int stage(const spgnb_batch_system& y, int T0, const float* pair_A0, const float* pair_B0, int index, Staged& z)
+{
+    if (y.atom_type_numbers < 0)
+        return fail(SPGNB_E_ARG, "batch: system %d has %d LJ types", index, y.atom_type_numbers);
+    const bool own = y.atom_type_numbers > 0;
+    const int T = own ? y.atom_type_numbers : T0;
+    const float* pair_A = own ? y.h_pair_A : pair_A0;
+    const float* pair_B = own ? y.h_pair_B : pair_B0;
+    if (own)
+    {
+        const int st = check_type_table(T, pair_A, pair_B);
+        if (st) return st;
+        z.t4 = coefficient_table(square_table(T, pair_A, pair_B).data(), T);
+    }
     if (y.atom_numbers <= 0 || !y.h_crd || !y.h_charge || !y.h_mass || !y.h_atom_type || !y.h_excluded_start ||
         !y.h_excluded_numbers || (y.excluded_total > 0 && !y.h_excluded_list) || y.water_begin < 0 ||
         y.water_numbers < 0 || y.water_begin + 3LL * y.water_numbers > y.atom_numbers || y.excluded_total < 0)
@@ -534,7 +574,7 @@ int stage(const spgnb_batch_system& y, int T, const std::vector<float>& pair_A, 
     f.use_fit = (zz * zz <= SPGNB_EWALD_W_MAX * 0.999f) ? 1 : 0;
     f.n_types = T;
     f.table_begin = 0;
-    f.t4_begin = 0;
+    f.t4_begin = 0;  // a table of its own gets its place on admission
     // Total_C6_Get and the factor of Lennard_Jones_force.cpp:263-268
     double c6 = 0.0;
     for (int p = 0; p < T; p++)
@@ -554,7 +594,7 @@ int stage(const spgnb_batch_system& y, int T, const std::vector<float>& pair_A, 
 
 // Device arrays for the capacities; every range free.
 int create_common(spgnb_batch* b, const NLPoolSpec& spec, long long ex_cap, int w_cap, int T, const float* pair_A,
-                  const float* pair_B)
+                  const float* pair_B, long long t4_cap)
 {
     int st;
     b->S = spec.systems;
@@ -568,13 +608,10 @@ int create_common(spgnb_batch* b, const NLPoolSpec& spec, long long ex_cap, int 
     b->rec.assign(b->S, SysRec{});
     b->h_flags.assign(b->S, 0);
     b->h_fps.assign(b->S + 1, ForceParams{});
-    std::vector<float2> table((size_t)T * T);
-    for (int p = 0; p < T; p++)
-        for (int q = 0; q < T; q++)
-        {
-            const int hi = p > q ? p : q, lo = p > q ? q : p;
-            table[(size_t)p * T + q] = make_float2(pair_A[hi * (hi + 1) / 2 + lo], pair_B[hi * (hi + 1) / 2 + lo]);
-        }
+    const std::vector<float4> t4 = coefficient_table(square_table(T, pair_A, pair_B).data(), T);
+    b->t4_cap = std::max<long long>(t4_cap, (long long)t4.size());
+    b->t4_pool.reset(b->t4_cap);
+    b->t4_pool.alloc((long long)t4.size());  // the batch's table at element 0
     spgnb_nl_options nlo;
     spgnb_nl_default_options(&nlo);
     nlo.refresh_interval = 0;
@@ -592,15 +629,14 @@ int create_common(spgnb_batch* b, const NLPoolSpec& spec, long long ex_cap, int 
         (st = zalloc(&b->d_inv_mass, n)) || (st = zalloc(&b->d_type, n)) || (st = zalloc(&b->d_atom_local, n)) ||
         (st = zalloc(&b->d_ex_start, n)) || (st = zalloc(&b->d_ex_num, n)) ||
         (st = zalloc(&b->d_ex_list, (size_t)b->ex_cap)) || (st = dalloc(&b->d_waters, (size_t)b->w_cap)) ||
-        (st = dalloc(&b->d_table, table.size())) || (st = zalloc(&b->d_fps, S1)) ||
+        (st = dalloc(&b->d_t4, (size_t)b->t4_cap)) || (st = zalloc(&b->d_fps, S1)) ||
         (st = zalloc(&b->d_totals, 8 * S1)) || (st = zalloc(&b->d_kin, S1)) || (st = zalloc(&b->d_ndof, S1)) ||
         (st = zalloc(&b->d_steps, S1)) || (st = zalloc(&b->d_left, S1)) || (st = zalloc(&b->d_flags, S1)) ||
         (st = dalloc(&b->d_slot_pos, (size_t)b->nl->clusters_cap * kClusterSize + 1)) ||
         (st = dalloc(&b->d_slot_aux, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
         return st;
-    SPGNB_CUDA(cudaMemcpy(b->d_table, table.data(), sizeof(float2) * table.size(), cudaMemcpyHostToDevice));
+    SPGNB_CUDA(cudaMemcpy(b->d_t4, t4.data(), sizeof(float4) * t4.size(), cudaMemcpyHostToDevice));
     SPGNB_CUDA(cudaMemset(b->d_waters, 0xff, sizeof(int) * b->w_cap));
-    if ((st = build_t4(table.data(), T, &b->d_t4))) return st;
     SPGNB_CUDA(cudaDeviceSynchronize());
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
@@ -614,9 +650,19 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
         return fail(SPGNB_E_UNSUPPORTED, "batch: beta * cutoff of this system is outside the pool's fitted range");
     if (z.water_numbers > 0 && b->have_water && (z.mO != b->mO || z.mH != b->mH))
         return fail(SPGNB_E_ARG, "batch: the rigid waters of a pool share one mass pair");
+    if (z.fp.n_types > b->max_T)
+        return fail(SPGNB_E_UNSUPPORTED, "batch: a type table of %d types (the pool takes at most %d)", z.fp.n_types,
+                    b->max_T);
     cudaStream_t s = b->stream;
+    const long long nt4 = (long long)z.t4.size();
+    const long long tb = nt4 ? b->t4_pool.alloc(nt4) : 0;
+    if (tb < 0) return fail(SPGNB_E_OOM, "batch: no room for the system's type table now");
     const long long ab = b->atom_pool.alloc(z.N);
-    if (ab < 0) return fail(SPGNB_E_OOM, "batch: no room for %d atoms now", z.N);
+    if (ab < 0)
+    {
+        b->t4_pool.release(tb, nt4);
+        return fail(SPGNB_E_OOM, "batch: no room for %d atoms now", z.N);
+    }
     const long long ne = (long long)z.ex_list.size();
     const long long eb = b->ex_pool.alloc(ne);
     const long long wb = eb < 0 ? -1 : b->water_pool.alloc(z.water_numbers);
@@ -624,21 +670,24 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
     {
         if (eb >= 0) b->ex_pool.release(eb, ne);
         b->atom_pool.release(ab, z.N);
+        b->t4_pool.release(tb, nt4);
         return fail(SPGNB_E_OOM, "batch: no room for the exclusions or waters now");
     }
+    z.fp.t4_begin = (int)tb;
     z.sh.atom_begin = (int)ab;
     // every upload of this admission goes through one pinned buffer, so the
     // copies queue behind the work in flight instead of waiting for it
     const size_t N = z.N;
     const size_t need = N * (2 * sizeof(float3) + 6 * sizeof(int)) + ne * sizeof(int) +
                         z.water_numbers * sizeof(int) + sizeof(ForceParams) + 3 * sizeof(int) + 16 * 20 +
-                        nl_admit_upload_bytes(z.sh, z.runs.size());
+                        nt4 * sizeof(float4) + nl_admit_upload_bytes(z.sh, z.runs.size());
     PinnedStage* ps = nullptr;
     if ((st = take_stage(b, need, &ps)))
     {
         b->water_pool.release(wb, z.water_numbers);
         b->ex_pool.release(eb, ne);
         b->atom_pool.release(ab, z.N);
+        b->t4_pool.release(tb, nt4);
         return st;
     }
     Uploader up{ps};
@@ -653,6 +702,7 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
         b->water_pool.release(wb, z.water_numbers);
         b->ex_pool.release(eb, ne);
         b->atom_pool.release(ab, z.N);
+        b->t4_pool.release(tb, nt4);
         return code;
     };
     st = nl_admit(b->nl, z.sh, &z.run_start, &z.runs, s, &sid, up);
@@ -690,7 +740,8 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
         (st = putv(b->d_type, ab, z.type)) || (st = putv(b->d_atom_local, ab, own)) ||
         (st = putv(b->d_ex_start, ab, ex_start)) || (st = putv(b->d_ex_num, ab, z.ex_num)) ||
         (st = putv(b->d_ex_list, eb, ex_list)) || (st = putv(b->d_waters, wb, waters)) ||
-        (st = putv(b->d_fps, sid, fp)) || (st = putv(b->d_ndof, sid, ndof)) || (st = putv(b->d_left, sid, left)))
+        (st = putv(b->d_fps, sid, fp)) || (st = putv(b->d_ndof, sid, ndof)) || (st = putv(b->d_left, sid, left)) ||
+        (nt4 && (st = putv(b->d_t4, tb, z.t4))))
         return bail(st);
     SPGNB_CUDA(cudaMemsetAsync(b->d_frc + ab, 0, sizeof(float3) * z.N, s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_steps + sid, 0, sizeof(int), s));
@@ -711,6 +762,8 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
     r.w_count = z.water_numbers;
     r.lr_factor = z.lr_factor;
     r.volume = z.volume;
+    r.t4_begin = tb;
+    r.t4_count = nt4;
     b->h_flags[sid] = 1;
     b->pending = true;
     *id = sid;
@@ -718,10 +771,10 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
 }
 
 // Batch-side device bytes for the capacities.
-double batch_bytes(long long atoms, long long ex, long long waters, long long slots, int S, int T)
+double batch_bytes(long long atoms, long long ex, long long waters, long long slots, int S, long long t4_cap)
 {
-    return (double)atoms * (12 * 4 + 4 * 6) + ex * 4.0 + waters * 4.0 + slots * 20.0 + (S + 1.0) * (32 + 64 + 8 + 16) +
-           T * (double)T * 8;
+    return (double)atoms * (12 * 4 + 4 * 6) + ex * 4.0 + waters * 4.0 + slots * 32.0 + (S + 1.0) * (32 + 64 + 8 + 16) +
+           t4_cap * 16.0;
 }
 
 // Pool capacities for `atoms` atoms under the pool options.
@@ -743,7 +796,7 @@ NLPoolSpec pool_spec(const spgnb_batch_pool_options& po, float prune_buffer, int
     return sp;
 }
 
-double pool_bytes(const spgnb_batch_pool_options& po, float prune_buffer, int atoms, int T)
+double pool_bytes(const spgnb_batch_pool_options& po, float prune_buffer, int atoms, long long t4_cap)
 {
     const NLPoolSpec sp = pool_spec(po, prune_buffer, atoms);
     spgnb_nl probe;
@@ -757,7 +810,8 @@ double pool_bytes(const spgnb_batch_pool_options& po, float prune_buffer, int at
     probe.opt.export_atom_groups = 0;
     const long long ex = po.max_excluded > 0 ? po.max_excluded : 2LL * atoms;
     const long long w = po.max_waters > 0 ? po.max_waters : atoms / 3;
-    return (double)nl_device_bytes(&probe) + batch_bytes(atoms, ex, w, (long long)sp.clusters * kClusterSize, sp.systems, T);
+    return (double)nl_device_bytes(&probe) +
+           batch_bytes(atoms, ex, w, (long long)sp.clusters * kClusterSize, sp.systems, t4_cap);
 }
 
 }  // namespace
@@ -794,6 +848,8 @@ void spgnb_batch_pool_default_options(spgnb_batch_pool_options* o)
     o->skin = 2.0f;
     o->density = 0.1003f;
     o->hbm_budget_bytes = 120e9;
+    o->max_types = 0;
+    o->type_table_bytes = 64.0 * (1 << 20);
 }
 
 int spgnb_batch_set_thermostat(spgnb_batch* b, float tau, float temperature)
@@ -803,14 +859,6 @@ int spgnb_batch_set_thermostat(spgnb_batch* b, float tau, float temperature)
     b->opt.thermostat_tau = tau;
     b->opt.temperature = temperature;
     free_graphs(b);
-    return SPGNB_OK;
-}
-
-static int check_type_table(int T, const float* A, const float* B)
-{
-    if (T <= 0 || !A || !B) return fail(SPGNB_E_ARG, "batch: bad LJ type table");
-    if (T > kMaxTypes || T * T * (int)sizeof(float2) > 96 * 1024)
-        return fail(SPGNB_E_UNSUPPORTED, "batch: %d LJ types exceed the shared-memory pair table", T);
     return SPGNB_OK;
 }
 
@@ -843,12 +891,16 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
     const std::vector<float>& pb = b->h_pair_B;
     std::vector<Staged> z(n_systems);
     long long atoms = 0, ex = 0, waters = 0, cells = 0, clusters = 0, runs = 0;
+    long long t4_cap = (long long)T * T * T;
+    b->max_T = T;
     double per_cluster = 0, per_list = 0;
     float rcmax = 0;
     for (int k = 0; k < n_systems && !st; k++)
     {
-        if ((st = stage(systems[k], T, pa, pb, k, z[k]))) break;
+        if ((st = stage(systems[k], T, pa.data(), pb.data(), k, z[k]))) break;
         const Staged& y = z[k];
+        t4_cap += (long long)y.t4.size();
+        b->max_T = std::max(b->max_T, y.fp.n_types);
         atoms += y.N;
         ex += (long long)y.ex_list.size();
         waters += y.water_numbers;
@@ -881,7 +933,7 @@ int spgnb_batch_create(int n_systems, const spgnb_batch_system* systems, int ato
     spec.table_cap = std::max((int)(per_cluster * 1.3) + 64, 128);
     spec.list_cap = list_cap_for(per_list);
     spec.prune_rc = rcmax;
-    if (!(st = create_common(b, spec, ex, (int)waters, T, pa.data(), pb.data())))
+    if (!(st = create_common(b, spec, ex, (int)waters, T, pa.data(), pb.data(), t4_cap)))
         for (int k = 0; k < n_systems && !st; k++)
         {
             int id = -1;
@@ -919,9 +971,12 @@ int spgnb_batch_create_pool(const spgnb_batch_pool_options* pool, int atom_type_
     else
         spgnb_batch_pool_default_options(&po);
     if (po.max_systems <= 0 || !(po.max_cutoff > 0.0f) || !(po.min_cutoff > 0.0f) || po.min_cutoff > po.max_cutoff ||
-        !(po.skin >= 0.0f) || !(po.density > 0.0f) || (po.max_atoms <= 0 && !(po.hbm_budget_bytes > 0.0)))
+        !(po.skin >= 0.0f) || !(po.density > 0.0f) || (po.max_atoms <= 0 && !(po.hbm_budget_bytes > 0.0)) ||
+        po.max_types < 0 || po.max_types > kMaxTypes || !(po.type_table_bytes >= 0.0))
         return fail(SPGNB_E_ARG, "spgnb_batch_create_pool: bad pool options");
     spgnb_batch* b = new_batch(opt, T, h_pair_A, h_pair_B);
+    b->max_T = std::max(T, po.max_types);
+    const long long t4_cap = (long long)T * T * T + (long long)(po.type_table_bytes / sizeof(float4));
     int atoms = po.max_atoms;
     // the largest atom count whose clusters fit the slot field of the lists
     {
@@ -939,8 +994,8 @@ int spgnb_batch_create_pool(const spgnb_batch_pool_options* pool, int atom_type_
         if (atoms <= 0)
         {
             // linear in the atom count: solve bytes(atoms) = budget
-            const double b1 = pool_bytes(po, b->opt.prune_buffer, 1 << 20, T);
-            const double b2 = pool_bytes(po, b->opt.prune_buffer, 1 << 21, T);
+            const double b1 = pool_bytes(po, b->opt.prune_buffer, 1 << 20, t4_cap);
+            const double b2 = pool_bytes(po, b->opt.prune_buffer, 1 << 21, t4_cap);
             const double per_atom = (b2 - b1) / (double)(1 << 20);
             const double fixed = b1 - per_atom * (1 << 20);
             atoms = (int)std::min<double>((po.hbm_budget_bytes - fixed) / per_atom, (double)(1 << 28));
@@ -957,7 +1012,7 @@ int spgnb_batch_create_pool(const spgnb_batch_pool_options* pool, int atom_type_
     const long long ex = po.max_excluded > 0 ? po.max_excluded : 2LL * atoms;
     const int w = po.max_waters > 0 ? po.max_waters : atoms / 3;
     b->fit = true;
-    if ((st = create_common(b, spec, ex, w, T, b->h_pair_A.data(), b->h_pair_B.data())))
+    if ((st = create_common(b, spec, ex, w, T, b->h_pair_A.data(), b->h_pair_B.data(), t4_cap)))
     {
         free_batch(b);
         delete b;
@@ -972,7 +1027,7 @@ int spgnb_batch_admit(spgnb_batch* b, const spgnb_batch_system* sys, int steps, 
     if (!b || !sys || !id) return fail(SPGNB_E_ARG, "spgnb_batch_admit: NULL argument");
     *id = -1;
     Staged z;
-    int st = stage(*sys, b->T, b->h_pair_A, b->h_pair_B, -1, z);
+    int st = stage(*sys, b->T, b->h_pair_A.data(), b->h_pair_B.data(), -1, z);
     if (st) return st;
     return admit_staged(b, z, steps, id);
 }
@@ -997,6 +1052,7 @@ int spgnb_batch_retire(spgnb_batch* b, int id)
     b->atom_pool.release(r.atom_begin, r.atom_count);
     b->ex_pool.release(r.ex_begin, r.ex_count);
     b->water_pool.release(r.w_begin, r.w_count);
+    b->t4_pool.release(r.t4_begin, r.t4_count);
     b->h_flags[id] = 0;
     r = SysRec{};
     return SPGNB_OK;
@@ -1051,7 +1107,7 @@ int spgnb_batch_capacity(spgnb_batch* b, int* max_systems, long long* max_atoms,
     if (free_atoms) *free_atoms = b->atom_pool.available();
     if (device_bytes)
         *device_bytes = (double)nl_device_bytes(b->nl) +
-                        batch_bytes(b->n, b->ex_cap, b->w_cap, (long long)b->nl->clusters_cap * kClusterSize, b->S, b->T);
+                        batch_bytes(b->n, b->ex_cap, b->w_cap, (long long)b->nl->clusters_cap * kClusterSize, b->S, b->t4_cap);
     return SPGNB_OK;
 }
 
@@ -1145,43 +1201,109 @@ int spgnb_batch_autotune(spgnb_batch* b, int steps_per_candidate, float* chosen_
 {
     if (!b) return fail(SPGNB_E_ARG, "spgnb_batch_autotune: NULL handle");
     if (steps_per_candidate <= 0) steps_per_candidate = 20;
-    // candidates up to the buffer the list was sized for
-    const float maxb = b->opt.prune_buffer;
-    const float cand[] = {0.4f, 0.6f, 0.8f, 1.0f, 1.3f, 1.6f};
-    float best = maxb;
-    float best_ms = 1e30f;
     cudaEvent_t e0, e1;
     SPGNB_CUDA(cudaEventCreate(&e0));
     SPGNB_CUDA(cudaEventCreate(&e1));
-    int st = SPGNB_OK;
-    for (float c : cand)
-    {
-        if (c > maxb + 1e-6f) continue;
-        b->nl->opt.prune_buffer = c;
-        if ((st = nl_prune_all(b->nl, b->stream))) break;
+    // steps of the current configuration per ms, warmed up (graphs captured,
+    // a pruning with a changed buffer done) before the timed steps; the
+    // timed count is a whole number of graphs
+    auto time_steps = [&](float* ms_per_step) -> int {
         free_graphs(b);
-        if ((st = spgnb_batch_run(b, b->opt.steps_per_graph, 0))) break;  // warm-up, includes the pruning
+        int st = spgnb_batch_run(b, b->opt.steps_per_graph, 0);
+        if (st) return st;
+        const int K = std::max(1, steps_per_candidate / b->opt.steps_per_graph) * b->opt.steps_per_graph;
         SPGNB_CUDA(cudaEventRecord(e0, b->stream));
-        if ((st = spgnb_batch_run(b, steps_per_candidate, 0))) break;
+        if ((st = spgnb_batch_run(b, K, 0))) return st;
         SPGNB_CUDA(cudaEventRecord(e1, b->stream));
         SPGNB_CUDA(cudaEventSynchronize(e1));
         float ms = 0;
         SPGNB_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-        if (ms < best_ms)
+        *ms_per_step = ms / K;
+        return SPGNB_OK;
+    };
+    int st = SPGNB_OK;
+    float best_ms = 1e30f;
+    // one setting at a time, the others at their best so far
+    auto tune = [&](auto set, const auto& candidates) {
+        auto best = candidates[0];
+        bool any = false;
+        for (auto c : candidates)
         {
-            best_ms = ms;
-            best = c;
+            if (!set(c)) continue;
+            float ms = 0;
+            if ((st = time_steps(&ms))) return;
+            if (!any || ms < best_ms)
+            {
+                best_ms = ms;
+                best = c;
+                any = true;
+            }
         }
+        set(best);
+    };
+    // the prune buffer, up to the one the lists were sized for
+    const float maxb = b->opt.prune_buffer;
+    const std::vector<float> buffers = {0.4f, 0.6f, 0.8f, 1.0f, 1.3f, 1.6f};
+    tune([&](float c) {
+        if (c > maxb + 1e-6f) return false;
+        b->nl->opt.prune_buffer = c;
+        b->opt.prune_buffer = c;
+        return nl_prune_all(b->nl, b->stream) == SPGNB_OK;
+    }, buffers);
+    if (!st)
+    {
+        // the force kernel's resident blocks per SM (0: all that fit)
+        const std::vector<int> pair_bps = {0, 3, 2};
+        best_ms = 1e30f;
+        tune([&](int c) { b->pair_bps = c; return true; }, pair_bps);
+    }
+    if (!st)
+    {
+        // the pruning kernel's blocks per SM
+        const std::vector<int> prune_bps = {5, 3, 8};
+        best_ms = 1e30f;
+        tune([&](int c) { b->prune_bps = c; return true; }, prune_bps);
+    }
+    if (!st)
+    {
+        const std::vector<int> graph_steps = {10, 5, 20};
+        best_ms = 1e30f;
+        tune([&](int c) { b->opt.steps_per_graph = c; return true; }, graph_steps);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (st) return st;
-    b->nl->opt.prune_buffer = best;
-    b->opt.prune_buffer = best;
+    b->tuned_ms = best_ms;
     free_graphs(b);
     if ((st = nl_prune_all(b->nl, b->stream))) return st;
     SPGNB_CUDA(cudaStreamSynchronize(b->stream));
-    if (chosen_buffer) *chosen_buffer = best;
+    if (chosen_buffer) *chosen_buffer = b->opt.prune_buffer;
+    return SPGNB_OK;
+}
+
+int spgnb_batch_set_tuning(spgnb_batch* b, const spgnb_batch_tuning* t)
+{
+    if (!b || !t) return fail(SPGNB_E_ARG, "spgnb_batch_set_tuning: NULL argument");
+    if (!(t->prune_buffer > 0.0f) || t->prune_buffer > b->opt.prune_buffer + 1e-6f || t->pair_blocks_per_sm < 0 ||
+        t->prune_blocks_per_sm < 0 || t->steps_per_graph <= 0)
+        return fail(SPGNB_E_ARG, "spgnb_batch_set_tuning: bad values (prune buffer in (0, %g])", b->opt.prune_buffer);
+    b->nl->opt.prune_buffer = t->prune_buffer;
+    b->opt.prune_buffer = t->prune_buffer;
+    b->pair_bps = t->pair_blocks_per_sm;
+    b->prune_bps = t->prune_blocks_per_sm;
+    b->opt.steps_per_graph = t->steps_per_graph;
+    free_graphs(b);
+    return nl_prune_all(b->nl, b->stream);
+}
+
+int spgnb_batch_get_tuning(spgnb_batch* b, spgnb_batch_tuning* out)
+{
+    if (!b || !out) return fail(SPGNB_E_ARG, "spgnb_batch_get_tuning: NULL argument");
+    out->prune_buffer = b->opt.prune_buffer;
+    out->pair_blocks_per_sm = b->pair_bps;
+    out->prune_blocks_per_sm = b->prune_bps > 0 ? b->prune_bps : 5;
+    out->steps_per_graph = b->opt.steps_per_graph;
+    out->ms_per_step = b->tuned_ms;
     return SPGNB_OK;
 }
 

@@ -10,14 +10,12 @@
 // cluster's atoms the partner pairs with (8 bits) << 22 | image flag << 30}.
 // A word's partner is evaluated against all eight atoms of I at once, so the
 // partner's gathers and the word's decoding are paid once per eight pairs.
-// The list has two parts:
-//   upper: partners in clusters J > I, and in I itself the pairs a < b;
-//   lower: partners in clusters J < I, and in I itself the pairs a > b.
-// The upper part alone holds every pair once (a half list); both parts hold
-// every pair from both sides (a full list).  Words are kept when the partner
-// lies within rc + buffer of one of the atoms at the last pruning, and a
-// pruning is redone when an atom has moved half the buffer since, so no pair
-// within rc is ever missing.
+// The list holds partners in clusters J > I, and in I itself the pairs
+// a < b: every pair once (a half list), the partner's share of each pair
+// scattered by int64 atomics.  Words are kept when the partner lies within
+// rc + buffer of one of the atoms at the last pruning, and a pruning is
+// redone when an atom has moved half the buffer since, so no pair within rc
+// is ever missing.
 #include <math.h>
 
 #include <algorithm>
@@ -110,15 +108,14 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
 
 // Pruning (no reference counterpart; results unchanged).  Runs after every
 // rebuild and whenever some atom of a system moved more than buffer/2 since
-// its last one (the pack kernel checks).  One warp per cluster I walks its
-// neighbour table, expands the union of the eight atoms' mask rows 32
-// elements at a time into shared memory, loads each candidate partner once,
-// tests it against all eight atoms without branches (packed FP32x2, two atoms
-// an instruction) and writes one word per partner within cutoff + buffer of
-// any of them: to the upper part (from the start of the cluster's region,
-// ascending) or the lower part (from its end, descending).  Both parts are
-// padded to whole windows with words whose mask is empty.  The last block to
-// finish clears the flags.
+// its last one (the pack kernel checks).  One warp per cluster I walks the
+// elements of its neighbour table with J >= I (a table built one-sided holds
+// no others), expands the union of the eight atoms' mask rows 32 elements at
+// a time into shared memory, loads each candidate partner once, tests it
+// against all eight atoms without branches (packed FP32x2, two atoms an
+// instruction) and writes one word per partner within cutoff + buffer of any
+// of them, in table order, padded to a whole window with words whose mask is
+// empty.  The last block to finish clears the flags.
 __global__ void __launch_bounds__(kPruneWarps * 32)
     k_prune8(ForceParams p0, const ForceParams* __restrict__ fps, float buffer, int* counters, int clusters_cap,
              int table_cap, int list_cap, const int* __restrict__ cl_sys, const SysDesc* __restrict__ sys,
@@ -171,8 +168,8 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
         const float4* __restrict__ tb = tab + (size_t)c * table_cap;
         const uint2* __restrict__ tm = tmask + (size_t)c * table_cap;
         unsigned* __restrict__ wc = words + (size_t)c * list_cap;
-        const int usable = list_cap - 2 * kWindow;  // room left for both parts' padding
-        int kh = 0, kl = 0;
+        const int usable = list_cap - kWindow;  // room left for the padding
+        int kh = 0;
         for (int t0 = 0; t0 < T; t0 += 32)
         {
             const int t = t0 + lane;
@@ -182,6 +179,8 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
             {
                 e = tb[t];
                 mm = tm[t];
+                // clusters below I hold the other side of its pairs
+                if (((__float_as_int(e.w) & 0x3fffffff) >> 3) < c) mm = make_uint2(0u, 0u);
             }
             // partners of any of the eight atoms
             unsigned u = mm.x | mm.y;
@@ -253,55 +252,32 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
                     }
                 }
                 hit &= am;
-                // the upper part takes the pairs of later clusters and, within
-                // the cluster, those with a < b; the lower part the others
-                const int J = js >> 3;
-                unsigned hb, lb;
-                if (J > c)
-                {
-                    hb = hit;
-                    lb = 0u;
-                }
-                else if (J < c)
-                {
-                    hb = 0u;
-                    lb = hit;
-                }
-                else
-                {
-                    const unsigned b = (unsigned)js & 7u;
-                    hb = hit & ((1u << b) - 1u);
-                    lb = hit & (0xfeu << b) & 0xffu;
-                }
+                // partners in later clusters pair with every atom they reach;
+                // within the cluster only the pairs a < b
+                if ((js >> 3) == c) hit &= (1u << (js & 7)) - 1u;
                 const unsigned wb = ((unsigned)js - slot0) | (img ? kWordImage : 0u);
-                const unsigned mh = __ballot_sync(0xffffffffu, hb != 0u);
-                const unsigned ml = __ballot_sync(0xffffffffu, lb != 0u);
-                const int kh_next = kh + __popc(mh), kl_next = kl + __popc(ml);
-                // the parts grow towards each other: [0, kh) and [cap - kl, cap)
-                if (kh_next + kl_next <= usable)
+                const unsigned mh = __ballot_sync(0xffffffffu, hit != 0u);
+                const int kh_next = kh + __popc(mh);
+                if (kh_next <= usable)
                 {
-                    if (hb) wc[kh + __popc(mh & below)] = wb | (hb << kWordMaskShift);
-                    if (lb) wc[list_cap - 1 - (kl + __popc(ml & below))] = wb | (lb << kWordMaskShift);
+                    if (hit) wc[kh + __popc(mh & below)] = wb | (hit << kWordMaskShift);
                 }
                 else if (lane == 0)
                     atomicOr(&counters[kCntOverflow], kOvfWords);
                 kh = kh_next;
-                kl = kl_next;
             }
             __syncwarp();
         }
         // an overflowed cluster keeps no list (the flag makes the caller regrow
-        // and rebuild); otherwise pad both parts to whole windows
-        if (kh + kl > usable) kh = kl = 0;
-        const int hp = (kh + kWindow - 1) & ~(kWindow - 1), lp = (kl + kWindow - 1) & ~(kWindow - 1);
+        // and rebuild); otherwise pad it to a whole window
+        if (kh > usable) kh = 0;
+        const int hp = (kh + kWindow - 1) & ~(kWindow - 1);
         const unsigned null_word = (unsigned)s0 - slot0;
         for (int k2 = kh + lane; k2 < hp; k2 += 32) wc[k2] = null_word;
-        for (int k2 = kl + lane; k2 < lp; k2 += 32) wc[list_cap - 1 - k2] = null_word;
         if (lane == 0)
         {
             lcount[s0] = hp;
-            lcount[s0 + 1] = lp;
-            atomicAdd(&kept_total, (unsigned long long)(kh + kl));
+            atomicAdd(&kept_total, (unsigned long long)kh);
         }
         __syncwarp();
     }
@@ -340,41 +316,33 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
 // asynchronous copies (cp.async) one iteration ahead of their use, list words
 // two, so their latency overlaps the pair arithmetic.
 //
-// HALF (forces, and forces with energy/virial totals): the upper part only,
-// each pair once; a lane holds all 8 atoms, the partner's force (summed over
-// the 8 in a fixed order) goes to its int64 fixed-point accumulator by one
-// atomic add per component and word, and the cluster's forces are summed
-// over the lanes as int64 and added the same way.  Integer addition does not
-// depend on order, so the forces are bitwise reproducible; the finishing pass
-// converts them.
-//
-// Full (per-atom energy and virial, MODE 2): both parts, each pair from both
-// sides.  Half-warps take four atoms each, over the same words; an atom's
-// force and its owned energy and virial (pairs whose other atom has the
-// higher global index, as the reference's half list credits them to the
-// owner; water sites hand theirs to the residue's first atom, as
-// SOLVENT_LENNARD_JONES does) are complete in the warp and added once.
+// Each pair is evaluated once; a lane holds all 8 atoms, the partner's force
+// (summed over the 8 in a fixed order) goes to its int64 fixed-point
+// accumulator by one atomic add per component and word, and the cluster's
+// forces are summed over the lanes as int64 and added the same way.  Integer
+// addition does not depend on order, so the forces are bitwise reproducible;
+// the finishing pass converts them.
 //
 // MODE 0: forces.  MODE 1: + energy and virial totals.  MODE 2: + per-atom
-// outputs, totals summed from them.
-template <int MODE, int FIT, bool TRI, bool HALF, int NI>
+// energy and virial: a pair's terms belong to its owner, the atom with the
+// lower global index, as the reference's half list credits them (water
+// sites hand theirs to the residue's first atom, as SOLVENT_LENNARD_JONES
+// does).  Cluster-owned sums stay in registers over the list; a word's
+// partner-owned sums go to the partner's int64 staging, 8 atomic adds; the
+// finishing pass turns the staging into the per-atom arrays and totals.
+template <int MODE, int FIT, bool TRI>
 __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
     k_pair8(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys, int n_clusters,
             int list_cap, const int* __restrict__ cl_sys, const int* __restrict__ lcount,
-            const unsigned* __restrict__ words, const int* __restrict__ slot_atom, const int4* __restrict__ cl_q,
-            const float4* __restrict__ pos, const int4* __restrict__ aux, const float4* __restrict__ t4,
-            float3* __restrict__ frc, long long* __restrict__ facc, long long* __restrict__ oacc,
-            long long* __restrict__ totals, OwnerMap om, PerAtomOut pa, const int* __restrict__ only,
+            const unsigned* __restrict__ words, const int4* __restrict__ cl_q, const float4* __restrict__ pos,
+            const int4* __restrict__ aux, const float4* __restrict__ t4, long long* __restrict__ facc,
+            long long* __restrict__ oacc, long long* __restrict__ totals, const int* __restrict__ only,
             int* __restrict__ counters, int max_types)
 {
     constexpr bool EN = MODE >= 1;
     constexpr bool PA = MODE >= 2;
-    static_assert(NI == 8 || NI == 4, "a lane holds all of the cluster's atoms or half of them");
-    // NI: cluster atoms a lane holds (with 4, two half-warps take the same
-    // words, each for half of the atoms)
-    constexpr int NP = NI / 2;   // as packed pairs
+    constexpr int NP = 4;        // the cluster's 8 atoms as packed pairs
     constexpr bool ISM = PA;     // the cluster's atoms in shared memory instead of registers
-    constexpr int WPI = 4 * NI;  // words an iteration takes
     __shared__ long long red[kPairWarps][8];  // per-warp fixed-point totals
     __shared__ int is_last;
     extern __shared__ float4 rows_all[];      // per warp: 4 x max_types coefficient rows
@@ -386,8 +354,6 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
     __shared__ __align__(16) int4 jaux_all[kPairWarps][2][32];    // partner aux records in flight
     const int lane = threadIdx.x & 31;
     const int w = threadIdx.x >> 5;
-    const int sub = NI == 8 ? 0 : lane >> 4;  // the half of the cluster this lane holds (NI = 4)
-    const int lw = lane & (WPI - 1);      // the word of an iteration this lane takes
     float4* __restrict__ rows = rows_all + w * 4 * max_types;
     unsigned(&wring)[3][32] = wring_all[w];
     float4(&iat)[4][2] = iat_all[w];
@@ -404,9 +370,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
         c = __shfl_sync(0xffffffffu, c, 0);
         if (c >= n_clusters) break;
         const int s0 = c * kClusterSize;
-        const int nh = lcount[s0];
-        const int nlo = HALF ? 0 : lcount[s0 + 1];
-        const int total = nh + nlo;  // multiples of the window
+        const int total = lcount[s0];  // a multiple of the window
         if (total == 0) continue;
         const int sy = cl_sys[c];
         if (only && !only[sy]) continue;
@@ -435,7 +399,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
         // (the per-atom mode keeps them in shared memory instead: its owned
         // sums already take 64 registers)
         float2 npx[ISM ? 1 : NP], npy[ISM ? 1 : NP], npz[ISM ? 1 : NP], qi[ISM ? 1 : NP];
-        int gi[ISM ? 1 : NI];
+        int gi[ISM ? 1 : 2 * NP];
         if (ISM)
         {
             __syncwarp();  // the previous cluster's atoms are no longer read
@@ -454,7 +418,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
 #pragma unroll
             for (int p = 0; p < NP; p++)
             {
-                const int a = sub * NI + 2 * p;
+                const int a = 2 * p;
                 const float4 u0 = pos[s0 + a], u1 = pos[s0 + a + 1];
                 const int4 x0 = aux[s0 + a], x1 = aux[s0 + a + 1];
                 npx[p] = make_float2(-u0.x, -u1.x);
@@ -494,17 +458,15 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
             for (int q = 0; q < (PA ? 8 : 1); q++) own[p][q] = f2(0.0f);
 
         const unsigned* __restrict__ wb = words + (size_t)c * list_cap;
-        // the k-th word of the list: the upper part, then the lower part
-        auto word_ptr = [&](int k) { return k < nh ? wb + k : wb + (list_cap - nlo) + (k - nh); };
         // a three-deep ring of list words and a two-deep ring of partner
         // records in shared memory, filled by asynchronous copies: a lane
         // only ever reads what it copied itself, so no warp barrier is needed
         auto stage_word = [&](int it) {
-            if (it * WPI < total) cp_async(&wring[it % 3][lane], word_ptr(it * WPI + lw), 4);
+            if (it * 32 < total) cp_async(&wring[it % 3][lane], wb + it * 32 + lane, 4);
             cp_async_commit();
         };
         auto stage_partner = [&](int it, unsigned w) {
-            if (it * WPI < total)
+            if (it * 32 < total)
             {
                 const int j = slot0 + (int)(w & kWordSlotMask);
                 cp_async(&jpos[it & 1][lane], pos + j, 16);
@@ -512,7 +474,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
             }
             cp_async_commit();
         };
-        const int iters = total / WPI;
+        const int iters = total / 32;
         stage_word(0);
         stage_word(1);
         cp_async_wait_prior();
@@ -530,8 +492,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
             const int jc = slot0 + (int)(wc & kWordSlotMask);
             stage_partner(it + 1, wn);
 
-            const unsigned m8 = (wc >> kWordMaskShift) & 0xffu;
-            const unsigned mi = NI == 8 ? m8 : (m8 >> (4 * sub)) & 0xfu;
+            const unsigned mi = (wc >> kWordMaskShift) & 0xffu;
             const float ux = centre_step(xjc.x, ci.x), uy = centre_step(xjc.y, ci.y), uz = centre_step(xjc.z, ci.z);
             // the partner in the frame of the cluster's centre
             float sx = __fmaf_rn(ux, qc.a11, pjc.x);
@@ -549,9 +510,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
             const int gj = xjc.w;
             const float2 qj = f2(pjc.w);
             float2 hx = f2(0.0f), hy = f2(0.0f), hz = f2(0.0f);  // the partner's force, negated
-            float2 jo[(PA && HALF) ? 8 : 1];                        // the partner's owned sums
+            float2 jo[PA ? 8 : 1];                                  // the partner's owned sums
 #pragma unroll
-            for (int q = 0; q < ((PA && HALF) ? 8 : 1); q++) jo[q] = f2(0.0f);
+            for (int q = 0; q < (PA ? 8 : 1); q++) jo[q] = f2(0.0f);
 #pragma unroll
             for (int p = 0; p < NP; p++)
             {
@@ -559,12 +520,12 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 int2 pg;
                 if (ISM)
                 {
-                    const float4 A = iat[sub * NP + p][0], B = iat[sub * NP + p][1];
+                    const float4 A = iat[p][0], B = iat[p][1];
                     pnx = make_float2(A.x, A.y);
                     pny = make_float2(A.z, A.w);
                     pnz = make_float2(B.x, B.y);
                     pq = make_float2(B.z, B.w);
-                    pg = igid[sub * NP + p];
+                    pg = igid[p];
                 }
                 else
                 {
@@ -596,7 +557,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 const float2 r2 = __ffma2_rn(dz, dz, __ffma2_rn(dy, dy, __fmul2_rn(dx, dx)));
                 const bool inA = ((mi >> (2 * p)) & 1u) && r2.x < pp.rc2;
                 const bool inB = ((mi >> (2 * p + 1)) & 1u) && r2.y < pp.rc2;
-                const float4 ab = rows[(sub * NP + p) * nt + tj];
+                const float4 ab = rows[p * nt + tj];
                 float2 elj, ec;
                 float2 f = pair_scalar2<EN, FIT>(r2, __fmul2_rn(qj, pq), make_float2(ab.x, ab.y),
                                                  make_float2(ab.z, ab.w), pp, elj, ec);
@@ -605,12 +566,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 fx[p] = __fadd2_rn(fx[p], gx);
                 fy[p] = __fadd2_rn(fy[p], gy);
                 fz[p] = __fadd2_rn(fz[p], gz);
-                if (HALF)
-                {
-                    hx = __fadd2_rn(hx, gx);
-                    hy = __fadd2_rn(hy, gy);
-                    hz = __fadd2_rn(hz, gz);
-                }
+                hx = __fadd2_rn(hx, gx);
+                hy = __fadd2_rn(hy, gy);
+                hz = __fadd2_rn(hz, gz);
                 if (EN && !PA)
                 {
                     acc[0] = __fadd2_rn(acc[0], make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f));
@@ -625,8 +583,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 if (PA)
                 {
                     // the pair's owner is the lower global index: this lane's
-                    // atom (kept over the list) or, over the half list, the
-                    // partner (summed over the word's atoms)
+                    // atom (kept over the list) or the partner (summed over
+                    // the word's atoms)
                     const float2 wi = make_float2(pg.x < gj ? 1.0f : 0.0f, pg.y < gj ? 1.0f : 0.0f);
                     const float2 v[8] = {make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f),
                                          make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f),
@@ -634,15 +592,12 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                                          __fmul2_rn(gx, dz), __fmul2_rn(gy, dz), __fmul2_rn(gz, dz)};
 #pragma unroll
                     for (int q = 0; q < 8; q++) own[p][q] = __ffma2_rn(v[q], wi, own[p][q]);
-                    if (HALF)
-                    {
-                        const float2 wj = __fadd2_rn(f2(1.0f), __fmul2_rn(wi, kPk[kPkMinusOne]));
+                    const float2 wj = __fadd2_rn(f2(1.0f), __fmul2_rn(wi, kPk[kPkMinusOne]));
 #pragma unroll
-                        for (int q = 0; q < 8; q++) jo[q] = __ffma2_rn(v[q], wj, jo[q]);
-                    }
+                    for (int q = 0; q < 8; q++) jo[q] = __ffma2_rn(v[q], wj, jo[q]);
                 }
             }
-            if (PA && HALF)
+            if (PA)
             {
                 // the partner's owned sums over this word: raw fixed point to
                 // its staging (scaled in the finishing pass)
@@ -652,10 +607,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                 for (int q = 0; q < 8; q++)
                 {
                     js[q] = jo[q].x + jo[q].y;
-                    if (NI == 4) js[q] += __shfl_xor_sync(0xffffffffu, js[q], 16);
                     any |= js[q] != 0.0f;
                 }
-                if (any && sub == 0)
+                if (any)
                 {
                     unsigned long long* oa = (unsigned long long*)(oacc + 8 * (size_t)jc);
 #pragma unroll
@@ -666,20 +620,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                     }
                 }
             }
-            if (HALF)
             {
                 // the partner's force: minus the sum over the cluster's atoms
-                if (NI == 4)
-                {
-                    // the other half-warp holds the other four atoms' share
-                    hx = __fadd2_rn(hx, make_float2(__shfl_xor_sync(0xffffffffu, hx.x, 16),
-                                                    __shfl_xor_sync(0xffffffffu, hx.y, 16)));
-                    hy = __fadd2_rn(hy, make_float2(__shfl_xor_sync(0xffffffffu, hy.x, 16),
-                                                    __shfl_xor_sync(0xffffffffu, hy.y, 16)));
-                    hz = __fadd2_rn(hz, make_float2(__shfl_xor_sync(0xffffffffu, hz.x, 16),
-                                                    __shfl_xor_sync(0xffffffffu, hz.y, 16)));
-                    if (sub) hx = hy = hz = f2(0.0f);
-                }
                 const long long qx = __float2ll_rn(-(hx.x + hx.y) * kTwoPow32);
                 const long long qy = __float2ll_rn(-(hy.x + hy.y) * kTwoPow32);
                 const long long qz = __float2ll_rn(-(hz.x + hz.y) * kTwoPow32);
@@ -698,37 +640,22 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
 #pragma unroll
         for (int a = 0; a < 8; a++)
         {
-            const int p = (a % NI) / 2;
-            const bool mine = NI == 8 || (a / NI) == sub;
+            const int p = a / 2;
             const float sxv = (a & 1) ? fx[p].y : fx[p].x, syv = (a & 1) ? fy[p].y : fy[p].x,
                         szv = (a & 1) ? fz[p].y : fz[p].x;
-            vx[a] = mine ? __float2ll_rn(sxv * kTwoPow32) : 0ll;
-            vy[a] = mine ? __float2ll_rn(syv * kTwoPow32) : 0ll;
-            vz[a] = mine ? __float2ll_rn(szv * kTwoPow32) : 0ll;
+            vx[a] = __float2ll_rn(sxv * kTwoPow32);
+            vy[a] = __float2ll_rn(syv * kTwoPow32);
+            vz[a] = __float2ll_rn(szv * kTwoPow32);
         }
         const long long Fx = reduce_scatter8(vx, lane), Fy = reduce_scatter8(vy, lane),
                         Fz = reduce_scatter8(vz, lane);
         const int va = lane >> 2;
         if ((lane & 3) == 0)
         {
-            if (HALF)
-            {
-                unsigned long long* fa = (unsigned long long*)(facc + 3 * (size_t)(s0 + va));
-                if (Fx) atomicAdd(fa + 0, (unsigned long long)Fx);
-                if (Fy) atomicAdd(fa + 1, (unsigned long long)Fy);
-                if (Fz) atomicAdd(fa + 2, (unsigned long long)Fz);
-            }
-            else
-            {
-                const int ai = slot_atom[s0 + va];
-                if (ai >= 0)
-                {
-                    // complete: one add per component and call
-                    atomicAdd(&frc[ai].x, (float)((double)Fx * kForceUnscale));
-                    atomicAdd(&frc[ai].y, (float)((double)Fy * kForceUnscale));
-                    atomicAdd(&frc[ai].z, (float)((double)Fz * kForceUnscale));
-                }
-            }
+            unsigned long long* fa = (unsigned long long*)(facc + 3 * (size_t)(s0 + va));
+            if (Fx) atomicAdd(fa + 0, (unsigned long long)Fx);
+            if (Fy) atomicAdd(fa + 1, (unsigned long long)Fy);
+            if (Fz) atomicAdd(fa + 2, (unsigned long long)Fz);
         }
         if (EN && !PA)
         {
@@ -747,48 +674,20 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
         }
         if (PA)
         {
+            // the cluster's owned sums: raw fixed point to each atom's
+            // staging (scaled in the finishing pass)
 #pragma unroll
             for (int a = 0; a < 8; a++)
             {
-                const int p = (a % NI) / 2;
-                const bool mine = (a / NI) == sub;
+                const int p = a / 2;
                 float v[8];
 #pragma unroll
-                for (int q = 0; q < 8; q++) v[q] = mine ? ((a & 1) ? own[p][q].y : own[p][q].x) : 0.0f;
+                for (int q = 0; q < 8; q++) v[q] = (a & 1) ? own[p][q].y : own[p][q].x;
                 // lanes 4q..4q+3 end with value q of atom a
                 const float val = reduce_scatter8(v, lane);
-                if (HALF)
-                {
-                    // raw fixed point to the atom's staging (scaled in the finishing pass)
-                    const long long r = __float2ll_rn(val * kTwoPow32);
-                    if ((lane & 3) == 0 && r) atomicAdd((unsigned long long*)(oacc + 8 * (size_t)(s0 + a) + va), (unsigned long long)r);
-                    continue;
-                }
-                const float sg = va >= 2 ? -1.0f : (va == 0 ? kLjEnergyScale : 1.0f);
-                const float sv = sg * val;
-                // an atom's energy is value 0 + value 1 (lanes 0 and 4)
-                const float ec_val = __shfl_down_sync(0xffffffffu, sv, 4);
-                if ((lane & 3) == 0)
-                {
-                    const bool twice = va == 3 || va == 5 || va == 6;
-                    red[w][va] += __double2ll_rn((double)sv * (twice ? 2.0 : 1.0) * kEnergyScale);
-                    const int ai = slot_atom[s0 + a];
-                    if (ai >= 0)
-                    {
-                        const int o = om.remap(ai);
-                        if (va == 0)
-                        {
-                            if (pa.energy) atomicAdd(pa.energy + o, sv + ec_val);
-                            if (pa.lj_energy) atomicAdd(pa.lj_energy + o, sv);
-                        }
-                        else if (va == 1)
-                        {
-                            if (pa.direct) atomicAdd(pa.direct + o, sv);
-                        }
-                        else if (pa.virial)
-                            atomicAdd(pa.virial + 6 * (size_t)o + (va - 2), twice ? 2.0f * sv : sv);
-                    }
-                }
+                const long long r = __float2ll_rn(val * kTwoPow32);
+                if ((lane & 3) == 0 && r)
+                    atomicAdd((unsigned long long*)(oacc + 8 * (size_t)(s0 + a) + va), (unsigned long long)r);
             }
         }
     }
@@ -992,21 +891,21 @@ int resident_blocks(K kernel, int threads, size_t smem)
     return per_sm * num_sms();
 }
 
-template <int M, int F, bool T, bool H, int NI>
+template <int M, int F, bool T>
 int launch_pair(const ForceInputs& in, cudaStream_t s)
 {
     const spgnb_nl* nl = in.nl;
-    const int mt = in.p0.n_types;
+    const int mt = in.max_types > 0 ? in.max_types : in.p0.n_types;
     const size_t smem = sizeof(float4) * kPairWarps * 4 * mt;
-    const int grid = std::max(1, std::min(resident_blocks(k_pair8<M, F, T, H, NI>, kPairWarps * 32, smem),
-                                          (nl->clusters_cap + kPairWarps - 1) / kPairWarps));
+    int resident = resident_blocks(k_pair8<M, F, T>, kPairWarps * 32, smem);
+    if (in.pair_blocks_per_sm > 0) resident = std::min(resident, in.pair_blocks_per_sm * num_sms());
+    const int grid = std::max(1, std::min(resident, (nl->clusters_cap + kPairWarps - 1) / kPairWarps));
     if (smem > 48 * 1024)
-        SPGNB_CUDA(cudaFuncSetAttribute(k_pair8<M, F, T, H, NI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        SPGNB_CUDA(cudaFuncSetAttribute(k_pair8<M, F, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
-    k_pair8<M, F, T, H, NI><<<grid, kPairWarps * 32, smem, s>>>(
-        in.p0, in.d_fps, nl->d_sys, nl->clusters_cap, nl->list_cap, nl->d_cl_sys, nl->d_pcount,
-        nl->d_pwords, nl->d_slot_atom, nl->d_cl_q, in.slot_pos, in.slot_aux, in.t4, in.frc, nl->d_facc, nl->d_oacc,
-        in.totals, in.om, in.pa, in.only, nl->d_counters, mt);
+    k_pair8<M, F, T><<<grid, kPairWarps * 32, smem, s>>>(
+        in.p0, in.d_fps, nl->d_sys, nl->clusters_cap, nl->list_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords,
+        nl->d_cl_q, in.slot_pos, in.slot_aux, in.t4, nl->d_facc, nl->d_oacc, in.totals, in.only, nl->d_counters, mt);
     SPGNB_CHECK_LAUNCH("k_pair8");
     return SPGNB_OK;
 }
@@ -1014,9 +913,7 @@ int launch_pair(const ForceInputs& in, cudaStream_t s)
 template <int M, int F>
 int launch_pair_t(const ForceInputs& in, bool tri, cudaStream_t s)
 {
-    // every mode walks the half list; the per-atom mode holds four atoms a lane
-    constexpr int NI = 8;
-    return tri ? launch_pair<M, F, true, true, NI>(in, s) : launch_pair<M, F, false, true, NI>(in, s);
+    return tri ? launch_pair<M, F, true>(in, s) : launch_pair<M, F, false>(in, s);
 }
 
 template <int M>
@@ -1027,7 +924,7 @@ int launch_pair_ft(const ForceInputs& in, bool tri, cudaStream_t s)
 
 }  // namespace
 
-int build_t4(const float2* table, int T, float4** d_t4)
+std::vector<float4> coefficient_table(const float2* table, int T)
 {
     std::vector<float4> t4((size_t)T * T * T);
     for (int a = 0; a < T; a++)
@@ -1037,6 +934,12 @@ int build_t4(const float2* table, int T, float4** d_t4)
                 const float2 ga = table[(size_t)a * T + j], gb = table[(size_t)b * T + j];
                 t4[((size_t)a * T + b) * T + j] = make_float4(-ga.x, -gb.x, ga.y, gb.y);
             }
+    return t4;
+}
+
+int build_t4(const float2* table, int T, float4** d_t4)
+{
+    const std::vector<float4> t4 = coefficient_table(table, T);
     dfree(*d_t4);
     int st = dalloc(d_t4, t4.size());
     if (st) return st;
@@ -1062,7 +965,8 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
                                                      nl->d_prune, in.clear.totals, in.clear.one, in.clear.a, in.clear.b,
                                                      in.clear.n);
     SPGNB_CHECK_LAUNCH("k_pack_slots");
-    const int grid = std::max(1, std::min(num_sms() * 5, (nl->clusters_cap + kPruneWarps - 1) / kPruneWarps));
+    const int prune_bps = in.prune_blocks_per_sm > 0 ? in.prune_blocks_per_sm : 5;
+    const int grid = std::max(1, std::min(num_sms() * prune_bps, (nl->clusters_cap + kPruneWarps - 1) / kPruneWarps));
     k_prune8<<<grid, kPruneWarps * 32, 0, s>>>(in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters,
                                                nl->clusters_cap, nl->table_cap, nl->list_cap,
                                                nl->d_cl_sys, nl->d_sys, nl->d_tcount, nl->d_tab, nl->d_tmask,

@@ -250,6 +250,11 @@ struct spgnb_nl
     float prune_rc = 0;    // cutoff the pruned lists are made for
     bool built = false;
     int local_atoms = 0;
+    // neighbour tables two-sided (every neighbour cluster) for the exports
+    // and the soft-core kernel, or one-sided (J >= I) when only the pruned
+    // half list reads them; the last build's kind, and its exclusion arrays
+    mutable bool sym_tables = false, sym_built = false;
+    const int *ex_start_last = nullptr, *ex_list_last = nullptr, *ex_num_last = nullptr;
 
     std::vector<spgnb::SysDesc> h_desc;  // host copy of d_sys
     spgnb::SysDesc* d_sys = nullptr;
@@ -448,11 +453,14 @@ struct ForceInputs
     ForceParams p0{};                  // the one system's parameters (d_fps null)
     const ForceParams* d_fps = nullptr;  // per system (several systems)
     bool fit = true;                   // every system inside the rational fits' range
-    const float4* t4 = nullptr;        // the T^3 pair table (build_t4)
+    const float4* t4 = nullptr;        // the T^3 pair tables (coefficient_table)
+    int max_types = 0;                 // most types of any system's table (0: p0.n_types)
     float3* frc = nullptr;             // += forces
     long long* totals = nullptr;       // 8 fixed-point sums per system (mode >= 1)
     const int* only = nullptr;         // per-system flags: evaluate these systems only (null: all)
     int mode = 0;                      // 0 forces, 1 + totals, 2 + per-atom outputs
+    int pair_blocks_per_sm = 0;        // force kernel grid: 0 = as many as are resident
+    int prune_blocks_per_sm = 0;       // pruning kernel grid: 0 = 5
     OwnerMap om{nullptr, 0, 3};
     PerAtomOut pa{nullptr, nullptr, nullptr, nullptr};
     ExclFuse xf{};                     // one system only
@@ -468,8 +476,11 @@ struct ForceInputs
     } clear;
 };
 int force_pipeline(const ForceInputs& in, cudaStream_t s);
-// Uploads the T^3 table the force kernel reads from a T x T {A, B} table:
-// element (a*T + b)*T + j is {-A(a,j), -A(b,j), B(a,j), B(b,j)}.
+// The force kernel's coefficient table of a T x T square pair table {A, B}:
+// element (a*T + b)*T + j = {-A_aj, -A_bj, B_aj, B_bj}, the rows of an atom
+// pair (a, b) of a cluster against every partner type j.
+std::vector<float4> coefficient_table(const float2* table, int T);
+// coefficient_table uploaded to a new device array (freeing the old one).
 int build_t4(const float2* table, int T, float4** d_t4);
 // Adds the module's int64 force accumulators of atoms [0, n) to frc and
 // clears them (the reference-layout and correction paths end with it).
@@ -533,6 +544,10 @@ size_t nl_admit_upload_bytes(const SysHost& sh, size_t n_runs);
 int nl_retire(spgnb_nl* nl, int id, cudaStream_t s);
 // Every live system re-prunes before the next force evaluation.
 int nl_prune_all(spgnb_nl* nl, cudaStream_t s);
+// Makes this and later builds' neighbour tables two-sided: re-runs the last
+// build's search (same clusters and build coordinates, so the same list) when
+// its tables are one-sided.
+int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s);
 enum BuildHow
 {
     kBuildSkin = 0,

@@ -373,10 +373,13 @@ __device__ __forceinline__ float3 frac_to_cart(float3 f, const Cell& c)
     return make_float3(f.x * c.a11 + f.y * c.a21 + f.z * c.a31, f.y * c.a22 + f.z * c.a32, f.z * c.a33);
 }
 
-// Neighbour search, one warp per cluster, symmetric: every cluster finds all
-// of its neighbour clusters (lower and higher), so its table comes out
-// complete and in a deterministic order (candidate runs, then cluster index)
-// with no sorting or atomics.  For each candidate cluster that passes a
+// Neighbour search, one warp per cluster.  Symmetric (two-sided) tables:
+// every cluster finds all of its neighbour clusters (lower and higher), so
+// its table comes out complete and in a deterministic order (candidate runs,
+// then cluster index) with no sorting or atomics; the reference-layout and
+// full-list exports and the soft-core kernel read those.  One-sided tables
+// (half set): a cluster keeps only neighbour clusters J >= I, each cluster
+// pair is searched once, and the pruned half list needs no more.  For each candidate cluster that passes a
 // conservative sphere test, the 64 atom pairs are decided as the reference
 // decides them: a pair needs the higher-index atom's cell in the stencil of
 // the lower-index atom's cell, squared distance below 4*grid_length^2 in the
@@ -411,9 +414,9 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
              const int2* __restrict__ slot_ex,
              const int* __restrict__ ex_start, const int* __restrict__ ex_list, const int* __restrict__ ex_num,
              int* __restrict__ tcount, float4* __restrict__ tab, uint2* __restrict__ tmask,
-             int* __restrict__ slot_count, int* counters)
+             int* __restrict__ slot_count, int* counters, const int* __restrict__ go, int half)
 {
-    if (counters[kCntNeed] == 0) return;
+    if (go && *go == 0) return;
     __shared__ float4 stage_t[kSearchWarps][kChunk];
     __shared__ uint2 stage_m[kSearchWarps][kChunk];
     const int lane = threadIdx.x & 31;
@@ -477,7 +480,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
             {
                 const int cj = b0 + lane;
                 bool ok = false;
-                if (cj < b1)
+                if (cj < b1 && (!half || cj >= c))
                 {
                     const uint4 uj = cl_u[cj];
                     const float3 f = frac_delta(ui, uj);
@@ -806,6 +809,17 @@ __global__ void k_fill_int(int* __restrict__ p, long long n, int v)
         p[i] = v;
 }
 
+// Before a search that re-makes the last build's tables two-sided: the
+// cluster counter and the table statistics start again.
+__global__ void k_sym_begin(int* counters)
+{
+    counters[kCntEntries] = 0;
+    counters[kCntEntries + 1] = 0;
+    counters[kCntWords] = 0;
+    counters[kCntWords + 1] = 0;
+    counters[kCntSearchNext] = 0;
+}
+
 __global__ void k_reset_list_counters(int* counters)
 {
     if (counters[kCntNeed] == 0) return;
@@ -1119,6 +1133,8 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemset(nl->d_counters, 0, sizeof(int) * kCntSize));
     if ((st = alloc_tables(nl))) return st;
     if ((st = alloc_words(nl))) return st;
+    // the reference-layout export reads each atom's partners on both sides
+    nl->sym_tables = nl->opt.export_atom_groups != 0;
     if (nl->opt.export_atom_groups)
     {
         if ((st = dalloc(&nl->d_nl, n))) return st;
@@ -1496,8 +1512,13 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
         nl->d_sys, ccap, nl->table_cap, nl->d_need, nl->d_ncl, nl->d_run_start, nl->d_runs, nl->d_cell_cl,
         nl->d_cl_cell, nl->d_cl_sys, nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex,
-        ex_start, ex_list, ex_num, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_counters);
+        ex_start, ex_list, ex_num, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_counters,
+        nl->d_counters + kCntNeed, nl->sym_tables ? 0 : 1);
     SPGNB_CHECK_LAUNCH("k_search");
+    nl->sym_built = nl->sym_tables;
+    nl->ex_start_last = ex_start;
+    nl->ex_list_last = ex_list;
+    nl->ex_num_last = ex_num;
     if (nl->opt.export_atom_groups)
     {
         k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
@@ -1752,6 +1773,35 @@ int spgnb_nl_copy_atom_groups(spgnb_nl* nl, int* h_counts, int* h_lists, long lo
     return SPGNB_OK;
 }
 
+}  // extern "C"
+
+namespace spgnb
+{
+
+int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s)
+{
+    nl->sym_tables = true;
+    if (!nl->built || nl->sym_built) return SPGNB_OK;
+    k_sym_begin<<<1, 1, 0, s>>>(nl->d_counters);
+    SPGNB_CHECK_LAUNCH("k_sym_begin");
+    const int ccap = nl->clusters_cap;
+    const int search_blocks = std::max(1, std::min((ccap + kSearchWarps - 1) / kSearchWarps, num_sms() * 5));
+    // every live system, whatever the last build flagged: a system's tables
+    // are those of its own last build either way
+    k_search<<<search_blocks, kSearchWarps * 32, 0, s>>>(
+        nl->d_sys, ccap, nl->table_cap, nl->d_live, nl->d_ncl, nl->d_run_start, nl->d_runs, nl->d_cell_cl,
+        nl->d_cl_cell, nl->d_cl_sys, nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex,
+        nl->ex_start_last, nl->ex_list_last, nl->ex_num_last, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_count,
+        nl->d_counters, nullptr, 0);
+    SPGNB_CHECK_LAUNCH("k_search");
+    nl->sym_built = true;
+    return SPGNB_OK;
+}
+
+}  // namespace spgnb
+
+extern "C" {
+
 int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector* d_crd, spgnb_ltmatrix3 cell,
                         spgnb_ltmatrix3 rcell, float cutoff, spgnb_atom_group* d_full_nl, int max_neighbor_numbers,
                         int* d_overflow)
@@ -1765,6 +1815,8 @@ int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector
     if (cutoff > 0.0f && !d_crd) return fail(SPGNB_E_ARG, "spgnb_nl_build_full: a cutoff needs coordinates");
     if (!d_overflow) return fail(SPGNB_E_ARG, "spgnb_nl_build_full: NULL overflow flag");
     cudaStream_t s = stream();
+    int st = nl_symmetrize(nl, s);
+    if (st) return st;
     const int n = local_atom_numbers;
     // atoms in no cluster with a table (none, normally) keep a zero count
     k_zero_groups<<<(n + 255) / 256, 256, 0, s>>>(n, d_full_nl);

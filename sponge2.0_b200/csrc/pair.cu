@@ -402,27 +402,25 @@ __global__ void k_long_range(int need_pressure, float* virial, int need_potentia
     if (need_potential) potential[0] += efac;
 }
 
+// SOLVENT_LENNARD_JONES get_local_device (solvent_LJ.cpp:433-467): the
+// solvent is the longest run of residues at the end of the local atoms that
+// are waters of water_points atoms (O mass about 16, H masses about 1.008),
+// counted from the last residue backwards.  Residue i of that run starts at
+// atom_numbers - water_points * (local_res_numbers - i); one thread per
+// residue tests it, and the run starts after the last residue that fails.
 __global__ void k_solvent_count(int local_res_numbers, const int* __restrict__ res_len, int water_points,
-                                int atom_numbers, const float* __restrict__ mass, int* out)
+                                int atom_numbers, const float* __restrict__ mass, int* last_fail)
 {
-    // SOLVENT_LENNARD_JONES get_local_device (solvent_LJ.cpp:433-467)
-    int start = local_res_numbers, cnt = 0;
-    for (int i = local_res_numbers - 1; i >= 0; i--)
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= local_res_numbers) return;
+    const int rs = atom_numbers - water_points * (local_res_numbers - i);
+    bool water = rs >= 0 && res_len[i] == water_points;
+    if (water)
     {
-        int rs = atom_numbers - water_points * (cnt + 1);
-        if (rs < 0) break;
-        float mo = mass[rs], m1 = mass[rs + 1], m2 = mass[rs + 2];
-        if (res_len[i] == water_points && mo > 15.8f && mo < 16.2f && m1 > 1.007f && m1 < 1.009f && m2 > 1.007f &&
-            m2 < 1.009f)
-        {
-            start--;
-            cnt++;
-        }
-        else
-            break;
+        const float mo = mass[rs], m1 = mass[rs + 1], m2 = mass[rs + 2];
+        water = mo > 15.8f && mo < 16.2f && m1 > 1.007f && m1 < 1.009f && m2 > 1.007f && m2 < 1.009f;
     }
-    out[0] = start;
-    out[1] = cnt * water_points;
+    if (!water) atomicMax(last_fail, i);
 }
 
 PairConst make_pair_const(const spgnb_lj* lj, float beta)
@@ -927,15 +925,19 @@ int spgnb_solvent_get_local(spgnb_solvent* s, int local_res_numbers, const int* 
                             const float* d_mass, int* local_solvent_numbers)
 {
     if (!s || !d_res_len || !d_mass) return fail(SPGNB_E_ARG, "spgnb_solvent_get_local: NULL argument");
-    k_solvent_count<<<1, 1, 0, stream()>>>(local_res_numbers, d_res_len, s->water_points, atom_numbers, d_mass,
-                                           s->d_scratch);
-    SPGNB_CHECK_LAUNCH("k_solvent_count");
-    int h[2];
-    SPGNB_CUDA(cudaMemcpyAsync(h, s->d_scratch, sizeof(h), cudaMemcpyDeviceToHost, stream()));
+    SPGNB_CUDA(cudaMemsetAsync(s->d_scratch, 0xff, sizeof(int), stream()));  // no failing residue: -1
+    if (local_res_numbers > 0)
+    {
+        k_solvent_count<<<(local_res_numbers + 255) / 256, 256, 0, stream()>>>(
+            local_res_numbers, d_res_len, s->water_points, atom_numbers, d_mass, s->d_scratch);
+        SPGNB_CHECK_LAUNCH("k_solvent_count");
+    }
+    int last_fail = -1;
+    SPGNB_CUDA(cudaMemcpyAsync(&last_fail, s->d_scratch, sizeof(int), cudaMemcpyDeviceToHost, stream()));
     SPGNB_CUDA(cudaStreamSynchronize(stream()));
-    s->solvent_start_local = h[0];
-    s->local_solvent_numbers = h[1];
-    if (local_solvent_numbers) *local_solvent_numbers = h[1];
+    s->solvent_start_local = last_fail + 1;
+    s->local_solvent_numbers = (local_res_numbers - (last_fail + 1)) * s->water_points;
+    if (local_solvent_numbers) *local_solvent_numbers = s->local_solvent_numbers;
     return SPGNB_OK;
 }
 

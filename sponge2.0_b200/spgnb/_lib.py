@@ -35,7 +35,8 @@ EXPORTED = [
     "spgnb_lj_soft_long_range_factors", "spgnb_lj_soft_atom_lj_energy", "spgnb_lj_soft_perturbed_atoms",
     "spgnb_lj_soft_destroy", "spgnb_solvent_create_soft",
     "spgnb_batch_default_options", "spgnb_batch_create", "spgnb_batch_run", "spgnb_batch_energies",
-    "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_stream",
+    "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_get_tuning", "spgnb_batch_set_tuning",
+    "spgnb_batch_stream",
     "spgnb_batch_check_overflow", "spgnb_batch_set_thermostat",
     "spgnb_batch_destroy",
     "spgnb_batch_pool_default_options", "spgnb_batch_create_pool", "spgnb_batch_admit", "spgnb_batch_retire",
@@ -73,7 +74,8 @@ class BatchSystem(C.Structure):
                 ("h_charge", C.c_void_p), ("h_mass", C.c_void_p), ("h_atom_type", C.c_void_p),
                 ("h_excluded_start", C.c_void_p), ("h_excluded_numbers", C.c_void_p),
                 ("h_excluded_list", C.c_void_p), ("excluded_total", C.c_int), ("water_begin", C.c_int),
-                ("water_numbers", C.c_int)]
+                ("water_numbers", C.c_int), ("atom_type_numbers", C.c_int), ("h_pair_A", C.c_void_p),
+                ("h_pair_B", C.c_void_p)]
 
 
 class BatchOptions(C.Structure):
@@ -82,10 +84,16 @@ class BatchOptions(C.Structure):
                 ("thermostat_tau", C.c_float), ("temperature", C.c_float), ("refresh_interval", C.c_int)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("prune_buffer", C.c_float), ("pair_blocks_per_sm", C.c_int), ("prune_blocks_per_sm", C.c_int),
+                ("steps_per_graph", C.c_int), ("ms_per_step", C.c_float)]
+
+
 class PoolOptions(C.Structure):
     _fields_ = [("max_systems", C.c_int), ("max_atoms", C.c_int), ("max_excluded", C.c_longlong),
                 ("max_waters", C.c_int), ("max_cutoff", C.c_float), ("min_cutoff", C.c_float), ("skin", C.c_float),
-                ("density", C.c_float), ("hbm_budget_bytes", C.c_double)]
+                ("density", C.c_float), ("hbm_budget_bytes", C.c_double), ("max_types", C.c_int),
+                ("type_table_bytes", C.c_double)]
 
 
 class SoftCoreParams(C.Structure):
@@ -138,6 +146,8 @@ def lib():
     L.spgnb_batch_stats.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong), C.POINTER(C.c_longlong),
                                     C.POINTER(C.c_int)]
     L.spgnb_batch_autotune.argtypes = [vp, i, C.POINTER(C.c_float)]
+    L.spgnb_batch_get_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
+    L.spgnb_batch_set_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
     L.spgnb_batch_check_overflow.argtypes = [vp, C.POINTER(i)]
     L.spgnb_batch_set_thermostat.argtypes = [vp, f, f]
     L.spgnb_batch_stream.argtypes = [vp]

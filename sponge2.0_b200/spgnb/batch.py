@@ -3,8 +3,8 @@
 ``Batch`` wraps the ``spgnb_batch_*`` C ABI for a fixed set of systems and
 ``Pool`` for a pool into which systems are admitted and from which they are
 retired while the others run (continuous batching).  Every system keeps its
-own box, cutoff, skin, Ewald beta, exclusions and rigid waters; all share one
-LJ type table.  A step is leap-frog velocity Verlet with SETTLE, the
+own box, cutoff, skin, Ewald beta, exclusions and rigid waters, and its own
+LJ type table where it differs from the batch's.  A step is leap-frog velocity Verlet with SETTLE, the
 per-system skin-triggered neighbour-list update and one LJ + PME direct-space
 force launch over all systems, replayed from captured CUDA graphs.  A
 system's results are bitwise the same alone and in any mix.
@@ -15,7 +15,7 @@ import ctypes as C
 
 import numpy as np
 
-from ._lib import SPGNB_OK, BatchOptions, BatchSystem, LTMatrix3, PoolOptions, SpgnbError, check, lib
+from ._lib import SPGNB_OK, BatchOptions, BatchSystem, BatchTuning, LTMatrix3, PoolOptions, SpgnbError, check, lib
 
 SPGNB_E_OOM = 2
 
@@ -40,8 +40,9 @@ def _ptr(a):
     return a.ctypes.data_as(C.c_void_p) if a is not None else None
 
 
-def _fill(y, s, keep):
-    """Fill a BatchSystem from a ``spgnb.systems`` system; arrays go to keep."""
+def _fill(y, s, keep, own_table=False):
+    """Fill a BatchSystem from a ``spgnb.systems`` system; arrays go to keep.
+    With own_table the system carries its type table (else the batch's)."""
     if getattr(s, "water_points", 3) != 3:
         raise ValueError("the batched engine constrains 3-site waters (SETTLE) only")
     crd = np.ascontiguousarray(s.crd, np.float32)
@@ -65,14 +66,16 @@ def _fill(y, s, keep):
     y.excluded_total = len(s.excl_list)
     y.water_begin = s.n_solute
     y.water_numbers = s.n_waters
+    if own_table:
+        pa = np.ascontiguousarray(s.pair_A, np.float32)
+        pb = np.ascontiguousarray(s.pair_B, np.float32)
+        keep += [pa, pb]
+        y.atom_type_numbers = s.n_types
+        y.h_pair_A, y.h_pair_B = _ptr(pa), _ptr(pb)
 
 
-def _same_table(systems):
-    s0 = systems[0]
-    for s in systems[1:]:
-        if s.n_types != s0.n_types or not np.array_equal(s.pair_A, s0.pair_A) or \
-                not np.array_equal(s.pair_B, s0.pair_B):
-            raise ValueError("the systems of a batch share one LJ type table")
+def _same_table(a, b):
+    return a.n_types == b.n_types and np.array_equal(a.pair_A, b.pair_A) and np.array_equal(a.pair_B, b.pair_B)
 
 
 class _Common:
@@ -110,9 +113,23 @@ class _Common:
         return bool(r.value)
 
     def autotune(self, steps_per_candidate=20):
+        """Picks the fastest launch configuration (the systems advance
+        meanwhile); returns the chosen prune buffer, ``tuning()`` the rest."""
         best = C.c_float()
         check(lib().spgnb_batch_autotune(self.handle, int(steps_per_candidate), C.byref(best)))
         return best.value
+
+    def tuning(self):
+        t = BatchTuning()
+        check(lib().spgnb_batch_get_tuning(self.handle, C.byref(t)))
+        return {"prune_buffer": t.prune_buffer, "pair_blocks_per_sm": t.pair_blocks_per_sm,
+                "prune_blocks_per_sm": t.prune_blocks_per_sm, "steps_per_graph": t.steps_per_graph,
+                "ms_per_step": t.ms_per_step}
+
+    def set_tuning(self, prune_buffer, pair_blocks_per_sm, prune_blocks_per_sm, steps_per_graph):
+        t = BatchTuning(float(prune_buffer), int(pair_blocks_per_sm), int(prune_blocks_per_sm),
+                        int(steps_per_graph), 0.0)
+        check(lib().spgnb_batch_set_tuning(self.handle, C.byref(t)))
 
     def evaluate(self, ids):
         """Forces, energies and virial now for these systems only."""
@@ -149,17 +166,17 @@ class _Common:
 
 
 class Batch(_Common):
-    """Systems from ``spgnb.systems`` (same ``pair_A``/``pair_B`` table), ids 0..n-1."""
+    """Systems from ``spgnb.systems``, ids 0..n-1.  The first system's type
+    table is the batch's; a system whose table differs carries its own."""
 
     def __init__(self, systems, options=None, **kw):
         L = lib()
         self.systems = list(systems)
-        _same_table(self.systems)
         s0 = self.systems[0]
         self._keep = []
         arr = (BatchSystem * len(self.systems))()
         for k, s in enumerate(self.systems):
-            _fill(arr[k], s, self._keep)
+            _fill(arr[k], s, self._keep, own_table=not _same_table(s, s0))
         self.options = options if options is not None else default_options(**kw)
         pa = np.ascontiguousarray(s0.pair_A, np.float32)
         pb = np.ascontiguousarray(s0.pair_B, np.float32)
@@ -176,7 +193,9 @@ class Batch(_Common):
 
 
 class Pool(_Common):
-    """An empty pool for systems sharing the type table of ``template``.
+    """An empty pool whose type table is that of ``template``; an admitted
+    system whose table differs carries its own (up to the pool options'
+    ``max_types`` types).
 
     ``admit`` returns an id, or None when the pool has no room now."""
 
@@ -195,10 +214,9 @@ class Pool(_Common):
         self.members = {}
 
     def admit(self, system, steps=0):
-        _same_table([self.template, system])
         keep = []
         y = BatchSystem()
-        _fill(y, system, keep)
+        _fill(y, system, keep, own_table=not _same_table(system, self.template))
         i = C.c_int(-1)
         st = lib().spgnb_batch_admit(self.handle, C.byref(y), int(steps), C.byref(i))
         if st == SPGNB_E_OOM:

@@ -90,3 +90,36 @@ def test_rigid_waters_stay_rigid(torch_cuda):
     st = b.stats()
     assert st["overflow"] == 0 and st["steps"] == 200
     b.close()
+
+
+def test_launch_configuration_changes_no_result(torch_cuda):
+    """The autotuner's knobs that keep the lists (the force and pruning
+    kernels' grids, the steps per graph) change no bit of the results."""
+    from spgnb.batch import Batch
+    systems = _small_batch(2, seed=15)
+    a = Batch(systems, steps_per_graph=10)
+    b = Batch(systems, steps_per_graph=10)
+    b.set_tuning(a.tuning()["prune_buffer"], 2, 3, 5)
+    assert b.tuning()["pair_blocks_per_sm"] == 2 and b.tuning()["steps_per_graph"] == 5
+    a.run(30, energy_interval=10)
+    b.run(30, energy_interval=10)
+    for k in range(len(systems)):
+        for x, y in zip(a.download(k), b.download(k)):
+            assert np.array_equal(x, y)
+    assert np.array_equal(a.energies(), b.energies())
+    a.close()
+    b.close()
+
+
+def test_autotune_picks_among_candidates(torch_cuda):
+    from spgnb.batch import Batch
+    b = Batch(_small_batch(2, seed=16), prune_buffer=1.6)
+    buf = b.autotune(5)
+    t = b.tuning()
+    assert buf == t["prune_buffer"] and 0.4 <= buf <= 1.6
+    assert t["pair_blocks_per_sm"] in (0, 2, 3) and t["prune_blocks_per_sm"] in (3, 5, 8)
+    assert t["steps_per_graph"] in (5, 10, 20) and t["ms_per_step"] > 0
+    b.run(20)
+    st = b.stats()
+    assert st["overflow"] == 0
+    b.close()

@@ -24,6 +24,17 @@ STEPS = 300
 REFRESH = 20
 
 
+def _timed(fn):
+    """fn() inside the NVTX range 'timed', so that a launch list of this
+    test (ncu --nvtx --nvtx-include timed/) holds the timed steps only."""
+    import torch
+    torch.cuda.nvtx.range_push("timed")
+    try:
+        return fn()
+    finally:
+        torch.cuda.nvtx.range_pop()
+
+
 def _harness_times(shim, s, f):
     """{(path, energy and virial?): seconds for STEPS steps}."""
     import oracle as O
@@ -33,14 +44,15 @@ def _harness_times(shim, s, f):
     ref.nl_update(forced=True)
     for ev in (True, False):
         ref.time_steps(10, need_energy=ev, need_virial=ev)
-        out[("plain", ev)] = ref.time_steps(STEPS, first_step=10, need_energy=ev, need_virial=ev)
+        out[("plain", ev)] = _timed(lambda: ref.time_steps(STEPS, first_step=10, need_energy=ev, need_virial=ev))
     ref.clear()
     ref.init(f.system(), refresh_interval=REFRESH, solvent=True)
     ref.nl_update(forced=True)
     ref.soft_init(f)
     for ev in (True, False):
         ref.soft_time_steps(10, need_energy=ev, need_virial=ev)
-        out[("soft_core", ev)] = ref.soft_time_steps(STEPS, first_step=10, need_energy=ev, need_virial=ev)
+        out[("soft_core", ev)] = _timed(
+            lambda: ref.soft_time_steps(STEPS, first_step=10, need_energy=ev, need_virial=ev))
     ref.clear()
     return out
 
