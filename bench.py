@@ -318,6 +318,7 @@ def batched_measure(systems_all, K, W, world, rank, local, dist, k_plain=None):
     ms = timed(B, K, energy_interval=100)
     launches = L.spgnb_launch_count() - launches0
     clocks = sampler.stop()
+    per_step, per_build = B.launch_counts()
     st = B.stats()
     atoms = sum(s.n for s in mine)
     e = B.energies()
@@ -352,7 +353,7 @@ def batched_measure(systems_all, K, W, world, rank, local, dist, k_plain=None):
             "plain": plain, "k_plain": k_plain, "tuned": tuned, "tuning": tuning,
             "rebuilds": st["rebuilds"] - st0["rebuilds"], "prunings": st["prunings"] - st0["prunings"],
             "overflow": st["overflow"], "energies_finite": bool(np.isfinite(e).all()), "clocks": clocks,
-            "launches": int(launches)}
+            "launches": int(launches), "build_launches": per_build}
 
 
 def batched_workload_name(m):
@@ -389,6 +390,7 @@ def run_batched(args, world, rank, local):
                 "rebuilds": m["rebuilds"], "prunings": m["prunings"], "overflow": m["overflow"],
                 "energies_finite": m["energies_finite"], "clocks": m["clocks"], "gpu_launches": m["launches"],
                 "gpu_launches_per_step": m["launches"] / K,
+                "build_launches_per_rebuild_step": m["build_launches"],
                 "e2e": {"value": m["value"], "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0,
                         "note": "state stays resident on the device between steps"}}
         print(json.dumps(line), flush=True)
@@ -761,7 +763,9 @@ def _main_box_extras(path, s, dev, stream, flush, world, rank, local, dist, args
                           "batched_over_plain": m["value"] / m["plain"],
                           "plain_how": f"each system alone from the same relaxed state, kernels launched step by "
                                        f"step, {m['k_plain']} steps each",
-                          "gpu_launches_per_step": m["launches"] / m["K"], "prune_buffer_autotuned": m["tuned"],
+                          "gpu_launches_per_step": m["launches"] / m["K"],
+                          "build_launches_per_rebuild_step": m["build_launches"],
+                          "prune_buffer_autotuned": m["tuned"],
                           "autotuned": m["tuning"],
                           "rebuilds": m["rebuilds"], "prunings": m["prunings"], "overflow": m["overflow"],
                           "energies_finite": m["energies_finite"], "clocks": m["clocks"]}

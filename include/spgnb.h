@@ -549,6 +549,10 @@ int spgnb_batch_get_tuning(spgnb_batch* b, spgnb_batch_tuning* in_use);
  * the prune buffer at most the one the lists were sized for.  ms_per_step
  * is ignored. */
 int spgnb_batch_set_tuning(spgnb_batch* b, const spgnb_batch_tuning* tuning);
+/* Kernel launches of a replayed step: those every step runs, and those of
+ * the list build, which run only on steps where some system rebuilds (the
+ * body of a conditional graph node). */
+int spgnb_batch_launch_counts(spgnb_batch* b, int* per_step, int* per_rebuild);
 /* The batch's CUDA stream (a cudaStream_t), for events around its work. */
 void* spgnb_batch_stream(spgnb_batch* b);
 int spgnb_batch_destroy(spgnb_batch* b);

@@ -82,7 +82,9 @@ struct spgnb_batch
     bool have_water = false;
     float ra = 0, rb = 0, rc = 0, mO = 0, mH = 0;
     cudaGraphExec_t g_plain = nullptr, g_energy = nullptr;
-    long long kernels_plain = 0, kernels_energy = 0;  // kernel launches inside each graph
+    // kernel launches inside each graph: those of every step, and those of
+    // the list builds, which run only on steps where some system rebuilds
+    long long kernels_plain = 0, kernels_energy = 0, kernels_build = 0;
     bool graph_tri = false;
     long long steps_done = 0;
     // launch configuration (spgnb_batch_autotune)
@@ -289,8 +291,80 @@ int batch_force(spgnb_batch* b, int mode, cudaStream_t s, const int* only = null
     return force_pipeline(in, s);
 }
 
+// Sets a graph's conditional from a device flag (non-zero: some system
+// rebuilds its list this step).
+__global__ void k_set_cond(cudaGraphConditionalHandle h, const int* __restrict__ any)
+{
+    cudaGraphSetConditional(h, *any != 0 ? 1u : 0u);
+}
+
+// During a graph capture, the list build of a step becomes the body of an
+// 'if' node on the device's rebuild flag, captured on a side stream, so a
+// step without a rebuild launches none of its kernels.  Outside a capture the
+// build runs inline.
+struct CondBuild : BuildBody
+{
+    cudaStream_t side = nullptr;
+    int status = SPGNB_OK;
+    bool open = false;
+    long long body_kernels = 0;
+    unsigned long long c0 = 0;
+    cudaStream_t body(cudaStream_t s, const int* d_any) override
+    {
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd);
+        if (e == cudaSuccess && cs != cudaStreamCaptureStatusActive) return s;
+        cudaGraphConditionalHandle h = 0;
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess)
+        {
+            k_set_cond<<<1, 1, 0, s>>>(h, d_any);
+            count_launch();
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd);
+        cudaGraphNodeParams p{};
+        cudaGraphNode_t node = nullptr;
+        if (e == cudaSuccess)
+        {
+            p.type = cudaGraphNodeTypeConditional;
+            p.conditional.handle = h;
+            p.conditional.type = cudaGraphCondTypeIf;
+            p.conditional.size = 1;
+            e = cudaGraphAddNode(&node, g, deps, nd, &p);
+        }
+        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+        if (e == cudaSuccess)
+            e = cudaStreamBeginCaptureToGraph(side, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                              cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess)
+        {
+            status = cuda_fail(e, "conditional list build");
+            return nullptr;
+        }
+        open = true;
+        c0 = launches_so_far();
+        return side;
+    }
+    int done() override
+    {
+        if (open)
+        {
+            body_kernels += (long long)(launches_so_far() - c0);
+            cudaGraph_t g = nullptr;
+            const cudaError_t e = cudaStreamEndCapture(side, &g);
+            open = false;
+            if (e != cudaSuccess && !status) status = cuda_fail(e, "conditional list build");
+        }
+        return status;
+    }
+};
+
 // One step: kick-drift, SETTLE, thermostat, list update, forces, counters.
-int batch_step(spgnb_batch* b, bool energy, cudaStream_t s)
+int batch_step(spgnb_batch* b, bool energy, cudaStream_t s, BuildBody* split = nullptr)
 {
     const float dt = b->opt.dt * kTimeUnitsPerPs;
     const int* atom_sys = b->nl->d_atom_sys;
@@ -316,7 +390,7 @@ int batch_step(spgnb_batch* b, bool energy, cudaStream_t s)
     }
     int st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num,
                             b->opt.refresh_interval > 0 ? kBuildInterval : kBuildSkin, s, b->d_steps,
-                            b->opt.refresh_interval, b->d_left);
+                            b->opt.refresh_interval, b->d_left, split);
     if (st) return st;
     if ((st = batch_force(b, energy ? 1 : 0, s))) return st;
     k_tick<<<(b->S + 255) / 256, 256, 0, s>>>(b->S, b->nl->d_live, b->d_left, b->d_steps);
@@ -351,15 +425,27 @@ void free_graphs(spgnb_batch* b)
 int capture(spgnb_batch* b, bool energy_last, cudaGraphExec_t* out, long long* kernels)
 {
     cudaGraph_t g = nullptr;
-    SPGNB_CUDA(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    CondBuild cb;
+    SPGNB_CUDA(cudaStreamCreateWithFlags(&cb.side, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess)
+    {
+        cudaStreamDestroy(cb.side);
+        return cuda_fail(e, "cudaStreamBeginCapture");
+    }
     int st = SPGNB_OK;
     const unsigned long long c0 = launches_so_far();
     for (int k = 0; k < b->opt.steps_per_graph && !st; k++)
-        st = batch_step(b, energy_last && k == b->opt.steps_per_graph - 1, b->stream);
-    // captured, not run: counted when the graph is launched
-    *kernels = (long long)(launches_so_far() - c0);
-    count_launches(-*kernels);
-    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+        st = batch_step(b, energy_last && k == b->opt.steps_per_graph - 1, b->stream, &cb);
+    // captured, not run: counted when the graph is launched (the build
+    // bodies, which run only on rebuild steps, apart)
+    const long long all = (long long)(launches_so_far() - c0);
+    count_launches(-all);
+    *kernels = all - cb.body_kernels;
+    b->kernels_build = cb.body_kernels / std::max(1, b->opt.steps_per_graph);
+    if (cb.open) cb.done();
+    e = cudaStreamEndCapture(b->stream, &g);
+    cudaStreamDestroy(cb.side);
     if (st)
     {
         if (g) cudaGraphDestroy(g);
@@ -1294,6 +1380,16 @@ int spgnb_batch_set_tuning(spgnb_batch* b, const spgnb_batch_tuning* t)
     b->opt.steps_per_graph = t->steps_per_graph;
     free_graphs(b);
     return nl_prune_all(b->nl, b->stream);
+}
+
+int spgnb_batch_launch_counts(spgnb_batch* b, int* per_step, int* per_rebuild)
+{
+    if (!b) return fail(SPGNB_E_ARG, "spgnb_batch_launch_counts: NULL handle");
+    int st = ensure_graphs(b);
+    if (st) return st;
+    if (per_step) *per_step = (int)(b->kernels_plain / std::max(1, b->opt.steps_per_graph));
+    if (per_rebuild) *per_rebuild = (int)b->kernels_build;
+    return SPGNB_OK;
 }
 
 int spgnb_batch_get_tuning(spgnb_batch* b, spgnb_batch_tuning* out)

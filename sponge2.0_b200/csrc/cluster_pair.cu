@@ -308,9 +308,11 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
 // {delta + displacement, q} and aux record {22-bit centre, LJ type, global
 // index} load once for all of the cluster's atoms the lane holds, and
 //   dr = (c_J - c_I) * cell / 2^22 + p_j - p_i
-// is formed with the exact integer centre difference.  The atoms are held in
-// registers as packed pairs, so every instruction of the pair function
-// serves two pairs (FP32x2).  The LJ coefficients of a pair of cluster atoms
+// is formed with the exact integer centre difference.  The cluster's atoms
+// are staged in shared memory as packed pairs, so every instruction of the
+// pair function serves two pairs (FP32x2) and the registers stay few enough
+// for 6 resident blocks per SM (5 with energy/virial totals, 3 with per-atom
+// outputs).  The LJ coefficients of a pair of cluster atoms
 // against the partner's type come as one float4 {-A_a, -A_b, B_a, B_b} of
 // the T^3 table.  Partner records are copied into shared memory by
 // asynchronous copies (cp.async) one iteration ahead of their use, list words
@@ -331,7 +333,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
 // partner-owned sums go to the partner's int64 staging, 8 atomic adds; the
 // finishing pass turns the staging into the per-atom arrays and totals.
 template <int MODE, int FIT, bool TRI>
-__global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
+__global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : (MODE == 1 ? 5 : 6))
     k_pair8(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys, int n_clusters,
             int list_cap, const int* __restrict__ cl_sys, const int* __restrict__ lcount,
             const unsigned* __restrict__ words, const int4* __restrict__ cl_q, const float4* __restrict__ pos,
@@ -342,12 +344,11 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
     constexpr bool EN = MODE >= 1;
     constexpr bool PA = MODE >= 2;
     constexpr int NP = 4;        // the cluster's 8 atoms as packed pairs
-    constexpr bool ISM = PA;     // the cluster's atoms in shared memory instead of registers
     __shared__ long long red[kPairWarps][8];  // per-warp fixed-point totals
     __shared__ int is_last;
     extern __shared__ float4 rows_all[];      // per warp: 4 x max_types coefficient rows
     __shared__ unsigned wring_all[kPairWarps][3][32];       // per warp: list words in flight
-    // per warp, when ISM: the cluster's atom pairs {-x, -y | -z, q} and global indices
+    // per warp: the cluster's atom pairs {-x, -y | -z, q} and global indices
     __shared__ float4 iat_all[kPairWarps][4][2];
     __shared__ int2 igid_all[kPairWarps][4];
     __shared__ __align__(16) float4 jpos_all[kPairWarps][2][32];  // partner offsets and charges in flight
@@ -395,40 +396,17 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
         const int slot0 = D.cl_begin * kClusterSize;
         const int4 ci = cl_q[c];
         const int nt = P.n_types;
-        // this lane's cluster atoms, negated, as packed pairs
-        // (the per-atom mode keeps them in shared memory instead: its owned
-        // sums already take 64 registers)
-        float2 npx[ISM ? 1 : NP], npy[ISM ? 1 : NP], npz[ISM ? 1 : NP], qi[ISM ? 1 : NP];
-        int gi[ISM ? 1 : 2 * NP];
-        if (ISM)
+        // the cluster's atoms, negated, as packed pairs
+        __syncwarp();  // the previous cluster's atoms are no longer read
+        if (lane < 4)
         {
-            __syncwarp();  // the previous cluster's atoms are no longer read
-            if (lane < 4)
-            {
-                const int a = 2 * lane;
-                const float4 u0 = pos[s0 + a], u1 = pos[s0 + a + 1];
-                iat[lane][0] = make_float4(-u0.x, -u1.x, -u0.y, -u1.y);
-                iat[lane][1] = make_float4(-u0.z, -u1.z, u0.w, u1.w);
-                igid[lane] = make_int2(aux[s0 + a].w, aux[s0 + a + 1].w);
-            }
-            __syncwarp();
+            const int a = 2 * lane;
+            const float4 u0 = pos[s0 + a], u1 = pos[s0 + a + 1];
+            iat[lane][0] = make_float4(-u0.x, -u1.x, -u0.y, -u1.y);
+            iat[lane][1] = make_float4(-u0.z, -u1.z, u0.w, u1.w);
+            igid[lane] = make_int2(aux[s0 + a].w, aux[s0 + a + 1].w);
         }
-        else
-        {
-#pragma unroll
-            for (int p = 0; p < NP; p++)
-            {
-                const int a = 2 * p;
-                const float4 u0 = pos[s0 + a], u1 = pos[s0 + a + 1];
-                const int4 x0 = aux[s0 + a], x1 = aux[s0 + a + 1];
-                npx[p] = make_float2(-u0.x, -u1.x);
-                npy[p] = make_float2(-u0.y, -u1.y);
-                npz[p] = make_float2(-u0.z, -u1.z);
-                qi[p] = make_float2(u0.w, u1.w);
-                gi[2 * p] = x0.w;
-                gi[2 * p + 1] = x1.w;
-            }
-        }
+        __syncwarp();
         // the coefficient rows of the cluster's four atom pairs against every
         // partner type, {-A_a, -A_b, B_a, B_b}, staged in shared memory
         {
@@ -516,25 +494,9 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
 #pragma unroll
             for (int p = 0; p < NP; p++)
             {
-                float2 pnx, pny, pnz, pq;
-                int2 pg;
-                if (ISM)
-                {
-                    const float4 A = iat[p][0], B = iat[p][1];
-                    pnx = make_float2(A.x, A.y);
-                    pny = make_float2(A.z, A.w);
-                    pnz = make_float2(B.x, B.y);
-                    pq = make_float2(B.z, B.w);
-                    pg = igid[p];
-                }
-                else
-                {
-                    pnx = npx[p];
-                    pny = npy[p];
-                    pnz = npz[p];
-                    pq = qi[p];
-                    pg = make_int2(gi[2 * p], gi[2 * p + 1]);
-                }
+                const float4 A = iat[p][0], B = iat[p][1];
+                const float2 pnx = make_float2(A.x, A.y), pny = make_float2(A.z, A.w), pnz = make_float2(B.x, B.y),
+                             pq = make_float2(B.z, B.w);
                 float2 dx = __fadd2_rn(f2(sx), pnx), dy = __fadd2_rn(f2(sy2), pny), dz = __fadd2_rn(f2(sz), pnz);
                 if (any_img && img)
                 {
@@ -585,6 +547,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : 4)
                     // the pair's owner is the lower global index: this lane's
                     // atom (kept over the list) or the partner (summed over
                     // the word's atoms)
+                    const int2 pg = igid[p];
                     const float2 wi = make_float2(pg.x < gj ? 1.0f : 0.0f, pg.y < gj ? 1.0f : 0.0f);
                     const float2 v[8] = {make_float2(inA ? elj.x : 0.0f, inB ? elj.y : 0.0f),
                                          make_float2(inA ? ec.x : 0.0f, inB ? ec.y : 0.0f),

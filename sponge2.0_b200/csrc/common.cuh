@@ -558,9 +558,22 @@ enum BuildHow
 // aux: kBuildInterval - per-system steps done; kBuildPreset - per-system
 // flags of the systems to rebuild.  active (optional): per system, 0 = frozen
 // (no forced or interval rebuild).
+// Optional split of a queued build: the decision (which systems rebuild)
+// goes to the caller's stream; the build itself (binning to the finish) to
+// the stream body() returns, given the device flag that is non-zero when
+// some system rebuilds.  A graph capture makes that part the body of a
+// conditional node, so steps without a rebuild launch none of it; done()
+// closes the body and returns its status.  body() returns null on an
+// error, which done() then reports.
+struct BuildBody
+{
+    virtual cudaStream_t body(cudaStream_t s, const int* d_any) = 0;
+    virtual int done() = 0;
+    virtual ~BuildBody() = default;
+};
 int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
                    const int* ex_list, const int* ex_num, int how, cudaStream_t s, const int* d_aux = nullptr,
-                   int interval = 0, const int* d_active = nullptr);
+                   int interval = 0, const int* d_active = nullptr, BuildBody* split = nullptr);
 int nl_regrow(spgnb_nl* nl, int flags);
 int nl_set_prune_rc(spgnb_nl* nl, float rc, cudaStream_t s);
 size_t nl_device_bytes(const spgnb_nl* nl);

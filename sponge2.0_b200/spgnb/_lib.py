@@ -36,6 +36,7 @@ EXPORTED = [
     "spgnb_lj_soft_destroy", "spgnb_solvent_create_soft",
     "spgnb_batch_default_options", "spgnb_batch_create", "spgnb_batch_run", "spgnb_batch_energies",
     "spgnb_batch_download", "spgnb_batch_stats", "spgnb_batch_autotune", "spgnb_batch_get_tuning", "spgnb_batch_set_tuning",
+    "spgnb_batch_launch_counts",
     "spgnb_batch_stream",
     "spgnb_batch_check_overflow", "spgnb_batch_set_thermostat",
     "spgnb_batch_destroy",
@@ -148,6 +149,7 @@ def lib():
     L.spgnb_batch_autotune.argtypes = [vp, i, C.POINTER(C.c_float)]
     L.spgnb_batch_get_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
     L.spgnb_batch_set_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
+    L.spgnb_batch_launch_counts.argtypes = [vp, C.POINTER(i), C.POINTER(i)]
     L.spgnb_batch_check_overflow.argtypes = [vp, C.POINTER(i)]
     L.spgnb_batch_set_thermostat.argtypes = [vp, f, f]
     L.spgnb_batch_stream.argtypes = [vp]

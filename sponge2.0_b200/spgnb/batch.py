@@ -126,6 +126,12 @@ class _Common:
                 "prune_blocks_per_sm": t.prune_blocks_per_sm, "steps_per_graph": t.steps_per_graph,
                 "ms_per_step": t.ms_per_step}
 
+    def launch_counts(self):
+        """(kernels every replayed step launches, kernels of a step's list build)."""
+        a, b = C.c_int(), C.c_int()
+        check(lib().spgnb_batch_launch_counts(self.handle, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def set_tuning(self, prune_buffer, pair_blocks_per_sm, prune_blocks_per_sm, steps_per_graph):
         t = BatchTuning(float(prune_buffer), int(pair_blocks_per_sm), int(prune_blocks_per_sm),
                         int(steps_per_graph), 0.0)

@@ -93,13 +93,18 @@ def test_rigid_waters_stay_rigid(torch_cuda):
 
 
 def test_launch_configuration_changes_no_result(torch_cuda):
-    """The autotuner's knobs that keep the lists (the force and pruning
-    kernels' grids, the steps per graph) change no bit of the results."""
+    """The autotuner's knobs other than the prune buffer (the force and
+    pruning kernels' grids, the steps per graph) change no bit of the
+    results.  Applying a tuning re-prunes the lists, and the list words'
+    order decides the FP32 partial sums, so both batches apply one at the
+    same step."""
     from spgnb.batch import Batch
     systems = _small_batch(2, seed=15)
     a = Batch(systems, steps_per_graph=10)
     b = Batch(systems, steps_per_graph=10)
-    b.set_tuning(a.tuning()["prune_buffer"], 2, 3, 5)
+    buf = a.tuning()["prune_buffer"]
+    a.set_tuning(buf, 0, 5, 10)
+    b.set_tuning(buf, 2, 3, 5)
     assert b.tuning()["pair_blocks_per_sm"] == 2 and b.tuning()["steps_per_graph"] == 5
     a.run(30, energy_interval=10)
     b.run(30, energy_interval=10)

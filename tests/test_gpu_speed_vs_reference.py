@@ -7,8 +7,9 @@ Main_Calculate_Force) and the alchemical path (list update + LJ_SOFT_CORE +
 the solvent module) with a 40-atom perturbed ligand.  Both sides rebuild the
 list every 20 steps; each path is timed with energy and virial (per-atom
 arrays) every step and with forces only, SPONGE's step between energy
-outputs.  Prints one JSON line per path (run with -s); fails only if this
-library is clearly slower than the reference kernels."""
+outputs.  Prints one JSON line per path (run with -s); fails when force-only
+steps are not at least 1.3x the reference kernels' speed, or energy steps
+fall behind them."""
 import json
 import os
 
@@ -20,7 +21,10 @@ pytestmark = pytest.mark.gpu
 
 REF_CUDA = os.path.join(ROOT, "oracle", "_ref", "libspgref_cuda.so")
 REF_SHIM = os.path.join(ROOT, "oracle", "_ref", "libspgref_shim.so")
-STEPS = 300
+# steps per timed loop; a launch-list capture of this test under a profiler
+# sets fewer, and then only prints (serialised launches time nothing)
+STEPS = int(os.environ.get("SPGNB_SPEED_STEPS", "300"))
+UNDER_PROFILER = "SPGNB_SPEED_STEPS" in os.environ
 REFRESH = 20
 
 
@@ -73,5 +77,10 @@ def test_plain_and_soft_core_paths_vs_reference_kernels(torch_cuda):
                 "speedup": theirs[key] / ours[key]}
         speedup[key] = line["speedup"]
         print(json.dumps(line))
-    for key, v in speedup.items():
-        assert v > 0.8, (key, v)
+    if UNDER_PROFILER:
+        return
+    for (name, ev), v in speedup.items():
+        # force-only steps (SPONGE's step between energy outputs) clearly
+        # ahead (measured 1.55x); energy steps with per-atom outputs not
+        # behind (measured 1.06x; host-clock loops on a shared box)
+        assert v >= (0.97 if ev else 1.3), (name, ev, v)
