@@ -102,6 +102,9 @@ def parse():
     p.add_argument("--profile-path", choices=["plain", "soft_core", "graph_resident"], default="plain",
                    help="with --profile: plain (the module API, default); soft_core (the same box with a 40-atom "
                         "perturbed ligand); graph_resident (the box as dynamics in captured graphs)")
+    p.add_argument("--step-launches", action="store_true",
+                   help="with --profile-path graph_resident: launch the kernels step by step instead of replaying "
+                        "graphs (a profiler's per-kernel list cannot look inside graphs with conditional nodes)")
     p.add_argument("--workload", choices=["mixed96k", "water1m", "batched", "served"], default="mixed96k",
                    help="mixed96k: the plain path on the 96k box (default); water1m: the plain path on the "
                         "1M-atom water box, rc 12; batched: 256 systems, batched engine against the plain "
@@ -854,6 +857,15 @@ def run_profile_path(args, s, dev):
         b.check_overflow()
         b.set_thermostat(0.1, 300.0)
         b.autotune(10)
+        if args.step_launches:
+            # the same relaxed state and prune buffer, launched step by step
+            import copy
+            t = b.tuning()
+            s2 = copy.copy(s)
+            s2.crd, s2.vel, _ = b.download(0)
+            b.close()
+            b = Batch([s2], refresh_interval=REFRESH_INTERVAL, thermostat_tau=0.1, temperature=300.0,
+                      prune_buffer=t["prune_buffer"], use_graphs=0)
         run = lambda first, n: b.run(n, 100)
     run(0, W)
     torch.cuda.synchronize()
