@@ -250,10 +250,14 @@ struct spgnb_nl
     float prune_rc = 0;    // cutoff the pruned lists are made for
     bool built = false;
     int local_atoms = 0;
-    // neighbour tables two-sided (every neighbour cluster) for the exports
-    // and the soft-core kernel, or one-sided (J >= I) when only the pruned
-    // half list reads them; the last build's kind, and its exclusion arrays
+    // neighbour tables two-sided (every neighbour cluster) for the exports,
+    // or one-sided (J >= I) when only the pruned half list reads them, except
+    // for the clusters holding an atom flagged in two_sided_atoms (the
+    // soft-core kernel's perturbed atoms); what the last build made, and its
+    // exclusion arrays
     mutable bool sym_tables = false, sym_built = false;
+    mutable const unsigned char* two_sided_atoms = nullptr;
+    mutable const unsigned char* two_sided_built = nullptr;
     const int *ex_start_last = nullptr, *ex_list_last = nullptr, *ex_num_last = nullptr;
 
     std::vector<spgnb::SysDesc> h_desc;  // host copy of d_sys
@@ -544,10 +548,14 @@ size_t nl_admit_upload_bytes(const SysHost& sh, size_t n_runs);
 int nl_retire(spgnb_nl* nl, int id, cudaStream_t s);
 // Every live system re-prunes before the next force evaluation.
 int nl_prune_all(spgnb_nl* nl, cudaStream_t s);
-// Makes this and later builds' neighbour tables two-sided: re-runs the last
-// build's search (same clusters and build coordinates, so the same list) when
-// its tables are one-sided.
-int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s);
+// Makes the last build's neighbour tables two-sided, and with persist the
+// later builds' too: re-runs the last build's search (same clusters and
+// build coordinates, so the same list) when its tables are one-sided.
+int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s, bool persist = true);
+// Makes the tables of the clusters holding a flagged atom (per local atom,
+// non-zero) two-sided, in the last build (re-searched if needed) and the
+// later ones.
+int nl_two_sided_atoms(const spgnb_nl* nl, const unsigned char* d_flags, cudaStream_t s);
 enum BuildHow
 {
     kBuildSkin = 0,

@@ -11,13 +11,13 @@ namespace
 {
 
 // Counts listed pairs (each once) and those inside the cutoff at the given
-// coordinates, from the neighbour tables, two-sided (sym) or one-sided.
+// coordinates, from the neighbour tables (one- or two-sided).
 __global__ void k_count_pairs(const int* __restrict__ counters, int clusters_cap, int table_cap,
                               const int* __restrict__ tcount, const float4* __restrict__ tab,
                               const uint2* __restrict__ tmask, const int* __restrict__ slot_atom,
                               const float4* __restrict__ x0, const float4* __restrict__ d0,
                               const float3* __restrict__ crd, Cell cell, Cell rcell, float rc2,
-                              unsigned long long* out, int sym)
+                              unsigned long long* out)
 {
     const int lane = threadIdx.x & 31;
     const int nc = clusters_cap;
@@ -53,9 +53,11 @@ __global__ void k_count_pairs(const int* __restrict__ counters, int clusters_cap
                 const int k = __ffsll((long long)m) - 1;
                 m &= m - 1;
                 const int si = c * kClusterSize + (k >> 3), sj = base + (k & 7);
-                // a two-sided table holds each pair on both sides, a one-sided
-                // one only within a cluster; count each pair once
-                if ((sym || (sj >> 3) == c) && !(__float_as_int(x0[si].w) < __float_as_int(x0[sj].w))) continue;
+                // every pair once: from the lower cluster's table (a
+                // two-sided table also holds the lower clusters), and
+                // within a cluster from its lower-index atom
+                const int J = sj >> 3;
+                if (J < c || (J == c && !(__float_as_int(x0[si].w) < __float_as_int(x0[sj].w)))) continue;
                 const float3 pi = pos(si), pj = pos(sj);
                 float dx = e.x + pj.x - pi.x, dy = e.y + pj.y - pi.y, dz = e.z + pj.z - pi.z;
                 const float sx = rintf(dx * rcell.a11 + dy * rcell.a21 + dz * rcell.a31);
@@ -127,7 +129,7 @@ int spgnb_nl_count_pairs(spgnb_nl* nl, const spgnb_vector* d_crd, spgnb_ltmatrix
     k_count_pairs<<<num_sms() * 8, 128, 0, s>>>(nl->d_counters, nl->clusters_cap, nl->table_cap, nl->d_tcount,
                                                 nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_d0,
                                                 (const float3*)d_crd, make_cell(cell), make_cell(rcell),
-                                                cutoff * cutoff, d, nl->sym_built ? 1 : 0);
+                                                cutoff * cutoff, d);
     cudaError_t e = cudaGetLastError();
     unsigned long long h[2] = {0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, 16, cudaMemcpyDeviceToHost, s);

@@ -414,7 +414,8 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
              const int2* __restrict__ slot_ex,
              const int* __restrict__ ex_start, const int* __restrict__ ex_list, const int* __restrict__ ex_num,
              int* __restrict__ tcount, float4* __restrict__ tab, uint2* __restrict__ tmask,
-             int* __restrict__ slot_count, int* counters, const int* __restrict__ go, int half)
+             int* __restrict__ slot_count, int* counters, const int* __restrict__ go, int half,
+             const int* __restrict__ slot_atom, const unsigned char* __restrict__ two_sided_atoms)
 {
     if (go && *go == 0) return;
     __shared__ float4 stage_t[kSearchWarps][kChunk];
@@ -439,6 +440,13 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
         const float ri = __uint_as_float(ui.w);
         const float4 hc = cl_c[c];
         const float band = kBorderBand * p.cs2;
+        // one-sided table, unless the cluster holds an atom flagged for two sides
+        bool one_sided = half != 0;
+        if (one_sided && two_sided_atoms)
+        {
+            const int sa = slot_atom[c * kClusterSize + (lane & 7)];
+            one_sided = !__any_sync(0xffffffffu, sa >= 0 && two_sided_atoms[sa]);
+        }
         // the two own atoms this lane tests (rounds h = 0, 1)
         int ga[2];
         float3 xa[2], da[2];
@@ -480,7 +488,7 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
             {
                 const int cj = b0 + lane;
                 bool ok = false;
-                if (cj < b1 && (!half || cj >= c))
+                if (cj < b1 && (!one_sided || cj >= c))
                 {
                     const uint4 uj = cl_u[cj];
                     const float3 f = frac_delta(ui, uj);
@@ -1515,9 +1523,10 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
         nl->d_sys, ccap, nl->table_cap, nl->d_need, nl->d_ncl, nl->d_run_start, nl->d_runs, nl->d_cell_cl,
         nl->d_cl_cell, nl->d_cl_sys, nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex,
         ex_start, ex_list, ex_num, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_counters,
-        nl->d_counters + kCntNeed, nl->sym_tables ? 0 : 1);
+        nl->d_counters + kCntNeed, nl->sym_tables ? 0 : 1, nl->d_slot_atom, nl->two_sided_atoms);
     SPGNB_CHECK_LAUNCH("k_search");
     nl->sym_built = nl->sym_tables;
+    nl->two_sided_built = nl->sym_tables ? nullptr : nl->two_sided_atoms;
     nl->ex_start_last = ex_start;
     nl->ex_list_last = ex_list;
     nl->ex_num_last = ex_num;
@@ -1785,10 +1794,11 @@ int spgnb_nl_copy_atom_groups(spgnb_nl* nl, int* h_counts, int* h_lists, long lo
 namespace spgnb
 {
 
-int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s)
+// Re-runs the search of the last build (same clusters and build
+// coordinates) with two-sided tables everywhere (flags null, half 0) or for
+// the flagged atoms' clusters.
+int research_last_build(const spgnb_nl* nl, cudaStream_t s, int half, const unsigned char* flags)
 {
-    nl->sym_tables = true;
-    if (!nl->built || nl->sym_built) return SPGNB_OK;
     k_sym_begin<<<1, 1, 0, s>>>(nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_sym_begin");
     const int ccap = nl->clusters_cap;
@@ -1799,9 +1809,29 @@ int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s)
         nl->d_sys, ccap, nl->table_cap, nl->d_live, nl->d_ncl, nl->d_run_start, nl->d_runs, nl->d_cell_cl,
         nl->d_cl_cell, nl->d_cl_sys, nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex,
         nl->ex_start_last, nl->ex_list_last, nl->ex_num_last, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_count,
-        nl->d_counters, nullptr, 0);
+        nl->d_counters, nullptr, half, nl->d_slot_atom, flags);
     SPGNB_CHECK_LAUNCH("k_search");
+    return SPGNB_OK;
+}
+
+int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s, bool persist)
+{
+    if (persist) nl->sym_tables = true;
+    if (!nl->built || nl->sym_built) return SPGNB_OK;
+    const int st = research_last_build(nl, s, 0, nullptr);
+    if (st) return st;
     nl->sym_built = true;
+    nl->two_sided_built = nullptr;
+    return SPGNB_OK;
+}
+
+int nl_two_sided_atoms(const spgnb_nl* nl, const unsigned char* d_flags, cudaStream_t s)
+{
+    nl->two_sided_atoms = d_flags;
+    if (!nl->built || nl->sym_built || nl->two_sided_built == d_flags) return SPGNB_OK;
+    const int st = research_last_build(nl, s, 1, d_flags);
+    if (st) return st;
+    nl->two_sided_built = d_flags;
     return SPGNB_OK;
 }
 

@@ -676,7 +676,7 @@ int spgnb_lj_soft_pme_direct_force(spgnb_lj_soft* lj, int atom_numbers, int loca
     if (st) return st;
     cudaStream_t s = stream();
     // the perturbed atoms' pairs come from their clusters' two-sided tables
-    if ((st = nl_symmetrize(nl, s))) return st;
+    if ((st = nl_two_sided_atoms(nl, lj->d_flag, s))) return st;
     const int n = local_atom_numbers;
     k_mask_charge<<<(n + 255) / 256, 256, 0, s>>>(n, d_charge, lj->d_flag, lj->d_masked_q);
     SPGNB_CHECK_LAUNCH("k_mask_charge");
@@ -733,7 +733,10 @@ int spgnb_lj_soft_partial_h_partial_lambda(spgnb_lj_soft* lj, int solvent_number
     int st = check_list(lj, nl, lj->local_atoms, who);
     if (st) return st;
     cudaStream_t s = stream();
-    if ((st = nl_symmetrize(nl, s))) return st;
+    // the atoms whose pairs it sums (the perturbed ones, and with charge
+    // perturbation every atom whose charge changes) read their clusters'
+    // tables: two-sided ones for this call (a rare one: output steps)
+    if ((st = nl_symmetrize(nl, s, false))) return st;
     SPGNB_CUDA(cudaMemsetAsync(lj->d_dh, 0, 2 * sizeof(long long), s));
     const SoftConst k = soft_const(lj, pme_beta);
     const float3* crd = (const float3*)d_crd;
