@@ -211,18 +211,29 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
                     mybuf[k++] = make_uint2(base + b, (unsigned)lane | (am << 5));
                 }
             __syncwarp();
+            // a lane's candidate of an iteration: its record and own-atom
+            // bits; the partner's position is loaded an iteration ahead
+            auto candidate = [&](int q, uint2& wv, unsigned& am, float4& pj) {
+                wv = mybuf[q < total ? q : 0];
+                am = q < total ? (wv.y >> 5) & 0xffu : 0u;
+                pj = make_float4(0, 0, 0, 0);
+                if (am) pj = pos[wv.x & 0x7fffffffu];
+            };
+            uint2 wv_next;
+            unsigned am_next;
+            float4 pj_next;
+            candidate(lane, wv_next, am_next, pj_next);
             for (int q0 = 0; q0 < total; q0 += 32)
             {
-                const int q = q0 + lane;
-                const uint2 wv = mybuf[q < total ? q : 0];
+                const uint2 wv = wv_next;
+                const unsigned am = am_next;
+                const float4 pj = pj_next;
+                if (q0 + 32 < total) candidate(q0 + 32 + lane, wv_next, am_next, pj_next);
                 // the element's centre difference, staged by the lane that read it
                 const float4 es = ent[wv.y & 31u];
                 const float ex = es.x, ey = es.y, ez = es.z;
-                const unsigned am = q < total ? (wv.y >> 5) & 0xffu : 0u;
                 const int js = (int)(wv.x & 0x7fffffffu);
                 const bool img = (wv.x & 0x80000000u) != 0;
-                float4 pj = make_float4(0, 0, 0, 0);
-                if (am) pj = pos[js];
                 // bit a: own atom a lies within the pruning radius of the
                 // partner.  All eight are tested without branches; the
                 // minimum-image path (small boxes) only when a lane needs it.

@@ -14,7 +14,9 @@ and Maxwell velocities (300 K, seeded) by
   (main.cpp:622-710).
 
 Compared: the LJ and direct Coulomb energies at every step, the positions and
-velocities after the run, and the rigid geometry.  The two integrate the same
+velocities after the run, and the rigid geometry.  A second test follows the
+reference's own trajectory for 1,000 steps and compares the two force paths on
+its states every 10 steps.  The two integrate the same
 equations in FP32 with different summation orders, so they drift apart
 slowly; the bounds are set well above that drift and far below any error in
 the forces, the constraints or the step order.
@@ -24,7 +26,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import ROOT
+from conftest import ROOT, rel_rms
 
 pytestmark = pytest.mark.gpu
 
@@ -121,3 +123,51 @@ def test_water6480_nve_trajectory_vs_reference(torch_cuda, oracle):
     # both keep the waters rigid to FP32 precision
     assert bond_ours <= 1e-4 and hh_ours <= 1e-4
     assert bond_ref <= 1e-4 and hh_ref <= 1e-4
+
+
+@pytest.mark.skipif(not os.path.exists(REF_CUDA), reason="reference CUDA harness not built")
+def test_water6480_force_energy_virial_along_1000_reference_steps(torch_cuda, oracle):
+    """1,000 NVE steps of the reference's own force path, leap-frog and
+    SETTLE from the Maxwell start; every 10 steps this library and the
+    reference's kernels evaluate forces, energies and virial on the
+    reference's state (each with a list built there): forces within 1e-5
+    relative RMS of each other, the totals within 1e-5 of the terms' size,
+    and every 20th state against the FP64 pair sum."""
+    import copy
+    import torch
+    import oracle as O
+    from spgnb import systems as S
+    from spgnb.engine import PlainPath
+    s = S.water_box_6480()
+    ref = O.Reference(gpu=True)
+    ref.init(s, refresh_interval=20, solvent=True)
+    ref.nl_update(forced=True)
+    assert ref.md_init(dt=0.002) == s.n_waters
+    p = PlainPath(s, refresh_interval=20)
+    crd, vel = s.crd, s.vel
+    worst = {"force": 0.0, "e": 0.0, "virial": 0.0, "fp64": 0.0}
+    for k in range(100):
+        crd, vel, _ = ref.md_run(crd, vel, 10, first_step=10 * k)
+        ref.nl_update(crd, step=10 * (k + 1), forced=True)
+        r = ref.force(crd)
+        p.crd.copy_(torch.from_numpy(np.ascontiguousarray(crd, np.float32)))
+        p.update(0, forced=True)
+        f = p.force(need_energy=True, need_virial=True).cpu().numpy()
+        tot = p.lj.totals()
+        e_lj, e_c = float(r["atom_lj"].astype(np.float64).sum()), float(r["atom_direct"].astype(np.float64).sum())
+        vir = r["atom_virial"].astype(np.float64).sum(0)
+        scale = abs(e_lj) + abs(e_c)
+        worst["force"] = max(worst["force"], rel_rms(f, r["frc"]))
+        worst["e"] = max(worst["e"], abs(tot[0] - e_lj) / scale, abs(tot[1] - e_c) / scale)
+        worst["virial"] = max(worst["virial"], float(np.abs(tot[2:] - vir).max() / np.abs(vir).max()))
+        if k % 20 == 19:
+            st = copy.copy(s)
+            st.crd = np.ascontiguousarray(crd, np.float32)
+            worst["fp64"] = max(worst["fp64"], rel_rms(f, oracle.direct_sum(st)["frc"]))
+    ref.clear()
+    print({"case": "water-6480 along 1000 reference steps", **worst})
+    assert worst["force"] <= 1e-5 and worst["fp64"] <= 1e-5
+    assert worst["e"] <= 1e-5 and worst["virial"] <= 1e-5
+    # the states stayed physical: rigid waters
+    bond, hh = _rigid_errors(crd, s)
+    assert bond <= 1e-4 and hh <= 1e-4
