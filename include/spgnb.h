@@ -455,12 +455,15 @@ int spgnb_lj_pme_direct_force_noalloc(int local_atom_numbers, int solvent_number
  * counterpart: the reference runs one system per process).  Every system
  * keeps its own box, cutoff, skin, Ewald beta, exclusions and rigid waters,
  * and either the batch's LJ type table or one of its own (as each SPONGE
- * process reads its own LJ_in_file, Lennard_Jones_force.cpp:186-231).  One step = leap-frog velocity Verlet (kick
- * with F(t), drift, SETTLE for the rigid waters) + the neighbour-list
- * update (per system, by the skin trigger of NEIGHBOR_LIST::Update) + LJ and
- * PME direct-space forces over all systems in one kernel launch.  Steps are
- * replayed from captured CUDA graphs.  A system's results do not depend on the
- * other systems in the batch. */
+ * process reads its own LJ_in_file, Lennard_Jones_force.cpp:186-231).  One
+ * step = one kernel for leap-frog (kick with F(t), drift), SETTLE for the
+ * rigid waters, a Berendsen thermostat when on (the velocity scale from the
+ * previous step's kinetic energy), the slot records of the force pass and
+ * the rebuild decision (refresh interval, or the skin trigger of
+ * NEIGHBOR_LIST::Update, per system); the list build and the pruning when
+ * some system needs them; the LJ and PME direct-space forces of all systems
+ * in one kernel.  Steps are replayed from captured CUDA graphs.  A system's
+ * results do not depend on the other systems in the batch. */
 typedef struct spgnb_batch spgnb_batch;
 
 typedef struct
@@ -549,9 +552,11 @@ int spgnb_batch_get_tuning(spgnb_batch* b, spgnb_batch_tuning* in_use);
  * the prune buffer at most the one the lists were sized for.  ms_per_step
  * is ignored. */
 int spgnb_batch_set_tuning(spgnb_batch* b, const spgnb_batch_tuning* tuning);
-/* Kernel launches of a replayed step: those every step runs, and those of
- * the list build, which run only on steps where some system rebuilds (the
- * body of a conditional graph node). */
+/* Kernel launches of a replayed step: those every step runs (the step
+ * kernel and the pair kernel), and those of the list build and the pruning
+ * that follows it, the bodies of conditional graph nodes, which run only on
+ * steps where some system rebuilds (the pruning alone, one kernel, on steps
+ * where some system prunes). */
 int spgnb_batch_launch_counts(spgnb_batch* b, int* per_step, int* per_rebuild);
 /* The batch's CUDA stream (a cudaStream_t), for events around its work. */
 void* spgnb_batch_stream(spgnb_batch* b);

@@ -61,6 +61,7 @@ struct spgnb_batch
     int* d_ex_num = nullptr;
     int* d_ex_list = nullptr;
     int* d_waters = nullptr;  // oxygen of each rigid water, -1 for a free entry
+    unsigned char* d_in_water = nullptr;  // per atom: moved with its water (SETTLE)
     // force field
     int T = 0;                    // types of the batch's table
     int max_T = 0;                // most types of any table (the force kernel's shared rows)
@@ -71,6 +72,9 @@ struct spgnb_batch
     bool fit = true;                  // the rational fits (every admitted system inside their range)
     long long* d_totals = nullptr;    // 8 per system id
     long long* d_kin = nullptr;       // per system: sum of m v^2, fixed point
+    float* d_lambda = nullptr;        // per system: the thermostat's velocity scale for the next step
+    int* d_skin_hit = nullptr;        // per system: an atom moved past the skin this step
+    int* d_done = nullptr;            // blocks of the step kernel finished
     float* d_ndof = nullptr;          // per system: degrees of freedom
     int* d_steps = nullptr;           // per system: steps done
     int* d_left = nullptr;            // per system: steps left (-1 unlimited, 0 stopped or parked)
@@ -99,24 +103,6 @@ namespace spgnb
 namespace
 {
 
-__global__ void k_leapfrog(int n, const int* __restrict__ atom_sys, const int* __restrict__ left,
-                           float3* __restrict__ crd, float3* __restrict__ vel, const float3* __restrict__ frc,
-                           const float* __restrict__ inv_mass, float3* __restrict__ crd_old, float dt)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || left[atom_sys[i]] == 0) return;  // parked, or its steps are done
-    const float3 x = crd[i];
-    const float3 f = frc[i];
-    const float im = inv_mass[i] * dt;
-    float3 v = vel[i];
-    v.x = fmaf(f.x, im, v.x);
-    v.y = fmaf(f.y, im, v.y);
-    v.z = fmaf(f.z, im, v.z);
-    crd_old[i] = x;
-    vel[i] = v;
-    crd[i] = make_float3(fmaf(v.x, dt, x.x), fmaf(v.y, dt, x.y), fmaf(v.z, dt, x.z));
-}
-
 __device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
 __device__ __forceinline__ float3 add3(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
 __device__ __forceinline__ float3 mul3(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
@@ -127,24 +113,21 @@ __device__ __forceinline__ float3 cross3(float3 a, float3 b)
 }
 __device__ __forceinline__ float3 unit3(float3 a) { return mul3(a, rsqrtf(dot3(a, a))); }
 
-// SETTLE: moves the unconstrained new positions of one rigid water onto its
-// geometry, keeping its centre of mass, from the old (constrained) ones.  The
-// triangle in its own frame has O at (0, ra, 0) and the hydrogens at
-// (-+rc, -rb, 0); the new plane orientation comes from rotations about the
-// frame axes solved in closed form.  Velocities follow from the displacement.
-__global__ void k_settle(int n_waters, const int* __restrict__ waters, const int* __restrict__ atom_sys,
-                         const int* __restrict__ left, float3* __restrict__ crd, float3* __restrict__ vel,
-                         const float3* __restrict__ crd_old, float mO, float mH, float ra, float rb, float rc,
-                         float inv_dt)
+// SETTLE for one rigid water (oxygen o, hydrogens o+1, o+2): moves the
+// unconstrained new positions onto the water's geometry, keeping its centre
+// of mass, from the old (constrained) ones.  The triangle in its own frame
+// has O at (0, ra, 0) and the hydrogens at (-+rc, -rb, 0); the new plane
+// orientation comes from rotations about the frame axes solved in closed
+// form (Miyamoto & Kollman 1992).  Velocities follow from the displacement.
+// Old positions o0..o2 (constrained), new ones n0..n2 (unconstrained) in;
+// the constrained new positions and their velocities out (in n and v).
+__device__ __forceinline__ void settle_water(float3 o0, float3 o1, float3 o2, float3 (&n)[3], float3 (&v)[3],
+                                             float mO, float mH, float ra, float rb, float rc, float inv_dt)
 {
-    const int w = blockIdx.x * blockDim.x + threadIdx.x;
-    if (w >= n_waters) return;
-    const int o = waters[w];
-    if (o < 0 || left[atom_sys[o]] == 0) return;
-    const float3 origin = crd_old[o];
+    const float3 origin = o0;
     // everything relative to the old oxygen, for precision
-    const float3 b0 = sub3(crd_old[o + 1], origin), c0 = sub3(crd_old[o + 2], origin);
-    const float3 a1 = sub3(crd[o], origin), b1 = sub3(crd[o + 1], origin), c1 = sub3(crd[o + 2], origin);
+    const float3 b0 = sub3(o1, origin), c0 = sub3(o2, origin);
+    const float3 a1 = sub3(n[0], origin), b1 = sub3(n[1], origin), c1 = sub3(n[2], origin);
     const float wt = mO + 2.0f * mH;
     const float3 com = mul3(add3(mul3(a1, mO), mul3(add3(b1, c1), mH)), 1.0f / wt);
     const float3 xa1 = sub3(a1, com), xb1 = sub3(b1, com), xc1 = sub3(c1, com);
@@ -178,97 +161,353 @@ __global__ void k_settle(int n_waters, const int* __restrict__ waters, const int
     const float3 a3 = add3(com, add3(add3(mul3(ex, xa3), mul3(ey, ya3)), mul3(ez, za1)));
     const float3 b3 = add3(com, add3(add3(mul3(ex, xb3), mul3(ey, yb3)), mul3(ez, zb1)));
     const float3 c3 = add3(com, add3(add3(mul3(ex, xc3), mul3(ey, yc3)), mul3(ez, zc1)));
-    crd[o] = add3(origin, a3);
-    crd[o + 1] = add3(origin, b3);
-    crd[o + 2] = add3(origin, c3);
-    vel[o] = mul3(a3, inv_dt);  // a0 is the origin
-    vel[o + 1] = mul3(sub3(b3, b0), inv_dt);
-    vel[o + 2] = mul3(sub3(c3, c0), inv_dt);
+    n[0] = add3(origin, a3);
+    n[1] = add3(origin, b3);
+    n[2] = add3(origin, c3);
+    v[0] = mul3(a3, inv_dt);  // a0 is the origin
+    v[1] = mul3(sub3(b3, b0), inv_dt);
+    v[2] = mul3(sub3(c3, c0), inv_dt);
 }
 
-// Berendsen weak coupling per system: twice the kinetic energy (summed in
-// fixed point, so the same in any order), then every velocity scaled by
-// sqrt(1 + dt/tau (T0/T - 1)) (clamped to [0.8, 1.25]).
-__global__ void k_kinetic(int n, const float3* __restrict__ vel, const float* __restrict__ inv_mass,
-                          const int* __restrict__ atom_sys, const int* __restrict__ left, long long* __restrict__ kin)
+// What one step of the batched engine's integrator needs (k_step_begin).
+struct StepArgs
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    int s = -1;
-    long long q = 0;
-    if (i < n && inv_mass[i] != 0.0f)
+    int n, w_cap, S;
+    const int* atom_sys;            // system of each atom (parked atoms: a system that is not live)
+    const int* atom_slot;           // slot of each atom in its system's last build
+    const unsigned char* in_water;  // atoms moved by their water's thread
+    const int* waters;              // oxygen of each rigid water, -1 for a free entry
+    const int* live;
+    int* left;
+    int* steps;
+    float3* crd;
+    float3* vel;
+    float3* frc;
+    float3* crd_old;
+    const float* inv_mass;
+    const float* charge;
+    long long* facc;                // the force pass's int64 staging per slot, taken and cleared here
+    float dt, inv_dt;
+    int settle;
+    float mO, mH, ra, rb, rc;
+    int thermostat;                 // Berendsen: lambda from the last step's kinetic energy
+    long long* kin;
+    float* lambda;
+    const float* ndof;
+    float kT0, coupling;
+    int interval;                   // > 0: rebuild by step count; 0: by the skin check
+    const spgnb::SysDesc* sys;
+    const float4* slot_x0;
+    const float4* slot_d0;
+    float4* slot_pos;
+    const float4* pref;             // positions at the last pruning (null: pruning off)
+    float half_buffer2;
+    int* prune;
+    int* skin_hit;
+    int* need;
+    int* counters;
+    int* done;                      // blocks finished (the last one decides)
+    cudaGraphConditionalHandle h_build, h_prune;  // 0 outside a captured graph
+};
+
+// One atom's state for a step, every load issued before any use (the
+// loads do not depend on each other beyond the slot index), so a thread waits
+// for memory about twice instead of once per access.
+struct AtomIn
+{
+    int slot;
+    long long f[3];  // the force pass's int64 sums for the atom's slot
+    float3 x, v;
+    float im, q;
+    float4 x0, d0, pref;
+};
+
+__device__ __forceinline__ void load_atom(const StepArgs& a, int i, AtomIn& t)
+{
+    t.slot = a.atom_slot[i];
+    const long long* f = a.facc + 3 * (size_t)t.slot;
+    t.f[0] = f[0];
+    t.f[1] = f[1];
+    t.f[2] = f[2];
+    t.x = a.crd[i];
+    t.v = a.vel[i];
+    t.im = a.inv_mass[i];
+    t.q = a.charge[i];
+    t.x0 = a.slot_x0[t.slot];
+    t.d0 = a.slot_d0[t.slot];
+    t.pref = a.pref ? a.pref[t.slot] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
+// F(t) from the staging, which is cleared for the next force pass; also the
+// caller-visible float force.
+__device__ __forceinline__ float3 take_force(const StepArgs& a, int i, const AtomIn& t)
+{
+    long long* f = a.facc + 3 * (size_t)t.slot;
+    f[0] = 0;
+    f[1] = 0;
+    f[2] = 0;
+    const float3 r = make_float3((float)((double)t.f[0] * kForceUnscale), (float)((double)t.f[1] * kForceUnscale),
+                                 (float)((double)t.f[2] * kForceUnscale));
+    a.frc[i] = r;
+    return r;
+}
+
+// Leap-frog kick with F(t) (velocities first scaled by the thermostat's
+// lambda) and drift, in registers: t.x becomes the new position.
+__device__ __forceinline__ void kick_drift(const StepArgs& a, AtomIn& t, float3 f, float lam)
+{
+    const float im = t.im * a.dt;
+    t.v.x = fmaf(f.x, im, t.v.x * lam);
+    t.v.y = fmaf(f.y, im, t.v.y * lam);
+    t.v.z = fmaf(f.z, im, t.v.z * lam);
+    t.x = make_float3(fmaf(t.v.x, a.dt, t.x.x), fmaf(t.v.y, a.dt, t.x.y), fmaf(t.v.z, a.dt, t.x.z));
+}
+
+struct BoxOf
+{
+    spgnb::Cell cell, rcell;
+    float permit2;
+};
+
+__device__ __forceinline__ BoxOf box_of(const StepArgs& a, int sy)
+{
+    const spgnb::SysDesc& D = a.sys[sy];
+    BoxOf b;
+    b.cell = D.cell;
+    b.rcell = D.rcell;
+    b.permit2 = D.permit2;
+    return b;
+}
+
+// The moved atom's slot record {offset from the build-time cluster centre
+// moved by the displacement since the build, charge} for the force pass, and
+// the checks that follow a move: a pruning when it moved more than half the
+// prune buffer since the last one, a rebuild (skin trigger) when it moved
+// more than the permitted skin since the build (UPDATOR::Check_Refresh,
+// neighbor_list.cpp:166-180, in the same expression as k_check_refresh).
+__device__ __forceinline__ void pack_atom(const StepArgs& a, const AtomIn& t, int sy, const BoxOf& D, bool& moved)
+{
+    const float3 c = t.x;
+    const float4 o = t.x0;
     {
-        s = atom_sys[i];
-        if (left[s] == 0)
-            s = -1;
-        else
+        float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+        const float sx = rintf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31);
+        const float sy2 = rintf(dy * D.rcell.a22 + dz * D.rcell.a32);
+        const float sz = rintf(dz * D.rcell.a33);
+        dx -= sx * D.cell.a11 + sy2 * D.cell.a21 + sz * D.cell.a31;
+        dy -= sy2 * D.cell.a22 + sz * D.cell.a32;
+        dz -= sz * D.cell.a33;
+        const float4 p = make_float4(t.d0.x + dx, t.d0.y + dy, t.d0.z + dz, t.q);
+        a.slot_pos[t.slot] = p;
+        if (a.pref)
         {
-            const float3 v = vel[i];
-            const double mv2 = (double)((v.x * v.x + v.y * v.y + v.z * v.z) / inv_mass[i]);
-            q = __double2ll_rn(mv2 * kEnergyScale);
+            const float ex = p.x - t.pref.x, ey = p.y - t.pref.y, ez = p.z - t.pref.z;
+            if (ex * ex + ey * ey + ez * ez > a.half_buffer2)
+            {
+                a.prune[sy] = 1;
+                moved = true;
+            }
         }
     }
-    // a warp's atoms nearly always belong to one system (atoms are
-    // contiguous per system): one atomic per warp then, per lane otherwise
-    const unsigned valid = __ballot_sync(0xffffffffu, s >= 0);
-    if (!valid) return;
-    const int s0 = __shfl_sync(0xffffffffu, s, __ffs(valid) - 1);
-    if (__all_sync(0xffffffffu, s < 0 || s == s0))
+    if (a.interval <= 0)
     {
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
-        if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long*)&kin[s0], (unsigned long long)q);
+        float dx = c.x - o.x, dy = c.y - o.y, dz = c.z - o.z;
+        const float sx = floorf(dx * D.rcell.a11 + dy * D.rcell.a21 + dz * D.rcell.a31 + 0.5f);
+        const float sy2 = floorf(dy * D.rcell.a22 + dz * D.rcell.a32 + 0.5f);
+        const float sz = floorf(dz * D.rcell.a33 + 0.5f);
+        dx -= sx * D.cell.a11 + sy2 * D.cell.a21 + sz * D.cell.a31;
+        dy -= sy2 * D.cell.a22 + sz * D.cell.a32;
+        dz -= sz * D.cell.a33;
+        if (dx * dx + dy * dy + dz * dz > D.permit2) a.skin_hit[sy] = 1;
     }
-    else if (s >= 0)
-        atomicAdd((unsigned long long*)&kin[s], (unsigned long long)q);
 }
 
-__global__ void k_rescale(int n, float3* __restrict__ vel, const int* __restrict__ atom_sys,
-                          const int* __restrict__ left, const long long* __restrict__ kin,
-                          const float* __restrict__ ndof, float kT0, float coupling)
+__device__ __forceinline__ double mv2(const AtomIn& t)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int s = atom_sys[i];
-    if (left[s] == 0) return;
-    const double kT = (double)kin[s] / kEnergyScale / fmax((double)ndof[s], 1.0);  // k_B T = 2 E_kin / dof
-    const float lam2 = kT > 0.0 ? 1.0f + coupling * (float)(kT0 / kT - 1.0) : 1.0f;
-    const float lam = sqrtf(fminf(fmaxf(lam2, 0.64f), 1.5625f));
-    float3 v = vel[i];
-    vel[i] = make_float3(v.x * lam, v.y * lam, v.z * lam);
+    return t.im != 0.0f ? (double)((t.v.x * t.v.x + t.v.y * t.v.y + t.v.z * t.v.z) / t.im) : 0.0;
 }
 
-// End of a step: per live system, one more step done, one fewer left.
-__global__ void k_tick(int S, const int* __restrict__ live, int* __restrict__ left, int* __restrict__ steps)
+// The start of a batched step, one kernel: threads [0, n) the atoms outside
+// rigid waters, [n, n + w_cap) the waters (their three atoms, then SETTLE).
+// Each takes its atoms' forces F(t) from the force pass's staging, kicks and
+// drifts them, writes their slot records for this step's force pass and
+// checks how far they moved, and adds m v^2 to its system's fixed-point sum.
+// Systems with no steps left keep their state (their forces are still taken).
+// The last block to finish, once every atom has moved, ends the step for
+// each system: its step counter, the thermostat's lambda for the next step,
+// the rebuild decision (refresh interval or skin trigger), and sets the
+// graph's conditionals: the list build when some system rebuilds, the
+// pruning when some system prunes.
+__global__ void k_step_begin(StepArgs a)
+{
+    const int u = blockIdx.x * blockDim.x + threadIdx.x;
+    int sy = -1;
+    double e = 0.0;
+    bool moved = false;
+    if (u < a.n)
+    {
+        const int i = u;
+        const int s = a.atom_sys[i];
+        if (!a.in_water[i] && s < a.S && a.live[s])
+        {
+            AtomIn t;
+            load_atom(a, i, t);
+            const float3 f = take_force(a, i, t);
+            if (a.left[s] != 0)
+            {
+                const BoxOf box = box_of(a, s);
+                const float3 x_old = t.x;
+                kick_drift(a, t, f, a.thermostat ? a.lambda[s] : 1.0f);
+                a.crd_old[i] = x_old;
+                a.crd[i] = t.x;
+                a.vel[i] = t.v;
+                pack_atom(a, t, s, box, moved);
+                e = mv2(t);
+                sy = s;
+            }
+        }
+    }
+    else if (u < a.n + a.w_cap)
+    {
+        const int o = a.waters[u - a.n];
+        const int s = o >= 0 ? a.atom_sys[o] : a.S;
+        if (s < a.S && a.live[s])
+        {
+            AtomIn t[3];
+            load_atom(a, o, t[0]);
+            load_atom(a, o + 1, t[1]);
+            load_atom(a, o + 2, t[2]);
+            const float3 f0 = take_force(a, o, t[0]), f1 = take_force(a, o + 1, t[1]),
+                         f2 = take_force(a, o + 2, t[2]);
+            if (a.left[s] != 0)
+            {
+                const BoxOf box = box_of(a, s);
+                const float lam = a.thermostat ? a.lambda[s] : 1.0f;
+                const float3 x0 = t[0].x, x1 = t[1].x, x2 = t[2].x;
+                kick_drift(a, t[0], f0, lam);
+                kick_drift(a, t[1], f1, lam);
+                kick_drift(a, t[2], f2, lam);
+                if (a.settle)
+                {
+                    float3 n[3] = {t[0].x, t[1].x, t[2].x}, v[3];
+                    settle_water(x0, x1, x2, n, v, a.mO, a.mH, a.ra, a.rb, a.rc, a.inv_dt);
+                    for (int k = 0; k < 3; k++)
+                    {
+                        t[k].x = n[k];
+                        t[k].v = v[k];
+                    }
+                }
+                a.crd_old[o] = x0;
+                a.crd_old[o + 1] = x1;
+                a.crd_old[o + 2] = x2;
+                for (int k = 0; k < 3; k++)
+                {
+                    a.crd[o + k] = t[k].x;
+                    a.vel[o + k] = t[k].v;
+                    pack_atom(a, t[k], s, box, moved);
+                }
+                e = mv2(t[0]) + mv2(t[1]) + mv2(t[2]);
+                sy = s;
+            }
+        }
+    }
+    if (__any_sync(0xffffffffu, moved) && (threadIdx.x & 31) == 0) a.counters[kCntPrune] = 1;
+    if (a.thermostat)
+    {
+        // twice the kinetic energy in fixed point (the same in any order):
+        // one atomic per warp when its atoms belong to one system
+        long long q = sy >= 0 ? __double2ll_rn(e * kEnergyScale) : 0ll;
+        const unsigned valid = __ballot_sync(0xffffffffu, sy >= 0);
+        if (valid)
+        {
+            const int s0 = __shfl_sync(0xffffffffu, sy, __ffs(valid) - 1);
+            if (__all_sync(0xffffffffu, sy < 0 || sy == s0))
+            {
+#pragma unroll
+                for (int k = 16; k > 0; k >>= 1) q += __shfl_xor_sync(0xffffffffu, q, k);
+                if ((threadIdx.x & 31) == 0) atomicAdd((unsigned long long*)&a.kin[s0], (unsigned long long)q);
+            }
+            else if (sy >= 0)
+                atomicAdd((unsigned long long*)&a.kin[sy], (unsigned long long)q);
+        }
+    }
+    // the last block ends the step for every system (the block's writes
+    // ordered before its count by the barrier and one fence)
+    __shared__ int is_last;
+    __syncthreads();
+    if (threadIdx.x == 0)
+    {
+        __threadfence();
+        is_last = atomicAdd(a.done, 1) == (int)gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!is_last) return;
+    __threadfence();
+    int any_need = 0, any_prune = 0;
+    for (int s = threadIdx.x; s < a.S; s += blockDim.x)
+    {
+        const bool active = a.live[s] && a.left[s] != 0;
+        const bool due = active && (a.interval > 0 ? (a.steps[s] + 1) % a.interval == 0 : a.skin_hit[s] != 0);
+        a.skin_hit[s] = 0;
+        a.need[s] = due ? 1 : 0;
+        any_need |= due ? 1 : 0;
+        any_prune |= a.prune[s] != 0 ? 1 : 0;
+        if (a.thermostat)
+        {
+            // Berendsen: lambda^2 = 1 + dt/tau (T0/T - 1), clamped to [0.64, 1.5625]
+            const double kT = (double)a.kin[s] / kEnergyScale / fmax((double)a.ndof[s], 1.0);
+            const float lam2 = kT > 0.0 ? 1.0f + a.coupling * (float)(a.kT0 / kT - 1.0) : 1.0f;
+            a.lambda[s] = sqrtf(fminf(fmaxf(lam2, 0.64f), 1.5625f));
+            a.kin[s] = 0;
+        }
+        if (active)
+        {
+            a.steps[s] += 1;
+            if (a.left[s] > 0) a.left[s] -= 1;
+        }
+    }
+    any_need = __syncthreads_or(any_need);
+    any_prune = __syncthreads_or(any_prune);
+    if (threadIdx.x == 0)
+    {
+        a.counters[kCntNeed] = any_need;
+        if (any_prune) a.counters[kCntPrune] = 1;
+        *a.done = 0;
+        if (a.h_build) cudaGraphSetConditional(a.h_build, any_need ? 1u : 0u);
+        if (a.h_prune) cudaGraphSetConditional(a.h_prune, (any_need || any_prune) ? 1u : 0u);
+    }
+}
+
+// Clears the force staging of the chosen systems' slots (all with flags
+// null), and their energy totals, before a force pass for them alone.
+__global__ void k_clear_staged(int slots, const int* __restrict__ cl_sys, const int* __restrict__ flags,
+                               long long* __restrict__ facc, int S, long long* __restrict__ totals)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= S || !live[s] || left[s] == 0) return;
-    steps[s] += 1;
-    if (left[s] > 0) left[s] -= 1;
+    if (s < slots && (!flags || flags[cl_sys[s >> 3]]))
+    {
+        facc[3 * (size_t)s] = 0;
+        facc[3 * (size_t)s + 1] = 0;
+        facc[3 * (size_t)s + 2] = 0;
+    }
+    if (totals && s < 8 * S && (!flags || flags[s >> 3])) totals[s] = 0;
 }
 
-// Zero the forces of the flagged systems' atoms and their totals.
-__global__ void k_clear_flagged(int n, const int* __restrict__ atom_sys, const int* __restrict__ flags,
-                                float3* __restrict__ frc, int S, long long* __restrict__ totals)
+// The forces of atoms [first, first + count) from their slots' staging
+// (left in place for the next step).
+__global__ void k_forces_out(int first, int count, const int* __restrict__ atom_slot,
+                             const long long* __restrict__ facc, float3* __restrict__ frc)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n && flags[atom_sys[i]]) frc[i] = make_float3(0.0f, 0.0f, 0.0f);
-    if (totals && i < 8 * S && flags[i >> 3]) totals[i] = 0;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const int i = first + k;
+    const long long* f = facc + 3 * (size_t)atom_slot[i];
+    frc[i] = make_float3((float)((double)f[0] * kForceUnscale), (float)((double)f[1] * kForceUnscale),
+                         (float)((double)f[2] * kForceUnscale));
 }
 
-int batch_force(spgnb_batch* b, int mode, cudaStream_t s, const int* only = nullptr)
+ForceInputs batch_inputs(spgnb_batch* b, int mode, const int* only)
 {
-    if (!only)
-    {
-        SPGNB_CUDA(cudaMemsetAsync(b->d_frc, 0, sizeof(float3) * b->n, s));
-        if (mode) SPGNB_CUDA(cudaMemsetAsync(b->d_totals, 0, sizeof(long long) * 8 * b->S, s));
-    }
-    else
-    {
-        const int m = std::max(b->n, 8 * b->S);
-        k_clear_flagged<<<(m + 255) / 256, 256, 0, s>>>(b->n, b->nl->d_atom_sys, only, b->d_frc, b->S,
-                                                         mode ? b->d_totals : nullptr);
-        SPGNB_CHECK_LAUNCH("k_clear_flagged");
-    }
     ForceInputs in;
     in.nl = b->nl;
     in.crd = b->d_crd;
@@ -288,114 +527,171 @@ int batch_force(spgnb_batch* b, int mode, cudaStream_t s, const int* only = null
     in.prune_blocks_per_sm = b->prune_bps;
     in.om.solvent_start = b->n;
     in.only = only;
-    return force_pipeline(in, s);
+    return in;
 }
 
-// Sets a graph's conditional from a device flag (non-zero: some system
-// rebuilds its list this step).
-__global__ void k_set_cond(cudaGraphConditionalHandle h, const int* __restrict__ any)
+// A force pass outside the step, for the flagged systems (all with only
+// null): their staging cleared, slot pack, pruning, pair kernel.  The forces
+// stay in the staging for the next step to take (k_forces_out reads them).
+int batch_force(spgnb_batch* b, int mode, cudaStream_t s, const int* only = nullptr)
 {
-    cudaGraphSetConditional(h, *any != 0 ? 1u : 0u);
+    const int slots = b->nl->clusters_cap * kClusterSize;
+    const int m = std::max(slots, 8 * b->S);
+    k_clear_staged<<<(m + 255) / 256, 256, 0, s>>>(slots, b->nl->d_cl_sys, only, b->nl->d_facc, b->S,
+                                                   mode ? b->d_totals : nullptr);
+    SPGNB_CHECK_LAUNCH("k_clear_staged");
+    const ForceInputs in = batch_inputs(b, mode, only);
+    int st = force_check(in);
+    if (!st) st = launch_pack(in, s, nullptr);
+    if (!st) st = launch_prune(in, s);
+    if (!st) st = launch_pair_kernel(in, s);
+    return st;
 }
 
-// During a graph capture, the list build of a step becomes the body of an
-// 'if' node on the device's rebuild flag, captured on a side stream, so a
-// step without a rebuild launches none of its kernels.  Outside a capture the
-// build runs inline.
-struct CondBuild : BuildBody
+// During a graph capture: an 'if' node on handle h after the work captured
+// so far on s, its body captured on the side stream (open .. close).
+struct CaptureIf
 {
     cudaStream_t side = nullptr;
-    int status = SPGNB_OK;
-    bool open = false;
-    long long body_kernels = 0;
-    unsigned long long c0 = 0;
-    cudaStream_t body(cudaStream_t s, const int* d_any) override
+    bool open_ = false;
+    static int handle(cudaStream_t s, cudaGraphConditionalHandle* h)
     {
         cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
         cudaGraph_t g = nullptr;
         const cudaGraphNode_t* deps = nullptr;
         size_t nd = 0;
-        cudaError_t e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd);
-        if (e == cudaSuccess && cs != cudaStreamCaptureStatusActive) return s;
-        cudaGraphConditionalHandle h = 0;
-        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
-        if (e == cudaSuccess)
-        {
-            k_set_cond<<<1, 1, 0, s>>>(h, d_any);
-            count_launch();
-            e = cudaGetLastError();
-        }
-        if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd);
-        cudaGraphNodeParams p{};
-        cudaGraphNode_t node = nullptr;
-        if (e == cudaSuccess)
-        {
-            p.type = cudaGraphNodeTypeConditional;
-            p.conditional.handle = h;
-            p.conditional.type = cudaGraphCondTypeIf;
-            p.conditional.size = 1;
-            e = cudaGraphAddNode(&node, g, deps, nd, &p);
-        }
-        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
-        if (e == cudaSuccess)
-            e = cudaStreamBeginCaptureToGraph(side, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
-                                              cudaStreamCaptureModeThreadLocal);
-        if (e != cudaSuccess)
-        {
-            status = cuda_fail(e, "conditional list build");
-            return nullptr;
-        }
-        open = true;
-        c0 = launches_so_far();
-        return side;
+        SPGNB_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+        *h = 0;
+        if (cs == cudaStreamCaptureStatusActive)
+            SPGNB_CUDA(cudaGraphConditionalHandleCreate(h, g, 0, cudaGraphCondAssignDefault));
+        return SPGNB_OK;
     }
-    int done() override
+    int open(cudaStream_t s, cudaGraphConditionalHandle h)
     {
-        if (open)
-        {
-            body_kernels += (long long)(launches_so_far() - c0);
-            cudaGraph_t g = nullptr;
-            const cudaError_t e = cudaStreamEndCapture(side, &g);
-            open = false;
-            if (e != cudaSuccess && !status) status = cuda_fail(e, "conditional list build");
-        }
-        return status;
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        SPGNB_CUDA(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+        cudaGraphNodeParams p{};
+        p.type = cudaGraphNodeTypeConditional;
+        p.conditional.handle = h;
+        p.conditional.type = cudaGraphCondTypeIf;
+        p.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        SPGNB_CUDA(cudaGraphAddNode(&node, g, deps, nd, &p));
+        SPGNB_CUDA(cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies));
+        SPGNB_CUDA(cudaStreamBeginCaptureToGraph(side, p.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                 cudaStreamCaptureModeThreadLocal));
+        open_ = true;
+        return SPGNB_OK;
+    }
+    int close()
+    {
+        if (!open_) return SPGNB_OK;
+        open_ = false;
+        cudaGraph_t g = nullptr;
+        SPGNB_CUDA(cudaStreamEndCapture(side, &g));
+        return SPGNB_OK;
     }
 };
 
-// One step: kick-drift, SETTLE, thermostat, list update, forces, counters.
-int batch_step(spgnb_batch* b, bool energy, cudaStream_t s, BuildBody* split = nullptr)
+// One step: k_step_begin (forces taken, kick, drift, SETTLE, slot records,
+// decisions), the list build (when some system rebuilds), the pruning (when
+// some system prunes), the pair kernel.  In a capture (cap set) the build
+// and the pruning are the bodies of conditional nodes the step kernel sets;
+// otherwise they are launched and return at once unless needed.  Counts the
+// kernels of the build and pruning bodies into *cond_kernels.
+int batch_step(spgnb_batch* b, bool energy, cudaStream_t s, CaptureIf* cap = nullptr,
+               long long* cond_kernels = nullptr)
 {
-    const float dt = b->opt.dt * kTimeUnitsPerPs;
-    const int* atom_sys = b->nl->d_atom_sys;
-    k_leapfrog<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, atom_sys, b->d_left, b->d_crd, b->d_vel, b->d_frc,
-                                                   b->d_inv_mass, b->d_crd_old, dt);
-    SPGNB_CHECK_LAUNCH("k_leapfrog");
-    if (b->have_water)
+    spgnb_nl* nl = b->nl;
+    StepArgs a{};
+    a.n = b->n;
+    a.w_cap = b->have_water ? b->w_cap : 0;
+    a.S = b->S;
+    a.atom_sys = nl->d_atom_sys;
+    a.atom_slot = nl->d_atom_slot;
+    a.in_water = b->d_in_water;
+    a.waters = b->d_waters;
+    a.live = nl->d_live;
+    a.left = b->d_left;
+    a.steps = b->d_steps;
+    a.crd = b->d_crd;
+    a.vel = b->d_vel;
+    a.frc = b->d_frc;
+    a.crd_old = b->d_crd_old;
+    a.inv_mass = b->d_inv_mass;
+    a.charge = b->d_charge;
+    a.facc = nl->d_facc;
+    a.dt = b->opt.dt * kTimeUnitsPerPs;
+    a.inv_dt = 1.0f / a.dt;
+    a.settle = b->have_water ? 1 : 0;
+    a.mO = b->mO;
+    a.mH = b->mH;
+    a.ra = b->ra;
+    a.rb = b->rb;
+    a.rc = b->rc;
+    a.thermostat = b->opt.thermostat_tau > 0.0f ? 1 : 0;
+    a.kin = b->d_kin;
+    a.lambda = b->d_lambda;
+    a.ndof = b->d_ndof;
+    a.kT0 = 0.00198716f * b->opt.temperature;  // kcal/mol
+    a.coupling = b->opt.thermostat_tau > 0.0f ? b->opt.dt / b->opt.thermostat_tau : 0.0f;
+    a.interval = b->opt.refresh_interval;
+    a.sys = nl->d_sys;
+    a.slot_x0 = nl->d_slot_x0;
+    a.slot_d0 = nl->d_slot_d0;
+    a.slot_pos = b->d_slot_pos;
+    const bool track = nl->opt.prune_buffer > 0.0f;
+    a.pref = track ? nl->d_pref : nullptr;
+    const float half = 0.5f * nl->opt.prune_buffer;
+    a.half_buffer2 = half * half;
+    a.prune = nl->d_prune;
+    a.skin_hit = b->d_skin_hit;
+    a.need = nl->d_need;
+    a.counters = nl->d_counters;
+    a.done = b->d_done;
+    int st;
+    if (cap && ((st = CaptureIf::handle(s, &a.h_build)) || (st = CaptureIf::handle(s, &a.h_prune)))) return st;
+    const int units = a.n + a.w_cap;
+    k_step_begin<<<(units + 255) / 256, 256, 0, s>>>(a);
+    SPGNB_CHECK_LAUNCH("k_step_begin");
+    const ForceInputs in = batch_inputs(b, energy ? 1 : 0, nullptr);
+    if ((st = force_check(in))) return st;
+    // the list build, then the slot records in the new slots
+    cudaStream_t bs = s;
+    if (cap && a.h_build)
     {
-        k_settle<<<(b->w_cap + 127) / 128, 128, 0, s>>>(b->w_cap, b->d_waters, atom_sys, b->d_left, b->d_crd,
-                                                         b->d_vel, b->d_crd_old, b->mO, b->mH, b->ra, b->rb, b->rc,
-                                                         1.0f / dt);
-        SPGNB_CHECK_LAUNCH("k_settle");
+        if ((st = cap->open(s, a.h_build))) return st;
+        bs = cap->side;
     }
-    if (b->opt.thermostat_tau > 0.0f)
+    const unsigned long long c0 = launches_so_far();
+    st = nl_queue_build_body(nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num, bs);
+    if (!st) st = launch_pack(in, bs, nl->d_counters + kCntNeed);
+    if (cap && a.h_build)
     {
-        SPGNB_CUDA(cudaMemsetAsync(b->d_kin, 0, sizeof(long long) * b->S, s));
-        k_kinetic<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_vel, b->d_inv_mass, atom_sys, b->d_left, b->d_kin);
-        SPGNB_CHECK_LAUNCH("k_kinetic");
-        const float kT0 = 0.00198716f * b->opt.temperature;  // kcal/mol
-        k_rescale<<<(b->n + 255) / 256, 256, 0, s>>>(b->n, b->d_vel, atom_sys, b->d_left, b->d_kin, b->d_ndof, kT0,
-                                                      b->opt.dt / b->opt.thermostat_tau);
-        SPGNB_CHECK_LAUNCH("k_rescale");
+        const int st2 = cap->close();
+        if (!st) st = st2;
     }
-    int st = nl_queue_build(b->nl, b->n, b->d_crd, b->d_atom_local, b->d_ex_start, b->d_ex_list, b->d_ex_num,
-                            b->opt.refresh_interval > 0 ? kBuildInterval : kBuildSkin, s, b->d_steps,
-                            b->opt.refresh_interval, b->d_left, split);
     if (st) return st;
-    if ((st = batch_force(b, energy ? 1 : 0, s))) return st;
-    k_tick<<<(b->S + 255) / 256, 256, 0, s>>>(b->S, b->nl->d_live, b->d_left, b->d_steps);
-    SPGNB_CHECK_LAUNCH("k_tick");
-    return SPGNB_OK;
+    // the pruning
+    cudaStream_t ps = s;
+    if (cap && a.h_prune)
+    {
+        if ((st = cap->open(s, a.h_prune))) return st;
+        ps = cap->side;
+    }
+    st = launch_prune(in, ps);
+    if (cap && a.h_prune)
+    {
+        const int st2 = cap->close();
+        if (!st) st = st2;
+    }
+    if (st) return st;
+    if (cond_kernels) *cond_kernels += (long long)(launches_so_far() - c0);
+    if (energy) SPGNB_CUDA(cudaMemsetAsync(b->d_totals, 0, sizeof(long long) * 8 * b->S, s));
+    return launch_pair_kernel(in, s);
 }
 
 // Lists and forces (with energies) of the systems admitted since the last
@@ -425,27 +721,28 @@ void free_graphs(spgnb_batch* b)
 int capture(spgnb_batch* b, bool energy_last, cudaGraphExec_t* out, long long* kernels)
 {
     cudaGraph_t g = nullptr;
-    CondBuild cb;
-    SPGNB_CUDA(cudaStreamCreateWithFlags(&cb.side, cudaStreamNonBlocking));
+    CaptureIf cap;
+    SPGNB_CUDA(cudaStreamCreateWithFlags(&cap.side, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
     if (e != cudaSuccess)
     {
-        cudaStreamDestroy(cb.side);
+        cudaStreamDestroy(cap.side);
         return cuda_fail(e, "cudaStreamBeginCapture");
     }
     int st = SPGNB_OK;
+    long long cond = 0;
     const unsigned long long c0 = launches_so_far();
     for (int k = 0; k < b->opt.steps_per_graph && !st; k++)
-        st = batch_step(b, energy_last && k == b->opt.steps_per_graph - 1, b->stream, &cb);
-    // captured, not run: counted when the graph is launched (the build
-    // bodies, which run only on rebuild steps, apart)
+        st = batch_step(b, energy_last && k == b->opt.steps_per_graph - 1, b->stream, &cap, &cond);
+    // captured, not run: counted when the graph is launched (the conditional
+    // bodies, which run only on rebuild and pruning steps, apart)
     const long long all = (long long)(launches_so_far() - c0);
     count_launches(-all);
-    *kernels = all - cb.body_kernels;
-    b->kernels_build = cb.body_kernels / std::max(1, b->opt.steps_per_graph);
-    if (cb.open) cb.done();
+    *kernels = all - cond;
+    b->kernels_build = cond / std::max(1, b->opt.steps_per_graph);
+    cap.close();
     e = cudaStreamEndCapture(b->stream, &g);
-    cudaStreamDestroy(cb.side);
+    cudaStreamDestroy(cap.side);
     if (st)
     {
         if (g) cudaGraphDestroy(g);
@@ -486,6 +783,10 @@ void free_batch(spgnb_batch* b)
     dfree(b->d_ex_num);
     dfree(b->d_ex_list);
     dfree(b->d_waters);
+    dfree(b->d_in_water);
+    dfree(b->d_lambda);
+    dfree(b->d_skin_hit);
+    dfree(b->d_done);
     dfree(b->d_fps);
     dfree(b->d_totals);
     dfree(b->d_kin);
@@ -717,12 +1018,18 @@ int create_common(spgnb_batch* b, const NLPoolSpec& spec, long long ex_cap, int 
         (st = zalloc(&b->d_ex_list, (size_t)b->ex_cap)) || (st = dalloc(&b->d_waters, (size_t)b->w_cap)) ||
         (st = dalloc(&b->d_t4, (size_t)b->t4_cap)) || (st = zalloc(&b->d_fps, S1)) ||
         (st = zalloc(&b->d_totals, 8 * S1)) || (st = zalloc(&b->d_kin, S1)) || (st = zalloc(&b->d_ndof, S1)) ||
+        (st = zalloc(&b->d_in_water, n)) || (st = dalloc(&b->d_lambda, S1)) || (st = zalloc(&b->d_skin_hit, S1)) ||
+        (st = zalloc(&b->d_done, 1)) ||
         (st = zalloc(&b->d_steps, S1)) || (st = zalloc(&b->d_left, S1)) || (st = zalloc(&b->d_flags, S1)) ||
         (st = dalloc(&b->d_slot_pos, (size_t)b->nl->clusters_cap * kClusterSize + 1)) ||
         (st = dalloc(&b->d_slot_aux, (size_t)b->nl->clusters_cap * kClusterSize + 1)))
         return st;
     SPGNB_CUDA(cudaMemcpy(b->d_t4, t4.data(), sizeof(float4) * t4.size(), cudaMemcpyHostToDevice));
     SPGNB_CUDA(cudaMemset(b->d_waters, 0xff, sizeof(int) * b->w_cap));
+    {
+        const std::vector<float> ones(S1, 1.0f);
+        SPGNB_CUDA(cudaMemcpy(b->d_lambda, ones.data(), sizeof(float) * S1, cudaMemcpyHostToDevice));
+    }
     SPGNB_CUDA(cudaDeviceSynchronize());
     cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) return cuda_fail(e, "cudaStreamCreate");
@@ -764,8 +1071,8 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
     // every upload of this admission goes through one pinned buffer, so the
     // copies queue behind the work in flight instead of waiting for it
     const size_t N = z.N;
-    const size_t need = N * (2 * sizeof(float3) + 6 * sizeof(int)) + ne * sizeof(int) +
-                        z.water_numbers * sizeof(int) + sizeof(ForceParams) + 3 * sizeof(int) + 16 * 20 +
+    const size_t need = N * (2 * sizeof(float3) + 6 * sizeof(int) + 1) + ne * sizeof(int) +
+                        z.water_numbers * sizeof(int) + sizeof(ForceParams) + 3 * sizeof(int) + sizeof(float) + 16 * 24 +
                         nt4 * sizeof(float4) + nl_admit_upload_bytes(z.sh, z.runs.size());
     PinnedStage* ps = nullptr;
     if ((st = take_stage(b, need, &ps)))
@@ -810,6 +1117,8 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
     }
     const int a0 = (int)ab;
     std::vector<int> own(z.N), ex_start(z.N), ex_list(ne), waters(z.water_numbers);
+    std::vector<unsigned char> in_water(z.N, 0);
+    for (int k = 0; k < 3 * z.water_numbers; k++) in_water[z.water_begin + k] = 1;
     for (int i = 0; i < z.N; i++)
     {
         own[i] = a0 + i;
@@ -820,10 +1129,12 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
     const std::vector<ForceParams> fp(1, z.fp);
     const std::vector<float> ndof(1, z.ndof);
     const std::vector<int> left(1, steps > 0 ? steps : -1);
+    const std::vector<float> lambda(1, 1.0f);
     auto putv = [&](auto* dst, size_t off, const auto& v) { return up.put(dst + off, v.data(), sizeof(v[0]) * v.size(), s); };
     if ((st = putv(b->d_crd, ab, z.crd)) || (st = putv(b->d_vel, ab, z.vel)) ||
         (st = putv(b->d_charge, ab, z.charge)) || (st = putv(b->d_inv_mass, ab, z.inv_mass)) ||
         (st = putv(b->d_type, ab, z.type)) || (st = putv(b->d_atom_local, ab, own)) ||
+        (st = putv(b->d_in_water, ab, in_water)) || (st = putv(b->d_lambda, sid, lambda)) ||
         (st = putv(b->d_ex_start, ab, ex_start)) || (st = putv(b->d_ex_num, ab, z.ex_num)) ||
         (st = putv(b->d_ex_list, eb, ex_list)) || (st = putv(b->d_waters, wb, waters)) ||
         (st = putv(b->d_fps, sid, fp)) || (st = putv(b->d_ndof, sid, ndof)) || (st = putv(b->d_left, sid, left)) ||
@@ -832,6 +1143,7 @@ int admit_staged(spgnb_batch* b, Staged& z, int steps, int* id)
     SPGNB_CUDA(cudaMemsetAsync(b->d_frc + ab, 0, sizeof(float3) * z.N, s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_steps + sid, 0, sizeof(int), s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_kin + sid, 0, sizeof(long long), s));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_skin_hit + sid, 0, sizeof(int), s));
     SPGNB_CUDA(cudaMemsetAsync(b->d_totals + 8 * (size_t)sid, 0, sizeof(long long) * 8, s));
     k_set_flag<<<1, 1, 0, s>>>(b->d_flags, sid);
     SPGNB_CHECK_LAUNCH("k_set_flag");
@@ -945,6 +1257,12 @@ int spgnb_batch_set_thermostat(spgnb_batch* b, float tau, float temperature)
     b->opt.thermostat_tau = tau;
     b->opt.temperature = temperature;
     free_graphs(b);
+    // the velocity scale starts again from 1 (the sums from zero)
+    const std::vector<float> ones(b->S + 1, 1.0f);
+    SPGNB_CUDA(cudaMemcpyAsync(b->d_lambda, ones.data(), sizeof(float) * ones.size(), cudaMemcpyHostToDevice,
+                               b->stream));
+    SPGNB_CUDA(cudaMemsetAsync(b->d_kin, 0, sizeof(long long) * (b->S + 1), b->stream));
+    SPGNB_CUDA(cudaStreamSynchronize(b->stream));
     return SPGNB_OK;
 }
 
@@ -1265,7 +1583,13 @@ int spgnb_batch_download(spgnb_batch* b, int sys, float* h_crd, float* h_vel, fl
     if (h_vel)
         SPGNB_CUDA(cudaMemcpyAsync(h_vel, b->d_vel + off, sizeof(float3) * cnt, cudaMemcpyDeviceToHost, b->stream));
     if (h_frc)
+    {
+        // the last force pass's forces, still in the staging for the next step
+        k_forces_out<<<((int)cnt + 255) / 256, 256, 0, b->stream>>>((int)off, (int)cnt, b->nl->d_atom_slot,
+                                                                     b->nl->d_facc, b->d_frc);
+        SPGNB_CHECK_LAUNCH("k_forces_out");
         SPGNB_CUDA(cudaMemcpyAsync(h_frc, b->d_frc + off, sizeof(float3) * cnt, cudaMemcpyDeviceToHost, b->stream));
+    }
     SPGNB_CUDA(cudaStreamSynchronize(b->stream));
     return SPGNB_OK;
 }

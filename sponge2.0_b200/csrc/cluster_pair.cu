@@ -45,7 +45,9 @@ constexpr int kPairWarps = 4;                       // warps per block of the fo
 // null slot: 10^4 A away from everything, charge 0.  With pruning on (pref
 // set) the kernel also flags a re-pruning when some atom moved more than half
 // the prune buffer since the last one.  It also clears the outputs the force
-// call must start from zero (totals, module-owned per-atom energies).
+// call must start from zero (totals, module-owned per-atom energies).  With
+// a gate it runs only when *gate is non-zero (after a rebuild, in the
+// batched step).
 __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict__ slot_atom,
                              const int* __restrict__ slot_gid, const int* __restrict__ cl_sys,
                              const SysDesc* __restrict__ sys, const int4* __restrict__ cl_q,
@@ -54,8 +56,10 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
                              const int* __restrict__ local_type, float4* __restrict__ pos, int4* __restrict__ aux,
                              const float4* __restrict__ pref, float half_buffer2, int* __restrict__ prune,
                              long long* __restrict__ clear_totals, long long* __restrict__ clear_one,
-                             float* __restrict__ clear_a, float* __restrict__ clear_b, int clear_n)
+                             float* __restrict__ clear_a, float* __restrict__ clear_b, int clear_n,
+                             const int* __restrict__ gate)
 {
+    if (gate && *gate == 0) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     bool moved = false;
     // the outputs the force call zeroes first
@@ -921,24 +925,35 @@ int build_t4(const float2* table, int T, float4** d_t4)
     return SPGNB_OK;
 }
 
-int force_pipeline(const ForceInputs& in, cudaStream_t s)
+int force_check(const ForceInputs& in)
+{
+    if (!in.t4) return fail(SPGNB_E_STATE, "force: the LJ module has no pair table");
+    if (in.mode == 2 && in.nl->S != 1)
+        return fail(SPGNB_E_UNSUPPORTED, "force: per-atom energy/virial outputs are for a one-system list");
+    if (in.p0.n_types <= 0 || in.p0.n_types > kMaxTypes)
+        return fail(SPGNB_E_UNSUPPORTED, "force: %d LJ types (at most %d)", in.p0.n_types, kMaxTypes);
+    return SPGNB_OK;
+}
+
+int launch_pack(const ForceInputs& in, cudaStream_t s, const int* gate)
 {
     spgnb_nl* nl = in.nl;
     const int slots = nl->clusters_cap * kClusterSize;
     const bool track = nl->opt.prune_buffer > 0.0f;
     const float half = 0.5f * nl->opt.prune_buffer;
-    if (!in.t4) return fail(SPGNB_E_STATE, "force: the LJ module has no pair table");
-    if (in.mode == 2 && nl->S != 1)
-        return fail(SPGNB_E_UNSUPPORTED, "force: per-atom energy/virial outputs are for a one-system list");
-    if (in.p0.n_types <= 0 || in.p0.n_types > kMaxTypes)
-        return fail(SPGNB_E_UNSUPPORTED, "force: %d LJ types (at most %d)", in.p0.n_types, kMaxTypes);
     k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_slot_gid,
                                                      nl->d_cl_sys, nl->d_sys, nl->d_cl_q, nl->d_slot_x0,
                                                      nl->d_slot_d0, in.crd, in.charge, in.atom_type, in.slot_pos,
                                                      in.slot_aux, track ? nl->d_pref : nullptr, half * half,
                                                      nl->d_prune, in.clear.totals, in.clear.one, in.clear.a, in.clear.b,
-                                                     in.clear.n);
+                                                     in.clear.n, gate);
     SPGNB_CHECK_LAUNCH("k_pack_slots");
+    return SPGNB_OK;
+}
+
+int launch_prune(const ForceInputs& in, cudaStream_t s)
+{
+    spgnb_nl* nl = in.nl;
     const int prune_bps = in.prune_blocks_per_sm > 0 ? in.prune_blocks_per_sm : 5;
     const int grid = std::max(1, std::min(num_sms() * prune_bps, (nl->clusters_cap + kPruneWarps - 1) / kPruneWarps));
     k_prune8<<<grid, kPruneWarps * 32, 0, s>>>(in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters,
@@ -947,6 +962,12 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
                                                in.slot_pos, nl->d_pref, nl->d_pcount, nl->d_pwords, nl->S,
                                                nl->d_prune);
     SPGNB_CHECK_LAUNCH("k_prune8");
+    return SPGNB_OK;
+}
+
+int launch_pair_kernel(const ForceInputs& in, cudaStream_t s)
+{
+    spgnb_nl* nl = in.nl;
     cudaEvent_t ev0, ev1;
     pair_events(&ev0, &ev1);
     if (ev0) SPGNB_CUDA(cudaEventRecord(ev0, s));
@@ -959,6 +980,18 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
         st = launch_pair_ft<2>(in, nl->triclinic, s);
     if (st) return st;
     if (ev1) SPGNB_CUDA(cudaEventRecord(ev1, s));
+    return SPGNB_OK;
+}
+
+int force_pipeline(const ForceInputs& in, cudaStream_t s)
+{
+    spgnb_nl* nl = in.nl;
+    const int slots = nl->clusters_cap * kClusterSize;
+    int st = force_check(in);
+    if (!st) st = launch_pack(in, s, nullptr);
+    if (!st) st = launch_prune(in, s);
+    if (!st) st = launch_pair_kernel(in, s);
+    if (st) return st;
     const bool excl = in.xf.list != nullptr;
     const int blocks = (slots + 255) / 256;
     if (in.mode == 2)

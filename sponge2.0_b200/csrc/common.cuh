@@ -480,6 +480,15 @@ struct ForceInputs
     } clear;
 };
 int force_pipeline(const ForceInputs& in, cudaStream_t s);
+// The pipeline's stages, for callers that place them themselves (the
+// batched step): argument checks, the slot pack (gated on *gate when given),
+// the pruning (runs for the systems flagged), the pair kernel (forces into
+// the list's int64 staging, d_facc, which the finishing pass or the caller
+// turns into float forces and clears).
+int force_check(const ForceInputs& in);
+int launch_pack(const ForceInputs& in, cudaStream_t s, const int* gate);
+int launch_prune(const ForceInputs& in, cudaStream_t s);
+int launch_pair_kernel(const ForceInputs& in, cudaStream_t s);
 // The force kernel's coefficient table of a T x T square pair table {A, B}:
 // element (a*T + b)*T + j = {-A_aj, -A_bj, B_aj, B_bj}, the rows of an atom
 // pair (a, b) of a cluster against every partner type j.
@@ -566,22 +575,14 @@ enum BuildHow
 // aux: kBuildInterval - per-system steps done; kBuildPreset - per-system
 // flags of the systems to rebuild.  active (optional): per system, 0 = frozen
 // (no forced or interval rebuild).
-// Optional split of a queued build: the decision (which systems rebuild)
-// goes to the caller's stream; the build itself (binning to the finish) to
-// the stream body() returns, given the device flag that is non-zero when
-// some system rebuilds.  A graph capture makes that part the body of a
-// conditional node, so steps without a rebuild launch none of it; done()
-// closes the body and returns its status.  body() returns null on an
-// error, which done() then reports.
-struct BuildBody
-{
-    virtual cudaStream_t body(cudaStream_t s, const int* d_any) = 0;
-    virtual int done() = 0;
-    virtual ~BuildBody() = default;
-};
 int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
                    const int* ex_list, const int* ex_num, int how, cudaStream_t s, const int* d_aux = nullptr,
-                   int interval = 0, const int* d_active = nullptr, BuildBody* split = nullptr);
+                   int interval = 0, const int* d_active = nullptr);
+// The build without the decision: the caller has set the per-system need
+// flags and the counters' rebuild flag (every kernel returns at once when
+// that flag is zero).
+int nl_queue_build_body(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
+                        const int* ex_list, const int* ex_num, cudaStream_t s);
 int nl_regrow(spgnb_nl* nl, int flags);
 int nl_set_prune_rc(spgnb_nl* nl, float rc, cudaStream_t s);
 size_t nl_device_bytes(const spgnb_nl* nl);

@@ -1467,11 +1467,9 @@ int nl_create_multi(int n_systems, const int* atom_counts, const spgnb_ltmatrix3
 // systems flagged in aux.
 int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
                    const int* ex_list, const int* ex_num, int how, cudaStream_t s, const int* d_aux, int interval,
-                   const int* d_active, BuildBody* split)
+                   const int* d_active)
 {
-    const int sms = num_sms();
     const int slots_cap = nl->clusters_cap * kClusterSize;
-    const int ccap = nl->clusters_cap;
     const int sb = (nl->S + 255) / 256;
     if (how != kBuildSkin)
     {
@@ -1495,8 +1493,15 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
                                                                   d_crd, nl->d_slot_x0, nl->d_need, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_check_refresh");
     }
-    const cudaStream_t decided = s;
-    if (split && !(s = split->body(decided, nl->d_counters + kCntNeed))) return split->done();
+    return nl_queue_build_body(nl, n, d_crd, d_atom_local, ex_start, ex_list, ex_num, s);
+}
+
+int nl_queue_build_body(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_local, const int* ex_start,
+                        const int* ex_list, const int* ex_num, cudaStream_t s)
+{
+    const int sms = num_sms();
+    const int slots_cap = nl->clusters_cap * kClusterSize;
+    const int ccap = nl->clusters_cap;
     k_reset_list_counters<<<1, 1, 0, s>>>(nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_reset_list_counters");
     k_bin<<<(n + 255) / 256, 256, 0, s>>>(n, d_crd, nl->d_atom_sys, nl->d_sys, nl->d_atom_cell, nl->d_atom_shift,
@@ -1545,11 +1550,6 @@ int nl_queue_build(spgnb_nl* nl, int n, const float3* d_crd, const int* d_atom_l
     k_finish<<<(fin + 255) / 256, 256, 0, s>>>(nl->G, nl->S, nl->d_cell_sys, nl->d_need, nl->d_prune,
                                                   nl->d_cell_count, nl->d_cell_cursor, nl->d_counters);
     SPGNB_CHECK_LAUNCH("k_finish");
-    if (split)
-    {
-        const int st = split->done();
-        if (st) return st;
-    }
     nl->built = true;
     nl->local_atoms = n;
     nl->host_builds++;
