@@ -299,10 +299,12 @@ struct spgnb_nl
     int* d_tcount = nullptr;      // elements of each cluster's table
     float4* d_tab = nullptr;      // {D = centre difference (minimum image), neighbour slot base | image flag << 30}
     uint2* d_tmask = nullptr;     // 64-bit pair mask: bit a*8 + b = own slot a with neighbour slot b
-    // pruned per-cluster partner lists, list_cap words reserved per
-    // cluster: {partner slot | atom mask << 22 | image flag << 30}, an upper
-    // part from the start and a lower part from the end, each padded to
-    // 32-word windows; their lengths at d_pcount[8c], d_pcount[8c + 1]
+    // pruned per-cluster partner lists (the half list: partners in clusters
+    // J > I, and within I the pairs a < b), list_cap words reserved per
+    // cluster: {partner slot | atom mask << 22 | image flag << 30}, padded to
+    // 32-word windows; the length at d_pcount[8c] (a cluster near the start
+    // of a periodic box can hold nearly its whole neighbourhood, so the
+    // reserve is sized for that)
     unsigned* d_pwords = nullptr;
     int* d_pcount = nullptr;
     long long* d_facc = nullptr;  // per slot: the half-list kernel's int64 force sums (3), cleared after use
@@ -541,7 +543,7 @@ int nl_init_system(SysHost& sh, int atom_count, spgnb_ltmatrix3 cell, spgnb_ltma
 int nl_system_runs(const SysHost& sh, std::vector<int>& run_start, std::vector<int2>& runs);
 // Table and pruned-list capacities for a system of this density and cutoff.
 // Words reserved per cluster for a pruned list of per_cluster partners
-// (margin and room for padding both parts to whole windows).
+// (with a margin and room for the padding to whole windows).
 int list_cap_for(double per_cluster);
 void nl_capacity_for(double atoms_per_A3, double atom_count, float cutoff, float skin, float prune_buffer,
                      double* table_per_cluster, double* words_per_cluster);
