@@ -348,7 +348,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
 // partner-owned sums go to the partner's int64 staging, 8 atomic adds; the
 // finishing pass turns the staging into the per-atom arrays and totals.
 template <int MODE, int FIT, bool TRI>
-__global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : (MODE == 1 ? 5 : 6))
+__global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : (MODE == 1 ? 5 : 7))
     k_pair8(ForceParams p0, const ForceParams* __restrict__ fps, const SysDesc* __restrict__ sys, int n_clusters,
             int list_cap, const int* __restrict__ cl_sys, const int* __restrict__ lcount,
             const unsigned* __restrict__ words, const int4* __restrict__ cl_q, const float4* __restrict__ pos,
