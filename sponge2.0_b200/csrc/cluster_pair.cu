@@ -578,7 +578,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : (MODE == 1 ? 
             if (PA)
             {
                 // the partner's owned sums over this word: raw fixed point to
-                // its staging (scaled in the finishing pass)
+                // its staging (scaled in the finishing pass), one quantity
+                // after another so that a warp's adds fall on few lines
                 float js[8];
                 bool any = false;
 #pragma unroll
@@ -589,12 +590,13 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : (MODE == 1 ? 
                 }
                 if (any)
                 {
-                    unsigned long long* oa = (unsigned long long*)(oacc + 8 * (size_t)jc);
+                    unsigned long long* oa = (unsigned long long*)(oacc + jc);
+                    const size_t ostride = (size_t)n_clusters * kClusterSize;
 #pragma unroll
                     for (int q = 0; q < 8; q++)
                     {
                         const long long v = __float2ll_rn(js[q] * kTwoPow32);
-                        if (v) atomicAdd(oa + q, (unsigned long long)v);
+                        if (v) atomicAdd(oa + q * ostride, (unsigned long long)v);
                     }
                 }
             }
@@ -665,7 +667,8 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : (MODE == 1 ? 
                 const float val = reduce_scatter8(v, lane);
                 const long long r = __float2ll_rn(val * kTwoPow32);
                 if ((lane & 3) == 0 && r)
-                    atomicAdd((unsigned long long*)(oacc + 8 * (size_t)(s0 + a) + va), (unsigned long long)r);
+                    atomicAdd((unsigned long long*)(oacc + (size_t)va * n_clusters * kClusterSize + (s0 + a)),
+                              (unsigned long long)r);
             }
         }
     }
@@ -730,19 +733,19 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
         }
         if (PA)
         {
-            long long* q = oacc + 8 * (size_t)s;
+            long long* q = oacc + s;
             long long r[8];
             long long any = 0;
 #pragma unroll
             for (int k = 0; k < 8; k++)
             {
-                r[k] = q[k];
+                r[k] = q[(size_t)k * slots];
                 any |= r[k];
             }
             if (any)
             {
 #pragma unroll
-                for (int k = 0; k < 8; k++) q[k] = 0;
+                for (int k = 0; k < 8; k++) q[(size_t)k * slots] = 0;
                 // raw sums: -12 E_lj, E_c, and +g (x) d; the virial is -g (x) d
                 // with the symmetric off-diagonal terms twice the one summed
                 double v[8];

@@ -308,7 +308,10 @@ struct spgnb_nl
     unsigned* d_pwords = nullptr;
     int* d_pcount = nullptr;
     long long* d_facc = nullptr;  // per slot: the half-list kernel's int64 force sums (3), cleared after use
-    long long* d_oacc = nullptr;  // per slot: owned energy/virial sums of the per-atom mode (8), cleared after use
+    // owned energy/virial sums of the per-atom mode, 8 per slot, cleared after
+    // use; quantity-major (sum q of slot s at q * slot capacity + s), so the
+    // lanes' adds of one quantity for consecutive partner slots share lines
+    long long* d_oacc = nullptr;
     float4* d_pref = nullptr;     // slot offsets at the last pruning
     int* d_counters = nullptr;
     // reference-layout export
