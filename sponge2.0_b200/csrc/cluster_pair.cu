@@ -694,80 +694,75 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : (MODE == 1 ? 
     }
 }
 
-// Finishing pass, one thread per slot: the half-list kernel's int64 force
-// sums go to the caller's float array, and its owned energy/virial sums
-// (per-atom mode) to the caller's per-atom arrays and the totals, the
-// staging cleared for the next call.  With the fused PME excluded-pair
-// correction each atom also adds its excluded pairs' terms
+// The fused PME excluded-pair correction of atom a
 // (Particle_Mesh::PME_Excluded_Force_With_Atom_Energy, PM_force.cpp:918-997):
 // its symmetric exclusion list holds both sides of every pair, so each atom
 // computes its own share, F_a += q_a q_x beta^3 h(beta r) dr with dr = the
 // reference's minimum image of r_x - r_a, and the pair's owner (lower global
 // index) adds -q_a q_x erf(beta r)/r to the energy and -F (x) dr to its
-// virial.  A thread touches only its own atom's force.
-template <bool EXCL, bool EN, bool PA>
+// virial (wv: xx, xy, yy, xz, yz, zz).
+template <bool EN>
+__device__ __forceinline__ void excl_terms(int a, const SysDesc& D, const ExclFuse& xf, float& fx, float& fy,
+                                           float& fz, float& eown, float (&wv)[6])
+{
+    const int2 sn = xf.sn[a];
+    const float3 ri = xf.crd[a];
+    const float qa = xf.charge[a];
+    const int ga = xf.atom_local[a];
+    for (int k = 0; k < sn.y; k++)
+    {
+        const int jx = xf.list[sn.x + k];
+        const float3 rj = xf.crd[jx];
+        float ex = rj.x - ri.x, ey = rj.y - ri.y, ez = rj.z - ri.z;
+        const float tx = floorf(ex * D.rcell.a11 + ey * D.rcell.a21 + ez * D.rcell.a31 + 0.5f);
+        const float ty = floorf(ey * D.rcell.a22 + ez * D.rcell.a32 + 0.5f);
+        const float tz = floorf(ez * D.rcell.a33 + 0.5f);
+        ex -= tx * D.cell.a11 + ty * D.cell.a21 + tz * D.cell.a31;
+        ey -= ty * D.cell.a22 + tz * D.cell.a32;
+        ez -= tz * D.cell.a33;
+        const float er = sqrtf(ex * ex + ey * ey + ez * ez);
+        const float xb = xf.beta * er;
+        const float qq = qa * xf.charge[jx];
+        const float fa = qq * xf.beta3 * excl_h(xb);
+        const float gx = fa * ex, gy = fa * ey, gz = fa * ez;
+        fx += gx;
+        fy += gy;
+        fz += gz;
+        if (EN && ga < xf.atom_local[jx])
+        {
+            eown -= qq * erff(xb) / er;
+            wv[0] -= gx * ex;
+            wv[1] -= gx * ey + gy * ex;
+            wv[2] -= gy * ey;
+            wv[3] -= gx * ez + gz * ex;
+            wv[4] -= gy * ez + gz * ey;
+            wv[5] -= gz * ez;
+        }
+    }
+}
+
+// Finishing pass of the force and totals modes, one thread per slot: the
+// half-list kernel's int64 force sums go to the caller's float array, the
+// staging cleared for the next call; with EXCL each atom also adds its
+// excluded pairs' correction (and, with EN, its owned energy to the total).
+// A thread touches only its own atom's force.
+template <bool EXCL, bool EN>
 __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* __restrict__ cl_sys,
-                       const SysDesc* __restrict__ sys, long long* __restrict__ facc, long long* __restrict__ oacc,
-                       float3* __restrict__ frc, long long* __restrict__ totals, OwnerMap om, PerAtomOut pa,
+                       const SysDesc* __restrict__ sys, long long* __restrict__ facc, float3* __restrict__ frc,
                        ExclFuse xf)
 {
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     float ene = 0.0f;
-    long long tq[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // this slot's share of the totals (per-atom mode)
     if (s < slots)
     {
         const int a = slot_atom[s];
-        long long x = 0, y = 0, z = 0;
-        if (facc)
+        long long* q = facc + 3 * (size_t)s;
+        const long long x = q[0], y = q[1], z = q[2];
+        if (x | y | z)
         {
-            long long* q = facc + 3 * (size_t)s;
-            x = q[0];
-            y = q[1];
-            z = q[2];
-            if (x | y | z)
-            {
-                q[0] = 0;
-                q[1] = 0;
-                q[2] = 0;
-            }
-        }
-        if (PA)
-        {
-            long long* q = oacc + s;
-            long long r[8];
-            long long any = 0;
-#pragma unroll
-            for (int k = 0; k < 8; k++)
-            {
-                r[k] = q[(size_t)k * slots];
-                any |= r[k];
-            }
-            if (any)
-            {
-#pragma unroll
-                for (int k = 0; k < 8; k++) q[(size_t)k * slots] = 0;
-                // raw sums: -12 E_lj, E_c, and +g (x) d; the virial is -g (x) d
-                // with the symmetric off-diagonal terms twice the one summed
-                double v[8];
-#pragma unroll
-                for (int k = 0; k < 8; k++)
-                {
-                    const double sg = k == 0 ? (double)kLjEnergyScale
-                                             : (k == 1 ? 1.0 : ((k == 3 || k == 5 || k == 6) ? -2.0 : -1.0));
-                    v[k] = (double)r[k] * sg;
-                    tq[k] = __double2ll_rn(v[k]);
-                }
-                if (a >= 0)
-                {
-                    const int o = om.remap(a);
-                    const float elj = (float)(v[0] * kForceUnscale), ec = (float)(v[1] * kForceUnscale);
-                    if (pa.energy) atomicAdd(pa.energy + o, elj + ec);
-                    if (pa.lj_energy) atomicAdd(pa.lj_energy + o, elj);
-                    if (pa.direct) atomicAdd(pa.direct + o, ec);
-                    if (pa.virial)
-                        for (int k = 0; k < 6; k++) atomicAdd(pa.virial + 6 * (size_t)o + k, (float)(v[2 + k] * kForceUnscale));
-                }
-            }
+            q[0] = 0;
+            q[1] = 0;
+            q[2] = 0;
         }
         if (a >= 0)
         {
@@ -775,50 +770,8 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
                   fz = (float)((double)z * kForceUnscale);
             if (EXCL)
             {
-                const SysDesc& D = sys[cl_sys[s >> 3]];
-                const int2 sn = xf.sn[a];
-                const float3 ri = xf.crd[a];
-                const float qa = xf.charge[a];
-                const int ga = xf.atom_local[a];
                 float wv[6] = {0, 0, 0, 0, 0, 0};
-                float eown = 0.0f;
-                for (int k = 0; k < sn.y; k++)
-                {
-                    const int jx = xf.list[sn.x + k];
-                    const float3 rj = xf.crd[jx];
-                    float ex = rj.x - ri.x, ey = rj.y - ri.y, ez = rj.z - ri.z;
-                    const float tx = floorf(ex * D.rcell.a11 + ey * D.rcell.a21 + ez * D.rcell.a31 + 0.5f);
-                    const float ty = floorf(ey * D.rcell.a22 + ez * D.rcell.a32 + 0.5f);
-                    const float tz = floorf(ez * D.rcell.a33 + 0.5f);
-                    ex -= tx * D.cell.a11 + ty * D.cell.a21 + tz * D.cell.a31;
-                    ey -= ty * D.cell.a22 + tz * D.cell.a32;
-                    ez -= tz * D.cell.a33;
-                    const float er = sqrtf(ex * ex + ey * ey + ez * ez);
-                    const float xb = xf.beta * er;
-                    const float qq = qa * xf.charge[jx];
-                    const float fa = qq * xf.beta3 * excl_h(xb);
-                    const float gx = fa * ex, gy = fa * ey, gz = fa * ez;
-                    fx += gx;
-                    fy += gy;
-                    fz += gz;
-                    if (EN && ga < xf.atom_local[jx])
-                    {
-                        eown -= qq * erff(xb) / er;
-                        wv[0] -= gx * ex;
-                        wv[1] -= gx * ey + gy * ex;
-                        wv[2] -= gy * ey;
-                        wv[3] -= gx * ez + gz * ex;
-                        wv[4] -= gy * ez + gz * ey;
-                        wv[5] -= gz * ez;
-                    }
-                }
-                if (EN)
-                {
-                    ene = eown;
-                    if (xf.energy && eown != 0.0f) atomicAdd(xf.energy + a, eown);
-                    if (xf.virial && sn.y > 0)
-                        for (int q = 0; q < 6; q++) atomicAdd(xf.virial + 6 * (size_t)a + q, wv[q]);
-                }
+                excl_terms<EN>(a, sys[cl_sys[s >> 3]], xf, fx, fy, fz, ene, wv);
             }
             if (fx != 0.0f || fy != 0.0f || fz != 0.0f)
             {
@@ -830,26 +783,132 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
             }
         }
     }
-    if (PA)
-    {
-        // the totals (the per-atom mode runs on one system): summed over the
-        // warp by shuffles, over the block in shared memory, one atomic per
-        // value and block
-        __shared__ long long bsum[8];
-        if (threadIdx.x < 8) bsum[threadIdx.x] = 0;
-        __syncthreads();
-#pragma unroll
-        for (int k = 0; k < 8; k++)
-        {
-            long long v = tq[k];
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-            if ((threadIdx.x & 31) == 0 && v) atomicAdd((unsigned long long*)&bsum[k], (unsigned long long)v);
-        }
-        __syncthreads();
-        if (threadIdx.x < 8 && bsum[threadIdx.x])
-            atomicAdd((unsigned long long*)&totals[threadIdx.x], (unsigned long long)bsum[threadIdx.x]);
-    }
     if (EXCL && EN)
+    {
+        // the correction's energy total: one atomic per warp
+        long long qe = __double2ll_rn((double)ene * kEnergyScale);
+        for (int o = 16; o > 0; o >>= 1) qe += __shfl_xor_sync(0xffffffffu, qe, o);
+        if ((threadIdx.x & 31) == 0 && qe) atomicAdd((unsigned long long*)xf.total, (unsigned long long)qe);
+    }
+}
+
+// Finishing pass of the per-atom mode (one system), one thread per local
+// atom a: its force from its slot's staging; the owned energy and virial of
+// a itself, or, for the first atom of a water of the solvent tail, of every
+// site of the residue (SOLVENT_LENNARD_JONES credits the residue's first
+// atom), summed exactly in int64 from the sites' slots, go to the per-atom
+// arrays by plain read-modify-writes (each element has one writer, so the
+// result does not depend on thread order) and to the totals; the staging
+// read is cleared for the next call.  With EXCL the atom's excluded-pair
+// correction is added as in k_fin8.
+template <bool EXCL>
+__global__ void k_fin8_atoms(int n, int slots, const int* __restrict__ atom_slot, const int* __restrict__ cl_sys,
+                             const SysDesc* __restrict__ sys, long long* __restrict__ facc,
+                             long long* __restrict__ oacc, float3* __restrict__ frc, long long* __restrict__ totals,
+                             OwnerMap om, PerAtomOut pa, ExclFuse xf)
+{
+    const int a = blockIdx.x * blockDim.x + threadIdx.x;
+    float ene = 0.0f;
+    long long tq[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // this atom's share of the totals
+    if (a < n)
+    {
+        const int s = atom_slot[a];
+        long long* q = facc + 3 * (size_t)s;
+        const long long x = q[0], y = q[1], z = q[2];
+        if (x | y | z)
+        {
+            q[0] = 0;
+            q[1] = 0;
+            q[2] = 0;
+        }
+        // the sites whose owned sums a receives
+        int sites = 1;
+        if (a >= om.solvent_start)
+            sites = (a - om.solvent_start) % om.water_points ? 0 : min(om.water_points, n - a);
+        long long r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        for (int k = 0; k < sites; k++)
+        {
+            long long* o = oacc + (k ? atom_slot[a + k] : s);
+#pragma unroll
+            for (int u = 0; u < 8; u++)
+            {
+                const long long v = o[(size_t)u * slots];
+                if (v)
+                {
+                    r[u] += v;
+                    o[(size_t)u * slots] = 0;
+                }
+            }
+        }
+        // raw sums: -12 E_lj, E_c, and +g (x) d; the virial is -g (x) d with
+        // the symmetric off-diagonal terms twice the one summed
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++)
+        {
+            const double sg = u == 0 ? (double)kLjEnergyScale
+                                     : (u == 1 ? 1.0 : ((u == 3 || u == 5 || u == 6) ? -2.0 : -1.0));
+            v[u] = (double)r[u] * sg;
+            tq[u] = __double2ll_rn(v[u]);
+        }
+        const float elj = (float)(v[0] * kForceUnscale), ec = (float)(v[1] * kForceUnscale);
+        float wv[6];
+#pragma unroll
+        for (int u = 0; u < 6; u++) wv[u] = (float)(v[2 + u] * kForceUnscale);
+        float fx = (float)((double)x * kForceUnscale), fy = (float)((double)y * kForceUnscale),
+              fz = (float)((double)z * kForceUnscale);
+        float xe = 0.0f;
+        float xw[6] = {0, 0, 0, 0, 0, 0};
+        if (EXCL) excl_terms<true>(a, sys[cl_sys[s >> 3]], xf, fx, fy, fz, xe, xw);
+        ene = xe;
+        if (fx != 0.0f || fy != 0.0f || fz != 0.0f)
+        {
+            float3 f = frc[a];
+            f.x += fx;
+            f.y += fy;
+            f.z += fz;
+            frc[a] = f;
+        }
+        if (sites)
+        {
+            if (pa.energy) pa.energy[a] += elj + ec;
+            if (pa.lj_energy) pa.lj_energy[a] += elj;
+            if (pa.direct) pa.direct[a] += ec;
+            if (pa.virial)
+            {
+                float* w = pa.virial + 6 * (size_t)a;
+#pragma unroll
+                for (int u = 0; u < 6; u++) w[u] += wv[u];
+            }
+        }
+        if (EXCL)
+        {
+            // the correction's own adds (its arrays may be the same ones)
+            if (xf.energy && xe != 0.0f) xf.energy[a] += xe;
+            if (xf.virial && xf.sn[a].y > 0)
+            {
+                float* w = xf.virial + 6 * (size_t)a;
+#pragma unroll
+                for (int u = 0; u < 6; u++) w[u] += xw[u];
+            }
+        }
+    }
+    // the totals: summed over the warp by shuffles, over the block in shared
+    // memory, one atomic per value and block
+    __shared__ long long bsum[8];
+    if (threadIdx.x < 8) bsum[threadIdx.x] = 0;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 8; k++)
+    {
+        long long v = tq[k];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd((unsigned long long*)&bsum[k], (unsigned long long)v);
+    }
+    __syncthreads();
+    if (threadIdx.x < 8 && bsum[threadIdx.x])
+        atomicAdd((unsigned long long*)&totals[threadIdx.x], (unsigned long long)bsum[threadIdx.x]);
+    if (EXCL)
     {
         // the correction's energy total: one atomic per warp
         long long qe = __double2ll_rn((double)ene * kEnergyScale);
@@ -999,25 +1058,24 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
     const int blocks = (slots + 255) / 256;
     if (in.mode == 2)
     {
+        const int n = nl->local_atoms;
+        const int ab = (n + 255) / 256;
         if (excl)
-            k_fin8<true, true, true><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
-                                                            nl->d_facc, nl->d_oacc, in.frc, in.totals, in.om, in.pa,
-                                                            in.xf);
+            k_fin8_atoms<true><<<ab, 256, 0, s>>>(n, slots, nl->d_atom_slot, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+                                                  nl->d_oacc, in.frc, in.totals, in.om, in.pa, in.xf);
         else
-            k_fin8<false, true, true><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
-                                                             nl->d_facc, nl->d_oacc, in.frc, in.totals, in.om, in.pa,
-                                                             in.xf);
+            k_fin8_atoms<false><<<ab, 256, 0, s>>>(n, slots, nl->d_atom_slot, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+                                                   nl->d_oacc, in.frc, in.totals, in.om, in.pa, in.xf);
     }
     else if (excl && in.mode == 1)
-        k_fin8<true, true, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc,
-                                                         nullptr, in.frc, in.totals, in.om, in.pa, in.xf);
+        k_fin8<true, true><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc, in.frc,
+                                                  in.xf);
     else if (excl)
-        k_fin8<true, false, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
-                                                          nl->d_facc, nullptr, in.frc, in.totals, in.om, in.pa, in.xf);
+        k_fin8<true, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+                                                   in.frc, in.xf);
     else
-        k_fin8<false, false, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys,
-                                                           nl->d_facc, nullptr, in.frc, in.totals, in.om, in.pa,
-                                                           in.xf);
+        k_fin8<false, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+                                                    in.frc, in.xf);
     SPGNB_CHECK_LAUNCH("k_fin8");
     return SPGNB_OK;
 }
