@@ -796,11 +796,11 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
 // atom a: its force from its slot's staging; the owned energy and virial of
 // a itself, or, for the first atom of a water of the solvent tail, of every
 // site of the residue (SOLVENT_LENNARD_JONES credits the residue's first
-// atom), summed exactly in int64 from the sites' slots, go to the per-atom
-// arrays by plain read-modify-writes (each element has one writer, so the
-// result does not depend on thread order) and to the totals; the staging
-// read is cleared for the next call.  With EXCL the atom's excluded-pair
-// correction is added as in k_fin8.
+// atom; three or four sites), summed exactly in int64 from the sites'
+// slots, go to the per-atom arrays by plain read-modify-writes (each element
+// has one writer, so the result does not depend on thread order) and to the
+// totals; the staging read is cleared for the next call.  With EXCL the
+// atom's excluded-pair correction is added as in k_fin8.
 template <bool EXCL>
 __global__ void k_fin8_atoms(int n, int slots, const int* __restrict__ atom_slot, const int* __restrict__ cl_sys,
                              const SysDesc* __restrict__ sys, long long* __restrict__ facc,
@@ -812,34 +812,51 @@ __global__ void k_fin8_atoms(int n, int slots, const int* __restrict__ atom_slot
     long long tq[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // this atom's share of the totals
     if (a < n)
     {
-        const int s = atom_slot[a];
-        long long* q = facc + 3 * (size_t)s;
+        // every load first (they do not depend on each other beyond the
+        // slots), then the arithmetic, then the stores: a thread waits for
+        // memory about twice
+        int sites = 1;  // the sites whose owned sums a receives
+        if (a >= om.solvent_start)
+            sites = (a - om.solvent_start) % om.water_points ? 0 : min(min(om.water_points, n - a), 4);
+        int sl[4];
+        sl[0] = atom_slot[a];
+#pragma unroll
+        for (int k = 1; k < 4; k++) sl[k] = k < sites ? atom_slot[a + k] : 0;
+        long long* q = facc + 3 * (size_t)sl[0];
         const long long x = q[0], y = q[1], z = q[2];
+        long long r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+            if (k < sites)
+            {
+#pragma unroll
+                for (int u = 0; u < 8; u++) r[u] += oacc[(size_t)u * slots + sl[k]];
+            }
+        const float3 f0 = frc[a];
+        const bool own = sites > 0;
+        const float e0 = own && pa.energy ? pa.energy[a] : 0.0f;
+        const float l0 = own && pa.lj_energy ? pa.lj_energy[a] : 0.0f;
+        const float d0 = own && pa.direct ? pa.direct[a] : 0.0f;
+        float w0[6] = {0, 0, 0, 0, 0, 0};
+        if (own && pa.virial)
+        {
+#pragma unroll
+            for (int u = 0; u < 6; u++) w0[u] = pa.virial[6 * (size_t)a + u];
+        }
+        // the staging read is cleared for the next call
         if (x | y | z)
         {
             q[0] = 0;
             q[1] = 0;
             q[2] = 0;
         }
-        // the sites whose owned sums a receives
-        int sites = 1;
-        if (a >= om.solvent_start)
-            sites = (a - om.solvent_start) % om.water_points ? 0 : min(om.water_points, n - a);
-        long long r[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-        for (int k = 0; k < sites; k++)
-        {
-            long long* o = oacc + (k ? atom_slot[a + k] : s);
 #pragma unroll
-            for (int u = 0; u < 8; u++)
+        for (int k = 0; k < 4; k++)
+            if (k < sites)
             {
-                const long long v = o[(size_t)u * slots];
-                if (v)
-                {
-                    r[u] += v;
-                    o[(size_t)u * slots] = 0;
-                }
+#pragma unroll
+                for (int u = 0; u < 8; u++) oacc[(size_t)u * slots + sl[k]] = 0;
             }
-        }
         // raw sums: -12 E_lj, E_c, and +g (x) d; the virial is -g (x) d with
         // the symmetric off-diagonal terms twice the one summed
         double v[8];
@@ -852,33 +869,22 @@ __global__ void k_fin8_atoms(int n, int slots, const int* __restrict__ atom_slot
             tq[u] = __double2ll_rn(v[u]);
         }
         const float elj = (float)(v[0] * kForceUnscale), ec = (float)(v[1] * kForceUnscale);
-        float wv[6];
-#pragma unroll
-        for (int u = 0; u < 6; u++) wv[u] = (float)(v[2 + u] * kForceUnscale);
         float fx = (float)((double)x * kForceUnscale), fy = (float)((double)y * kForceUnscale),
               fz = (float)((double)z * kForceUnscale);
         float xe = 0.0f;
         float xw[6] = {0, 0, 0, 0, 0, 0};
-        if (EXCL) excl_terms<true>(a, sys[cl_sys[s >> 3]], xf, fx, fy, fz, xe, xw);
+        if (EXCL) excl_terms<true>(a, sys[cl_sys[sl[0] >> 3]], xf, fx, fy, fz, xe, xw);
         ene = xe;
-        if (fx != 0.0f || fy != 0.0f || fz != 0.0f)
+        if (fx != 0.0f || fy != 0.0f || fz != 0.0f) frc[a] = make_float3(f0.x + fx, f0.y + fy, f0.z + fz);
+        if (own)
         {
-            float3 f = frc[a];
-            f.x += fx;
-            f.y += fy;
-            f.z += fz;
-            frc[a] = f;
-        }
-        if (sites)
-        {
-            if (pa.energy) pa.energy[a] += elj + ec;
-            if (pa.lj_energy) pa.lj_energy[a] += elj;
-            if (pa.direct) pa.direct[a] += ec;
+            if (pa.energy) pa.energy[a] = e0 + (elj + ec);
+            if (pa.lj_energy) pa.lj_energy[a] = l0 + elj;
+            if (pa.direct) pa.direct[a] = d0 + ec;
             if (pa.virial)
             {
-                float* w = pa.virial + 6 * (size_t)a;
 #pragma unroll
-                for (int u = 0; u < 6; u++) w[u] += wv[u];
+                for (int u = 0; u < 6; u++) pa.virial[6 * (size_t)a + u] = w0[u] + (float)(v[2 + u] * kForceUnscale);
             }
         }
         if (EXCL)

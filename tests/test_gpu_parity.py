@@ -108,6 +108,24 @@ def test_bitwise_reproducible(torch_cuda):
     assert torch_cuda.equal(a, c)
 
 
+def test_per_atom_outputs_bitwise_reproducible(torch_cuda):
+    """The per-atom energies and virials (a water's sites summed into its
+    first atom) come out bitwise the same on every call: the staging sums in
+    int64 and each per-atom element has one writer."""
+    s = SYSTEMS["mixed-small"]()
+    p = _path(s)
+    runs = []
+    for k in range(3):
+        if k == 2:
+            p.update(0, forced=True)
+        f = p.force(need_energy=True, need_virial=True).clone()
+        runs.append((f, p.atom_energy.clone(), p.atom_virial.clone(), p.atom_direct.clone(), p.lj.totals()))
+    for r in runs[1:]:
+        for x, y in zip(runs[0][:4], r[:4]):
+            assert torch_cuda.equal(x, y)
+        assert np.array_equal(runs[0][4], r[4])
+
+
 def test_atom_group_path_matches(torch_cuda, oracle):
     """The reference-layout entry point over the exported list gives the same
     forces (generic kernel for solutes, solvent module for waters)."""
