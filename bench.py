@@ -119,6 +119,26 @@ def parse():
     return p.parse_args()
 
 
+def rank_reduce(maxes, sums, dist, device):
+    """Across the ranks: the max of each value of `maxes` (device times) and
+    the sum of each of `sums` (work done); as given on one rank (dist None).
+    Every rank passes lists of the same lengths, so all take the same
+    collectives in the same order."""
+    maxes, sums = [float(x) for x in maxes], [float(x) for x in sums]
+    if dist is None:
+        return maxes, sums
+    import torch
+    if maxes:
+        tm = torch.tensor(maxes, dtype=torch.float64, device=device)
+        dist.all_reduce(tm, op=dist.ReduceOp.MAX)
+        maxes = tm.tolist()
+    if sums:
+        ts = torch.tensor(sums, dtype=torch.float64, device=device)
+        dist.all_reduce(ts, op=dist.ReduceOp.SUM)
+        sums = ts.tolist()
+    return maxes, sums
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -339,16 +359,7 @@ def batched_measure(systems_all, K, W, world, rank, local, dist, k_plain=None):
         plain_as += s.n * k_plain
         b.close()
     B.close()
-    if dist is not None:
-        t = torch.tensor([ms, plain_ms, float(atoms), float(plain_as)], dtype=torch.float64, device="cuda")
-        tmax = t[:2].clone()
-        dist.all_reduce(tmax, op=dist.ReduceOp.MAX)
-        tsum = t[2:].clone()
-        dist.all_reduce(tsum, op=dist.ReduceOp.SUM)
-        ms, plain_ms = float(tmax[0]), float(tmax[1])
-        atoms_all, plain_as_all = float(tsum[0]), float(tsum[1])
-    else:
-        atoms_all, plain_as_all = float(atoms), float(plain_as)
+    (ms, plain_ms), (atoms_all, plain_as_all) = rank_reduce([ms, plain_ms], [atoms, plain_as], dist, "cuda")
     value = atoms_all * K / (ms * 1e-3)
     plain = plain_as_all / (plain_ms * 1e-3)
     return {"value": value, "ms": ms, "K": K, "W": W, "systems": len(systems_all), "systems_per_gpu": len(mine),
@@ -638,10 +649,7 @@ def main():
     if main_box:
         extras = _main_box_extras(path, s, dev, stream, flush, world, rank, local, dist, args)
 
-    if dist is not None:
-        t = torch.tensor([total_ms, e2e_total], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_total = float(t[0]), float(t[1])
+    (total_ms, e2e_total), _ = rank_reduce([total_ms, e2e_total], [], dist, dev)
 
     from spgnb._lib import NLStats
     st = NLStats()
