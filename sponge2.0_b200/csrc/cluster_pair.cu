@@ -59,6 +59,7 @@ __global__ void k_pack_slots(int slots_cap, int* counters, const int* __restrict
                              float* __restrict__ clear_a, float* __restrict__ clear_b, int clear_n,
                              const int* __restrict__ gate)
 {
+    grid_dep_wait();
     if (gate && *gate == 0) return;
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     bool moved = false;
@@ -127,6 +128,7 @@ __global__ void __launch_bounds__(kPruneWarps * 32)
              const float4* __restrict__ pos, float4* __restrict__ pref, int* __restrict__ lcount,
              unsigned* __restrict__ words, int n_sys, int* __restrict__ prune)
 {
+    grid_dep_wait();
     if (counters[kCntPrune] == 0) return;
     // a chunk's candidates {partner slot | image flag, element lane | own-atom bits << 5}
     __shared__ uint2 buf[kPruneWarps][kChunk * kClusterSize];
@@ -356,6 +358,7 @@ __global__ void __launch_bounds__(kPairWarps * 32, MODE == 2 ? 3 : (MODE == 1 ? 
             long long* __restrict__ oacc, long long* __restrict__ totals, const int* __restrict__ only,
             int* __restrict__ counters, int max_types)
 {
+    grid_dep_wait();
     constexpr bool EN = MODE >= 1;
     constexpr bool PA = MODE >= 2;
     constexpr int NP = 4;        // the cluster's 8 atoms as packed pairs
@@ -751,6 +754,7 @@ __global__ void k_fin8(int slots, const int* __restrict__ slot_atom, const int* 
                        const SysDesc* __restrict__ sys, long long* __restrict__ facc, float3* __restrict__ frc,
                        ExclFuse xf)
 {
+    grid_dep_wait();
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     float ene = 0.0f;
     if (s < slots)
@@ -807,6 +811,7 @@ __global__ void k_fin8_atoms(int n, int slots, const int* __restrict__ atom_slot
                              long long* __restrict__ oacc, float3* __restrict__ frc, long long* __restrict__ totals,
                              OwnerMap om, PerAtomOut pa, ExclFuse xf)
 {
+    grid_dep_wait();
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     float ene = 0.0f;
     long long tq[8] = {0, 0, 0, 0, 0, 0, 0, 0};  // this atom's share of the totals
@@ -949,7 +954,7 @@ int launch_pair(const ForceInputs& in, cudaStream_t s)
     if (smem > 48 * 1024)
         SPGNB_CUDA(cudaFuncSetAttribute(k_pair8<M, F, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                         (int)smem));
-    k_pair8<M, F, T><<<grid, kPairWarps * 32, smem, s>>>(
+    launch_dependent(k_pair8<M, F, T>, grid, kPairWarps * 32, smem, s,
         in.p0, in.d_fps, nl->d_sys, nl->clusters_cap, nl->list_cap, nl->d_cl_sys, nl->d_pcount, nl->d_pwords,
         nl->d_cl_q, in.slot_pos, in.slot_aux, in.t4, nl->d_facc, nl->d_oacc, in.totals, in.only, nl->d_counters, mt);
     SPGNB_CHECK_LAUNCH("k_pair8");
@@ -1009,7 +1014,7 @@ int launch_pack(const ForceInputs& in, cudaStream_t s, const int* gate)
     const int slots = nl->clusters_cap * kClusterSize;
     const bool track = nl->opt.prune_buffer > 0.0f;
     const float half = 0.5f * nl->opt.prune_buffer;
-    k_pack_slots<<<(slots + 256) / 256, 256, 0, s>>>(slots, nl->d_counters, nl->d_slot_atom, nl->d_slot_gid,
+    launch_dependent(k_pack_slots, (slots + 256) / 256, 256, 0, s, slots, nl->d_counters, nl->d_slot_atom, nl->d_slot_gid,
                                                      nl->d_cl_sys, nl->d_sys, nl->d_cl_q, nl->d_slot_x0,
                                                      nl->d_slot_d0, in.crd, in.charge, in.atom_type, in.slot_pos,
                                                      in.slot_aux, track ? nl->d_pref : nullptr, half * half,
@@ -1024,7 +1029,7 @@ int launch_prune(const ForceInputs& in, cudaStream_t s)
     spgnb_nl* nl = in.nl;
     const int prune_bps = in.prune_blocks_per_sm > 0 ? in.prune_blocks_per_sm : 5;
     const int grid = std::max(1, std::min(num_sms() * prune_bps, (nl->clusters_cap + kPruneWarps - 1) / kPruneWarps));
-    k_prune8<<<grid, kPruneWarps * 32, 0, s>>>(in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters,
+    launch_dependent(k_prune8, grid, kPruneWarps * 32, 0, s, in.p0, in.d_fps, nl->opt.prune_buffer, nl->d_counters,
                                                nl->clusters_cap, nl->table_cap, nl->list_cap,
                                                nl->d_cl_sys, nl->d_sys, nl->d_tcount, nl->d_tab, nl->d_tmask,
                                                in.slot_pos, nl->d_pref, nl->d_pcount, nl->d_pwords, nl->S,
@@ -1067,20 +1072,20 @@ int force_pipeline(const ForceInputs& in, cudaStream_t s)
         const int n = nl->local_atoms;
         const int ab = (n + 255) / 256;
         if (excl)
-            k_fin8_atoms<true><<<ab, 256, 0, s>>>(n, slots, nl->d_atom_slot, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+            launch_dependent(k_fin8_atoms<true>, ab, 256, 0, s, n, slots, nl->d_atom_slot, nl->d_cl_sys, nl->d_sys, nl->d_facc,
                                                   nl->d_oacc, in.frc, in.totals, in.om, in.pa, in.xf);
         else
-            k_fin8_atoms<false><<<ab, 256, 0, s>>>(n, slots, nl->d_atom_slot, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+            launch_dependent(k_fin8_atoms<false>, ab, 256, 0, s, n, slots, nl->d_atom_slot, nl->d_cl_sys, nl->d_sys, nl->d_facc,
                                                    nl->d_oacc, in.frc, in.totals, in.om, in.pa, in.xf);
     }
     else if (excl && in.mode == 1)
-        k_fin8<true, true><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc, in.frc,
+        launch_dependent(k_fin8<true, true>, blocks, 256, 0, s, slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc, in.frc,
                                                   in.xf);
     else if (excl)
-        k_fin8<true, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+        launch_dependent(k_fin8<true, false>, blocks, 256, 0, s, slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc,
                                                    in.frc, in.xf);
     else
-        k_fin8<false, false><<<blocks, 256, 0, s>>>(slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc,
+        launch_dependent(k_fin8<false, false>, blocks, 256, 0, s, slots, nl->d_slot_atom, nl->d_cl_sys, nl->d_sys, nl->d_facc,
                                                     in.frc, in.xf);
     SPGNB_CHECK_LAUNCH("k_fin8");
     return SPGNB_OK;

@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <map>
+#include <utility>
 #include <set>
 #include <string>
 #include <vector>
@@ -41,6 +42,39 @@ bool sync_check();
         if (e__ == cudaSuccess && ::spgnb::sync_check()) e__ = cudaDeviceSynchronize(); \
         if (e__ != cudaSuccess) return ::spgnb::cuda_fail(e__, name);   \
     } while (0)
+
+// The force pass's kernels (slot pack, pruning, pair kernel, finishing pass,
+// and the soft-core and long-range kernels around it) are launched as
+// programmatic dependents of the kernel before them on the
+// stream: a grid may be scheduled while its predecessor drains, and each of
+// them starts with grid_dep_wait(), which returns once the predecessor has
+// completed and its writes are visible.  Every thread of these kernels passes
+// that wait before anything else, so a grid never completes before its
+// predecessor and the chain stays ordered.  Inside a stream capture (the
+// batched engine's graphs) they are launched plainly.
+template <typename... KArgs, typename... Args>
+cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                             Args&&... args)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusActive;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = cs == cudaStreamCaptureStatusNone ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
+// Waits for the grid launched before this one on the stream (a programmatic
+// dependent launch) to complete with its writes visible; a no-op when the
+// grid was launched plainly.
+__device__ __forceinline__ void grid_dep_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
 // events recorded around the pair kernel when set (benchmark instrumentation)
 void pair_events(cudaEvent_t* start, cudaEvent_t* stop);

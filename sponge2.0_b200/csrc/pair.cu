@@ -393,6 +393,7 @@ __global__ void k_pair_solvent(PairConst pc, Cell cell, Cell rcell, int res_begi
 __global__ void k_long_range(int need_pressure, float* virial, int need_potential, float* potential, float vfac,
                              float efac)
 {
+    grid_dep_wait();
     if (need_pressure)
     {
         virial[0] += vfac;
@@ -792,7 +793,8 @@ int spgnb_lj_long_range_correction(spgnb_lj* lj, int need_pressure, spgnb_ltmatr
     float efac = f / volume;
     lj->last_volume = volume;
     if (need_potential) lj->h_last_long_energy = efac;
-    k_long_range<<<1, 1, 0, stream()>>>(need_pressure, (float*)d_virial, need_potential, d_potential, vfac, efac);
+    launch_dependent(k_long_range, 1, 1, 0, stream(), need_pressure, (float*)d_virial, need_potential, d_potential,
+                     vfac, efac);
     SPGNB_CHECK_LAUNCH("k_long_range");
     return SPGNB_OK;
 }

@@ -184,6 +184,7 @@ __global__ void __launch_bounds__(kSoftWarps * 32)
                  const float* __restrict__ tBA, const float* __restrict__ tBB, long long* __restrict__ acc,
                  long long* __restrict__ totals, PerAtomOut pa, long long* __restrict__ dh)
 {
+    grid_dep_wait();
     const int lane = threadIdx.x & 31;
     const long long item = (long long)blockIdx.x * kSoftWarps + (threadIdx.x >> 5);
     if (item >= n_items) return;  // whole warps
@@ -336,6 +337,7 @@ __global__ void k_soft_local(int n, const int* __restrict__ atom_local, const in
 __global__ void k_mask_charge(int n, const float* __restrict__ q, const unsigned char* __restrict__ flag,
                               float* __restrict__ out)
 {
+    grid_dep_wait();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = flag[i] ? 0.0f : q[i];
 }
@@ -365,7 +367,7 @@ int launch_soft(const SoftConst& k, const spgnb_ltmatrix3& cell, const spgnb_ltm
     const long long warps = (long long)n_items * chunks;
     const long long grid = (warps + kSoftWarps - 1) / kSoftWarps;
     if (grid > 0x7fffffffLL) return fail(SPGNB_E_UNSUPPORTED, "soft-core kernel: %lld blocks", grid);
-    k_soft_pairs<FORCE, EN, PA, DH, DHC><<<(unsigned)grid, kSoftWarps * 32, 0, s>>>(
+    launch_dependent(k_soft_pairs<FORCE, EN, PA, DH, DHC>, (unsigned)grid, kSoftWarps * 32, 0, s,
         k, make_cell(cell), make_cell(rcell), warps, chunks, list, flag, atom_local, nl->d_atom_slot,
         nl->d_slot_atom,
         nl->d_tcount, nl->d_tab, nl->d_tmask, nl->table_cap, crd, charge, charge_ba, types, AA, AB, BA, BB, acc,
@@ -678,7 +680,7 @@ int spgnb_lj_soft_pme_direct_force(spgnb_lj_soft* lj, int atom_numbers, int loca
     // the perturbed atoms' pairs come from their clusters' two-sided tables
     if ((st = nl_two_sided_atoms(nl, lj->d_flag, s))) return st;
     const int n = local_atom_numbers;
-    k_mask_charge<<<(n + 255) / 256, 256, 0, s>>>(n, d_charge, lj->d_flag, lj->d_masked_q);
+    launch_dependent(k_mask_charge, (n + 255) / 256, 256, 0, s, n, d_charge, lj->d_flag, lj->d_masked_q);
     SPGNB_CHECK_LAUNCH("k_mask_charge");
     st = spgnb_lj_pme_direct_force(lj->inner, atom_numbers, local_atom_numbers, solvent_numbers, ghost_numbers, d_crd,
                                    lj->d_masked_q, d_frc, cell, rcell, nl, pme_beta, need_atom_energy, d_atom_energy,
