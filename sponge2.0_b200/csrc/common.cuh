@@ -284,12 +284,18 @@ struct spgnb_nl
     float prune_rc = 0;    // cutoff the pruned lists are made for
     bool built = false;
     int local_atoms = 0;
-    // neighbour tables two-sided (every neighbour cluster) for the exports,
-    // or one-sided (J >= I) when only the pruned half list reads them, except
-    // for the clusters holding an atom flagged in two_sided_atoms (the
-    // soft-core kernel's perturbed atoms); what the last build made, and its
-    // exclusion arrays
-    mutable bool sym_tables = false, sym_built = false;
+    // neighbour tables one-sided (J >= I), except for the clusters holding an
+    // atom flagged in two_sided_atoms (the soft-core kernel's perturbed
+    // atoms) and after nl_symmetrize (every cluster two-sided, until the next
+    // build); what the last build made, and its exclusion arrays
+    mutable bool sym_built = false;
+    // reverse index of the tables: for each cluster J, the elements
+    // c * table_cap + t of the lower clusters' tables (c < J) that hold J,
+    // ascending; with the cluster's own elements J' >= J it gives every atom
+    // its partners on both sides (the exports) from one-sided tables
+    int* d_rev = nullptr;        // clusters_cap x table_cap
+    int* d_rev_count = nullptr;  // clusters_cap
+    mutable bool rev_built = false;  // made from the current tables
     mutable const unsigned char* two_sided_atoms = nullptr;
     mutable const unsigned char* two_sided_built = nullptr;
     const int *ex_start_last = nullptr, *ex_list_last = nullptr, *ex_num_last = nullptr;
@@ -596,10 +602,9 @@ size_t nl_admit_upload_bytes(const SysHost& sh, size_t n_runs);
 int nl_retire(spgnb_nl* nl, int id, cudaStream_t s);
 // Every live system re-prunes before the next force evaluation.
 int nl_prune_all(spgnb_nl* nl, cudaStream_t s);
-// Makes the last build's neighbour tables two-sided, and with persist the
-// later builds' too: re-runs the last build's search (same clusters and
-// build coordinates, so the same list) when its tables are one-sided.
-int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s, bool persist = true);
+// Makes the last build's neighbour tables two-sided: re-runs its search (same
+// clusters and build coordinates, so the same list) when they are one-sided.
+int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s);
 // Makes the tables of the clusters holding a flagged atom (per local atom,
 // non-zero) two-sided, in the last build (re-searched if needed) and the
 // later ones.

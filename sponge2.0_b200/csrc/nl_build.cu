@@ -609,10 +609,74 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
     }
 }
 
+// Reverse index of the tables, made after a search: k_rev_clear and
+// k_rev_fill append every element (c, t) whose neighbour cluster J lies
+// above c to J's list (an atomic cursor), then k_rev_sort puts each list in
+// ascending element order (c, then t), so the index is the same on every
+// call.  A list longer than table_cap sets the table overflow flag (the
+// tables grow, as for the search's own overflow).  With need, only after a
+// rebuild.
+__global__ void k_rev_clear(int clusters_cap, int* __restrict__ rev_count, const int* __restrict__ need)
+{
+    if (need && *need == 0) return;
+    const int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c < clusters_cap) rev_count[c] = 0;
+}
+
+__global__ void k_rev_fill(int clusters_cap, int table_cap, const int* __restrict__ tcount,
+                           const float4* __restrict__ tab, int* __restrict__ rev, int* __restrict__ rev_count,
+                           int* counters, const int* __restrict__ need)
+{
+    if (need && *need == 0) return;
+    const int lane = threadIdx.x & 31;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < clusters_cap; c += warps)
+    {
+        const int T = tcount[c];
+        for (int t = lane; t < T; t += 32)
+        {
+            const int J = (__float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff) / kClusterSize;
+            if (J <= c) continue;
+            const int pos = atomicAdd(&rev_count[J], 1);
+            if (pos < table_cap)
+                rev[(size_t)J * table_cap + pos] = c * table_cap + t;
+            else
+                atomicOr(&counters[kCntOverflow], kOvfPairs);
+        }
+    }
+}
+
+constexpr int kRevWarps = 4;
+
+// One warp per cluster: its list staged in shared memory; each entry's place
+// is the number of entries below it (the entries differ).
+__global__ void k_rev_sort(int clusters_cap, int table_cap, int* __restrict__ rev, const int* __restrict__ rev_count,
+                           const int* __restrict__ need)
+{
+    if (need && *need == 0) return;
+    extern __shared__ int rev_buf[];  // kRevWarps x table_cap
+    const int lane = threadIdx.x & 31;
+    int* b = rev_buf + (threadIdx.x >> 5) * table_cap;
+    const int warps = gridDim.x * (blockDim.x >> 5);
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < clusters_cap; c += warps)
+    {
+        const int m = min(rev_count[c], table_cap);
+        int* r = rev + (size_t)c * table_cap;
+        for (int k = lane; k < m; k += 32) b[k] = r[k];
+        __syncwarp();
+        for (int k = lane; k < m; k += 32)
+        {
+            const int v = b[k];
+            int rank = 0;
+            for (int q = 0; q < m; q++) rank += b[q] < v ? 1 : 0;
+            r[rank] = v;
+        }
+        __syncwarp();
+    }
+}
+
 // Reference-layout export: zero the counts, then every listed pair goes to
-// its owner (the lower atom_local index) as the reference stores it.  Each
-// pair sits in both clusters' tables; the side whose own atom is the lower
-// index emits it.
+// its owner (the lower atom_local index) as the reference stores it.
 __global__ void k_export_zero(int n, spgnb_atom_group* __restrict__ nl, const int* __restrict__ counters)
 {
     if (counters[kCntNeed] == 0) return;
@@ -624,9 +688,11 @@ __global__ void k_export_zero(int n, spgnb_atom_group* __restrict__ nl, const in
     }
 }
 
-// ATOM_GROUP lists from the cluster tables, where each atom's partners on
-// both sides already sit with its own cluster, so one warp per atom writes
-// its list in table order: no atomics, the same order on every call.
+// ATOM_GROUP lists from the cluster tables: one warp per atom walks its own
+// cluster's elements with J >= its cluster (its upper partners) and then the
+// cluster's reverse index (the lower clusters' elements that hold it, whose
+// masks give the atom's column), so every partner on both sides comes once,
+// in the same order on every call, with no atomics.
 //   HALF: the reference-layout half list of NEIGHBOR_LIST::d_nl, each listed
 //   pair with its owner (the lower atom_local index) as the reference stores
 //   it; runs after a rebuild only (need: the device's rebuild flag).
@@ -643,7 +709,8 @@ __global__ void k_export_lists(int clusters_cap, int table_cap, const int* __res
                                const int* __restrict__ slot_gid, const float3* __restrict__ crd, Cell cell,
                                Cell rcell, float cut2,
                                spgnb_atom_group* __restrict__ full, int max_nb, int* __restrict__ overflow,
-                               int ovf_bits, const int* __restrict__ need)
+                               int ovf_bits, const int* __restrict__ need, const int* __restrict__ rev,
+                               const int* __restrict__ rev_count)
 {
     if (HALF && *need == 0) return;
     // a chunk's kept partners, compacted here so that the list is written
@@ -660,11 +727,12 @@ __global__ void k_export_lists(int clusters_cap, int table_cap, const int* __res
         const int ia = slot_atom[item];
         if (ia < 0) continue;  // warp-uniform
         const int T = tcount[c];
+        const int V = T + min(rev_count[c], table_cap);  // own elements, then the reverse index
         const int gia = __float_as_int(slot_x0[item].w);
         int* list = full[ia].atom_serial;
         const float3 xi = (!HALF && cut2 >= 0.0f) ? crd[ia] : make_float3(0.0f, 0.0f, 0.0f);
         int count = 0;
-        for (int t0 = 0; t0 < T; t0 += 32)
+        for (int t0 = 0; t0 < V; t0 += 32)
         {
             const int t = t0 + lane;
             unsigned row = 0;
@@ -674,15 +742,34 @@ __global__ void k_export_lists(int clusters_cap, int table_cap, const int* __res
             int4 na0 = make_int4(-1, -1, -1, -1), na1 = na0;
             if (t < T)
             {
-                const uint2 mm = tmask[(size_t)c * table_cap + t];
-                row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
+                // an own element: the atom's row; a neighbour cluster below
+                // this one (a two-sided table) comes from the reverse index
                 base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
-                if (row)
+                if (base >= c * kClusterSize)
                 {
-                    const int4* sa = reinterpret_cast<const int4*>(slot_atom + base);
-                    na0 = sa[0];
-                    na1 = sa[1];
+                    const uint2 mm = tmask[(size_t)c * table_cap + t];
+                    row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
                 }
+            }
+            else if (t < V)
+            {
+                // a lower cluster's element that holds this cluster: the
+                // atom's column of its mask (bit a' * 8 + a)
+                const int e = rev[(size_t)c * table_cap + (t - T)];
+                const uint2 mm = tmask[e];
+                base = (e / table_cap) * kClusterSize;
+#pragma unroll
+                for (int q = 0; q < 4; q++)
+                {
+                    row |= ((mm.x >> (8 * q + a)) & 1u) << q;
+                    row |= ((mm.y >> (8 * q + a)) & 1u) << (q + 4);
+                }
+            }
+            if (row)
+            {
+                const int4* sa = reinterpret_cast<const int4*>(slot_atom + base);
+                na0 = sa[0];
+                na1 = sa[1];
             }
             const int nb[kClusterSize] = {na0.x, na0.y, na0.z, na0.w, na1.x, na1.y, na1.z, na1.w};
             unsigned keep = row;
@@ -997,6 +1084,22 @@ void free_nl(spgnb_nl* nl)
     dfree(nl->d_counters);
     dfree(nl->d_nl);
     dfree(nl->d_temp);
+    dfree(nl->d_rev);
+    dfree(nl->d_rev_count);
+}
+
+// The reverse index of the tables (clusters_cap x table_cap element indices).
+int alloc_rev(spgnb_nl* nl)
+{
+    int st;
+    dfree(nl->d_rev);
+    dfree(nl->d_rev_count);
+    nl->rev_built = false;
+    const size_t n = (size_t)nl->clusters_cap * nl->table_cap;
+    if (n >= (size_t)0x7fffffff)
+        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %zu table elements exceed the reverse index's int range", n);
+    if ((st = dalloc(&nl->d_rev, n))) return st;
+    return dalloc(&nl->d_rev_count, nl->clusters_cap);
 }
 
 int alloc_tables(spgnb_nl* nl)
@@ -1007,6 +1110,30 @@ int alloc_tables(spgnb_nl* nl)
     const size_t n = (size_t)nl->clusters_cap * nl->table_cap;
     if ((st = dalloc(&nl->d_tab, n))) return st;
     if ((st = dalloc(&nl->d_tmask, n))) return st;
+    // the reverse index follows the tables' size once it exists
+    return nl->d_rev ? alloc_rev(nl) : SPGNB_OK;
+}
+
+// Makes the reverse index from the current tables (with need, only when the
+// device's rebuild flag is set).
+int build_rev(const spgnb_nl* nl, cudaStream_t s, const int* need)
+{
+    const int ccap = nl->clusters_cap;
+    const size_t smem = sizeof(int) * kRevWarps * (size_t)nl->table_cap;
+    if (smem > 227 * 1024)
+        return fail(SPGNB_E_UNSUPPORTED, "neighbour list: %d table elements per cluster exceed the reverse index's "
+                                         "sort", nl->table_cap);
+    const int warp_blocks = std::max(1, std::min((ccap + kRevWarps - 1) / kRevWarps, num_sms() * 16));
+    k_rev_clear<<<(ccap + 255) / 256, 256, 0, s>>>(ccap, nl->d_rev_count, need);
+    SPGNB_CHECK_LAUNCH("k_rev_clear");
+    k_rev_fill<<<warp_blocks, kRevWarps * 32, 0, s>>>(ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_rev,
+                                                      nl->d_rev_count, nl->d_counters, need);
+    SPGNB_CHECK_LAUNCH("k_rev_fill");
+    if (smem > 48 * 1024)
+        SPGNB_CUDA(cudaFuncSetAttribute(k_rev_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_rev_sort<<<warp_blocks, kRevWarps * 32, smem, s>>>(ccap, nl->table_cap, nl->d_rev, nl->d_rev_count, need);
+    SPGNB_CHECK_LAUNCH("k_rev_sort");
+    nl->rev_built = true;
     return SPGNB_OK;
 }
 
@@ -1141,8 +1268,9 @@ int alloc_nl(spgnb_nl* nl)
     SPGNB_CUDA(cudaMemset(nl->d_counters, 0, sizeof(int) * kCntSize));
     if ((st = alloc_tables(nl))) return st;
     if ((st = alloc_words(nl))) return st;
-    // the reference-layout export reads each atom's partners on both sides
-    nl->sym_tables = nl->opt.export_atom_groups != 0;
+    // the reference-layout export reads each atom's partners on both sides,
+    // the lower ones through the reverse index
+    if (nl->opt.export_atom_groups && (st = alloc_rev(nl))) return st;
     if (nl->opt.export_atom_groups)
     {
         if ((st = dalloc(&nl->d_nl, n))) return st;
@@ -1528,22 +1656,25 @@ int nl_queue_build_body(spgnb_nl* nl, int n, const float3* d_crd, const int* d_a
         nl->d_sys, ccap, nl->table_cap, nl->d_need, nl->d_ncl, nl->d_run_start, nl->d_runs, nl->d_cell_cl,
         nl->d_cl_cell, nl->d_cl_sys, nl->d_cl_u, nl->d_cl_q, nl->d_cl_c, nl->d_slot_x0, nl->d_slot_d0, nl->d_slot_ex,
         ex_start, ex_list, ex_num, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_count, nl->d_counters,
-        nl->d_counters + kCntNeed, nl->sym_tables ? 0 : 1, nl->d_slot_atom, nl->two_sided_atoms);
+        nl->d_counters + kCntNeed, 1, nl->d_slot_atom, nl->two_sided_atoms);
     SPGNB_CHECK_LAUNCH("k_search");
-    nl->sym_built = nl->sym_tables;
-    nl->two_sided_built = nl->sym_tables ? nullptr : nl->two_sided_atoms;
+    nl->sym_built = false;
+    nl->two_sided_built = nl->two_sided_atoms;
+    nl->rev_built = false;
     nl->ex_start_last = ex_start;
     nl->ex_list_last = ex_list;
     nl->ex_num_last = ex_num;
     if (nl->opt.export_atom_groups)
     {
+        int st = build_rev(nl, s, nl->d_counters + kCntNeed);
+        if (st) return st;
         k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_export_zero");
         k_export_lists<true><<<std::max(1, std::min((ccap * kClusterSize + 3) / 4, sms * 16)), 128, 0, s>>>(
             ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_gid,
             nullptr,
             Cell{}, Cell{}, -1.0f, nl->d_nl, nl->opt.max_neighbor_numbers, nl->d_counters + kCntOverflow, kOvfList,
-            nl->d_counters + kCntNeed);
+            nl->d_counters + kCntNeed, nl->d_rev, nl->d_rev_count);
         SPGNB_CHECK_LAUNCH("k_export_lists");
     }
     const int fin = std::max(nl->G, nl->S);
@@ -1811,12 +1942,12 @@ int research_last_build(const spgnb_nl* nl, cudaStream_t s, int half, const unsi
         nl->ex_start_last, nl->ex_list_last, nl->ex_num_last, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_count,
         nl->d_counters, nullptr, half, nl->d_slot_atom, flags);
     SPGNB_CHECK_LAUNCH("k_search");
+    nl->rev_built = false;  // the tables' elements moved
     return SPGNB_OK;
 }
 
-int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s, bool persist)
+int nl_symmetrize(const spgnb_nl* nl, cudaStream_t s)
 {
-    if (persist) nl->sym_tables = true;
     if (!nl->built || nl->sym_built) return SPGNB_OK;
     const int st = research_last_build(nl, s, 0, nullptr);
     if (st) return st;
@@ -1852,8 +1983,10 @@ int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector
     if (cutoff > 0.0f && !d_crd) return fail(SPGNB_E_ARG, "spgnb_nl_build_full: a cutoff needs coordinates");
     if (!d_overflow) return fail(SPGNB_E_ARG, "spgnb_nl_build_full: NULL overflow flag");
     cudaStream_t s = stream();
-    int st = nl_symmetrize(nl, s);
-    if (st) return st;
+    int st;
+    // each atom's lower partners through the reverse index of the tables
+    if (!nl->d_rev && (st = alloc_rev(nl))) return st;
+    if (!nl->rev_built && (st = build_rev(nl, s, nullptr))) return st;
     const int n = local_atom_numbers;
     // atoms in no cluster with a table (none, normally) keep a zero count
     k_zero_groups<<<(n + 255) / 256, 256, 0, s>>>(n, d_full_nl);
@@ -1862,7 +1995,7 @@ int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector
     k_export_lists<false><<<std::max(1, std::min((ccap * kClusterSize + 3) / 4, num_sms() * 16)), 128, 0, s>>>(
         ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_gid,
         (const float3*)d_crd, make_cell(cell), make_cell(rcell), cutoff > 0.0f ? cutoff * cutoff : -1.0f, d_full_nl,
-        max_neighbor_numbers, d_overflow, 1, nullptr);
+        max_neighbor_numbers, d_overflow, 1, nullptr, nl->d_rev, nl->d_rev_count);
     SPGNB_CHECK_LAUNCH("k_export_lists");
     return SPGNB_OK;
 }

@@ -738,7 +738,7 @@ int spgnb_lj_soft_partial_h_partial_lambda(spgnb_lj_soft* lj, int solvent_number
     // the atoms whose pairs it sums (the perturbed ones, and with charge
     // perturbation every atom whose charge changes) read their clusters'
     // tables: two-sided ones for this call (a rare one: output steps)
-    if ((st = nl_symmetrize(nl, s, false))) return st;
+    if ((st = nl_symmetrize(nl, s))) return st;
     SPGNB_CUDA(cudaMemsetAsync(lj->d_dh, 0, 2 * sizeof(long long), s));
     const SoftConst k = soft_const(lj, pme_beta);
     const float3* crd = (const float3*)d_crd;
