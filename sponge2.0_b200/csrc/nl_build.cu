@@ -688,11 +688,13 @@ __global__ void k_export_zero(int n, spgnb_atom_group* __restrict__ nl, const in
     }
 }
 
-// ATOM_GROUP lists from the cluster tables: one warp per atom walks its own
-// cluster's elements with J >= its cluster (its upper partners) and then the
-// cluster's reverse index (the lower clusters' elements that hold it, whose
-// masks give the atom's column), so every partner on both sides comes once,
-// in the same order on every call, with no atomics.
+// ATOM_GROUP lists from the cluster tables: one warp per cluster walks its
+// own elements with J >= the cluster (its atoms' upper partners) and then
+// its reverse index (the lower clusters' elements that hold it, whose masks
+// give each own atom's column), a chunk of 32 elements at a time loaded once
+// for the cluster's eight atoms; each atom's kept partners are compacted and
+// appended to its list, so every partner on both sides comes once, in the
+// same order on every call, with no atomics.
 //   HALF: the reference-layout half list of NEIGHBOR_LIST::d_nl, each listed
 //   pair with its owner (the lower atom_local index) as the reference stores
 //   it; runs after a rebuild only (need: the device's rebuild flag).
@@ -713,116 +715,142 @@ __global__ void k_export_lists(int clusters_cap, int table_cap, const int* __res
                                const int* __restrict__ rev_count)
 {
     if (HALF && *need == 0) return;
-    // a chunk's kept partners, compacted here so that the list is written
-    // with contiguous stores (blocks of 128 threads)
+    // an atom's kept partners of a chunk, compacted here so that its list is
+    // written with contiguous stores (blocks of 128 threads)
     __shared__ int staged[4][32 * kClusterSize];
     const int lane = threadIdx.x & 31;
     int* const stage = staged[threadIdx.x >> 5];
     const int warps = gridDim.x * (blockDim.x >> 5);
-    // one warp per own slot (cluster c, atom a): its list in table order
-    for (int item = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); item < clusters_cap * kClusterSize;
-         item += warps)
+    for (int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); c < clusters_cap; c += warps)
     {
-        const int c = item / kClusterSize, a = item % kClusterSize;
-        const int ia = slot_atom[item];
-        if (ia < 0) continue;  // warp-uniform
         const int T = tcount[c];
         const int V = T + min(rev_count[c], table_cap);  // own elements, then the reverse index
-        const int gia = __float_as_int(slot_x0[item].w);
-        int* list = full[ia].atom_serial;
-        const float3 xi = (!HALF && cut2 >= 0.0f) ? crd[ia] : make_float3(0.0f, 0.0f, 0.0f);
-        int count = 0;
+        // the cluster's own atoms (the same in every lane)
+        int ia[kClusterSize], gia[kClusterSize], count[kClusterSize];
+#pragma unroll
+        for (int a = 0; a < kClusterSize; a++)
+        {
+            ia[a] = slot_atom[c * kClusterSize + a];
+            gia[a] = __float_as_int(slot_x0[c * kClusterSize + a].w);
+            count[a] = 0;
+        }
         for (int t0 = 0; t0 < V; t0 += 32)
         {
             const int t = t0 + lane;
-            unsigned row = 0;
+            uint2 mm = make_uint2(0u, 0u);
+            bool col = false;  // a reverse element: the own atom's column of the mask
             int base = 0;
-            // the neighbour cluster's eight atoms (and global indices), in two
-            // 16-byte loads each: a cluster's slots start on an 8-slot boundary
-            int4 na0 = make_int4(-1, -1, -1, -1), na1 = na0;
             if (t < T)
             {
-                // an own element: the atom's row; a neighbour cluster below
-                // this one (a two-sided table) comes from the reverse index
+                // a neighbour cluster below this one (a two-sided table) comes
+                // from the reverse index
                 base = __float_as_int(tab[(size_t)c * table_cap + t].w) & 0x3fffffff;
-                if (base >= c * kClusterSize)
-                {
-                    const uint2 mm = tmask[(size_t)c * table_cap + t];
-                    row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
-                }
+                if (base >= c * kClusterSize) mm = tmask[(size_t)c * table_cap + t];
             }
             else if (t < V)
             {
-                // a lower cluster's element that holds this cluster: the
-                // atom's column of its mask (bit a' * 8 + a)
                 const int e = rev[(size_t)c * table_cap + (t - T)];
-                const uint2 mm = tmask[e];
+                mm = tmask[e];
                 base = (e / table_cap) * kClusterSize;
-#pragma unroll
-                for (int q = 0; q < 4; q++)
-                {
-                    row |= ((mm.x >> (8 * q + a)) & 1u) << q;
-                    row |= ((mm.y >> (8 * q + a)) & 1u) << (q + 4);
-                }
+                col = true;
             }
-            if (row)
+            // the neighbour cluster's eight atoms (and global indices), in two
+            // 16-byte loads each: a cluster's slots start on an 8-slot boundary
+            int4 na0 = make_int4(-1, -1, -1, -1), na1 = na0, g0 = na0, g1 = na0;
+            if (mm.x | mm.y)
             {
                 const int4* sa = reinterpret_cast<const int4*>(slot_atom + base);
                 na0 = sa[0];
                 na1 = sa[1];
-            }
-            const int nb[kClusterSize] = {na0.x, na0.y, na0.z, na0.w, na1.x, na1.y, na1.z, na1.w};
-            unsigned keep = row;
-            if (HALF && row)
-            {
-                const int4* sg = reinterpret_cast<const int4*>(slot_gid + base);
-                const int4 g0 = sg[0], g1 = sg[1];
-                const int gb[kClusterSize] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
-                unsigned above = 0;
-#pragma unroll
-                for (int b = 0; b < kClusterSize; b++) above |= (gia < gb[b] ? 1u : 0u) << b;
-                keep = row & above;
-            }
-            else if (!HALF && cut2 >= 0.0f && row)
-            {
-                keep = 0;
-                for (unsigned r = row; r; r &= r - 1)
+                if (HALF)
                 {
-                    const int b = __ffs(r) - 1;
-                    const int jb = slot_atom[base + b];
-                    const float3 xj = crd[jb];
-                    const bool i_lo = gia < __float_as_int(slot_x0[base + b].w);
-                    const float d2 = i_lo ? ref_pair_dr2(xi, xj, cell, rcell) : ref_pair_dr2(xj, xi, cell, rcell);
-                    if (d2 <= cut2) keep |= 1u << b;
+                    const int4* sg = reinterpret_cast<const int4*>(slot_gid + base);
+                    g0 = sg[0];
+                    g1 = sg[1];
                 }
             }
-            const int k = __popc(keep);
-            int incl = k;
-            for (int o = 1; o < 32; o <<= 1)
-            {
-                const int y = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += y;
-            }
-            int pos = incl - k;
+            const int nb[kClusterSize] = {na0.x, na0.y, na0.z, na0.w, na1.x, na1.y, na1.z, na1.w};
+            const int gb[kClusterSize] = {g0.x, g0.y, g0.z, g0.w, g1.x, g1.y, g1.z, g1.w};
 #pragma unroll
-            for (int b = 0; b < kClusterSize; b++)
-                if ((keep >> b) & 1u) stage[pos++] = nb[b];
-            __syncwarp();
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            for (int q = lane; q < total; q += 32)
+            for (int a = 0; a < kClusterSize; a++)
             {
-                if (count + q < max_nb)
-                    list[count + q] = stage[q];
+                if (ia[a] < 0) continue;  // warp-uniform
+                unsigned row;
+                if (col)
+                {
+                    // bit a' * 8 + a of the lower cluster's element
+                    row = 0;
+#pragma unroll
+                    for (int q = 0; q < 4; q++)
+                    {
+                        row |= ((mm.x >> (8 * q + a)) & 1u) << q;
+                        row |= ((mm.y >> (8 * q + a)) & 1u) << (q + 4);
+                    }
+                }
                 else
-                    atomicOr(overflow, ovf_bits);
+                    row = ((a < 4 ? mm.x : mm.y) >> (8 * (a & 3))) & 0xffu;
+                unsigned keep = row;
+                if (HALF && row)
+                {
+                    unsigned above = 0;
+#pragma unroll
+                    for (int b = 0; b < kClusterSize; b++) above |= (gia[a] < gb[b] ? 1u : 0u) << b;
+                    keep = row & above;
+                }
+                else if (!HALF && cut2 >= 0.0f && row)
+                {
+                    const float3 xi = crd[ia[a]];
+                    keep = 0;
+                    for (unsigned r = row; r; r &= r - 1)
+                    {
+                        const int b = __ffs(r) - 1;
+                        const float3 xj = crd[nb[b]];
+                        const bool i_lo = gia[a] < __float_as_int(slot_x0[base + b].w);
+                        const float d2 = i_lo ? ref_pair_dr2(xi, xj, cell, rcell) : ref_pair_dr2(xj, xi, cell, rcell);
+                        if (d2 <= cut2) keep |= 1u << b;
+                    }
+                }
+                const int k = __popc(keep);
+                int incl = k;
+                for (int o = 1; o < 32; o <<= 1)
+                {
+                    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+                    if (lane >= o) incl += y;
+                }
+                const int total = __shfl_sync(0xffffffffu, incl, 31);
+                if (total == 0) continue;  // warp-uniform
+                int pos = incl - k;
+#pragma unroll
+                for (int b = 0; b < kClusterSize; b++)
+                    if ((keep >> b) & 1u) stage[pos++] = nb[b];
+                __syncwarp();
+                int* list = full[ia[a]].atom_serial;
+                for (int q = lane; q < total; q += 32)
+                {
+                    if (count[a] + q < max_nb)
+                        list[count[a] + q] = stage[q];
+                    else
+                        atomicOr(overflow, ovf_bits);
+                }
+                __syncwarp();
+                count[a] += total;
             }
-            __syncwarp();
-            count += total;
         }
-        if (lane == 0)
+        if (lane < kClusterSize)
         {
-            full[ia].atom_numbers = count;
-            full[ia].ghost_numbers = 0;
+            int ca = 0, ja = -1;
+#pragma unroll
+            for (int a = 0; a < kClusterSize; a++)
+                if (a == lane)
+                {
+                    ca = count[a];
+                    ja = ia[a];
+                }
+            if (ja >= 0)
+            {
+                full[ja].atom_numbers = ca;
+                full[ja].ghost_numbers = 0;
+            }
         }
     }
 }
@@ -1670,7 +1698,7 @@ int nl_queue_build_body(spgnb_nl* nl, int n, const float3* d_crd, const int* d_a
         if (st) return st;
         k_export_zero<<<(n + 255) / 256, 256, 0, s>>>(n, nl->d_nl, nl->d_counters);
         SPGNB_CHECK_LAUNCH("k_export_zero");
-        k_export_lists<true><<<std::max(1, std::min((ccap * kClusterSize + 3) / 4, sms * 16)), 128, 0, s>>>(
+        k_export_lists<true><<<std::max(1, std::min((ccap + 3) / 4, sms * 16)), 128, 0, s>>>(
             ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_gid,
             nullptr,
             Cell{}, Cell{}, -1.0f, nl->d_nl, nl->opt.max_neighbor_numbers, nl->d_counters + kCntOverflow, kOvfList,
@@ -1992,7 +2020,7 @@ int spgnb_nl_build_full(spgnb_nl* nl, int local_atom_numbers, const spgnb_vector
     k_zero_groups<<<(n + 255) / 256, 256, 0, s>>>(n, d_full_nl);
     SPGNB_CHECK_LAUNCH("k_zero_groups");
     const int ccap = nl->clusters_cap;
-    k_export_lists<false><<<std::max(1, std::min((ccap * kClusterSize + 3) / 4, num_sms() * 16)), 128, 0, s>>>(
+    k_export_lists<false><<<std::max(1, std::min((ccap + 3) / 4, num_sms() * 16)), 128, 0, s>>>(
         ccap, nl->table_cap, nl->d_tcount, nl->d_tab, nl->d_tmask, nl->d_slot_atom, nl->d_slot_x0, nl->d_slot_gid,
         (const float3*)d_crd, make_cell(cell), make_cell(rcell), cutoff > 0.0f ? cutoff * cutoff : -1.0f, d_full_nl,
         max_neighbor_numbers, d_overflow, 1, nullptr, nl->d_rev, nl->d_rev_count);
