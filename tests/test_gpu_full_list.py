@@ -64,3 +64,34 @@ def test_full_list_matches_reference_rule(torch_cuda, oracle, name, cutoff_full)
         assert len(got) == counts[i], f"atom {i}: repeated partners"
         diff = {(i, j) for j in got ^ want[i]}
         assert diff <= ambiguous, f"atom {i}: {sorted(diff)[:5]}"
+
+
+def test_full_list_same_from_one_and_two_sided_tables(torch_cuda):
+    """Each atom's upper partners come from its own cluster's table, its lower
+    ones through the reverse index of the tables; the full list must come out
+    bitwise the same whether the tables are one-sided (a plain build),
+    two-sided for the perturbed atoms' clusters (after a soft-core force
+    call) or two-sided everywhere (after dH/dlambda), and hold every pair in
+    both atoms' lists once."""
+    from spgnb import systems as S
+    from spgnb.engine import SoftCorePath
+    f = S.fep_system(S.water_system(1000, 31.0, 41, n_solute=100, cutoff=8.0, skin=2.0), n_perturbed=24)
+    p = SoftCorePath(f, device="cuda:0")
+    s = p.system
+
+    def full():
+        counts, temp, ovf = p.nl.build_full(s.n, p.crd, s.cell, s.rcell, 0.0, 1200)
+        assert int(ovf.item()) == 0
+        return counts.cpu().numpy().copy(), temp.cpu().numpy().copy()
+
+    one = full()
+    p.force(need_energy=True, need_virial=True)
+    part = full()
+    p.dhdl(charge_perturbated=True)
+    every = full()
+    for what, x in (("perturbed atoms' clusters two-sided", part), ("every cluster two-sided", every)):
+        assert np.array_equal(one[0], x[0]) and np.array_equal(one[1], x[1]), what
+    counts, temp = one
+    pairs = {(i, int(j)) for i in range(s.n) for j in temp[i, :counts[i]]}
+    assert len(pairs) == int(counts.sum()), "a partner listed twice"
+    assert all((j, i) in pairs for (i, j) in pairs), "a pair in one atom's list only"
