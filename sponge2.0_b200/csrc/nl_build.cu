@@ -373,13 +373,14 @@ __device__ __forceinline__ float3 frac_to_cart(float3 f, const Cell& c)
     return make_float3(f.x * c.a11 + f.y * c.a21 + f.z * c.a31, f.y * c.a22 + f.z * c.a32, f.z * c.a33);
 }
 
-// Neighbour search, one warp per cluster.  Symmetric (two-sided) tables:
-// every cluster finds all of its neighbour clusters (lower and higher), so
-// its table comes out complete and in a deterministic order (candidate runs,
-// then cluster index) with no sorting or atomics; the reference-layout and
-// full-list exports and the soft-core kernel read those.  One-sided tables
-// (half set): a cluster keeps only neighbour clusters J >= I, each cluster
-// pair is searched once, and the pruned half list needs no more.  For each candidate cluster that passes a
+// Neighbour search, one warp per cluster, its table in a deterministic order
+// (candidate runs, then cluster index) with no sorting or atomics.
+// One-sided tables (half set): a cluster keeps only neighbour clusters
+// J >= I, so each cluster pair is searched once; the pruned half list needs
+// no more, and the exports reach the lower side through the reverse index.
+// Symmetric (two-sided) tables, every neighbour cluster lower and higher:
+// for the clusters holding a flagged atom (the soft-core kernel's perturbed
+// atoms), or all clusters (dH/dlambda).  For each candidate cluster that passes a
 // conservative sphere test, the 64 atom pairs are decided as the reference
 // decides them: a pair needs the higher-index atom's cell in the stencil of
 // the lower-index atom's cell, squared distance below 4*grid_length^2 in the
