@@ -546,22 +546,39 @@ __global__ void __launch_bounds__(kSearchWarps * 32, 5)
                                fabsf(fd.z) + rr * p.frac_norm[2] < 0.49f;
                     }
                     unsigned bits[2];
+                    // both rounds' distances first, then one vote for the border
+                    // cases (the cheap distance only decides pairs well away
+                    // from the threshold, so its rounding does not matter)
+                    const float ex = Dx + dj.x, ey = Dy + dj.y, ez = Dz + dj.z;
+                    const bool gb_ok = gb >= 0, self = cjs == c;
+                    bool in_h[2], border_h[2], rule_h[2];
+#pragma unroll
                     for (int h = 0; h < 2; h++)
                     {
                         const int a = h * 4 + (lane >> 3);
                         const bool a_lo = ga[h] < gb;
-                        const bool rule = ga[h] >= 0 && gb >= 0 && (cjs != c || b != a) && (a_lo ? fwd : rev);
-                        const float dx = Dx + (dj.x - da[h].x), dy = Dy + (dj.y - da[h].y), dz = Dz + (dj.z - da[h].z);
+                        rule_h[h] = ga[h] >= 0 && gb_ok && (!self || b != a) && (a_lo ? fwd : rev);
+                        const float dx = ex - da[h].x, dy = ey - da[h].y, dz = ez - da[h].z;
                         const float d2 = dx * dx + dy * dy + dz * dz;
-                        const bool border = rule && (!safe || fabsf(d2 - p.cs2) < band);
-                        bool in = d2 < p.cs2;
-                        if (__any_sync(0xffffffffu, border) && border)
-                        {
-                            const float e2 = a_lo ? ref_pair_dr2(xa[h], xb, p.cell, p.rcell)
-                                                  : ref_pair_dr2(xb, xa[h], p.cell, p.rcell);
-                            in = e2 < p.cs2;
-                        }
-                        in = in && rule;
+                        border_h[h] = rule_h[h] && (!safe || fabsf(d2 - p.cs2) < band);
+                        in_h[h] = d2 < p.cs2;
+                    }
+                    if (__any_sync(0xffffffffu, border_h[0] || border_h[1]))
+                    {
+#pragma unroll
+                        for (int h = 0; h < 2; h++)
+                            if (border_h[h])
+                            {
+                                const float e2 = ga[h] < gb ? ref_pair_dr2(xa[h], xb, p.cell, p.rcell)
+                                                            : ref_pair_dr2(xb, xa[h], p.cell, p.rcell);
+                                in_h[h] = e2 < p.cs2;
+                            }
+                    }
+#pragma unroll
+                    for (int h = 0; h < 2; h++)
+                    {
+                        const bool a_lo = ga[h] < gb;
+                        bool in = in_h[h] && rule_h[h];
                         if (in)
                         {
                             // the lower index's exclusion list, scanned only within its range
