@@ -57,7 +57,13 @@ cudaError_t launch_dependent(void (*kernel)(KArgs...), dim3 grid, dim3 block, si
                              Args&&... args)
 {
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess) cs = cudaStreamCaptureStatusActive;
+    if (cudaStreamIsCapturing(s, &cs) != cudaSuccess)
+    {
+        // not known: launch plainly, and leave no error behind for the
+        // launch check that follows
+        cudaGetLastError();
+        cs = cudaStreamCaptureStatusActive;
+    }
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
     attr[0].val.programmaticStreamSerializationAllowed = 1;
