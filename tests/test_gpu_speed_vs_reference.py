@@ -8,8 +8,8 @@ the solvent module) with a 40-atom perturbed ligand.  Both sides rebuild the
 list every 20 steps; each path is timed with energy and virial (per-atom
 arrays) every step and with forces only, SPONGE's step between energy
 outputs.  Prints one JSON line per path (run with -s); fails when force-only
-steps are not at least 1.3x the reference kernels' speed, or energy steps
-fall behind them."""
+steps are not at least 1.5x the reference kernels' speed, or energy steps
+not at least 1.1x."""
 import json
 import os
 
@@ -80,7 +80,7 @@ def test_plain_and_soft_core_paths_vs_reference_kernels(torch_cuda):
     if UNDER_PROFILER:
         return
     for (name, ev), v in speedup.items():
-        # force-only steps (SPONGE's step between energy outputs) clearly
-        # ahead (measured 1.55x); energy steps with per-atom outputs not
-        # behind (measured 1.06x; host-clock loops on a shared box)
-        assert v >= (0.97 if ev else 1.3), (name, ev, v)
+        # measured 1.93x (force-only, SPONGE's step between energy outputs)
+        # and 1.26x (per-atom energy and virial every step); the floors leave
+        # room for host-clock loops on a shared box
+        assert v >= (1.1 if ev else 1.5), (name, ev, v)
